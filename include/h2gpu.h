@@ -1,0 +1,202 @@
+/*
+ * h2gpu.h -- C ABI of the B200 (sm_100a) H2 matrix apply engine.
+ *
+ * The engine multiplies an H2 matrix representation produced by H2Pack's
+ * construction (H2P_partition_points + H2P_build) by vectors and matrices on one
+ * GPU.  Everything here is plain C: pointers, sizes and status codes; no CUDA or
+ * torch types appear in the signatures (streams are passed as void*).
+ *
+ * What each entry point replaces in the reference (paths are within the
+ * H2Pack project):
+ *   h2gpu_image_create   the per-handle state that H2P_matvec/H2P_matmul keep in
+ *                        struct H2Pack (src/H2Pack_typedef.h:88-205): y0/y1
+ *                        buffers (src/H2Pack_matvec.c:68-92, :234-269), thread
+ *                        buffers, B_blk/D_blk task partitions
+ *                        (src/H2Pack_build.c:762-764, :1006-1008)
+ *   h2gpu_matvec         H2P_matvec (src/H2Pack_matvec.h:17, src/H2Pack_matvec.c:1162-1284)
+ *   h2gpu_matmul         H2P_matmul (src/H2Pack_matmul.h:25-28, src/H2Pack_matmul.c:455-583)
+ *   h2gpu_permute_*      H2P_permute_vector_{forward,backward} (src/H2Pack_matvec.h:29-30)
+ *                        and H2P_permute_matrix_row_{forward,backward}
+ *                        (src/H2Pack_matmul.h:47-54)
+ *   h2gpu_direct_sum     direct_nbody (examples/direct_nbody.h:2-54)
+ *   h2gpu_get_stats      the timers[] / mat_size[] / JIT_flops[] counters
+ *                        (src/H2Pack_typedef.h:200-204, :226-239) read by
+ *                        H2P_print_statistic (src/H2Pack_typedef.c:345-524)
+ *
+ * All functions return H2GPU_OK (0) or a negative status; h2gpu_last_error()
+ * returns a thread-local message for the last failure.  No function traps on the
+ * device and there is no CPU fallback: a missing GPU is an error.
+ */
+#ifndef H2GPU_H
+#define H2GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define H2GPU_ABI_VERSION 1
+
+/* Status codes */
+#define H2GPU_OK               0
+#define H2GPU_ERR_INVALID     -1   /* malformed descriptor or argument          */
+#define H2GPU_ERR_UNSUPPORTED -2   /* mode the engine does not implement        */
+#define H2GPU_ERR_CUDA        -3   /* CUDA runtime error (no GPU, launch, ...)  */
+#define H2GPU_ERR_NOMEM       -4   /* device or host allocation failed          */
+#define H2GPU_ERR_STATE       -5   /* call out of order / handle destroyed      */
+#define H2GPU_ERR_DEVICE      -6   /* device-side check failed (status word)    */
+
+/* Kernel functions K(x, y).  The reference keeps only function pointers to
+ * static functions (src/H2Pack_typedef.h:193-196, src/H2Pack_3D_kernels.h), so
+ * the kernel identity crosses the ABI as an id plus its parameter array. */
+#define H2GPU_KRNL_NONE      0    /* AOT only: B and D are stored               */
+#define H2GPU_KRNL_COULOMB   1    /* 1/r, param[0] on r == 0 (0 if no param),    src/H2Pack_3D_kernels.h:50-161 */
+#define H2GPU_KRNL_GAUSSIAN  2    /* exp(-l r^2), l = param[0],                  src/H2Pack_3D_kernels.h:167-268 */
+#define H2GPU_KRNL_MATERN32  3    /* (1+sqrt3 l r) exp(-sqrt3 l r), l = param[0], src/H2Pack_3D_kernels.h:384-497 */
+#define H2GPU_KRNL_RPY       4    /* 3x3 Rotne-Prager-Yamakawa, eta = param[0], radius in coord row 3,
+                                     src/H2Pack_3D_kernels.h:893-959, :1310-1430 */
+
+/* Arithmetic of the apply */
+#define H2GPU_PREC_FP64   0       /* plain drop-in: every product and sum in FP64       */
+#define H2GPU_PREC_MIXED  1       /* FP32 blocks / FP32 re-centred kernel evaluation,
+                                     FP32 sums inside one block, FP64 across blocks     */
+
+/* Matrix layouts of h2gpu_matmul (numerically equal to CBLAS_LAYOUT) */
+#define H2GPU_ROW_MAJOR 101
+#define H2GPU_COL_MAJOR 102
+
+/*
+ * Plain-pointer view of one H2 representation.  Every field has the meaning of
+ * the struct H2Pack field of the same name (src/H2Pack_typedef.h:88-205); arrays
+ * are read during h2gpu_image_create only and may be freed afterwards.
+ */
+typedef struct h2gpu_desc
+{
+    int n_point;            /* number of points                                    */
+    int pt_dim;             /* point dimension (3)                                 */
+    int xpt_dim;            /* coordinate rows (4 for RPY: x, y, z, radius)        */
+    int krnl_dim;           /* kernel block dimension (1, or 3 for RPY)            */
+    int n_node;
+    int n_leaf_node;
+    int max_child;          /* 2^pt_dim                                            */
+    int max_level;
+    int min_adm_level;      /* H2 mode value (HSS mode is rejected)                */
+    int BD_JIT;             /* 1: B and D are evaluated on the fly                 */
+
+    const int *n_child;     /* [n_node]                                            */
+    const int *children;    /* [n_node * max_child]                                */
+    const int *node_level;  /* [n_node]                                            */
+    const int *pt_cluster;  /* [2 * n_node] first and last (inclusive) point       */
+    const int *mat_cluster; /* [2 * n_node] first and last (inclusive) vector row  */
+    const int *level_n_node;/* [max_level + 1]                                     */
+    const int *level_nodes; /* [(max_level + 1) * n_leaf_node]                     */
+    const int *leaf_nodes;  /* [n_leaf_node] = height_nodes row 0: order of the
+                               diagonal D blocks (src/H2Pack_build.c:948-968)       */
+
+    const int *U_nrow;      /* [n_node]                                            */
+    const int *U_ncol;      /* [n_node]                                            */
+    const int *U_ld;        /* [n_node] row stride of U[i] (>= U_ncol[i])          */
+    const double *const *U; /* [n_node] row-major U[i]; NULL when empty            */
+
+    int n_r_adm_pair;
+    const int *r_adm_pairs;   /* [2 * n_r_adm_pair]                                */
+    int n_r_inadm_pair;
+    const int *r_inadm_pairs; /* [2 * n_r_inadm_pair]                              */
+
+    int n_B;                  /* == n_r_adm_pair                                    */
+    const int *B_nrow;        /* [n_B]                                              */
+    const int *B_ncol;        /* [n_B]                                              */
+    const size_t *B_ptr;      /* [n_B + 1] element offsets into B_data              */
+    const double *B_data;     /* AOT only (NULL when BD_JIT)                        */
+    int n_D;                  /* == n_leaf_node + n_r_inadm_pair                    */
+    const int *D_nrow;
+    const int *D_ncol;
+    const size_t *D_ptr;
+    const double *D_data;     /* AOT only                                           */
+
+    const double *coord;      /* [xpt_dim * n_point], row d at coord + d * n_point,
+                                 points in H2Pack's sorted order                    */
+    const int *J_n;           /* [n_node] skeleton point counts                     */
+    const double *const *J_coord; /* [n_node] xpt_dim x J_n[i], ld = J_n[i]        */
+
+    const int *fwd_pmt_idx;   /* [krnl_dim * n_point]                               */
+    const int *bwd_pmt_idx;   /* [krnl_dim * n_point]                               */
+
+    int kernel_id;            /* H2GPU_KRNL_*; required when BD_JIT                 */
+    int n_krnl_param;         /* 0 .. 4                                             */
+    double krnl_param[4];
+} h2gpu_desc;
+
+/* Options of an image */
+typedef struct h2gpu_options
+{
+    int precision;      /* H2GPU_PREC_FP64 or H2GPU_PREC_MIXED                        */
+    int max_n_vec;      /* widest right-hand-side panel per pass (default 16)         */
+    int device;         /* CUDA device ordinal (default: current device)              */
+} h2gpu_options;
+
+typedef struct h2gpu_image h2gpu_image;
+
+/* Phase statistics, accumulated over calls (the reference's timers[] and
+ * mat_size[] plus the device-side view). */
+typedef struct h2gpu_stats
+{
+    long long n_matvec;       /* right-hand sides applied (src/H2Pack_matvec.c:1283)  */
+    double ms_total;          /* device time of all applies                           */
+    double ms_phase[5];       /* gather/up, B, down, D, assemble (device events)      */
+    double bytes_U;           /* U bytes read by one upward + one downward sweep       */
+    double bytes_B;           /* stored B bytes (AOT)                                  */
+    double bytes_D;           /* stored D bytes (AOT)                                  */
+    double ref_mv_bytes;      /* 8*(mat_size[MV_FWD]+[MV_MID]+[MV_BWD]+[MV_DEN]) model */
+    double jit_pairs_B;       /* kernel evaluations of the B phase per RHS panel       */
+    double jit_pairs_D;       /* kernel evaluations of the D phase per RHS panel       */
+    long long n_tasks_B, n_tasks_D;
+    long long device_bytes;   /* device memory held by the image                      */
+} h2gpu_stats;
+
+int  h2gpu_abi_version(void);
+const char *h2gpu_last_error(void);
+void h2gpu_default_options(h2gpu_options *opt);
+
+int h2gpu_image_create(const h2gpu_desc *desc, const h2gpu_options *opt, h2gpu_image **out);
+int h2gpu_image_destroy(h2gpu_image *img);
+int h2gpu_set_precision(h2gpu_image *img, int precision);
+
+/* y := A x with host vectors in the caller's original point order. */
+int h2gpu_matvec(h2gpu_image *img, const double *x, double *y);
+
+/* Y := A X, n_vec right-hand sides, host matrices, CBLAS-style layout. */
+int h2gpu_matmul(h2gpu_image *img, int layout, int n_vec,
+                 const double *X, int ldx, double *Y, int ldy);
+
+/* Device-resident forms: X and Y are device pointers, row-major
+ * (krnl_mat_size x n_vec, leading dimensions ldx / ldy >= n_vec), original
+ * order; stream is a cudaStream_t or NULL for the image's own stream. */
+int h2gpu_matmul_device(h2gpu_image *img, int n_vec, const double *dX, int ldx,
+                        double *dY, int ldy, void *stream);
+
+/* Permutations between the caller's order and H2Pack's sorted order, on host data. */
+int h2gpu_permute_vector(h2gpu_image *img, int forward, const double *x, double *px);
+int h2gpu_permute_matrix_rows(h2gpu_image *img, int forward, int layout, int n_vec,
+                              const double *X, int ldx, double *PX, int ldp);
+
+int h2gpu_get_stats(h2gpu_image *img, h2gpu_stats *st);
+int h2gpu_reset_stats(h2gpu_image *img);
+size_t h2gpu_image_bytes(const h2gpu_image *img);
+
+/*
+ * FP64 direct sum on the device: y_t = sum_s K(x_t, x_s) v_s for n_trg targets
+ * and n_src sources (coordinates xpt_dim x n, ld = n, host arrays; values are
+ * krnl_dim-interleaved per point as in the H2 vectors).
+ */
+int h2gpu_direct_sum(int kernel_id, const double *krnl_param, int n_krnl_param,
+                     int xpt_dim, int krnl_dim,
+                     const double *src_coord, int n_src, const double *src_val,
+                     const double *trg_coord, int n_trg, double *trg_val);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
