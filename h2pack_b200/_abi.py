@@ -60,6 +60,7 @@ class Stats(C.Structure):
         ("bytes_U", C.c_double), ("bytes_B", C.c_double), ("bytes_D", C.c_double),
         ("ref_mv_bytes", C.c_double), ("jit_pairs_B", C.c_double), ("jit_pairs_D", C.c_double),
         ("n_tasks_B", C.c_longlong), ("n_tasks_D", C.c_longlong), ("device_bytes", C.c_longlong),
+        ("n_launches", C.c_longlong),
     ]
 
 

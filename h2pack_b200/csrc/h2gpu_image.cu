@@ -1,0 +1,1091 @@
+// h2gpu_image.cu -- device image of one H2 representation and the C ABI (include/h2gpu.h).
+//
+// h2gpu_image_create turns the plain-pointer view of struct H2Pack into flat task
+// lists per phase (built once on the host, uploaded once):
+//   * upward / downward tasks per tree level (levels are the only serial
+//     dependency, src/H2Pack_matvec.c:113, :314),
+//   * AOT: one record per <= 64-row chunk of every stored B / D block
+//     (replacing the static B_blk / D_blk thread partitions, src/H2Pack_build.c:762-764,
+//     :1006-1008, and the per-thread output copies, src/H2Pack_matvec.c:1191-1263),
+//   * JIT: one record per target chunk with the list of its source point sets
+//     (the admissible / inadmissible pair lists of src/H2Pack_partition.c:327-432
+//     turned into per-node interaction lists),
+//   * slot lists that say which partial results sum into which output rows.
+// Applying the matrix is then a fixed sequence of kernel launches per panel of
+// right-hand sides; nothing is allocated or built in the apply path once the
+// buffers for the widest panel exist.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "h2gpu.h"
+#include "h2gpu_internal.cuh"
+#include "h2gpu_launch.h"
+
+using namespace h2gpu;
+
+#define H2G_API extern "C" __attribute__((visibility("default")))
+
+static thread_local std::string g_err;
+
+static int fail(int code, const char* fmt, ...)
+{
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CK(call)                                                                                       \
+    do {                                                                                               \
+        cudaError_t e_ = (call);                                                                       \
+        if (e_ != cudaSuccess)                                                                         \
+            return fail(e_ == cudaErrorMemoryAllocation ? H2GPU_ERR_NOMEM : H2GPU_ERR_CUDA,            \
+                        "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__);  \
+    } while (0)
+
+#define REQ(cond, ...)                                               \
+    do {                                                             \
+        if (!(cond)) return fail(H2GPU_ERR_INVALID, __VA_ARGS__);    \
+    } while (0)
+
+#define TRY(expr)                        \
+    do {                                 \
+        int s_ = (expr);                 \
+        if (s_ != H2GPU_OK) return s_;   \
+    } while (0)
+
+namespace {
+
+template <typename T>
+int upload(const std::vector<T>& h, T** d, size_t& total)
+{
+    *d = nullptr;
+    if (h.empty()) return H2GPU_OK;
+    CK(cudaMalloc((void**) d, sizeof(T) * h.size()));
+    CK(cudaMemcpy(*d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
+    total += sizeof(T) * h.size();
+    return H2GPU_OK;
+}
+
+struct Ev {
+    cudaEvent_t e[8] = {};
+};
+
+}  // namespace
+
+struct h2gpu_image {
+    std::mutex mu;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int precision = H2GPU_PREC_FP64;
+    int max_nv = 16;
+
+    // dimensions
+    int n_point = 0, kd = 1, xpt_dim = 3, n_node = 0, n_leaf = 0, max_level = 0, min_adm = 0, BD_JIT = 0;
+    int kernel_id = 0, n_kp = 0;
+    double kp[4] = {0, 0, 0, 0};
+    int N = 0;
+    long long y0_rows = 0, ps_rows = 0;
+
+    // plan (host copies kept for launches by level)
+    std::vector<int> up_beg, dn_beg;     // task ranges per level step
+    int n_up = 0, n_dn = 0, n_y1 = 0, n_blkB = 0, n_blkD = 0, n_jtN = 0, n_jtF = 0, n_asm = 0;
+
+    // device plan
+    UpTask* d_up = nullptr;
+    DownTask* d_dn = nullptr;
+    Y1Task* d_y1t = nullptr;
+    int* d_y1_slots = nullptr;
+    BlkTask* d_blkB = nullptr;
+    BlkTask* d_blkD = nullptr;
+    JitTarget* d_jtN = nullptr;
+    JitTarget* d_jtF = nullptr;
+    JitSource* d_js = nullptr;
+    AsmTask* d_asm = nullptr;
+    int* d_asm_slots = nullptr;
+    int* d_fwd = nullptr;
+    int* d_bwd = nullptr;
+
+    // data
+    double* d_U64 = nullptr;
+    float* d_U32 = nullptr;
+    size_t U_elems = 0;
+    double* d_B64 = nullptr;
+    float* d_B32 = nullptr;
+    size_t B_elems = 0;
+    double* d_D64 = nullptr;
+    float* d_D32 = nullptr;
+    size_t D_elems = 0;
+    double4* d_pts64 = nullptr;   // global coordinates (x, y, z, radius)
+    float4* d_pts32 = nullptr;    // coordinates relative to their node's box center
+    size_t n_pts = 0;
+
+    // work buffers sized for panels of width NVb
+    int NVb = 0;
+    double* d_XS = nullptr;
+    double* d_PS = nullptr;
+    double* d_Y1 = nullptr;
+    double* d_PUSH = nullptr;
+    // host-API staging
+    double* d_io = nullptr;
+    size_t io_elems = 0;
+
+    size_t bytes = 0;        // plan + data
+    size_t work_bytes = 0;   // work buffers
+    h2gpu_stats st{};
+    Ev ev;
+};
+
+namespace {
+
+void free_all(h2gpu_image* im)
+{
+    void* ptrs[] = {im->d_up, im->d_dn, im->d_y1t, im->d_y1_slots, im->d_blkB, im->d_blkD, im->d_jtN, im->d_jtF,
+                    im->d_js, im->d_asm, im->d_asm_slots, im->d_fwd, im->d_bwd, im->d_U64, im->d_U32, im->d_B64,
+                    im->d_B32, im->d_D64, im->d_D32, im->d_pts64, im->d_pts32, im->d_XS, im->d_PS, im->d_Y1,
+                    im->d_PUSH, im->d_io};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    for (auto& e : im->ev.e)
+        if (e) cudaEventDestroy(e);
+    if (im->stream) cudaStreamDestroy(im->stream);
+}
+
+int npt_of(const h2gpu_desc* d, int n) { return d->pt_cluster[2 * n + 1] - d->pt_cluster[2 * n] + 1; }
+
+// Structural checks of the descriptor; every index used by a kernel is checked here,
+// so the device code indexes without bounds checks.
+int validate(const h2gpu_desc* d)
+{
+    REQ(d != nullptr, "descriptor is NULL");
+    REQ(d->n_point > 0 && d->n_node > 0 && d->n_leaf_node > 0, "empty representation");
+    REQ(d->pt_dim == 3, "pt_dim %d: only 3-D kernels are supported", d->pt_dim);
+    REQ(d->krnl_dim == 1 || d->krnl_dim == 3, "krnl_dim %d not supported", d->krnl_dim);
+    REQ(d->xpt_dim >= 3 && d->xpt_dim <= 4, "xpt_dim %d not supported", d->xpt_dim);
+    REQ(d->max_child == 8, "max_child must be 8 for 3-D trees");
+    REQ(d->max_level >= 0 && d->min_adm_level >= 0, "bad level data");
+    REQ((long long) d->krnl_dim * d->n_point < (1LL << 30), "problem too large for 32-bit row indices");
+    REQ(d->n_child && d->children && d->node_level && d->pt_cluster && d->mat_cluster && d->level_n_node &&
+            d->level_nodes && d->leaf_nodes && d->U_nrow && d->U_ncol && d->U_ld && d->U && d->fwd_pmt_idx &&
+            d->bwd_pmt_idx,
+        "descriptor is missing a required array");
+    REQ(d->n_r_adm_pair == 0 || d->r_adm_pairs, "r_adm_pairs missing");
+    REQ(d->n_r_inadm_pair == 0 || d->r_inadm_pairs, "r_inadm_pairs missing");
+    REQ(d->n_D == d->n_leaf_node + d->n_r_inadm_pair, "n_D != n_leaf_node + n_r_inadm_pair");
+    const int kd = d->krnl_dim;
+    for (int n = 0; n < d->n_node; n++)
+    {
+        int s = d->pt_cluster[2 * n], e = d->pt_cluster[2 * n + 1];
+        REQ(s >= 0 && e < d->n_point && s <= e, "node %d: bad pt_cluster [%d, %d]", n, s, e);
+        REQ(d->mat_cluster[2 * n] == kd * s && d->mat_cluster[2 * n + 1] == kd * (e + 1) - 1,
+            "node %d: mat_cluster does not match pt_cluster", n);
+        REQ(d->n_child[n] >= 0 && d->n_child[n] <= d->max_child, "node %d: bad n_child", n);
+        for (int k = 0; k < d->n_child[n]; k++)
+        {
+            int c = d->children[n * d->max_child + k];
+            REQ(c >= 0 && c < d->n_node && c != n, "node %d: bad child index", n);
+        }
+        REQ(d->node_level[n] >= 0 && d->node_level[n] <= d->max_level, "node %d: bad level", n);
+        REQ(d->U_nrow[n] >= 0 && d->U_ncol[n] >= 0, "node %d: negative U size", n);
+        if (d->U_nrow[n] > 0 && d->U_ncol[n] > 0)
+            REQ(d->U[n] != nullptr && d->U_ld[n] >= d->U_ncol[n], "node %d: U data missing", n);
+    }
+    for (int l = 0; l <= d->max_level; l++)
+    {
+        REQ(d->level_n_node[l] >= 0 && d->level_n_node[l] <= d->n_leaf_node, "level %d: bad node count", l);
+        for (int j = 0; j < d->level_n_node[l]; j++)
+        {
+            int n = d->level_nodes[(size_t) l * d->n_leaf_node + j];
+            REQ(n >= 0 && n < d->n_node && d->node_level[n] == l, "level %d: bad node list", l);
+        }
+    }
+    for (int i = 0; i < d->n_leaf_node; i++)
+    {
+        int n = d->leaf_nodes[i];
+        REQ(n >= 0 && n < d->n_node && d->n_child[n] == 0, "leaf_nodes[%d] is not a leaf", i);
+    }
+    for (int i = 0; i < d->n_r_adm_pair; i++)
+    {
+        int a = d->r_adm_pairs[2 * i], b = d->r_adm_pairs[2 * i + 1];
+        REQ(a >= 0 && a < d->n_node && b >= 0 && b < d->n_node && a != b, "admissible pair %d out of range", i);
+    }
+    for (int i = 0; i < d->n_r_inadm_pair; i++)
+    {
+        int a = d->r_inadm_pairs[2 * i], b = d->r_inadm_pairs[2 * i + 1];
+        REQ(a >= 0 && a < d->n_node && b >= 0 && b < d->n_node, "inadmissible pair %d out of range", i);
+        REQ(d->n_child[a] == 0 && d->n_child[b] == 0, "inadmissible pair %d is not leaf-leaf", i);
+    }
+    const int N = kd * d->n_point;
+    std::vector<char> seen(N, 0);
+    for (int i = 0; i < N; i++)
+    {
+        int f = d->fwd_pmt_idx[i], b = d->bwd_pmt_idx[i];
+        REQ(f >= 0 && f < N && b >= 0 && b < N, "permutation index out of range");
+        REQ(!seen[f], "fwd_pmt_idx is not a permutation");
+        seen[f] = 1;
+        REQ(d->bwd_pmt_idx[f] == i, "bwd_pmt_idx is not the inverse of fwd_pmt_idx");
+    }
+    if (d->BD_JIT)
+    {
+        REQ(d->kernel_id >= H2GPU_KRNL_COULOMB && d->kernel_id <= H2GPU_KRNL_RPY,
+            "JIT mode needs a kernel id (H2GPU_KRNL_*), got %d", d->kernel_id);
+        REQ((d->kernel_id == H2GPU_KRNL_RPY) == (kd == 3), "kernel id does not match krnl_dim");
+        REQ(d->kernel_id != H2GPU_KRNL_RPY || d->xpt_dim == 4, "RPY needs 4 coordinate rows");
+        REQ(d->kernel_id == H2GPU_KRNL_COULOMB || d->n_krnl_param >= 1, "kernel needs a parameter");
+        REQ(d->coord && d->J_n && d->J_coord, "JIT mode needs coordinates and skeleton points");
+    } else {
+        REQ(d->n_B == d->n_r_adm_pair, "n_B != n_r_adm_pair");
+        REQ(d->n_B == 0 || (d->B_nrow && d->B_ncol && d->B_ptr && d->B_data), "AOT mode needs B blocks");
+        REQ(d->D_nrow && d->D_ncol && d->D_ptr && d->D_data, "AOT mode needs D blocks");
+    }
+    return H2GPU_OK;
+}
+
+// Center of the bounding box of every node's points.
+void node_centers(const h2gpu_desc* d, std::vector<double>& c)
+{
+    c.assign(3 * (size_t) d->n_node, 0.0);
+    for (int n = 0; n < d->n_node; n++)
+    {
+        double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+        for (int p = d->pt_cluster[2 * n]; p <= d->pt_cluster[2 * n + 1]; p++)
+            for (int k = 0; k < 3; k++)
+            {
+                double x = d->coord[(size_t) k * d->n_point + p];
+                lo[k] = std::min(lo[k], x);
+                hi[k] = std::max(hi[k], x);
+            }
+        for (int k = 0; k < 3; k++) c[3 * n + k] = 0.5 * (lo[k] + hi[k]);
+    }
+}
+
+// Everything build_plan produces on the host; uploaded by upload_plan once a device is known.
+struct HostPlan {
+    std::vector<double> U;
+    std::vector<UpTask> up;
+    std::vector<DownTask> dn;
+    std::vector<Y1Task> y1t;
+    std::vector<int> y1_slots;
+    std::vector<BlkTask> blkB, blkD;
+    std::vector<JitTarget> jtN, jtF;
+    std::vector<JitSource> js;
+    std::vector<AsmTask> at;
+    std::vector<int> at_slots;
+    std::vector<int> fw, bw;
+    std::vector<double4> p64;
+    std::vector<float4> p32;
+};
+
+int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
+{
+    const int kd = d->krnl_dim, N = kd * d->n_point, n_node = d->n_node, min_adm = d->min_adm_level;
+    const int* lvl = d->node_level;
+    const int* mc = d->mat_cluster;
+    im->n_point = d->n_point; im->kd = kd; im->xpt_dim = d->xpt_dim; im->n_node = n_node;
+    im->n_leaf = d->n_leaf_node; im->max_level = d->max_level; im->min_adm = min_adm; im->BD_JIT = d->BD_JIT;
+    im->kernel_id = d->kernel_id; im->n_kp = d->n_krnl_param; im->N = N;
+    for (int i = 0; i < 4; i++) im->kp[i] = d->krnl_param[i];
+
+    // ---- parents, and the y0 layout with each node's children contiguous
+    std::vector<int> parent(n_node, -1);
+    for (int n = 0; n < n_node; n++)
+        for (int k = 0; k < d->n_child[n]; k++) parent[d->children[n * d->max_child + k]] = n;
+    std::vector<int> y0r(n_node, -1);
+    long long cur = 0;
+    for (int p = 0; p < n_node; p++)
+        for (int k = 0; k < d->n_child[p]; k++)
+        {
+            int c = d->children[p * d->max_child + k];
+            if (lvl[c] >= min_adm) { y0r[c] = (int) cur; cur += d->U_ncol[c]; }
+        }
+    for (int n = 0; n < n_node; n++)
+        if (parent[n] < 0 && lvl[n] >= min_adm) { y0r[n] = (int) cur; cur += d->U_ncol[n]; }
+    REQ(cur < (1LL << 30), "skeleton space too large");
+    im->y0_rows = cur;
+
+    // ---- U shapes and arena
+    std::vector<long long> u_off(n_node, 0);
+    long long ue = 0;
+    for (int n = 0; n < n_node; n++)
+    {
+        int nr = d->U_nrow[n], nc = d->U_ncol[n];
+        if (nr == 0 || nc == 0 || lvl[n] < min_adm) continue;
+        if (d->n_child[n] == 0)
+            REQ(nr == kd * npt_of(d, n), "leaf %d: U has %d rows, expected %d", n, nr, kd * npt_of(d, n));
+        else
+        {
+            int s = 0;
+            for (int k = 0; k < d->n_child[n]; k++) s += d->U_ncol[d->children[n * d->max_child + k]];
+            REQ(nr == s, "node %d: U has %d rows, children ranks sum to %d", n, nr, s);
+        }
+        u_off[n] = ue;
+        ue += (long long) nr * nc;
+    }
+    std::vector<double>& U = hp.U;
+    U.resize(ue);
+    for (int n = 0; n < n_node; n++)
+    {
+        int nr = d->U_nrow[n], nc = d->U_ncol[n], ld = d->U_ld[n];
+        if (nr == 0 || nc == 0 || lvl[n] < min_adm) continue;
+        for (int r = 0; r < nr; r++) memcpy(&U[u_off[n] + (long long) r * nc], d->U[n] + (size_t) r * ld, 8 * nc);
+    }
+    im->U_elems = ue;
+
+    // ---- upward tasks, levels max_level .. min_adm
+    std::vector<UpTask>& up = hp.up;
+    im->up_beg.clear();
+    for (int L = d->max_level; L >= min_adm; L--)
+    {
+        im->up_beg.push_back((int) up.size());
+        for (int j = 0; j < d->level_n_node[L]; j++)
+        {
+            int n = d->level_nodes[(size_t) L * d->n_leaf_node + j];
+            int nr = d->U_nrow[n], nc = d->U_ncol[n];
+            if (nr == 0 || nc == 0) continue;
+            UpTask t;
+            t.u_off = u_off[n];
+            t.nrow = nr;
+            t.ncol = nc;
+            t.in_row = d->n_child[n] == 0 ? mc[2 * n] : N + y0r[d->children[n * d->max_child]];
+            t.out_row = N + y0r[n];
+            up.push_back(t);
+        }
+    }
+    im->up_beg.push_back((int) up.size());
+    im->n_up = (int) up.size();
+
+    // ---- partial slots
+    long long ps = 0;
+    auto alloc = [&](int rows) { long long r = ps; ps += rows; return (int) r; };
+    std::vector<std::vector<int>> y1s(n_node), asms(n_node);
+    std::vector<char> has_y1(n_node, 0);
+    const int R = 64;
+    std::vector<BlkTask>& blkB = hp.blkB;
+    std::vector<BlkTask>& blkD = hp.blkD;
+    std::vector<JitTarget>& jtN = hp.jtN;
+    std::vector<JitTarget>& jtF = hp.jtF;
+    std::vector<JitSource>& js = hp.js;
+    std::vector<double> ctr;
+
+    if (!d->BD_JIT)
+    {
+        for (int i = 0; i < d->n_B; i++)
+        {
+            int n0 = d->r_adm_pairs[2 * i], n1 = d->r_adm_pairs[2 * i + 1];
+            int l0 = lvl[n0], l1 = lvl[n1];
+            int nr = d->B_nrow[i], nc = d->B_ncol[i];
+            int er = (l0 >= l1) ? d->U_ncol[n0] : kd * npt_of(d, n0);
+            int ec = (l1 >= l0) ? d->U_ncol[n1] : kd * npt_of(d, n1);
+            REQ(nr == er && nc == ec, "B block %d is %dx%d, expected %dx%d", i, nr, nc, er, ec);
+            REQ(l0 < l1 || (l0 >= min_adm && y0r[n0] >= 0), "B block %d: node %d has no skeleton", i, n0);
+            REQ(l1 < l0 || (l1 >= min_adm && y0r[n1] >= 0), "B block %d: node %d has no skeleton", i, n1);
+            if (nr == 0 || nc == 0) continue;
+            int in0 = (l0 > l1) ? mc[2 * n1] : N + y0r[n1];
+            int in1 = (l0 < l1) ? mc[2 * n0] : N + y0r[n0];
+            int s0 = alloc(nr);
+            if (l0 < l1) asms[n0].push_back(s0); else { y1s[n0].push_back(s0); }
+            for (int r0 = 0; r0 < nr; r0 += R)
+            {
+                int rr = std::min(R, nr - r0);
+                int s1 = alloc(nc);
+                if (l0 > l1) asms[n1].push_back(s1); else y1s[n1].push_back(s1);
+                BlkTask t;
+                t.a_off = (long long) d->B_ptr[i] + (long long) r0 * nc;
+                t.nrow = rr; t.ncol = nc; t.in0_row = in0; t.in1_row = in1 + r0;
+                t.out0_row = s0 + r0; t.out1_row = s1;
+                blkB.push_back(t);
+            }
+        }
+        for (int i = 0; i < d->n_D; i++)
+        {
+            int n0, n1;
+            if (i < d->n_leaf_node) n0 = n1 = d->leaf_nodes[i];
+            else { n0 = d->r_inadm_pairs[2 * (i - d->n_leaf_node)]; n1 = d->r_inadm_pairs[2 * (i - d->n_leaf_node) + 1]; }
+            int nr = d->D_nrow[i], nc = d->D_ncol[i];
+            REQ(nr == kd * npt_of(d, n0) && nc == kd * npt_of(d, n1), "D block %d has a wrong shape", i);
+            bool diag = i < d->n_leaf_node;
+            int s0 = alloc(nr);
+            asms[n0].push_back(s0);
+            for (int r0 = 0; r0 < nr; r0 += R)
+            {
+                int rr = std::min(R, nr - r0);
+                int s1 = -1;
+                if (!diag) { s1 = alloc(nc); asms[n1].push_back(s1); }
+                BlkTask t;
+                t.a_off = (long long) d->D_ptr[i] + (long long) r0 * nc;
+                t.nrow = rr; t.ncol = nc; t.in0_row = mc[2 * n1]; t.in1_row = mc[2 * n0] + r0;
+                t.out0_row = s0 + r0; t.out1_row = s1;
+                blkD.push_back(t);
+            }
+        }
+        for (int n = 0; n < n_node; n++) has_y1[n] = !y1s[n].empty();
+    } else {
+        // ---- JIT: point space = sorted points, then the skeleton points of every node
+        node_centers(d, ctr);
+        std::vector<int> jp0(n_node, 0);
+        long long np = d->n_point;
+        for (int n = 0; n < n_node; n++) { jp0[n] = (int) np; np += d->J_n[n]; }
+        REQ(np < (1LL << 31), "too many points");
+        im->n_pts = np;
+        std::vector<int> leaf_of(d->n_point, -1);
+        for (int i = 0; i < d->n_leaf_node; i++)
+        {
+            int n = d->leaf_nodes[i];
+            for (int p = d->pt_cluster[2 * n]; p <= d->pt_cluster[2 * n + 1]; p++) leaf_of[p] = n;
+        }
+        std::vector<double4>& p64 = hp.p64;
+        std::vector<float4>& p32 = hp.p32;
+        p64.resize(np);
+        p32.resize(np);
+        const bool rad = d->xpt_dim >= 4;
+        for (int p = 0; p < d->n_point; p++)
+        {
+            double x = d->coord[p], y = d->coord[(size_t) d->n_point + p], z = d->coord[2 * (size_t) d->n_point + p];
+            double a = rad ? d->coord[3 * (size_t) d->n_point + p] : 0.0;
+            REQ(leaf_of[p] >= 0, "point %d belongs to no leaf", p);
+            const double* c = &ctr[3 * leaf_of[p]];
+            p64[p] = make_double4(x, y, z, a);
+            p32[p] = make_float4((float) (x - c[0]), (float) (y - c[1]), (float) (z - c[2]), (float) a);
+        }
+        for (int n = 0; n < n_node; n++)
+        {
+            int nj = d->J_n[n];
+            if (nj > 0) REQ(d->J_coord[n] != nullptr, "node %d: skeleton coordinates missing", n);
+            const double* c = &ctr[3 * n];
+            for (int j = 0; j < nj; j++)
+            {
+                const double* J = d->J_coord[n];
+                double x = J[j], y = J[nj + j], z = J[2 * nj + j], a = rad ? J[3 * nj + j] : 0.0;
+                p64[jp0[n] + j] = make_double4(x, y, z, a);
+                p32[jp0[n] + j] = make_float4((float) (x - c[0]), (float) (y - c[1]), (float) (z - c[2]), (float) a);
+            }
+        }
+
+        struct Src { int pt0, npt, in_row, node; };
+        auto shift = [&](int tn, int sn, JitSource& s) {
+            s.sx = (float) (ctr[3 * tn] - ctr[3 * sn]);
+            s.sy = (float) (ctr[3 * tn + 1] - ctr[3 * sn + 1]);
+            s.sz = (float) (ctr[3 * tn + 2] - ctr[3 * sn + 2]);
+        };
+        const int TCH = 128;
+        auto emit = [&](std::vector<JitTarget>& out, int tnode, int pt0, int npt, int out_row, int out_y1,
+                        const std::vector<Src>& srcs) {
+            int sb = (int) js.size();
+            for (const Src& s : srcs)
+            {
+                JitSource j;
+                j.pt0 = s.pt0; j.npt = s.npt; j.in_row = s.in_row;
+                shift(tnode, s.node, j);
+                js.push_back(j);
+            }
+            int se = (int) js.size();
+            for (int c0 = 0; c0 < npt; c0 += TCH)
+            {
+                JitTarget t;
+                t.pt0 = pt0 + c0; t.npt = std::min(TCH, npt - c0);
+                t.out_row = out_row + kd * c0; t.out_y1 = out_y1;
+                t.src_beg = sb; t.src_end = se;
+                out.push_back(t);
+            }
+        };
+        // near field: every leaf against itself and its inadmissible partners
+        std::vector<std::vector<Src>> near(n_node), farJ(n_node), farL(n_node);
+        auto pts_src = [&](int n) { return Src{d->pt_cluster[2 * n], npt_of(d, n), mc[2 * n], n}; };
+        auto J_src = [&](int n) { return Src{jp0[n], d->J_n[n], N + y0r[n], n}; };
+        for (int i = 0; i < d->n_leaf_node; i++)
+        {
+            int n = d->leaf_nodes[i];
+            near[n].push_back(pts_src(n));
+        }
+        for (int i = 0; i < d->n_r_inadm_pair; i++)
+        {
+            int a = d->r_inadm_pairs[2 * i], b = d->r_inadm_pairs[2 * i + 1];
+            near[a].push_back(pts_src(b));
+            near[b].push_back(pts_src(a));
+        }
+        for (int i = 0; i < d->n_r_adm_pair; i++)
+        {
+            int a = d->r_adm_pairs[2 * i], b = d->r_adm_pairs[2 * i + 1];
+            int la = lvl[a], lb = lvl[b];
+            if (la >= lb) REQ(y0r[a] >= 0 && d->U_ncol[a] == kd * d->J_n[a], "node %d: skeleton size mismatch", a);
+            if (lb >= la) REQ(y0r[b] >= 0 && d->U_ncol[b] == kd * d->J_n[b], "node %d: skeleton size mismatch", b);
+            if (la == lb) { farJ[a].push_back(J_src(b)); farJ[b].push_back(J_src(a)); }
+            else if (la > lb) { farJ[a].push_back(pts_src(b)); farL[b].push_back(J_src(a)); }
+            else { farL[a].push_back(J_src(b)); farJ[b].push_back(pts_src(a)); }
+        }
+        for (int i = 0; i < d->n_leaf_node; i++)
+        {
+            int n = d->leaf_nodes[i];
+            int s = alloc(kd * npt_of(d, n));
+            asms[n].push_back(s);
+            emit(jtN, n, d->pt_cluster[2 * n], npt_of(d, n), s, 0, near[n]);
+        }
+        for (int n = 0; n < n_node; n++)
+        {
+            if (!farJ[n].empty() && d->J_n[n] > 0)
+            {
+                has_y1[n] = 1;
+                emit(jtF, n, jp0[n], d->J_n[n], y0r[n], 1, farJ[n]);
+            }
+            if (!farL[n].empty())
+            {
+                int s = alloc(kd * npt_of(d, n));
+                asms[n].push_back(s);
+                emit(jtF, n, d->pt_cluster[2 * n], npt_of(d, n), s, 0, farL[n]);
+            }
+        }
+    }
+
+    // ---- y1 sums (AOT)
+    std::vector<Y1Task>& y1t = hp.y1t;
+    std::vector<int>& y1_slots = hp.y1_slots;
+    for (int n = 0; n < n_node; n++)
+    {
+        if (y1s[n].empty()) continue;
+        Y1Task t;
+        t.row = y0r[n]; t.nrow = d->U_ncol[n];
+        t.slot_beg = (int) y1_slots.size();
+        for (int s : y1s[n]) y1_slots.push_back(s);
+        t.slot_end = (int) y1_slots.size();
+        y1t.push_back(t);
+    }
+
+    // ---- downward tasks, levels min_adm .. max_level
+    std::vector<DownTask>& dn = hp.dn;
+    std::vector<char> done(n_node, 0);
+    im->dn_beg.clear();
+    for (int L = min_adm; L <= d->max_level; L++)
+    {
+        im->dn_beg.push_back((int) dn.size());
+        for (int j = 0; j < d->level_n_node[L]; j++)
+        {
+            int n = d->level_nodes[(size_t) L * d->n_leaf_node + j];
+            int nr = d->U_nrow[n], nc = d->U_ncol[n];
+            if (nr == 0 || nc == 0) continue;
+            bool push = parent[n] >= 0 && lvl[parent[n]] >= min_adm && done[parent[n]];
+            if (!has_y1[n] && !push) continue;
+            done[n] = 1;
+            bool leaf = d->n_child[n] == 0;
+            int dst = leaf ? alloc(nr) : y0r[d->children[n * d->max_child]];
+            if (leaf) asms[n].push_back(dst);
+            for (int r0 = 0; r0 < nr; r0 += R)
+            {
+                DownTask t;
+                t.u_off = u_off[n] + (long long) r0 * nc;
+                t.nrow = std::min(R, nr - r0); t.ncol = nc;
+                t.y1_row = has_y1[n] ? y0r[n] : -1;
+                t.push_row = push ? y0r[n] : -1;
+                t.dst_ps = leaf ? 1 : 0;
+                t.dst_row = dst + r0;
+                dn.push_back(t);
+            }
+        }
+    }
+    im->dn_beg.push_back((int) dn.size());
+
+    // ---- assembly, one task per leaf
+    std::vector<AsmTask>& at = hp.at;
+    std::vector<int>& at_slots = hp.at_slots;
+    for (int i = 0; i < d->n_leaf_node; i++)
+    {
+        int n = d->leaf_nodes[i];
+        AsmTask t;
+        t.row0 = mc[2 * n]; t.nrow = kd * npt_of(d, n);
+        t.slot_beg = (int) at_slots.size();
+        for (int s : asms[n]) at_slots.push_back(s);
+        t.slot_end = (int) at_slots.size();
+        at.push_back(t);
+    }
+    REQ(ps < (1LL << 31), "partial space too large");
+    im->ps_rows = ps;
+
+    // ---- statistics of the algorithm (per right-hand side)
+    double ub = 0, bb = 0, db = 0, fwd = 0, mid = 0, bwd = 0, den = 0, pB = 0, pD = 0;
+    for (int n = 0; n < n_node; n++)
+    {
+        double nr = d->U_nrow[n], nc = d->U_ncol[n];
+        if (nr == 0 || nc == 0) continue;
+        ub += nr * nc;
+        fwd += nr * nc + nr + nc;
+    }
+    bwd = fwd;
+    for (int i = 0; i < d->n_r_adm_pair; i++)
+    {
+        int a = d->r_adm_pairs[2 * i], b = d->r_adm_pairs[2 * i + 1];
+        double na = lvl[a] >= lvl[b] ? d->J_n ? d->J_n[a] : d->U_ncol[a] / kd : npt_of(d, a);
+        double nb = lvl[b] >= lvl[a] ? d->J_n ? d->J_n[b] : d->U_ncol[b] / kd : npt_of(d, b);
+        pB += na * nb;
+        if (!d->BD_JIT)
+        {
+            double nr = d->B_nrow[i], nc = d->B_ncol[i];
+            bb += nr * nc;
+            mid += nr * nc + 2 * (nr + nc);
+        }
+    }
+    for (int i = 0; i < d->n_D; i++)
+    {
+        int n0, n1;
+        if (i < d->n_leaf_node) n0 = n1 = d->leaf_nodes[i];
+        else { n0 = d->r_inadm_pairs[2 * (i - d->n_leaf_node)]; n1 = d->r_inadm_pairs[2 * (i - d->n_leaf_node) + 1]; }
+        pD += (double) npt_of(d, n0) * npt_of(d, n1);
+        double nr = kd * npt_of(d, n0), nc = kd * npt_of(d, n1);
+        db += nr * nc;
+        den += nr * nc + (i < d->n_leaf_node ? 1 : 2) * (nr + nc);
+    }
+    im->st.bytes_U = 2.0 * ub;       // element counts here, scaled by the element size at query time
+    im->st.bytes_B = bb;
+    im->st.bytes_D = d->BD_JIT ? 0.0 : db;
+    im->st.ref_mv_bytes = 8.0 * (fwd + mid + bwd + (d->BD_JIT ? 0.0 : den));
+    im->st.jit_pairs_B = pB;
+    im->st.jit_pairs_D = pD;
+    im->st.n_tasks_B = d->BD_JIT ? (long long) jtF.size() : (long long) blkB.size();
+    im->st.n_tasks_D = d->BD_JIT ? (long long) jtN.size() : (long long) blkD.size();
+
+    hp.fw.assign(d->fwd_pmt_idx, d->fwd_pmt_idx + N);
+    hp.bw.assign(d->bwd_pmt_idx, d->bwd_pmt_idx + N);
+    im->n_dn = (int) dn.size(); im->n_y1 = (int) y1t.size(); im->n_blkB = (int) blkB.size();
+    im->n_blkD = (int) blkD.size(); im->n_jtN = (int) jtN.size(); im->n_jtF = (int) jtF.size(); im->n_asm = (int) at.size();
+    if (!d->BD_JIT)
+    {
+        im->B_elems = d->n_B > 0 ? d->B_ptr[d->n_B] : 0;
+        im->D_elems = d->D_ptr[d->n_D];
+    }
+    return H2GPU_OK;
+}
+
+
+int upload_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
+{
+    TRY(upload(hp.U, &im->d_U64, im->bytes));
+    TRY(upload(hp.up, &im->d_up, im->bytes));
+    TRY(upload(hp.dn, &im->d_dn, im->bytes));
+    TRY(upload(hp.y1t, &im->d_y1t, im->bytes));
+    TRY(upload(hp.y1_slots, &im->d_y1_slots, im->bytes));
+    TRY(upload(hp.blkB, &im->d_blkB, im->bytes));
+    TRY(upload(hp.blkD, &im->d_blkD, im->bytes));
+    TRY(upload(hp.jtN, &im->d_jtN, im->bytes));
+    TRY(upload(hp.jtF, &im->d_jtF, im->bytes));
+    TRY(upload(hp.js, &im->d_js, im->bytes));
+    TRY(upload(hp.at, &im->d_asm, im->bytes));
+    TRY(upload(hp.at_slots, &im->d_asm_slots, im->bytes));
+    TRY(upload(hp.fw, &im->d_fwd, im->bytes));
+    TRY(upload(hp.bw, &im->d_bwd, im->bytes));
+    TRY(upload(hp.p64, &im->d_pts64, im->bytes));
+    TRY(upload(hp.p32, &im->d_pts32, im->bytes));
+    if (!d->BD_JIT)
+    {
+        if (im->B_elems)
+        {
+            CK(cudaMalloc(&im->d_B64, 8 * im->B_elems));
+            CK(cudaMemcpy(im->d_B64, d->B_data, 8 * im->B_elems, cudaMemcpyHostToDevice));
+            im->bytes += 8 * im->B_elems;
+        }
+        CK(cudaMalloc(&im->d_D64, 8 * im->D_elems));
+        CK(cudaMemcpy(im->d_D64, d->D_data, 8 * im->D_elems, cudaMemcpyHostToDevice));
+        im->bytes += 8 * im->D_elems;
+    }
+    return H2GPU_OK;
+}
+
+__global__ void k_to_f32(const double* __restrict__ a, float* __restrict__ b, size_t n)
+{
+    for (size_t i = blockIdx.x * (size_t) blockDim.x + threadIdx.x; i < n; i += (size_t) gridDim.x * blockDim.x)
+        b[i] = (float) a[i];
+}
+
+int make_f32(h2gpu_image* im, const double* src, float** dst, size_t n)
+{
+    if (n == 0 || *dst) return H2GPU_OK;
+    CK(cudaMalloc(dst, 4 * n));
+    k_to_f32<<<148 * 8, 256, 0, im->stream>>>(src, *dst, n);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(im->stream));
+    im->bytes += 4 * n;
+    return H2GPU_OK;
+}
+
+int ensure_work(h2gpu_image* im, int NV)
+{
+    if (im->NVb >= NV) return H2GPU_OK;
+    for (double** p : {&im->d_XS, &im->d_PS, &im->d_Y1, &im->d_PUSH})
+        if (*p) { cudaFree(*p); *p = nullptr; }
+    size_t xs = ((size_t) im->N + im->y0_rows) * NV, ps = (size_t) im->ps_rows * NV, y1 = (size_t) im->y0_rows * NV;
+    CK(cudaMalloc(&im->d_XS, 8 * std::max<size_t>(xs, 1)));
+    CK(cudaMalloc(&im->d_PS, 8 * std::max<size_t>(ps, 1)));
+    CK(cudaMalloc(&im->d_Y1, 8 * std::max<size_t>(y1, 1)));
+    CK(cudaMalloc(&im->d_PUSH, 8 * std::max<size_t>(y1, 1)));
+    im->work_bytes = 8 * (xs + ps + 2 * y1);
+    im->NVb = NV;
+    return H2GPU_OK;
+}
+
+int panel_width(int n_vec, int max_nv)
+{
+    int w = 1;
+    while (w < n_vec && w < max_nv && w < 16) w <<= 1;
+    return w;
+}
+
+KParam kparam_of(const h2gpu_image* im)
+{
+    KParam k{0.0, 0.0};
+    switch (im->kernel_id)
+    {
+        case H2GPU_KRNL_COULOMB: k.p0 = im->n_kp > 0 ? im->kp[0] : 0.0; break;
+        case H2GPU_KRNL_GAUSSIAN: k.p0 = im->kp[0]; break;
+        case H2GPU_KRNL_MATERN32: k.p0 = im->kp[0]; k.c0 = -1.7320508075688772 * im->kp[0]; break;
+        case H2GPU_KRNL_RPY: k.p0 = im->kp[0]; k.c0 = 1.0 / (6.0 * M_PI * im->kp[0]); break;
+    }
+    return k;
+}
+
+// One panel of NV right-hand sides: X (original order, strides x_rs, x_cs) -> Y.
+int run_panel(h2gpu_image* im, int NV, int nv, const double* X, long long x_rs, long long x_cs, double* Y,
+              long long y_rs, long long y_cs, cudaStream_t s, bool timed)
+{
+    const bool f32 = im->precision == H2GPU_PREC_MIXED;
+    cudaEvent_t* e = im->ev.e;
+    if (timed) CK(cudaEventRecord(e[0], s));
+    CK(launch_gather(NV, X, x_rs, x_cs, nv, im->d_fwd, im->N, im->d_XS, s));
+    // D phase first: it needs only x (in the graph-free stream order it simply runs before the upward sweep)
+    if (timed) CK(cudaEventRecord(e[1], s));
+    if (!im->BD_JIT)
+    {
+        if (f32) CK(launch_blk<float>(NV, im->d_blkD, im->n_blkD, im->d_D32, im->d_XS, im->d_PS, s));
+        else CK(launch_blk<double>(NV, im->d_blkD, im->n_blkD, im->d_D64, im->d_XS, im->d_PS, s));
+    } else {
+        CK(launch_jit(im->kernel_id, f32, NV, im->d_jtN, im->n_jtN, im->d_js, f32 ? (const void*) im->d_pts32 : (const void*) im->d_pts64,
+                      kparam_of(im), f32 ? 1 : 0, im->d_XS, im->d_PS, im->d_Y1, s));
+    }
+    if (timed) CK(cudaEventRecord(e[2], s));
+    for (size_t L = 0; L + 1 < im->up_beg.size(); L++)
+    {
+        int b = im->up_beg[L], n = im->up_beg[L + 1] - b;
+        if (f32) CK(launch_up<float>(NV, im->d_up + b, n, im->d_U32, im->d_XS, s));
+        else CK(launch_up<double>(NV, im->d_up + b, n, im->d_U64, im->d_XS, s));
+    }
+    if (timed) CK(cudaEventRecord(e[3], s));
+    if (!im->BD_JIT)
+    {
+        if (f32) CK(launch_blk<float>(NV, im->d_blkB, im->n_blkB, im->d_B32, im->d_XS, im->d_PS, s));
+        else CK(launch_blk<double>(NV, im->d_blkB, im->n_blkB, im->d_B64, im->d_XS, im->d_PS, s));
+        CK(launch_y1sum(NV, im->d_y1t, im->n_y1, im->d_y1_slots, im->d_PS, im->d_Y1, s));
+    } else {
+        CK(launch_jit(im->kernel_id, f32, NV, im->d_jtF, im->n_jtF, im->d_js, f32 ? (const void*) im->d_pts32 : (const void*) im->d_pts64,
+                      kparam_of(im), f32 ? 1 : 0, im->d_XS, im->d_PS, im->d_Y1, s));
+    }
+    if (timed) CK(cudaEventRecord(e[4], s));
+    for (size_t L = 0; L + 1 < im->dn_beg.size(); L++)
+    {
+        int b = im->dn_beg[L], n = im->dn_beg[L + 1] - b;
+        if (f32) CK(launch_down<float>(NV, im->d_dn + b, n, im->d_U32, im->d_Y1, im->d_PS, im->d_PUSH, s));
+        else CK(launch_down<double>(NV, im->d_dn + b, n, im->d_U64, im->d_Y1, im->d_PS, im->d_PUSH, s));
+    }
+    if (timed) CK(cudaEventRecord(e[5], s));
+    CK(launch_asm(NV, im->d_asm, im->n_asm, im->d_asm_slots, im->d_PS, im->d_fwd, Y, y_rs, y_cs, nv, s));
+    if (timed) CK(cudaEventRecord(e[6], s));
+    im->st.n_launches += 4 + (long long) (im->up_beg.size() - 1) + (long long) (im->dn_beg.size() - 1)
+                         + (im->BD_JIT ? 0 : 1);
+    return H2GPU_OK;
+}
+
+int prepare(h2gpu_image* im, int NV)
+{
+    CK(cudaSetDevice(im->device));
+    if (im->precision == H2GPU_PREC_MIXED)
+    {
+        TRY(make_f32(im, im->d_U64, &im->d_U32, im->U_elems));
+        TRY(make_f32(im, im->d_B64, &im->d_B32, im->B_elems));
+        TRY(make_f32(im, im->d_D64, &im->d_D32, im->D_elems));
+    }
+    return ensure_work(im, NV);
+}
+
+// Apply to n_vec columns of a device matrix (strides in elements), panel by panel.
+int apply_device(h2gpu_image* im, int n_vec, const double* X, long long x_rs, long long x_cs, double* Y,
+                 long long y_rs, long long y_cs, cudaStream_t s)
+{
+    int NV = panel_width(n_vec, im->max_nv);
+    TRY(prepare(im, NV));
+    float ph[5] = {0, 0, 0, 0, 0};
+    for (int c0 = 0; c0 < n_vec; c0 += NV)
+    {
+        int nv = std::min(NV, n_vec - c0);
+        TRY(run_panel(im, NV, nv, X + c0 * x_cs, x_rs, x_cs, Y + c0 * y_cs, y_rs, y_cs, s, true));
+        CK(cudaEventSynchronize(im->ev.e[6]));
+        float t[6];
+        for (int k = 0; k < 6; k++) CK(cudaEventElapsedTime(&t[k], im->ev.e[k], im->ev.e[k + 1]));
+        ph[0] += t[0] + t[2];   // gather + upward
+        ph[1] += t[3];          // B
+        ph[2] += t[4];          // downward
+        ph[3] += t[1];          // D
+        ph[4] += t[5];          // assemble
+    }
+    for (int k = 0; k < 5; k++) { im->st.ms_phase[k] += ph[k]; im->st.ms_total += ph[k]; }
+    im->st.n_matvec += n_vec;
+    return H2GPU_OK;
+}
+
+int ensure_io(h2gpu_image* im, size_t elems)
+{
+    if (im->io_elems >= elems) return H2GPU_OK;
+    if (im->d_io) cudaFree(im->d_io);
+    im->d_io = nullptr;
+    im->io_elems = 0;
+    CK(cudaMalloc(&im->d_io, 8 * elems));
+    im->io_elems = elems;
+    return H2GPU_OK;
+}
+
+}  // namespace
+
+// ===================================================================== C ABI
+
+H2G_API int h2gpu_abi_version(void) { return H2GPU_ABI_VERSION; }
+
+H2G_API const char* h2gpu_last_error(void) { return g_err.c_str(); }
+
+H2G_API void h2gpu_default_options(h2gpu_options* opt)
+{
+    if (!opt) return;
+    opt->precision = H2GPU_PREC_FP64;
+    opt->max_n_vec = 16;
+    opt->device = -1;
+}
+
+H2G_API int h2gpu_image_create(const h2gpu_desc* desc, const h2gpu_options* opt, h2gpu_image** out)
+{
+    if (!out) return fail(H2GPU_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    TRY(validate(desc));
+    h2gpu_options o;
+    h2gpu_default_options(&o);
+    if (opt) o = *opt;
+    REQ(o.precision == H2GPU_PREC_FP64 || o.precision == H2GPU_PREC_MIXED, "unknown precision %d", o.precision);
+    h2gpu_image* im = new h2gpu_image();
+    HostPlan hp;
+    int pst = build_plan(im, desc, hp);   // all structural checks happen here, before any CUDA call
+    if (pst != H2GPU_OK) { delete im; return pst; }
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0)
+    {
+        delete im;
+        return fail(H2GPU_ERR_CUDA, "no CUDA device available (%s); the H2 apply path has no CPU fallback",
+                    cudaGetErrorString(e));
+    }
+    im->precision = o.precision;
+    im->max_nv = (o.max_n_vec >= 1 && o.max_n_vec <= 16) ? o.max_n_vec : 16;
+    if (o.device >= 0) im->device = o.device;
+    else cudaGetDevice(&im->device);
+    int st = H2GPU_OK;
+    do {
+        if (cudaSetDevice(im->device) != cudaSuccess) { st = fail(H2GPU_ERR_CUDA, "cudaSetDevice(%d) failed", im->device); break; }
+        if (cudaStreamCreateWithFlags(&im->stream, cudaStreamNonBlocking) != cudaSuccess) { st = fail(H2GPU_ERR_CUDA, "stream creation failed"); break; }
+        for (auto& ev : im->ev.e)
+            if (cudaEventCreate(&ev) != cudaSuccess) { st = fail(H2GPU_ERR_CUDA, "event creation failed"); break; }
+        if (st != H2GPU_OK) break;
+        st = upload_plan(im, desc, hp);
+    } while (0);
+    if (st != H2GPU_OK)
+    {
+        free_all(im);
+        delete im;
+        return st;
+    }
+    *out = im;
+    return H2GPU_OK;
+}
+
+H2G_API int h2gpu_image_destroy(h2gpu_image* im)
+{
+    if (!im) return H2GPU_OK;
+    {
+        std::lock_guard<std::mutex> lk(im->mu);
+        cudaSetDevice(im->device);
+        if (im->stream) cudaStreamSynchronize(im->stream);
+        free_all(im);
+    }
+    delete im;
+    return H2GPU_OK;
+}
+
+H2G_API int h2gpu_set_precision(h2gpu_image* im, int precision)
+{
+    if (!im) return fail(H2GPU_ERR_INVALID, "image is NULL");
+    REQ(precision == H2GPU_PREC_FP64 || precision == H2GPU_PREC_MIXED, "unknown precision %d", precision);
+    std::lock_guard<std::mutex> lk(im->mu);
+    im->precision = precision;
+    return H2GPU_OK;
+}
+
+H2G_API int h2gpu_matmul_device(h2gpu_image* im, int n_vec, const double* dX, int ldx, double* dY, int ldy,
+                                void* stream)
+{
+    if (!im) return fail(H2GPU_ERR_INVALID, "image is NULL");
+    REQ(n_vec >= 1 && ldx >= n_vec && ldy >= n_vec && dX && dY, "bad matmul_device arguments");
+    std::lock_guard<std::mutex> lk(im->mu);
+    cudaStream_t s = stream ? (cudaStream_t) stream : im->stream;
+    TRY(apply_device(im, n_vec, dX, ldx, 1, dY, ldy, 1, s));
+    return H2GPU_OK;
+}
+
+H2G_API int h2gpu_matmul(h2gpu_image* im, int layout, int n_vec, const double* X, int ldx, double* Y, int ldy)
+{
+    if (!im) return fail(H2GPU_ERR_INVALID, "image is NULL");
+    REQ(X && Y && n_vec >= 1, "bad matmul arguments");
+    REQ(layout == H2GPU_ROW_MAJOR || layout == H2GPU_COL_MAJOR, "bad layout %d", layout);
+    const long long N = 0;
+    (void) N;
+    std::lock_guard<std::mutex> lk(im->mu);
+    const size_t n = (size_t) im->N;
+    if (layout == H2GPU_ROW_MAJOR) REQ(ldx >= n_vec && ldy >= n_vec, "row-major leading dimension < n_vec");
+    else REQ((size_t) ldx >= n && (size_t) ldy >= n, "column-major leading dimension < krnl_mat_size");
+    CK(cudaSetDevice(im->device));
+    TRY(ensure_io(im, 2 * n * n_vec));
+    double* dX = im->d_io;
+    double* dY = im->d_io + n * n_vec;
+    cudaStream_t s = im->stream;
+    if (layout == H2GPU_ROW_MAJOR)
+    {
+        CK(cudaMemcpy2DAsync(dX, 8 * (size_t) n_vec, X, 8 * (size_t) ldx, 8 * (size_t) n_vec, n, cudaMemcpyHostToDevice, s));
+        TRY(apply_device(im, n_vec, dX, n_vec, 1, dY, n_vec, 1, s));
+        CK(cudaMemcpy2DAsync(Y, 8 * (size_t) ldy, dY, 8 * (size_t) n_vec, 8 * (size_t) n_vec, n, cudaMemcpyDeviceToHost, s));
+    } else {
+        CK(cudaMemcpy2DAsync(dX, 8 * n, X, 8 * (size_t) ldx, 8 * n, n_vec, cudaMemcpyHostToDevice, s));
+        TRY(apply_device(im, n_vec, dX, 1, (long long) n, dY, 1, (long long) n, s));
+        CK(cudaMemcpy2DAsync(Y, 8 * (size_t) ldy, dY, 8 * n, 8 * n, n_vec, cudaMemcpyDeviceToHost, s));
+    }
+    CK(cudaStreamSynchronize(s));
+    return H2GPU_OK;
+}
+
+H2G_API int h2gpu_matvec(h2gpu_image* im, const double* x, double* y)
+{
+    if (!im) return fail(H2GPU_ERR_INVALID, "image is NULL");
+    return h2gpu_matmul(im, H2GPU_COL_MAJOR, 1, x, im->N, y, im->N);
+}
+
+namespace h2gpu {
+cudaError_t launch_permute(const double* X, long long x_rs, long long x_cs, const int* idx, int n, int nv, double* Y,
+                           long long y_rs, long long y_cs, cudaStream_t st);
+}
+
+H2G_API int h2gpu_permute_matrix_rows(h2gpu_image* im, int forward, int layout, int n_vec, const double* X, int ldx,
+                                      double* PX, int ldp)
+{
+    if (!im) return fail(H2GPU_ERR_INVALID, "image is NULL");
+    REQ(X && PX && n_vec >= 1, "bad permute arguments");
+    REQ(layout == H2GPU_ROW_MAJOR || layout == H2GPU_COL_MAJOR, "bad layout %d", layout);
+    std::lock_guard<std::mutex> lk(im->mu);
+    const size_t n = (size_t) im->N;
+    if (layout == H2GPU_ROW_MAJOR) REQ(ldx >= n_vec && ldp >= n_vec, "row-major leading dimension < n_vec");
+    else REQ((size_t) ldx >= n && (size_t) ldp >= n, "column-major leading dimension < krnl_mat_size");
+    CK(cudaSetDevice(im->device));
+    TRY(ensure_io(im, 2 * n * n_vec));
+    double* dX = im->d_io;
+    double* dY = im->d_io + n * n_vec;
+    cudaStream_t s = im->stream;
+    const int* idx = forward ? im->d_fwd : im->d_bwd;
+    if (layout == H2GPU_ROW_MAJOR)
+    {
+        CK(cudaMemcpy2DAsync(dX, 8 * (size_t) n_vec, X, 8 * (size_t) ldx, 8 * (size_t) n_vec, n, cudaMemcpyHostToDevice, s));
+        CK(launch_permute(dX, n_vec, 1, idx, (int) n, n_vec, dY, n_vec, 1, s));
+        CK(cudaMemcpy2DAsync(PX, 8 * (size_t) ldp, dY, 8 * (size_t) n_vec, 8 * (size_t) n_vec, n, cudaMemcpyDeviceToHost, s));
+    } else {
+        CK(cudaMemcpy2DAsync(dX, 8 * n, X, 8 * (size_t) ldx, 8 * n, n_vec, cudaMemcpyHostToDevice, s));
+        CK(launch_permute(dX, 1, (long long) n, idx, (int) n, n_vec, dY, 1, (long long) n, s));
+        CK(cudaMemcpy2DAsync(PX, 8 * (size_t) ldp, dY, 8 * n, 8 * n, n_vec, cudaMemcpyDeviceToHost, s));
+    }
+    CK(cudaStreamSynchronize(s));
+    return H2GPU_OK;
+}
+
+H2G_API int h2gpu_permute_vector(h2gpu_image* im, int forward, const double* x, double* px)
+{
+    if (!im) return fail(H2GPU_ERR_INVALID, "image is NULL");
+    return h2gpu_permute_matrix_rows(im, forward, H2GPU_COL_MAJOR, 1, x, im->N, px, im->N);
+}
+
+H2G_API int h2gpu_get_stats(h2gpu_image* im, h2gpu_stats* st)
+{
+    if (!im || !st) return fail(H2GPU_ERR_INVALID, "NULL argument");
+    std::lock_guard<std::mutex> lk(im->mu);
+    *st = im->st;
+    const double es = im->precision == H2GPU_PREC_MIXED ? 4.0 : 8.0;
+    st->bytes_U = im->st.bytes_U * es;
+    st->bytes_B = im->st.bytes_B * es;
+    st->bytes_D = im->st.bytes_D * es;
+    st->device_bytes = (long long) (im->bytes + im->work_bytes + 8 * im->io_elems);
+    return H2GPU_OK;
+}
+
+H2G_API int h2gpu_reset_stats(h2gpu_image* im)
+{
+    if (!im) return fail(H2GPU_ERR_INVALID, "image is NULL");
+    std::lock_guard<std::mutex> lk(im->mu);
+    im->st.n_matvec = 0;
+    im->st.ms_total = 0;
+    for (double& m : im->st.ms_phase) m = 0;
+    return H2GPU_OK;
+}
+
+H2G_API size_t h2gpu_image_bytes(const h2gpu_image* im)
+{
+    return im ? im->bytes + im->work_bytes + 8 * im->io_elems : 0;
+}
+
+H2G_API int h2gpu_direct_sum(int kernel_id, const double* krnl_param, int n_krnl_param, int xpt_dim, int krnl_dim,
+                             const double* src_coord, int n_src, const double* src_val, const double* trg_coord,
+                             int n_trg, double* trg_val)
+{
+    REQ(kernel_id >= H2GPU_KRNL_COULOMB && kernel_id <= H2GPU_KRNL_RPY, "bad kernel id %d", kernel_id);
+    REQ((kernel_id == H2GPU_KRNL_RPY) == (krnl_dim == 3), "kernel id does not match krnl_dim");
+    REQ(xpt_dim >= 3 && xpt_dim <= 4 && (kernel_id != H2GPU_KRNL_RPY || xpt_dim == 4), "bad xpt_dim");
+    REQ(n_src > 0 && n_trg > 0 && src_coord && src_val && trg_coord && trg_val, "bad direct-sum arguments");
+    REQ(kernel_id == H2GPU_KRNL_COULOMB || (krnl_param && n_krnl_param >= 1), "kernel needs a parameter");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(H2GPU_ERR_CUDA, "no CUDA device available for the direct sum");
+    h2gpu_image tmp;
+    tmp.kernel_id = kernel_id;
+    tmp.n_kp = n_krnl_param;
+    for (int i = 0; i < n_krnl_param && i < 4; i++) tmp.kp[i] = krnl_param[i];
+    KParam kp = kparam_of(&tmp);
+    auto pack = [&](const double* c, int n) {
+        std::vector<double4> p(n);
+        for (int i = 0; i < n; i++)
+            p[i] = make_double4(c[i], c[(size_t) n + i], c[2 * (size_t) n + i], xpt_dim >= 4 ? c[3 * (size_t) n + i] : 0.0);
+        return p;
+    };
+    std::vector<double4> hs = pack(src_coord, n_src), ht = pack(trg_coord, n_trg);
+    double4 *ds = nullptr, *dt = nullptr;
+    double *dv = nullptr, *dout = nullptr;
+    int st = H2GPU_OK;
+    do {
+        if (cudaMalloc(&ds, sizeof(double4) * n_src) != cudaSuccess || cudaMalloc(&dt, sizeof(double4) * n_trg) != cudaSuccess ||
+            cudaMalloc(&dv, 8 * (size_t) n_src * krnl_dim) != cudaSuccess ||
+            cudaMalloc(&dout, 8 * (size_t) n_trg * krnl_dim) != cudaSuccess)
+        { st = fail(H2GPU_ERR_NOMEM, "direct sum: device allocation failed"); break; }
+        cudaMemcpy(ds, hs.data(), sizeof(double4) * n_src, cudaMemcpyHostToDevice);
+        cudaMemcpy(dt, ht.data(), sizeof(double4) * n_trg, cudaMemcpyHostToDevice);
+        cudaMemcpy(dv, src_val, 8 * (size_t) n_src * krnl_dim, cudaMemcpyHostToDevice);
+        cudaError_t e = launch_direct(kernel_id, dt, n_trg, ds, n_src, dv, kp, dout, 0);
+        if (e == cudaSuccess) e = cudaMemcpy(trg_val, dout, 8 * (size_t) n_trg * krnl_dim, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) st = fail(H2GPU_ERR_CUDA, "direct sum: %s", cudaGetErrorString(e));
+    } while (0);
+    cudaFree(ds); cudaFree(dt); cudaFree(dv); cudaFree(dout);
+    return st;
+}

@@ -1,0 +1,86 @@
+// h2gpu_internal.cuh -- device-side data layout and task records of the H2 apply engine.
+//
+// Vector spaces.  Every vector space is a matrix of `rows` x NV (row-major, the
+// right-hand sides of one row contiguous, NV = panel width):
+//   XS   input space:   rows [0, N)        the forward-permuted input (N = krnl_mat_size)
+//                       rows [N, N+Y0)     y0 = U^T x of every node, laid out so that the
+//                                          children of a node are contiguous in child order
+//                                          (the upward input of a non-leaf node is then one slice)
+//   PS   partial space: disjoint slots written by the block tasks; every output row is
+//                       the sum of its slots in a fixed order (deterministic, no atomics)
+//   PUSH downward push: rows indexed like the y0 region; a non-leaf node writes
+//                       U_node * y1_node there and each child reads its own slice
+// This replaces the reference's per-thread y copies and y1 rows (src/H2Pack_matvec.c:234-300,
+// :1191-1263) and the H2P_dense_mat y0/y1 arrays (src/H2Pack_typedef.h:171-172).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace h2gpu {
+
+// Upward task: XS[out_row + c][v] = sum_r U[r][c] * XS[in_row + r][v]
+// (H2P_matvec_fwd_transform, src/H2Pack_matvec.c:126-156)
+struct UpTask {
+    long long u_off;   // element offset of U in the U arena (row-major, ld = ncol)
+    int nrow, ncol;
+    int in_row;        // leaf: first row of its x slice; non-leaf: y0 row of its first child
+    int out_row;       // y0 row of the node
+};
+
+// Downward task (a chunk of <= 64 rows of U):  t = U[rows] * y1t,
+//   y1t[c][v] = Y1[y1_row + c][v] + PUSH[push_row + c][v]   (absent terms are zero)
+// (H2P_matvec_bwd_transform, src/H2Pack_matvec.c:806-841)
+struct DownTask {
+    long long u_off;          // element offset of the chunk's first row of U
+    int nrow, ncol;
+    int y1_row;               // -1: the node has no admissible-pair contributions
+    int push_row;             // -1: no push-down from the parent
+    int dst_ps;               // 1: destination is a PS slot (leaf), 0: PUSH rows (children)
+    int dst_row;
+};
+
+// Sum of a node's y1 slots into Y1 (rows indexed like the y0 region)
+struct Y1Task {
+    int row, nrow;
+    int slot_beg, slot_end;
+};
+
+// Stored block (AOT) chunk: PS[out0_row + r] = A[r, :] * XS[in0_row : +ncol]  (r < nrow)
+//                           PS[out1_row + c] = A[:, c]^T * XS[in1_row : +nrow]
+// One read of the block feeds both products, as CBLAS_BI_GEMV does
+// (src/H2Pack_matvec.c:26-65, used at :333-379 and :929-932).
+struct BlkTask {
+    long long a_off;   // element offset of the chunk's first row in the block arena
+    int nrow, ncol;    // rows in this chunk, columns (= leading dimension)
+    int in0_row, in1_row;
+    int out0_row, out1_row;   // -1: product not needed
+};
+
+// JIT target: a set of points whose outputs accumulate over a list of source sets
+// (owner computes; each (target, source) kernel block is evaluated by its owner).
+struct JitTarget {
+    int pt0, npt;      // point-space range of this chunk of targets
+    int out_row;       // row of the chunk's first output row (PS, or Y1 when out_y1)
+    int out_y1;        // 1: outputs are the node's y1 rows
+    int src_beg, src_end;
+};
+
+struct JitSource {
+    int pt0, npt;      // point-space range of the source set
+    int in_row;        // XS row of the input of the first source point
+    float sx, sy, sz;  // center(target set) - center(source set), for re-centred FP32 evaluation
+};
+
+// Final assembly of a leaf: Y[fwd[row0 + r]][v] = sum_s PS[slot_s + r][v]
+struct AsmTask {
+    int row0, nrow;
+    int slot_beg, slot_end;
+};
+
+// Kernel parameters as the device sees them
+struct KParam {
+    double p0;         // Coulomb: value on r == 0; Gaussian: l; Matern: l; RPY: eta
+    double c0;         // derived constant (Matern: -sqrt(3) l; RPY: 1 / (6 pi eta))
+};
+
+}  // namespace h2gpu

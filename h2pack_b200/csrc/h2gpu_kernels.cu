@@ -1,0 +1,678 @@
+// h2gpu_kernels.cu -- sm_100a kernels of the H2 apply engine.
+//
+// Phases (reference: H2P_matvec, src/H2Pack_matvec.c:1162-1284; H2P_matmul,
+// src/H2Pack_matmul.c:455-583):
+//   k_gather      forward permutation of the input panel into XS          (matvec.c:1174-1179)
+//   k_up          upward sweep y0 = U^T x, one CTA per node                 (matvec.c:95-177)
+//   k_blk         stored B / D block chunks, one read feeds A*v and A^T*w  (matvec.c:303-437, 864-998)
+//   k_jit         on-the-fly B / D kernel blocks, owner computes           (matvec.c:586-764, 1002-1145)
+//   k_down        downward sweep U * y1 with slot sums and push-down       (matvec.c:767-861)
+//   k_asm         sum of a leaf's partial slots + backward permutation     (matvec.c:1251-1278)
+//   k_direct      FP64 direct sum (examples/direct_nbody.h:2-54)
+// All right-hand-side panels are NV wide (NV in {1,2,4,8,16}); vector spaces are
+// row-major with row stride NV.  Sums inside one block use the block's warps; sums
+// across blocks go through PS slots in a fixed order, so results are bitwise
+// reproducible run to run.
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include "h2gpu_internal.cuh"
+#include "h2gpu_launch.h"
+
+namespace h2gpu {
+
+constexpr int kWarps = 8;               // warps per CTA of the sweep / block kernels
+constexpr int kThreads = kWarps * 32;
+constexpr unsigned kFull = 0xffffffffu;
+
+template <int NV> struct SV { static constexpr int v = (NV > 1) ? NV + 1 : 1; };  // padded smem row stride
+
+__device__ __forceinline__ double to_d(double x) { return x; }
+__device__ __forceinline__ double to_d(float x) { return (double) x; }
+
+// Reduce NV per-lane values over the 32 lanes of a warp.  After the call a[0] of
+// lane l holds the warp sum for right-hand side v = nv_of_lane(l); the lanes with
+// (lane & (32/NV - 1)) == 0 hold distinct v.  Uses NV-1 + log2(32/NV) shuffles.
+template <int NV>
+__device__ __forceinline__ void warp_transpose_reduce(double (&a)[NV], int lane)
+{
+    int m = NV;
+    int o = 16;
+#pragma unroll
+    for (int s = 0; (1 << s) < NV; s++)
+    {
+        const int half = m >> 1;
+        const bool up = (lane & o) != 0;
+#pragma unroll
+        for (int i = 0; i < NV / 2; i++)
+        {
+            if (i < half)
+            {
+                double send = up ? a[i] : a[i + half];
+                double keep = up ? a[i + half] : a[i];
+                double recv = __shfl_xor_sync(kFull, send, o);
+                a[i] = keep + recv;
+            }
+        }
+        m = half;
+        o >>= 1;
+    }
+#pragma unroll
+    for (; o >= 1; o >>= 1) a[0] += __shfl_xor_sync(kFull, a[0], o);
+}
+
+template <int NV>
+__device__ __forceinline__ int nv_of_lane(int lane)
+{
+    // bits of v from MSB: lane bit 16 -> v bit log2(NV)-1, lane bit 8 -> next, ...
+    int v = 0, o = 16;
+#pragma unroll
+    for (int s = 0; (1 << s) < NV; s++) { v = (v << 1) | ((lane & o) ? 1 : 0); o >>= 1; }
+    return v;
+}
+
+template <int NV>
+__device__ __forceinline__ bool lane_writes(int lane) { return (lane & (32 / NV - 1)) == 0; }
+
+// ------------------------------------------------------------------ gather
+
+// XS[r][v] = X[fwd[r]][v] (v < nv), zero-padded to NV columns.
+template <int NV>
+__global__ void k_gather(const double* __restrict__ X, long long x_rs, long long x_cs, int nv,
+                         const int* __restrict__ fwd, int N, double* __restrict__ XS)
+{
+    long long total = (long long) N * NV;
+    for (long long i = blockIdx.x * (long long) blockDim.x + threadIdx.x; i < total;
+         i += (long long) gridDim.x * blockDim.x)
+    {
+        int r = (int) (i / NV), v = (int) (i % NV);
+        XS[i] = (v < nv) ? X[(long long) fwd[r] * x_rs + (long long) v * x_cs] : 0.0;
+    }
+}
+
+// Y[i][v] = X[idx[i]][v] for general strides (H2P_permute_* on device)
+__global__ void k_permute(const double* __restrict__ X, long long x_rs, long long x_cs, const int* __restrict__ idx,
+                          int n, int nv, double* __restrict__ Y, long long y_rs, long long y_cs)
+{
+    long long total = (long long) n * nv;
+    for (long long i = blockIdx.x * (long long) blockDim.x + threadIdx.x; i < total;
+         i += (long long) gridDim.x * blockDim.x)
+    {
+        int r = (int) (i / nv), v = (int) (i % nv);
+        Y[(long long) r * y_rs + (long long) v * y_cs] = X[(long long) idx[r] * x_rs + (long long) v * x_cs];
+    }
+}
+
+// ---------------------------------------------------------------- upward
+
+// y0 = U^T w for one node per CTA.  Lanes own columns, warps split the rows,
+// the warps' column partials are summed in shared memory.
+template <typename TA, int NV>
+__global__ void __launch_bounds__(kThreads) k_up(const UpTask* __restrict__ tasks, const TA* __restrict__ Uar,
+                                                 double* __restrict__ XS)
+{
+    constexpr int S = SV<NV>::v;
+    constexpr int RT = 64;
+    __shared__ double s_w[RT * S];
+    __shared__ double s_red[kWarps][32][NV];
+    const UpTask t = tasks[blockIdx.x];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const TA* U = Uar + t.u_off;
+    for (int ct = 0; ct < t.ncol; ct += 32)
+    {
+        const int c = ct + lane;
+        double acc[NV];
+#pragma unroll
+        for (int v = 0; v < NV; v++) acc[v] = 0.0;
+        for (int rc = 0; rc < t.nrow; rc += RT)
+        {
+            const int nr = min(RT, t.nrow - rc);
+            __syncthreads();
+            for (int i = threadIdx.x; i < nr * NV; i += kThreads)
+            {
+                int r = i / NV, v = i % NV;
+                s_w[r * S + v] = XS[(long long) (t.in_row + rc + r) * NV + v];
+            }
+            __syncthreads();
+            if (c < t.ncol)
+            {
+                int r = w;
+                for (; r + kWarps < nr; r += 2 * kWarps)
+                {
+                    double a0 = to_d(U[(long long) (rc + r) * t.ncol + c]);
+                    double a1 = to_d(U[(long long) (rc + r + kWarps) * t.ncol + c]);
+#pragma unroll
+                    for (int v = 0; v < NV; v++)
+                        acc[v] = fma(a1, s_w[(r + kWarps) * S + v], fma(a0, s_w[r * S + v], acc[v]));
+                }
+                if (r < nr)
+                {
+                    double a0 = to_d(U[(long long) (rc + r) * t.ncol + c]);
+#pragma unroll
+                    for (int v = 0; v < NV; v++) acc[v] = fma(a0, s_w[r * S + v], acc[v]);
+                }
+            }
+        }
+#pragma unroll
+        for (int v = 0; v < NV; v++) s_red[w][lane][v] = acc[v];
+        __syncthreads();
+        for (int i = threadIdx.x; i < 32 * NV; i += kThreads)
+        {
+            int cc = i / NV, v = i % NV;
+            if (ct + cc < t.ncol)
+            {
+                double s = 0.0;
+#pragma unroll
+                for (int k = 0; k < kWarps; k++) s += s_red[k][cc][v];
+                XS[(long long) (t.out_row + ct + cc) * NV + v] = s;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------- row-chunk block apply
+
+// Input of the "A * v" product for a column tile: either rows of XS, or (downward
+// sweep) the node's summed y1 plus the parent's push-down slice.
+struct VFromXS {
+    const double* XS; int row;
+    __device__ double operator()(int c, int v, int NVs) const { return XS[(long long) (row + c) * NVs + v]; }
+};
+struct VFromY1 {
+    const double* Y1; const double* PUSH; int y1_row, push_row;
+    __device__ double operator()(int c, int v, int NVs) const
+    {
+        double s = (y1_row >= 0) ? Y1[(long long) (y1_row + c) * NVs + v] : 0.0;
+        if (push_row >= 0) s += PUSH[(long long) (push_row + c) * NVs + v];
+        return s;
+    }
+};
+
+// One chunk of R <= 64 rows of a row-major block (ld = ncol):
+//   out0[r][v] = sum_c A[r][c] vin[c][v]     (if out0 != nullptr)
+//   out1[c][v] = sum_r A[r][c] win[r][v]     (if out1 != nullptr)
+template <int NV>
+constexpr int chunk_smem_bytes() { return 8 * (64 * SV<NV>::v + 32 * SV<NV>::v + 64 * NV + kWarps * 32 * NV); }
+
+template <typename TA, int NV, typename VIN>
+__device__ __forceinline__ void chunk_apply(const TA* __restrict__ A, int R, int ncol, VIN vin,
+                                            const double* __restrict__ win_XS, int win_row,
+                                            double* __restrict__ out0, double* __restrict__ out1,
+                                            double* __restrict__ smem)
+{
+    constexpr int S = SV<NV>::v;
+    double* s_w = smem;
+    double* s_v = s_w + 64 * S;
+    double* s_o0 = s_v + 32 * S;
+    double (*s_red)[32][NV] = reinterpret_cast<double (*)[32][NV]>(s_o0 + 64 * NV);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const bool do0 = out0 != nullptr, do1 = out1 != nullptr;
+    if (do1)
+        for (int i = threadIdx.x; i < R * NV; i += kThreads)
+            s_w[(i / NV) * S + (i % NV)] = win_XS[(long long) (win_row + i / NV) * NV + (i % NV)];
+    for (int i = threadIdx.x; i < R * NV; i += kThreads) s_o0[i] = 0.0;
+    for (int ct = 0; ct < ncol; ct += 32)
+    {
+        const int c = ct + lane;
+        const bool cin = c < ncol;
+        __syncthreads();
+        if (do0)
+            for (int i = threadIdx.x; i < 32 * NV; i += kThreads)
+            {
+                int cc = i / NV, v = i % NV;
+                s_v[cc * S + v] = (ct + cc < ncol) ? vin(ct + cc, v, NV) : 0.0;
+            }
+        __syncthreads();
+        double acc1[NV];
+#pragma unroll
+        for (int v = 0; v < NV; v++) acc1[v] = 0.0;
+        for (int r = w; r < R; r += kWarps)
+        {
+            double a = cin ? to_d(A[(long long) r * ncol + c]) : 0.0;
+            if (do1)
+            {
+#pragma unroll
+                for (int v = 0; v < NV; v++) acc1[v] = fma(a, s_w[r * S + v], acc1[v]);
+            }
+            if (do0)
+            {
+                double p[NV];
+#pragma unroll
+                for (int v = 0; v < NV; v++) p[v] = a * s_v[lane * S + v];
+                warp_transpose_reduce<NV>(p, lane);
+                if (lane_writes<NV>(lane)) s_o0[r * NV + nv_of_lane<NV>(lane)] += p[0];
+            }
+        }
+        if (do1)
+        {
+#pragma unroll
+            for (int v = 0; v < NV; v++) s_red[w][lane][v] = acc1[v];
+            __syncthreads();
+            for (int i = threadIdx.x; i < 32 * NV; i += kThreads)
+            {
+                int cc = i / NV, v = i % NV;
+                if (ct + cc < ncol)
+                {
+                    double s = 0.0;
+#pragma unroll
+                    for (int k = 0; k < kWarps; k++) s += s_red[k][cc][v];
+                    out1[(long long) (ct + cc) * NV + v] = s;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    if (do0)
+        for (int i = threadIdx.x; i < R * NV; i += kThreads) out0[i] = s_o0[i];
+}
+
+template <typename TA, int NV>
+__global__ void __launch_bounds__(kThreads) k_blk(const BlkTask* __restrict__ tasks, const TA* __restrict__ arena,
+                                                  const double* __restrict__ XS, double* __restrict__ PS)
+{
+    extern __shared__ double dsm[];
+    const BlkTask t = tasks[blockIdx.x];
+    VFromXS vin{XS, t.in0_row};
+    chunk_apply<TA, NV>(arena + t.a_off, t.nrow, t.ncol, vin, XS, t.in1_row,
+                        t.out0_row >= 0 ? PS + (long long) t.out0_row * NV : nullptr,
+                        t.out1_row >= 0 ? PS + (long long) t.out1_row * NV : nullptr, dsm);
+}
+
+template <typename TA, int NV>
+__global__ void __launch_bounds__(kThreads) k_down(const DownTask* __restrict__ tasks, const TA* __restrict__ Uar,
+                                                   const double* __restrict__ Y1, double* __restrict__ PS,
+                                                   double* __restrict__ PUSH)
+{
+    extern __shared__ double dsm[];
+    const DownTask t = tasks[blockIdx.x];
+    VFromY1 vin{Y1, PUSH, t.y1_row, t.push_row};
+    double* dst = t.dst_ps ? PS + (long long) t.dst_row * NV : PUSH + (long long) t.dst_row * NV;
+    chunk_apply<TA, NV>(Uar + t.u_off, t.nrow, t.ncol, vin, nullptr, 0, dst, nullptr, dsm);
+}
+
+// y1 of a node = sum of its PS slots (fixed order); rows indexed like the y0 region.
+template <int NV>
+__global__ void k_y1sum(const Y1Task* __restrict__ tasks, const int* __restrict__ slots,
+                        const double* __restrict__ PS, double* __restrict__ Y1)
+{
+    const Y1Task t = tasks[blockIdx.x];
+    for (int i = threadIdx.x; i < t.nrow * NV; i += blockDim.x)
+    {
+        double s = 0.0;
+        for (int k = t.slot_beg; k < t.slot_end; k++) s += PS[(long long) slots[k] * NV + i];
+        Y1[(long long) t.row * NV + i] = s;
+    }
+}
+
+// --------------------------------------------------------------- assemble
+
+// Y[fwd[row0 + r]][v] = sum over the leaf's slots (fixed order)
+template <int NV>
+__global__ void k_asm(const AsmTask* __restrict__ tasks, const int* __restrict__ slots,
+                      const double* __restrict__ PS, const int* __restrict__ fwd,
+                      double* __restrict__ Y, long long y_rs, long long y_cs, int nv)
+{
+    const AsmTask t = tasks[blockIdx.x];
+    for (int i = threadIdx.x; i < t.nrow * NV; i += blockDim.x)
+    {
+        int r = i / NV, v = i % NV;
+        if (v >= nv) continue;
+        double s = 0.0;
+        for (int k = t.slot_beg; k < t.slot_end; k++) s += PS[(long long) (slots[k] + r) * NV + v];
+        Y[(long long) fwd[t.row0 + r] * y_rs + (long long) v * y_cs] = s;
+    }
+}
+
+// ------------------------------------------------------------------- kernels
+
+// Kernel functions, restated from src/H2Pack_3D_kernels.h (Coulomb :98-161,
+// Gaussian :209-268, Matern 3/2 :435-497, RPY :893-959).
+template <typename T> struct Math;
+template <> struct Math<double> {
+    static __device__ __forceinline__ double rsqrt_(double x) { return 1.0 / sqrt(x); }
+    static __device__ __forceinline__ double sqrt_(double x) { return sqrt(x); }
+    static __device__ __forceinline__ double exp_(double x) { return exp(x); }
+    static __device__ __forceinline__ double div_(double a, double b) { return a / b; }
+};
+template <> struct Math<float> {
+    static __device__ __forceinline__ float rsqrt_(float x) { return rsqrtf(x); }
+    static __device__ __forceinline__ float sqrt_(float x) { return x > 0.f ? x * rsqrtf(x) : 0.f; }
+    static __device__ __forceinline__ float exp_(float x) { return __expf(x); }
+    static __device__ __forceinline__ float div_(float a, float b) { return __fdividef(a, b); }
+};
+
+template <int KID, typename T> struct Scalar;
+template <typename T> struct Scalar<KRNL_COULOMB_ID, T> {
+    static __device__ __forceinline__ T f(T r2, T p0, T) { return r2 == T(0) ? p0 : Math<T>::rsqrt_(r2); }
+};
+template <typename T> struct Scalar<KRNL_GAUSSIAN_ID, T> {
+    static __device__ __forceinline__ T f(T r2, T p0, T) { return Math<T>::exp_(-p0 * r2); }
+};
+template <typename T> struct Scalar<KRNL_MATERN32_ID, T> {
+    static __device__ __forceinline__ T f(T r2, T, T c0)
+    {
+        T t = c0 * Math<T>::sqrt_(r2);   // c0 = -sqrt(3) l
+        return (T(1) - t) * Math<T>::exp_(t);
+    }
+};
+
+// RPY 3x3 block: K_ab = t2 u_a u_b + t1 delta_ab, u = (dx,dy,dz)/r (0 at r = 0)
+template <typename T>
+__device__ __forceinline__ void rpy_coef(T dx, T dy, T dz, T ta, T sa, T C, T& t1, T& t2, T& ux, T& uy, T& uz)
+{
+    T r2 = dx * dx + dy * dy + dz * dz;
+    T r = Math<T>::sqrt_(r2);
+    T inv_r = (r == T(0)) ? T(0) : Math<T>::div_(T(1), r);
+    T inv_r2 = inv_r * inv_r;
+    ux = dx * inv_r; uy = dy * inv_r; uz = dz * inv_r;
+    T ta_p_sa = ta + sa, ta_m_sa = ta - sa;
+    if (r > ta_p_sa)
+    {
+        T tmp0 = C * T(0.75) * inv_r;
+        T tmp1 = (ta * ta + sa * sa) * inv_r2;
+        t1 = tmp0 * (T(1) + tmp1 / T(3));
+        t2 = tmp0 * (T(1) - tmp1);
+    } else if (r > fabs(ta_m_sa)) {
+        T tmp0 = ta_m_sa * ta_m_sa;
+        T tmp1 = Math<T>::div_(inv_r2 * inv_r * C, ta * sa * T(32));
+        T a = tmp0 + T(3) * r2;
+        t1 = tmp1 * (T(16) * r2 * r * ta_p_sa - a * a);
+        T b = tmp0 - r2;
+        t2 = tmp1 * T(3) * b * b;
+    } else {
+        t1 = Math<T>::div_(C, (ta > sa ? ta : sa));
+        t2 = T(0);
+    }
+}
+
+template <typename T> struct Vec4;
+template <> struct Vec4<double> { using t = double4; };
+template <> struct Vec4<float> { using t = float4; };
+
+// ------------------------------------------------------------ JIT owner kernel
+
+// One CTA per target chunk (<= 128*TPT points).  For every source set of the
+// target, source points and their inputs are staged in shared memory in tiles of
+// 128; each thread evaluates its targets against every staged source point and
+// accumulates K * in in registers (the one-sided form of H2P_ext_krnl_bimv,
+// src/H2Pack_matvec.c:463-539).  Outputs are written once, no atomics.
+template <int KID, typename T, int NV, int KD, int TPT>
+__global__ void __launch_bounds__(128) k_jit(const JitTarget* __restrict__ tgts, const JitSource* __restrict__ srcs,
+                                             const typename Vec4<T>::t* __restrict__ pts, KParam kp, int use_shift,
+                                             const double* __restrict__ XS, double* __restrict__ PS,
+                                             double* __restrict__ Y1)
+{
+    using T4 = typename Vec4<T>::t;
+    constexpr int W = KD * NV;
+    constexpr int TILE = (128 * W * (int) sizeof(T) > 32768) ? 64 : 128;
+    __shared__ T4 s_pt[TILE];
+    __shared__ T s_in[TILE * W];
+    const JitTarget tg = tgts[blockIdx.x];
+    const T p0 = (T) kp.p0, c0 = (T) kp.c0;
+
+    T4 xi[TPT];
+    bool valid[TPT];
+    T acc[TPT][W];
+#pragma unroll
+    for (int q = 0; q < TPT; q++)
+    {
+        int i = threadIdx.x + q * 128;
+        valid[q] = i < tg.npt;
+        xi[q] = pts[tg.pt0 + (valid[q] ? i : 0)];
+#pragma unroll
+        for (int k = 0; k < W; k++) acc[q][k] = T(0);
+    }
+
+    for (int s = tg.src_beg; s < tg.src_end; s++)
+    {
+        const JitSource sc = srcs[s];
+        T4 xs[TPT];
+#pragma unroll
+        for (int q = 0; q < TPT; q++)
+        {
+            xs[q] = xi[q];
+            if (use_shift) { xs[q].x += (T) sc.sx; xs[q].y += (T) sc.sy; xs[q].z += (T) sc.sz; }
+        }
+        for (int j0 = 0; j0 < sc.npt; j0 += TILE)
+        {
+            const int nj = min(TILE, sc.npt - j0);
+            __syncthreads();
+            for (int j = threadIdx.x; j < nj; j += 128) s_pt[j] = pts[sc.pt0 + j0 + j];
+            for (int i = threadIdx.x; i < nj * W; i += 128)
+                s_in[i] = (T) XS[(long long) (sc.in_row + KD * j0) * NV + i];
+            __syncthreads();
+            for (int j = 0; j < nj; j++)
+            {
+                const T4 pj = s_pt[j];
+                const T* inj = s_in + j * W;
+#pragma unroll
+                for (int q = 0; q < TPT; q++)
+                {
+                    T dx = xs[q].x - pj.x, dy = xs[q].y - pj.y, dz = xs[q].z - pj.z;
+                    if constexpr (KD == 1)
+                    {
+                        T r2 = dx * dx + dy * dy + dz * dz;
+                        T k = Scalar<KID, T>::f(r2, p0, c0);
+#pragma unroll
+                        for (int v = 0; v < NV; v++) acc[q][v] = fma(k, inj[v], acc[q][v]);
+                    } else {
+                        T t1, t2, ux, uy, uz;
+                        rpy_coef<T>(dx, dy, dz, xi[q].w, pj.w, c0, t1, t2, ux, uy, uz);
+#pragma unroll
+                        for (int v = 0; v < NV; v++)
+                        {
+                            T bx = inj[0 * NV + v], by = inj[1 * NV + v], bz = inj[2 * NV + v];
+                            T dot = t2 * (ux * bx + uy * by + uz * bz);
+                            acc[q][0 * NV + v] = fma(dot, ux, fma(t1, bx, acc[q][0 * NV + v]));
+                            acc[q][1 * NV + v] = fma(dot, uy, fma(t1, by, acc[q][1 * NV + v]));
+                            acc[q][2 * NV + v] = fma(dot, uz, fma(t1, bz, acc[q][2 * NV + v]));
+                        }
+                    }
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < TPT; q++)
+    {
+        if (!valid[q]) continue;
+        int i = threadIdx.x + q * 128;
+        double* o = (tg.out_y1 ? Y1 : PS) + (long long) (tg.out_row + KD * i) * NV;
+#pragma unroll
+        for (int k = 0; k < W; k++) o[k] = (double) acc[q][k];
+    }
+}
+
+// --------------------------------------------------------------- direct sum
+
+template <int KID, int KD>
+__global__ void __launch_bounds__(128) k_direct(const double4* __restrict__ trg, int n_trg,
+                                                const double4* __restrict__ src, int n_src,
+                                                const double* __restrict__ val, KParam kp, double* __restrict__ out)
+{
+    constexpr int TILE = 128;
+    __shared__ double4 s_pt[TILE];
+    __shared__ double s_v[TILE * KD];
+    const int i = blockIdx.x * 128 + threadIdx.x;
+    const double4 xi = trg[i < n_trg ? i : 0];
+    double acc[KD];
+#pragma unroll
+    for (int a = 0; a < KD; a++) acc[a] = 0.0;
+    for (int j0 = 0; j0 < n_src; j0 += TILE)
+    {
+        const int nj = min(TILE, n_src - j0);
+        __syncthreads();
+        for (int j = threadIdx.x; j < nj; j += 128) s_pt[j] = src[j0 + j];
+        for (int j = threadIdx.x; j < nj * KD; j += 128) s_v[j] = val[(long long) j0 * KD + j];
+        __syncthreads();
+        for (int j = 0; j < nj; j++)
+        {
+            double dx = xi.x - s_pt[j].x, dy = xi.y - s_pt[j].y, dz = xi.z - s_pt[j].z;
+            if constexpr (KD == 1)
+            {
+                double r2 = dx * dx + dy * dy + dz * dz;
+                acc[0] = fma(Scalar<KID, double>::f(r2, kp.p0, kp.c0), s_v[j], acc[0]);
+            } else {
+                double t1, t2, ux, uy, uz;
+                rpy_coef<double>(dx, dy, dz, xi.w, s_pt[j].w, kp.c0, t1, t2, ux, uy, uz);
+                double bx = s_v[3 * j], by = s_v[3 * j + 1], bz = s_v[3 * j + 2];
+                double dot = t2 * (ux * bx + uy * by + uz * bz);
+                acc[0] += dot * ux + t1 * bx;
+                acc[1] += dot * uy + t1 * by;
+                acc[2] += dot * uz + t1 * bz;
+            }
+        }
+    }
+    if (i < n_trg)
+#pragma unroll
+        for (int a = 0; a < KD; a++) out[(long long) i * KD + a] = acc[a];
+}
+
+// ------------------------------------------------------------- launchers
+
+static inline unsigned grid_for(long long n, int threads)
+{
+    long long g = (n + threads - 1) / threads;
+    if (g > 148LL * 64) g = 148LL * 64;
+    return (unsigned) (g < 1 ? 1 : g);
+}
+
+#define NV_DISPATCH(nv, ...)                                  \
+    switch (nv) {                                             \
+        case 1:  { constexpr int NVc = 1;  __VA_ARGS__; } break; \
+        case 2:  { constexpr int NVc = 2;  __VA_ARGS__; } break; \
+        case 4:  { constexpr int NVc = 4;  __VA_ARGS__; } break; \
+        case 8:  { constexpr int NVc = 8;  __VA_ARGS__; } break; \
+        case 16: { constexpr int NVc = 16; __VA_ARGS__; } break; \
+        default: return cudaErrorInvalidValue;                \
+    }
+
+cudaError_t launch_gather(int NV, const double* X, long long x_rs, long long x_cs, int nv, const int* fwd, int N,
+                          double* XS, cudaStream_t st)
+{
+    NV_DISPATCH(NV, k_gather<NVc><<<grid_for((long long) N * NVc, 256), 256, 0, st>>>(X, x_rs, x_cs, nv, fwd, N, XS));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_permute(const double* X, long long x_rs, long long x_cs, const int* idx, int n, int nv, double* Y,
+                           long long y_rs, long long y_cs, cudaStream_t st)
+{
+    k_permute<<<grid_for((long long) n * nv, 256), 256, 0, st>>>(X, x_rs, x_cs, idx, n, nv, Y, y_rs, y_cs);
+    return cudaGetLastError();
+}
+
+template <typename TA>
+cudaError_t launch_up(int NV, const UpTask* t, int n, const TA* U, double* XS, cudaStream_t st)
+{
+    if (n <= 0) return cudaSuccess;
+    NV_DISPATCH(NV, k_up<TA, NVc><<<n, kThreads, 0, st>>>(t, U, XS));
+    return cudaGetLastError();
+}
+
+template <typename K>
+static cudaError_t allow_smem(K kern, int bytes)
+{
+    if (bytes <= 48 * 1024) return cudaSuccess;
+    return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
+template <typename TA>
+cudaError_t launch_blk(int NV, const BlkTask* t, int n, const TA* arena, const double* XS, double* PS, cudaStream_t st)
+{
+    if (n <= 0) return cudaSuccess;
+    NV_DISPATCH(NV, {
+        constexpr int b = chunk_smem_bytes<NVc>();
+        cudaError_t e = allow_smem(k_blk<TA, NVc>, b);
+        if (e != cudaSuccess) return e;
+        k_blk<TA, NVc><<<n, kThreads, b, st>>>(t, arena, XS, PS);
+    });
+    return cudaGetLastError();
+}
+
+template <typename TA>
+cudaError_t launch_down(int NV, const DownTask* t, int n, const TA* U, const double* Y1, double* PS, double* PUSH,
+                        cudaStream_t st)
+{
+    if (n <= 0) return cudaSuccess;
+    NV_DISPATCH(NV, {
+        constexpr int b = chunk_smem_bytes<NVc>();
+        cudaError_t e = allow_smem(k_down<TA, NVc>, b);
+        if (e != cudaSuccess) return e;
+        k_down<TA, NVc><<<n, kThreads, b, st>>>(t, U, Y1, PS, PUSH);
+    });
+    return cudaGetLastError();
+}
+
+cudaError_t launch_y1sum(int NV, const Y1Task* t, int n, const int* slots, const double* PS, double* Y1, cudaStream_t st)
+{
+    if (n <= 0) return cudaSuccess;
+    NV_DISPATCH(NV, k_y1sum<NVc><<<n, 256, 0, st>>>(t, slots, PS, Y1));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_asm(int NV, const AsmTask* t, int n, const int* slots, const double* PS, const int* fwd,
+                       double* Y, long long y_rs, long long y_cs, int nv, cudaStream_t st)
+{
+    if (n <= 0) return cudaSuccess;
+    NV_DISPATCH(NV, k_asm<NVc><<<n, 256, 0, st>>>(t, slots, PS, fwd, Y, y_rs, y_cs, nv));
+    return cudaGetLastError();
+}
+
+template <int KID, typename T, int KD>
+static cudaError_t launch_jit_k(int NV, const JitTarget* tg, int n, const JitSource* sr, const void* pts, KParam kp,
+                                int use_shift, const double* XS, double* PS, double* Y1, cudaStream_t st)
+{
+    using T4 = typename Vec4<T>::t;
+    const T4* p = (const T4*) pts;
+    // two targets per thread where the accumulators allow it
+    NV_DISPATCH(NV, {
+        if constexpr (KD * NVc <= 16)
+            k_jit<KID, T, NVc, KD, 2><<<n, 128, 0, st>>>(tg, sr, p, kp, use_shift, XS, PS, Y1);
+        else
+            k_jit<KID, T, NVc, KD, 1><<<n, 128, 0, st>>>(tg, sr, p, kp, use_shift, XS, PS, Y1);
+    });
+    return cudaGetLastError();
+}
+
+cudaError_t launch_jit(int kid, int fp32, int NV, const JitTarget* tg, int n, const JitSource* sr, const void* pts,
+                       KParam kp, int use_shift, const double* XS, double* PS, double* Y1, cudaStream_t st)
+{
+    if (n <= 0) return cudaSuccess;
+    switch (kid)
+    {
+        case KRNL_COULOMB_ID:  return fp32 ? launch_jit_k<KRNL_COULOMB_ID, float, 1>(NV, tg, n, sr, pts, kp, use_shift, XS, PS, Y1, st)
+                                           : launch_jit_k<KRNL_COULOMB_ID, double, 1>(NV, tg, n, sr, pts, kp, use_shift, XS, PS, Y1, st);
+        case KRNL_GAUSSIAN_ID: return fp32 ? launch_jit_k<KRNL_GAUSSIAN_ID, float, 1>(NV, tg, n, sr, pts, kp, use_shift, XS, PS, Y1, st)
+                                           : launch_jit_k<KRNL_GAUSSIAN_ID, double, 1>(NV, tg, n, sr, pts, kp, use_shift, XS, PS, Y1, st);
+        case KRNL_MATERN32_ID: return fp32 ? launch_jit_k<KRNL_MATERN32_ID, float, 1>(NV, tg, n, sr, pts, kp, use_shift, XS, PS, Y1, st)
+                                           : launch_jit_k<KRNL_MATERN32_ID, double, 1>(NV, tg, n, sr, pts, kp, use_shift, XS, PS, Y1, st);
+        case KRNL_RPY_ID:      return fp32 ? launch_jit_k<KRNL_RPY_ID, float, 3>(NV, tg, n, sr, pts, kp, use_shift, XS, PS, Y1, st)
+                                           : launch_jit_k<KRNL_RPY_ID, double, 3>(NV, tg, n, sr, pts, kp, use_shift, XS, PS, Y1, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_direct(int kid, const double4* trg, int n_trg, const double4* src, int n_src, const double* val,
+                          KParam kp, double* out, cudaStream_t st)
+{
+    unsigned g = (unsigned) ((n_trg + 127) / 128);
+    switch (kid)
+    {
+        case KRNL_COULOMB_ID:  k_direct<KRNL_COULOMB_ID, 1><<<g, 128, 0, st>>>(trg, n_trg, src, n_src, val, kp, out); break;
+        case KRNL_GAUSSIAN_ID: k_direct<KRNL_GAUSSIAN_ID, 1><<<g, 128, 0, st>>>(trg, n_trg, src, n_src, val, kp, out); break;
+        case KRNL_MATERN32_ID: k_direct<KRNL_MATERN32_ID, 1><<<g, 128, 0, st>>>(trg, n_trg, src, n_src, val, kp, out); break;
+        case KRNL_RPY_ID:      k_direct<KRNL_RPY_ID, 3><<<g, 128, 0, st>>>(trg, n_trg, src, n_src, val, kp, out); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_up<double>(int, const UpTask*, int, const double*, double*, cudaStream_t);
+template cudaError_t launch_up<float>(int, const UpTask*, int, const float*, double*, cudaStream_t);
+template cudaError_t launch_blk<double>(int, const BlkTask*, int, const double*, const double*, double*, cudaStream_t);
+template cudaError_t launch_blk<float>(int, const BlkTask*, int, const float*, const double*, double*, cudaStream_t);
+template cudaError_t launch_down<double>(int, const DownTask*, int, const double*, const double*, double*, double*, cudaStream_t);
+template cudaError_t launch_down<float>(int, const DownTask*, int, const float*, const double*, double*, double*, cudaStream_t);
+
+}  // namespace h2gpu

@@ -1,0 +1,257 @@
+"""Host-side API of the B200 H2 apply engine.
+
+Two layers, mirroring how H2Pack is used:
+
+* :class:`H2Matrix` -- an H2 representation built by H2Pack's own construction
+  (``H2P_init -> H2P_partition_points -> proxy points -> H2P_build``, through
+  ``libH2Pack_gpu.so``) and applied with H2Pack's entry points ``H2P_matvec`` /
+  ``H2P_matmul``, which in that library run on the GPU.  This is the drop-in:
+  the calls and their argument meaning are H2Pack's (src/H2Pack_matvec.h:17,
+  src/H2Pack_matmul.h:25-28), with host arrays in the caller's point order.
+* :class:`Image` -- the engine's C ABI (include/h2gpu.h) on a plain-pointer
+  descriptor, including the device-resident apply on torch CUDA tensors.
+
+There is no CPU fallback: every apply goes through ``libh2gpu.so``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi
+
+_dp = C.POINTER(C.c_double)
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(_dp)
+
+
+def _kernel_id(kernel) -> int:
+    return _abi.KERNEL_IDS[kernel] if isinstance(kernel, str) else int(kernel)
+
+
+def _prec(p) -> int:
+    if isinstance(p, str):
+        return {"fp64": _abi.PREC_FP64, "mixed": _abi.PREC_MIXED}[p]
+    return int(p)
+
+
+class Image:
+    """Device image of one H2 representation (h2gpu_image_create)."""
+
+    def __init__(self, desc: _abi.Desc, precision="fp64", max_n_vec: int = 16, device: int = -1):
+        self.lib = _abi.libh2gpu()
+        opt = _abi.Options(_prec(precision), int(max_n_vec), int(device))
+        h = C.c_void_p()
+        _abi.check(self.lib.h2gpu_image_create(C.byref(desc), C.byref(opt), C.byref(h)), self.lib, "h2gpu_image_create")
+        self.handle = h
+        self.N = int(desc.krnl_dim) * int(desc.n_point)
+
+    def set_precision(self, precision):
+        _abi.check(self.lib.h2gpu_set_precision(self.handle, _prec(precision)), self.lib, "h2gpu_set_precision")
+
+    def matvec(self, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.empty(self.N)
+        _abi.check(self.lib.h2gpu_matvec(self.handle, _dptr(x), _dptr(y)), self.lib, "h2gpu_matvec")
+        return y
+
+    def matmul(self, X: np.ndarray, layout: int = _abi.ROW_MAJOR) -> np.ndarray:
+        """Y = A X for X of shape (N, n_vec); layout picks the storage handed to the ABI."""
+        N, nv = X.shape
+        if layout == _abi.ROW_MAJOR:
+            Xc = np.ascontiguousarray(X, dtype=np.float64)
+            Y = np.empty((N, nv))
+            st = self.lib.h2gpu_matmul(self.handle, layout, nv, _dptr(Xc), nv, _dptr(Y), nv)
+            res = Y
+        else:
+            Xc = np.ascontiguousarray(X.T, dtype=np.float64)
+            Y = np.empty((nv, N))
+            st = self.lib.h2gpu_matmul(self.handle, layout, nv, _dptr(Xc), N, _dptr(Y), N)
+            res = Y.T
+        _abi.check(st, self.lib, "h2gpu_matmul")
+        return res
+
+    def matmul_device(self, X, Y=None, stream=None):
+        """Device-resident apply on torch CUDA tensors of shape (N, n_vec), float64, row-major."""
+        import torch
+        assert X.is_cuda and X.dtype == torch.float64 and X.dim() == 2 and X.stride(1) == 1
+        if Y is None:
+            Y = torch.empty_like(X)
+        s = C.c_void_p(stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream)
+        st = self.lib.h2gpu_matmul_device(self.handle, X.shape[1], C.c_void_p(X.data_ptr()), X.stride(0),
+                                          C.c_void_p(Y.data_ptr()), Y.stride(0), s)
+        _abi.check(st, self.lib, "h2gpu_matmul_device")
+        return Y
+
+    def permute(self, x: np.ndarray, forward: bool = True) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.empty_like(x)
+        _abi.check(self.lib.h2gpu_permute_vector(self.handle, 1 if forward else 0, _dptr(x), _dptr(y)),
+                   self.lib, "h2gpu_permute_vector")
+        return y
+
+    def stats(self) -> dict:
+        s = _abi.Stats()
+        _abi.check(self.lib.h2gpu_get_stats(self.handle, C.byref(s)), self.lib, "h2gpu_get_stats")
+        out = {k: getattr(s, k) for k, _ in _abi.Stats._fields_}
+        out["ms_phase"] = list(s.ms_phase)
+        return out
+
+    def reset_stats(self):
+        self.lib.h2gpu_reset_stats(self.handle)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.h2gpu_image_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def direct_sum(kernel, param, src_coord, src_val, trg_coord) -> np.ndarray:
+    """FP64 direct sum on the GPU: y_t = sum_s K(x_t, x_s) v_s (examples/direct_nbody.h)."""
+    lib = _abi.libh2gpu()
+    kid = _kernel_id(kernel)
+    kd = 3 if kid == _abi.KRNL_RPY else 1
+    src = np.ascontiguousarray(src_coord, dtype=np.float64)
+    trg = np.ascontiguousarray(trg_coord, dtype=np.float64)
+    val = np.ascontiguousarray(src_val, dtype=np.float64)
+    p = np.zeros(4)
+    p[:len(param)] = param
+    out = np.empty(trg.shape[1] * kd)
+    st = lib.h2gpu_direct_sum(kid, _dptr(p), len(param), src.shape[0], kd, _dptr(src), src.shape[1], _dptr(val),
+                              _dptr(trg), trg.shape[1], _dptr(out))
+    _abi.check(st, lib, "h2gpu_direct_sum")
+    return out
+
+
+class H2Matrix:
+    """An H2 matrix built by H2Pack's construction and applied by the GPU drop-in.
+
+    ``proxy`` selects the proxy points: ``"id"`` numerical (H2P_generate_proxy_point_ID_file,
+    cached in ``pp_fname``) or ``"surface"`` (H2P_generate_proxy_point_surface).
+    """
+
+    def __init__(self, kernel, coord: np.ndarray, param=(), reltol: float = 1e-6, BD_JIT: int = 0,
+                 max_leaf_points: int = 0, max_leaf_size: float = 0.0, proxy: str = "surface",
+                 pp_fname: str | None = None, precision="fp64", n_thread: int = 0):
+        self.lib = _abi.libh2pack_gpu()
+        self.kernel_id = _kernel_id(kernel)
+        self.param = np.zeros(4)
+        self.param[:len(param)] = param
+        self.n_param = len(param)
+        self.coord = np.ascontiguousarray(coord, dtype=np.float64)
+        n_point = self.coord.shape[1]
+        h = self.lib.h2pb_build(self.kernel_id, _dptr(self.param), self.n_param, n_point, _dptr(self.coord),
+                                float(reltol), int(max_leaf_points), float(max_leaf_size), int(BD_JIT),
+                                0 if proxy == "id" else 1, pp_fname.encode() if pp_fname else None, 1, int(n_thread))
+        if not h:
+            raise RuntimeError("H2Pack construction (h2pb_build) failed")
+        self.handle = h
+        self.h2pack = self.lib.h2pb_h2pack(h)
+        info = (C.c_longlong * 16)()
+        self.lib.h2pb_info(self.h2pack, info)
+        self.info = dict(zip(["n_point", "krnl_dim", "xpt_dim", "n_node", "n_leaf_node", "max_level",
+                              "min_adm_level", "n_r_adm_pair", "n_r_inadm_pair", "n_B", "n_D", "BD_JIT",
+                              "krnl_mat_size", "max_leaf_points", "n_thread", "mm_max_n_vec"], list(info)))
+        self.N = self.info["krnl_mat_size"]
+        self.build_seconds = self.lib.h2pb_build_seconds(h)
+        self._check(self.lib.H2P_gpu_set_kernel(self.h2pack, self.kernel_id, _dptr(self.param), self.n_param),
+                    "H2P_gpu_set_kernel")
+        self.set_precision(precision)
+
+    def _check(self, st, what):
+        if st != 0:
+            m = self.lib.H2P_gpu_last_error()
+            raise RuntimeError(f"{what} failed with status {st}: {m.decode() if m else ''}")
+
+    def set_precision(self, precision):
+        self._check(self.lib.H2P_gpu_set_precision(self.h2pack, _prec(precision)), "H2P_gpu_set_precision")
+
+    def matvec(self, x: np.ndarray) -> np.ndarray:
+        """y = A x through H2Pack's H2P_matvec signature (status-returning form)."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.empty(self.N)
+        self._check(self.lib.H2P_gpu_matvec(self.h2pack, _dptr(x), _dptr(y)), "H2P_matvec")
+        return y
+
+    def matmul(self, X: np.ndarray, layout: int = _abi.ROW_MAJOR) -> np.ndarray:
+        N, nv = X.shape
+        if layout == _abi.ROW_MAJOR:
+            Xc = np.ascontiguousarray(X, dtype=np.float64)
+            Y = np.empty((N, nv))
+            st = self.lib.H2P_gpu_matmul(self.h2pack, layout, nv, _dptr(Xc), nv, _dptr(Y), nv)
+            res = Y
+        else:
+            Xc = np.ascontiguousarray(X.T, dtype=np.float64)
+            Y = np.empty((nv, N))
+            st = self.lib.H2P_gpu_matmul(self.h2pack, layout, nv, _dptr(Xc), N, _dptr(Y), N)
+            res = Y.T
+        self._check(st, "H2P_matmul")
+        return res
+
+    def matmul_raw(self, layout: int, n_vec: int, X_ptr: int, ldx: int, Y_ptr: int, ldy: int):
+        """H2P_matmul on caller-owned host memory (e.g. pinned torch tensors)."""
+        st = self.lib.H2P_gpu_matmul(self.h2pack, layout, n_vec, C.cast(X_ptr, _dp), ldx, C.cast(Y_ptr, _dp), ldy)
+        self._check(st, "H2P_matmul")
+
+    def image(self) -> Image:
+        """A non-owning Image view of the handle's device image."""
+        ptr = self.lib.H2P_gpu_image(self.h2pack)
+        if not ptr:
+            self._check(-5, "H2P_gpu_image")
+        img = Image.__new__(Image)
+        img.lib = _abi.libh2gpu()
+        img.handle = None          # not owned: released with the H2Matrix
+        img._view = C.c_void_p(ptr)
+        img.N = self.N
+        return _ImageView(img._view, self.N)
+
+    def describe(self) -> _abi.Desc:
+        d = _abi.Desc()
+        self._check(self.lib.h2pb_describe(self.handle, C.byref(d)), "h2pb_describe")
+        return d
+
+    def sorted_coord(self) -> np.ndarray:
+        xd = self.info["xpt_dim"]
+        p = self.lib.h2pb_coord(self.h2pack)
+        return np.ctypeslib.as_array(p, shape=(xd * self.info["n_point"],)).reshape(xd, -1).copy()
+
+    def counters(self) -> dict:
+        ms = (C.c_double * 11)()
+        tm = (C.c_double * 11)()
+        jf = (C.c_double * 2)()
+        nmv = C.c_longlong()
+        self.lib.h2pb_counters(self.h2pack, ms, tm, jf, C.byref(nmv))
+        return {"mat_size": list(ms), "timers": list(tm), "JIT_flops": list(jf), "n_matvec": nmv.value}
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.H2P_gpu_release(self.h2pack)
+            self.lib.h2pb_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class _ImageView(Image):
+    """Image methods on an image owned by someone else (the drop-in registry)."""
+
+    def __init__(self, handle, N):  # noqa: D401 - thin view
+        self.lib = _abi.libh2gpu()
+        self.handle = handle
+        self.N = N
+
+    def close(self):
+        self.handle = None

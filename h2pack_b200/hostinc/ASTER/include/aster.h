@@ -1,7 +1,7 @@
 /*
  * Scalar-lane stand-in for the ASTER SIMD wrapper used by H2Pack.
  *
- * TEST INFRASTRUCTURE ONLY.  The reference includes "ASTER/include/aster.h"
+ * Build support for compiling H2Pack's own sources.  H2Pack includes "ASTER/include/aster.h"
  * (src/H2Pack_config.h:109, src/H2Pack_3D_kernels.h:7), a git submodule
  * (https://github.com/huanghua1994/ASTER, pinned commit not recoverable) whose
  * directory is empty in the reference tree.  This header is NOT the ASTER source:

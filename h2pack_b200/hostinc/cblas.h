@@ -1,10 +1,9 @@
 /*
- * Minimal CBLAS prototype header for building the H2Pack oracle.
+ * Minimal CBLAS prototype header for compiling H2Pack's own sources.
  *
- * TEST INFRASTRUCTURE ONLY: this header exists so that the reference H2Pack
- * sources (src/linalg_lib_wrapper.h:16 includes <cblas.h>) compile against the
- * OpenBLAS shared object that ships inside the Python environment, which has no
- * development headers.  It declares only the enums and routines that the
+ * Build support: H2Pack (src/linalg_lib_wrapper.h:16 includes <cblas.h>) is
+ * compiled unchanged against the OpenBLAS shared object that ships inside the
+ * Python environment, which has no development headers.  It declares only the enums and routines that the
  * reference's construction and matvec/matmul files call, with the standard
  * CBLAS enum values (Netlib CBLAS ABI), written from the public CBLAS API.
  */

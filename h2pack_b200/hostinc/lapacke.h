@@ -1,7 +1,7 @@
 /*
- * Minimal LAPACKE prototype header for building the H2Pack oracle.
+ * Minimal LAPACKE prototype header for compiling H2Pack's own sources.
  *
- * TEST INFRASTRUCTURE ONLY.  The reference's src/linalg_lib_wrapper.h:17 includes
+ * Build support.  H2Pack's src/linalg_lib_wrapper.h:17 includes
  * <lapacke.h>; the construction and matvec/matmul sources compiled by the oracle
  * recipe call no LAPACKE routine, so this header only supplies the layout
  * constants and the lapack_int type, written from the public LAPACKE API.

@@ -153,6 +153,7 @@ typedef struct h2gpu_stats
     double jit_pairs_D;       /* kernel evaluations of the D phase per RHS panel       */
     long long n_tasks_B, n_tasks_D;
     long long device_bytes;   /* device memory held by the image                      */
+    long long n_launches;     /* kernels launched by all applies so far               */
 } h2gpu_stats;
 
 int  h2gpu_abi_version(void);

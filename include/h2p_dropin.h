@@ -1,0 +1,72 @@
+/*
+ * h2p_dropin.h -- GPU drop-in for H2Pack's apply path.
+ *
+ * libH2Pack_gpu.so exports H2Pack's own apply entry points with byte-identical
+ * signatures, so a program built against H2Pack links this library in place of
+ * H2Pack_matvec.o / H2Pack_matmul.o and runs the four phases on the GPU:
+ *
+ *   H2P_matvec                       src/H2Pack_matvec.h:17
+ *   H2P_permute_vector_forward       src/H2Pack_matvec.h:29
+ *   H2P_permute_vector_backward      src/H2Pack_matvec.h:30
+ *   H2P_matmul                       src/H2Pack_matmul.h:25-28
+ *   H2P_permute_matrix_row_forward   src/H2Pack_matmul.h:47-50
+ *   H2P_permute_matrix_row_backward  src/H2Pack_matmul.h:51-54
+ *
+ * The first call on an H2Pack handle uploads its representation (tree, pair
+ * lists, U, B, D, coordinates, permutations) into a device image kept in a
+ * registry keyed by the handle; later calls reuse it.  A fingerprint of the
+ * handle's arrays is checked on every call, so a handle rebuilt at the same
+ * address is re-uploaded.  Like the reference (ASSERT_PRINTF, src/utils.h:56-66)
+ * the void entry points print the reason and abort on failure; the H2P_gpu_*
+ * variants return an h2gpu status instead.
+ *
+ * Extra entry points (no counterpart in the reference):
+ *   H2P_gpu_set_kernel     name the kernel function of a JIT-mode handle.  The
+ *                          reference keeps only function pointers to static
+ *                          functions (src/H2Pack_typedef.h:193-196), which cannot be
+ *                          identified across translation units, so JIT mode needs it.
+ *   H2P_gpu_set_precision  H2GPU_PREC_FP64 (default) or H2GPU_PREC_MIXED
+ *   H2P_gpu_matvec / H2P_gpu_matmul   status-returning forms
+ *   H2P_gpu_image          the handle's device image (for h2gpu_get_stats)
+ *   H2P_gpu_release        free the handle's device image (call before H2P_destroy)
+ *   H2P_gpu_last_error     message of the last failure
+ *
+ * Handles in HSS mode, RPY-Ewald / periodic handles and H2ERI handles are
+ * rejected with H2GPU_ERR_UNSUPPORTED.
+ */
+#ifndef H2P_DROPIN_H
+#define H2P_DROPIN_H
+
+#include "h2gpu.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+struct H2Pack;
+
+/* Same signatures as H2Pack (DTYPE = double, CBLAS_LAYOUT passed as its int value). */
+void H2P_matvec(struct H2Pack *h2pack, const double *x, double *y);
+void H2P_permute_vector_forward(struct H2Pack *h2pack, const double *x, double *pmt_x);
+void H2P_permute_vector_backward(struct H2Pack *h2pack, const double *x, double *pmt_x);
+void H2P_matmul(struct H2Pack *h2pack, const int layout, const int n_vec,
+                const double *mat_x, const int ldx, double *mat_y, const int ldy);
+void H2P_permute_matrix_row_forward(struct H2Pack *h2pack, const int layout, const int n_vec,
+                                    const double *mat_x, const int ldx, double *pmt_mat_x, const int ldp);
+void H2P_permute_matrix_row_backward(struct H2Pack *h2pack, const int layout, const int n_vec,
+                                     const double *mat_x, const int ldx, double *pmt_mat_x, const int ldp);
+
+int  H2P_gpu_set_kernel(struct H2Pack *h2pack, int kernel_id, const double *param, int n_param);
+int  H2P_gpu_set_precision(struct H2Pack *h2pack, int precision);
+int  H2P_gpu_matvec(struct H2Pack *h2pack, const double *x, double *y);
+int  H2P_gpu_matmul(struct H2Pack *h2pack, int layout, int n_vec,
+                    const double *mat_x, int ldx, double *mat_y, int ldy);
+h2gpu_image *H2P_gpu_image(struct H2Pack *h2pack);
+int  H2P_gpu_release(struct H2Pack *h2pack);
+const char *H2P_gpu_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
