@@ -817,7 +817,8 @@ int prepare(h2gpu_image* im, int NV)
 int apply_device(h2gpu_image* im, int n_vec, const double* X, long long x_rs, long long x_cs, double* Y,
                  long long y_rs, long long y_cs, cudaStream_t s)
 {
-    int NV = panel_width(n_vec, im->max_nv);
+    // JIT tensor kernels keep 3 x NV accumulators per target: panels of at most 8 there
+    int NV = panel_width(n_vec, (im->BD_JIT && im->kd == 3) ? std::min(im->max_nv, 8) : im->max_nv);
     TRY(prepare(im, NV));
     float ph[5] = {0, 0, 0, 0, 0};
     for (int c0 = 0; c0 < n_vec; c0 += NV)

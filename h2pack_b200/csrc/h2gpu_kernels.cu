@@ -392,20 +392,24 @@ template <> struct Vec4<float> { using t = float4; };
 
 // ------------------------------------------------------------ JIT owner kernel
 
-// One CTA per target chunk (<= 128*TPT points).  For every source set of the
-// target, source points and their inputs are staged in shared memory in tiles of
-// 128; each thread evaluates its targets against every staged source point and
-// accumulates K * in in registers (the one-sided form of H2P_ext_krnl_bimv,
-// src/H2Pack_matvec.c:463-539).  Outputs are written once, no atomics.
+// One CTA per chunk of <= 128 target points, 128/TPT threads, TPT targets per thread.
+// For every source set of the target, source points and their inputs are staged in
+// shared memory in tiles; each thread evaluates its targets against every staged
+// source point and accumulates K * in (the one-sided form of H2P_ext_krnl_bimv,
+// src/H2Pack_matvec.c:463-539).  With T = float the products of one tile are summed
+// in FP32 and every tile sum is added to FP64 accumulators, so an FP32 sum never
+// spans more than one tile of sources.  Outputs are written once, no atomics.
 template <int KID, typename T, int NV, int KD, int TPT>
-__global__ void __launch_bounds__(128) k_jit(const JitTarget* __restrict__ tgts, const JitSource* __restrict__ srcs,
-                                             const typename Vec4<T>::t* __restrict__ pts, KParam kp, int use_shift,
-                                             const double* __restrict__ XS, double* __restrict__ PS,
-                                             double* __restrict__ Y1)
+__global__ void __launch_bounds__(128 / TPT) k_jit(const JitTarget* __restrict__ tgts, const JitSource* __restrict__ srcs,
+                                                   const typename Vec4<T>::t* __restrict__ pts, KParam kp, int use_shift,
+                                                   const double* __restrict__ XS, double* __restrict__ PS,
+                                                   double* __restrict__ Y1)
 {
     using T4 = typename Vec4<T>::t;
+    constexpr int NT = 128 / TPT;
     constexpr int W = KD * NV;
     constexpr int TILE = (128 * W * (int) sizeof(T) > 32768) ? 64 : 128;
+    constexpr bool SPLIT = sizeof(T) < sizeof(double);
     __shared__ T4 s_pt[TILE];
     __shared__ T s_in[TILE * W];
     const JitTarget tg = tgts[blockIdx.x];
@@ -413,15 +417,21 @@ __global__ void __launch_bounds__(128) k_jit(const JitTarget* __restrict__ tgts,
 
     T4 xi[TPT];
     bool valid[TPT];
+    double acc64[SPLIT ? TPT : 1][SPLIT ? W : 1];
     T acc[TPT][W];
 #pragma unroll
     for (int q = 0; q < TPT; q++)
     {
-        int i = threadIdx.x + q * 128;
+        int i = threadIdx.x + q * NT;
         valid[q] = i < tg.npt;
         xi[q] = pts[tg.pt0 + (valid[q] ? i : 0)];
 #pragma unroll
         for (int k = 0; k < W; k++) acc[q][k] = T(0);
+        if constexpr (SPLIT)
+        {
+#pragma unroll
+            for (int k = 0; k < W; k++) acc64[q][k] = 0.0;
+        }
     }
 
     for (int s = tg.src_beg; s < tg.src_end; s++)
@@ -438,14 +448,18 @@ __global__ void __launch_bounds__(128) k_jit(const JitTarget* __restrict__ tgts,
         {
             const int nj = min(TILE, sc.npt - j0);
             __syncthreads();
-            for (int j = threadIdx.x; j < nj; j += 128) s_pt[j] = pts[sc.pt0 + j0 + j];
-            for (int i = threadIdx.x; i < nj * W; i += 128)
+            for (int j = threadIdx.x; j < nj; j += NT) s_pt[j] = pts[sc.pt0 + j0 + j];
+            for (int i = threadIdx.x; i < nj * W; i += NT)
                 s_in[i] = (T) XS[(long long) (sc.in_row + KD * j0) * NV + i];
             __syncthreads();
+#pragma unroll 2
             for (int j = 0; j < nj; j++)
             {
                 const T4 pj = s_pt[j];
                 const T* inj = s_in + j * W;
+                T in[W];
+#pragma unroll
+                for (int k = 0; k < W; k++) in[k] = inj[k];
 #pragma unroll
                 for (int q = 0; q < TPT; q++)
                 {
@@ -455,14 +469,14 @@ __global__ void __launch_bounds__(128) k_jit(const JitTarget* __restrict__ tgts,
                         T r2 = dx * dx + dy * dy + dz * dz;
                         T k = Scalar<KID, T>::f(r2, p0, c0);
 #pragma unroll
-                        for (int v = 0; v < NV; v++) acc[q][v] = fma(k, inj[v], acc[q][v]);
+                        for (int v = 0; v < NV; v++) acc[q][v] = fma(k, in[v], acc[q][v]);
                     } else {
                         T t1, t2, ux, uy, uz;
                         rpy_coef<T>(dx, dy, dz, xi[q].w, pj.w, c0, t1, t2, ux, uy, uz);
 #pragma unroll
                         for (int v = 0; v < NV; v++)
                         {
-                            T bx = inj[0 * NV + v], by = inj[1 * NV + v], bz = inj[2 * NV + v];
+                            T bx = in[0 * NV + v], by = in[1 * NV + v], bz = in[2 * NV + v];
                             T dot = t2 * (ux * bx + uy * by + uz * bz);
                             acc[q][0 * NV + v] = fma(dot, ux, fma(t1, bx, acc[q][0 * NV + v]));
                             acc[q][1 * NV + v] = fma(dot, uy, fma(t1, by, acc[q][1 * NV + v]));
@@ -471,16 +485,27 @@ __global__ void __launch_bounds__(128) k_jit(const JitTarget* __restrict__ tgts,
                     }
                 }
             }
+            if constexpr (SPLIT)
+            {
+#pragma unroll
+                for (int q = 0; q < TPT; q++)
+#pragma unroll
+                    for (int k = 0; k < W; k++) { acc64[q][k] += (double) acc[q][k]; acc[q][k] = T(0); }
+            }
         }
     }
 #pragma unroll
     for (int q = 0; q < TPT; q++)
     {
         if (!valid[q]) continue;
-        int i = threadIdx.x + q * 128;
+        int i = threadIdx.x + q * NT;
         double* o = (tg.out_y1 ? Y1 : PS) + (long long) (tg.out_row + KD * i) * NV;
 #pragma unroll
-        for (int k = 0; k < W; k++) o[k] = (double) acc[q][k];
+        for (int k = 0; k < W; k++)
+        {
+            if constexpr (SPLIT) o[k] = acc64[q][k];
+            else o[k] = (double) acc[q][k];
+        }
     }
 }
 
@@ -625,10 +650,10 @@ static cudaError_t launch_jit_k(int NV, const JitTarget* tg, int n, const JitSou
 {
     using T4 = typename Vec4<T>::t;
     const T4* p = (const T4*) pts;
-    // two targets per thread where the accumulators allow it
+    // two targets per thread (64 threads per 128-point chunk) where the accumulators allow it
     NV_DISPATCH(NV, {
         if constexpr (KD * NVc <= 16)
-            k_jit<KID, T, NVc, KD, 2><<<n, 128, 0, st>>>(tg, sr, p, kp, use_shift, XS, PS, Y1);
+            k_jit<KID, T, NVc, KD, 2><<<n, 64, 0, st>>>(tg, sr, p, kp, use_shift, XS, PS, Y1);
         else
             k_jit<KID, T, NVc, KD, 1><<<n, 128, 0, st>>>(tg, sr, p, kp, use_shift, XS, PS, Y1);
     });
