@@ -77,6 +77,7 @@ H2GPU_SYMBOLS = {
     "h2gpu_matmul_device": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
     "h2gpu_permute_vector": (C.c_int, [C.c_void_p, C.c_int, _dp, _dp]),
     "h2gpu_permute_matrix_rows": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, _dp, C.c_int, _dp, C.c_int]),
+    "h2gpu_matvec_device_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "h2gpu_get_stats": (C.c_int, [C.c_void_p, C.POINTER(Stats)]),
     "h2gpu_reset_stats": (C.c_int, [C.c_void_p]),
     "h2gpu_image_bytes": (C.c_size_t, [C.c_void_p]),

@@ -1090,3 +1090,84 @@ H2G_API int h2gpu_direct_sum(int kernel_id, const double* krnl_param, int n_krnl
     cudaFree(ds); cudaFree(dt); cudaFree(dv); cudaFree(dout);
     return st;
 }
+
+// ================================================== apply without allocation
+//
+// h2gpu_matvec_device_noalloc: y = A x for one device-resident vector, with every
+// work buffer (input space, partial sums, y1 sums, push-down) taken from the fixed
+// device array below instead of cudaMalloc.  For callers that cannot allocate device
+// memory at apply time: code whose device memory is owned entirely by another
+// allocator (a framework's caching allocator or a pool reserved up front, where a
+// direct cudaMalloc fails or fragments memory), and code that must not stall, since
+// cudaMalloc / cudaFree synchronize the device.  The image itself is created
+// beforehand, at set-up, where allocation is allowed.
+//
+// Limit: the work buffers of one right-hand side must fit in
+// H2GPU_NOALLOC_SCRATCH_DOUBLES doubles (16 MiB); larger images are rejected with
+// H2GPU_ERR_INVALID.  The array is a static device symbol, so every GPU that loads
+// the library holds these 16 MiB until the process exits.  Every call shares it and
+// it keeps the last call's contents: nothing needs clearing (each value read within a
+// call is written earlier in the same call), but calls that overlap on the GPU
+// (different streams, or different host threads on the same device) race on it.
+// The first call on a device looks up the array's device address with that device
+// current (cudaGetSymbolAddress), so that first call should come before any stream
+// capture.
+
+#define H2GPU_NOALLOC_SCRATCH_DOUBLES (2u * 1024u * 1024u)
+
+static __device__ __align__(256) double g_noalloc_scratch[H2GPU_NOALLOC_SCRATCH_DOUBLES];
+
+namespace {
+
+std::mutex g_noalloc_mu;
+double* g_noalloc_addr[64] = {};
+
+// Device address of the scratch array for `dev` (the current device), looked up once.
+int noalloc_scratch(int dev, double** out)
+{
+    if (dev < 0 || dev >= 64) return fail(H2GPU_ERR_INVALID, "device ordinal %d out of range", dev);
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (g_noalloc_addr[dev] == nullptr)
+    {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || p == nullptr)
+            return fail(H2GPU_ERR_CUDA, "cudaGetSymbolAddress of the scratch array failed: %s", cudaGetErrorString(e));
+        g_noalloc_addr[dev] = (double*) p;
+    }
+    *out = g_noalloc_addr[dev];
+    return H2GPU_OK;
+}
+
+}  // namespace
+
+H2G_API int h2gpu_matvec_device_noalloc(h2gpu_image* im, const double* d_x, double* d_y, void* stream)
+{
+    if (!im) return fail(H2GPU_ERR_INVALID, "image is NULL");
+    REQ(d_x && d_y, "device vectors are NULL");
+    std::lock_guard<std::mutex> lk(im->mu);
+    CK(cudaSetDevice(im->device));
+    if (im->precision == H2GPU_PREC_MIXED &&
+        ((im->U_elems && !im->d_U32) || (im->B_elems && !im->d_B32) || (im->D_elems && !im->d_D32)))
+        return fail(H2GPU_ERR_STATE, "the FP32 copies of this image are created by its first allocating apply "
+                                     "in mixed precision; run one h2gpu_matmul_device call first or use FP64");
+    const unsigned long long xs = (unsigned long long) im->N + im->y0_rows, ps = im->ps_rows, y1 = im->y0_rows;
+    const unsigned long long need = xs + ps + 2 * y1;
+    if (need > H2GPU_NOALLOC_SCRATCH_DOUBLES)
+        return fail(H2GPU_ERR_INVALID, "image needs %llu doubles of work space per right-hand side; the "
+                                       "no-allocation apply is limited to %u (16 MiB)", need,
+                    (unsigned) H2GPU_NOALLOC_SCRATCH_DOUBLES);
+    double* base = nullptr;
+    TRY(noalloc_scratch(im->device, &base));
+    cudaStream_t s = stream ? (cudaStream_t) stream : im->stream;
+    // run the regular panel sequence on the scratch buffers
+    double* keep[4] = {im->d_XS, im->d_PS, im->d_Y1, im->d_PUSH};
+    im->d_XS = base;
+    im->d_PS = base + xs;
+    im->d_Y1 = base + xs + ps;
+    im->d_PUSH = base + xs + ps + y1;
+    int st = run_panel(im, 1, 1, d_x, 1, 0, d_y, 1, 0, s, false);
+    im->d_XS = keep[0]; im->d_PS = keep[1]; im->d_Y1 = keep[2]; im->d_PUSH = keep[3];
+    if (st == H2GPU_OK) im->st.n_matvec += 1;
+    return st;
+}

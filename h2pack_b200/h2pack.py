@@ -86,6 +86,17 @@ class Image:
         _abi.check(st, self.lib, "h2gpu_matmul_device")
         return Y
 
+    def matvec_device_noalloc(self, x, y, stream=None):
+        """y = A x on torch CUDA float64 vectors of length N, with no device allocation
+        (h2gpu_matvec_device_noalloc: work buffers in the library's fixed device array)."""
+        import torch
+        assert x.is_cuda and y.is_cuda and x.dtype == torch.float64 and y.dtype == torch.float64
+        assert x.numel() == self.N and y.numel() == self.N and x.is_contiguous() and y.is_contiguous()
+        s = C.c_void_p(stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream)
+        st = self.lib.h2gpu_matvec_device_noalloc(self.handle, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), s)
+        _abi.check(st, self.lib, "h2gpu_matvec_device_noalloc")
+        return y
+
     def permute(self, x: np.ndarray, forward: bool = True) -> np.ndarray:
         x = np.ascontiguousarray(x, dtype=np.float64)
         y = np.empty_like(x)

@@ -182,6 +182,22 @@ int h2gpu_permute_vector(h2gpu_image *img, int forward, const double *x, double 
 int h2gpu_permute_matrix_rows(h2gpu_image *img, int forward, int layout, int n_vec,
                               const double *X, int ldx, double *PX, int ldp);
 
+/*
+ * y := A x for one device-resident vector (original order) without allocating:
+ * no cudaMalloc, cudaFree or allocating library routine is called.  No counterpart
+ * in the reference.  It is for callers that cannot allocate device memory when they
+ * apply the matrix -- code whose device memory is owned by another allocator (a
+ * framework's caching allocator or a pool reserved up front, where cudaMalloc fails
+ * or fragments memory) and code that must not stall on cudaMalloc / cudaFree, which
+ * synchronize the device.  The image is created beforehand.  Work buffers come from
+ * a fixed 16 MiB device array in the library (held by every GPU that loads it);
+ * images needing more work space for one right-hand side are rejected with
+ * H2GPU_ERR_INVALID.  Calls share that array, so calls that overlap on the GPU race;
+ * the first call on a device looks up the array's address and should come before
+ * any stream capture.  stream: a cudaStream_t or NULL for the image's own stream.
+ */
+int h2gpu_matvec_device_noalloc(h2gpu_image *img, const double *d_x, double *d_y, void *stream);
+
 int h2gpu_get_stats(h2gpu_image *img, h2gpu_stats *st);
 int h2gpu_reset_stats(h2gpu_image *img);
 size_t h2gpu_image_bytes(const h2gpu_image *img);
