@@ -354,13 +354,18 @@ int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
             int n = d->level_nodes[(size_t) L * d->n_leaf_node + j];
             int nr = d->U_nrow[n], nc = d->U_ncol[n];
             if (nr == 0 || nc == 0) continue;
-            UpTask t;
-            t.u_off = u_off[n];
-            t.nrow = nr;
-            t.ncol = nc;
-            t.in_row = d->n_child[n] == 0 ? mc[2 * n] : N + y0r[d->children[n * d->max_child]];
-            t.out_row = N + y0r[n];
-            up.push_back(t);
+            for (int c0 = 0; c0 < nc; c0 += 64)
+            {
+                UpTask t;
+                t.u_off = u_off[n];
+                t.nrow = nr;
+                t.ld = nc;
+                t.c0 = c0;
+                t.nc = std::min(64, nc - c0);
+                t.in_row = d->n_child[n] == 0 ? mc[2 * n] : N + y0r[d->children[n * d->max_child]];
+                t.out_row = N + y0r[n];
+                up.push_back(t);
+            }
         }
     }
     im->up_beg.push_back((int) up.size());

@@ -18,11 +18,13 @@
 
 namespace h2gpu {
 
-// Upward task: XS[out_row + c][v] = sum_r U[r][c] * XS[in_row + r][v]
+// Upward task, one tile of <= 64 columns of a node's U:
+//   XS[out_row + c][v] = sum_r U[r][c] * XS[in_row + r][v],  c0 <= c < c0 + nc
 // (H2P_matvec_fwd_transform, src/H2Pack_matvec.c:126-156)
 struct UpTask {
-    long long u_off;   // element offset of U in the U arena (row-major, ld = ncol)
-    int nrow, ncol;
+    long long u_off;   // element offset of the node's U in the U arena (row-major)
+    int nrow, ld;      // rows of U, row stride (= columns of U)
+    int c0, nc;        // column tile
     int in_row;        // leaf: first row of its x slice; non-leaf: y0 row of its first child
     int out_row;       // y0 row of the node
 };

@@ -105,8 +105,8 @@ __global__ void k_permute(const double* __restrict__ X, long long x_rs, long lon
 
 // ---------------------------------------------------------------- upward
 
-// y0 = U^T w for one node per CTA.  Lanes own columns, warps split the rows,
-// the warps' column partials are summed in shared memory.
+// y0 = U^T w for one column tile of a node per CTA (narrow panels).  Lanes own
+// columns, warps split the rows, the warps' column partials are summed in shared memory.
 template <typename TA, int NV>
 __global__ void __launch_bounds__(kThreads) k_up(const UpTask* __restrict__ tasks, const TA* __restrict__ Uar,
                                                  double* __restrict__ XS)
@@ -118,7 +118,8 @@ __global__ void __launch_bounds__(kThreads) k_up(const UpTask* __restrict__ task
     const UpTask t = tasks[blockIdx.x];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const TA* U = Uar + t.u_off;
-    for (int ct = 0; ct < t.ncol; ct += 32)
+    const int cend = t.c0 + t.nc;
+    for (int ct = t.c0; ct < cend; ct += 32)
     {
         const int c = ct + lane;
         double acc[NV];
@@ -134,20 +135,20 @@ __global__ void __launch_bounds__(kThreads) k_up(const UpTask* __restrict__ task
                 s_w[r * S + v] = XS[(long long) (t.in_row + rc + r) * NV + v];
             }
             __syncthreads();
-            if (c < t.ncol)
+            if (c < cend)
             {
                 int r = w;
                 for (; r + kWarps < nr; r += 2 * kWarps)
                 {
-                    double a0 = to_d(U[(long long) (rc + r) * t.ncol + c]);
-                    double a1 = to_d(U[(long long) (rc + r + kWarps) * t.ncol + c]);
+                    double a0 = to_d(U[(long long) (rc + r) * t.ld + c]);
+                    double a1 = to_d(U[(long long) (rc + r + kWarps) * t.ld + c]);
 #pragma unroll
                     for (int v = 0; v < NV; v++)
                         acc[v] = fma(a1, s_w[(r + kWarps) * S + v], fma(a0, s_w[r * S + v], acc[v]));
                 }
                 if (r < nr)
                 {
-                    double a0 = to_d(U[(long long) (rc + r) * t.ncol + c]);
+                    double a0 = to_d(U[(long long) (rc + r) * t.ld + c]);
 #pragma unroll
                     for (int v = 0; v < NV; v++) acc[v] = fma(a0, s_w[r * S + v], acc[v]);
                 }
@@ -159,7 +160,7 @@ __global__ void __launch_bounds__(kThreads) k_up(const UpTask* __restrict__ task
         for (int i = threadIdx.x; i < 32 * NV; i += kThreads)
         {
             int cc = i / NV, v = i % NV;
-            if (ct + cc < t.ncol)
+            if (ct + cc < cend)
             {
                 double s = 0.0;
 #pragma unroll
@@ -169,6 +170,93 @@ __global__ void __launch_bounds__(kThreads) k_up(const UpTask* __restrict__ task
         }
         __syncthreads();
     }
+}
+
+// Sweep products for panels of NV >= 4 right-hand sides as small tiled GEMMs:
+//   upward   (UP):  C[m][v] = sum_k U[k][c0 + m] * XS[in_row + k][v]      (m < nc, a column tile)
+//   downward (!UP): C[m][v] = sum_k U[r0 + m][k] * (Y1 + PUSH)[k][v]       (m < 64, a row chunk)
+// A 64 x 32 tile of U and a 32 x NV tile of the right-hand sides are staged in shared
+// memory per step (coalesced global reads along the contiguous index); each thread
+// accumulates (NV * 64 / 256) outputs of one row in FP64.
+template <typename TA, int NV, bool UP>
+__global__ void __launch_bounds__(256) k_sweep_gemm(const UpTask* __restrict__ ups, const DownTask* __restrict__ dns,
+                                                    const TA* __restrict__ Uar, double* __restrict__ XS,
+                                                    const double* __restrict__ Y1, double* __restrict__ PS,
+                                                    double* __restrict__ PUSH)
+{
+    constexpr int MT = 64, KT = 32;
+    constexpr int VPT = (NV * MT) / 256;
+    constexpr int NG = NV / VPT;
+    static_assert(VPT >= 1 && NG * VPT == NV, "panel width");
+    __shared__ double sA[KT][MT + 1];
+    __shared__ double sB[KT][NV];
+    const int t = threadIdx.x;
+    const int m = t / NG, v0 = (t % NG) * VPT;
+    int K, M, lda, brow = 0, y1_row = -1, push_row = -1;
+    const TA* A;
+    double* out;
+    if constexpr (UP)
+    {
+        const UpTask T = ups[blockIdx.x];
+        K = T.nrow; M = T.nc; lda = T.ld;
+        A = Uar + T.u_off + T.c0;
+        brow = T.in_row;
+        out = XS + (long long) (T.out_row + T.c0) * NV;
+    } else {
+        const DownTask T = dns[blockIdx.x];
+        K = T.ncol; M = T.nrow; lda = T.ncol;
+        A = Uar + T.u_off;
+        y1_row = T.y1_row; push_row = T.push_row;
+        out = (T.dst_ps ? PS : PUSH) + (long long) T.dst_row * NV;
+    }
+    double acc[VPT];
+#pragma unroll
+    for (int j = 0; j < VPT; j++) acc[j] = 0.0;
+    for (int k0 = 0; k0 < K; k0 += KT)
+    {
+        __syncthreads();
+        if constexpr (UP)
+        {
+            for (int i = t; i < KT * MT; i += 256)
+            {
+                int k = i / MT, mm = i % MT;
+                sA[k][mm] = (k0 + k < K && mm < M) ? to_d(A[(long long) (k0 + k) * lda + mm]) : 0.0;
+            }
+            for (int i = t; i < KT * NV; i += 256)
+            {
+                int k = i / NV, v = i % NV;
+                sB[k][v] = (k0 + k < K) ? XS[(long long) (brow + k0 + k) * NV + v] : 0.0;
+            }
+        } else {
+            for (int i = t; i < KT * MT; i += 256)
+            {
+                int mm = i / KT, k = i % KT;
+                sA[k][mm] = (k0 + k < K && mm < M) ? to_d(A[(long long) mm * lda + k0 + k]) : 0.0;
+            }
+            for (int i = t; i < KT * NV; i += 256)
+            {
+                int k = i / NV, v = i % NV;
+                double b = 0.0;
+                if (k0 + k < K)
+                {
+                    if (y1_row >= 0) b = Y1[(long long) (y1_row + k0 + k) * NV + v];
+                    if (push_row >= 0) b += PUSH[(long long) (push_row + k0 + k) * NV + v];
+                }
+                sB[k][v] = b;
+            }
+        }
+        __syncthreads();
+#pragma unroll 8
+        for (int k = 0; k < KT; k++)
+        {
+            const double a = sA[k][m];
+#pragma unroll
+            for (int j = 0; j < VPT; j++) acc[j] = fma(a, sB[k][v0 + j], acc[j]);
+        }
+    }
+    if (m < M)
+#pragma unroll
+        for (int j = 0; j < VPT; j++) out[(long long) m * NV + v0 + j] = acc[j];
 }
 
 // ------------------------------------------------- row-chunk block apply
@@ -267,6 +355,81 @@ __device__ __forceinline__ void chunk_apply(const TA* __restrict__ A, int R, int
         for (int i = threadIdx.x; i < R * NV; i += kThreads) out0[i] = s_o0[i];
 }
 
+// Stored block chunk for panels of NV >= 4: the R x 32 tile of A staged in shared
+// memory feeds both products, C0 = A V (accumulated over the column tiles in
+// registers) and C1 = A^T W (complete per column tile, written at once).
+template <typename TA, int NV>
+__global__ void __launch_bounds__(256) k_blk_gemm(const BlkTask* __restrict__ tasks, const TA* __restrict__ arena,
+                                                  const double* __restrict__ XS, double* __restrict__ PS)
+{
+    constexpr int RT = 64, CT = 32;
+    constexpr int VPT0 = (NV * RT) / 256;        // C0 outputs per thread
+    constexpr int NG0 = NV / VPT0;
+    constexpr int VPT1 = (NV * CT + 255) / 256;  // C1 outputs per thread
+    constexpr int NG1 = NV / VPT1;
+    __shared__ double sA[RT][CT + 1];
+    __shared__ double sV[CT][NV];
+    __shared__ double sW[RT][NV];
+    const BlkTask T = tasks[blockIdx.x];
+    const TA* A = arena + T.a_off;
+    const int t = threadIdx.x, R = T.nrow, ncol = T.ncol;
+    const bool do0 = T.out0_row >= 0, do1 = T.out1_row >= 0;
+    const int m = t / NG0, v0 = (t % NG0) * VPT0;
+    const int c1 = t / NG1, w0 = (t % NG1) * VPT1;
+    double acc0[VPT0];
+#pragma unroll
+    for (int j = 0; j < VPT0; j++) acc0[j] = 0.0;
+    if (do1)
+        for (int i = t; i < RT * NV; i += 256)
+        {
+            int r = i / NV, v = i % NV;
+            sW[r][v] = (r < R) ? XS[(long long) (T.in1_row + r) * NV + v] : 0.0;
+        }
+    for (int ct = 0; ct < ncol; ct += CT)
+    {
+        __syncthreads();
+        for (int i = t; i < RT * CT; i += 256)
+        {
+            int r = i / CT, c = i % CT;
+            sA[r][c] = (r < R && ct + c < ncol) ? to_d(A[(long long) r * ncol + ct + c]) : 0.0;
+        }
+        if (do0)
+            for (int i = t; i < CT * NV; i += 256)
+            {
+                int c = i / NV, v = i % NV;
+                sV[c][v] = (ct + c < ncol) ? XS[(long long) (T.in0_row + ct + c) * NV + v] : 0.0;
+            }
+        __syncthreads();
+        if (do0)
+        {
+#pragma unroll 8
+            for (int c = 0; c < CT; c++)
+            {
+                const double a = sA[m][c];
+#pragma unroll
+                for (int j = 0; j < VPT0; j++) acc0[j] = fma(a, sV[c][v0 + j], acc0[j]);
+            }
+        }
+        if (do1 && c1 < CT && ct + c1 < ncol)
+        {
+            double acc1[VPT1];
+#pragma unroll
+            for (int j = 0; j < VPT1; j++) acc1[j] = 0.0;
+            for (int r = 0; r < R; r++)
+            {
+                const double a = sA[r][c1];
+#pragma unroll
+                for (int j = 0; j < VPT1; j++) acc1[j] = fma(a, sW[r][w0 + j], acc1[j]);
+            }
+#pragma unroll
+            for (int j = 0; j < VPT1; j++) PS[(long long) (T.out1_row + ct + c1) * NV + w0 + j] = acc1[j];
+        }
+    }
+    if (do0 && m < R)
+#pragma unroll
+        for (int j = 0; j < VPT0; j++) PS[(long long) (T.out0_row + m) * NV + v0 + j] = acc0[j];
+}
+
 template <typename TA, int NV>
 __global__ void __launch_bounds__(kThreads) k_blk(const BlkTask* __restrict__ tasks, const TA* __restrict__ arena,
                                                   const double* __restrict__ XS, double* __restrict__ PS)
@@ -335,10 +498,26 @@ template <> struct Math<double> {
     static __device__ __forceinline__ double exp_(double x) { return exp(x); }
     static __device__ __forceinline__ double div_(double a, double b) { return a / b; }
 };
+// FP32 path: the hardware approximations (MUFU ex2 / rsqrt, flush-to-zero),
+// relative error below 2^-22, written as PTX so no library code is involved.
+__device__ __forceinline__ float ex2_approx(float x)
+{
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float rsqrt_approx(float x)
+{
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+constexpr float kLog2e = 1.4426950408889634f;
+
 template <> struct Math<float> {
-    static __device__ __forceinline__ float rsqrt_(float x) { return rsqrtf(x); }
-    static __device__ __forceinline__ float sqrt_(float x) { return x > 0.f ? x * rsqrtf(x) : 0.f; }
-    static __device__ __forceinline__ float exp_(float x) { return __expf(x); }
+    static __device__ __forceinline__ float rsqrt_(float x) { return rsqrt_approx(x); }
+    static __device__ __forceinline__ float sqrt_(float x) { return x * rsqrt_approx(fmaxf(x, 1e-30f)); }
+    static __device__ __forceinline__ float exp_(float x) { return ex2_approx(x * kLog2e); }
     static __device__ __forceinline__ float div_(float a, float b) { return __fdividef(a, b); }
 };
 
@@ -354,6 +533,15 @@ template <typename T> struct Scalar<KRNL_MATERN32_ID, T> {
     {
         T t = c0 * Math<T>::sqrt_(r2);   // c0 = -sqrt(3) l
         return (T(1) - t) * Math<T>::exp_(t);
+    }
+};
+// (1 - t) e^t = e - t e with e = 2^(t log2 e): 7 instructions, 2 of them MUFU
+template <> struct Scalar<KRNL_MATERN32_ID, float> {
+    static __device__ __forceinline__ float f(float r2, float, float c0)
+    {
+        float t = c0 * (r2 * rsqrt_approx(fmaxf(r2, 1e-30f)));
+        float e = ex2_approx(t * kLog2e);
+        return fmaf(-t, e, e);
     }
 };
 
@@ -400,7 +588,7 @@ template <> struct Vec4<float> { using t = float4; };
 // in FP32 and every tile sum is added to FP64 accumulators, so an FP32 sum never
 // spans more than one tile of sources.  Outputs are written once, no atomics.
 template <int KID, typename T, int NV, int KD, int TPT>
-__global__ void __launch_bounds__(128 / TPT) k_jit(const JitTarget* __restrict__ tgts, const JitSource* __restrict__ srcs,
+__global__ void __launch_bounds__(128 / TPT, 10 * TPT / 2) k_jit(const JitTarget* __restrict__ tgts, const JitSource* __restrict__ srcs,
                                                    const typename Vec4<T>::t* __restrict__ pts, KParam kp, int use_shift,
                                                    const double* __restrict__ XS, double* __restrict__ PS,
                                                    double* __restrict__ Y1)
@@ -408,16 +596,18 @@ __global__ void __launch_bounds__(128 / TPT) k_jit(const JitTarget* __restrict__
     using T4 = typename Vec4<T>::t;
     constexpr int NT = 128 / TPT;
     constexpr int W = KD * NV;
-    constexpr int TILE = (128 * W * (int) sizeof(T) > 32768) ? 64 : 128;
     constexpr bool SPLIT = sizeof(T) < sizeof(double);
+    // FP32: 64-point tiles keep shared memory at ~21 KB so 10 CTAs fit an SM
+    constexpr int TILE = (SPLIT || 128 * W * (int) sizeof(T) > 32768) ? 64 : 128;
     __shared__ T4 s_pt[TILE];
     __shared__ T s_in[TILE * W];
+    // FP64 sums of the FP32 tile sums, one column per thread (conflict-free)
+    __shared__ double s_acc[SPLIT ? TPT * W * NT : 1];
     const JitTarget tg = tgts[blockIdx.x];
     const T p0 = (T) kp.p0, c0 = (T) kp.c0;
 
     T4 xi[TPT];
     bool valid[TPT];
-    double acc64[SPLIT ? TPT : 1][SPLIT ? W : 1];
     T acc[TPT][W];
 #pragma unroll
     for (int q = 0; q < TPT; q++)
@@ -430,7 +620,7 @@ __global__ void __launch_bounds__(128 / TPT) k_jit(const JitTarget* __restrict__
         if constexpr (SPLIT)
         {
 #pragma unroll
-            for (int k = 0; k < W; k++) acc64[q][k] = 0.0;
+            for (int k = 0; k < W; k++) s_acc[(q * W + k) * NT + threadIdx.x] = 0.0;
         }
     }
 
@@ -490,7 +680,11 @@ __global__ void __launch_bounds__(128 / TPT) k_jit(const JitTarget* __restrict__
 #pragma unroll
                 for (int q = 0; q < TPT; q++)
 #pragma unroll
-                    for (int k = 0; k < W; k++) { acc64[q][k] += (double) acc[q][k]; acc[q][k] = T(0); }
+                    for (int k = 0; k < W; k++)
+                    {
+                        s_acc[(q * W + k) * NT + threadIdx.x] += (double) acc[q][k];
+                        acc[q][k] = T(0);
+                    }
             }
         }
     }
@@ -503,7 +697,7 @@ __global__ void __launch_bounds__(128 / TPT) k_jit(const JitTarget* __restrict__
 #pragma unroll
         for (int k = 0; k < W; k++)
         {
-            if constexpr (SPLIT) o[k] = acc64[q][k];
+            if constexpr (SPLIT) o[k] = s_acc[(q * W + k) * NT + threadIdx.x];
             else o[k] = (double) acc[q][k];
         }
     }
@@ -591,7 +785,12 @@ template <typename TA>
 cudaError_t launch_up(int NV, const UpTask* t, int n, const TA* U, double* XS, cudaStream_t st)
 {
     if (n <= 0) return cudaSuccess;
-    NV_DISPATCH(NV, k_up<TA, NVc><<<n, kThreads, 0, st>>>(t, U, XS));
+    NV_DISPATCH(NV, {
+        if constexpr (NVc >= 4)
+            k_sweep_gemm<TA, NVc, true><<<n, 256, 0, st>>>(t, nullptr, U, XS, nullptr, nullptr, nullptr);
+        else
+            k_up<TA, NVc><<<n, kThreads, 0, st>>>(t, U, XS);
+    });
     return cudaGetLastError();
 }
 
@@ -607,10 +806,15 @@ cudaError_t launch_blk(int NV, const BlkTask* t, int n, const TA* arena, const d
 {
     if (n <= 0) return cudaSuccess;
     NV_DISPATCH(NV, {
-        constexpr int b = chunk_smem_bytes<NVc>();
-        cudaError_t e = allow_smem(k_blk<TA, NVc>, b);
-        if (e != cudaSuccess) return e;
-        k_blk<TA, NVc><<<n, kThreads, b, st>>>(t, arena, XS, PS);
+        if constexpr (NVc >= 4)
+        {
+            k_blk_gemm<TA, NVc><<<n, 256, 0, st>>>(t, arena, XS, PS);
+        } else {
+            constexpr int b = chunk_smem_bytes<NVc>();
+            cudaError_t e = allow_smem(k_blk<TA, NVc>, b);
+            if (e != cudaSuccess) return e;
+            k_blk<TA, NVc><<<n, kThreads, b, st>>>(t, arena, XS, PS);
+        }
     });
     return cudaGetLastError();
 }
@@ -621,10 +825,15 @@ cudaError_t launch_down(int NV, const DownTask* t, int n, const TA* U, const dou
 {
     if (n <= 0) return cudaSuccess;
     NV_DISPATCH(NV, {
-        constexpr int b = chunk_smem_bytes<NVc>();
-        cudaError_t e = allow_smem(k_down<TA, NVc>, b);
-        if (e != cudaSuccess) return e;
-        k_down<TA, NVc><<<n, kThreads, b, st>>>(t, U, Y1, PS, PUSH);
+        if constexpr (NVc >= 4)
+        {
+            k_sweep_gemm<TA, NVc, false><<<n, 256, 0, st>>>(nullptr, t, U, nullptr, Y1, PS, PUSH);
+        } else {
+            constexpr int b = chunk_smem_bytes<NVc>();
+            cudaError_t e = allow_smem(k_down<TA, NVc>, b);
+            if (e != cudaSuccess) return e;
+            k_down<TA, NVc><<<n, kThreads, b, st>>>(t, U, Y1, PS, PUSH);
+        }
     });
     return cudaGetLastError();
 }
@@ -652,7 +861,9 @@ static cudaError_t launch_jit_k(int NV, const JitTarget* tg, int n, const JitSou
     const T4* p = (const T4*) pts;
     // two targets per thread (64 threads per 128-point chunk) where the accumulators allow it
     NV_DISPATCH(NV, {
-        if constexpr (KD * NVc <= 16)
+        if constexpr (KD == 3 && NVc > 8)
+            return cudaErrorInvalidValue;   // tensor kernels run in panels of <= 8 right-hand sides
+        else if constexpr (KD * NVc <= 16)
             k_jit<KID, T, NVc, KD, 2><<<n, 64, 0, st>>>(tg, sr, p, kp, use_shift, XS, PS, Y1);
         else
             k_jit<KID, T, NVc, KD, 1><<<n, 128, 0, st>>>(tg, sr, p, kp, use_shift, XS, PS, Y1);
