@@ -553,6 +553,23 @@ int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
         }
     }
 
+    // ---- JIT targets, largest work first (shorter tail of the launch)
+    auto by_work = [&](std::vector<JitTarget>& v) {
+        std::vector<std::pair<double, int>> w(v.size());
+        for (size_t i = 0; i < v.size(); i++)
+        {
+            double srcpts = 0;
+            for (int k = v[i].src_beg; k < v[i].src_end; k++) srcpts += js[k].npt;
+            w[i] = {-(double) v[i].npt * srcpts, (int) i};
+        }
+        std::stable_sort(w.begin(), w.end());
+        std::vector<JitTarget> out(v.size());
+        for (size_t i = 0; i < v.size(); i++) out[i] = v[w[i].second];
+        v.swap(out);
+    };
+    by_work(jtN);
+    by_work(jtF);
+
     // ---- y1 sums (AOT)
     std::vector<Y1Task>& y1t = hp.y1t;
     std::vector<int>& y1_slots = hp.y1_slots;

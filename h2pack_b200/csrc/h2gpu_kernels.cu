@@ -588,7 +588,7 @@ template <> struct Vec4<float> { using t = float4; };
 // in FP32 and every tile sum is added to FP64 accumulators, so an FP32 sum never
 // spans more than one tile of sources.  Outputs are written once, no atomics.
 template <int KID, typename T, int NV, int KD, int TPT>
-__global__ void __launch_bounds__(128 / TPT, 10 * TPT / 2) k_jit(const JitTarget* __restrict__ tgts, const JitSource* __restrict__ srcs,
+__global__ void __launch_bounds__(128 / TPT, sizeof(T) == 4 ? 5 * TPT : 1) k_jit(const JitTarget* __restrict__ tgts, const JitSource* __restrict__ srcs,
                                                    const typename Vec4<T>::t* __restrict__ pts, KParam kp, int use_shift,
                                                    const double* __restrict__ XS, double* __restrict__ PS,
                                                    double* __restrict__ Y1)
@@ -701,6 +701,126 @@ __global__ void __launch_bounds__(128 / TPT, 10 * TPT / 2) k_jit(const JitTarget
             else o[k] = (double) acc[q][k];
         }
     }
+}
+
+// ------------------------------------------------ JIT owner kernel, tensor cores
+
+// TF32 pieces of an FP32 value: hi = rna(x), lo = rna(x - hi); hi*b + lo*b recovers
+// ~22 bits, the 3xTF32 split (hi*hi + hi*lo + lo*hi) keeps products at ~2^-21.
+__device__ __forceinline__ uint32_t tf32_rna(float x)
+{
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
+}
+
+__device__ __forceinline__ void mma_tf32(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                         uint32_t b0, uint32_t b1)
+{
+    asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+                 : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+                 : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// Same work split as k_jit (one CTA per 128-target chunk, owner computes), with the
+// right-hand-side products on the tensor cores.  Warp w owns targets 16w..16w+15.
+// Per group of 8 staged sources each lane evaluates the 4 kernel values of its
+// m16n8k8 A fragment (targets g, g+8 x sources t, t+4; g = lane/4, t = lane%4),
+// splits them into TF32 hi/lo and issues 3 MMAs per 8-RHS n-tile against the
+// sources' inputs, which are staged in shared memory already split and in B-fragment
+// order.  FP32 accumulation per 64-source tile, FP64 sums across tiles.
+template <int KID, int NV>
+__global__ void __launch_bounds__(256, 2) k_jit_tc(const JitTarget* __restrict__ tgts, const JitSource* __restrict__ srcs,
+                                                   const float4* __restrict__ pts, KParam kp,
+                                                   const double* __restrict__ XS, double* __restrict__ PS,
+                                                   double* __restrict__ Y1)
+{
+    constexpr int NT = NV / 8;    // n-tiles of 8 right-hand sides
+    constexpr int TS = 64;        // sources per shared-memory tile
+    constexpr int NG = TS / 8;    // groups of 8 sources per tile
+    __shared__ float4 s_pt[TS];
+    __shared__ uint4 s_b[NG][NT][32];
+    __shared__ double s_acc[8][NT * 4][32];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, tq = lane & 3;
+    const JitTarget tg = tgts[blockIdx.x];
+    const float p0 = (float) kp.p0, c0 = (float) kp.c0;
+    const int i0 = warp * 16 + g, i1 = i0 + 8;
+    const bool v0 = i0 < tg.npt, v1 = i1 < tg.npt;
+    const float4 x0 = pts[tg.pt0 + (v0 ? i0 : 0)], x1 = pts[tg.pt0 + (v1 ? i1 : 0)];
+    float acc[NT][4];
+#pragma unroll
+    for (int n = 0; n < NT; n++)
+#pragma unroll
+        for (int q = 0; q < 4; q++) { acc[n][q] = 0.f; s_acc[warp][n * 4 + q][lane] = 0.0; }
+
+    for (int s = tg.src_beg; s < tg.src_end; s++)
+    {
+        const JitSource sc = srcs[s];
+        const float ax = x0.x + sc.sx, ay = x0.y + sc.sy, az = x0.z + sc.sz;
+        const float bx = x1.x + sc.sx, by = x1.y + sc.sy, bz = x1.z + sc.sz;
+        for (int j0 = 0; j0 < sc.npt; j0 += TS)
+        {
+            const int nj = min(TS, sc.npt - j0);
+            __syncthreads();
+            for (int j = threadIdx.x; j < TS; j += 256)
+                s_pt[j] = (j < nj) ? pts[sc.pt0 + j0 + j] : make_float4(1e6f, 1e6f, 1e6f, 0.f);
+            for (int e = threadIdx.x; e < NG * NT * 32; e += 256)
+            {
+                const int ln = e & 31, n = (e >> 5) % NT, grp = e / (32 * NT);
+                const int sa = grp * 8 + (ln & 3), sb = sa + 4, r = n * 8 + (ln >> 2);
+                const float xa = (sa < nj) ? (float) XS[(long long) (sc.in_row + j0 + sa) * NV + r] : 0.f;
+                const float xb = (sb < nj) ? (float) XS[(long long) (sc.in_row + j0 + sb) * NV + r] : 0.f;
+                const uint32_t ha = tf32_rna(xa), hb = tf32_rna(xb);
+                s_b[grp][n][ln] = make_uint4(ha, hb, tf32_rna(xa - __uint_as_float(ha)), tf32_rna(xb - __uint_as_float(hb)));
+            }
+            __syncthreads();
+            const int ngrp = (nj + 7) >> 3;
+            for (int grp = 0; grp < ngrp; grp++)
+            {
+                const float4 pa = s_pt[grp * 8 + tq], pb = s_pt[grp * 8 + tq + 4];
+                float k[4];
+                {
+                    float dx = ax - pa.x, dy = ay - pa.y, dz = az - pa.z;
+                    k[0] = Scalar<KID, float>::f(dx * dx + dy * dy + dz * dz, p0, c0);   // (g,   t)
+                    dx = bx - pa.x; dy = by - pa.y; dz = bz - pa.z;
+                    k[1] = Scalar<KID, float>::f(dx * dx + dy * dy + dz * dz, p0, c0);   // (g+8, t)
+                    dx = ax - pb.x; dy = ay - pb.y; dz = az - pb.z;
+                    k[2] = Scalar<KID, float>::f(dx * dx + dy * dy + dz * dz, p0, c0);   // (g,   t+4)
+                    dx = bx - pb.x; dy = by - pb.y; dz = bz - pb.z;
+                    k[3] = Scalar<KID, float>::f(dx * dx + dy * dy + dz * dz, p0, c0);   // (g+8, t+4)
+                }
+                uint32_t hi[4], lo[4];
+#pragma unroll
+                for (int q = 0; q < 4; q++)
+                {
+                    hi[q] = tf32_rna(k[q]);
+                    lo[q] = tf32_rna(k[q] - __uint_as_float(hi[q]));
+                }
+#pragma unroll
+                for (int n = 0; n < NT; n++)
+                {
+                    const uint4 b = s_b[grp][n][lane];
+                    mma_tf32(acc[n], lo[0], lo[1], lo[2], lo[3], b.x, b.y);
+                    mma_tf32(acc[n], hi[0], hi[1], hi[2], hi[3], b.z, b.w);
+                    mma_tf32(acc[n], hi[0], hi[1], hi[2], hi[3], b.x, b.y);
+                }
+            }
+#pragma unroll
+            for (int n = 0; n < NT; n++)
+#pragma unroll
+                for (int q = 0; q < 4; q++) { s_acc[warp][n * 4 + q][lane] += (double) acc[n][q]; acc[n][q] = 0.f; }
+        }
+    }
+    double* base = (tg.out_y1 ? Y1 : PS) + (long long) tg.out_row * NV;
+#pragma unroll
+    for (int n = 0; n < NT; n++)
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+        {
+            const int row = (q < 2) ? i0 : i1;
+            const bool ok = (q < 2) ? v0 : v1;
+            if (ok) base[(long long) row * NV + n * 8 + 2 * tq + (q & 1)] = s_acc[warp][n * 4 + q][lane];
+        }
 }
 
 // --------------------------------------------------------------- direct sum
@@ -859,6 +979,20 @@ static cudaError_t launch_jit_k(int NV, const JitTarget* tg, int n, const JitSou
 {
     using T4 = typename Vec4<T>::t;
     const T4* p = (const T4*) pts;
+    // FP32 scalar kernels on panels of 8 or 16: right-hand-side products on the tensor cores
+    if constexpr (KD == 1 && sizeof(T) == 4)
+    {
+        if (NV == 16 && use_shift)
+        {
+            k_jit_tc<KID, 16><<<n, 256, 0, st>>>(tg, sr, (const float4*) pts, kp, XS, PS, Y1);
+            return cudaGetLastError();
+        }
+        if (NV == 8 && use_shift)
+        {
+            k_jit_tc<KID, 8><<<n, 256, 0, st>>>(tg, sr, (const float4*) pts, kp, XS, PS, Y1);
+            return cudaGetLastError();
+        }
+    }
     // two targets per thread (64 threads per 128-point chunk) where the accumulators allow it
     NV_DISPATCH(NV, {
         if constexpr (KD == 3 && NVc > 8)

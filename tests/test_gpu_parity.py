@@ -81,9 +81,10 @@ def test_deterministic(h2):
     assert np.array_equal(h2.matmul(X), h2.matmul(X))
 
 
-def test_mixed_precision_close(h2):
+@pytest.mark.parametrize("nv", [8, 16])
+def test_mixed_precision_close(h2, nv):
     rng = np.random.default_rng(4)
-    X = rng.standard_normal((h2.N, 16))
+    X = rng.standard_normal((h2.N, nv))
     Y64 = h2.matmul(X)
     h2.set_precision("mixed")
     try:
