@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include "h2gpu_internal.cuh"
 #include "h2gpu_launch.h"
 
@@ -709,9 +710,9 @@ __global__ void __launch_bounds__(128 / TPT, sizeof(T) == 4 ? 5 * TPT : 1) k_jit
 // ~22 bits, the 3xTF32 split (hi*hi + hi*lo + lo*hi) keeps products at ~2^-21.
 __device__ __forceinline__ uint32_t tf32_rna(float x)
 {
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-    return r;
+    // round to nearest (ties away from zero) at 10 mantissa bits with two integer ops;
+    // finite inputs far below FLT_MAX only, which holds for kernel values and inputs here
+    return (__float_as_uint(x) + 0x1000u) & 0xffffe000u;
 }
 
 __device__ __forceinline__ void mma_tf32(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
@@ -730,7 +731,7 @@ __device__ __forceinline__ void mma_tf32(float (&d)[4], uint32_t a0, uint32_t a1
 // sources' inputs, which are staged in shared memory already split and in B-fragment
 // order.  FP32 accumulation per 64-source tile, FP64 sums across tiles.
 template <int KID, int NV>
-__global__ void __launch_bounds__(256, 2) k_jit_tc(const JitTarget* __restrict__ tgts, const JitSource* __restrict__ srcs,
+__global__ void __launch_bounds__(256, 4) k_jit_tc(const JitTarget* __restrict__ tgts, const JitSource* __restrict__ srcs,
                                                    const float4* __restrict__ pts, KParam kp,
                                                    const double* __restrict__ XS, double* __restrict__ PS,
                                                    double* __restrict__ Y1)
@@ -979,15 +980,20 @@ static cudaError_t launch_jit_k(int NV, const JitTarget* tg, int n, const JitSou
 {
     using T4 = typename Vec4<T>::t;
     const T4* p = (const T4*) pts;
-    // FP32 scalar kernels on panels of 8 or 16: right-hand-side products on the tensor cores
+    // FP32 scalar kernels on panels of 8 or 16: right-hand-side products on the tensor
+    // cores (H2G_JIT_TC=0 selects the CUDA-core kernel instead)
+    static const bool use_tc = [] {
+        const char* e = getenv("H2G_JIT_TC");
+        return !(e && e[0] == '0');
+    }();
     if constexpr (KD == 1 && sizeof(T) == 4)
     {
-        if (NV == 16 && use_shift)
+        if (use_tc && NV == 16 && use_shift)
         {
             k_jit_tc<KID, 16><<<n, 256, 0, st>>>(tg, sr, (const float4*) pts, kp, XS, PS, Y1);
             return cudaGetLastError();
         }
-        if (NV == 8 && use_shift)
+        if (use_tc && NV == 8 && use_shift)
         {
             k_jit_tc<KID, 8><<<n, 256, 0, st>>>(tg, sr, (const float4*) pts, kp, XS, PS, Y1);
             return cudaGetLastError();
