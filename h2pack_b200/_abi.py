@@ -78,6 +78,11 @@ H2GPU_SYMBOLS = {
     "h2gpu_permute_vector": (C.c_int, [C.c_void_p, C.c_int, _dp, _dp]),
     "h2gpu_permute_matrix_rows": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, _dp, C.c_int, _dp, C.c_int]),
     "h2gpu_matvec_device_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "h2gpu_batch_create": (C.c_int, [C.POINTER(Desc), C.c_int, C.POINTER(Options), C.POINTER(C.c_void_p)]),
+    "h2gpu_graph_capture": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int]),
+    "h2gpu_graph_launch": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "h2gpu_autotune": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int,
+                                 C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "h2gpu_get_stats": (C.c_int, [C.c_void_p, C.POINTER(Stats)]),
     "h2gpu_reset_stats": (C.c_int, [C.c_void_p]),
     "h2gpu_image_bytes": (C.c_size_t, [C.c_void_p]),

@@ -146,6 +146,13 @@ struct h2gpu_image {
     size_t work_bytes = 0;   // work buffers
     h2gpu_stats st{};
     Ev ev;
+
+    // tuning (h2gpu_autotune) and captured graph (h2gpu_graph_capture)
+    int jit_tc = 1;          // tensor-core JIT kernel for FP32 panels of 8 / 16
+    int tuned_nv = 0;        // panel width chosen by the autotuner (0: default rule)
+    int n_images = 1;        // matrices in this image (batched images hold several)
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
 };
 
 namespace {
@@ -160,6 +167,8 @@ void free_all(h2gpu_image* im)
         if (p) cudaFree(p);
     for (auto& e : im->ev.e)
         if (e) cudaEventDestroy(e);
+    if (im->graph_exec) cudaGraphExecDestroy(im->graph_exec);
+    if (im->graph) cudaGraphDestroy(im->graph);
     if (im->stream) cudaStreamDestroy(im->stream);
 }
 
@@ -789,7 +798,7 @@ int run_panel(h2gpu_image* im, int NV, int nv, const double* X, long long x_rs, 
         else CK(launch_blk<double>(NV, im->d_blkD, im->n_blkD, im->d_D64, im->d_XS, im->d_PS, s));
     } else {
         CK(launch_jit(im->kernel_id, f32, NV, im->d_jtN, im->n_jtN, im->d_js, f32 ? (const void*) im->d_pts32 : (const void*) im->d_pts64,
-                      kparam_of(im), f32 ? 1 : 0, im->d_XS, im->d_PS, im->d_Y1, s));
+                      kparam_of(im), f32 ? 1 : 0, im->jit_tc, im->d_XS, im->d_PS, im->d_Y1, s));
     }
     if (timed) CK(cudaEventRecord(e[2], s));
     for (size_t L = 0; L + 1 < im->up_beg.size(); L++)
@@ -806,7 +815,7 @@ int run_panel(h2gpu_image* im, int NV, int nv, const double* X, long long x_rs, 
         CK(launch_y1sum(NV, im->d_y1t, im->n_y1, im->d_y1_slots, im->d_PS, im->d_Y1, s));
     } else {
         CK(launch_jit(im->kernel_id, f32, NV, im->d_jtF, im->n_jtF, im->d_js, f32 ? (const void*) im->d_pts32 : (const void*) im->d_pts64,
-                      kparam_of(im), f32 ? 1 : 0, im->d_XS, im->d_PS, im->d_Y1, s));
+                      kparam_of(im), f32 ? 1 : 0, im->jit_tc, im->d_XS, im->d_PS, im->d_Y1, s));
     }
     if (timed) CK(cudaEventRecord(e[4], s));
     for (size_t L = 0; L + 1 < im->dn_beg.size(); L++)
@@ -841,6 +850,7 @@ int apply_device(h2gpu_image* im, int n_vec, const double* X, long long x_rs, lo
 {
     // JIT tensor kernels keep 3 x NV accumulators per target: panels of at most 8 there
     int NV = panel_width(n_vec, (im->BD_JIT && im->kd == 3) ? std::min(im->max_nv, 8) : im->max_nv);
+    if (im->tuned_nv > 0) NV = std::min(NV, im->tuned_nv);
     TRY(prepare(im, NV));
     float ph[5] = {0, 0, 0, 0, 0};
     for (int c0 = 0; c0 < n_vec; c0 += NV)
@@ -898,6 +908,10 @@ H2G_API int h2gpu_image_create(const h2gpu_desc* desc, const h2gpu_options* opt,
     if (opt) o = *opt;
     REQ(o.precision == H2GPU_PREC_FP64 || o.precision == H2GPU_PREC_MIXED, "unknown precision %d", o.precision);
     h2gpu_image* im = new h2gpu_image();
+    {
+        const char* e = getenv("H2G_JIT_TC");
+        im->jit_tc = !(e && e[0] == '0');
+    }
     HostPlan hp;
     int pst = build_plan(im, desc, hp);   // all structural checks happen here, before any CUDA call
     if (pst != H2GPU_OK) { delete im; return pst; }
@@ -1192,4 +1206,244 @@ H2G_API int h2gpu_matvec_device_noalloc(h2gpu_image* im, const double* d_x, doub
     im->d_XS = keep[0]; im->d_PS = keep[1]; im->d_Y1 = keep[2]; im->d_PUSH = keep[3];
     if (st == H2GPU_OK) im->st.n_matvec += 1;
     return st;
+}
+
+// ============================================================ batched images
+//
+// A batch of independent H2 representations (same kernel, precision and mode) is
+// applied as one: their descriptors are merged into one forest -- node, point and
+// block indices offset, per-level node lists concatenated, B/D blocks re-packed
+// diagonal blocks first -- so every phase is one launch per tree level over all
+// matrices of the batch (flattened cross-matrix work lists).  The caller stacks the
+// matrices' vectors in batch order.
+
+namespace {
+
+struct MergedDesc {
+    h2gpu_desc d{};
+    std::vector<int> n_child, children, node_level, pt_cluster, mat_cluster, level_n_node, level_nodes, leaf_nodes,
+        U_nrow, U_ncol, U_ld, r_adm, r_inadm, B_nrow, B_ncol, D_nrow, D_ncol, J_n, fwd, bwd;
+    std::vector<size_t> B_ptr, D_ptr;
+    std::vector<double> B_data, D_data, coord;
+    std::vector<const double*> U, J;
+};
+
+int merge_descs(const h2gpu_desc* ds, int n, MergedDesc& m)
+{
+    REQ(ds && n >= 1, "empty batch");
+    const h2gpu_desc& a = ds[0];
+    int n_point = 0, n_node = 0, n_leaf = 0, max_level = 0, min_adm = 1 << 30, nadm = 0, ninadm = 0;
+    for (int i = 0; i < n; i++)
+    {
+        TRY(validate(&ds[i]));
+        const h2gpu_desc& d = ds[i];
+        REQ(d.krnl_dim == a.krnl_dim && d.xpt_dim == a.xpt_dim && d.BD_JIT == a.BD_JIT && d.kernel_id == a.kernel_id &&
+                d.n_krnl_param == a.n_krnl_param,
+            "batch member %d differs in kernel, dimension or mode", i);
+        for (int k = 0; k < d.n_krnl_param; k++) REQ(d.krnl_param[k] == a.krnl_param[k], "batch member %d: kernel parameter differs", i);
+        n_point += d.n_point; n_node += d.n_node; n_leaf += d.n_leaf_node;
+        max_level = std::max(max_level, d.max_level);
+        min_adm = std::min(min_adm, d.min_adm_level);
+        nadm += d.n_r_adm_pair; ninadm += d.n_r_inadm_pair;
+    }
+    const int kd = a.krnl_dim, L = max_level + 1;
+    REQ((long long) kd * n_point < (1LL << 30), "batch too large for 32-bit row indices");
+    m.level_n_node.assign(L, 0);
+    m.level_nodes.assign((size_t) L * n_leaf, 0);
+    std::vector<int> lfill(L, 0);
+    int no = 0, po = 0;
+    size_t bo = 0;
+    // first pass: node-indexed arrays, pairs, coordinates
+    m.coord.assign((size_t) a.xpt_dim * n_point, 0.0);
+    for (int i = 0; i < n; i++)
+    {
+        const h2gpu_desc& d = ds[i];
+        for (int v = 0; v < d.n_node; v++)
+        {
+            m.n_child.push_back(d.n_child[v]);
+            for (int k = 0; k < d.max_child; k++)
+                m.children.push_back(k < d.n_child[v] ? d.children[v * d.max_child + k] + no : -1);
+            m.node_level.push_back(d.node_level[v]);
+            m.pt_cluster.push_back(d.pt_cluster[2 * v] + po);
+            m.pt_cluster.push_back(d.pt_cluster[2 * v + 1] + po);
+            m.mat_cluster.push_back(d.mat_cluster[2 * v] + kd * po);
+            m.mat_cluster.push_back(d.mat_cluster[2 * v + 1] + kd * po);
+            m.U_nrow.push_back(d.U_nrow[v]); m.U_ncol.push_back(d.U_ncol[v]); m.U_ld.push_back(d.U_ld[v]);
+            m.U.push_back(d.U[v]);
+            m.J_n.push_back(d.J_n ? d.J_n[v] : 0);
+            m.J.push_back(d.J_coord ? d.J_coord[v] : nullptr);
+        }
+        for (int l = 0; l <= d.max_level; l++)
+            for (int j = 0; j < d.level_n_node[l]; j++)
+                m.level_nodes[(size_t) l * n_leaf + lfill[l]++] = d.level_nodes[(size_t) l * d.n_leaf_node + j] + no;
+        for (int j = 0; j < d.n_leaf_node; j++) m.leaf_nodes.push_back(d.leaf_nodes[j] + no);
+        for (int j = 0; j < 2 * d.n_r_adm_pair; j++) m.r_adm.push_back(d.r_adm_pairs[j] + no);
+        for (int j = 0; j < 2 * d.n_r_inadm_pair; j++) m.r_inadm.push_back(d.r_inadm_pairs[j] + no);
+        if (d.coord)
+            for (int k = 0; k < a.xpt_dim; k++)
+                memcpy(&m.coord[(size_t) k * n_point + po], d.coord + (size_t) k * d.n_point, 8 * (size_t) d.n_point);
+        for (int j = 0; j < kd * d.n_point; j++)
+        {
+            m.fwd.push_back(d.fwd_pmt_idx[j] + kd * po);
+            m.bwd.push_back(d.bwd_pmt_idx[j] + kd * po);
+        }
+        no += d.n_node; po += d.n_point;
+    }
+    for (int l = 0; l < L; l++) m.level_n_node[l] = lfill[l];
+    // B / D blocks: B in member order; D diagonal blocks of all members first, then the others
+    if (!a.BD_JIT)
+    {
+        m.B_ptr.push_back(0);
+        for (int i = 0; i < n; i++)
+        {
+            const h2gpu_desc& d = ds[i];
+            for (int j = 0; j < d.n_B; j++)
+            {
+                m.B_nrow.push_back(d.B_nrow[j]); m.B_ncol.push_back(d.B_ncol[j]);
+                size_t sz = d.B_ptr[j + 1] - d.B_ptr[j];
+                m.B_data.insert(m.B_data.end(), d.B_data + d.B_ptr[j], d.B_data + d.B_ptr[j] + sz);
+                bo += sz;
+                m.B_ptr.push_back(bo);
+            }
+        }
+        m.D_ptr.push_back(0);
+        size_t dofs = 0;
+        for (int pass = 0; pass < 2; pass++)
+            for (int i = 0; i < n; i++)
+            {
+                const h2gpu_desc& d = ds[i];
+                int j0 = pass == 0 ? 0 : d.n_leaf_node, j1 = pass == 0 ? d.n_leaf_node : d.n_D;
+                for (int j = j0; j < j1; j++)
+                {
+                    m.D_nrow.push_back(d.D_nrow[j]); m.D_ncol.push_back(d.D_ncol[j]);
+                    size_t sz = d.D_ptr[j + 1] - d.D_ptr[j];
+                    m.D_data.insert(m.D_data.end(), d.D_data + d.D_ptr[j], d.D_data + d.D_ptr[j] + sz);
+                    dofs += sz;
+                    m.D_ptr.push_back(dofs);
+                }
+            }
+    } else {
+        m.B_ptr.assign(1, 0);
+        m.D_ptr.assign(1, 0);
+    }
+    h2gpu_desc& d = m.d;
+    d.n_point = n_point; d.pt_dim = a.pt_dim; d.xpt_dim = a.xpt_dim; d.krnl_dim = kd;
+    d.n_node = n_node; d.n_leaf_node = n_leaf; d.max_child = a.max_child; d.max_level = max_level;
+    d.min_adm_level = min_adm; d.BD_JIT = a.BD_JIT;
+    d.n_child = m.n_child.data(); d.children = m.children.data(); d.node_level = m.node_level.data();
+    d.pt_cluster = m.pt_cluster.data(); d.mat_cluster = m.mat_cluster.data();
+    d.level_n_node = m.level_n_node.data(); d.level_nodes = m.level_nodes.data(); d.leaf_nodes = m.leaf_nodes.data();
+    d.U_nrow = m.U_nrow.data(); d.U_ncol = m.U_ncol.data(); d.U_ld = m.U_ld.data(); d.U = m.U.data();
+    d.n_r_adm_pair = nadm; d.r_adm_pairs = m.r_adm.data();
+    d.n_r_inadm_pair = ninadm; d.r_inadm_pairs = m.r_inadm.data();
+    d.n_B = a.BD_JIT ? nadm : (int) m.B_nrow.size();
+    d.B_nrow = m.B_nrow.data(); d.B_ncol = m.B_ncol.data(); d.B_ptr = m.B_ptr.data();
+    d.B_data = m.B_data.empty() ? nullptr : m.B_data.data();
+    d.n_D = n_leaf + ninadm;
+    d.D_nrow = m.D_nrow.data(); d.D_ncol = m.D_ncol.data(); d.D_ptr = m.D_ptr.data();
+    d.D_data = m.D_data.empty() ? nullptr : m.D_data.data();
+    d.coord = m.coord.data(); d.J_n = m.J_n.data(); d.J_coord = m.J.data();
+    d.fwd_pmt_idx = m.fwd.data(); d.bwd_pmt_idx = m.bwd.data();
+    d.kernel_id = a.kernel_id; d.n_krnl_param = a.n_krnl_param;
+    for (int k = 0; k < 4; k++) d.krnl_param[k] = a.krnl_param[k];
+    return H2GPU_OK;
+}
+
+}  // namespace
+
+H2G_API int h2gpu_batch_create(const h2gpu_desc* descs, int n_desc, const h2gpu_options* opt, h2gpu_image** out)
+{
+    if (!out) return fail(H2GPU_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    MergedDesc m;
+    TRY(merge_descs(descs, n_desc, m));
+    TRY(h2gpu_image_create(&m.d, opt, out));
+    (*out)->n_images = n_desc;
+    return H2GPU_OK;
+}
+
+// ================================================================ CUDA graph
+
+H2G_API int h2gpu_graph_capture(h2gpu_image* im, int n_vec, const double* dX, int ldx, double* dY, int ldy)
+{
+    if (!im) return fail(H2GPU_ERR_INVALID, "image is NULL");
+    REQ(n_vec >= 1 && ldx >= n_vec && ldy >= n_vec && dX && dY, "bad graph_capture arguments");
+    std::lock_guard<std::mutex> lk(im->mu);
+    int NV = panel_width(n_vec, (im->BD_JIT && im->kd == 3) ? std::min(im->max_nv, 8) : im->max_nv);
+    if (im->tuned_nv > 0) NV = std::min(NV, im->tuned_nv);
+    TRY(prepare(im, NV));
+    if (im->graph_exec) { cudaGraphExecDestroy(im->graph_exec); im->graph_exec = nullptr; }
+    if (im->graph) { cudaGraphDestroy(im->graph); im->graph = nullptr; }
+    cudaStream_t s = im->stream;
+    // one eager pass first so that every kernel attribute is set outside the capture
+    for (int c0 = 0; c0 < n_vec; c0 += NV)
+        TRY(run_panel(im, NV, std::min(NV, n_vec - c0), dX + c0, ldx, 1, dY + c0, ldy, 1, s, false));
+    CK(cudaStreamSynchronize(s));
+    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    int st = H2GPU_OK;
+    for (int c0 = 0; c0 < n_vec && st == H2GPU_OK; c0 += NV)
+        st = run_panel(im, NV, std::min(NV, n_vec - c0), dX + c0, ldx, 1, dY + c0, ldy, 1, s, false);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s, &g);
+    if (st != H2GPU_OK) { if (g) cudaGraphDestroy(g); return st; }
+    if (e != cudaSuccess) return fail(H2GPU_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&im->graph_exec, g, 0);
+    if (e != cudaSuccess) { cudaGraphDestroy(g); return fail(H2GPU_ERR_CUDA, "graph instantiation failed: %s", cudaGetErrorString(e)); }
+    im->graph = g;
+    im->st.n_matvec += 0;
+    return H2GPU_OK;
+}
+
+H2G_API int h2gpu_graph_launch(h2gpu_image* im, void* stream)
+{
+    if (!im) return fail(H2GPU_ERR_INVALID, "image is NULL");
+    std::lock_guard<std::mutex> lk(im->mu);
+    if (!im->graph_exec) return fail(H2GPU_ERR_STATE, "no graph captured (call h2gpu_graph_capture first)");
+    CK(cudaGraphLaunch(im->graph_exec, stream ? (cudaStream_t) stream : im->stream));
+    return H2GPU_OK;
+}
+
+// ================================================================= autotuner
+//
+// Times the apply of n_vec device-resident right-hand sides under each candidate
+// (panel width among 4, 8, 16 not above n_vec's panel; for FP32 JIT images the
+// tensor-core and the CUDA-core kernels) and keeps the fastest for this image.
+
+H2G_API int h2gpu_autotune(h2gpu_image* im, int n_vec, const double* dX, int ldx, double* dY, int ldy, int* best_nv,
+                           int* best_tc)
+{
+    if (!im) return fail(H2GPU_ERR_INVALID, "image is NULL");
+    REQ(n_vec >= 1 && ldx >= n_vec && ldy >= n_vec && dX && dY, "bad autotune arguments");
+    std::lock_guard<std::mutex> lk(im->mu);
+    const int full = panel_width(n_vec, (im->BD_JIT && im->kd == 3) ? std::min(im->max_nv, 8) : im->max_nv);
+    std::vector<int> nvs;
+    for (int w = 1; w <= full; w <<= 1)
+        if (w == full || w >= 4) nvs.push_back(w);
+    std::vector<int> tcs = {im->jit_tc};
+    if (im->BD_JIT && im->kd == 1 && im->precision == H2GPU_PREC_MIXED) tcs = {1, 0};
+    float best = 1e30f;
+    int bnv = full, btc = im->jit_tc;
+    cudaEvent_t* e = im->ev.e;
+    for (int nv : nvs)
+        for (int tc : tcs)
+        {
+            im->jit_tc = tc;
+            TRY(prepare(im, nv));
+            float ms = 0;
+            for (int rep = 0; rep < 2; rep++)
+            {
+                CK(cudaEventRecord(e[7], im->stream));
+                for (int c0 = 0; c0 < n_vec; c0 += nv)
+                    TRY(run_panel(im, nv, std::min(nv, n_vec - c0), dX + c0, ldx, 1, dY + c0, ldy, 1, im->stream, false));
+                CK(cudaEventRecord(e[6], im->stream));
+                CK(cudaEventSynchronize(e[6]));
+                CK(cudaEventElapsedTime(&ms, e[7], e[6]));
+            }
+            if (ms < best) { best = ms; bnv = nv; btc = tc; }
+        }
+    im->tuned_nv = bnv;
+    im->jit_tc = btc;
+    if (best_nv) *best_nv = bnv;
+    if (best_tc) *best_tc = btc;
+    return H2GPU_OK;
 }

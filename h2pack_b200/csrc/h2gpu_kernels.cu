@@ -739,8 +739,10 @@ __global__ void __launch_bounds__(256, 4) k_jit_tc(const JitTarget* __restrict__
     constexpr int NT = NV / 8;    // n-tiles of 8 right-hand sides
     constexpr int TS = 64;        // sources per shared-memory tile
     constexpr int NG = TS / 8;    // groups of 8 sources per tile
-    __shared__ float4 s_pt[TS];
-    __shared__ uint4 s_b[NG][NT][32];
+    constexpr int NB = NG * NT * 32 / 256;   // B-fragment entries staged per thread and tile
+    static_assert(NB >= 1 && NB * 256 == NG * NT * 32, "staging split");
+    __shared__ float4 s_pt[2][TS];
+    __shared__ uint4 s_b[2][NG][NT][32];
     __shared__ double s_acc[8][NT * 4][32];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, tq = lane & 3;
     const JitTarget tg = tgts[blockIdx.x];
@@ -754,31 +756,65 @@ __global__ void __launch_bounds__(256, 4) k_jit_tc(const JitTarget* __restrict__
 #pragma unroll
         for (int q = 0; q < 4; q++) { acc[n][q] = 0.f; s_acc[warp][n * 4 + q][lane] = 0.0; }
 
-    for (int s = tg.src_beg; s < tg.src_end; s++)
-    {
-        const JitSource sc = srcs[s];
-        const float ax = x0.x + sc.sx, ay = x0.y + sc.sy, az = x0.z + sc.sz;
-        const float bx = x1.x + sc.sx, by = x1.y + sc.sy, bz = x1.z + sc.sz;
-        for (int j0 = 0; j0 < sc.npt; j0 += TS)
+    // The tiles of all source sets form one sequence; tile k+1 is read from global
+    // memory into registers while tile k is computed from shared memory.
+    int ls = tg.src_beg, lj = 0;            // tile being loaded: source index and offset
+    float4 rp = make_float4(0.f, 0.f, 0.f, 0.f);
+    double rxa[NB], rxb[NB];
+    auto load_tile = [&](int sidx, int j0) {
+        const JitSource sc = srcs[sidx];
+        const int nj = min(TS, sc.npt - j0);
+        if (threadIdx.x < TS)
+            rp = (threadIdx.x < nj) ? pts[sc.pt0 + j0 + threadIdx.x] : make_float4(1e6f, 1e6f, 1e6f, 0.f);
+#pragma unroll
+        for (int u = 0; u < NB; u++)
         {
-            const int nj = min(TS, sc.npt - j0);
-            __syncthreads();
-            for (int j = threadIdx.x; j < TS; j += 256)
-                s_pt[j] = (j < nj) ? pts[sc.pt0 + j0 + j] : make_float4(1e6f, 1e6f, 1e6f, 0.f);
-            for (int e = threadIdx.x; e < NG * NT * 32; e += 256)
-            {
-                const int ln = e & 31, n = (e >> 5) % NT, grp = e / (32 * NT);
-                const int sa = grp * 8 + (ln & 3), sb = sa + 4, r = n * 8 + (ln >> 2);
-                const float xa = (sa < nj) ? (float) XS[(long long) (sc.in_row + j0 + sa) * NV + r] : 0.f;
-                const float xb = (sb < nj) ? (float) XS[(long long) (sc.in_row + j0 + sb) * NV + r] : 0.f;
-                const uint32_t ha = tf32_rna(xa), hb = tf32_rna(xb);
-                s_b[grp][n][ln] = make_uint4(ha, hb, tf32_rna(xa - __uint_as_float(ha)), tf32_rna(xb - __uint_as_float(hb)));
-            }
-            __syncthreads();
+            const int e = threadIdx.x + u * 256;
+            const int ln = e & 31, n = (e >> 5) % NT, grp = e / (32 * NT);
+            const int sa = grp * 8 + (ln & 3), sb = sa + 4, r = n * 8 + (ln >> 2);
+            rxa[u] = (sa < nj) ? XS[(long long) (sc.in_row + j0 + sa) * NV + r] : 0.0;
+            rxb[u] = (sb < nj) ? XS[(long long) (sc.in_row + j0 + sb) * NV + r] : 0.0;
+        }
+    };
+    auto store_tile = [&](int buf) {
+        if (threadIdx.x < TS) s_pt[buf][threadIdx.x] = rp;
+#pragma unroll
+        for (int u = 0; u < NB; u++)
+        {
+            const int e = threadIdx.x + u * 256;
+            const int ln = e & 31, n = (e >> 5) % NT, grp = e / (32 * NT);
+            const float xa = (float) rxa[u], xb = (float) rxb[u];
+            const uint32_t ha = tf32_rna(xa), hb = tf32_rna(xb);
+            s_b[buf][grp][n][ln] = make_uint4(ha, hb, tf32_rna(xa - __uint_as_float(ha)), tf32_rna(xb - __uint_as_float(hb)));
+        }
+    };
+    auto advance = [&](int& sidx, int& j0) {
+        j0 += TS;
+        if (j0 >= srcs[sidx].npt) { sidx++; j0 = 0; }
+    };
+
+    if (ls < tg.src_end)
+    {
+        load_tile(ls, lj);
+        store_tile(0);
+    }
+    __syncthreads();
+    int cs = ls, cj = lj, buf = 0;           // tile being computed
+    if (ls < tg.src_end) advance(ls, lj);
+    while (cs < tg.src_end)
+    {
+        const bool more = ls < tg.src_end;
+        if (more) load_tile(ls, lj);
+        {
+            const JitSource sc = srcs[cs];
+            const int nj = min(TS, sc.npt - cj);
+            const float ax = x0.x + sc.sx, ay = x0.y + sc.sy, az = x0.z + sc.sz;
+            const float bx = x1.x + sc.sx, by = x1.y + sc.sy, bz = x1.z + sc.sz;
             const int ngrp = (nj + 7) >> 3;
+#pragma unroll 2
             for (int grp = 0; grp < ngrp; grp++)
             {
-                const float4 pa = s_pt[grp * 8 + tq], pb = s_pt[grp * 8 + tq + 4];
+                const float4 pa = s_pt[buf][grp * 8 + tq], pb = s_pt[buf][grp * 8 + tq + 4];
                 float k[4];
                 {
                     float dx = ax - pa.x, dy = ay - pa.y, dz = az - pa.z;
@@ -800,7 +836,7 @@ __global__ void __launch_bounds__(256, 4) k_jit_tc(const JitTarget* __restrict__
 #pragma unroll
                 for (int n = 0; n < NT; n++)
                 {
-                    const uint4 b = s_b[grp][n][lane];
+                    const uint4 b = s_b[buf][grp][n][lane];
                     mma_tf32(acc[n], lo[0], lo[1], lo[2], lo[3], b.x, b.y);
                     mma_tf32(acc[n], hi[0], hi[1], hi[2], hi[3], b.z, b.w);
                     mma_tf32(acc[n], hi[0], hi[1], hi[2], hi[3], b.x, b.y);
@@ -811,6 +847,10 @@ __global__ void __launch_bounds__(256, 4) k_jit_tc(const JitTarget* __restrict__
 #pragma unroll
                 for (int q = 0; q < 4; q++) { s_acc[warp][n * 4 + q][lane] += (double) acc[n][q]; acc[n][q] = 0.f; }
         }
+        if (more) store_tile(buf ^ 1);
+        __syncthreads();
+        cs = ls; cj = lj; buf ^= 1;
+        if (more) advance(ls, lj);
     }
     double* base = (tg.out_y1 ? Y1 : PS) + (long long) tg.out_row * NV;
 #pragma unroll
@@ -976,16 +1016,12 @@ cudaError_t launch_asm(int NV, const AsmTask* t, int n, const int* slots, const 
 
 template <int KID, typename T, int KD>
 static cudaError_t launch_jit_k(int NV, const JitTarget* tg, int n, const JitSource* sr, const void* pts, KParam kp,
-                                int use_shift, const double* XS, double* PS, double* Y1, cudaStream_t st)
+                                int use_shift, int use_tc, const double* XS, double* PS, double* Y1, cudaStream_t st)
 {
     using T4 = typename Vec4<T>::t;
     const T4* p = (const T4*) pts;
     // FP32 scalar kernels on panels of 8 or 16: right-hand-side products on the tensor
-    // cores (H2G_JIT_TC=0 selects the CUDA-core kernel instead)
-    static const bool use_tc = [] {
-        const char* e = getenv("H2G_JIT_TC");
-        return !(e && e[0] == '0');
-    }();
+    // cores unless the image chose the CUDA-core kernel (autotuner, H2G_JIT_TC=0)
     if constexpr (KD == 1 && sizeof(T) == 4)
     {
         if (use_tc && NV == 16 && use_shift)
@@ -1012,19 +1048,19 @@ static cudaError_t launch_jit_k(int NV, const JitTarget* tg, int n, const JitSou
 }
 
 cudaError_t launch_jit(int kid, int fp32, int NV, const JitTarget* tg, int n, const JitSource* sr, const void* pts,
-                       KParam kp, int use_shift, const double* XS, double* PS, double* Y1, cudaStream_t st)
+                       KParam kp, int use_shift, int use_tc, const double* XS, double* PS, double* Y1, cudaStream_t st)
 {
     if (n <= 0) return cudaSuccess;
     switch (kid)
     {
-        case KRNL_COULOMB_ID:  return fp32 ? launch_jit_k<KRNL_COULOMB_ID, float, 1>(NV, tg, n, sr, pts, kp, use_shift, XS, PS, Y1, st)
-                                           : launch_jit_k<KRNL_COULOMB_ID, double, 1>(NV, tg, n, sr, pts, kp, use_shift, XS, PS, Y1, st);
-        case KRNL_GAUSSIAN_ID: return fp32 ? launch_jit_k<KRNL_GAUSSIAN_ID, float, 1>(NV, tg, n, sr, pts, kp, use_shift, XS, PS, Y1, st)
-                                           : launch_jit_k<KRNL_GAUSSIAN_ID, double, 1>(NV, tg, n, sr, pts, kp, use_shift, XS, PS, Y1, st);
-        case KRNL_MATERN32_ID: return fp32 ? launch_jit_k<KRNL_MATERN32_ID, float, 1>(NV, tg, n, sr, pts, kp, use_shift, XS, PS, Y1, st)
-                                           : launch_jit_k<KRNL_MATERN32_ID, double, 1>(NV, tg, n, sr, pts, kp, use_shift, XS, PS, Y1, st);
-        case KRNL_RPY_ID:      return fp32 ? launch_jit_k<KRNL_RPY_ID, float, 3>(NV, tg, n, sr, pts, kp, use_shift, XS, PS, Y1, st)
-                                           : launch_jit_k<KRNL_RPY_ID, double, 3>(NV, tg, n, sr, pts, kp, use_shift, XS, PS, Y1, st);
+        case KRNL_COULOMB_ID:  return fp32 ? launch_jit_k<KRNL_COULOMB_ID, float, 1>(NV, tg, n, sr, pts, kp, use_shift, use_tc, XS, PS, Y1, st)
+                                           : launch_jit_k<KRNL_COULOMB_ID, double, 1>(NV, tg, n, sr, pts, kp, use_shift, use_tc, XS, PS, Y1, st);
+        case KRNL_GAUSSIAN_ID: return fp32 ? launch_jit_k<KRNL_GAUSSIAN_ID, float, 1>(NV, tg, n, sr, pts, kp, use_shift, use_tc, XS, PS, Y1, st)
+                                           : launch_jit_k<KRNL_GAUSSIAN_ID, double, 1>(NV, tg, n, sr, pts, kp, use_shift, use_tc, XS, PS, Y1, st);
+        case KRNL_MATERN32_ID: return fp32 ? launch_jit_k<KRNL_MATERN32_ID, float, 1>(NV, tg, n, sr, pts, kp, use_shift, use_tc, XS, PS, Y1, st)
+                                           : launch_jit_k<KRNL_MATERN32_ID, double, 1>(NV, tg, n, sr, pts, kp, use_shift, use_tc, XS, PS, Y1, st);
+        case KRNL_RPY_ID:      return fp32 ? launch_jit_k<KRNL_RPY_ID, float, 3>(NV, tg, n, sr, pts, kp, use_shift, use_tc, XS, PS, Y1, st)
+                                           : launch_jit_k<KRNL_RPY_ID, double, 3>(NV, tg, n, sr, pts, kp, use_shift, use_tc, XS, PS, Y1, st);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -49,8 +49,42 @@ class Image:
         self.handle = h
         self.N = int(desc.krnl_dim) * int(desc.n_point)
 
+    @classmethod
+    def batch(cls, descs, precision="fp64", max_n_vec: int = 16, device: int = -1) -> "Image":
+        """One image for many representations (h2gpu_batch_create); vectors are stacked in order."""
+        lib = _abi.libh2gpu()
+        arr = (_abi.Desc * len(descs))(*descs)
+        opt = _abi.Options(_prec(precision), int(max_n_vec), int(device))
+        h = C.c_void_p()
+        _abi.check(lib.h2gpu_batch_create(arr, len(descs), C.byref(opt), C.byref(h)), lib, "h2gpu_batch_create")
+        img = cls.__new__(cls)
+        img.lib = lib
+        img.handle = h
+        img.N = sum(int(d.krnl_dim) * int(d.n_point) for d in descs)
+        img.sizes = [int(d.krnl_dim) * int(d.n_point) for d in descs]
+        return img
+
     def set_precision(self, precision):
         _abi.check(self.lib.h2gpu_set_precision(self.handle, _prec(precision)), self.lib, "h2gpu_set_precision")
+
+    def graph_capture(self, X, Y):
+        """Capture the device apply X -> Y (torch CUDA float64, row-major) in a CUDA graph."""
+        st = self.lib.h2gpu_graph_capture(self.handle, X.shape[1], C.c_void_p(X.data_ptr()), X.stride(0),
+                                          C.c_void_p(Y.data_ptr()), Y.stride(0))
+        _abi.check(st, self.lib, "h2gpu_graph_capture")
+
+    def graph_launch(self, stream=None):
+        import torch
+        s = C.c_void_p(stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream)
+        _abi.check(self.lib.h2gpu_graph_launch(self.handle, s), self.lib, "h2gpu_graph_launch")
+
+    def autotune(self, X, Y):
+        """Pick the panel width (and JIT kernel variant) that applies X fastest; returns (nv, tensor_cores)."""
+        nv, tc = C.c_int(), C.c_int()
+        st = self.lib.h2gpu_autotune(self.handle, X.shape[1], C.c_void_p(X.data_ptr()), X.stride(0),
+                                     C.c_void_p(Y.data_ptr()), Y.stride(0), C.byref(nv), C.byref(tc))
+        _abi.check(st, self.lib, "h2gpu_autotune")
+        return nv.value, bool(tc.value)
 
     def matvec(self, x: np.ndarray) -> np.ndarray:
         x = np.ascontiguousarray(x, dtype=np.float64)

@@ -198,6 +198,31 @@ int h2gpu_permute_matrix_rows(h2gpu_image *img, int forward, int layout, int n_v
  */
 int h2gpu_matvec_device_noalloc(h2gpu_image *img, const double *d_x, double *d_y, void *stream);
 
+/*
+ * Batched form: one image for n_desc independent representations with the same
+ * kernel, kernel parameters, krnl_dim and mode.  Every phase runs as one launch per
+ * tree level over all of them (flattened cross-matrix task lists).  Vectors of the
+ * batch are the members' vectors stacked in order (rows sum of krnl_dim * n_point).
+ * No counterpart in the reference (its callers loop over handles).
+ */
+int h2gpu_batch_create(const h2gpu_desc *descs, int n_desc, const h2gpu_options *opt, h2gpu_image **out);
+
+/*
+ * Capture the device-resident apply of n_vec right-hand sides (dX -> dY, row-major,
+ * fixed pointers) in a CUDA graph, and replay it on a stream (NULL: the image's).
+ * No counterpart in the reference.
+ */
+int h2gpu_graph_capture(h2gpu_image *img, int n_vec, const double *dX, int ldx, double *dY, int ldy);
+int h2gpu_graph_launch(h2gpu_image *img, void *stream);
+
+/*
+ * Autotuner: time the device apply of n_vec right-hand sides for each candidate
+ * panel width (and, for FP32 JIT images, tensor-core vs CUDA-core kernel) and keep
+ * the fastest for this image.  dY is overwritten.  No counterpart in the reference.
+ */
+int h2gpu_autotune(h2gpu_image *img, int n_vec, const double *dX, int ldx, double *dY, int ldy,
+                   int *best_nv, int *best_tc);
+
 int h2gpu_get_stats(h2gpu_image *img, h2gpu_stats *st);
 int h2gpu_reset_stats(h2gpu_image *img);
 size_t h2gpu_image_bytes(const h2gpu_image *img);
