@@ -46,6 +46,12 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-fp64", action="store_true")
     p.add_argument("--check-rows", type=int, default=10_000)
+    p.add_argument("--workload", default="jit_matern",
+                   choices=["jit_matern", "aot_coulomb", "batched", "served"],
+                   help="jit_matern: the headline configuration; the others print extra lines for the "
+                        "other configurations (AOT Coulomb matvec, batched matrices, served requests)")
+    p.add_argument("--n-matrices", type=int, default=64)
+    p.add_argument("--n-requests", type=int, default=96)
     return p.parse_args()
 
 
@@ -326,10 +332,194 @@ def cpu_baseline(H, args):
                       f"handle, {sec:.1f} s"}
 
 
+def timed_loop(fn, steps, warm):
+    import torch
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def run_aot_coulomb(args):
+    """Config 1: Coulomb 1/r, N = 80,000, max 300 points per leaf, reltol 1e-6, stored U/B/D,
+    one RHS U[-0.5, 0.5]; HBM-bound.  value = matvecs/s of the plain FP64 drop-in."""
+    import torch
+    from h2pack_b200 import H2Matrix, direct_sum
+    n = 80_000 if args.n == 1_000_000 else args.n
+    coord = points(n, seed=11)
+    t0 = time.time()
+    H = H2Matrix("coulomb", coord, [], 1e-6, BD_JIT=0, max_leaf_points=300, proxy="id",
+                 pp_fname="/tmp/h2b200_pp_coulomb_1e-6.dat", n_thread=os.cpu_count())
+    build_s = time.time() - t0
+    img = H.image()
+    x = (torch.rand(H.N, 1, dtype=torch.float64, device="cuda") - 0.5)
+    y = torch.empty_like(x)
+    out = {}
+    for prec in ("fp64", "mixed"):
+        H.set_precision(prec)
+        s0 = img.stats()
+        ms = timed_loop(lambda: img.matmul_device(x, y), args.steps, args.warmup)
+        s1 = img.stats()
+        ph = [(b - a) / (args.steps + 0) for a, b in zip(s0["ms_phase"], s1["ms_phase"])]
+        st = img.stats()
+        stored = st["bytes_U"] + st["bytes_B"] + st["bytes_D"]
+        out[prec] = {"ms": ms, "matvecs_per_s": 1e3 / ms, "phase_ms": ph,
+                     "stored_GBps": stored / (ms * 1e-3) / 1e9, "ref_model_GBps": st["ref_mv_bytes"] / (ms * 1e-3) / 1e9,
+                     "stored_bytes": stored}
+    H.set_precision("fp64")
+    y64 = img.matmul_device(x).cpu().numpy()[:, 0]
+    rng = np.random.default_rng(2)
+    rows = rng.choice(H.N, min(args.check_rows, H.N), replace=False)
+    yd = direct_sum("coulomb", [], coord, x.cpu().numpy()[:, 0], coord[:, rows])
+    err = float(np.linalg.norm(y64[rows] - yd) / np.linalg.norm(yd))
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+        xh = x.cpu().numpy()[:, 0].copy()
+        yh = np.zeros(H.N)
+        O.libref().H2P_matvec(H.h2pack, O.dptr(xh), O.dptr(yh))
+        t = time.perf_counter()
+        reps = 3
+        for _ in range(reps):
+            O.libref().H2P_matvec(H.h2pack, O.dptr(xh), O.dptr(yh))
+        sec = (time.perf_counter() - t) / reps
+        cpu = {"value": 1.0 / sec, "unit": "matvecs/s", "cores": H.info["n_thread"], "kind": "reference",
+               "sample": f"{reps} H2P_matvec of H2Pack compiled from its sources, same handle"}
+    peak = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]) \
+        if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else 6650.0
+    line = {"metric": "H2 matvecs/s (Coulomb N=80k AOT FP64, 1 RHS)", "value": out["fp64"]["matvecs_per_s"],
+            "unit": "matvecs/s", "workload": "aot_coulomb", "n": n, "build_seconds": build_s,
+            "fp64": out["fp64"], "mixed": out["mixed"], "rel_err_vs_direct_fp64": err,
+            "roofline": {"bound": "hbm", "achieved": out["fp64"]["stored_GBps"], "peak": peak, "unit": "GB/s",
+                         "frac": out["fp64"]["stored_GBps"] / peak,
+                         "note": "stored U (read twice), B and D bytes per matvec / matvec time, of measured copy BW"},
+            "cpu_baseline": cpu, "info": H.info}
+    print(json.dumps(line), flush=True)
+    H.close()
+
+
+def log_uniform(rng, lo, hi, k):
+    return np.exp(rng.uniform(np.log(lo), np.log(hi), k)).astype(int)
+
+
+def run_batched(args):
+    """Config 4 (reduced count by default): independent H2 matrices with N log-uniform in
+    [2000, 64000], kernels alternating Coulomb / Gaussian exp(-r^2) (l = 1), reltol 1e-6, JIT
+    mode, 8 RHS each.  One batched image per kernel (flattened cross-matrix task lists),
+    CUDA-graph-captured apply, autotuned panel / kernel choice.  value = matrix-RHS products/s."""
+    import torch
+    from h2pack_b200 import H2Matrix, Image
+    rng = np.random.default_rng(4)
+    ns = log_uniform(rng, 2000, 64000, args.n_matrices)
+    t0 = time.time()
+    Hs = []
+    for i, n in enumerate(ns):
+        kern = "coulomb" if i % 2 == 0 else "gaussian"
+        Hs.append(H2Matrix(kern, points(int(n), seed=100 + i), [] if kern == "coulomb" else [1.0], 1e-6, BD_JIT=1,
+                           proxy="id", pp_fname=f"/tmp/h2b200_pp_{kern}_1e-6.dat", n_thread=os.cpu_count()))
+    build_s = time.time() - t0
+    groups = {"coulomb": [H for i, H in enumerate(Hs) if i % 2 == 0],
+              "gaussian": [H for i, H in enumerate(Hs) if i % 2 == 1]}
+    res = {}
+    for prec in ("mixed", "fp64"):
+        imgs, bufs = [], []
+        for kern, hs in groups.items():
+            img = Image.batch([H.describe() for H in hs], precision=prec)
+            X = torch.rand(img.N, 8, dtype=torch.float64, device="cuda") - 0.5
+            Y = torch.empty_like(X)
+            tuned = img.autotune(X, Y)
+            img.graph_capture(X, Y)
+            imgs.append((img, tuned))
+            bufs.append((X, Y))
+        ms = timed_loop(lambda: [img.graph_launch() for img, _ in imgs], args.steps, args.warmup)
+        # the same matrices one image each, eager (no batching, no graph)
+        singles = [Image(H.describe(), precision=prec) for H in Hs]
+        sx = [torch.rand(s.N, 8, dtype=torch.float64, device="cuda") - 0.5 for s in singles]
+        ms1 = timed_loop(lambda: [s.matmul_device(x) for s, x in zip(singles, sx)], max(2, args.steps // 2), 1)
+        res[prec] = {"ms": ms, "products_per_s": len(Hs) * 8 * 1e3 / ms, "unbatched_ms": ms1,
+                     "tuned": [t for _, t in imgs]}
+        for s in singles:
+            s.close()
+        for img, _ in imgs:
+            img.close()
+    line = {"metric": "batched H2 matrix-RHS products/s", "value": res["mixed"]["products_per_s"], "unit": "products/s",
+            "workload": "batched", "n_matrices": len(Hs), "n_total_points": int(ns.sum()), "nvec": 8,
+            "build_seconds": build_s, "mixed": res["mixed"], "fp64": res["fp64"],
+            "speedup_mixed_vs_fp64": res["fp64"]["ms"] / res["mixed"]["ms"],
+            "speedup_batched_vs_unbatched_mixed": res["mixed"]["unbatched_ms"] / res["mixed"]["ms"]}
+    print(json.dumps(line), flush=True)
+    for H in Hs:
+        H.close()
+
+
+def run_served(args):
+    """Config 5 (reduced sizes by default): resident GP matrices K + mu I (Gaussian or
+    Matern-3/2, l uniform in [0.5, 2], mu = 1e-2, N log-uniform in [1e4, 5e4], reltol 1e-6);
+    a Poisson stream at 2000 req/s of matvec / PCG (relres 1e-6) requests, 50/50; HBM budget
+    150 GB.  Reports throughput and p50/p99 latency, mixed vs FP64."""
+    import copy
+    import torch
+    from h2pack_b200 import H2Matrix
+    from h2pack_b200.serve import Request, Server, latency_stats
+    rng = np.random.default_rng(5)
+    n_mat = 8
+    ns = log_uniform(rng, 10_000, 50_000, n_mat)
+    Hs = {}
+    t0 = time.time()
+    for i, n in enumerate(ns):
+        kern = "gaussian" if i % 2 == 0 else "matern32"
+        ell = float(rng.uniform(0.5, 2.0))
+        param = [1.0 / ell ** 2] if kern == "gaussian" else [1.0 / ell]
+        Hs[f"m{i}"] = H2Matrix(kern, points(int(n), seed=200 + i), param, 1e-6, BD_JIT=1, proxy="surface",
+                               n_thread=os.cpu_count())
+    build_s = time.time() - t0
+    g = torch.Generator(device="cuda").manual_seed(9)
+    arr = np.cumsum(rng.exponential(1.0 / 2000.0, args.n_requests))
+    base = []
+    for i in range(args.n_requests):
+        name = f"m{int(rng.integers(n_mat))}"
+        kind = "pcg" if rng.random() < 0.5 else "matvec"
+        base.append(Request(rid=i, matrix=name, kind=kind, arrival=float(arr[i]),
+                            b=torch.randn(Hs[name].N, dtype=torch.float64, device="cuda", generator=g)))
+    out = {}
+    for prec in ("mixed", "fp64"):
+        srv = Server(budget_bytes=150e9, max_slots=16)
+        for name, H in Hs.items():
+            assert srv.admit_matrix(name, H.image(), 1e-2, prec)
+        reqs = [copy.copy(r) for r in base]
+        done = srv.run(reqs, realtime=True)
+        st = latency_stats(done)
+        pcg = [r for r in done if r.kind == "pcg"]
+        st.update({"pcg_iters_mean": float(np.mean([r.iters for r in pcg])) if pcg else 0,
+                   "pcg_converged": int(sum(r.converged for r in pcg)), "n_pcg": len(pcg),
+                   "max_relres": max((r.relres for r in pcg), default=None)})
+        out[prec] = st
+    line = {"metric": "served requests/s (matvec + PCG on K+mu I, Poisson 2000 req/s)",
+            "value": out["mixed"]["throughput_req_s"], "unit": "req/s", "workload": "served",
+            "n_matrices": n_mat, "sizes": [int(n) for n in ns], "n_requests": args.n_requests,
+            "build_seconds": build_s, "mixed": out["mixed"], "fp64": out["fp64"],
+            "speedup_mixed_vs_fp64": out["fp64"]["mean_ms"] / out["mixed"]["mean_ms"]}
+    print(json.dumps(line), flush=True)
+    for H in Hs.values():
+        H.close()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "aot_coulomb":
+        run_aot_coulomb(args)
+    elif args.workload == "batched":
+        run_batched(args)
+    elif args.workload == "served":
+        run_served(args)
     else:
         run_ours(args)
 

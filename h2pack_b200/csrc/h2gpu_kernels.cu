@@ -826,12 +826,14 @@ __global__ void __launch_bounds__(256, 4) k_jit_tc(const JitTarget* __restrict__
                     dx = bx - pb.x; dy = by - pb.y; dz = bz - pb.z;
                     k[3] = Scalar<KID, float>::f(dx * dx + dy * dy + dz * dz, p0, c0);   // (g+8, t+4)
                 }
+                // hi rounded to TF32; the remainder is exact in FP32 and handed over
+                // as is: the MMA reads its TF32 bits (error < 2^-22 of the kernel value)
                 uint32_t hi[4], lo[4];
 #pragma unroll
                 for (int q = 0; q < 4; q++)
                 {
                     hi[q] = tf32_rna(k[q]);
-                    lo[q] = tf32_rna(k[q] - __uint_as_float(hi[q]));
+                    lo[q] = __float_as_uint(k[q] - __uint_as_float(hi[q]));
                 }
 #pragma unroll
                 for (int n = 0; n < NT; n++)
