@@ -147,6 +147,19 @@ struct h2gpu_image {
     h2gpu_stats st{};
     Ev ev;
 
+    // pair plan: each unordered JIT pair evaluated once (FP32 tensor-core path)
+    int has_pair = 0;
+    PairOwner* d_owN = nullptr;
+    PairOwner* d_owF = nullptr;
+    PairPartner* d_pp = nullptr;
+    JitTarget* d_jtN2 = nullptr;
+    JitTarget* d_jtF2 = nullptr;
+    Y1Task* d_y1t2 = nullptr;
+    int* d_y1_slots2 = nullptr;
+    AsmTask* d_asm2 = nullptr;
+    int* d_asm_slots2 = nullptr;
+    int n_owN = 0, n_owF = 0, n_jtN2 = 0, n_jtF2 = 0, n_y12 = 0;
+
     // tuning (h2gpu_autotune) and captured graph (h2gpu_graph_capture)
     int jit_tc = 1;          // tensor-core JIT kernel for FP32 panels of 8 / 16
     int tuned_nv = 0;        // panel width chosen by the autotuner (0: default rule)
@@ -162,7 +175,8 @@ void free_all(h2gpu_image* im)
     void* ptrs[] = {im->d_up, im->d_dn, im->d_y1t, im->d_y1_slots, im->d_blkB, im->d_blkD, im->d_jtN, im->d_jtF,
                     im->d_js, im->d_asm, im->d_asm_slots, im->d_fwd, im->d_bwd, im->d_U64, im->d_U32, im->d_B64,
                     im->d_B32, im->d_D64, im->d_D32, im->d_pts64, im->d_pts32, im->d_XS, im->d_PS, im->d_Y1,
-                    im->d_PUSH, im->d_io};
+                    im->d_PUSH, im->d_io, im->d_owN, im->d_owF, im->d_pp, im->d_jtN2, im->d_jtF2, im->d_y1t2,
+                    im->d_y1_slots2, im->d_asm2, im->d_asm_slots2};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (auto& e : im->ev.e)
@@ -295,6 +309,14 @@ struct HostPlan {
     std::vector<int> fw, bw;
     std::vector<double4> p64;
     std::vector<float4> p32;
+    // pair plan (FP32 tensor-core path of scalar JIT kernels)
+    std::vector<PairOwner> owN, owF;
+    std::vector<PairPartner> partners;
+    std::vector<JitTarget> jtN2, jtF2;
+    std::vector<Y1Task> y1t2;
+    std::vector<int> y1_slots2;
+    std::vector<AsmTask> at2;
+    std::vector<int> at_slots2;
 };
 
 int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
@@ -383,7 +405,7 @@ int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
     // ---- partial slots
     long long ps = 0;
     auto alloc = [&](int rows) { long long r = ps; ps += rows; return (int) r; };
-    std::vector<std::vector<int>> y1s(n_node), asms(n_node);
+    std::vector<std::vector<int>> y1s(n_node), asms(n_node), pair_y1, pair_asm;
     std::vector<char> has_y1(n_node, 0);
     const int R = 64;
     std::vector<BlkTask>& blkB = hp.blkB;
@@ -560,6 +582,113 @@ int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
                 emit(jtF, n, d->pt_cluster[2 * n], npt_of(d, n), s, 0, farL[n]);
             }
         }
+
+        // ---- pair plan for the FP32 tensor-core path of scalar kernels: every unordered
+        // pair (same-level skeleton sets, and inadmissible leaf pairs) is evaluated once
+        // and applied both ways; its owner accumulates its side over all its partners,
+        // each partner's side goes to a slot of its own.  Diagonal leaf blocks and the
+        // level-mismatched pairs stay one-sided.  Slots are disjoint from the one-sided
+        // plan's, so both plans share the partial space.
+        if (kd == 1)
+        {
+            im->has_pair = 1;
+            pair_y1.assign(n_node, {});
+            pair_asm.assign(n_node, {});
+            std::vector<double> load(n_node, 0.0);
+            std::vector<std::vector<int>> fpart(n_node), npart(n_node);
+            auto choose = [&](int a, int b, double w) {
+                int o = (load[a] <= load[b]) ? a : b;
+                load[o] += w;
+                return o;
+            };
+            for (int i = 0; i < d->n_r_adm_pair; i++)
+            {
+                int a = d->r_adm_pairs[2 * i], b = d->r_adm_pairs[2 * i + 1];
+                if (lvl[a] != lvl[b] || d->J_n[a] == 0 || d->J_n[b] == 0) continue;
+                int o = choose(a, b, (double) d->J_n[a] * d->J_n[b]);
+                fpart[o].push_back(o == a ? b : a);
+            }
+            for (int i = 0; i < d->n_r_inadm_pair; i++)
+            {
+                int a = d->r_inadm_pairs[2 * i], b = d->r_inadm_pairs[2 * i + 1];
+                int o = choose(a, b, (double) npt_of(d, a) * npt_of(d, b));
+                npart[o].push_back(o == a ? b : a);
+            }
+            const int PCH = 256;
+            auto emit_owner = [&](std::vector<PairOwner>& out, int a, bool isJ, const std::vector<int>& parts,
+                                  std::vector<std::vector<int>>& lists) {
+                int na = isJ ? d->J_n[a] : npt_of(d, a);
+                int pa = isJ ? jp0[a] : d->pt_cluster[2 * a];
+                int in_a = isJ ? N + y0r[a] : mc[2 * a];
+                int slot_a = alloc(na);
+                lists[a].push_back(slot_a);
+                for (int c0 = 0; c0 < na; c0 += PCH)
+                {
+                    PairOwner ow;
+                    ow.pa = pa + c0; ow.na = std::min(PCH, na - c0); ow.in_a = in_a + c0; ow.out_a = slot_a + c0;
+                    ow.p_beg = (int) hp.partners.size();
+                    for (int b : parts)
+                    {
+                        PairPartner pp;
+                        pp.pb = isJ ? jp0[b] : d->pt_cluster[2 * b];
+                        pp.nb = isJ ? d->J_n[b] : npt_of(d, b);
+                        pp.in_b = isJ ? N + y0r[b] : mc[2 * b];
+                        pp.out_b = alloc(pp.nb);
+                        lists[b].push_back(pp.out_b);
+                        pp.sx = (float) (ctr[3 * a] - ctr[3 * b]);
+                        pp.sy = (float) (ctr[3 * a + 1] - ctr[3 * b + 1]);
+                        pp.sz = (float) (ctr[3 * a + 2] - ctr[3 * b + 2]);
+                        hp.partners.push_back(pp);
+                    }
+                    ow.p_end = (int) hp.partners.size();
+                    out.push_back(ow);
+                }
+            };
+            for (int n = 0; n < n_node; n++)
+                if (!fpart[n].empty()) emit_owner(hp.owF, n, true, fpart[n], pair_y1);
+            for (int n = 0; n < n_node; n++)
+                if (!npart[n].empty()) emit_owner(hp.owN, n, false, npart[n], pair_asm);
+            for (int i = 0; i < d->n_leaf_node; i++)
+            {
+                int n = d->leaf_nodes[i];
+                int s = alloc(npt_of(d, n));
+                pair_asm[n].push_back(s);
+                emit(hp.jtN2, n, d->pt_cluster[2 * n], npt_of(d, n), s, 0, std::vector<Src>{pts_src(n)});
+            }
+            for (int n = 0; n < n_node; n++)
+            {
+                std::vector<Src> left;
+                for (const Src& sr : farJ[n])
+                    if (sr.pt0 < d->n_point) left.push_back(sr);   // leaf points of a coarser node
+                if (!left.empty() && d->J_n[n] > 0)
+                {
+                    int s = alloc(d->U_ncol[n]);
+                    pair_y1[n].push_back(s);
+                    emit(hp.jtF2, n, jp0[n], d->J_n[n], s, 0, left);
+                }
+                if (!farL[n].empty())
+                {
+                    int s = alloc(npt_of(d, n));
+                    pair_asm[n].push_back(s);
+                    emit(hp.jtF2, n, d->pt_cluster[2 * n], npt_of(d, n), s, 0, farL[n]);
+                }
+            }
+            auto owner_work = [&](std::vector<PairOwner>& v) {
+                std::vector<std::pair<double, int>> w(v.size());
+                for (size_t i = 0; i < v.size(); i++)
+                {
+                    double sb = 0;
+                    for (int k = v[i].p_beg; k < v[i].p_end; k++) sb += hp.partners[k].nb;
+                    w[i] = {-(double) v[i].na * sb, (int) i};
+                }
+                std::stable_sort(w.begin(), w.end());
+                std::vector<PairOwner> o(v.size());
+                for (size_t i = 0; i < v.size(); i++) o[i] = v[w[i].second];
+                v.swap(o);
+            };
+            owner_work(hp.owF);
+            owner_work(hp.owN);
+        }
     }
 
     // ---- JIT targets, largest work first (shorter tail of the launch)
@@ -578,6 +707,8 @@ int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
     };
     by_work(jtN);
     by_work(jtF);
+    by_work(hp.jtN2);
+    by_work(hp.jtF2);
 
     // ---- y1 sums (AOT)
     std::vector<Y1Task>& y1t = hp.y1t;
@@ -611,6 +742,7 @@ int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
             bool leaf = d->n_child[n] == 0;
             int dst = leaf ? alloc(nr) : y0r[d->children[n * d->max_child]];
             if (leaf) asms[n].push_back(dst);
+            if (leaf && !pair_asm.empty()) pair_asm[n].push_back(dst);
             for (int r0 = 0; r0 < nr; r0 += R)
             {
                 DownTask t;
@@ -638,6 +770,31 @@ int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
         for (int s : asms[n]) at_slots.push_back(s);
         t.slot_end = (int) at_slots.size();
         at.push_back(t);
+    }
+    if (im->has_pair)
+    {
+        for (int n = 0; n < n_node; n++)
+        {
+            if (!has_y1[n]) continue;
+            Y1Task t;
+            t.row = y0r[n]; t.nrow = d->U_ncol[n];
+            t.slot_beg = (int) hp.y1_slots2.size();
+            for (int sl : pair_y1[n]) hp.y1_slots2.push_back(sl);
+            t.slot_end = (int) hp.y1_slots2.size();
+            hp.y1t2.push_back(t);
+        }
+        for (int i = 0; i < d->n_leaf_node; i++)
+        {
+            int n = d->leaf_nodes[i];
+            AsmTask t;
+            t.row0 = mc[2 * n]; t.nrow = kd * npt_of(d, n);
+            t.slot_beg = (int) hp.at_slots2.size();
+            for (int sl : pair_asm[n]) hp.at_slots2.push_back(sl);
+            t.slot_end = (int) hp.at_slots2.size();
+            hp.at2.push_back(t);
+        }
+        im->n_owN = (int) hp.owN.size(); im->n_owF = (int) hp.owF.size();
+        im->n_jtN2 = (int) hp.jtN2.size(); im->n_jtF2 = (int) hp.jtF2.size(); im->n_y12 = (int) hp.y1t2.size();
     }
     REQ(ps < (1LL << 31), "partial space too large");
     im->ps_rows = ps;
@@ -715,6 +872,15 @@ int upload_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
     TRY(upload(hp.bw, &im->d_bwd, im->bytes));
     TRY(upload(hp.p64, &im->d_pts64, im->bytes));
     TRY(upload(hp.p32, &im->d_pts32, im->bytes));
+    TRY(upload(hp.owN, &im->d_owN, im->bytes));
+    TRY(upload(hp.owF, &im->d_owF, im->bytes));
+    TRY(upload(hp.partners, &im->d_pp, im->bytes));
+    TRY(upload(hp.jtN2, &im->d_jtN2, im->bytes));
+    TRY(upload(hp.jtF2, &im->d_jtF2, im->bytes));
+    TRY(upload(hp.y1t2, &im->d_y1t2, im->bytes));
+    TRY(upload(hp.y1_slots2, &im->d_y1_slots2, im->bytes));
+    TRY(upload(hp.at2, &im->d_asm2, im->bytes));
+    TRY(upload(hp.at_slots2, &im->d_asm_slots2, im->bytes));
     if (!d->BD_JIT)
     {
         if (im->B_elems)
@@ -788,6 +954,39 @@ int run_panel(h2gpu_image* im, int NV, int nv, const double* X, long long x_rs, 
 {
     const bool f32 = im->precision == H2GPU_PREC_MIXED;
     cudaEvent_t* e = im->ev.e;
+    if (im->has_pair && f32 && im->jit_tc && (NV == 8 || NV == 16))
+    {
+        // each unordered JIT pair evaluated once, applied both ways (tensor cores)
+        const KParam kp = kparam_of(im);
+        if (timed) CK(cudaEventRecord(e[0], s));
+        CK(launch_gather(NV, X, x_rs, x_cs, nv, im->d_fwd, im->N, im->d_XS, s));
+        if (timed) CK(cudaEventRecord(e[1], s));
+        CK(launch_jit(im->kernel_id, 1, NV, im->d_jtN2, im->n_jtN2, im->d_js, im->d_pts32, kp, 1, 1, im->d_XS,
+                      im->d_PS, im->d_Y1, s));
+        CK(launch_pair(im->kernel_id, NV, im->d_owN, im->n_owN, im->d_pp, im->d_pts32, kp, im->d_XS, im->d_PS, s));
+        if (timed) CK(cudaEventRecord(e[2], s));
+        for (size_t L = 0; L + 1 < im->up_beg.size(); L++)
+        {
+            int b = im->up_beg[L], n = im->up_beg[L + 1] - b;
+            CK(launch_up<float>(NV, im->d_up + b, n, im->d_U32, im->d_XS, s));
+        }
+        if (timed) CK(cudaEventRecord(e[3], s));
+        CK(launch_pair(im->kernel_id, NV, im->d_owF, im->n_owF, im->d_pp, im->d_pts32, kp, im->d_XS, im->d_PS, s));
+        CK(launch_jit(im->kernel_id, 1, NV, im->d_jtF2, im->n_jtF2, im->d_js, im->d_pts32, kp, 1, 1, im->d_XS,
+                      im->d_PS, im->d_Y1, s));
+        CK(launch_y1sum(NV, im->d_y1t2, im->n_y12, im->d_y1_slots2, im->d_PS, im->d_Y1, s));
+        if (timed) CK(cudaEventRecord(e[4], s));
+        for (size_t L = 0; L + 1 < im->dn_beg.size(); L++)
+        {
+            int b = im->dn_beg[L], n = im->dn_beg[L + 1] - b;
+            CK(launch_down<float>(NV, im->d_dn + b, n, im->d_U32, im->d_Y1, im->d_PS, im->d_PUSH, s));
+        }
+        if (timed) CK(cudaEventRecord(e[5], s));
+        CK(launch_asm(NV, im->d_asm2, im->n_leaf, im->d_asm_slots2, im->d_PS, im->d_fwd, Y, y_rs, y_cs, nv, s));
+        if (timed) CK(cudaEventRecord(e[6], s));
+        im->st.n_launches += 7 + (long long) (im->up_beg.size() - 1) + (long long) (im->dn_beg.size() - 1);
+        return H2GPU_OK;
+    }
     if (timed) CK(cudaEventRecord(e[0], s));
     CK(launch_gather(NV, X, x_rs, x_cs, nv, im->d_fwd, im->N, im->d_XS, s));
     // D phase first: it needs only x (in the graph-free stream order it simply runs before the upward sweep)

@@ -73,6 +73,22 @@ struct JitSource {
     float sx, sy, sz;  // center(target set) - center(source set), for re-centred FP32 evaluation
 };
 
+// JIT pair tasks (FP32 tensor-core path): every unordered pair of point sets (a, b)
+// is evaluated once and applied both ways.  One record per chunk of <= 256 points of
+// an owner set a, with the list of its partners b.
+struct PairOwner {
+    int pa, na;          // point-space range of this chunk of a
+    int in_a;            // XS row of y0 / x of the chunk's first point
+    int out_a;           // PS row of the chunk's first output row (sum over all partners)
+    int p_beg, p_end;    // partner range
+};
+struct PairPartner {
+    int pb, nb;          // point-space range of b
+    int in_b;            // XS row of b's input
+    int out_b;           // PS row of b's output slot (this chunk of a only)
+    float sx, sy, sz;    // center(a) - center(b)
+};
+
 // Final assembly of a leaf: Y[fwd[row0 + r]][v] = sum_s PS[slot_s + r][v]
 struct AsmTask {
     int row0, nrow;

@@ -356,6 +356,84 @@ __device__ __forceinline__ void chunk_apply(const TA* __restrict__ A, int R, int
         for (int i = threadIdx.x; i < R * NV; i += kThreads) out0[i] = s_o0[i];
 }
 
+// Stored block chunk, single right-hand side (the matvec path, memory bound).
+// Warp w owns columns 32w + lane (+256k) and walks all rows of the chunk 8 at a time:
+// 8 independent loads per lane in flight, A^T w completes in registers (no reduction),
+// and the 8 row partials of A v are combined with one transposed butterfly per
+// 8 x 32 tile; the warps' row partials are summed once at the end.
+template <typename TA>
+__global__ void __launch_bounds__(256) k_blk1(const BlkTask* __restrict__ tasks, const TA* __restrict__ arena,
+                                              const double* __restrict__ XS, double* __restrict__ PS)
+{
+    constexpr int CS = 1024;
+    __shared__ double s_v[CS];
+    __shared__ double s_w[64];
+    __shared__ double s_red[kWarps][64];
+    const BlkTask T = tasks[blockIdx.x];
+    const TA* A = arena + T.a_off;
+    const int R = T.nrow, ncol = T.ncol, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const bool do0 = T.out0_row >= 0, do1 = T.out1_row >= 0;
+    for (int r = threadIdx.x; r < 64; r += 256) s_w[r] = (do1 && r < R) ? XS[T.in1_row + r] : 0.0;
+    double part[8];
+#pragma unroll
+    for (int gI = 0; gI < 8; gI++) part[gI] = 0.0;
+    const int myrow = nv_of_lane<8>(lane);
+    for (int cs = 0; cs < ncol; cs += CS)
+    {
+        const int cend = min(ncol, cs + CS);
+        __syncthreads();
+        if (do0)
+            for (int c = cs + threadIdx.x; c < cend; c += 256) s_v[c - cs] = XS[T.in0_row + c];
+        __syncthreads();
+        for (int cc = cs + 32 * w; cc < cend; cc += 256)
+        {
+            const int c = cc + lane;
+            const bool cv = c < cend;
+            const double vc = (do0 && cv) ? s_v[c - cs] : 0.0;
+            double acc1 = 0.0;
+#pragma unroll
+            for (int gI = 0; gI < 8; gI++)
+            {
+                if (8 * gI >= R) break;
+                double a[8];
+#pragma unroll
+                for (int k = 0; k < 8; k++)
+                {
+                    const int r = 8 * gI + k;
+                    a[k] = (cv && r < R) ? to_d(A[(long long) r * ncol + c]) : 0.0;
+                }
+                double p[8];
+#pragma unroll
+                for (int k = 0; k < 8; k++)
+                {
+                    acc1 = fma(a[k], s_w[8 * gI + k], acc1);
+                    p[k] = a[k] * vc;
+                }
+                if (do0)
+                {
+                    warp_transpose_reduce<8>(p, lane);
+                    part[gI] += p[0];
+                }
+            }
+            if (do1 && cv) PS[T.out1_row + c] = acc1;
+        }
+    }
+    if (do0)
+    {
+        if (lane_writes<8>(lane))
+#pragma unroll
+            for (int gI = 0; gI < 8; gI++) s_red[w][8 * gI + myrow] = part[gI];
+        __syncthreads();
+        for (int r = threadIdx.x; r < R; r += 256)
+        {
+            double sum = 0.0;
+#pragma unroll
+            for (int k = 0; k < kWarps; k++) sum += s_red[k][r];
+            PS[T.out0_row + r] = sum;
+        }
+    }
+}
+
 // Stored block chunk for panels of NV >= 4: the R x 32 tile of A staged in shared
 // memory feeds both products, C0 = A V (accumulated over the column tiles in
 // registers) and C1 = A^T W (complete per column tile, written at once).
@@ -866,6 +944,197 @@ __global__ void __launch_bounds__(256, 4) k_jit_tc(const JitTarget* __restrict__
         }
 }
 
+// ---------------------------------------- JIT pair kernel (both directions at once)
+
+// One CTA (16 warps) per owner chunk a (<= 256 points; warp w owns rows 16w..16w+15).
+// For every partner b, source tiles of 64 points are staged as in k_jit_tc.  Per
+// group of 8 points of b each lane evaluates the 4 kernel values of its m16n8k8
+// A fragment once and uses them twice:
+//   direction a <- b:  out_a (16 rows x NV) += K (16 x 8) * in_b (8 x NV)   [A = K]
+//   direction b <- a:  out_b^T (16 RHS x 8) += in_a^T (16 RHS x 16) * K (16 x 8)
+//                      [A = in_a^T, kept in registers; B = K, transposed through a
+//                       warp-private shared tile]
+// 3xTF32 products, FP32 accumulation; the b-side partials of the 16 warps are summed
+// in shared memory per tile and written to b's slot (FP64), the a-side sums go to
+// FP64 per tile as in k_jit_tc.
+template <int KID, int NV>
+__global__ void __launch_bounds__(512, 1) k_jit_pair(const PairOwner* __restrict__ owners,
+                                                     const PairPartner* __restrict__ partners,
+                                                     const float4* __restrict__ pts, KParam kp,
+                                                     const double* __restrict__ XS, double* __restrict__ PS)
+{
+    constexpr int NT = NV / 8;
+    constexpr int TS = 64, NG = TS / 8, NW = 16;
+    constexpr int NB = NG * NT * 32 / 512 > 0 ? NG * NT * 32 / 512 : 1;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float4* s_pt = reinterpret_cast<float4*>(smem_raw);                              // [TS]
+    uint4* s_b = reinterpret_cast<uint4*>(s_pt + TS);                                // [NG][NT][32]
+    double* s_acc = reinterpret_cast<double*>(s_b + NG * NT * 32);                   // [NW][NT*4][32]
+    float* s_d2 = reinterpret_cast<float*>(s_acc + NW * NT * 4 * 32);                // [TS][NV]
+    float* s_k = s_d2 + TS * NV;                                                     // [NW][16][9]
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, tq = lane & 3;
+    const PairOwner ow = owners[blockIdx.x];
+    const float p0 = (float) kp.p0, c0 = (float) kp.c0;
+    const int i0 = warp * 16 + g, i1 = i0 + 8;
+    const bool v0 = i0 < ow.na, v1 = i1 < ow.na;
+    const bool warp_on = warp * 16 < ow.na;
+    const float4 x0 = pts[ow.pa + (v0 ? i0 : 0)], x1 = pts[ow.pa + (v1 ? i1 : 0)];
+    float* sk = s_k + warp * 16 * 9;
+
+    // in_a^T fragments (16 RHS x 8 rows of a per k-step), hi / lo
+    uint32_t ah[2][4], al[2][4];
+#pragma unroll
+    for (int ks = 0; ks < 2; ks++)
+    {
+        const int ra = warp * 16 + 8 * ks + tq, rb = ra + 4;
+        float v[4];
+        v[0] = (ra < ow.na && g < NV) ? (float) XS[(long long) (ow.in_a + ra) * NV + g] : 0.f;
+        v[1] = (ra < ow.na && g + 8 < NV) ? (float) XS[(long long) (ow.in_a + ra) * NV + g + 8] : 0.f;
+        v[2] = (rb < ow.na && g < NV) ? (float) XS[(long long) (ow.in_a + rb) * NV + g] : 0.f;
+        v[3] = (rb < ow.na && g + 8 < NV) ? (float) XS[(long long) (ow.in_a + rb) * NV + g + 8] : 0.f;
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+        {
+            ah[ks][q] = tf32_rna(v[q]);
+            al[ks][q] = __float_as_uint(v[q] - __uint_as_float(ah[ks][q]));
+        }
+    }
+    float acc[NT][4];
+#pragma unroll
+    for (int n = 0; n < NT; n++)
+#pragma unroll
+        for (int q = 0; q < 4; q++) { acc[n][q] = 0.f; s_acc[(warp * NT * 4 + n * 4 + q) * 32 + lane] = 0.0; }
+
+    for (int pi = ow.p_beg; pi < ow.p_end; pi++)
+    {
+        const PairPartner pb = partners[pi];
+        const float ax = x0.x + pb.sx, ay = x0.y + pb.sy, az = x0.z + pb.sz;
+        const float bx = x1.x + pb.sx, by = x1.y + pb.sy, bz = x1.z + pb.sz;
+        for (int j0 = 0; j0 < pb.nb; j0 += TS)
+        {
+            const int nj = min(TS, pb.nb - j0);
+            __syncthreads();
+            for (int j = threadIdx.x; j < TS; j += 512)
+                s_pt[j] = (j < nj) ? pts[pb.pb + j0 + j] : make_float4(1e6f, 1e6f, 1e6f, 0.f);
+            for (int e = threadIdx.x; e < NG * NT * 32; e += 512)
+            {
+                const int ln = e & 31, n = (e >> 5) % NT, grp = e / (32 * NT);
+                const int sa = grp * 8 + (ln & 3), sb = sa + 4, r = n * 8 + (ln >> 2);
+                const float xa = (sa < nj) ? (float) XS[(long long) (pb.in_b + j0 + sa) * NV + r] : 0.f;
+                const float xb = (sb < nj) ? (float) XS[(long long) (pb.in_b + j0 + sb) * NV + r] : 0.f;
+                const uint32_t ha = tf32_rna(xa), hb = tf32_rna(xb);
+                s_b[(grp * NT + n) * 32 + ln] =
+                    make_uint4(ha, hb, __float_as_uint(xa - __uint_as_float(ha)), __float_as_uint(xb - __uint_as_float(hb)));
+            }
+            for (int e = threadIdx.x; e < TS * NV; e += 512) s_d2[e] = 0.f;
+            __syncthreads();
+            if (warp_on)
+            {
+                const int ngrp = (nj + 7) >> 3;
+                for (int grp = 0; grp < ngrp; grp++)
+                {
+                    const float4 pa = s_pt[grp * 8 + tq], pc = s_pt[grp * 8 + tq + 4];
+                    float k[4];
+                    {
+                        float dx = ax - pa.x, dy = ay - pa.y, dz = az - pa.z;
+                        k[0] = Scalar<KID, float>::f(dx * dx + dy * dy + dz * dz, p0, c0);   // (a g,   b t)
+                        dx = bx - pa.x; dy = by - pa.y; dz = bz - pa.z;
+                        k[1] = Scalar<KID, float>::f(dx * dx + dy * dy + dz * dz, p0, c0);   // (a g+8, b t)
+                        dx = ax - pc.x; dy = ay - pc.y; dz = az - pc.z;
+                        k[2] = Scalar<KID, float>::f(dx * dx + dy * dy + dz * dz, p0, c0);   // (a g,   b t+4)
+                        dx = bx - pc.x; dy = by - pc.y; dz = bz - pc.z;
+                        k[3] = Scalar<KID, float>::f(dx * dx + dy * dy + dz * dz, p0, c0);   // (a g+8, b t+4)
+                    }
+                    // rows of a beyond the chunk contribute nothing to b
+                    if (!v0) { k[0] = 0.f; k[2] = 0.f; }
+                    if (!v1) { k[1] = 0.f; k[3] = 0.f; }
+                    uint32_t hi[4], lo[4];
+#pragma unroll
+                    for (int q = 0; q < 4; q++)
+                    {
+                        hi[q] = tf32_rna(k[q]);
+                        lo[q] = __float_as_uint(k[q] - __uint_as_float(hi[q]));
+                    }
+#pragma unroll
+                    for (int n = 0; n < NT; n++)
+                    {
+                        const uint4 b = s_b[(grp * NT + n) * 32 + lane];
+                        mma_tf32(acc[n], lo[0], lo[1], lo[2], lo[3], b.x, b.y);
+                        mma_tf32(acc[n], hi[0], hi[1], hi[2], hi[3], b.z, b.w);
+                        mma_tf32(acc[n], hi[0], hi[1], hi[2], hi[3], b.x, b.y);
+                    }
+                    // K tile (16 rows of a x 8 points of b) through shared memory, transposed
+                    sk[g * 9 + tq] = k[0];
+                    sk[(g + 8) * 9 + tq] = k[1];
+                    sk[g * 9 + tq + 4] = k[2];
+                    sk[(g + 8) * 9 + tq + 4] = k[3];
+                    __syncwarp();
+                    float kt[4];
+                    kt[0] = sk[tq * 9 + g];          // k-step 0: K[a = tq][b = g]
+                    kt[1] = sk[(tq + 4) * 9 + g];    //           K[a = tq + 4][b = g]
+                    kt[2] = sk[(tq + 8) * 9 + g];    // k-step 1: K[a = 8 + tq][b = g]
+                    kt[3] = sk[(tq + 12) * 9 + g];   //           K[a = 12 + tq][b = g]
+                    __syncwarp();
+                    uint32_t th[4], tl[4];
+#pragma unroll
+                    for (int q = 0; q < 4; q++)
+                    {
+                        th[q] = tf32_rna(kt[q]);
+                        tl[q] = __float_as_uint(kt[q] - __uint_as_float(th[q]));
+                    }
+                    float d2[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+                    for (int ks = 0; ks < 2; ks++)
+                    {
+                        mma_tf32(d2, al[ks][0], al[ks][1], al[ks][2], al[ks][3], th[2 * ks], th[2 * ks + 1]);
+                        mma_tf32(d2, ah[ks][0], ah[ks][1], ah[ks][2], ah[ks][3], tl[2 * ks], tl[2 * ks + 1]);
+                        mma_tf32(d2, ah[ks][0], ah[ks][1], ah[ks][2], ah[ks][3], th[2 * ks], th[2 * ks + 1]);
+                    }
+                    // d2: rows = RHS (g, g+8), columns = points of b (2t, 2t+1)
+                    float* row0 = s_d2 + (grp * 8 + 2 * tq) * NV;
+                    atomicAdd(row0 + g, d2[0]);
+                    atomicAdd(row0 + NV + g, d2[1]);
+                    if (NV > 8)
+                    {
+                        atomicAdd(row0 + g + 8, d2[2]);
+                        atomicAdd(row0 + NV + g + 8, d2[3]);
+                    }
+                }
+#pragma unroll
+                for (int n = 0; n < NT; n++)
+#pragma unroll
+                    for (int q = 0; q < 4; q++)
+                    {
+                        s_acc[(warp * NT * 4 + n * 4 + q) * 32 + lane] += (double) acc[n][q];
+                        acc[n][q] = 0.f;
+                    }
+            }
+            __syncthreads();
+            for (int e = threadIdx.x; e < nj * NV; e += 512)
+                PS[(long long) (pb.out_b + j0) * NV + e] = (double) s_d2[e];
+        }
+    }
+    if (warp_on)
+    {
+        double* base = PS + (long long) ow.out_a * NV;
+#pragma unroll
+        for (int n = 0; n < NT; n++)
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+            {
+                const int row = (q < 2) ? i0 : i1;
+                const bool ok = (q < 2) ? v0 : v1;
+                if (ok) base[(long long) row * NV + n * 8 + 2 * tq + (q & 1)] = s_acc[(warp * NT * 4 + n * 4 + q) * 32 + lane];
+            }
+    }
+}
+
+template <int NV>
+constexpr int pair_smem_bytes()
+{
+    return 64 * 16 + 8 * (NV / 8) * 32 * 16 + 16 * (NV / 8) * 4 * 32 * 8 + 64 * NV * 4 + 16 * 16 * 9 * 4;
+}
+
 // --------------------------------------------------------------- direct sum
 
 template <int KID, int KD>
@@ -972,6 +1241,8 @@ cudaError_t launch_blk(int NV, const BlkTask* t, int n, const TA* arena, const d
         if constexpr (NVc >= 4)
         {
             k_blk_gemm<TA, NVc><<<n, 256, 0, st>>>(t, arena, XS, PS);
+        } else if constexpr (NVc == 1) {
+            k_blk1<TA><<<n, 256, 0, st>>>(t, arena, XS, PS);
         } else {
             constexpr int b = chunk_smem_bytes<NVc>();
             cudaError_t e = allow_smem(k_blk<TA, NVc>, b);
@@ -1063,6 +1334,41 @@ cudaError_t launch_jit(int kid, int fp32, int NV, const JitTarget* tg, int n, co
                                            : launch_jit_k<KRNL_MATERN32_ID, double, 1>(NV, tg, n, sr, pts, kp, use_shift, use_tc, XS, PS, Y1, st);
         case KRNL_RPY_ID:      return fp32 ? launch_jit_k<KRNL_RPY_ID, float, 3>(NV, tg, n, sr, pts, kp, use_shift, use_tc, XS, PS, Y1, st)
                                            : launch_jit_k<KRNL_RPY_ID, double, 3>(NV, tg, n, sr, pts, kp, use_shift, use_tc, XS, PS, Y1, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+template <int KID>
+static cudaError_t launch_pair_k(int NV, const PairOwner* ow, int n, const PairPartner* pp, const float4* pts, KParam kp,
+                                 const double* XS, double* PS, cudaStream_t st)
+{
+    if (NV == 16)
+    {
+        constexpr int b = pair_smem_bytes<16>();
+        cudaError_t e = allow_smem(k_jit_pair<KID, 16>, b);
+        if (e != cudaSuccess) return e;
+        k_jit_pair<KID, 16><<<n, 512, b, st>>>(ow, pp, pts, kp, XS, PS);
+    } else if (NV == 8) {
+        constexpr int b = pair_smem_bytes<8>();
+        cudaError_t e = allow_smem(k_jit_pair<KID, 8>, b);
+        if (e != cudaSuccess) return e;
+        k_jit_pair<KID, 8><<<n, 512, b, st>>>(ow, pp, pts, kp, XS, PS);
+    } else {
+        return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pair(int kid, int NV, const PairOwner* ow, int n, const PairPartner* pp, const void* pts, KParam kp,
+                        const double* XS, double* PS, cudaStream_t st)
+{
+    if (n <= 0) return cudaSuccess;
+    const float4* p = (const float4*) pts;
+    switch (kid)
+    {
+        case KRNL_COULOMB_ID:  return launch_pair_k<KRNL_COULOMB_ID>(NV, ow, n, pp, p, kp, XS, PS, st);
+        case KRNL_GAUSSIAN_ID: return launch_pair_k<KRNL_GAUSSIAN_ID>(NV, ow, n, pp, p, kp, XS, PS, st);
+        case KRNL_MATERN32_ID: return launch_pair_k<KRNL_MATERN32_ID>(NV, ow, n, pp, p, kp, XS, PS, st);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -25,6 +25,8 @@ cudaError_t launch_asm(int NV, const AsmTask* t, int n, const int* slots, const 
                        double* Y, long long y_rs, long long y_cs, int nv, cudaStream_t st);
 cudaError_t launch_jit(int kid, int fp32, int NV, const JitTarget* tg, int n, const JitSource* sr, const void* pts,
                        KParam kp, int use_shift, int use_tc, const double* XS, double* PS, double* Y1, cudaStream_t st);
+cudaError_t launch_pair(int kid, int NV, const PairOwner* ow, int n, const PairPartner* pp, const void* pts, KParam kp,
+                        const double* XS, double* PS, cudaStream_t st);
 cudaError_t launch_direct(int kid, const double4* trg, int n_trg, const double4* src, int n_src, const double* val,
                           KParam kp, double* out, cudaStream_t st);
 

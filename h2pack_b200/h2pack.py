@@ -28,6 +28,15 @@ def _dptr(a: np.ndarray):
     return a.ctypes.data_as(_dp)
 
 
+def _stream_arg(stream=None):
+    """cudaStream_t for the C ABI: the given torch stream, else torch's current stream.
+    torch's default stream has handle 0, which the ABI reads as "the image's own stream";
+    it is passed as cudaStreamLegacy so that work is ordered with torch's default stream."""
+    import torch
+    h = stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream
+    return C.c_void_p(h if h else 0x1)
+
+
 def _kernel_id(kernel) -> int:
     return _abi.KERNEL_IDS[kernel] if isinstance(kernel, str) else int(kernel)
 
@@ -74,8 +83,7 @@ class Image:
         _abi.check(st, self.lib, "h2gpu_graph_capture")
 
     def graph_launch(self, stream=None):
-        import torch
-        s = C.c_void_p(stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream)
+        s = _stream_arg(stream)
         _abi.check(self.lib.h2gpu_graph_launch(self.handle, s), self.lib, "h2gpu_graph_launch")
 
     def autotune(self, X, Y):
@@ -114,7 +122,7 @@ class Image:
         assert X.is_cuda and X.dtype == torch.float64 and X.dim() == 2 and X.stride(1) == 1
         if Y is None:
             Y = torch.empty_like(X)
-        s = C.c_void_p(stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream)
+        s = _stream_arg(stream)
         st = self.lib.h2gpu_matmul_device(self.handle, X.shape[1], C.c_void_p(X.data_ptr()), X.stride(0),
                                           C.c_void_p(Y.data_ptr()), Y.stride(0), s)
         _abi.check(st, self.lib, "h2gpu_matmul_device")
@@ -126,7 +134,7 @@ class Image:
         import torch
         assert x.is_cuda and y.is_cuda and x.dtype == torch.float64 and y.dtype == torch.float64
         assert x.numel() == self.N and y.numel() == self.N and x.is_contiguous() and y.is_contiguous()
-        s = C.c_void_p(stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream)
+        s = _stream_arg(stream)
         st = self.lib.h2gpu_matvec_device_noalloc(self.handle, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), s)
         _abi.check(st, self.lib, "h2gpu_matvec_device_noalloc")
         return y
