@@ -45,6 +45,7 @@ def parse():
     p.add_argument("--nvec", type=int, default=16)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-fp64", action="store_true")
+    p.add_argument("--no-tune", action="store_true", help="keep the default panel width and JIT variant")
     p.add_argument("--check-rows", type=int, default=10_000)
     p.add_argument("--workload", default="jit_matern",
                    choices=["jit_matern", "aot_coulomb", "batched", "served"],
@@ -203,6 +204,7 @@ def run_ours(args):
     g = torch.Generator(device="cuda").manual_seed(7 + rank)
     X = torch.randn(N, nv, dtype=torch.float64, device="cuda", generator=g)
     Y = torch.empty_like(X)
+    tuned = img.autotune(X, Y) if not args.no_tune else None
 
     def timed(steps, warm):
         for _ in range(warm):
@@ -296,7 +298,7 @@ def run_ours(args):
                                    f"reltol 1e-6, {nv} RHS N(0,1), numerical proxy points, leaf 400",
                        "n": args.n, "nvec": nv, "parallelism": f"replicas x{world}",
                        "l2": "working set (U arena, coordinates, vectors) > 126 MB L2, no flush",
-                       "build_seconds": build_s,
+                       "build_seconds": build_s, "tuned_panel_variant": tuned,
                        "n_node": H.info["n_node"], "max_level": H.info["max_level"],
                        "jit_pairs_B": st["jit_pairs_B"], "jit_pairs_D": st["jit_pairs_D"]},
             "phase_ms": {"gather+up": phase[0], "B_far": phase[1], "down": phase[2], "D_near": phase[3],

@@ -162,6 +162,7 @@ struct h2gpu_image {
 
     // tuning (h2gpu_autotune) and captured graph (h2gpu_graph_capture)
     int jit_tc = 1;          // tensor-core JIT kernel for FP32 panels of 8 / 16
+    int jit_pair = 0;        // with jit_tc: the pair kernel (each unordered pair once)
     int tuned_nv = 0;        // panel width chosen by the autotuner (0: default rule)
     int n_images = 1;        // matrices in this image (batched images hold several)
     cudaGraph_t graph = nullptr;
@@ -954,7 +955,7 @@ int run_panel(h2gpu_image* im, int NV, int nv, const double* X, long long x_rs, 
 {
     const bool f32 = im->precision == H2GPU_PREC_MIXED;
     cudaEvent_t* e = im->ev.e;
-    if (im->has_pair && f32 && im->jit_tc && (NV == 8 || NV == 16))
+    if (im->has_pair && im->jit_pair && f32 && im->jit_tc && (NV == 8 || NV == 16))
     {
         // each unordered JIT pair evaluated once, applied both ways (tensor cores)
         const KParam kp = kparam_of(im);
@@ -1110,6 +1111,8 @@ H2G_API int h2gpu_image_create(const h2gpu_desc* desc, const h2gpu_options* opt,
     {
         const char* e = getenv("H2G_JIT_TC");
         im->jit_tc = !(e && e[0] == '0');
+        e = getenv("H2G_JIT_PAIR");
+        im->jit_pair = (e && e[0] == '1');
     }
     HostPlan hp;
     int pst = build_plan(im, desc, hp);   // all structural checks happen here, before any CUDA call
@@ -1602,14 +1605,27 @@ H2G_API int h2gpu_graph_launch(h2gpu_image* im, void* stream)
     return H2GPU_OK;
 }
 
+H2G_API int h2gpu_set_jit_variant(h2gpu_image* im, int variant)
+{
+    if (!im) return fail(H2GPU_ERR_INVALID, "image is NULL");
+    REQ(variant == H2GPU_JIT_SIMT || variant == H2GPU_JIT_TC || variant == H2GPU_JIT_PAIR, "unknown JIT variant %d",
+        variant);
+    if (variant == H2GPU_JIT_PAIR && !im->has_pair)
+        return fail(H2GPU_ERR_UNSUPPORTED, "the pair variant needs a JIT image of a scalar kernel");
+    std::lock_guard<std::mutex> lk(im->mu);
+    im->jit_tc = variant != H2GPU_JIT_SIMT;
+    im->jit_pair = variant == H2GPU_JIT_PAIR;
+    return H2GPU_OK;
+}
+
 // ================================================================= autotuner
 //
 // Times the apply of n_vec device-resident right-hand sides under each candidate
 // (panel width among 4, 8, 16 not above n_vec's panel; for FP32 JIT images the
-// tensor-core and the CUDA-core kernels) and keeps the fastest for this image.
+// CUDA-core, tensor-core and pair tensor-core kernels) and keeps the fastest.
 
 H2G_API int h2gpu_autotune(h2gpu_image* im, int n_vec, const double* dX, int ldx, double* dY, int ldy, int* best_nv,
-                           int* best_tc)
+                           int* best_variant)
 {
     if (!im) return fail(H2GPU_ERR_INVALID, "image is NULL");
     REQ(n_vec >= 1 && ldx >= n_vec && ldy >= n_vec && dX && dY, "bad autotune arguments");
@@ -1618,15 +1634,22 @@ H2G_API int h2gpu_autotune(h2gpu_image* im, int n_vec, const double* dX, int ldx
     std::vector<int> nvs;
     for (int w = 1; w <= full; w <<= 1)
         if (w == full || w >= 4) nvs.push_back(w);
-    std::vector<int> tcs = {im->jit_tc};
-    if (im->BD_JIT && im->kd == 1 && im->precision == H2GPU_PREC_MIXED) tcs = {1, 0};
+    auto variant = [&]() { return im->jit_tc ? (im->jit_pair ? H2GPU_JIT_PAIR : H2GPU_JIT_TC) : H2GPU_JIT_SIMT; };
+    std::vector<int> vars = {variant()};
+    if (im->BD_JIT && im->kd == 1 && im->precision == H2GPU_PREC_MIXED)
+    {
+        vars = {H2GPU_JIT_TC, H2GPU_JIT_SIMT};
+        if (im->has_pair) vars.push_back(H2GPU_JIT_PAIR);
+    }
     float best = 1e30f;
-    int bnv = full, btc = im->jit_tc;
+    int bnv = full, bvar = variant();
     cudaEvent_t* e = im->ev.e;
     for (int nv : nvs)
-        for (int tc : tcs)
+        for (int var : vars)
         {
-            im->jit_tc = tc;
+            if (var == H2GPU_JIT_PAIR && nv != 8 && nv != 16) continue;
+            im->jit_tc = var != H2GPU_JIT_SIMT;
+            im->jit_pair = var == H2GPU_JIT_PAIR;
             TRY(prepare(im, nv));
             float ms = 0;
             for (int rep = 0; rep < 2; rep++)
@@ -1638,11 +1661,12 @@ H2G_API int h2gpu_autotune(h2gpu_image* im, int n_vec, const double* dX, int ldx
                 CK(cudaEventSynchronize(e[6]));
                 CK(cudaEventElapsedTime(&ms, e[7], e[6]));
             }
-            if (ms < best) { best = ms; bnv = nv; btc = tc; }
+            if (ms < best) { best = ms; bnv = nv; bvar = var; }
         }
     im->tuned_nv = bnv;
-    im->jit_tc = btc;
+    im->jit_tc = bvar != H2GPU_JIT_SIMT;
+    im->jit_pair = bvar == H2GPU_JIT_PAIR;
     if (best_nv) *best_nv = bnv;
-    if (best_tc) *best_tc = btc;
+    if (best_variant) *best_variant = bvar;
     return H2GPU_OK;
 }

@@ -954,9 +954,10 @@ __global__ void __launch_bounds__(256, 4) k_jit_tc(const JitTarget* __restrict__
 //   direction b <- a:  out_b^T (16 RHS x 8) += in_a^T (16 RHS x 16) * K (16 x 8)
 //                      [A = in_a^T, kept in registers; B = K, transposed through a
 //                       warp-private shared tile]
-// 3xTF32 products, FP32 accumulation; the b-side partials of the 16 warps are summed
-// in shared memory per tile and written to b's slot (FP64), the a-side sums go to
-// FP64 per tile as in k_jit_tc.
+// 3xTF32 products, FP32 accumulation.  Each warp stores its b-side partial of a tile
+// in its own shared region; the 16 partials are then summed in warp order (fixed, so
+// the result does not depend on scheduling) and written to b's slot (FP64).  The
+// a-side sums go to FP64 per tile as in k_jit_tc.
 template <int KID, int NV>
 __global__ void __launch_bounds__(512, 1) k_jit_pair(const PairOwner* __restrict__ owners,
                                                      const PairPartner* __restrict__ partners,
@@ -965,19 +966,20 @@ __global__ void __launch_bounds__(512, 1) k_jit_pair(const PairOwner* __restrict
 {
     constexpr int NT = NV / 8;
     constexpr int TS = 64, NG = TS / 8, NW = 16;
-    constexpr int NB = NG * NT * 32 / 512 > 0 ? NG * NT * 32 / 512 : 1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float4* s_pt = reinterpret_cast<float4*>(smem_raw);                              // [TS]
     uint4* s_b = reinterpret_cast<uint4*>(s_pt + TS);                                // [NG][NT][32]
     double* s_acc = reinterpret_cast<double*>(s_b + NG * NT * 32);                   // [NW][NT*4][32]
-    float* s_d2 = reinterpret_cast<float*>(s_acc + NW * NT * 4 * 32);                // [TS][NV]
-    float* s_k = s_d2 + TS * NV;                                                     // [NW][16][9]
+    float* s_d2 = reinterpret_cast<float*>(s_acc + NW * NT * 4 * 32);                // [NW][TS][NV]
+    float* s_k = s_d2 + NW * TS * NV;                                                // [NW][16][9]
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, tq = lane & 3;
     const PairOwner ow = owners[blockIdx.x];
     const float p0 = (float) kp.p0, c0 = (float) kp.c0;
     const int i0 = warp * 16 + g, i1 = i0 + 8;
     const bool v0 = i0 < ow.na, v1 = i1 < ow.na;
     const bool warp_on = warp * 16 < ow.na;
+    const int n_on = (ow.na + 15) >> 4;
+    float* d2w = s_d2 + warp * TS * NV;
     const float4 x0 = pts[ow.pa + (v0 ? i0 : 0)], x1 = pts[ow.pa + (v1 ? i1 : 0)];
     float* sk = s_k + warp * 16 * 9;
 
@@ -1026,7 +1028,6 @@ __global__ void __launch_bounds__(512, 1) k_jit_pair(const PairOwner* __restrict
                 s_b[(grp * NT + n) * 32 + ln] =
                     make_uint4(ha, hb, __float_as_uint(xa - __uint_as_float(ha)), __float_as_uint(xb - __uint_as_float(hb)));
             }
-            for (int e = threadIdx.x; e < TS * NV; e += 512) s_d2[e] = 0.f;
             __syncthreads();
             if (warp_on)
             {
@@ -1091,13 +1092,13 @@ __global__ void __launch_bounds__(512, 1) k_jit_pair(const PairOwner* __restrict
                         mma_tf32(d2, ah[ks][0], ah[ks][1], ah[ks][2], ah[ks][3], th[2 * ks], th[2 * ks + 1]);
                     }
                     // d2: rows = RHS (g, g+8), columns = points of b (2t, 2t+1)
-                    float* row0 = s_d2 + (grp * 8 + 2 * tq) * NV;
-                    atomicAdd(row0 + g, d2[0]);
-                    atomicAdd(row0 + NV + g, d2[1]);
+                    float* row0 = d2w + (grp * 8 + 2 * tq) * NV;
+                    row0[g] = d2[0];
+                    row0[NV + g] = d2[1];
                     if (NV > 8)
                     {
-                        atomicAdd(row0 + g + 8, d2[2]);
-                        atomicAdd(row0 + NV + g + 8, d2[3]);
+                        row0[g + 8] = d2[2];
+                        row0[NV + g + 8] = d2[3];
                     }
                 }
 #pragma unroll
@@ -1111,7 +1112,11 @@ __global__ void __launch_bounds__(512, 1) k_jit_pair(const PairOwner* __restrict
             }
             __syncthreads();
             for (int e = threadIdx.x; e < nj * NV; e += 512)
-                PS[(long long) (pb.out_b + j0) * NV + e] = (double) s_d2[e];
+            {
+                float t = 0.f;
+                for (int w = 0; w < n_on; w++) t += s_d2[w * TS * NV + e];
+                PS[(long long) (pb.out_b + j0) * NV + e] = (double) t;
+            }
         }
     }
     if (warp_on)
@@ -1132,7 +1137,7 @@ __global__ void __launch_bounds__(512, 1) k_jit_pair(const PairOwner* __restrict
 template <int NV>
 constexpr int pair_smem_bytes()
 {
-    return 64 * 16 + 8 * (NV / 8) * 32 * 16 + 16 * (NV / 8) * 4 * 32 * 8 + 64 * NV * 4 + 16 * 16 * 9 * 4;
+    return 64 * 16 + 8 * (NV / 8) * 32 * 16 + 16 * (NV / 8) * 4 * 32 * 8 + 16 * 64 * NV * 4 + 16 * 16 * 9 * 4;
 }
 
 // --------------------------------------------------------------- direct sum

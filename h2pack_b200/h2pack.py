@@ -86,13 +86,19 @@ class Image:
         s = _stream_arg(stream)
         _abi.check(self.lib.h2gpu_graph_launch(self.handle, s), self.lib, "h2gpu_graph_launch")
 
+    def set_jit_variant(self, variant: str):
+        """FP32 JIT kernel variant: "simt", "tc" (default) or "pair"."""
+        code = {"simt": _abi.JIT_SIMT, "tc": _abi.JIT_TC, "pair": _abi.JIT_PAIR}[variant]
+        _abi.check(self.lib.h2gpu_set_jit_variant(self.handle, code), self.lib, "h2gpu_set_jit_variant")
+
     def autotune(self, X, Y):
-        """Pick the panel width (and JIT kernel variant) that applies X fastest; returns (nv, tensor_cores)."""
-        nv, tc = C.c_int(), C.c_int()
+        """Pick the panel width and JIT kernel variant that apply X fastest; returns
+        (nv, variant) with variant one of "simt", "tc", "pair"."""
+        nv, var = C.c_int(), C.c_int()
         st = self.lib.h2gpu_autotune(self.handle, X.shape[1], C.c_void_p(X.data_ptr()), X.stride(0),
-                                     C.c_void_p(Y.data_ptr()), Y.stride(0), C.byref(nv), C.byref(tc))
+                                     C.c_void_p(Y.data_ptr()), Y.stride(0), C.byref(nv), C.byref(var))
         _abi.check(st, self.lib, "h2gpu_autotune")
-        return nv.value, bool(tc.value)
+        return nv.value, ("simt", "tc", "pair")[var.value]
 
     def matvec(self, x: np.ndarray) -> np.ndarray:
         x = np.ascontiguousarray(x, dtype=np.float64)

@@ -217,11 +217,27 @@ int h2gpu_graph_launch(h2gpu_image *img, void *stream);
 
 /*
  * Autotuner: time the device apply of n_vec right-hand sides for each candidate
- * panel width (and, for FP32 JIT images, tensor-core vs CUDA-core kernel) and keep
- * the fastest for this image.  dY is overwritten.  No counterpart in the reference.
+ * panel width and, for FP32 JIT images, each JIT kernel variant, and keep the
+ * fastest for this image.  dY is overwritten.  *best_variant receives
+ * H2GPU_JIT_SIMT (CUDA cores), H2GPU_JIT_TC (tensor cores, every target evaluates
+ * its own sources) or H2GPU_JIT_PAIR (tensor cores, each unordered pair of leaves /
+ * nodes evaluated once and applied in both directions).  No counterpart in the
+ * reference.
  */
+#define H2GPU_JIT_SIMT 0
+#define H2GPU_JIT_TC   1
+#define H2GPU_JIT_PAIR 2
 int h2gpu_autotune(h2gpu_image *img, int n_vec, const double *dX, int ldx, double *dY, int ldy,
-                   int *best_nv, int *best_tc);
+                   int *best_nv, int *best_variant);
+
+/*
+ * Select the JIT kernel variant used by FP32 panels of JIT images (H2GPU_JIT_SIMT,
+ * H2GPU_JIT_TC (default) or H2GPU_JIT_PAIR; the pair variant needs a scalar kernel
+ * and applies to panels of 8 or 16 right-hand sides, others use H2GPU_JIT_TC).
+ * FP64 panels always use the CUDA-core kernel; a captured graph keeps the variant it
+ * was captured with.  No counterpart in the reference.
+ */
+int h2gpu_set_jit_variant(h2gpu_image *img, int variant);
 
 int h2gpu_get_stats(h2gpu_image *img, h2gpu_stats *st);
 int h2gpu_reset_stats(h2gpu_image *img);
