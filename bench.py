@@ -48,9 +48,10 @@ def parse():
     p.add_argument("--no-tune", action="store_true", help="keep the default panel width and JIT variant")
     p.add_argument("--check-rows", type=int, default=10_000)
     p.add_argument("--workload", default="jit_matern",
-                   choices=["jit_matern", "aot_coulomb", "batched", "served"],
+                   choices=["jit_matern", "aot_coulomb", "aot_rpy", "batched", "served"],
                    help="jit_matern: the headline configuration; the others print extra lines for the "
-                        "other configurations (AOT Coulomb matvec, batched matrices, served requests)")
+                        "other configurations (AOT Coulomb matvec, AOT RPY matmul, batched matrices, "
+                        "served requests)")
     p.add_argument("--n-matrices", type=int, default=64)
     p.add_argument("--n-requests", type=int, default=96)
     return p.parse_args()
@@ -402,6 +403,85 @@ def run_aot_coulomb(args):
     H.close()
 
 
+def run_aot_rpy(args):
+    """RPY 3x3 tensor kernel (a = 1, eta = 1/(6 pi), so C = 1), particles uniform in a cube
+    sized for volume fraction 0.1, reltol 1e-8, stored U/B/D, 64 RHS forces N(0,1); matmul in
+    panels of 16.  The N = 500,000 case needs about 200 GB of FP64 B blocks at this tolerance
+    (25.4 GB measured at N = 50,000 with 512 leaves; 4096 leaves at 500,000), more than one
+    GPU holds, so the default N is the largest tested size whose FP64 image and FP32 copy fit.
+    value = right-hand-side matvecs/s of the mixed (FP32 stored blocks) matmul."""
+    import torch
+    from h2pack_b200 import H2Matrix, direct_sum
+    n = 100_000 if args.n == 1_000_000 else args.n
+    nv = 64
+    rng = np.random.default_rng(31)
+    L = (n * 4.0 * np.pi / 3.0 / 0.1) ** (1.0 / 3.0)
+    coord = np.vstack([rng.random((3, n)) * L, np.ones((1, n))])
+    eta = 1.0 / (6.0 * np.pi)
+    t0 = time.time()
+    H = H2Matrix("rpy", coord, [eta], 1e-8, BD_JIT=0, max_leaf_points=300, max_leaf_size=4.0, proxy="surface",
+                 n_thread=os.cpu_count())
+    build_s = time.time() - t0
+    img = H.image()
+    g = torch.Generator(device="cuda").manual_seed(5)
+    X = torch.randn(H.N, nv, dtype=torch.float64, device="cuda", generator=g)
+    Y = torch.empty_like(X)
+    out, Ys = {}, {}
+    for prec in ("fp64", "mixed"):
+        H.set_precision(prec)
+        s0 = img.stats()
+        ms = timed_loop(lambda: img.matmul_device(X, Y), args.steps, args.warmup)
+        s1 = img.stats()
+        ph = [(b - a) / (args.steps + args.warmup) for a, b in zip(s0["ms_phase"], s1["ms_phase"])]
+        st = img.stats()
+        # bytes of the current precision's copies; U counted twice (upward and downward sweep)
+        stored = st["bytes_U"] + st["bytes_B"] + st["bytes_D"]
+        panels = (nv + 15) // 16
+        entries = (st["bytes_U"] / 2 + st["bytes_B"] + st["bytes_D"]) / (8.0 if prec == "fp64" else 4.0)
+        out[prec] = {"ms": ms, "matvecs_per_s": nv * 1e3 / ms, "phase_ms": ph, "stored_bytes": stored,
+                     "streamed_GBps": panels * stored / (ms * 1e-3) / 1e9,
+                     "model_TFs": 2.0 * nv * 2 * entries / (ms * 1e-3) / 1e12}
+        Ys[prec] = Y.clone()
+    # error of both paths against the FP64 direct sum on sampled points (3 rows each)
+    m = min(args.check_rows // 3 if args.check_rows else 0, n)
+    err = {}
+    if m > 0:
+        pts = np.sort(rng.choice(n, m, replace=False))
+        rows = (3 * pts[:, None] + np.arange(3)[None, :]).ravel()
+        Xc = X.cpu().numpy()
+        for prec in ("fp64", "mixed"):
+            e = []
+            for c in (0, nv // 2):
+                yd = direct_sum("rpy", [eta], coord, Xc[:, c], coord[:, pts])
+                yc = Ys[prec][:, c].cpu().numpy()[rows]
+                e.append(float(np.linalg.norm(yc - yd) / np.linalg.norm(yd)))
+            err[prec] = max(e)
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+        from h2pack_b200 import _abi
+        Xh = np.ascontiguousarray(X.cpu().numpy())
+        Yh = np.zeros_like(Xh)
+        t = time.perf_counter()
+        O.libref().H2P_matmul(H.h2pack, _abi.ROW_MAJOR, nv, O.dptr(Xh), nv, O.dptr(Yh), nv)
+        sec = time.perf_counter() - t
+        cpu = {"value": nv / sec, "unit": "matvecs/s", "cores": H.info["n_thread"], "kind": "reference",
+               "sample": f"1 H2P_matmul ({nv} RHS) of H2Pack compiled from its sources, same handle, {sec:.1f} s"}
+    peak = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]) \
+        if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else 6650.0
+    line = {"metric": f"H2 matvecs/s (RPY N={n} AOT, reltol 1e-8, {nv} RHS)", "value": out["mixed"]["matvecs_per_s"],
+            "unit": "matvecs/s", "workload": "aot_rpy", "n": n, "nvec": nv, "build_seconds": build_s,
+            "fp64": out["fp64"], "mixed": out["mixed"], "rel_err_vs_direct": err,
+            "speedup_mixed_vs_fp64": out["fp64"]["ms"] / out["mixed"]["ms"],
+            "roofline": {"bound": "hbm", "achieved": out["mixed"]["streamed_GBps"], "peak": peak, "unit": "GB/s",
+                         "frac": out["mixed"]["streamed_GBps"] / peak,
+                         "note": "stored FP32 U (read twice), B, D bytes x 16-RHS panels per matmul / matmul "
+                                 "time, of measured copy BW"},
+            "cpu_baseline": cpu, "info": H.info}
+    print(json.dumps(line), flush=True)
+    H.close()
+
+
 def log_uniform(rng, lo, hi, k):
     return np.exp(rng.uniform(np.log(lo), np.log(hi), k)).astype(int)
 
@@ -514,6 +594,8 @@ def main():
         run_reference(args)
     elif args.workload == "aot_coulomb":
         run_aot_coulomb(args)
+    elif args.workload == "aot_rpy":
+        run_aot_rpy(args)
     elif args.workload == "batched":
         run_batched(args)
     elif args.workload == "served":

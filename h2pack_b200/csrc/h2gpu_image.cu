@@ -163,6 +163,7 @@ struct h2gpu_image {
     // tuning (h2gpu_autotune) and captured graph (h2gpu_graph_capture)
     int jit_tc = 1;          // tensor-core JIT kernel for FP32 panels of 8 / 16
     int jit_pair = 0;        // with jit_tc: the pair kernel (each unordered pair once)
+    int blk_tc = 1;          // tensor-core stored-block kernel for FP32 panels of 8 / 16
     int tuned_nv = 0;        // panel width chosen by the autotuner (0: default rule)
     int n_images = 1;        // matrices in this image (batched images hold several)
     cudaGraph_t graph = nullptr;
@@ -615,34 +616,53 @@ int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
                 int o = choose(a, b, (double) npt_of(d, a) * npt_of(d, b));
                 npart[o].push_back(o == a ? b : a);
             }
-            const int PCH = 256;
+            // Work units: a chunk of <= 128 points of the owner a (one CTA's rows) and a
+            // run of its partners whose work na * sum(nb) stays under a cap sized for
+            // about 12 units per SM (148 SMs x 3 CTAs x 4 waves), so the largest owners
+            // do not leave a tail.  Every unit has its own slot for a's side and one per
+            // partner for b's side.
+            const int PCH = 128;
+            double w_total = 0.0;
+            for (int n = 0; n < n_node; n++)
+            {
+                for (int b : fpart[n]) w_total += (double) d->J_n[n] * d->J_n[b];
+                for (int b : npart[n]) w_total += (double) npt_of(d, n) * npt_of(d, b);
+            }
+            const double w_cap = std::max(w_total / (148.0 * 3 * 4), 128.0 * 512.0);
             auto emit_owner = [&](std::vector<PairOwner>& out, int a, bool isJ, const std::vector<int>& parts,
                                   std::vector<std::vector<int>>& lists) {
-                int na = isJ ? d->J_n[a] : npt_of(d, a);
-                int pa = isJ ? jp0[a] : d->pt_cluster[2 * a];
-                int in_a = isJ ? N + y0r[a] : mc[2 * a];
-                int slot_a = alloc(na);
-                lists[a].push_back(slot_a);
-                for (int c0 = 0; c0 < na; c0 += PCH)
+                const int na_all = isJ ? d->J_n[a] : npt_of(d, a);
+                const int pa = isJ ? jp0[a] : d->pt_cluster[2 * a];
+                const int in_a = isJ ? N + y0r[a] : mc[2 * a];
+                for (int c0 = 0; c0 < na_all; c0 += PCH)
                 {
-                    PairOwner ow;
-                    ow.pa = pa + c0; ow.na = std::min(PCH, na - c0); ow.in_a = in_a + c0; ow.out_a = slot_a + c0;
-                    ow.p_beg = (int) hp.partners.size();
-                    for (int b : parts)
+                    const int na = std::min(PCH, na_all - c0);
+                    size_t k = 0;
+                    while (k < parts.size())
                     {
-                        PairPartner pp;
-                        pp.pb = isJ ? jp0[b] : d->pt_cluster[2 * b];
-                        pp.nb = isJ ? d->J_n[b] : npt_of(d, b);
-                        pp.in_b = isJ ? N + y0r[b] : mc[2 * b];
-                        pp.out_b = alloc(pp.nb);
-                        lists[b].push_back(pp.out_b);
-                        pp.sx = (float) (ctr[3 * a] - ctr[3 * b]);
-                        pp.sy = (float) (ctr[3 * a + 1] - ctr[3 * b + 1]);
-                        pp.sz = (float) (ctr[3 * a + 2] - ctr[3 * b + 2]);
-                        hp.partners.push_back(pp);
+                        PairOwner ow;
+                        ow.na = na; ow.pa = pa + c0; ow.in_a = in_a + c0;
+                        ow.out_a = alloc(na);
+                        lists[a].push_back(ow.out_a);
+                        ow.p_beg = (int) hp.partners.size();
+                        double w = 0.0;
+                        do {
+                            const int b = parts[k++];
+                            PairPartner pp;
+                            pp.pb = isJ ? jp0[b] : d->pt_cluster[2 * b];
+                            pp.nb = isJ ? d->J_n[b] : npt_of(d, b);
+                            pp.in_b = isJ ? N + y0r[b] : mc[2 * b];
+                            pp.out_b = alloc(pp.nb);
+                            lists[b].push_back(pp.out_b);
+                            pp.sx = (float) (ctr[3 * a] - ctr[3 * b]);
+                            pp.sy = (float) (ctr[3 * a + 1] - ctr[3 * b + 1]);
+                            pp.sz = (float) (ctr[3 * a + 2] - ctr[3 * b + 2]);
+                            hp.partners.push_back(pp);
+                            w += (double) na * pp.nb;
+                        } while (k < parts.size() && w < w_cap);
+                        ow.p_end = (int) hp.partners.size();
+                        out.push_back(ow);
                     }
-                    ow.p_end = (int) hp.partners.size();
-                    out.push_back(ow);
                 }
             };
             for (int n = 0; n < n_node; n++)
@@ -974,7 +994,7 @@ int run_panel(h2gpu_image* im, int NV, int nv, const double* X, long long x_rs, 
         if (timed) CK(cudaEventRecord(e[3], s));
         CK(launch_pair(im->kernel_id, NV, im->d_owF, im->n_owF, im->d_pp, im->d_pts32, kp, im->d_XS, im->d_PS, s));
         CK(launch_jit(im->kernel_id, 1, NV, im->d_jtF2, im->n_jtF2, im->d_js, im->d_pts32, kp, 1, 1, im->d_XS,
-                      im->d_PS, im->d_Y1, s));
+                      im->d_PS, im->d_Y1, s, 1));
         CK(launch_y1sum(NV, im->d_y1t2, im->n_y12, im->d_y1_slots2, im->d_PS, im->d_Y1, s));
         if (timed) CK(cudaEventRecord(e[4], s));
         for (size_t L = 0; L + 1 < im->dn_beg.size(); L++)
@@ -994,7 +1014,7 @@ int run_panel(h2gpu_image* im, int NV, int nv, const double* X, long long x_rs, 
     if (timed) CK(cudaEventRecord(e[1], s));
     if (!im->BD_JIT)
     {
-        if (f32) CK(launch_blk<float>(NV, im->d_blkD, im->n_blkD, im->d_D32, im->d_XS, im->d_PS, s));
+        if (f32) CK(launch_blk<float>(NV, im->d_blkD, im->n_blkD, im->d_D32, im->d_XS, im->d_PS, s, im->blk_tc));
         else CK(launch_blk<double>(NV, im->d_blkD, im->n_blkD, im->d_D64, im->d_XS, im->d_PS, s));
     } else {
         CK(launch_jit(im->kernel_id, f32, NV, im->d_jtN, im->n_jtN, im->d_js, f32 ? (const void*) im->d_pts32 : (const void*) im->d_pts64,
@@ -1010,12 +1030,12 @@ int run_panel(h2gpu_image* im, int NV, int nv, const double* X, long long x_rs, 
     if (timed) CK(cudaEventRecord(e[3], s));
     if (!im->BD_JIT)
     {
-        if (f32) CK(launch_blk<float>(NV, im->d_blkB, im->n_blkB, im->d_B32, im->d_XS, im->d_PS, s));
+        if (f32) CK(launch_blk<float>(NV, im->d_blkB, im->n_blkB, im->d_B32, im->d_XS, im->d_PS, s, im->blk_tc));
         else CK(launch_blk<double>(NV, im->d_blkB, im->n_blkB, im->d_B64, im->d_XS, im->d_PS, s));
         CK(launch_y1sum(NV, im->d_y1t, im->n_y1, im->d_y1_slots, im->d_PS, im->d_Y1, s));
     } else {
         CK(launch_jit(im->kernel_id, f32, NV, im->d_jtF, im->n_jtF, im->d_js, f32 ? (const void*) im->d_pts32 : (const void*) im->d_pts64,
-                      kparam_of(im), f32 ? 1 : 0, im->jit_tc, im->d_XS, im->d_PS, im->d_Y1, s));
+                      kparam_of(im), f32 ? 1 : 0, im->jit_tc, im->d_XS, im->d_PS, im->d_Y1, s, 1));
     }
     if (timed) CK(cudaEventRecord(e[4], s));
     for (size_t L = 0; L + 1 < im->dn_beg.size(); L++)
@@ -1113,6 +1133,8 @@ H2G_API int h2gpu_image_create(const h2gpu_desc* desc, const h2gpu_options* opt,
         im->jit_tc = !(e && e[0] == '0');
         e = getenv("H2G_JIT_PAIR");
         im->jit_pair = (e && e[0] == '1');
+        e = getenv("H2G_BLK_TC");
+        im->blk_tc = !(e && e[0] == '0');
     }
     HostPlan hp;
     int pst = build_plan(im, desc, hp);   // all structural checks happen here, before any CUDA call
@@ -1615,6 +1637,7 @@ H2G_API int h2gpu_set_jit_variant(h2gpu_image* im, int variant)
     std::lock_guard<std::mutex> lk(im->mu);
     im->jit_tc = variant != H2GPU_JIT_SIMT;
     im->jit_pair = variant == H2GPU_JIT_PAIR;
+    im->blk_tc = variant != H2GPU_JIT_SIMT;
     return H2GPU_OK;
 }
 
@@ -1634,12 +1657,15 @@ H2G_API int h2gpu_autotune(h2gpu_image* im, int n_vec, const double* dX, int ldx
     std::vector<int> nvs;
     for (int w = 1; w <= full; w <<= 1)
         if (w == full || w >= 4) nvs.push_back(w);
-    auto variant = [&]() { return im->jit_tc ? (im->jit_pair ? H2GPU_JIT_PAIR : H2GPU_JIT_TC) : H2GPU_JIT_SIMT; };
+    auto variant = [&]() {
+        if (!im->BD_JIT) return im->blk_tc ? H2GPU_JIT_TC : H2GPU_JIT_SIMT;
+        return im->jit_tc ? (im->jit_pair ? H2GPU_JIT_PAIR : H2GPU_JIT_TC) : H2GPU_JIT_SIMT;
+    };
     std::vector<int> vars = {variant()};
-    if (im->BD_JIT && im->kd == 1 && im->precision == H2GPU_PREC_MIXED)
+    if (im->precision == H2GPU_PREC_MIXED && (!im->BD_JIT || im->kd == 1))
     {
         vars = {H2GPU_JIT_TC, H2GPU_JIT_SIMT};
-        if (im->has_pair) vars.push_back(H2GPU_JIT_PAIR);
+        if (im->BD_JIT && im->has_pair) vars.push_back(H2GPU_JIT_PAIR);
     }
     float best = 1e30f;
     int bnv = full, bvar = variant();
@@ -1650,6 +1676,7 @@ H2G_API int h2gpu_autotune(h2gpu_image* im, int n_vec, const double* dX, int ldx
             if (var == H2GPU_JIT_PAIR && nv != 8 && nv != 16) continue;
             im->jit_tc = var != H2GPU_JIT_SIMT;
             im->jit_pair = var == H2GPU_JIT_PAIR;
+            im->blk_tc = var != H2GPU_JIT_SIMT;
             TRY(prepare(im, nv));
             float ms = 0;
             for (int rep = 0; rep < 2; rep++)
@@ -1666,6 +1693,7 @@ H2G_API int h2gpu_autotune(h2gpu_image* im, int n_vec, const double* dX, int ldx
     im->tuned_nv = bnv;
     im->jit_tc = bvar != H2GPU_JIT_SIMT;
     im->jit_pair = bvar == H2GPU_JIT_PAIR;
+    im->blk_tc = bvar != H2GPU_JIT_SIMT;
     if (best_nv) *best_nv = bnv;
     if (best_variant) *best_variant = bvar;
     return H2GPU_OK;

@@ -77,15 +77,15 @@ struct JitSource {
 // is evaluated once and applied both ways.  One record per chunk of <= 256 points of
 // an owner set a, with the list of its partners b.
 struct PairOwner {
-    int pa, na;          // point-space range of this chunk of a
-    int in_a;            // XS row of y0 / x of the chunk's first point
-    int out_a;           // PS row of the chunk's first output row (sum over all partners)
+    int pa, na;          // point-space range of a
+    int in_a;            // XS row of y0 / x of a's first point
+    int out_a;           // PS row of a's first output row (sum over all partners)
     int p_beg, p_end;    // partner range
 };
 struct PairPartner {
     int pb, nb;          // point-space range of b
     int in_b;            // XS row of b's input
-    int out_b;           // PS row of b's output slot (this chunk of a only)
+    int out_b;           // PS row of b's output slot (its pair with this owner only)
     float sx, sy, sz;    // center(a) - center(b)
 };
 

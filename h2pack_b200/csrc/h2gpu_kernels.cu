@@ -357,14 +357,17 @@ __device__ __forceinline__ void chunk_apply(const TA* __restrict__ A, int R, int
 }
 
 // Stored block chunk, single right-hand side (the matvec path, memory bound).
-// Warp w owns columns 32w + lane (+256k) and walks all rows of the chunk 8 at a time:
-// 8 independent loads per lane in flight, A^T w completes in registers (no reduction),
-// and the 8 row partials of A v are combined with one transposed butterfly per
-// 8 x 32 tile; the warps' row partials are summed once at the end.
+// Warp w owns columns CPL*32*w + lane + 32j (j < CPL, +CPL*256k) and walks all rows
+// of the chunk 8 at a time: 8*CPL independent loads per lane in flight (CPL = 2 for
+// FP32 blocks, so both precisions keep the same bytes in flight), A^T w completes in
+// registers (no reduction), and the 8 row partials of A v are combined with one
+// transposed butterfly per 8 x 32*CPL tile; the warps' row partials are summed once
+// at the end.
 template <typename TA>
-__global__ void __launch_bounds__(256) k_blk1(const BlkTask* __restrict__ tasks, const TA* __restrict__ arena,
+__global__ void __launch_bounds__(256, sizeof(TA) == 4 ? 3 : 4) k_blk1(const BlkTask* __restrict__ tasks, const TA* __restrict__ arena,
                                               const double* __restrict__ XS, double* __restrict__ PS)
 {
+    constexpr int CPL = sizeof(TA) == 4 ? 2 : 1;
     constexpr int CS = 1024;
     __shared__ double s_v[CS];
     __shared__ double s_w[64];
@@ -385,29 +388,44 @@ __global__ void __launch_bounds__(256) k_blk1(const BlkTask* __restrict__ tasks,
         if (do0)
             for (int c = cs + threadIdx.x; c < cend; c += 256) s_v[c - cs] = XS[T.in0_row + c];
         __syncthreads();
-        for (int cc = cs + 32 * w; cc < cend; cc += 256)
+        for (int cc = cs + 32 * CPL * w; cc < cend; cc += 256 * CPL)
         {
-            const int c = cc + lane;
-            const bool cv = c < cend;
-            const double vc = (do0 && cv) ? s_v[c - cs] : 0.0;
-            double acc1 = 0.0;
+            int c[CPL];
+            bool cv[CPL];
+            double vc[CPL], acc1[CPL];
+#pragma unroll
+            for (int j = 0; j < CPL; j++)
+            {
+                c[j] = cc + lane + 32 * j;
+                cv[j] = c[j] < cend;
+                vc[j] = (do0 && cv[j]) ? s_v[c[j] - cs] : 0.0;
+                acc1[j] = 0.0;
+            }
 #pragma unroll
             for (int gI = 0; gI < 8; gI++)
             {
                 if (8 * gI >= R) break;
-                double a[8];
+                TA a[CPL][8];            // raw loads in flight, widened at use
 #pragma unroll
-                for (int k = 0; k < 8; k++)
-                {
-                    const int r = 8 * gI + k;
-                    a[k] = (cv && r < R) ? to_d(A[(long long) r * ncol + c]) : 0.0;
-                }
+                for (int j = 0; j < CPL; j++)
+#pragma unroll
+                    for (int k = 0; k < 8; k++)
+                    {
+                        const int r = 8 * gI + k;
+                        a[j][k] = (cv[j] && r < R) ? A[(long long) r * ncol + c[j]] : TA(0);
+                    }
                 double p[8];
 #pragma unroll
                 for (int k = 0; k < 8; k++)
                 {
-                    acc1 = fma(a[k], s_w[8 * gI + k], acc1);
-                    p[k] = a[k] * vc;
+                    p[k] = 0.0;
+#pragma unroll
+                    for (int j = 0; j < CPL; j++)
+                    {
+                        const double ad = to_d(a[j][k]);
+                        acc1[j] = fma(ad, s_w[8 * gI + k], acc1[j]);
+                        p[k] = fma(ad, vc[j], p[k]);
+                    }
                 }
                 if (do0)
                 {
@@ -415,7 +433,9 @@ __global__ void __launch_bounds__(256) k_blk1(const BlkTask* __restrict__ tasks,
                     part[gI] += p[0];
                 }
             }
-            if (do1 && cv) PS[T.out1_row + c] = acc1;
+#pragma unroll
+            for (int j = 0; j < CPL; j++)
+                if (do1 && cv[j]) PS[T.out1_row + c[j]] = acc1[j];
         }
     }
     if (do0)
@@ -624,6 +644,27 @@ template <> struct Scalar<KRNL_MATERN32_ID, float> {
     }
 };
 
+// FP32 kernel values for admissible (well-separated) pairs only: r2 > 0 always, so the
+// coincident-point cases drop out; constants are folded once per launch (prep).
+template <int KID> struct ScalarFar;
+template <> struct ScalarFar<KRNL_COULOMB_ID> {
+    static __device__ __forceinline__ void prep(float, float, float& q0, float& q1) { q0 = 0.f; q1 = 0.f; }
+    static __device__ __forceinline__ float f(float r2, float, float) { return rsqrt_approx(r2); }
+};
+template <> struct ScalarFar<KRNL_GAUSSIAN_ID> {
+    static __device__ __forceinline__ void prep(float p0, float, float& q0, float& q1) { q0 = -p0 * kLog2e; q1 = 0.f; }
+    static __device__ __forceinline__ float f(float r2, float q0, float) { return ex2_approx(r2 * q0); }
+};
+template <> struct ScalarFar<KRNL_MATERN32_ID> {
+    static __device__ __forceinline__ void prep(float, float c0, float& q0, float& q1) { q0 = c0; q1 = c0 * kLog2e; }
+    static __device__ __forceinline__ float f(float r2, float q0, float q1)
+    {
+        const float r = r2 * rsqrt_approx(r2);
+        const float e = ex2_approx(q1 * r);
+        return fmaf(-q0 * r, e, e);
+    }
+};
+
 // RPY 3x3 block: K_ab = t2 u_a u_b + t1 delta_ab, u = (dx,dy,dz)/r (0 at r = 0)
 template <typename T>
 __device__ __forceinline__ void rpy_coef(T dx, T dy, T dz, T ta, T sa, T C, T& t1, T& t2, T& ux, T& uy, T& uz)
@@ -796,7 +837,7 @@ __device__ __forceinline__ uint32_t tf32_rna(float x)
 __device__ __forceinline__ void mma_tf32(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
                                          uint32_t b0, uint32_t b1)
 {
-    asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+    asm("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
                  : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
                  : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
@@ -808,7 +849,11 @@ __device__ __forceinline__ void mma_tf32(float (&d)[4], uint32_t a0, uint32_t a1
 // splits them into TF32 hi/lo and issues 3 MMAs per 8-RHS n-tile against the
 // sources' inputs, which are staged in shared memory already split and in B-fragment
 // order.  FP32 accumulation per 64-source tile, FP64 sums across tiles.
-template <int KID, int NV>
+// FAR (admissible pairs only): r^2 = |a|^2 + |b|^2 - 2 a.b with a the target in the
+// source set's frame (|a|^2 and -2a once per tile, |b|^2 staged in the point's w):
+// 4 instructions instead of 6.  Admissible boxes keep r above the box size, so the
+// cancellation stays at a few FP32 ulps of r^2 (the near field keeps differences).
+template <int KID, int NV, bool FAR>
 __global__ void __launch_bounds__(256, 4) k_jit_tc(const JitTarget* __restrict__ tgts, const JitSource* __restrict__ srcs,
                                                    const float4* __restrict__ pts, KParam kp,
                                                    const double* __restrict__ XS, double* __restrict__ PS,
@@ -825,6 +870,8 @@ __global__ void __launch_bounds__(256, 4) k_jit_tc(const JitTarget* __restrict__
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, tq = lane & 3;
     const JitTarget tg = tgts[blockIdx.x];
     const float p0 = (float) kp.p0, c0 = (float) kp.c0;
+    float q0 = 0.f, q1 = 0.f;
+    if constexpr (FAR) ScalarFar<KID>::prep(p0, c0, q0, q1);
     const int i0 = warp * 16 + g, i1 = i0 + 8;
     const bool v0 = i0 < tg.npt, v1 = i1 < tg.npt;
     const float4 x0 = pts[tg.pt0 + (v0 ? i0 : 0)], x1 = pts[tg.pt0 + (v1 ? i1 : 0)];
@@ -855,7 +902,12 @@ __global__ void __launch_bounds__(256, 4) k_jit_tc(const JitTarget* __restrict__
         }
     };
     auto store_tile = [&](int buf) {
-        if (threadIdx.x < TS) s_pt[buf][threadIdx.x] = rp;
+        if (threadIdx.x < TS)
+        {
+            float4 q = rp;
+            if (FAR) q.w = q.x * q.x + q.y * q.y + q.z * q.z;
+            s_pt[buf][threadIdx.x] = q;
+        }
 #pragma unroll
         for (int u = 0; u < NB; u++)
         {
@@ -888,13 +940,25 @@ __global__ void __launch_bounds__(256, 4) k_jit_tc(const JitTarget* __restrict__
             const int nj = min(TS, sc.npt - cj);
             const float ax = x0.x + sc.sx, ay = x0.y + sc.sy, az = x0.z + sc.sz;
             const float bx = x1.x + sc.sx, by = x1.y + sc.sy, bz = x1.z + sc.sz;
+            // far form: -2a and |a|^2 of both target rows in the source set's frame
+            const float ma_x = -2.f * ax, ma_y = -2.f * ay, ma_z = -2.f * az, a2 = ax * ax + ay * ay + az * az;
+            const float mb_x = -2.f * bx, mb_y = -2.f * by, mb_z = -2.f * bz, b2 = bx * bx + by * by + bz * bz;
             const int ngrp = (nj + 7) >> 3;
 #pragma unroll 2
             for (int grp = 0; grp < ngrp; grp++)
             {
                 const float4 pa = s_pt[buf][grp * 8 + tq], pb = s_pt[buf][grp * 8 + tq + 4];
                 float k[4];
+                if constexpr (FAR)
                 {
+                    auto r2f = [](float mx, float my, float mz, float s2, const float4& p) {
+                        return fmaxf(fmaf(mx, p.x, fmaf(my, p.y, fmaf(mz, p.z, s2 + p.w))), 1e-30f);
+                    };
+                    k[0] = ScalarFar<KID>::f(r2f(ma_x, ma_y, ma_z, a2, pa), q0, q1);   // (g,   t)
+                    k[1] = ScalarFar<KID>::f(r2f(mb_x, mb_y, mb_z, b2, pa), q0, q1);   // (g+8, t)
+                    k[2] = ScalarFar<KID>::f(r2f(ma_x, ma_y, ma_z, a2, pb), q0, q1);   // (g,   t+4)
+                    k[3] = ScalarFar<KID>::f(r2f(mb_x, mb_y, mb_z, b2, pb), q0, q1);   // (g+8, t+4)
+                } else {
                     float dx = ax - pa.x, dy = ay - pa.y, dz = az - pa.z;
                     k[0] = Scalar<KID, float>::f(dx * dx + dy * dy + dz * dz, p0, c0);   // (g,   t)
                     dx = bx - pa.x; dy = by - pa.y; dz = bz - pa.z;
@@ -913,14 +977,16 @@ __global__ void __launch_bounds__(256, 4) k_jit_tc(const JitTarget* __restrict__
                     hi[q] = tf32_rna(k[q]);
                     lo[q] = __float_as_uint(k[q] - __uint_as_float(hi[q]));
                 }
+                uint4 b[NT];
 #pragma unroll
-                for (int n = 0; n < NT; n++)
-                {
-                    const uint4 b = s_b[buf][grp][n][lane];
-                    mma_tf32(acc[n], lo[0], lo[1], lo[2], lo[3], b.x, b.y);
-                    mma_tf32(acc[n], hi[0], hi[1], hi[2], hi[3], b.z, b.w);
-                    mma_tf32(acc[n], hi[0], hi[1], hi[2], hi[3], b.x, b.y);
-                }
+                for (int n = 0; n < NT; n++) b[n] = s_b[buf][grp][n][lane];
+                // the NT accumulator chains interleaved: consecutive MMAs are independent
+#pragma unroll
+                for (int n = 0; n < NT; n++) mma_tf32(acc[n], lo[0], lo[1], lo[2], lo[3], b[n].x, b[n].y);
+#pragma unroll
+                for (int n = 0; n < NT; n++) mma_tf32(acc[n], hi[0], hi[1], hi[2], hi[3], b[n].z, b[n].w);
+#pragma unroll
+                for (int n = 0; n < NT; n++) mma_tf32(acc[n], hi[0], hi[1], hi[2], hi[3], b[n].x, b[n].y);
             }
 #pragma unroll
             for (int n = 0; n < NT; n++)
@@ -946,95 +1012,146 @@ __global__ void __launch_bounds__(256, 4) k_jit_tc(const JitTarget* __restrict__
 
 // ---------------------------------------- JIT pair kernel (both directions at once)
 
-// One CTA (16 warps) per owner chunk a (<= 256 points; warp w owns rows 16w..16w+15).
-// For every partner b, source tiles of 64 points are staged as in k_jit_tc.  Per
-// group of 8 points of b each lane evaluates the 4 kernel values of its m16n8k8
-// A fragment once and uses them twice:
+// One CTA (8 warps) per work unit: up to 128 points of an owner a (longer owners are
+// walked in chunks of 128; warp w owns rows 16w..16w+15 of a chunk) and a run of a's
+// partners.  For every partner b, source tiles of 64 points are
+// staged as in k_jit_tc (double-buffered: the next tile is read from global memory
+// while the current one is computed).  Per group of 8 points of b each lane evaluates
+// the 4 kernel values of its m16n8k8 A fragment once and uses them twice:
 //   direction a <- b:  out_a (16 rows x NV) += K (16 x 8) * in_b (8 x NV)   [A = K]
 //   direction b <- a:  out_b^T (16 RHS x 8) += in_a^T (16 RHS x 16) * K (16 x 8)
 //                      [A = in_a^T, kept in registers; B = K, transposed through a
 //                       warp-private shared tile]
 // 3xTF32 products, FP32 accumulation.  Each warp stores its b-side partial of a tile
-// in its own shared region; the 16 partials are then summed in warp order (fixed, so
-// the result does not depend on scheduling) and written to b's slot (FP64).  The
-// a-side sums go to FP64 per tile as in k_jit_tc.
+// in its own shared region; the 8 partials are then summed in warp order (fixed, so
+// the result does not depend on scheduling) and written to b's slot (FP64): stored by
+// the first chunk of a, added by the later ones (the same thread owns the same
+// element in every chunk, so program order keeps the sum ordered).  The a-side sums
+// go to FP64 per tile as in k_jit_tc.
+constexpr int kPairWarps = 8;
+constexpr int kPairChunk = 16 * kPairWarps;
+
+template <int NV>
+struct PairSmem {
+    static constexpr int NT = NV / 8, TS = 64, NG = TS / 8, NW = kPairWarps;
+    float4 pt[2][TS];
+    uint4 b[2][NG][NT][32];
+    double acc[NW][NT * 4][32];
+    float d2[NW][TS][NV];
+    float k[NW][16][9];
+};
+
 template <int KID, int NV>
-__global__ void __launch_bounds__(512, 1) k_jit_pair(const PairOwner* __restrict__ owners,
-                                                     const PairPartner* __restrict__ partners,
-                                                     const float4* __restrict__ pts, KParam kp,
-                                                     const double* __restrict__ XS, double* __restrict__ PS)
+__global__ void __launch_bounds__(32 * kPairWarps, 3) k_jit_pair(const PairOwner* __restrict__ owners,
+                                                                 const PairPartner* __restrict__ partners,
+                                                                 const float4* __restrict__ pts, KParam kp,
+                                                                 const double* __restrict__ XS, double* __restrict__ PS)
 {
-    constexpr int NT = NV / 8;
-    constexpr int TS = 64, NG = TS / 8, NW = 16;
+    using SM = PairSmem<NV>;
+    constexpr int NT = SM::NT, TS = SM::TS, NG = SM::NG, NW = SM::NW, NTH = 32 * NW;
+    constexpr int NB = NG * NT * 32 / NTH;        // B-fragment entries staged per thread and tile
+    static_assert(NB >= 1 && NB * NTH == NG * NT * 32, "staging split");
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    float4* s_pt = reinterpret_cast<float4*>(smem_raw);                              // [TS]
-    uint4* s_b = reinterpret_cast<uint4*>(s_pt + TS);                                // [NG][NT][32]
-    double* s_acc = reinterpret_cast<double*>(s_b + NG * NT * 32);                   // [NW][NT*4][32]
-    float* s_d2 = reinterpret_cast<float*>(s_acc + NW * NT * 4 * 32);                // [NW][TS][NV]
-    float* s_k = s_d2 + NW * TS * NV;                                                // [NW][16][9]
+    SM& sm = *reinterpret_cast<SM*>(smem_raw);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, tq = lane & 3;
     const PairOwner ow = owners[blockIdx.x];
     const float p0 = (float) kp.p0, c0 = (float) kp.c0;
-    const int i0 = warp * 16 + g, i1 = i0 + 8;
-    const bool v0 = i0 < ow.na, v1 = i1 < ow.na;
-    const bool warp_on = warp * 16 < ow.na;
-    const int n_on = (ow.na + 15) >> 4;
-    float* d2w = s_d2 + warp * TS * NV;
-    const float4 x0 = pts[ow.pa + (v0 ? i0 : 0)], x1 = pts[ow.pa + (v1 ? i1 : 0)];
-    float* sk = s_k + warp * 16 * 9;
+    float* sk = &sm.k[warp][0][0];
+    float* d2w = &sm.d2[warp][0][0];
 
-    // in_a^T fragments (16 RHS x 8 rows of a per k-step), hi / lo
-    uint32_t ah[2][4], al[2][4];
-#pragma unroll
-    for (int ks = 0; ks < 2; ks++)
-    {
-        const int ra = warp * 16 + 8 * ks + tq, rb = ra + 4;
-        float v[4];
-        v[0] = (ra < ow.na && g < NV) ? (float) XS[(long long) (ow.in_a + ra) * NV + g] : 0.f;
-        v[1] = (ra < ow.na && g + 8 < NV) ? (float) XS[(long long) (ow.in_a + ra) * NV + g + 8] : 0.f;
-        v[2] = (rb < ow.na && g < NV) ? (float) XS[(long long) (ow.in_a + rb) * NV + g] : 0.f;
-        v[3] = (rb < ow.na && g + 8 < NV) ? (float) XS[(long long) (ow.in_a + rb) * NV + g + 8] : 0.f;
-#pragma unroll
-        for (int q = 0; q < 4; q++)
-        {
-            ah[ks][q] = tf32_rna(v[q]);
-            al[ks][q] = __float_as_uint(v[q] - __uint_as_float(ah[ks][q]));
-        }
-    }
-    float acc[NT][4];
-#pragma unroll
-    for (int n = 0; n < NT; n++)
-#pragma unroll
-        for (int q = 0; q < 4; q++) { acc[n][q] = 0.f; s_acc[(warp * NT * 4 + n * 4 + q) * 32 + lane] = 0.0; }
-
-    for (int pi = ow.p_beg; pi < ow.p_end; pi++)
-    {
+    // staging of one tile (points of b and its inputs split into TF32 hi / lo)
+    float4 rp = make_float4(0.f, 0.f, 0.f, 0.f);
+    double rxa[NB], rxb[NB];
+    auto load_tile = [&](int pi, int j0) {
         const PairPartner pb = partners[pi];
-        const float ax = x0.x + pb.sx, ay = x0.y + pb.sy, az = x0.z + pb.sz;
-        const float bx = x1.x + pb.sx, by = x1.y + pb.sy, bz = x1.z + pb.sz;
-        for (int j0 = 0; j0 < pb.nb; j0 += TS)
+        const int nj = min(TS, pb.nb - j0);
+        if (threadIdx.x < TS)
+            rp = (threadIdx.x < nj) ? pts[pb.pb + j0 + threadIdx.x] : make_float4(1e6f, 1e6f, 1e6f, 0.f);
+#pragma unroll
+        for (int u = 0; u < NB; u++)
         {
-            const int nj = min(TS, pb.nb - j0);
-            __syncthreads();
-            for (int j = threadIdx.x; j < TS; j += 512)
-                s_pt[j] = (j < nj) ? pts[pb.pb + j0 + j] : make_float4(1e6f, 1e6f, 1e6f, 0.f);
-            for (int e = threadIdx.x; e < NG * NT * 32; e += 512)
+            const int e = threadIdx.x + u * NTH;
+            const int ln = e & 31, n = (e >> 5) % NT, grp = e / (32 * NT);
+            const int sa = grp * 8 + (ln & 3), sb = sa + 4, r = n * 8 + (ln >> 2);
+            rxa[u] = (sa < nj) ? XS[(long long) (pb.in_b + j0 + sa) * NV + r] : 0.0;
+            rxb[u] = (sb < nj) ? XS[(long long) (pb.in_b + j0 + sb) * NV + r] : 0.0;
+        }
+    };
+    auto store_tile = [&](int buf) {
+        if (threadIdx.x < TS) sm.pt[buf][threadIdx.x] = rp;
+#pragma unroll
+        for (int u = 0; u < NB; u++)
+        {
+            const int e = threadIdx.x + u * NTH;
+            const int ln = e & 31, n = (e >> 5) % NT, grp = e / (32 * NT);
+            const float xa = (float) rxa[u], xb = (float) rxb[u];
+            const uint32_t ha = tf32_rna(xa), hb = tf32_rna(xb);
+            sm.b[buf][grp][n][ln] = make_uint4(ha, hb, __float_as_uint(xa - __uint_as_float(ha)),
+                                               __float_as_uint(xb - __uint_as_float(hb)));
+        }
+    };
+    auto advance = [&](int& pi, int& j0) {
+        j0 += TS;
+        if (j0 >= partners[pi].nb) { pi++; j0 = 0; }
+    };
+
+    for (int ch = 0; ch < ow.na; ch += kPairChunk)
+    {
+        const int na = min(kPairChunk, ow.na - ch);
+        const int i0 = warp * 16 + g, i1 = i0 + 8;
+        const bool v0 = i0 < na, v1 = i1 < na;
+        const bool warp_on = warp * 16 < na;
+        const int n_on = (na + 15) >> 4;
+        const float4 x0 = pts[ow.pa + ch + (v0 ? i0 : 0)], x1 = pts[ow.pa + ch + (v1 ? i1 : 0)];
+        // in_a^T fragments (16 RHS x 8 rows of a per k-step), hi / lo
+        uint32_t ah[2][4], al[2][4];
+#pragma unroll
+        for (int ks = 0; ks < 2; ks++)
+        {
+            const int ra = warp * 16 + 8 * ks + tq, rb = ra + 4;
+            const long long ia = (long long) (ow.in_a + ch + ra) * NV, ib = (long long) (ow.in_a + ch + rb) * NV;
+            float v[4];
+            v[0] = (ra < na && g < NV) ? (float) XS[ia + g] : 0.f;
+            v[1] = (ra < na && g + 8 < NV) ? (float) XS[ia + g + 8] : 0.f;
+            v[2] = (rb < na && g < NV) ? (float) XS[ib + g] : 0.f;
+            v[3] = (rb < na && g + 8 < NV) ? (float) XS[ib + g + 8] : 0.f;
+#pragma unroll
+            for (int q = 0; q < 4; q++)
             {
-                const int ln = e & 31, n = (e >> 5) % NT, grp = e / (32 * NT);
-                const int sa = grp * 8 + (ln & 3), sb = sa + 4, r = n * 8 + (ln >> 2);
-                const float xa = (sa < nj) ? (float) XS[(long long) (pb.in_b + j0 + sa) * NV + r] : 0.f;
-                const float xb = (sb < nj) ? (float) XS[(long long) (pb.in_b + j0 + sb) * NV + r] : 0.f;
-                const uint32_t ha = tf32_rna(xa), hb = tf32_rna(xb);
-                s_b[(grp * NT + n) * 32 + ln] =
-                    make_uint4(ha, hb, __float_as_uint(xa - __uint_as_float(ha)), __float_as_uint(xb - __uint_as_float(hb)));
+                ah[ks][q] = tf32_rna(v[q]);
+                al[ks][q] = __float_as_uint(v[q] - __uint_as_float(ah[ks][q]));
             }
-            __syncthreads();
+        }
+        float acc[NT][4];
+#pragma unroll
+        for (int n = 0; n < NT; n++)
+#pragma unroll
+            for (int q = 0; q < 4; q++) { acc[n][q] = 0.f; sm.acc[warp][n * 4 + q][lane] = 0.0; }
+
+        int ls = ow.p_beg, lj = 0;              // tile being loaded
+        __syncthreads();                        // previous chunk's readers of the buffers are done
+        if (ls < ow.p_end)
+        {
+            load_tile(ls, lj);
+            store_tile(0);
+            advance(ls, lj);
+        }
+        __syncthreads();
+        int cs = ow.p_beg, cj = 0, buf = 0;     // tile being computed
+        while (cs < ow.p_end)
+        {
+            const bool more = ls < ow.p_end;
+            if (more) load_tile(ls, lj);
+            const PairPartner pb = partners[cs];
+            const int nj = min(TS, pb.nb - cj);
             if (warp_on)
             {
+                const float ax = x0.x + pb.sx, ay = x0.y + pb.sy, az = x0.z + pb.sz;
+                const float bx = x1.x + pb.sx, by = x1.y + pb.sy, bz = x1.z + pb.sz;
                 const int ngrp = (nj + 7) >> 3;
                 for (int grp = 0; grp < ngrp; grp++)
                 {
-                    const float4 pa = s_pt[grp * 8 + tq], pc = s_pt[grp * 8 + tq + 4];
+                    const float4 pa = sm.pt[buf][grp * 8 + tq], pc = sm.pt[buf][grp * 8 + tq + 4];
                     float k[4];
                     {
                         float dx = ax - pa.x, dy = ay - pa.y, dz = az - pa.z;
@@ -1049,6 +1166,11 @@ __global__ void __launch_bounds__(512, 1) k_jit_pair(const PairOwner* __restrict
                     // rows of a beyond the chunk contribute nothing to b
                     if (!v0) { k[0] = 0.f; k[2] = 0.f; }
                     if (!v1) { k[1] = 0.f; k[3] = 0.f; }
+                    // K tile (16 rows of a x 8 points of b) to the warp's shared tile
+                    sk[g * 9 + tq] = k[0];
+                    sk[(g + 8) * 9 + tq] = k[1];
+                    sk[g * 9 + tq + 4] = k[2];
+                    sk[(g + 8) * 9 + tq + 4] = k[3];
                     uint32_t hi[4], lo[4];
 #pragma unroll
                     for (int q = 0; q < 4; q++)
@@ -1056,19 +1178,15 @@ __global__ void __launch_bounds__(512, 1) k_jit_pair(const PairOwner* __restrict
                         hi[q] = tf32_rna(k[q]);
                         lo[q] = __float_as_uint(k[q] - __uint_as_float(hi[q]));
                     }
+                    uint4 b[NT];
 #pragma unroll
-                    for (int n = 0; n < NT; n++)
-                    {
-                        const uint4 b = s_b[(grp * NT + n) * 32 + lane];
-                        mma_tf32(acc[n], lo[0], lo[1], lo[2], lo[3], b.x, b.y);
-                        mma_tf32(acc[n], hi[0], hi[1], hi[2], hi[3], b.z, b.w);
-                        mma_tf32(acc[n], hi[0], hi[1], hi[2], hi[3], b.x, b.y);
-                    }
-                    // K tile (16 rows of a x 8 points of b) through shared memory, transposed
-                    sk[g * 9 + tq] = k[0];
-                    sk[(g + 8) * 9 + tq] = k[1];
-                    sk[g * 9 + tq + 4] = k[2];
-                    sk[(g + 8) * 9 + tq + 4] = k[3];
+                    for (int n = 0; n < NT; n++) b[n] = sm.b[buf][grp][n][lane];
+#pragma unroll
+                    for (int n = 0; n < NT; n++) mma_tf32(acc[n], lo[0], lo[1], lo[2], lo[3], b[n].x, b[n].y);
+#pragma unroll
+                    for (int n = 0; n < NT; n++) mma_tf32(acc[n], hi[0], hi[1], hi[2], hi[3], b[n].z, b[n].w);
+#pragma unroll
+                    for (int n = 0; n < NT; n++) mma_tf32(acc[n], hi[0], hi[1], hi[2], hi[3], b[n].x, b[n].y);
                     __syncwarp();
                     float kt[4];
                     kt[0] = sk[tq * 9 + g];          // k-step 0: K[a = tq][b = g]
@@ -1083,22 +1201,22 @@ __global__ void __launch_bounds__(512, 1) k_jit_pair(const PairOwner* __restrict
                         th[q] = tf32_rna(kt[q]);
                         tl[q] = __float_as_uint(kt[q] - __uint_as_float(th[q]));
                     }
-                    float d2[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-                    for (int ks = 0; ks < 2; ks++)
-                    {
-                        mma_tf32(d2, al[ks][0], al[ks][1], al[ks][2], al[ks][3], th[2 * ks], th[2 * ks + 1]);
-                        mma_tf32(d2, ah[ks][0], ah[ks][1], ah[ks][2], ah[ks][3], tl[2 * ks], tl[2 * ks + 1]);
-                        mma_tf32(d2, ah[ks][0], ah[ks][1], ah[ks][2], ah[ks][3], th[2 * ks], th[2 * ks + 1]);
-                    }
-                    // d2: rows = RHS (g, g+8), columns = points of b (2t, 2t+1)
+                    // two independent chains (one per k-step), summed at the end
+                    float da[4] = {0.f, 0.f, 0.f, 0.f}, db[4] = {0.f, 0.f, 0.f, 0.f};
+                    mma_tf32(da, al[0][0], al[0][1], al[0][2], al[0][3], th[0], th[1]);
+                    mma_tf32(db, al[1][0], al[1][1], al[1][2], al[1][3], th[2], th[3]);
+                    mma_tf32(da, ah[0][0], ah[0][1], ah[0][2], ah[0][3], tl[0], tl[1]);
+                    mma_tf32(db, ah[1][0], ah[1][1], ah[1][2], ah[1][3], tl[2], tl[3]);
+                    mma_tf32(da, ah[0][0], ah[0][1], ah[0][2], ah[0][3], th[0], th[1]);
+                    mma_tf32(db, ah[1][0], ah[1][1], ah[1][2], ah[1][3], th[2], th[3]);
+                    // rows = RHS (g, g+8), columns = points of b (2t, 2t+1)
                     float* row0 = d2w + (grp * 8 + 2 * tq) * NV;
-                    row0[g] = d2[0];
-                    row0[NV + g] = d2[1];
+                    row0[g] = da[0] + db[0];
+                    row0[NV + g] = da[1] + db[1];
                     if (NV > 8)
                     {
-                        row0[g + 8] = d2[2];
-                        row0[NV + g + 8] = d2[3];
+                        row0[g + 8] = da[2] + db[2];
+                        row0[NV + g + 8] = da[3] + db[3];
                     }
                 }
 #pragma unroll
@@ -1106,38 +1224,207 @@ __global__ void __launch_bounds__(512, 1) k_jit_pair(const PairOwner* __restrict
 #pragma unroll
                     for (int q = 0; q < 4; q++)
                     {
-                        s_acc[(warp * NT * 4 + n * 4 + q) * 32 + lane] += (double) acc[n][q];
+                        sm.acc[warp][n * 4 + q][lane] += (double) acc[n][q];
                         acc[n][q] = 0.f;
                     }
             }
-            __syncthreads();
-            for (int e = threadIdx.x; e < nj * NV; e += 512)
+            if (more) store_tile(buf ^ 1);
+            __syncthreads();                    // all partials of this tile written; next tile staged
+            for (int e = threadIdx.x; e < nj * NV; e += NTH)
             {
                 float t = 0.f;
-                for (int w = 0; w < n_on; w++) t += s_d2[w * TS * NV + e];
-                PS[(long long) (pb.out_b + j0) * NV + e] = (double) t;
+                for (int w = 0; w < n_on; w++) t += (&sm.d2[w][0][0])[e];
+                double* o = PS + (long long) (pb.out_b + cj) * NV + e;
+                *o = (ch == 0) ? (double) t : *o + (double) t;
             }
+            __syncthreads();                    // partials read before the next tile overwrites them
+            cs = ls; cj = lj; buf ^= 1;
+            if (more) advance(ls, lj);
         }
-    }
-    if (warp_on)
-    {
-        double* base = PS + (long long) ow.out_a * NV;
+        if (warp_on)
+        {
+            double* base = PS + (long long) (ow.out_a + ch) * NV;
 #pragma unroll
-        for (int n = 0; n < NT; n++)
+            for (int n = 0; n < NT; n++)
 #pragma unroll
-            for (int q = 0; q < 4; q++)
-            {
-                const int row = (q < 2) ? i0 : i1;
-                const bool ok = (q < 2) ? v0 : v1;
-                if (ok) base[(long long) row * NV + n * 8 + 2 * tq + (q & 1)] = s_acc[(warp * NT * 4 + n * 4 + q) * 32 + lane];
-            }
+                for (int q = 0; q < 4; q++)
+                {
+                    const int row = (q < 2) ? i0 : i1;
+                    const bool ok = (q < 2) ? v0 : v1;
+                    if (ok) base[(long long) row * NV + n * 8 + 2 * tq + (q & 1)] = sm.acc[warp][n * 4 + q][lane];
+                }
+        }
     }
 }
 
 template <int NV>
 constexpr int pair_smem_bytes()
 {
-    return 64 * 16 + 8 * (NV / 8) * 32 * 16 + 16 * (NV / 8) * 4 * 32 * 8 + 16 * 64 * NV * 4 + 16 * 16 * 9 * 4;
+    return (int) sizeof(PairSmem<NV>);
+}
+
+// --------------------------------------- stored blocks on the tensor cores (FP32)
+
+// Stored block chunk (R <= 64 rows x ncol, FP32 copy) for panels of 8 / 16 right-hand
+// sides, both products on the tensor cores with the right-hand sides as the M = 16
+// side of m16n8k8 (3xTF32, FP32 accumulation):
+//   C1^T (NV x ncol) = W^T (NV x R) A        [B operand = A, k = rows]      warps 0-3
+//   C0^T (NV x R)    = V^T (NV x ncol) A^T   [B operand = A^T, k = columns] warps 4-7
+// Column tiles of 32 are staged in shared memory (double-buffered through registers);
+// each tile feeds both products.  Warp w < 4 owns columns 8w..8w+7 of every tile and
+// completes C1 for them over the R rows; warp 4 + u owns rows 16u..16u+15 and sums
+// C0 over the tiles (FP32 per tile, FP64 across tiles).
+template <int NV>
+__global__ void __launch_bounds__(256, 3) k_blk_tc(const BlkTask* __restrict__ tasks, const float* __restrict__ arena,
+                                                   const double* __restrict__ XS, double* __restrict__ PS)
+{
+    constexpr int CT = 32, S = CT + 4;            // tile width; padded shared row (conflict-free C0 reads)
+    __shared__ float s_a[2][64][S];
+    __shared__ uint4 s_w[8][32][2];               // W^T fragments per k-step of 8 rows: hi, lo
+    __shared__ uint4 s_v[2][4][32][2];            // V^T fragments per k-step of 8 columns: hi, lo
+    const BlkTask T = tasks[blockIdx.x];
+    const float* A = arena + T.a_off;
+    const int R = T.nrow, ncol = T.ncol;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, tq = lane & 3;
+    const bool do0 = T.out0_row >= 0, do1 = T.out1_row >= 0;
+
+    // A-fragment of an (NV x 8) slice of X^T: X rows k0 + {tq, tq+4}, right-hand sides {g, g+8}
+    auto frag = [&](int row0, int nrows, int k0, uint4& hi, uint4& lo) {
+        float v[4];
+        const int ra = k0 + tq, rb = ra + 4;
+        v[0] = (ra < nrows && g < NV) ? (float) XS[(long long) (row0 + ra) * NV + g] : 0.f;
+        v[1] = (ra < nrows && g + 8 < NV) ? (float) XS[(long long) (row0 + ra) * NV + g + 8] : 0.f;
+        v[2] = (rb < nrows && g < NV) ? (float) XS[(long long) (row0 + rb) * NV + g] : 0.f;
+        v[3] = (rb < nrows && g + 8 < NV) ? (float) XS[(long long) (row0 + rb) * NV + g + 8] : 0.f;
+        uint32_t h[4], l[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+        {
+            h[q] = tf32_rna(v[q]);
+            l[q] = __float_as_uint(v[q] - __uint_as_float(h[q]));
+        }
+        hi = make_uint4(h[0], h[1], h[2], h[3]);
+        lo = make_uint4(l[0], l[1], l[2], l[3]);
+    };
+    // W^T fragments for the whole chunk (8 k-steps of 8 rows), one warp per k-step
+    if (do1)
+        frag(T.in1_row, R, 8 * warp, s_w[warp][lane][0], s_w[warp][lane][1]);
+
+    // tile staging: 64 x 32 floats, 8 per thread; V^T fragments of the tile's columns
+    float ra[8];
+    uint4 rvh = make_uint4(0, 0, 0, 0), rvl = rvh;
+    auto load_tile = [&](int c0) {
+#pragma unroll
+        for (int u = 0; u < 8; u++)
+        {
+            const int e = threadIdx.x + 256 * u, r = e >> 5, c = e & 31;
+            ra[u] = (r < R && c0 + c < ncol) ? A[(long long) r * ncol + c0 + c] : 0.f;
+        }
+        if (do0 && warp < 4) frag(T.in0_row + c0, ncol - c0, 8 * warp, rvh, rvl);
+    };
+    auto store_tile = [&](int buf) {
+#pragma unroll
+        for (int u = 0; u < 8; u++)
+        {
+            const int e = threadIdx.x + 256 * u;
+            s_a[buf][e >> 5][e & 31] = ra[u];
+        }
+        if (do0 && warp < 4) { s_v[buf][warp][lane][0] = rvh; s_v[buf][warp][lane][1] = rvl; }
+    };
+
+    double c0acc[2][4];
+#pragma unroll
+    for (int n = 0; n < 2; n++)
+#pragma unroll
+        for (int q = 0; q < 4; q++) c0acc[n][q] = 0.0;
+
+    if (ncol > 0)
+    {
+        load_tile(0);
+        store_tile(0);
+    }
+    __syncthreads();
+    int buf = 0;
+    for (int c0 = 0; c0 < ncol; c0 += CT)
+    {
+        const bool more = c0 + CT < ncol;
+        if (more) load_tile(c0 + CT);
+        if (warp < 4)
+        {
+            if (do1)
+            {
+                // C1^T for columns c0 + 8w .. +7: k over the R rows (8 k-steps)
+                float d[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};   // two chains, summed
+                const int ksteps = (R + 7) >> 3;
+#pragma unroll
+                for (int ks = 0; ks < 8; ks++)
+                {
+                    if (ks >= ksteps) break;
+                    const float b0 = s_a[buf][8 * ks + tq][8 * warp + g];
+                    const float b1 = s_a[buf][8 * ks + tq + 4][8 * warp + g];
+                    const uint32_t h0 = tf32_rna(b0), h1 = tf32_rna(b1);
+                    const uint32_t l0 = __float_as_uint(b0 - __uint_as_float(h0)),
+                                   l1 = __float_as_uint(b1 - __uint_as_float(h1));
+                    const uint4 wh = s_w[ks][lane][0], wl = s_w[ks][lane][1];
+                    float (&dd)[4] = d[ks & 1];
+                    mma_tf32(dd, wl.x, wl.y, wl.z, wl.w, h0, h1);
+                    mma_tf32(dd, wh.x, wh.y, wh.z, wh.w, l0, l1);
+                    mma_tf32(dd, wh.x, wh.y, wh.z, wh.w, h0, h1);
+                }
+                // rows of the fragment = right-hand sides (g, g+8), columns = (2tq, 2tq+1)
+                const int cb = c0 + 8 * warp + 2 * tq;
+#pragma unroll
+                for (int q = 0; q < 4; q++)
+                {
+                    const int rhs = (q < 2) ? g : g + 8, col = cb + (q & 1);
+                    if (rhs < NV && col < ncol) PS[(long long) (T.out1_row + col) * NV + rhs] = (double) (d[0][q] + d[1][q]);
+                }
+            }
+        } else if (do0) {
+            // C0^T for rows 16u .. 16u+15 (two n-tiles of 8): k over the tile's 32 columns
+            const int u = warp - 4;
+            if (16 * u < R)
+            {
+                float d[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+#pragma unroll
+                for (int ks = 0; ks < 4; ks++)
+                {
+                    const uint4 vh = s_v[buf][ks][lane][0], vl = s_v[buf][ks][lane][1];
+#pragma unroll
+                    for (int n = 0; n < 2; n++)
+                    {
+                        const int row = 16 * u + 8 * n + g;
+                        const float b0 = s_a[buf][row][8 * ks + tq], b1 = s_a[buf][row][8 * ks + tq + 4];
+                        const uint32_t h0 = tf32_rna(b0), h1 = tf32_rna(b1);
+                        const uint32_t l0 = __float_as_uint(b0 - __uint_as_float(h0)),
+                                       l1 = __float_as_uint(b1 - __uint_as_float(h1));
+                        mma_tf32(d[n], vl.x, vl.y, vl.z, vl.w, h0, h1);
+                        mma_tf32(d[n], vh.x, vh.y, vh.z, vh.w, l0, l1);
+                        mma_tf32(d[n], vh.x, vh.y, vh.z, vh.w, h0, h1);
+                    }
+                }
+#pragma unroll
+                for (int n = 0; n < 2; n++)
+#pragma unroll
+                    for (int q = 0; q < 4; q++) c0acc[n][q] += (double) d[n][q];
+            }
+        }
+        if (more) store_tile(buf ^ 1);
+        __syncthreads();
+        buf ^= 1;
+    }
+    if (do0 && warp >= 4)
+    {
+        const int u = warp - 4;
+#pragma unroll
+        for (int n = 0; n < 2; n++)
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+            {
+                const int rhs = (q < 2) ? g : g + 8, row = 16 * u + 8 * n + 2 * tq + (q & 1);
+                if (rhs < NV && row < R) PS[(long long) (T.out0_row + row) * NV + rhs] = c0acc[n][q];
+            }
+    }
 }
 
 // --------------------------------------------------------------- direct sum
@@ -1239,8 +1526,18 @@ static cudaError_t allow_smem(K kern, int bytes)
 }
 
 template <typename TA>
-cudaError_t launch_blk(int NV, const BlkTask* t, int n, const TA* arena, const double* XS, double* PS, cudaStream_t st)
+cudaError_t launch_blk(int NV, const BlkTask* t, int n, const TA* arena, const double* XS, double* PS, cudaStream_t st,
+                       int use_tc)
 {
+    if constexpr (sizeof(TA) == 4)
+    {
+        if (use_tc && n > 0 && (NV == 8 || NV == 16))
+        {
+            if (NV == 16) k_blk_tc<16><<<n, 256, 0, st>>>(t, arena, XS, PS);
+            else k_blk_tc<8><<<n, 256, 0, st>>>(t, arena, XS, PS);
+            return cudaGetLastError();
+        }
+    }
     if (n <= 0) return cudaSuccess;
     NV_DISPATCH(NV, {
         if constexpr (NVc >= 4)
@@ -1294,7 +1591,8 @@ cudaError_t launch_asm(int NV, const AsmTask* t, int n, const int* slots, const 
 
 template <int KID, typename T, int KD>
 static cudaError_t launch_jit_k(int NV, const JitTarget* tg, int n, const JitSource* sr, const void* pts, KParam kp,
-                                int use_shift, int use_tc, const double* XS, double* PS, double* Y1, cudaStream_t st)
+                                int use_shift, int use_tc, const double* XS, double* PS, double* Y1, cudaStream_t st,
+                                int far)
 {
     using T4 = typename Vec4<T>::t;
     const T4* p = (const T4*) pts;
@@ -1302,14 +1600,13 @@ static cudaError_t launch_jit_k(int NV, const JitTarget* tg, int n, const JitSou
     // cores unless the image chose the CUDA-core kernel (autotuner, H2G_JIT_TC=0)
     if constexpr (KD == 1 && sizeof(T) == 4)
     {
-        if (use_tc && NV == 16 && use_shift)
+        if (use_tc && (NV == 16 || NV == 8) && use_shift)
         {
-            k_jit_tc<KID, 16><<<n, 256, 0, st>>>(tg, sr, (const float4*) pts, kp, XS, PS, Y1);
-            return cudaGetLastError();
-        }
-        if (use_tc && NV == 8 && use_shift)
-        {
-            k_jit_tc<KID, 8><<<n, 256, 0, st>>>(tg, sr, (const float4*) pts, kp, XS, PS, Y1);
+            const float4* p4 = (const float4*) pts;
+            if (NV == 16 && far) k_jit_tc<KID, 16, true><<<n, 256, 0, st>>>(tg, sr, p4, kp, XS, PS, Y1);
+            else if (NV == 16) k_jit_tc<KID, 16, false><<<n, 256, 0, st>>>(tg, sr, p4, kp, XS, PS, Y1);
+            else if (far) k_jit_tc<KID, 8, true><<<n, 256, 0, st>>>(tg, sr, p4, kp, XS, PS, Y1);
+            else k_jit_tc<KID, 8, false><<<n, 256, 0, st>>>(tg, sr, p4, kp, XS, PS, Y1);
             return cudaGetLastError();
         }
     }
@@ -1326,19 +1623,20 @@ static cudaError_t launch_jit_k(int NV, const JitTarget* tg, int n, const JitSou
 }
 
 cudaError_t launch_jit(int kid, int fp32, int NV, const JitTarget* tg, int n, const JitSource* sr, const void* pts,
-                       KParam kp, int use_shift, int use_tc, const double* XS, double* PS, double* Y1, cudaStream_t st)
+                       KParam kp, int use_shift, int use_tc, const double* XS, double* PS, double* Y1, cudaStream_t st,
+                       int far)
 {
     if (n <= 0) return cudaSuccess;
     switch (kid)
     {
-        case KRNL_COULOMB_ID:  return fp32 ? launch_jit_k<KRNL_COULOMB_ID, float, 1>(NV, tg, n, sr, pts, kp, use_shift, use_tc, XS, PS, Y1, st)
-                                           : launch_jit_k<KRNL_COULOMB_ID, double, 1>(NV, tg, n, sr, pts, kp, use_shift, use_tc, XS, PS, Y1, st);
-        case KRNL_GAUSSIAN_ID: return fp32 ? launch_jit_k<KRNL_GAUSSIAN_ID, float, 1>(NV, tg, n, sr, pts, kp, use_shift, use_tc, XS, PS, Y1, st)
-                                           : launch_jit_k<KRNL_GAUSSIAN_ID, double, 1>(NV, tg, n, sr, pts, kp, use_shift, use_tc, XS, PS, Y1, st);
-        case KRNL_MATERN32_ID: return fp32 ? launch_jit_k<KRNL_MATERN32_ID, float, 1>(NV, tg, n, sr, pts, kp, use_shift, use_tc, XS, PS, Y1, st)
-                                           : launch_jit_k<KRNL_MATERN32_ID, double, 1>(NV, tg, n, sr, pts, kp, use_shift, use_tc, XS, PS, Y1, st);
-        case KRNL_RPY_ID:      return fp32 ? launch_jit_k<KRNL_RPY_ID, float, 3>(NV, tg, n, sr, pts, kp, use_shift, use_tc, XS, PS, Y1, st)
-                                           : launch_jit_k<KRNL_RPY_ID, double, 3>(NV, tg, n, sr, pts, kp, use_shift, use_tc, XS, PS, Y1, st);
+        case KRNL_COULOMB_ID:  return fp32 ? launch_jit_k<KRNL_COULOMB_ID, float, 1>(NV, tg, n, sr, pts, kp, use_shift, use_tc, XS, PS, Y1, st, far)
+                                           : launch_jit_k<KRNL_COULOMB_ID, double, 1>(NV, tg, n, sr, pts, kp, use_shift, use_tc, XS, PS, Y1, st, far);
+        case KRNL_GAUSSIAN_ID: return fp32 ? launch_jit_k<KRNL_GAUSSIAN_ID, float, 1>(NV, tg, n, sr, pts, kp, use_shift, use_tc, XS, PS, Y1, st, far)
+                                           : launch_jit_k<KRNL_GAUSSIAN_ID, double, 1>(NV, tg, n, sr, pts, kp, use_shift, use_tc, XS, PS, Y1, st, far);
+        case KRNL_MATERN32_ID: return fp32 ? launch_jit_k<KRNL_MATERN32_ID, float, 1>(NV, tg, n, sr, pts, kp, use_shift, use_tc, XS, PS, Y1, st, far)
+                                           : launch_jit_k<KRNL_MATERN32_ID, double, 1>(NV, tg, n, sr, pts, kp, use_shift, use_tc, XS, PS, Y1, st, far);
+        case KRNL_RPY_ID:      return fp32 ? launch_jit_k<KRNL_RPY_ID, float, 3>(NV, tg, n, sr, pts, kp, use_shift, use_tc, XS, PS, Y1, st, far)
+                                           : launch_jit_k<KRNL_RPY_ID, double, 3>(NV, tg, n, sr, pts, kp, use_shift, use_tc, XS, PS, Y1, st, far);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -1352,12 +1650,12 @@ static cudaError_t launch_pair_k(int NV, const PairOwner* ow, int n, const PairP
         constexpr int b = pair_smem_bytes<16>();
         cudaError_t e = allow_smem(k_jit_pair<KID, 16>, b);
         if (e != cudaSuccess) return e;
-        k_jit_pair<KID, 16><<<n, 512, b, st>>>(ow, pp, pts, kp, XS, PS);
+        k_jit_pair<KID, 16><<<n, 32 * kPairWarps, b, st>>>(ow, pp, pts, kp, XS, PS);
     } else if (NV == 8) {
         constexpr int b = pair_smem_bytes<8>();
         cudaError_t e = allow_smem(k_jit_pair<KID, 8>, b);
         if (e != cudaSuccess) return e;
-        k_jit_pair<KID, 8><<<n, 512, b, st>>>(ow, pp, pts, kp, XS, PS);
+        k_jit_pair<KID, 8><<<n, 32 * kPairWarps, b, st>>>(ow, pp, pts, kp, XS, PS);
     } else {
         return cudaErrorInvalidValue;
     }
@@ -1395,8 +1693,8 @@ cudaError_t launch_direct(int kid, const double4* trg, int n_trg, const double4*
 
 template cudaError_t launch_up<double>(int, const UpTask*, int, const double*, double*, cudaStream_t);
 template cudaError_t launch_up<float>(int, const UpTask*, int, const float*, double*, cudaStream_t);
-template cudaError_t launch_blk<double>(int, const BlkTask*, int, const double*, const double*, double*, cudaStream_t);
-template cudaError_t launch_blk<float>(int, const BlkTask*, int, const float*, const double*, double*, cudaStream_t);
+template cudaError_t launch_blk<double>(int, const BlkTask*, int, const double*, const double*, double*, cudaStream_t, int);
+template cudaError_t launch_blk<float>(int, const BlkTask*, int, const float*, const double*, double*, cudaStream_t, int);
 template cudaError_t launch_down<double>(int, const DownTask*, int, const double*, const double*, double*, double*, cudaStream_t);
 template cudaError_t launch_down<float>(int, const DownTask*, int, const float*, const double*, double*, double*, cudaStream_t);
 

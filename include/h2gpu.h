@@ -217,8 +217,8 @@ int h2gpu_graph_launch(h2gpu_image *img, void *stream);
 
 /*
  * Autotuner: time the device apply of n_vec right-hand sides for each candidate
- * panel width and, for FP32 JIT images, each JIT kernel variant, and keep the
- * fastest for this image.  dY is overwritten.  *best_variant receives
+ * panel width and, for FP32 images, each kernel variant (h2gpu_set_jit_variant), and
+ * keep the fastest for this image.  dY is overwritten.  *best_variant receives
  * H2GPU_JIT_SIMT (CUDA cores), H2GPU_JIT_TC (tensor cores, every target evaluates
  * its own sources) or H2GPU_JIT_PAIR (tensor cores, each unordered pair of leaves /
  * nodes evaluated once and applied in both directions).  No counterpart in the
@@ -231,11 +231,12 @@ int h2gpu_autotune(h2gpu_image *img, int n_vec, const double *dX, int ldx, doubl
                    int *best_nv, int *best_variant);
 
 /*
- * Select the JIT kernel variant used by FP32 panels of JIT images (H2GPU_JIT_SIMT,
- * H2GPU_JIT_TC (default) or H2GPU_JIT_PAIR; the pair variant needs a scalar kernel
- * and applies to panels of 8 or 16 right-hand sides, others use H2GPU_JIT_TC).
- * FP64 panels always use the CUDA-core kernel; a captured graph keeps the variant it
- * was captured with.  No counterpart in the reference.
+ * Select the kernel variant used by FP32 panels: for JIT images H2GPU_JIT_SIMT,
+ * H2GPU_JIT_TC (default) or H2GPU_JIT_PAIR (needs a scalar kernel; panels of 8 or
+ * 16 right-hand sides, others use H2GPU_JIT_TC); for stored-block images
+ * H2GPU_JIT_TC (default: block products of panels of 8 or 16 on the tensor cores) or
+ * H2GPU_JIT_SIMT (CUDA cores).  FP64 panels always use the CUDA cores; a captured
+ * graph keeps the variant it was captured with.  No counterpart in the reference.
  */
 int h2gpu_set_jit_variant(h2gpu_image *img, int variant);
 

@@ -1,5 +1,6 @@
-"""The three FP32 JIT kernel variants (CUDA cores, tensor cores per target, tensor
-cores per unordered pair) against the FP64 apply of the same image.
+"""The FP32 kernel variants against the FP64 apply of the same image: for JIT images
+CUDA cores, tensor cores per target and tensor cores per unordered pair; for stored
+blocks CUDA cores and tensor cores.
 
 The reference evaluates every JIT block from both sides with one bi-matvec
 (src/H2Pack_matvec.c:170-236, H2P_matvec_fwd_transform/intmd_mult_JIT); the pair
@@ -15,7 +16,7 @@ from test_batched import holder
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("name", ["matern32_jit", "coulomb_jit", "gaussian_jit"])
+@pytest.mark.parametrize("name", ["matern32_jit", "coulomb_jit", "gaussian_jit", "coulomb_aot", "rpy_aot"])
 @pytest.mark.parametrize("nv", [8, 16, 5])
 def test_variants_match_fp64(name, nv):
     import torch
@@ -27,7 +28,7 @@ def test_variants_match_fp64(name, nv):
         Y64 = img.matmul_device(X).cpu().numpy()
         img.set_precision("mixed")
         outs = {}
-        for var in ("simt", "tc", "pair"):
+        for var in (("simt", "tc", "pair") if name.endswith("jit") else ("simt", "tc")):
             img.set_jit_variant(var)
             Ya = img.matmul_device(X).cpu().numpy()
             Yb = img.matmul_device(X).cpu().numpy()
@@ -35,14 +36,15 @@ def test_variants_match_fp64(name, nv):
             assert rel(Ya, Y64) < 2e-6, var
             outs[var] = Ya
         # the variants differ only by FP32 rounding
-        assert rel(outs["pair"], outs["tc"]) < 2e-6
+        assert rel(outs["simt"], outs["tc"]) < 2e-6
     finally:
         img.close()
 
 
-def test_pair_variant_refused_for_vector_kernel():
+@pytest.mark.parametrize("name", ["rpy_jit", "coulomb_aot"])
+def test_pair_variant_refused(name):
     from h2pack_b200 import Image
-    h, _ = holder("rpy_jit")
+    h, _ = holder(name)
     img = Image(h.desc, precision="mixed")
     try:
         with pytest.raises(RuntimeError):
