@@ -22,6 +22,8 @@ KRNL_COULOMB, KRNL_GAUSSIAN, KRNL_MATERN32, KRNL_RPY = 1, 2, 3, 4
 KERNEL_IDS = {"coulomb": KRNL_COULOMB, "gaussian": KRNL_GAUSSIAN, "matern32": KRNL_MATERN32, "rpy": KRNL_RPY}
 PREC_FP64, PREC_MIXED = 0, 1
 JIT_SIMT, JIT_TC, JIT_PAIR = 0, 1, 2
+CG_FREE, CG_RUN, CG_CHECK, CG_DONE = 0, 1, 2, 3
+CG_MATVEC, CG_PCG = 0, 1
 ROW_MAJOR, COL_MAJOR = 101, 102
 
 _ip = C.POINTER(C.c_int)
@@ -80,6 +82,14 @@ H2GPU_SYMBOLS = {
     "h2gpu_permute_matrix_rows": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, _dp, C.c_int, _dp, C.c_int]),
     "h2gpu_matvec_device_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "h2gpu_set_jit_variant": (C.c_int, [C.c_void_p, C.c_int]),
+    "h2gpu_cg_create": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.POINTER(C.c_void_p)]),
+    "h2gpu_cg_destroy": (C.c_int, [C.c_void_p]),
+    "h2gpu_cg_admit": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_double, C.c_int]),
+    "h2gpu_cg_step": (C.c_int, [C.c_void_p, C.c_int]),
+    "h2gpu_cg_check": (C.c_int, [C.c_void_p]),
+    "h2gpu_cg_sync": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), _dp]),
+    "h2gpu_cg_take": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "h2gpu_cg_history": (C.c_int, [C.c_void_p, C.c_int, _dp, C.c_int]),
     "h2gpu_batch_create": (C.c_int, [C.POINTER(Desc), C.c_int, C.POINTER(Options), C.POINTER(C.c_void_p)]),
     "h2gpu_graph_capture": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int]),
     "h2gpu_graph_launch": (C.c_int, [C.c_void_p, C.c_void_p]),

@@ -1091,6 +1091,22 @@ int apply_device(h2gpu_image* im, int n_vec, const double* X, long long x_rs, lo
     return H2GPU_OK;
 }
 
+// Apply without events or host synchronisation (the CG engine), in the given precision.
+int apply_quiet(h2gpu_image* im, int precision, int n_vec, const double* X, int ldx, double* Y, int ldy,
+                cudaStream_t s)
+{
+    const int saved = im->precision;
+    im->precision = precision;
+    int NV = panel_width(n_vec, (im->BD_JIT && im->kd == 3) ? std::min(im->max_nv, 8) : im->max_nv);
+    if (im->tuned_nv > 0) NV = std::min(NV, im->tuned_nv);
+    int st = prepare(im, NV);
+    for (int c0 = 0; st == H2GPU_OK && c0 < n_vec; c0 += NV)
+        st = run_panel(im, NV, std::min(NV, n_vec - c0), X + c0, ldx, 1, Y + c0, ldy, 1, s, false);
+    im->precision = saved;
+    if (st == H2GPU_OK) im->st.n_matvec += n_vec;
+    return st;
+}
+
 int ensure_io(h2gpu_image* im, size_t elems)
 {
     if (im->io_elems >= elems) return H2GPU_OK;
@@ -1698,3 +1714,27 @@ H2G_API int h2gpu_autotune(h2gpu_image* im, int n_vec, const double* dX, int ldx
     if (best_variant) *best_variant = bvar;
     return H2GPU_OK;
 }
+
+// ------------------------------------------------ hooks for the CG engine (h2gpu_solve.cu)
+
+namespace h2gpu {
+
+int set_error(int code, const char* msg) { return fail(code, "%s", msg); }
+
+int image_apply_quiet(h2gpu_image* im, int precision, int n_vec, const double* dX, int ldx, double* dY, int ldy)
+{
+    std::lock_guard<std::mutex> lk(im->mu);
+    if (cudaSetDevice(im->device) != cudaSuccess) return fail(H2GPU_ERR_CUDA, "cudaSetDevice failed");
+    return apply_quiet(im, precision, n_vec, dX, ldx, dY, ldy, im->stream);
+}
+
+int image_info(const h2gpu_image* im, int* N, int* device, int* precision, void** stream)
+{
+    *N = im->N;
+    *device = im->device;
+    *precision = im->precision;
+    *stream = (void*) im->stream;
+    return H2GPU_OK;
+}
+
+}  // namespace h2gpu

@@ -2,23 +2,26 @@
 
 A :class:`Server` keeps several H2 images resident in HBM (admitted while their
 device footprint fits a budget) and serves requests for (K + mu I) x = b solves and
-(K + mu I) b products.  Requests that arrive while others run are admitted into free
-slots of their matrix's slot block at the next iteration boundary; every step applies
-each busy matrix once to the panel of all its active slots (one device matmul of up
-to ``max_slots`` right-hand sides), so the work of different requests overlaps on the
-device.  A finished request frees its slot at once.
+(K + mu I) b products.  Each resident matrix has a device CG engine
+(``h2gpu_cg_*``, include/h2gpu.h) with 16 slots: requests that arrive while others
+run are admitted into free slots between batches of iterations, every iteration
+applies the matrix once to the panel of all its slots (one H2 matmul), a finished
+request frees its slot at once, and the engines of different matrices run on their
+images' own streams, so their work overlaps on the device.
 
 The solver is H2Pack's left-preconditioned CG (examples/PCG/pcg.c:11-152, identity
-preconditioner, shift wrapper of examples/SPDHSS-H2/pcg_tests.c:13-20) run in lock
-step for all slots of a block: FP64 vectors and inner products on the device, the
-operator in the image's precision, and every ``refresh`` iterations (and before
-declaring convergence) the true residual b - (K + mu I) x recomputed with the FP64
-operator and CG restarted from it -- iterative refinement, so a mixed-precision
-operator still reaches the FP64 tolerance (with an FP64 operator the true residual is
-only recomputed when the recursive one claims convergence, as pcg.c:129-138 does once).
+preconditioner, shift wrapper of examples/SPDHSS-H2/pcg_tests.c:13-20) in lock step
+for the slots of an engine: FP64 vectors and inner products on the device, the
+operator in the image's precision, and every ``refresh`` iterations (and whenever
+the recursive residual claims convergence) the true residual b - (K + mu I) x
+recomputed with the FP64 operator and CG restarted from it -- iterative refinement,
+so a mixed-precision operator still reaches the FP64 tolerance.  The host enqueues
+``iters_per_sync`` iterations per engine and reads the 16 slot records once after
+them; it never waits per iteration.
 """
 from __future__ import annotations
 
+import ctypes as C
 import dataclasses
 import heapq
 import time
@@ -26,6 +29,7 @@ import time
 import numpy as np
 import torch
 
+from . import _abi
 from .h2pack import Image
 
 
@@ -45,41 +49,40 @@ class Request:
     iters: int = 0
     relres: float | None = None
     converged: bool = False
-
-
-class ShiftedOperator:
-    """y = (K + mu I) x for device panels, K applied by an image in its precision and,
-    for residual recomputation, in FP64 (the same image switched for that call)."""
-
-    def __init__(self, image: Image, mu: float, precision: str):
-        self.img, self.mu, self.precision = image, float(mu), precision
-        self.N = image.N
-
-    def apply(self, X: torch.Tensor, fp64: bool = False) -> torch.Tensor:
-        if fp64 and self.precision != "fp64":
-            self.img.set_precision("fp64")
-            try:
-                Y = self.img.matmul_device(X)
-            finally:
-                self.img.set_precision(self.precision)
-        else:
-            Y = self.img.matmul_device(X)
-        return Y.add_(X, alpha=self.mu)
+    history: list | None = None   # ||r||_2 after every CG iteration (Server.run(history=True))
 
 
 class SlotBlock:
-    """Up to ``max_slots`` requests of one matrix advanced in lock step."""
+    """Up to 16 requests of one matrix advanced in lock step by its device CG engine."""
 
-    def __init__(self, op: ShiftedOperator, max_slots: int, refresh: int):
-        self.op, self.S, self.refresh = op, max_slots, refresh
-        N = op.N
-        z = lambda: torch.zeros(N, max_slots, dtype=torch.float64, device="cuda")  # noqa: E731
-        self.B, self.X, self.R, self.P = z(), z(), z(), z()
-        self.rho = torch.ones(max_slots, dtype=torch.float64, device="cuda")
-        self.bnorm = torch.ones(max_slots, dtype=torch.float64, device="cuda")
-        self.req: list[Request | None] = [None] * max_slots
-        self.it = [0] * max_slots          # iterations since the last restart
-        self.free = list(range(max_slots))
+    def __init__(self, image: Image, mu: float, precision: str, max_slots: int, refresh: int,
+                 iters_per_sync: int):
+        self.img, self.lib, self.N = image, image.lib, image.N
+        image.set_precision(precision)
+        h = C.c_void_p()
+        _abi.check(self.lib.h2gpu_cg_create(image.handle, float(mu), int(refresh), C.byref(h)), self.lib,
+                   "h2gpu_cg_create")
+        self.h = h
+        self.S = max(1, min(int(max_slots), 16))
+        self.k = max(1, int(iters_per_sync))
+        self.req: list[Request | None] = [None] * 16
+        self.free = list(range(self.S - 1, -1, -1))
+        self.history = False
+        self.need_check = False
+        self._st = (C.c_int * 16)()
+        self._it = (C.c_int * 16)()
+        self._rr = (C.c_double * 16)()
+
+    def close(self):
+        if self.h:
+            self.lib.h2gpu_cg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # pragma: no cover - interpreter shutdown
+            pass
 
     def busy(self) -> bool:
         return len(self.free) < self.S
@@ -90,92 +93,54 @@ class SlotBlock:
         k = self.free.pop()
         self.req[k] = r
         r.start = now
-        self.B[:, k] = r.b
-        self.X[:, k] = 0.0
-        self.R[:, k] = r.b                 # r = b - A*0
-        self.P[:, k] = 0.0
-        self.rho[k] = 1.0
-        self.bnorm[k] = torch.linalg.vector_norm(r.b)
-        self.it[k] = 0
+        kind = _abi.CG_PCG if r.kind == "pcg" else _abi.CG_MATVEC
+        _abi.check(self.lib.h2gpu_cg_admit(self.h, k, kind, C.c_void_p(r.b.data_ptr()), float(r.tol),
+                                           int(r.max_iter)), self.lib, "h2gpu_cg_admit")
         return True
 
-    def _release(self, k: int, now: float, out: list):
-        r = self.req[k]
-        r.finish = now
-        out.append(r)
-        self.req[k] = None
-        self.free.append(k)
+    def launch(self):
+        """Enqueue (without waiting) the pending true-residual checks and k iterations."""
+        if self.need_check:
+            _abi.check(self.lib.h2gpu_cg_check(self.h), self.lib, "h2gpu_cg_check")
+        _abi.check(self.lib.h2gpu_cg_step(self.h, self.k), self.lib, "h2gpu_cg_step")
 
-    def step(self, now_fn, out: list):
-        """One operator application for every active slot of the block."""
-        act = [k for k in range(self.S) if self.req[k] is not None]
-        if not act:
-            return
-        idx = torch.tensor(act, device="cuda")
-        mv = [k for k in act if self.req[k].kind == "matvec"]
-        cg = [k for k in act if self.req[k].kind == "pcg"]
-        # panel: b for matvec slots, the CG direction for PCG slots
-        if cg:
-            cgi = torch.tensor(cg, device="cuda")
-            # z = r (identity preconditioner); rho0 = rho; rho = r'z; p = z + beta p
-            rho_new = (self.R[:, cgi] * self.R[:, cgi]).sum(0)
-            first = torch.tensor([self.it[k] == 0 for k in cg], device="cuda")
-            beta = torch.where(first, torch.zeros_like(rho_new), rho_new / self.rho[cgi])
-            self.P[:, cgi] = self.R[:, cgi] + beta * self.P[:, cgi]
-            self.rho[cgi] = rho_new
-        panel = torch.empty(self.op.N, len(act), dtype=torch.float64, device="cuda")
-        for j, k in enumerate(act):
-            panel[:, j] = self.B[:, k] if self.req[k].kind == "matvec" else self.P[:, k]
-        AP = self.op.apply(panel)
-        col = {k: j for j, k in enumerate(act)}
+    def collect(self, now_fn, out: list):
+        """Wait for the engine, hand out finished requests, note slots awaiting a check."""
+        _abi.check(self.lib.h2gpu_cg_sync(self.h, self._st, self._it, self._rr), self.lib, "h2gpu_cg_sync")
         t = now_fn()
-        for k in mv:
+        self.need_check = False
+        for k in range(16):
             r = self.req[k]
-            r.x = AP[:, col[k]].clone()
-            r.iters = 1
-            self._release(k, t, out)
-        if cg:
-            cgi = torch.tensor(cg, device="cuda")
-            S = AP[:, [col[k] for k in cg]]
-            pAp = (self.P[:, cgi] * S).sum(0)
-            alpha = self.rho[cgi] / pAp
-            self.X[:, cgi] += alpha * self.P[:, cgi]
-            self.R[:, cgi] -= alpha * S
-            rn = torch.linalg.vector_norm(self.R[:, cgi], dim=0) / self.bnorm[cgi]
-            rn_h = rn.cpu().numpy()
-            refresh = []
-            for j, k in enumerate(cg):
-                self.it[k] += 1
-                self.req[k].iters += 1
-                periodic = self.op.precision != "fp64" and self.refresh > 0 and self.it[k] >= self.refresh
-                if rn_h[j] <= self.req[k].tol or periodic or self.req[k].iters >= self.req[k].max_iter:
-                    refresh.append(k)
-            if refresh:
-                self._refresh(refresh, now_fn, out)
-
-    def _refresh(self, ks, now_fn, out):
-        """True residual with the FP64 operator; converged slots leave, others restart CG."""
-        ki = torch.tensor(ks, device="cuda")
-        AX = self.op.apply(self.X[:, ki].contiguous(), fp64=True)
-        Rt = self.B[:, ki] - AX
-        rn = (torch.linalg.vector_norm(Rt, dim=0) / self.bnorm[ki]).cpu().numpy()
-        t = now_fn()
-        for j, k in enumerate(ks):
-            r = self.req[k]
-            self.R[:, k] = Rt[:, j]
-            self.it[k] = 0
-            if rn[j] <= r.tol or r.iters >= r.max_iter:
-                r.relres = float(rn[j])
-                r.converged = bool(rn[j] <= r.tol)
-                r.x = self.X[:, k].clone()
-                self._release(k, t, out)
+            if r is None:
+                continue
+            st = self._st[k]
+            if st == _abi.CG_CHECK:
+                self.need_check = True
+            elif st == _abi.CG_DONE:
+                x = torch.empty(self.N, dtype=torch.float64, device="cuda")
+                _abi.check(self.lib.h2gpu_cg_take(self.h, k, C.c_void_p(x.data_ptr())), self.lib, "h2gpu_cg_take")
+                r.x = x
+                r.iters = int(self._it[k])
+                if r.kind == "pcg":
+                    r.relres = float(self._rr[k])
+                    r.converged = r.relres <= r.tol
+                    if self.history:
+                        buf = np.zeros(max(1, r.iters))
+                        n = self.lib.h2gpu_cg_history(self.h, k, buf.ctypes.data_as(C.POINTER(C.c_double)), len(buf))
+                        r.history = [float(v) for v in buf[:max(0, n)]]
+                r.finish = t
+                out.append(r)
+                self.req[k] = None
+                self.free.append(k)
 
 
 class Server:
     """Resident matrices + continuous batching of matvec / PCG requests."""
 
-    def __init__(self, budget_bytes: float = 150e9, max_slots: int = 16, refresh: int = 200):
-        self.budget, self.max_slots, self.refresh = float(budget_bytes), max_slots, refresh
+    def __init__(self, budget_bytes: float = 150e9, max_slots: int = 16, refresh: int = 200,
+                 iters_per_sync: int = 8):
+        self.budget, self.max_slots, self.refresh = float(budget_bytes), min(int(max_slots), 16), refresh
+        self.iters_per_sync = iters_per_sync
         self.blocks: dict[str, SlotBlock] = {}
         self.footprint: dict[str, float] = {}
 
@@ -185,22 +150,27 @@ class Server:
     def admit_matrix(self, name: str, image: Image, mu: float, precision: str = "mixed") -> bool:
         """Keep the image resident if its footprint (image + slot block) fits the budget."""
         st = image.stats()
-        slot_bytes = 8.0 * image.N * self.max_slots * 6
-        need = float(st["device_bytes"]) + slot_bytes + 8.0 * image.N * self.max_slots * 4
+        engine_bytes = 8.0 * image.N * 16 * 5          # b, x, r, p, Ap panels of the CG engine
+        need = float(st["device_bytes"]) + engine_bytes
         if self.used_bytes() + need > self.budget:
             return False
-        image.set_precision(precision)
-        self.blocks[name] = SlotBlock(ShiftedOperator(image, mu, precision), self.max_slots, self.refresh)
+        self.blocks[name] = SlotBlock(image, mu, precision, self.max_slots,
+                                      self.refresh if precision != "fp64" else 0, self.iters_per_sync)
         self.footprint[name] = need
         return True
 
     def evict(self, name: str):
-        self.blocks.pop(name, None)
+        blk = self.blocks.pop(name, None)
+        if blk is not None:
+            blk.close()
         self.footprint.pop(name, None)
 
-    def run(self, requests: list[Request], realtime: bool = True) -> list[Request]:
+    def run(self, requests: list[Request], realtime: bool = True, history: bool = False) -> list[Request]:
         """Serve requests whose ``arrival`` offsets follow the wall clock (realtime) or
-        are all present at time 0 (realtime=False).  Returns them in completion order."""
+        are all present at time 0 (realtime=False).  Returns them in completion order.
+        ``history`` records every PCG request's residual norm after each iteration."""
+        for blk in self.blocks.values():
+            blk.history = history
         pending = [(r.arrival if realtime else 0.0, r.rid, r) for r in requests]
         heapq.heapify(pending)
         waiting: dict[str, list[Request]] = {n: [] for n in self.blocks}
@@ -208,9 +178,11 @@ class Server:
         t0 = time.perf_counter()
 
         def now():
-            torch.cuda.synchronize()
             return time.perf_counter() - t0
 
+        # the right-hand sides were written on torch's stream; the engines read them on
+        # their images' streams
+        torch.cuda.current_stream().synchronize()
         while pending or any(waiting.values()) or any(b.busy() for b in self.blocks.values()):
             t = now()
             while pending and pending[0][0] <= t:
@@ -227,8 +199,10 @@ class Server:
                 if pending:
                     time.sleep(max(0.0, min(pending[0][0] - now(), 0.001)))
                 continue
+            for blk in busy:          # all engines enqueue first: their work overlaps
+                blk.launch()
             for blk in busy:
-                blk.step(now, done)
+                blk.collect(now, done)
         return done
 
 

@@ -240,6 +240,42 @@ int h2gpu_autotune(h2gpu_image *img, int n_vec, const double *dX, int ldx, doubl
  */
 int h2gpu_set_jit_variant(h2gpu_image *img, int variant);
 
+/*
+ * Lock-step conjugate gradients on (K + mu I) for up to 16 requests ("slots") of one
+ * image, on the device.  Each PCG slot runs H2Pack's left-preconditioned CG with the
+ * identity preconditioner (examples/PCG/pcg.c:11-152) on the shifted operator of
+ * examples/SPDHSS-H2/pcg_tests.c:13-20, with FP64 vectors and inner products and
+ * the operator in the image's precision at h2gpu_cg_create; a MATVEC slot computes
+ * (K + mu I) b once.  All 16 slots are the columns of one panel, so each iteration
+ * is one H2 matmul plus five small kernels, enqueued on the image's stream; the host
+ * reads the slot records with h2gpu_cg_sync once per batch of iterations.
+ *
+ * A slot whose recursive residual reaches tol ||b|| (or max_iter, or, for a mixed
+ * operator, `refresh` iterations since its last restart) enters H2GPU_CG_CHECK;
+ * h2gpu_cg_check recomputes b - (K + mu I) x with the FP64 operator and the slot
+ * either finishes (H2GPU_CG_DONE; relres is then the true relative residual) or
+ * restarts CG from that residual.  Reductions have a fixed order and columns are
+ * independent.  d_b / d_x are device vectors of krnl_dim * n_point doubles in the
+ * caller's (original) order; the caller orders its own writes of d_b before
+ * h2gpu_cg_admit.  One engine per image (it uses the image's work buffers and
+ * stream).  No counterpart in the reference (pcg.c runs one vector on the host).
+ */
+typedef struct h2gpu_cg h2gpu_cg;
+#define H2GPU_CG_FREE   0
+#define H2GPU_CG_RUN    1
+#define H2GPU_CG_CHECK  2
+#define H2GPU_CG_DONE   3
+#define H2GPU_CG_MATVEC 0
+#define H2GPU_CG_PCG    1
+int h2gpu_cg_create(h2gpu_image *img, double mu, int refresh, h2gpu_cg **out);
+int h2gpu_cg_destroy(h2gpu_cg *cg);
+int h2gpu_cg_admit(h2gpu_cg *cg, int slot, int kind, const double *d_b, double tol, int max_iter);
+int h2gpu_cg_step(h2gpu_cg *cg, int n_iter);
+int h2gpu_cg_check(h2gpu_cg *cg);
+int h2gpu_cg_sync(h2gpu_cg *cg, int *state, int *iters, double *relres);   /* 16 entries each */
+int h2gpu_cg_take(h2gpu_cg *cg, int slot, double *d_x);
+int h2gpu_cg_history(h2gpu_cg *cg, int slot, double *out, int max_n);      /* ||r|| per iteration; returns count */
+
 int h2gpu_get_stats(h2gpu_image *img, h2gpu_stats *st);
 int h2gpu_reset_stats(h2gpu_image *img);
 size_t h2gpu_image_bytes(const h2gpu_image *img);

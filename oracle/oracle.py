@@ -238,6 +238,39 @@ def matmul(desc: _abi.Desc, X: np.ndarray, layout: int = _abi.ROW_MAJOR) -> np.n
     return res
 
 
+# ------------------------------------------------------------ PCG restated
+
+def pcg(apply, b: np.ndarray, tol: float, max_iter: int, x0: np.ndarray | None = None):
+    """Left-preconditioned CG with the identity preconditioner, restated step by step from
+    examples/PCG/pcg.c:11-152 (r = b - A x; rho = r'z; p = z + (rho/rho0) p, p = z at the
+    first iteration; alpha = rho / p'Ap; stop when ||r|| <= tol ||b|| or max_iter).
+    ``apply`` maps a vector to A x (e.g. H2Pack's CPU H2P_matvec plus mu x, the wrapper of
+    examples/SPDHSS-H2/pcg_tests.c:13-20).  Returns (x, flag, relres, iters, res_history),
+    flag 0 when converged as pcg.c:131; relres is the recursive residual as pcg.c:132."""
+    b = np.asarray(b, dtype=np.float64)
+    x = np.zeros_like(b) if x0 is None else np.array(x0, dtype=np.float64)
+    r = b - apply(x)
+    b2 = float(np.sqrt(b @ b))
+    rn = float(np.sqrt(r @ r))
+    stop = b2 * tol
+    it, rho = 0, 1.0
+    p = np.zeros_like(b)
+    hist = []
+    while it < max_iter and rn > stop:
+        z = r                                  # invMx == NULL: z = r (pcg.c:71-72)
+        rho0, rho = rho, float(r @ z)
+        beta = rho / rho0
+        p = z.copy() if it == 0 else z + beta * p
+        s = apply(p)
+        alpha = rho / float(p @ s)
+        x = x + alpha * p
+        r = r - alpha * s
+        rn = float(np.sqrt(r @ r))
+        hist.append(rn)
+        it += 1
+    return x, (0 if rn <= stop else 1), rn / b2, it, np.array(hist)
+
+
 # -------------------------------------------------- the reference library
 
 class RefH2:

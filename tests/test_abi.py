@@ -43,3 +43,16 @@ def test_missing_library_fails_loudly(tmp_path, monkeypatch):
     monkeypatch.setattr(_abi, "_cache", {})
     with pytest.raises(RuntimeError, match="no CPU fallback"):
         _abi.libh2gpu()
+
+
+def test_cg_engine_argument_checks_without_gpu():
+    """The CG engine refuses bad handles and arguments before any CUDA call."""
+    lib = _abi.libh2gpu()
+    h = C.c_void_p()
+    assert lib.h2gpu_cg_create(None, 1e-2, 0, C.byref(h)) == _abi.H2GPU_OK - 1
+    assert lib.h2gpu_cg_admit(None, 0, _abi.CG_PCG, None, 1e-6, 10) == _abi.H2GPU_OK - 1
+    assert lib.h2gpu_cg_step(None, 1) == _abi.H2GPU_OK - 1
+    assert lib.h2gpu_cg_check(None) == _abi.H2GPU_OK - 1
+    assert lib.h2gpu_cg_take(None, 0, None) == _abi.H2GPU_OK - 1
+    assert lib.h2gpu_cg_destroy(None) == _abi.H2GPU_OK
+    assert b"NULL" in lib.h2gpu_last_error()

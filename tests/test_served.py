@@ -106,3 +106,34 @@ def test_admission_by_footprint(mats):
     srv = Server(budget_bytes=need * 10 + 1e8, max_slots=4)
     assert srv.admit_matrix("g", img, MU)
     assert not srv.admit_matrix("g2", img, MU) or srv.used_bytes() <= srv.budget
+
+
+def test_pcg_fp64_follows_reference_pcg(mats):
+    """The served solver with the FP64 operator against pcg.c restated (oracle.pcg) driven by
+    the reference library's own CPU H2P_matvec on the same handle: the residual histories
+    agree while rounding differences are still small, and both converge in nearly the same
+    number of iterations."""
+    import torch
+    from oracle import oracle as O
+    from h2pack_b200.serve import Server, Request
+    H = mats["m"]
+    g = torch.Generator(device="cuda").manual_seed(21)
+    b = torch.randn(H.N, dtype=torch.float64, device="cuda", generator=g)
+    srv = Server(max_slots=2)
+    assert srv.admit_matrix("m", H.image(), MU, "fp64")
+    done = srv.run([Request(rid=1, matrix="m", kind="pcg", b=b, tol=1e-6)], realtime=False, history=True)
+    r = done[0]
+
+    def cpu_apply(x):
+        y = np.zeros_like(x)
+        O.libref().H2P_matvec(H.h2pack, O.dptr(np.ascontiguousarray(x)), O.dptr(y))
+        return y + MU * x
+
+    bh = b.cpu().numpy()
+    x, flag, relres, iters, hist = O.pcg(cpu_apply, bh, 1e-6, 5000)
+    assert flag == 0 and r.converged
+    assert abs(r.iters - iters) <= max(3, iters // 20)
+    h_gpu = np.array(r.history)
+    k = min(20, len(hist), len(h_gpu))
+    assert np.max(np.abs(h_gpu[:k] - hist[:k]) / hist[:k]) < 1e-8
+    assert rel(r.x.cpu().numpy(), x) < 1e-3
