@@ -409,7 +409,15 @@ int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
     auto alloc = [&](int rows) { long long r = ps; ps += rows; return (int) r; };
     std::vector<std::vector<int>> y1s(n_node), asms(n_node), pair_y1, pair_asm;
     std::vector<char> has_y1(n_node, 0);
-    const int R = 64;
+    // Stored blocks: one task per block of up to RB rows (larger blocks split evenly
+    // into tasks of a multiple of 64 rows).  A task's kernel walks its rows in chunks
+    // of 64 and adds the chunks' transposed products into the task's single slot, so
+    // a block has one A^T w slot per task instead of one per 64-row chunk.
+    const int RB = 1024;
+    auto rows_per_task = [&](int nr) {
+        const int nt = (nr + RB - 1) / RB;
+        return ((nr + nt - 1) / nt + 63) / 64 * 64;
+    };
     std::vector<BlkTask>& blkB = hp.blkB;
     std::vector<BlkTask>& blkD = hp.blkD;
     std::vector<JitTarget>& jtN = hp.jtN;
@@ -434,6 +442,7 @@ int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
             int in1 = (l0 < l1) ? mc[2 * n0] : N + y0r[n0];
             int s0 = alloc(nr);
             if (l0 < l1) asms[n0].push_back(s0); else { y1s[n0].push_back(s0); }
+            const int R = rows_per_task(nr);
             for (int r0 = 0; r0 < nr; r0 += R)
             {
                 int rr = std::min(R, nr - r0);
@@ -456,6 +465,7 @@ int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
             bool diag = i < d->n_leaf_node;
             int s0 = alloc(nr);
             asms[n0].push_back(s0);
+            const int R = rows_per_task(nr);
             for (int r0 = 0; r0 < nr; r0 += R)
             {
                 int rr = std::min(R, nr - r0);
@@ -764,11 +774,12 @@ int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
             int dst = leaf ? alloc(nr) : y0r[d->children[n * d->max_child]];
             if (leaf) asms[n].push_back(dst);
             if (leaf && !pair_asm.empty()) pair_asm[n].push_back(dst);
-            for (int r0 = 0; r0 < nr; r0 += R)
+            const int RD = 64;       // downward tasks: one 64-row chunk of U each
+            for (int r0 = 0; r0 < nr; r0 += RD)
             {
                 DownTask t;
                 t.u_off = u_off[n] + (long long) r0 * nc;
-                t.nrow = std::min(R, nr - r0); t.ncol = nc;
+                t.nrow = std::min(RD, nr - r0); t.ncol = nc;
                 t.y1_row = has_y1[n] ? y0r[n] : -1;
                 t.push_row = push ? y0r[n] : -1;
                 t.dst_ps = leaf ? 1 : 0;

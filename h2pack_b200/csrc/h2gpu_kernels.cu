@@ -288,7 +288,7 @@ template <typename TA, int NV, typename VIN>
 __device__ __forceinline__ void chunk_apply(const TA* __restrict__ A, int R, int ncol, VIN vin,
                                             const double* __restrict__ win_XS, int win_row,
                                             double* __restrict__ out0, double* __restrict__ out1,
-                                            double* __restrict__ smem)
+                                            double* __restrict__ smem, bool add1 = false)
 {
     constexpr int S = SV<NV>::v;
     double* s_w = smem;
@@ -346,7 +346,8 @@ __device__ __forceinline__ void chunk_apply(const TA* __restrict__ A, int R, int
                     double s = 0.0;
 #pragma unroll
                     for (int k = 0; k < kWarps; k++) s += s_red[k][cc][v];
-                    out1[(long long) (ct + cc) * NV + v] = s;
+                    double* o = out1 + (long long) (ct + cc) * NV + v;
+                    *o = add1 ? *o + s : s;
                 }
             }
         }
@@ -356,100 +357,86 @@ __device__ __forceinline__ void chunk_apply(const TA* __restrict__ A, int R, int
         for (int i = threadIdx.x; i < R * NV; i += kThreads) out0[i] = s_o0[i];
 }
 
-// Stored block chunk, single right-hand side (the matvec path, memory bound).
-// Warp w owns columns CPL*32*w + lane + 32j (j < CPL, +CPL*256k) and walks all rows
-// of the chunk 8 at a time: 8*CPL independent loads per lane in flight (CPL = 2 for
-// FP32 blocks, so both precisions keep the same bytes in flight), A^T w completes in
-// registers (no reduction), and the 8 row partials of A v are combined with one
-// transposed butterfly per 8 x 32*CPL tile; the warps' row partials are summed once
-// at the end.
+// Stored block (task of up to 1024 rows), single right-hand side (the matvec path,
+// memory bound).  The task is walked in chunks of 64 rows; warp w owns rows
+// 8w..8w+7 of a chunk and its lanes sweep the columns 32*CPL at a time (CPL = 2 for
+// FP32 blocks, so both precisions keep the same bytes in flight per lane).  A v completes per lane across the sweep and is combined with one transposed
+// butterfly per chunk (no cross-warp sum: the warp owns its rows); the 8 warps'
+// partials of A^T w are summed in warp order through shared memory every 256 columns
+// and added into the task's single out1 slot (stored by the first chunk, added by
+// the later ones; the same thread owns the same column in every chunk).
 template <typename TA>
-__global__ void __launch_bounds__(256, sizeof(TA) == 4 ? 3 : 4) k_blk1(const BlkTask* __restrict__ tasks, const TA* __restrict__ arena,
+__global__ void __launch_bounds__(256, 3) k_blk1(const BlkTask* __restrict__ tasks, const TA* __restrict__ arena,
                                               const double* __restrict__ XS, double* __restrict__ PS)
 {
     constexpr int CPL = sizeof(TA) == 4 ? 2 : 1;
-    constexpr int CS = 1024;
-    __shared__ double s_v[CS];
-    __shared__ double s_w[64];
-    __shared__ double s_red[kWarps][64];
+    constexpr int CW = 256;                       // columns per shared reduction of A^T w
+    __shared__ double s_q[kWarps][CW];
     const BlkTask T = tasks[blockIdx.x];
-    const TA* A = arena + T.a_off;
-    const int R = T.nrow, ncol = T.ncol, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int ncol = T.ncol, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const bool do0 = T.out0_row >= 0, do1 = T.out1_row >= 0;
-    for (int r = threadIdx.x; r < 64; r += 256) s_w[r] = (do1 && r < R) ? XS[T.in1_row + r] : 0.0;
-    double part[8];
-#pragma unroll
-    for (int gI = 0; gI < 8; gI++) part[gI] = 0.0;
-    const int myrow = nv_of_lane<8>(lane);
-    for (int cs = 0; cs < ncol; cs += CS)
+    for (int rc = 0; rc < T.nrow; rc += 64)
     {
-        const int cend = min(ncol, cs + CS);
-        __syncthreads();
-        if (do0)
-            for (int c = cs + threadIdx.x; c < cend; c += 256) s_v[c - cs] = XS[T.in0_row + c];
-        __syncthreads();
-        for (int cc = cs + 32 * CPL * w; cc < cend; cc += 256 * CPL)
+        const int nr = max(0, min(8, min(64, T.nrow - rc) - 8 * w));   // rows of this warp
+        const int r0 = rc + 8 * w;
+        const TA* A = arena + T.a_off + (long long) r0 * ncol;
+        double wr[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) wr[k] = (do1 && k < nr) ? XS[T.in1_row + r0 + k] : 0.0;
+        double p[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) p[k] = 0.0;
+        for (int cw = 0; cw < ncol; cw += CW)
         {
-            int c[CPL];
-            bool cv[CPL];
-            double vc[CPL], acc1[CPL];
-#pragma unroll
-            for (int j = 0; j < CPL; j++)
+            const int cend = min(ncol, cw + CW);
+            for (int cs = cw; cs < cend; cs += 32 * CPL)
             {
-                c[j] = cc + lane + 32 * j;
-                cv[j] = c[j] < cend;
-                vc[j] = (do0 && cv[j]) ? s_v[c[j] - cs] : 0.0;
-                acc1[j] = 0.0;
-            }
-#pragma unroll
-            for (int gI = 0; gI < 8; gI++)
-            {
-                if (8 * gI >= R) break;
+                int c[CPL];
+                bool cv[CPL];
+                double vc[CPL];
                 TA a[CPL][8];            // raw loads in flight, widened at use
 #pragma unroll
                 for (int j = 0; j < CPL; j++)
+                {
+                    c[j] = cs + lane + 32 * j;
+                    cv[j] = c[j] < cend;
+                    vc[j] = (do0 && cv[j]) ? XS[T.in0_row + c[j]] : 0.0;
+#pragma unroll
+                    for (int k = 0; k < 8; k++) a[j][k] = (cv[j] && k < nr) ? A[(long long) k * ncol + c[j]] : TA(0);
+                }
+#pragma unroll
+                for (int j = 0; j < CPL; j++)
+                {
+                    double q = 0.0;
 #pragma unroll
                     for (int k = 0; k < 8; k++)
                     {
-                        const int r = 8 * gI + k;
-                        a[j][k] = (cv[j] && r < R) ? A[(long long) r * ncol + c[j]] : TA(0);
-                    }
-                double p[8];
-#pragma unroll
-                for (int k = 0; k < 8; k++)
-                {
-                    p[k] = 0.0;
-#pragma unroll
-                    for (int j = 0; j < CPL; j++)
-                    {
                         const double ad = to_d(a[j][k]);
-                        acc1[j] = fma(ad, s_w[8 * gI + k], acc1[j]);
+                        q = fma(ad, wr[k], q);
                         p[k] = fma(ad, vc[j], p[k]);
                     }
-                }
-                if (do0)
-                {
-                    warp_transpose_reduce<8>(p, lane);
-                    part[gI] += p[0];
+                    if (do1) s_q[w][cs - cw + lane + 32 * j] = q;
                 }
             }
+            if (do1)
+            {
+                __syncthreads();
+                for (int t = threadIdx.x; t < cend - cw; t += 256)
+                {
+                    double sum = 0.0;
 #pragma unroll
-            for (int j = 0; j < CPL; j++)
-                if (do1 && cv[j]) PS[T.out1_row + c[j]] = acc1[j];
+                    for (int k = 0; k < kWarps; k++) sum += s_q[k][t];
+                    double* o = PS + T.out1_row + cw + t;
+                    *o = (rc == 0) ? sum : *o + sum;
+                }
+                __syncthreads();
+            }
         }
-    }
-    if (do0)
-    {
-        if (lane_writes<8>(lane))
-#pragma unroll
-            for (int gI = 0; gI < 8; gI++) s_red[w][8 * gI + myrow] = part[gI];
-        __syncthreads();
-        for (int r = threadIdx.x; r < R; r += 256)
+        if (do0)
         {
-            double sum = 0.0;
-#pragma unroll
-            for (int k = 0; k < kWarps; k++) sum += s_red[k][r];
-            PS[T.out0_row + r] = sum;
+            warp_transpose_reduce<8>(p, lane);
+            const int row = nv_of_lane<8>(lane);
+            if (lane_writes<8>(lane) && row < nr) PS[T.out0_row + r0 + row] = p[0];
         }
     }
 }
@@ -470,19 +457,24 @@ __global__ void __launch_bounds__(256) k_blk_gemm(const BlkTask* __restrict__ ta
     __shared__ double sV[CT][NV];
     __shared__ double sW[RT][NV];
     const BlkTask T = tasks[blockIdx.x];
-    const TA* A = arena + T.a_off;
-    const int t = threadIdx.x, R = T.nrow, ncol = T.ncol;
+    const int t = threadIdx.x, ncol = T.ncol;
     const bool do0 = T.out0_row >= 0, do1 = T.out1_row >= 0;
     const int m = t / NG0, v0 = (t % NG0) * VPT0;
     const int c1 = t / NG1, w0 = (t % NG1) * VPT1;
+    // the task's rows in chunks of RT; the chunks' C1 parts add into one slot
+    for (int rc = 0; rc < T.nrow; rc += RT)
+    {
+    const TA* A = arena + T.a_off + (long long) rc * ncol;
+    const int R = min(RT, T.nrow - rc);
     double acc0[VPT0];
 #pragma unroll
     for (int j = 0; j < VPT0; j++) acc0[j] = 0.0;
+    __syncthreads();
     if (do1)
         for (int i = t; i < RT * NV; i += 256)
         {
             int r = i / NV, v = i % NV;
-            sW[r][v] = (r < R) ? XS[(long long) (T.in1_row + r) * NV + v] : 0.0;
+            sW[r][v] = (r < R) ? XS[(long long) (T.in1_row + rc + r) * NV + v] : 0.0;
         }
     for (int ct = 0; ct < ncol; ct += CT)
     {
@@ -521,12 +513,17 @@ __global__ void __launch_bounds__(256) k_blk_gemm(const BlkTask* __restrict__ ta
                 for (int j = 0; j < VPT1; j++) acc1[j] = fma(a, sW[r][w0 + j], acc1[j]);
             }
 #pragma unroll
-            for (int j = 0; j < VPT1; j++) PS[(long long) (T.out1_row + ct + c1) * NV + w0 + j] = acc1[j];
+            for (int j = 0; j < VPT1; j++)
+            {
+                double* o = PS + (long long) (T.out1_row + ct + c1) * NV + w0 + j;
+                *o = (rc == 0) ? acc1[j] : *o + acc1[j];
+            }
         }
     }
     if (do0 && m < R)
 #pragma unroll
-        for (int j = 0; j < VPT0; j++) PS[(long long) (T.out0_row + m) * NV + v0 + j] = acc0[j];
+        for (int j = 0; j < VPT0; j++) PS[(long long) (T.out0_row + rc + m) * NV + v0 + j] = acc0[j];
+    }
 }
 
 template <typename TA, int NV>
@@ -536,9 +533,14 @@ __global__ void __launch_bounds__(kThreads) k_blk(const BlkTask* __restrict__ ta
     extern __shared__ double dsm[];
     const BlkTask t = tasks[blockIdx.x];
     VFromXS vin{XS, t.in0_row};
-    chunk_apply<TA, NV>(arena + t.a_off, t.nrow, t.ncol, vin, XS, t.in1_row,
-                        t.out0_row >= 0 ? PS + (long long) t.out0_row * NV : nullptr,
-                        t.out1_row >= 0 ? PS + (long long) t.out1_row * NV : nullptr, dsm);
+    // the task's rows in chunks of 64; the chunks' A^T w parts add into one slot
+    for (int rc = 0; rc < t.nrow; rc += 64)
+    {
+        chunk_apply<TA, NV>(arena + t.a_off + (long long) rc * t.ncol, min(64, t.nrow - rc), t.ncol, vin, XS,
+                            t.in1_row + rc, t.out0_row >= 0 ? PS + (long long) (t.out0_row + rc) * NV : nullptr,
+                            t.out1_row >= 0 ? PS + (long long) t.out1_row * NV : nullptr, dsm, rc > 0);
+        __syncthreads();
+    }
 }
 
 template <typename TA, int NV>
@@ -1265,15 +1267,17 @@ constexpr int pair_smem_bytes()
 
 // --------------------------------------- stored blocks on the tensor cores (FP32)
 
-// Stored block chunk (R <= 64 rows x ncol, FP32 copy) for panels of 8 / 16 right-hand
-// sides, both products on the tensor cores with the right-hand sides as the M = 16
-// side of m16n8k8 (3xTF32, FP32 accumulation):
+// Stored block task (up to 1024 rows x ncol, FP32 copy, walked in chunks of R <= 64
+// rows) for panels of 8 / 16 right-hand sides, both products on the tensor cores with
+// the right-hand sides as the M = 16 side of m16n8k8 (3xTF32, FP32 accumulation):
 //   C1^T (NV x ncol) = W^T (NV x R) A        [B operand = A, k = rows]      warps 0-3
 //   C0^T (NV x R)    = V^T (NV x ncol) A^T   [B operand = A^T, k = columns] warps 4-7
 // Column tiles of 32 are staged in shared memory (double-buffered through registers);
 // each tile feeds both products.  Warp w < 4 owns columns 8w..8w+7 of every tile and
-// completes C1 for them over the R rows; warp 4 + u owns rows 16u..16u+15 and sums
-// C0 over the tiles (FP32 per tile, FP64 across tiles).
+// completes the chunk's part of C1 for them over its R rows, stored by the first chunk
+// into the task's single C1 slot and added by the later ones (FP64; the same thread
+// owns the same element in every chunk); warp 4 + u owns rows 16u..16u+15 of the chunk
+// and sums C0 over the tiles (FP32 per tile, FP64 across tiles).
 template <int NV>
 __global__ void __launch_bounds__(256, 3) k_blk_tc(const BlkTask* __restrict__ tasks, const float* __restrict__ arena,
                                                    const double* __restrict__ XS, double* __restrict__ PS)
@@ -1283,8 +1287,7 @@ __global__ void __launch_bounds__(256, 3) k_blk_tc(const BlkTask* __restrict__ t
     __shared__ uint4 s_w[8][32][2];               // W^T fragments per k-step of 8 rows: hi, lo
     __shared__ uint4 s_v[2][4][32][2];            // V^T fragments per k-step of 8 columns: hi, lo
     const BlkTask T = tasks[blockIdx.x];
-    const float* A = arena + T.a_off;
-    const int R = T.nrow, ncol = T.ncol;
+    const int ncol = T.ncol;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, tq = lane & 3;
     const bool do0 = T.out0_row >= 0, do1 = T.out1_row >= 0;
 
@@ -1306,124 +1309,137 @@ __global__ void __launch_bounds__(256, 3) k_blk_tc(const BlkTask* __restrict__ t
         hi = make_uint4(h[0], h[1], h[2], h[3]);
         lo = make_uint4(l[0], l[1], l[2], l[3]);
     };
-    // W^T fragments for the whole chunk (8 k-steps of 8 rows), one warp per k-step
-    if (do1)
-        frag(T.in1_row, R, 8 * warp, s_w[warp][lane][0], s_w[warp][lane][1]);
 
-    // tile staging: 64 x 32 floats, 8 per thread; V^T fragments of the tile's columns
-    float ra[8];
-    uint4 rvh = make_uint4(0, 0, 0, 0), rvl = rvh;
-    auto load_tile = [&](int c0) {
-#pragma unroll
-        for (int u = 0; u < 8; u++)
-        {
-            const int e = threadIdx.x + 256 * u, r = e >> 5, c = e & 31;
-            ra[u] = (r < R && c0 + c < ncol) ? A[(long long) r * ncol + c0 + c] : 0.f;
-        }
-        if (do0 && warp < 4) frag(T.in0_row + c0, ncol - c0, 8 * warp, rvh, rvl);
-    };
-    auto store_tile = [&](int buf) {
-#pragma unroll
-        for (int u = 0; u < 8; u++)
-        {
-            const int e = threadIdx.x + 256 * u;
-            s_a[buf][e >> 5][e & 31] = ra[u];
-        }
-        if (do0 && warp < 4) { s_v[buf][warp][lane][0] = rvh; s_v[buf][warp][lane][1] = rvl; }
-    };
-
-    double c0acc[2][4];
-#pragma unroll
-    for (int n = 0; n < 2; n++)
-#pragma unroll
-        for (int q = 0; q < 4; q++) c0acc[n][q] = 0.0;
-
-    if (ncol > 0)
+    // the task's rows in chunks of 64; the chunks' C1 parts add into one slot
+    for (int rc = 0; rc < T.nrow; rc += 64)
     {
-        load_tile(0);
-        store_tile(0);
-    }
-    __syncthreads();
-    int buf = 0;
-    for (int c0 = 0; c0 < ncol; c0 += CT)
-    {
-        const bool more = c0 + CT < ncol;
-        if (more) load_tile(c0 + CT);
-        if (warp < 4)
-        {
-            if (do1)
+        const float* A = arena + T.a_off + (long long) rc * ncol;
+        const int R = min(64, T.nrow - rc);
+        __syncthreads();                          // previous chunk done with s_w / s_a / s_v
+        // W^T fragments for the chunk (8 k-steps of 8 rows), one warp per k-step
+        if (do1)
+            frag(T.in1_row + rc, R, 8 * warp, s_w[warp][lane][0], s_w[warp][lane][1]);
+
+        // tile staging: 64 x 32 floats, 8 per thread; V^T fragments of the tile's columns
+        float ra[8];
+        uint4 rvh = make_uint4(0, 0, 0, 0), rvl = rvh;
+        auto load_tile = [&](int c0) {
+#pragma unroll
+            for (int u = 0; u < 8; u++)
             {
-                // C1^T for columns c0 + 8w .. +7: k over the R rows (8 k-steps)
-                float d[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};   // two chains, summed
-                const int ksteps = (R + 7) >> 3;
-#pragma unroll
-                for (int ks = 0; ks < 8; ks++)
-                {
-                    if (ks >= ksteps) break;
-                    const float b0 = s_a[buf][8 * ks + tq][8 * warp + g];
-                    const float b1 = s_a[buf][8 * ks + tq + 4][8 * warp + g];
-                    const uint32_t h0 = tf32_rna(b0), h1 = tf32_rna(b1);
-                    const uint32_t l0 = __float_as_uint(b0 - __uint_as_float(h0)),
-                                   l1 = __float_as_uint(b1 - __uint_as_float(h1));
-                    const uint4 wh = s_w[ks][lane][0], wl = s_w[ks][lane][1];
-                    float (&dd)[4] = d[ks & 1];
-                    mma_tf32(dd, wl.x, wl.y, wl.z, wl.w, h0, h1);
-                    mma_tf32(dd, wh.x, wh.y, wh.z, wh.w, l0, l1);
-                    mma_tf32(dd, wh.x, wh.y, wh.z, wh.w, h0, h1);
-                }
-                // rows of the fragment = right-hand sides (g, g+8), columns = (2tq, 2tq+1)
-                const int cb = c0 + 8 * warp + 2 * tq;
-#pragma unroll
-                for (int q = 0; q < 4; q++)
-                {
-                    const int rhs = (q < 2) ? g : g + 8, col = cb + (q & 1);
-                    if (rhs < NV && col < ncol) PS[(long long) (T.out1_row + col) * NV + rhs] = (double) (d[0][q] + d[1][q]);
-                }
+                const int e = threadIdx.x + 256 * u, r = e >> 5, c = e & 31;
+                ra[u] = (r < R && c0 + c < ncol) ? A[(long long) r * ncol + c0 + c] : 0.f;
             }
-        } else if (do0) {
-            // C0^T for rows 16u .. 16u+15 (two n-tiles of 8): k over the tile's 32 columns
-            const int u = warp - 4;
-            if (16 * u < R)
+            if (do0 && warp < 4) frag(T.in0_row + c0, ncol - c0, 8 * warp, rvh, rvl);
+        };
+        auto store_tile = [&](int buf) {
+#pragma unroll
+            for (int u = 0; u < 8; u++)
             {
-                float d[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
-#pragma unroll
-                for (int ks = 0; ks < 4; ks++)
-                {
-                    const uint4 vh = s_v[buf][ks][lane][0], vl = s_v[buf][ks][lane][1];
-#pragma unroll
-                    for (int n = 0; n < 2; n++)
-                    {
-                        const int row = 16 * u + 8 * n + g;
-                        const float b0 = s_a[buf][row][8 * ks + tq], b1 = s_a[buf][row][8 * ks + tq + 4];
-                        const uint32_t h0 = tf32_rna(b0), h1 = tf32_rna(b1);
-                        const uint32_t l0 = __float_as_uint(b0 - __uint_as_float(h0)),
-                                       l1 = __float_as_uint(b1 - __uint_as_float(h1));
-                        mma_tf32(d[n], vl.x, vl.y, vl.z, vl.w, h0, h1);
-                        mma_tf32(d[n], vh.x, vh.y, vh.z, vh.w, l0, l1);
-                        mma_tf32(d[n], vh.x, vh.y, vh.z, vh.w, h0, h1);
-                    }
-                }
-#pragma unroll
-                for (int n = 0; n < 2; n++)
-#pragma unroll
-                    for (int q = 0; q < 4; q++) c0acc[n][q] += (double) d[n][q];
+                const int e = threadIdx.x + 256 * u;
+                s_a[buf][e >> 5][e & 31] = ra[u];
             }
-        }
-        if (more) store_tile(buf ^ 1);
-        __syncthreads();
-        buf ^= 1;
-    }
-    if (do0 && warp >= 4)
-    {
-        const int u = warp - 4;
+            if (do0 && warp < 4) { s_v[buf][warp][lane][0] = rvh; s_v[buf][warp][lane][1] = rvl; }
+        };
+
+        double c0acc[2][4];
 #pragma unroll
         for (int n = 0; n < 2; n++)
 #pragma unroll
-            for (int q = 0; q < 4; q++)
+            for (int q = 0; q < 4; q++) c0acc[n][q] = 0.0;
+
+        if (ncol > 0)
+        {
+            load_tile(0);
+            store_tile(0);
+        }
+        __syncthreads();
+        int buf = 0;
+        for (int c0 = 0; c0 < ncol; c0 += CT)
+        {
+            const bool more = c0 + CT < ncol;
+            if (more) load_tile(c0 + CT);
+            if (warp < 4)
             {
-                const int rhs = (q < 2) ? g : g + 8, row = 16 * u + 8 * n + 2 * tq + (q & 1);
-                if (rhs < NV && row < R) PS[(long long) (T.out0_row + row) * NV + rhs] = c0acc[n][q];
+                if (do1)
+                {
+                    // C1^T for columns c0 + 8w .. +7: k over the R rows (8 k-steps)
+                    float d[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};   // two chains, summed
+                    const int ksteps = (R + 7) >> 3;
+#pragma unroll
+                    for (int ks = 0; ks < 8; ks++)
+                    {
+                        if (ks >= ksteps) break;
+                        const float b0 = s_a[buf][8 * ks + tq][8 * warp + g];
+                        const float b1 = s_a[buf][8 * ks + tq + 4][8 * warp + g];
+                        const uint32_t h0 = tf32_rna(b0), h1 = tf32_rna(b1);
+                        const uint32_t l0 = __float_as_uint(b0 - __uint_as_float(h0)),
+                                       l1 = __float_as_uint(b1 - __uint_as_float(h1));
+                        const uint4 wh = s_w[ks][lane][0], wl = s_w[ks][lane][1];
+                        float (&dd)[4] = d[ks & 1];
+                        mma_tf32(dd, wl.x, wl.y, wl.z, wl.w, h0, h1);
+                        mma_tf32(dd, wh.x, wh.y, wh.z, wh.w, l0, l1);
+                        mma_tf32(dd, wh.x, wh.y, wh.z, wh.w, h0, h1);
+                    }
+                    // rows of the fragment = right-hand sides (g, g+8), columns = (2tq, 2tq+1)
+                    const int cb = c0 + 8 * warp + 2 * tq;
+#pragma unroll
+                    for (int q = 0; q < 4; q++)
+                    {
+                        const int rhs = (q < 2) ? g : g + 8, col = cb + (q & 1);
+                        if (rhs < NV && col < ncol)
+                        {
+                            double* o = PS + (long long) (T.out1_row + col) * NV + rhs;
+                            const double v = (double) (d[0][q] + d[1][q]);
+                            *o = (rc == 0) ? v : *o + v;
+                        }
+                    }
+                }
+            } else if (do0) {
+                // C0^T for rows 16u .. 16u+15 (two n-tiles of 8): k over the tile's 32 columns
+                const int u = warp - 4;
+                if (16 * u < R)
+                {
+                    float d[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+#pragma unroll
+                    for (int ks = 0; ks < 4; ks++)
+                    {
+                        const uint4 vh = s_v[buf][ks][lane][0], vl = s_v[buf][ks][lane][1];
+#pragma unroll
+                        for (int n = 0; n < 2; n++)
+                        {
+                            const int row = 16 * u + 8 * n + g;
+                            const float b0 = s_a[buf][row][8 * ks + tq], b1 = s_a[buf][row][8 * ks + tq + 4];
+                            const uint32_t h0 = tf32_rna(b0), h1 = tf32_rna(b1);
+                            const uint32_t l0 = __float_as_uint(b0 - __uint_as_float(h0)),
+                                           l1 = __float_as_uint(b1 - __uint_as_float(h1));
+                            mma_tf32(d[n], vl.x, vl.y, vl.z, vl.w, h0, h1);
+                            mma_tf32(d[n], vh.x, vh.y, vh.z, vh.w, l0, l1);
+                            mma_tf32(d[n], vh.x, vh.y, vh.z, vh.w, h0, h1);
+                        }
+                    }
+#pragma unroll
+                    for (int n = 0; n < 2; n++)
+#pragma unroll
+                        for (int q = 0; q < 4; q++) c0acc[n][q] += (double) d[n][q];
+                }
             }
+            if (more) store_tile(buf ^ 1);
+            __syncthreads();
+            buf ^= 1;
+        }
+        if (do0 && warp >= 4)
+        {
+            const int u = warp - 4;
+#pragma unroll
+            for (int n = 0; n < 2; n++)
+#pragma unroll
+                for (int q = 0; q < 4; q++)
+                {
+                    const int rhs = (q < 2) ? g : g + 8, row = 16 * u + 8 * n + 2 * tq + (q & 1);
+                    if (rhs < NV && row < R) PS[(long long) (T.out0_row + rc + row) * NV + rhs] = c0acc[n][q];
+                }
+        }
     }
 }
 
