@@ -54,7 +54,7 @@ def parse():
                         "served requests)")
     p.add_argument("--precisions", default="fp64,mixed",
                    help="stored-block workloads: which paths to time (comma list)")
-    p.add_argument("--n-matrices", type=int, default=64)
+    p.add_argument("--n-matrices", type=int, default=512)
     p.add_argument("--n-requests", type=int, default=96)
     p.add_argument("--served-matrices", type=int, default=32)
     p.add_argument("--served-nmax", type=int, default=500_000)
@@ -497,7 +497,7 @@ def log_uniform(rng, lo, hi, k):
 
 
 def run_batched(args):
-    """Config 4 (reduced count by default): independent H2 matrices with N log-uniform in
+    """Config 4: --n-matrices (512) independent H2 matrices with N log-uniform in
     [2000, 64000], kernels alternating Coulomb / Gaussian exp(-r^2) (l = 1), reltol 1e-6, JIT
     mode, 8 RHS each.  One batched image per kernel (flattened cross-matrix task lists),
     CUDA-graph-captured apply, autotuned panel / kernel choice.  value = matrix-RHS products/s."""
