@@ -1267,44 +1267,29 @@ constexpr int pair_smem_bytes()
 
 // --------------------------------------- stored blocks on the tensor cores (FP32)
 
-// Stored block task (up to 1024 rows x ncol, FP32 copy) for panels of 8 / 16
-// right-hand sides, both products on the tensor cores with the right-hand sides as
-// the M = 16 side of m16n8k8 (3xTF32, FP32 accumulation):
+// Stored block task (up to 1024 rows x ncol, FP32 copy, walked in chunks of R <= 64
+// rows) for panels of 8 / 16 right-hand sides, both products on the tensor cores with
+// the right-hand sides as the M = 16 side of m16n8k8 (3xTF32, FP32 accumulation):
 //   C1^T (NV x ncol) = W^T (NV x R) A        [B operand = A, k = rows]      warps 0-3
 //   C0^T (NV x R)    = V^T (NV x ncol) A^T   [B operand = A^T, k = columns] warps 4-7
-// The task is one flat sequence of 64 x 64 tiles (64-row chunk, then its column tiles);
-// tile t+1 (A, and the V^T fragments of its columns; W^T of its chunk when it starts
-// one) is read from global memory into registers while tile t is multiplied from
-// shared memory, so global latency overlaps the MMAs across chunk boundaries too.
-// Warp w < 4 owns columns 16w..16w+15 of a tile and completes the tile's C1 part over
-// the chunk's rows (stored by the first chunk into the task's single C1 slot, added by
-// the later ones; FP64, the same thread owns the same element in every chunk); warp
-// 4 + u owns rows 16u..16u+15 of the chunk and sums C0 over the chunk's tiles (FP32 per
-// tile, FP64 across tiles).  Shared A rows are swizzled (column ^ 4 * bit 2 of the row)
-// so that both fragment patterns read conflict-free.
-struct BlkTcSmem {
-    float a[2][64][72];                           // A tiles (64 x 64, padded, swizzled)
-    uint4 v[2][8][32][2];                         // V^T fragments per k-step of 8 columns: hi, lo
-    uint4 w[2][8][32][2];                         // W^T fragments per k-step of 8 rows (per chunk parity)
-};
-
+// Column tiles of 32 are staged in shared memory (double-buffered through registers);
+// each tile feeds both products.  Warp w < 4 owns columns 8w..8w+7 of every tile and
+// completes the chunk's part of C1 for them over its R rows, stored by the first chunk
+// into the task's single C1 slot and added by the later ones (FP64; the same thread
+// owns the same element in every chunk); warp 4 + u owns rows 16u..16u+15 of the chunk
+// and sums C0 over the tiles (FP32 per tile, FP64 across tiles).
 template <int NV>
-__global__ void __launch_bounds__(256, 2) k_blk_tc(const BlkTask* __restrict__ tasks, const float* __restrict__ arena,
+__global__ void __launch_bounds__(256, 3) k_blk_tc(const BlkTask* __restrict__ tasks, const float* __restrict__ arena,
                                                    const double* __restrict__ XS, double* __restrict__ PS)
 {
-    constexpr int CT = 64;
-    extern __shared__ __align__(16) unsigned char blk_smem[];
-    BlkTcSmem& sm = *reinterpret_cast<BlkTcSmem*>(blk_smem);
-    auto& s_a = sm.a;
-    auto& s_v = sm.v;
-    auto& s_w = sm.w;
+    constexpr int CT = 32, S = CT + 4;            // tile width; padded shared row (conflict-free C0 reads)
+    __shared__ float s_a[2][64][S];
+    __shared__ uint4 s_w[8][32][2];               // W^T fragments per k-step of 8 rows: hi, lo
+    __shared__ uint4 s_v[2][4][32][2];            // V^T fragments per k-step of 8 columns: hi, lo
     const BlkTask T = tasks[blockIdx.x];
-    const int ncol = T.ncol, nrow = T.nrow;
+    const int ncol = T.ncol;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, tq = lane & 3;
     const bool do0 = T.out0_row >= 0, do1 = T.out1_row >= 0;
-    const int ntc = (ncol + CT - 1) / CT;         // column tiles per chunk
-    const int nt = ntc * ((nrow + 63) / 64);      // tiles of the task
-    auto swz = [](int r, int c) { return c ^ (((r >> 2) & 1) << 2); };
 
     // A-fragment of an (NV x 8) slice of X^T: X rows k0 + {tq, tq+4}, right-hand sides {g, g+8}
     auto frag = [&](int row0, int nrows, int k0, uint4& hi, uint4& lo) {
@@ -1325,151 +1310,136 @@ __global__ void __launch_bounds__(256, 2) k_blk_tc(const BlkTask* __restrict__ t
         lo = make_uint4(l[0], l[1], l[2], l[3]);
     };
 
-    // staging registers of one tile
-    float ra[16];
-    uint4 rvh = make_uint4(0, 0, 0, 0), rvl = rvh, rwh = rvh, rwl = rvh;
-    auto load_tile = [&](int t) {
-        const int rc = (t / ntc) * 64, c0 = (t % ntc) * CT, R = min(64, nrow - rc);
-        const float* A = arena + T.a_off + (long long) rc * ncol + c0;
-#pragma unroll
-        for (int u = 0; u < 16; u++)
-        {
-            const int e = threadIdx.x + 256 * u, r = e >> 6, c = e & 63;
-            ra[u] = (r < R && c0 + c < ncol) ? A[(long long) r * ncol + c] : 0.f;
-        }
-        if (do0) frag(T.in0_row + c0, ncol - c0, 8 * warp, rvh, rvl);
-        if (do1 && c0 == 0) frag(T.in1_row + rc, R, 8 * warp, rwh, rwl);
-    };
-    auto store_tile = [&](int t, int buf) {
-        const int c0 = (t % ntc) * CT, chunk = t / ntc;
-#pragma unroll
-        for (int u = 0; u < 16; u++)
-        {
-            const int e = threadIdx.x + 256 * u, r = e >> 6, c = e & 63;
-            s_a[buf][r][swz(r, c)] = ra[u];
-        }
-        if (do0) { s_v[buf][warp][lane][0] = rvh; s_v[buf][warp][lane][1] = rvl; }
-        if (do1 && c0 == 0) { s_w[chunk & 1][warp][lane][0] = rwh; s_w[chunk & 1][warp][lane][1] = rwl; }
-    };
-
-    double c0acc[2][4];
-#pragma unroll
-    for (int n = 0; n < 2; n++)
-#pragma unroll
-        for (int q = 0; q < 4; q++) c0acc[n][q] = 0.0;
-
-    if (nt > 0)
+    // the task's rows in chunks of 64; the chunks' C1 parts add into one slot
+    for (int rc = 0; rc < T.nrow; rc += 64)
     {
-        load_tile(0);
-        store_tile(0, 0);
-    }
-    __syncthreads();
-    for (int t = 0; t < nt; t++)
-    {
-        const int buf = t & 1, chunk = t / ntc, rc = chunk * 64, c0 = (t % ntc) * CT;
-        const int R = min(64, nrow - rc);
-        const bool more = t + 1 < nt;
-        if (more) load_tile(t + 1);
-        if (warp < 4)
-        {
-            if (do1)
+        const float* A = arena + T.a_off + (long long) rc * ncol;
+        const int R = min(64, T.nrow - rc);
+        __syncthreads();                          // previous chunk done with s_w / s_a / s_v
+        // W^T fragments for the chunk (8 k-steps of 8 rows), one warp per k-step
+        if (do1)
+            frag(T.in1_row + rc, R, 8 * warp, s_w[warp][lane][0], s_w[warp][lane][1]);
+
+        // tile staging: 64 x 32 floats, 8 per thread; V^T fragments of the tile's columns
+        float ra[8];
+        uint4 rvh = make_uint4(0, 0, 0, 0), rvl = rvh;
+        auto load_tile = [&](int c0) {
+#pragma unroll
+            for (int u = 0; u < 8; u++)
             {
-                // C1^T for columns c0 + 16w .. +15 (two n-tiles): k over the chunk's rows
-                float d[2][2][4];
+                const int e = threadIdx.x + 256 * u, r = e >> 5, c = e & 31;
+                ra[u] = (r < R && c0 + c < ncol) ? A[(long long) r * ncol + c0 + c] : 0.f;
+            }
+            if (do0 && warp < 4) frag(T.in0_row + c0, ncol - c0, 8 * warp, rvh, rvl);
+        };
+        auto store_tile = [&](int buf) {
 #pragma unroll
-                for (int n = 0; n < 2; n++)
+            for (int u = 0; u < 8; u++)
+            {
+                const int e = threadIdx.x + 256 * u;
+                s_a[buf][e >> 5][e & 31] = ra[u];
+            }
+            if (do0 && warp < 4) { s_v[buf][warp][lane][0] = rvh; s_v[buf][warp][lane][1] = rvl; }
+        };
+
+        double c0acc[2][4];
 #pragma unroll
-                    for (int p = 0; p < 2; p++)
+        for (int n = 0; n < 2; n++)
 #pragma unroll
-                        for (int q = 0; q < 4; q++) d[n][p][q] = 0.f;
-                const int ksteps = (R + 7) >> 3;
-#pragma unroll
-                for (int ks = 0; ks < 8; ks++)
+            for (int q = 0; q < 4; q++) c0acc[n][q] = 0.0;
+
+        if (ncol > 0)
+        {
+            load_tile(0);
+            store_tile(0);
+        }
+        __syncthreads();
+        int buf = 0;
+        for (int c0 = 0; c0 < ncol; c0 += CT)
+        {
+            const bool more = c0 + CT < ncol;
+            if (more) load_tile(c0 + CT);
+            if (warp < 4)
+            {
+                if (do1)
                 {
-                    if (ks >= ksteps) break;
-                    const uint4 wh = s_w[chunk & 1][ks][lane][0], wl = s_w[chunk & 1][ks][lane][1];
-                    const int r0 = 8 * ks + tq, r1 = r0 + 4;
+                    // C1^T for columns c0 + 8w .. +7: k over the R rows (8 k-steps)
+                    float d[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};   // two chains, summed
+                    const int ksteps = (R + 7) >> 3;
 #pragma unroll
-                    for (int n = 0; n < 2; n++)
+                    for (int ks = 0; ks < 8; ks++)
                     {
-                        const int col = 16 * warp + 8 * n + g;
-                        const float b0 = s_a[buf][r0][swz(r0, col)], b1 = s_a[buf][r1][swz(r1, col)];
+                        if (ks >= ksteps) break;
+                        const float b0 = s_a[buf][8 * ks + tq][8 * warp + g];
+                        const float b1 = s_a[buf][8 * ks + tq + 4][8 * warp + g];
                         const uint32_t h0 = tf32_rna(b0), h1 = tf32_rna(b1);
                         const uint32_t l0 = __float_as_uint(b0 - __uint_as_float(h0)),
                                        l1 = __float_as_uint(b1 - __uint_as_float(h1));
-                        float (&dd)[4] = d[n][ks & 1];
+                        const uint4 wh = s_w[ks][lane][0], wl = s_w[ks][lane][1];
+                        float (&dd)[4] = d[ks & 1];
                         mma_tf32(dd, wl.x, wl.y, wl.z, wl.w, h0, h1);
                         mma_tf32(dd, wh.x, wh.y, wh.z, wh.w, l0, l1);
                         mma_tf32(dd, wh.x, wh.y, wh.z, wh.w, h0, h1);
                     }
-                }
-                // rows of the fragment = right-hand sides (g, g+8), columns = (2tq, 2tq+1)
-#pragma unroll
-                for (int n = 0; n < 2; n++)
+                    // rows of the fragment = right-hand sides (g, g+8), columns = (2tq, 2tq+1)
+                    const int cb = c0 + 8 * warp + 2 * tq;
 #pragma unroll
                     for (int q = 0; q < 4; q++)
                     {
-                        const int rhs = (q < 2) ? g : g + 8, col = c0 + 16 * warp + 8 * n + 2 * tq + (q & 1);
+                        const int rhs = (q < 2) ? g : g + 8, col = cb + (q & 1);
                         if (rhs < NV && col < ncol)
                         {
                             double* o = PS + (long long) (T.out1_row + col) * NV + rhs;
-                            const double v = (double) (d[n][0][q] + d[n][1][q]);
+                            const double v = (double) (d[0][q] + d[1][q]);
                             *o = (rc == 0) ? v : *o + v;
                         }
                     }
-            }
-        } else if (do0) {
-            // C0^T for rows 16u .. 16u+15 (two n-tiles of 8): k over the tile's 64 columns
-            const int u = warp - 4;
-            if (16 * u < R)
-            {
-                float d[2][2][4];
-#pragma unroll
-                for (int n = 0; n < 2; n++)
-#pragma unroll
-                    for (int p = 0; p < 2; p++)
-#pragma unroll
-                        for (int q = 0; q < 4; q++) d[n][p][q] = 0.f;
-#pragma unroll
-                for (int ks = 0; ks < 8; ks++)
+                }
+            } else if (do0) {
+                // C0^T for rows 16u .. 16u+15 (two n-tiles of 8): k over the tile's 32 columns
+                const int u = warp - 4;
+                if (16 * u < R)
                 {
-                    const uint4 vh = s_v[buf][ks][lane][0], vl = s_v[buf][ks][lane][1];
+                    float d[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+#pragma unroll
+                    for (int ks = 0; ks < 4; ks++)
+                    {
+                        const uint4 vh = s_v[buf][ks][lane][0], vl = s_v[buf][ks][lane][1];
+#pragma unroll
+                        for (int n = 0; n < 2; n++)
+                        {
+                            const int row = 16 * u + 8 * n + g;
+                            const float b0 = s_a[buf][row][8 * ks + tq], b1 = s_a[buf][row][8 * ks + tq + 4];
+                            const uint32_t h0 = tf32_rna(b0), h1 = tf32_rna(b1);
+                            const uint32_t l0 = __float_as_uint(b0 - __uint_as_float(h0)),
+                                           l1 = __float_as_uint(b1 - __uint_as_float(h1));
+                            mma_tf32(d[n], vl.x, vl.y, vl.z, vl.w, h0, h1);
+                            mma_tf32(d[n], vh.x, vh.y, vh.z, vh.w, l0, l1);
+                            mma_tf32(d[n], vh.x, vh.y, vh.z, vh.w, h0, h1);
+                        }
+                    }
 #pragma unroll
                     for (int n = 0; n < 2; n++)
-                    {
-                        const int row = 16 * u + 8 * n + g;
-                        const float b0 = s_a[buf][row][swz(row, 8 * ks + tq)];
-                        const float b1 = s_a[buf][row][swz(row, 8 * ks + tq + 4)];
-                        const uint32_t h0 = tf32_rna(b0), h1 = tf32_rna(b1);
-                        const uint32_t l0 = __float_as_uint(b0 - __uint_as_float(h0)),
-                                       l1 = __float_as_uint(b1 - __uint_as_float(h1));
-                        float (&dd)[4] = d[n][ks & 1];
-                        mma_tf32(dd, vl.x, vl.y, vl.z, vl.w, h0, h1);
-                        mma_tf32(dd, vh.x, vh.y, vh.z, vh.w, l0, l1);
-                        mma_tf32(dd, vh.x, vh.y, vh.z, vh.w, h0, h1);
-                    }
+#pragma unroll
+                        for (int q = 0; q < 4; q++) c0acc[n][q] += (double) d[n][q];
                 }
-#pragma unroll
-                for (int n = 0; n < 2; n++)
-#pragma unroll
-                    for (int q = 0; q < 4; q++) c0acc[n][q] += (double) (d[n][0][q] + d[n][1][q]);
             }
-            if (c0 + CT >= ncol)
-            {
-                // last tile of the chunk: its rows of C0 are complete
-#pragma unroll
-                for (int n = 0; n < 2; n++)
-#pragma unroll
-                    for (int q = 0; q < 4; q++)
-                    {
-                        const int rhs = (q < 2) ? g : g + 8, row = 16 * u + 8 * n + 2 * tq + (q & 1);
-                        if (rhs < NV && row < R) PS[(long long) (T.out0_row + rc + row) * NV + rhs] = c0acc[n][q];
-                        c0acc[n][q] = 0.0;
-                    }
-            }
+            if (more) store_tile(buf ^ 1);
+            __syncthreads();
+            buf ^= 1;
         }
-        if (more) store_tile(t + 1, buf ^ 1);
-        __syncthreads();
+        if (do0 && warp >= 4)
+        {
+            const int u = warp - 4;
+#pragma unroll
+            for (int n = 0; n < 2; n++)
+#pragma unroll
+                for (int q = 0; q < 4; q++)
+                {
+                    const int rhs = (q < 2) ? g : g + 8, row = 16 * u + 8 * n + 2 * tq + (q & 1);
+                    if (rhs < NV && row < R) PS[(long long) (T.out0_row + rc + row) * NV + rhs] = c0acc[n][q];
+                }
+        }
     }
 }
 
@@ -1579,17 +1549,8 @@ cudaError_t launch_blk(int NV, const BlkTask* t, int n, const TA* arena, const d
     {
         if (use_tc && n > 0 && (NV == 8 || NV == 16))
         {
-            constexpr int b = (int) sizeof(BlkTcSmem);
-            if (NV == 16)
-            {
-                cudaError_t e = allow_smem(k_blk_tc<16>, b);
-                if (e != cudaSuccess) return e;
-                k_blk_tc<16><<<n, 256, b, st>>>(t, arena, XS, PS);
-            } else {
-                cudaError_t e = allow_smem(k_blk_tc<8>, b);
-                if (e != cudaSuccess) return e;
-                k_blk_tc<8><<<n, 256, b, st>>>(t, arena, XS, PS);
-            }
+            if (NV == 16) k_blk_tc<16><<<n, 256, 0, st>>>(t, arena, XS, PS);
+            else k_blk_tc<8><<<n, 256, 0, st>>>(t, arena, XS, PS);
             return cudaGetLastError();
         }
     }
