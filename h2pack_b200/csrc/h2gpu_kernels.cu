@@ -649,13 +649,23 @@ template <> struct Scalar<KRNL_MATERN32_ID, float> {
 // FP32 kernel values for admissible (well-separated) pairs only: r2 > 0 always, so the
 // coincident-point cases drop out; constants are folded once per launch (prep).
 template <int KID> struct ScalarFar;
+// f2: the same for two values at once with packed FP32x2 arithmetic (sm_100).
 template <> struct ScalarFar<KRNL_COULOMB_ID> {
     static __device__ __forceinline__ void prep(float, float, float& q0, float& q1) { q0 = 0.f; q1 = 0.f; }
     static __device__ __forceinline__ float f(float r2, float, float) { return rsqrt_approx(r2); }
+    static __device__ __forceinline__ float2 f2(float2 r2, float, float)
+    {
+        return make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
+    }
 };
 template <> struct ScalarFar<KRNL_GAUSSIAN_ID> {
     static __device__ __forceinline__ void prep(float p0, float, float& q0, float& q1) { q0 = -p0 * kLog2e; q1 = 0.f; }
     static __device__ __forceinline__ float f(float r2, float q0, float) { return ex2_approx(r2 * q0); }
+    static __device__ __forceinline__ float2 f2(float2 r2, float q0, float)
+    {
+        const float2 t = __fmul2_rn(r2, make_float2(q0, q0));
+        return make_float2(ex2_approx(t.x), ex2_approx(t.y));
+    }
 };
 template <> struct ScalarFar<KRNL_MATERN32_ID> {
     static __device__ __forceinline__ void prep(float, float c0, float& q0, float& q1) { q0 = c0; q1 = c0 * kLog2e; }
@@ -664,6 +674,13 @@ template <> struct ScalarFar<KRNL_MATERN32_ID> {
         const float r = r2 * rsqrt_approx(r2);
         const float e = ex2_approx(q1 * r);
         return fmaf(-q0 * r, e, e);
+    }
+    static __device__ __forceinline__ float2 f2(float2 r2, float q0, float q1)
+    {
+        const float2 r = __fmul2_rn(r2, make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y)));
+        const float2 t = __fmul2_rn(r, make_float2(q1, q1));
+        const float2 e = make_float2(ex2_approx(t.x), ex2_approx(t.y));
+        return __ffma2_rn(__fmul2_rn(r, make_float2(-q0, -q0)), e, e);
     }
 };
 
@@ -942,9 +959,11 @@ __global__ void __launch_bounds__(256, 4) k_jit_tc(const JitTarget* __restrict__
             const int nj = min(TS, sc.npt - cj);
             const float ax = x0.x + sc.sx, ay = x0.y + sc.sy, az = x0.z + sc.sz;
             const float bx = x1.x + sc.sx, by = x1.y + sc.sy, bz = x1.z + sc.sz;
-            // far form: -2a and |a|^2 of both target rows in the source set's frame
-            const float ma_x = -2.f * ax, ma_y = -2.f * ay, ma_z = -2.f * az, a2 = ax * ax + ay * ay + az * az;
-            const float mb_x = -2.f * bx, mb_y = -2.f * by, mb_z = -2.f * bz, b2 = bx * bx + by * by + bz * bz;
+            // far form: -2a and |a|^2 of both target rows in the source set's frame, as
+            // (row g, row g+8) pairs for packed FP32x2 arithmetic
+            const float2 m_x = make_float2(-2.f * ax, -2.f * bx), m_y = make_float2(-2.f * ay, -2.f * by),
+                         m_z = make_float2(-2.f * az, -2.f * bz);
+            const float2 s2 = make_float2(ax * ax + ay * ay + az * az, bx * bx + by * by + bz * bz);
             const int ngrp = (nj + 7) >> 3;
 #pragma unroll 2
             for (int grp = 0; grp < ngrp; grp++)
@@ -953,31 +972,44 @@ __global__ void __launch_bounds__(256, 4) k_jit_tc(const JitTarget* __restrict__
                 float k[4];
                 if constexpr (FAR)
                 {
-                    auto r2f = [](float mx, float my, float mz, float s2, const float4& p) {
-                        return fmaxf(fmaf(mx, p.x, fmaf(my, p.y, fmaf(mz, p.z, s2 + p.w))), 1e-30f);
+                    // r^2 of rows (g, g+8) against one source point: 4 packed instructions
+                    // for two values.  No clamp: admissible pairs keep r^2 far from 0.
+                    auto r2p = [&](const float4& p) {
+                        float2 t = __fadd2_rn(s2, make_float2(p.w, p.w));
+                        t = __ffma2_rn(m_z, make_float2(p.z, p.z), t);
+                        t = __ffma2_rn(m_y, make_float2(p.y, p.y), t);
+                        return __ffma2_rn(m_x, make_float2(p.x, p.x), t);
                     };
-                    k[0] = ScalarFar<KID>::f(r2f(ma_x, ma_y, ma_z, a2, pa), q0, q1);   // (g,   t)
-                    k[1] = ScalarFar<KID>::f(r2f(mb_x, mb_y, mb_z, b2, pa), q0, q1);   // (g+8, t)
-                    k[2] = ScalarFar<KID>::f(r2f(ma_x, ma_y, ma_z, a2, pb), q0, q1);   // (g,   t+4)
-                    k[3] = ScalarFar<KID>::f(r2f(mb_x, mb_y, mb_z, b2, pb), q0, q1);   // (g+8, t+4)
+                    const float2 ka = ScalarFar<KID>::f2(r2p(pa), q0, q1);   // (g, t), (g+8, t)
+                    const float2 kb = ScalarFar<KID>::f2(r2p(pb), q0, q1);   // (g, t+4), (g+8, t+4)
+                    k[0] = ka.x; k[1] = ka.y; k[2] = kb.x; k[3] = kb.y;
                 } else {
-                    float dx = ax - pa.x, dy = ay - pa.y, dz = az - pa.z;
-                    k[0] = Scalar<KID, float>::f(dx * dx + dy * dy + dz * dz, p0, c0);   // (g,   t)
-                    dx = bx - pa.x; dy = by - pa.y; dz = bz - pa.z;
-                    k[1] = Scalar<KID, float>::f(dx * dx + dy * dy + dz * dz, p0, c0);   // (g+8, t)
-                    dx = ax - pb.x; dy = ay - pb.y; dz = az - pb.z;
-                    k[2] = Scalar<KID, float>::f(dx * dx + dy * dy + dz * dz, p0, c0);   // (g,   t+4)
-                    dx = bx - pb.x; dy = by - pb.y; dz = bz - pb.z;
-                    k[3] = Scalar<KID, float>::f(dx * dx + dy * dy + dz * dz, p0, c0);   // (g+8, t+4)
+                    // differences of rows (g, g+8) to one source point, packed in pairs
+                    auto r2d = [&](const float4& p) {
+                        const float2 dx = __fadd2_rn(make_float2(ax, bx), make_float2(-p.x, -p.x));
+                        const float2 dy = __fadd2_rn(make_float2(ay, by), make_float2(-p.y, -p.y));
+                        const float2 dz = __fadd2_rn(make_float2(az, bz), make_float2(-p.z, -p.z));
+                        return __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+                    };
+                    const float2 ra2 = r2d(pa), rb2 = r2d(pb);
+                    k[0] = Scalar<KID, float>::f(ra2.x, p0, c0);   // (g,   t)
+                    k[1] = Scalar<KID, float>::f(ra2.y, p0, c0);   // (g+8, t)
+                    k[2] = Scalar<KID, float>::f(rb2.x, p0, c0);   // (g,   t+4)
+                    k[3] = Scalar<KID, float>::f(rb2.y, p0, c0);   // (g+8, t+4)
                 }
-                // hi rounded to TF32; the remainder is exact in FP32 and handed over
-                // as is: the MMA reads its TF32 bits (error < 2^-22 of the kernel value)
+                // hi rounded to TF32; the remainder k - hi (exact in FP32, one packed FMA per
+                // pair) is handed over as is: the MMA reads its TF32 bits (error < 2^-22 of
+                // the kernel value)
                 uint32_t hi[4], lo[4];
 #pragma unroll
-                for (int q = 0; q < 4; q++)
+                for (int q = 0; q < 4; q++) hi[q] = tf32_rna(k[q]);
+#pragma unroll
+                for (int q = 0; q < 4; q += 2)
                 {
-                    hi[q] = tf32_rna(k[q]);
-                    lo[q] = __float_as_uint(k[q] - __uint_as_float(hi[q]));
+                    const float2 l = __ffma2_rn(make_float2(__uint_as_float(hi[q]), __uint_as_float(hi[q + 1])),
+                                                make_float2(-1.f, -1.f), make_float2(k[q], k[q + 1]));
+                    lo[q] = __float_as_uint(l.x);
+                    lo[q + 1] = __float_as_uint(l.y);
                 }
                 uint4 b[NT];
 #pragma unroll
