@@ -404,18 +404,40 @@ __global__ void __launch_bounds__(256, 3) k_blk1(const BlkTask* __restrict__ tas
 #pragma unroll
                     for (int k = 0; k < 8; k++) a[j][k] = (cv[j] && k < nr) ? A[(long long) k * ncol + c[j]] : TA(0);
                 }
-#pragma unroll
-                for (int j = 0; j < CPL; j++)
+                if constexpr (sizeof(TA) == 4)
                 {
-                    double q = 0.0;
+                    // FP32 blocks: products and the sums over one pass (8 rows, or CPL
+                    // columns) in FP32, widened once per sum
+#pragma unroll
+                    for (int j = 0; j < CPL; j++)
+                    {
+                        float q = 0.f;
+#pragma unroll
+                        for (int k = 0; k < 8; k++) q = fmaf(a[j][k], (float) wr[k], q);
+                        if (do1) s_q[w][cs - cw + lane + 32 * j] = (double) q;
+                    }
 #pragma unroll
                     for (int k = 0; k < 8; k++)
                     {
-                        const double ad = to_d(a[j][k]);
-                        q = fma(ad, wr[k], q);
-                        p[k] = fma(ad, vc[j], p[k]);
+                        float pk = 0.f;
+#pragma unroll
+                        for (int j = 0; j < CPL; j++) pk = fmaf(a[j][k], (float) vc[j], pk);
+                        p[k] += (double) pk;
                     }
-                    if (do1) s_q[w][cs - cw + lane + 32 * j] = q;
+                } else {
+#pragma unroll
+                    for (int j = 0; j < CPL; j++)
+                    {
+                        double q = 0.0;
+#pragma unroll
+                        for (int k = 0; k < 8; k++)
+                        {
+                            const double ad = to_d(a[j][k]);
+                            q = fma(ad, wr[k], q);
+                            p[k] = fma(ad, vc[j], p[k]);
+                        }
+                        if (do1) s_q[w][cs - cw + lane + 32 * j] = q;
+                    }
                 }
             }
             if (do1)
@@ -1311,7 +1333,7 @@ constexpr int pair_smem_bytes()
 // owns the same element in every chunk); warp 4 + u owns rows 16u..16u+15 of the chunk
 // and sums C0 over the tiles (FP32 per tile, FP64 across tiles).
 template <int NV>
-__global__ void __launch_bounds__(256, 3) k_blk_tc(const BlkTask* __restrict__ tasks, const float* __restrict__ arena,
+__global__ void __launch_bounds__(256, 4) k_blk_tc(const BlkTask* __restrict__ tasks, const float* __restrict__ arena,
                                                    const double* __restrict__ XS, double* __restrict__ PS)
 {
     constexpr int CT = 32, S = CT + 4;            // tile width; padded shared row (conflict-free C0 reads)
