@@ -359,8 +359,8 @@ __device__ __forceinline__ void chunk_apply(const TA* __restrict__ A, int R, int
 
 // Stored block (task of up to 1024 rows), single right-hand side (the matvec path,
 // memory bound).  The task is walked in chunks of 64 rows; warp w owns rows
-// 8w..8w+7 of a chunk and its lanes sweep the columns 32*CPL at a time (CPL = 2 for
-// FP32 blocks, so both precisions keep the same bytes in flight per lane).  A v completes per lane across the sweep and is combined with one transposed
+// 8w..8w+7 of a chunk and its lanes sweep the columns 32*CPL at a time (CPL = 1: with
+// two columns per lane the FP32 copy measured 1.7x slower, latency-bound).  A v completes per lane across the sweep and is combined with one transposed
 // butterfly per chunk (no cross-warp sum: the warp owns its rows); the 8 warps'
 // partials of A^T w are summed in warp order through shared memory every 256 columns
 // and added into the task's single out1 slot (stored by the first chunk, added by
@@ -369,7 +369,7 @@ template <typename TA>
 __global__ void __launch_bounds__(256, 3) k_blk1(const BlkTask* __restrict__ tasks, const TA* __restrict__ arena,
                                               const double* __restrict__ XS, double* __restrict__ PS)
 {
-    constexpr int CPL = sizeof(TA) == 4 ? 2 : 1;
+    constexpr int CPL = 1;
     constexpr int CW = 256;                       // columns per shared reduction of A^T w
     __shared__ double s_q[kWarps][CW];
     const BlkTask T = tasks[blockIdx.x];
@@ -1321,58 +1321,38 @@ constexpr int pair_smem_bytes()
 
 // --------------------------------------- stored blocks on the tensor cores (FP32)
 
-// Asynchronous global -> shared copies (cp.async, 4 or 8 bytes; src-size 0 fills zeros).
-__device__ __forceinline__ void cp_async4(void* smem, const void* gmem, bool pred)
-{
-    const unsigned sa = (unsigned) __cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(sa), "l"(gmem), "r"(pred ? 4 : 0) : "memory");
-}
-__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool pred)
-{
-    const unsigned sa = (unsigned) __cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(sa), "l"(gmem), "r"(pred ? 8 : 0) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
-
-template <int NV>
-struct BlkTcSmem {
-    float a[3][64][36];          // A tiles (64 rows x 32 columns, padded), three stages
-    double w[3][64][NV];         // raw W rows of a chunk (three chunk buffers)
-    uint4 wf[8][32][2];          // W^T fragments of the current chunk: hi, lo
-    uint4 v[3][4][32][2];        // V^T fragments per tile stage: hi, lo
-};
-
-// Stored block task (up to 1024 rows x ncol, FP32 copy) for panels of 8 / 16
-// right-hand sides, both products on the tensor cores with the right-hand sides as
-// the M = 16 side of m16n8k8 (3xTF32, FP32 accumulation):
+// Stored block task (up to 1024 rows x ncol, FP32 copy, walked in chunks of R <= 64
+// rows) for panels of 8 / 16 right-hand sides, both products on the tensor cores with
+// the right-hand sides as the M = 16 side of m16n8k8 (3xTF32, FP32 accumulation):
 //   C1^T (NV x ncol) = W^T (NV x R) A        [B operand = A, k = rows]      warps 0-3
 //   C0^T (NV x R)    = V^T (NV x ncol) A^T   [B operand = A^T, k = columns] warps 4-7
-// The task is one sequence of 64 x 32 tiles (a 64-row chunk, then its column tiles).
-// A tiles and the chunks' W rows move with cp.async in a three-stage ring, so two
-// tiles are in flight while one is multiplied; the V^T fragments of the next tile are
-// read into registers during the current one.  Warp w < 4 owns columns 8w..8w+7 of a
-// tile and completes the tile's C1 part over the chunk's rows (stored by the first
-// chunk into the task's single C1 slot, added by the later ones; FP64, the same thread
+// Column tiles of 32 are staged in shared memory (double-buffered through registers);
+// each tile feeds both products.  Warp w < 4 owns columns 8w..8w+7 of every tile and
+// completes the chunk's part of C1 for them over its R rows, stored by the first chunk
+// into the task's single C1 slot and added by the later ones (FP64; the same thread
 // owns the same element in every chunk); warp 4 + u owns rows 16u..16u+15 of the chunk
-// and sums C0 over the chunk's tiles (FP32 per tile, FP64 across tiles).
+// and sums C0 over the tiles (FP32 per tile, FP64 across tiles).
 template <int NV>
-__global__ void __launch_bounds__(256, 3) k_blk_tc(const BlkTask* __restrict__ tasks, const float* __restrict__ arena,
+__global__ void __launch_bounds__(256, 4) k_blk_tc(const BlkTask* __restrict__ tasks, const float* __restrict__ arena,
                                                    const double* __restrict__ XS, double* __restrict__ PS)
 {
-    constexpr int CT = 32;
-    extern __shared__ __align__(16) unsigned char blk_smem[];
-    BlkTcSmem<NV>& sm = *reinterpret_cast<BlkTcSmem<NV>*>(blk_smem);
+    constexpr int CT = 32, S = CT + 4;            // tile width; padded shared row (conflict-free C0 reads)
+    __shared__ float s_a[2][64][S];
+    __shared__ uint4 s_w[8][32][2];               // W^T fragments per k-step of 8 rows: hi, lo
+    __shared__ uint4 s_v[2][4][32][2];            // V^T fragments per k-step of 8 columns: hi, lo
     const BlkTask T = tasks[blockIdx.x];
-    const int ncol = T.ncol, nrow = T.nrow;
+    const int ncol = T.ncol;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, tq = lane & 3;
     const bool do0 = T.out0_row >= 0, do1 = T.out1_row >= 0;
-    const int ntc = (ncol + CT - 1) / CT;
-    const int nt = ntc * ((nrow + 63) / 64);
-    const float* A0 = arena + T.a_off;
 
-    auto split4 = [&](const float (&v)[4], uint4& hi, uint4& lo) {
+    // A-fragment of an (NV x 8) slice of X^T: X rows k0 + {tq, tq+4}, right-hand sides {g, g+8}
+    auto frag = [&](int row0, int nrows, int k0, uint4& hi, uint4& lo) {
+        float v[4];
+        const int ra = k0 + tq, rb = ra + 4;
+        v[0] = (ra < nrows && g < NV) ? (float) XS[(long long) (row0 + ra) * NV + g] : 0.f;
+        v[1] = (ra < nrows && g + 8 < NV) ? (float) XS[(long long) (row0 + ra) * NV + g + 8] : 0.f;
+        v[2] = (rb < nrows && g < NV) ? (float) XS[(long long) (row0 + rb) * NV + g] : 0.f;
+        v[3] = (rb < nrows && g + 8 < NV) ? (float) XS[(long long) (row0 + rb) * NV + g + 8] : 0.f;
         uint32_t h[4], l[4];
 #pragma unroll
         for (int q = 0; q < 4; q++)
@@ -1383,160 +1363,138 @@ __global__ void __launch_bounds__(256, 3) k_blk_tc(const BlkTask* __restrict__ t
         hi = make_uint4(h[0], h[1], h[2], h[3]);
         lo = make_uint4(l[0], l[1], l[2], l[3]);
     };
-    // V^T fragment (right-hand sides {g, g+8} x columns c0 + k0 + {tq, tq+4}) from XS
-    auto vfrag = [&](int c0, int k0, uint4& hi, uint4& lo) {
-        float v[4];
-        const int ca = c0 + k0 + tq, cb = ca + 4;
-        const long long ra = (long long) (T.in0_row + ca) * NV, rb = (long long) (T.in0_row + cb) * NV;
-        v[0] = (ca < ncol && g < NV) ? (float) XS[ra + g] : 0.f;
-        v[1] = (ca < ncol && g + 8 < NV) ? (float) XS[ra + g + 8] : 0.f;
-        v[2] = (cb < ncol && g < NV) ? (float) XS[rb + g] : 0.f;
-        v[3] = (cb < ncol && g + 8 < NV) ? (float) XS[rb + g + 8] : 0.f;
-        split4(v, hi, lo);
-    };
-    auto issue = [&](int t) {
-        const int st = t % 3, chunk = t / ntc, rc = chunk * 64, c0 = (t % ntc) * CT, R = min(64, nrow - rc);
-        const float* A = A0 + (long long) rc * ncol + c0;
-#pragma unroll
-        for (int u = 0; u < 8; u++)
-        {
-            const int e = threadIdx.x + 256 * u, r = e >> 5, c = e & 31;
-            const bool ok = r < R && c0 + c < ncol;
-            cp_async4(&sm.a[st][r][c], ok ? (const void*) (A + (long long) r * ncol + c) : (const void*) A0, ok);
-        }
-        if (do1 && c0 == 0)
-            for (int e = threadIdx.x; e < 64 * NV; e += 256)
-            {
-                const int r = e / NV, v = e % NV;
-                const bool ok = r < R;
-                cp_async8(&sm.w[chunk % 3][r][v], ok ? (const void*) (XS + (long long) (T.in1_row + rc + r) * NV + v)
-                                                     : (const void*) XS, ok);
-            }
-    };
 
-    double c0acc[2][4];
-#pragma unroll
-    for (int n = 0; n < 2; n++)
-#pragma unroll
-        for (int q = 0; q < 4; q++) c0acc[n][q] = 0.0;
-
-    // prologue: tiles 0 and 1 in flight, V^T fragments of tile 0 in shared memory
-    if (nt > 0) issue(0);
-    cp_async_commit();
-    if (nt > 1) issue(1);
-    cp_async_commit();
-    if (nt > 0 && do0 && warp < 4)
-        vfrag(0, 8 * warp, sm.v[0][warp][lane][0], sm.v[0][warp][lane][1]);
-    uint4 rvh = make_uint4(0, 0, 0, 0), rvl = rvh;
-    for (int t = 0; t < nt; t++)
+    // the task's rows in chunks of 64; the chunks' C1 parts add into one slot
+    for (int rc = 0; rc < T.nrow; rc += 64)
     {
-        const int st = t % 3, chunk = t / ntc, rc = chunk * 64, c0 = (t % ntc) * CT, R = min(64, nrow - rc);
-        cp_async_wait<1>();          // tile t (and its chunk's W rows) have landed
-        __syncthreads();             // ... for every thread; stage (t + 2) % 3 is free again
-        if (t + 2 < nt) issue(t + 2);
-        cp_async_commit();
-        const bool nextv = t + 1 < nt && do0 && warp < 4;
-        if (nextv) vfrag(((t + 1) % ntc) * CT, 8 * warp, rvh, rvl);
-        if (c0 == 0 && do1)
-        {
-            // W^T fragments of the chunk, one k-step of 8 rows per warp
-            float v[4];
-            const int ra = 8 * warp + tq, rb = ra + 4;
-            v[0] = (g < NV) ? (float) sm.w[chunk % 3][ra][g < NV ? g : 0] : 0.f;
-            v[1] = (g + 8 < NV) ? (float) sm.w[chunk % 3][ra][g + 8 < NV ? g + 8 : 0] : 0.f;
-            v[2] = (g < NV) ? (float) sm.w[chunk % 3][rb][g < NV ? g : 0] : 0.f;
-            v[3] = (g + 8 < NV) ? (float) sm.w[chunk % 3][rb][g + 8 < NV ? g + 8 : 0] : 0.f;
-            split4(v, sm.wf[warp][lane][0], sm.wf[warp][lane][1]);
-            __syncthreads();
-        }
-        if (warp < 4)
-        {
-            if (do1)
+        const float* A = arena + T.a_off + (long long) rc * ncol;
+        const int R = min(64, T.nrow - rc);
+        __syncthreads();                          // previous chunk done with s_w / s_a / s_v
+        // W^T fragments for the chunk (8 k-steps of 8 rows), one warp per k-step
+        if (do1)
+            frag(T.in1_row + rc, R, 8 * warp, s_w[warp][lane][0], s_w[warp][lane][1]);
+
+        // tile staging: 64 x 32 floats, 8 per thread; V^T fragments of the tile's columns
+        float ra[8];
+        uint4 rvh = make_uint4(0, 0, 0, 0), rvl = rvh;
+        auto load_tile = [&](int c0) {
+#pragma unroll
+            for (int u = 0; u < 8; u++)
             {
-                // C1^T for columns c0 + 8w .. +7: k over the chunk's rows (8 k-steps)
-                float d[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};   // two chains, summed
-                const int ksteps = (R + 7) >> 3;
-#pragma unroll
-                for (int ks = 0; ks < 8; ks++)
-                {
-                    if (ks >= ksteps) break;
-                    const float b0 = sm.a[st][8 * ks + tq][8 * warp + g];
-                    const float b1 = sm.a[st][8 * ks + tq + 4][8 * warp + g];
-                    const uint32_t h0 = tf32_rna(b0), h1 = tf32_rna(b1);
-                    const uint32_t l0 = __float_as_uint(b0 - __uint_as_float(h0)),
-                                   l1 = __float_as_uint(b1 - __uint_as_float(h1));
-                    const uint4 wh = sm.wf[ks][lane][0], wl = sm.wf[ks][lane][1];
-                    float (&dd)[4] = d[ks & 1];
-                    mma_tf32(dd, wl.x, wl.y, wl.z, wl.w, h0, h1);
-                    mma_tf32(dd, wh.x, wh.y, wh.z, wh.w, l0, l1);
-                    mma_tf32(dd, wh.x, wh.y, wh.z, wh.w, h0, h1);
-                }
-                // rows of the fragment = right-hand sides (g, g+8), columns = (2tq, 2tq+1)
-                const int cb = c0 + 8 * warp + 2 * tq;
-#pragma unroll
-                for (int q = 0; q < 4; q++)
-                {
-                    const int rhs = (q < 2) ? g : g + 8, col = cb + (q & 1);
-                    if (rhs < NV && col < ncol)
-                    {
-                        double* o = PS + (long long) (T.out1_row + col) * NV + rhs;
-                        const double v = (double) (d[0][q] + d[1][q]);
-                        *o = (rc == 0) ? v : *o + v;
-                    }
-                }
+                const int e = threadIdx.x + 256 * u, r = e >> 5, c = e & 31;
+                ra[u] = (r < R && c0 + c < ncol) ? A[(long long) r * ncol + c0 + c] : 0.f;
             }
-        } else if (do0) {
-            // C0^T for rows 16u .. 16u+15 (two n-tiles of 8): k over the tile's 32 columns
-            const int u = warp - 4;
-            if (16 * u < R)
+            if (do0 && warp < 4) frag(T.in0_row + c0, ncol - c0, 8 * warp, rvh, rvl);
+        };
+        auto store_tile = [&](int buf) {
+#pragma unroll
+            for (int u = 0; u < 8; u++)
             {
-                float d[2][2][4];
+                const int e = threadIdx.x + 256 * u;
+                s_a[buf][e >> 5][e & 31] = ra[u];
+            }
+            if (do0 && warp < 4) { s_v[buf][warp][lane][0] = rvh; s_v[buf][warp][lane][1] = rvl; }
+        };
+
+        double c0acc[2][4];
 #pragma unroll
-                for (int n = 0; n < 2; n++)
+        for (int n = 0; n < 2; n++)
 #pragma unroll
-                    for (int p = 0; p < 2; p++)
-#pragma unroll
-                        for (int q = 0; q < 4; q++) d[n][p][q] = 0.f;
-#pragma unroll
-                for (int ks = 0; ks < 4; ks++)
+            for (int q = 0; q < 4; q++) c0acc[n][q] = 0.0;
+
+        if (ncol > 0)
+        {
+            load_tile(0);
+            store_tile(0);
+        }
+        __syncthreads();
+        int buf = 0;
+        for (int c0 = 0; c0 < ncol; c0 += CT)
+        {
+            const bool more = c0 + CT < ncol;
+            if (more) load_tile(c0 + CT);
+            if (warp < 4)
+            {
+                if (do1)
                 {
-                    const uint4 vh = sm.v[st][ks][lane][0], vl = sm.v[st][ks][lane][1];
+                    // C1^T for columns c0 + 8w .. +7: k over the R rows (8 k-steps)
+                    float d[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};   // two chains, summed
+                    const int ksteps = (R + 7) >> 3;
 #pragma unroll
-                    for (int n = 0; n < 2; n++)
+                    for (int ks = 0; ks < 8; ks++)
                     {
-                        const int row = 16 * u + 8 * n + g;
-                        const float b0 = sm.a[st][row][8 * ks + tq], b1 = sm.a[st][row][8 * ks + tq + 4];
+                        if (ks >= ksteps) break;
+                        const float b0 = s_a[buf][8 * ks + tq][8 * warp + g];
+                        const float b1 = s_a[buf][8 * ks + tq + 4][8 * warp + g];
                         const uint32_t h0 = tf32_rna(b0), h1 = tf32_rna(b1);
                         const uint32_t l0 = __float_as_uint(b0 - __uint_as_float(h0)),
                                        l1 = __float_as_uint(b1 - __uint_as_float(h1));
-                        float (&dd)[4] = d[n][ks & 1];
-                        mma_tf32(dd, vl.x, vl.y, vl.z, vl.w, h0, h1);
-                        mma_tf32(dd, vh.x, vh.y, vh.z, vh.w, l0, l1);
-                        mma_tf32(dd, vh.x, vh.y, vh.z, vh.w, h0, h1);
+                        const uint4 wh = s_w[ks][lane][0], wl = s_w[ks][lane][1];
+                        float (&dd)[4] = d[ks & 1];
+                        mma_tf32(dd, wl.x, wl.y, wl.z, wl.w, h0, h1);
+                        mma_tf32(dd, wh.x, wh.y, wh.z, wh.w, l0, l1);
+                        mma_tf32(dd, wh.x, wh.y, wh.z, wh.w, h0, h1);
                     }
-                }
-#pragma unroll
-                for (int n = 0; n < 2; n++)
-#pragma unroll
-                    for (int q = 0; q < 4; q++) c0acc[n][q] += (double) (d[n][0][q] + d[n][1][q]);
-            }
-            if (c0 + CT >= ncol)
-            {
-                // last tile of the chunk: its rows of C0 are complete
-#pragma unroll
-                for (int n = 0; n < 2; n++)
+                    // rows of the fragment = right-hand sides (g, g+8), columns = (2tq, 2tq+1)
+                    const int cb = c0 + 8 * warp + 2 * tq;
 #pragma unroll
                     for (int q = 0; q < 4; q++)
                     {
-                        const int rhs = (q < 2) ? g : g + 8, row = 16 * u + 8 * n + 2 * tq + (q & 1);
-                        if (rhs < NV && row < R) PS[(long long) (T.out0_row + rc + row) * NV + rhs] = c0acc[n][q];
-                        c0acc[n][q] = 0.0;
+                        const int rhs = (q < 2) ? g : g + 8, col = cb + (q & 1);
+                        if (rhs < NV && col < ncol)
+                        {
+                            double* o = PS + (long long) (T.out1_row + col) * NV + rhs;
+                            const double v = (double) (d[0][q] + d[1][q]);
+                            *o = (rc == 0) ? v : *o + v;
+                        }
                     }
+                }
+            } else if (do0) {
+                // C0^T for rows 16u .. 16u+15 (two n-tiles of 8): k over the tile's 32 columns
+                const int u = warp - 4;
+                if (16 * u < R)
+                {
+                    float d[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+#pragma unroll
+                    for (int ks = 0; ks < 4; ks++)
+                    {
+                        const uint4 vh = s_v[buf][ks][lane][0], vl = s_v[buf][ks][lane][1];
+#pragma unroll
+                        for (int n = 0; n < 2; n++)
+                        {
+                            const int row = 16 * u + 8 * n + g;
+                            const float b0 = s_a[buf][row][8 * ks + tq], b1 = s_a[buf][row][8 * ks + tq + 4];
+                            const uint32_t h0 = tf32_rna(b0), h1 = tf32_rna(b1);
+                            const uint32_t l0 = __float_as_uint(b0 - __uint_as_float(h0)),
+                                           l1 = __float_as_uint(b1 - __uint_as_float(h1));
+                            mma_tf32(d[n], vl.x, vl.y, vl.z, vl.w, h0, h1);
+                            mma_tf32(d[n], vh.x, vh.y, vh.z, vh.w, l0, l1);
+                            mma_tf32(d[n], vh.x, vh.y, vh.z, vh.w, h0, h1);
+                        }
+                    }
+#pragma unroll
+                    for (int n = 0; n < 2; n++)
+#pragma unroll
+                        for (int q = 0; q < 4; q++) c0acc[n][q] += (double) d[n][q];
+                }
             }
+            if (more) store_tile(buf ^ 1);
+            __syncthreads();
+            buf ^= 1;
         }
-        if (nextv) { sm.v[(t + 1) % 3][warp][lane][0] = rvh; sm.v[(t + 1) % 3][warp][lane][1] = rvl; }
+        if (do0 && warp >= 4)
+        {
+            const int u = warp - 4;
+#pragma unroll
+            for (int n = 0; n < 2; n++)
+#pragma unroll
+                for (int q = 0; q < 4; q++)
+                {
+                    const int rhs = (q < 2) ? g : g + 8, row = 16 * u + 8 * n + 2 * tq + (q & 1);
+                    if (rhs < NV && row < R) PS[(long long) (T.out0_row + rc + row) * NV + rhs] = c0acc[n][q];
+                }
+        }
     }
-    cp_async_wait<0>();
 }
 
 // --------------------------------------------------------------- direct sum
@@ -1645,18 +1603,8 @@ cudaError_t launch_blk(int NV, const BlkTask* t, int n, const TA* arena, const d
     {
         if (use_tc && n > 0 && (NV == 8 || NV == 16))
         {
-            if (NV == 16)
-            {
-                constexpr int b = (int) sizeof(BlkTcSmem<16>);
-                cudaError_t e = allow_smem(k_blk_tc<16>, b);
-                if (e != cudaSuccess) return e;
-                k_blk_tc<16><<<n, 256, b, st>>>(t, arena, XS, PS);
-            } else {
-                constexpr int b = (int) sizeof(BlkTcSmem<8>);
-                cudaError_t e = allow_smem(k_blk_tc<8>, b);
-                if (e != cudaSuccess) return e;
-                k_blk_tc<8><<<n, 256, b, st>>>(t, arena, XS, PS);
-            }
+            if (NV == 16) k_blk_tc<16><<<n, 256, 0, st>>>(t, arena, XS, PS);
+            else k_blk_tc<8><<<n, 256, 0, st>>>(t, arena, XS, PS);
             return cudaGetLastError();
         }
     }
