@@ -5,8 +5,8 @@
 // (examples/PCG/pcg.c:11-152) on the shifted operator of
 // examples/SPDHSS-H2/pcg_tests.c:13-20, run for up to 16 right-hand sides ("slots")
 // at once: the slots are the columns of one 16-wide panel, so every iteration is one
-// H2 matmul of the panel plus five small kernels (direction update, p'Ap, alpha,
-// x/r update with ||r||^2, status).  The host only enqueues iterations and reads the
+// H2 matmul (of the panel's columns up to the highest busy slot) plus five small
+// kernels (direction update, p'Ap, alpha, x/r update with ||r||^2, status).  The host only enqueues iterations and reads the
 // 16 slot records once per batch of iterations; it never waits per iteration.
 //
 // Precision: vectors, inner products and the residual recomputation are FP64; the
@@ -399,6 +399,17 @@ H2G_API int h2gpu_cg_admit(h2gpu_cg* g, int slot, int kind, const double* d_b, d
     return H2GPU_OK;
 }
 
+// Columns the operator must be applied to: up to the highest slot in `state` (by the
+// host's latest view: the last sync plus admissions since, an upper bound of the
+// device's), so a panel with few busy slots applies a narrower panel.
+static int busy_width(const h2gpu_cg* g, int state)
+{
+    int hi = 0;
+    for (int k = 0; k < kS; k++)
+        if (g->h_sl[k].state == state) hi = k + 1;
+    return hi;
+}
+
 H2G_API int h2gpu_cg_step(h2gpu_cg* g, int n_iter)
 {
     if (!g || n_iter < 1) return h2gpu::set_error(H2GPU_ERR_INVALID, "bad engine or n_iter");
@@ -406,10 +417,12 @@ H2G_API int h2gpu_cg_step(h2gpu_cg* g, int n_iter)
     CGCK(cudaSetDevice(g->device));
     const int G = g->c.G;
     const int ge = std::max(1, std::min(kRedBlocks, (g->N * kS + 255) / 256));
+    const int width = busy_width(g, H2GPU_CG_RUN);
+    if (width == 0) return H2GPU_OK;
     for (int t = 0; t < n_iter; t++)
     {
         k_cg_dir<<<ge, 256, 0, g->stream>>>(g->c);
-        int st = h2gpu::image_apply_quiet(g->img, g->precision, kS, g->c.P, kS, g->c.AP, kS);
+        int st = h2gpu::image_apply_quiet(g->img, g->precision, width, g->c.P, kS, g->c.AP, kS);
         if (st != H2GPU_OK) return st;
         k_cg_dot<<<G, 256, 0, g->stream>>>(g->c);
         k_cg_alpha<<<1, 256, 0, g->stream>>>(g->c);
@@ -425,11 +438,17 @@ H2G_API int h2gpu_cg_check(h2gpu_cg* g)
     if (!g) return h2gpu::set_error(H2GPU_ERR_INVALID, "engine is NULL");
     std::lock_guard<std::mutex> lk(g->lock);
     CGCK(cudaSetDevice(g->device));
-    int st = h2gpu::image_apply_quiet(g->img, H2GPU_PREC_FP64, kS, g->c.X, kS, g->c.AP, kS);
+    const int width = busy_width(g, H2GPU_CG_CHECK);
+    if (width == 0) return H2GPU_OK;
+    int st = h2gpu::image_apply_quiet(g->img, H2GPU_PREC_FP64, width, g->c.X, kS, g->c.AP, kS);
     if (st != H2GPU_OK) return st;
     k_cg_resid<<<g->c.G, 256, 0, g->stream>>>(g->c);
     k_cg_check_finish<<<1, 256, 0, g->stream>>>(g->c);
     CGCK(cudaGetLastError());
+    // a checked slot either finished or restarts: until the next sync the host view
+    // counts it as running, so the next step's panel covers it
+    for (int k = 0; k < kS; k++)
+        if (g->h_sl[k].state == H2GPU_CG_CHECK) g->h_sl[k].state = H2GPU_CG_RUN;
     return H2GPU_OK;
 }
 
