@@ -980,6 +980,9 @@ KParam kparam_of(const h2gpu_image* im)
     return k;
 }
 
+// FP32 sweeps on the tensor cores when the image's kernel variant is a tensor-core one.
+int sweep_tc(const h2gpu_image* im) { return im->BD_JIT ? im->jit_tc : im->blk_tc; }
+
 // One panel of NV right-hand sides: X (original order, strides x_rs, x_cs) -> Y.
 int run_panel(h2gpu_image* im, int NV, int nv, const double* X, long long x_rs, long long x_cs, double* Y,
               long long y_rs, long long y_cs, cudaStream_t s, bool timed)
@@ -1000,7 +1003,7 @@ int run_panel(h2gpu_image* im, int NV, int nv, const double* X, long long x_rs, 
         for (size_t L = 0; L + 1 < im->up_beg.size(); L++)
         {
             int b = im->up_beg[L], n = im->up_beg[L + 1] - b;
-            CK(launch_up<float>(NV, im->d_up + b, n, im->d_U32, im->d_XS, s));
+            CK(launch_up<float>(NV, im->d_up + b, n, im->d_U32, im->d_XS, s, sweep_tc(im)));
         }
         if (timed) CK(cudaEventRecord(e[3], s));
         CK(launch_pair(im->kernel_id, NV, im->d_owF, im->n_owF, im->d_pp, im->d_pts32, kp, im->d_XS, im->d_PS, s));
@@ -1011,7 +1014,7 @@ int run_panel(h2gpu_image* im, int NV, int nv, const double* X, long long x_rs, 
         for (size_t L = 0; L + 1 < im->dn_beg.size(); L++)
         {
             int b = im->dn_beg[L], n = im->dn_beg[L + 1] - b;
-            CK(launch_down<float>(NV, im->d_dn + b, n, im->d_U32, im->d_Y1, im->d_PS, im->d_PUSH, s));
+            CK(launch_down<float>(NV, im->d_dn + b, n, im->d_U32, im->d_Y1, im->d_PS, im->d_PUSH, s, sweep_tc(im)));
         }
         if (timed) CK(cudaEventRecord(e[5], s));
         CK(launch_asm(NV, im->d_asm2, im->n_leaf, im->d_asm_slots2, im->d_PS, im->d_fwd, Y, y_rs, y_cs, nv, s));
@@ -1035,7 +1038,7 @@ int run_panel(h2gpu_image* im, int NV, int nv, const double* X, long long x_rs, 
     for (size_t L = 0; L + 1 < im->up_beg.size(); L++)
     {
         int b = im->up_beg[L], n = im->up_beg[L + 1] - b;
-        if (f32) CK(launch_up<float>(NV, im->d_up + b, n, im->d_U32, im->d_XS, s));
+        if (f32) CK(launch_up<float>(NV, im->d_up + b, n, im->d_U32, im->d_XS, s, sweep_tc(im)));
         else CK(launch_up<double>(NV, im->d_up + b, n, im->d_U64, im->d_XS, s));
     }
     if (timed) CK(cudaEventRecord(e[3], s));
@@ -1052,7 +1055,7 @@ int run_panel(h2gpu_image* im, int NV, int nv, const double* X, long long x_rs, 
     for (size_t L = 0; L + 1 < im->dn_beg.size(); L++)
     {
         int b = im->dn_beg[L], n = im->dn_beg[L + 1] - b;
-        if (f32) CK(launch_down<float>(NV, im->d_dn + b, n, im->d_U32, im->d_Y1, im->d_PS, im->d_PUSH, s));
+        if (f32) CK(launch_down<float>(NV, im->d_dn + b, n, im->d_U32, im->d_Y1, im->d_PS, im->d_PUSH, s, sweep_tc(im)));
         else CK(launch_down<double>(NV, im->d_dn + b, n, im->d_U64, im->d_Y1, im->d_PS, im->d_PUSH, s));
     }
     if (timed) CK(cudaEventRecord(e[5], s));

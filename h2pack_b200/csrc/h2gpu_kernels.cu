@@ -1497,6 +1497,147 @@ __global__ void __launch_bounds__(256, 4) k_blk_tc(const BlkTask* __restrict__ t
     }
 }
 
+// ---------------------------------------------- sweeps on the tensor cores (FP32 U)
+
+// Upward / downward sweep products for FP32 U and panels of 8 / 16 right-hand sides on
+// the tensor cores (3xTF32, FP32 accumulation per 32-deep k tile, FP64 across tiles),
+// right-hand sides as the M = 16 side of m16n8k8:
+//   upward   (UP):  C^T (NV x nc) = X^T (NV x nrow) U[:, c0 : c0 + nc]    B = U,   k = rows of U
+//   downward (!UP): C^T (NV x 64) = Y^T (NV x ncol) U[r0 : r0 + 64, :]^T  B = U^T, k = columns of U
+// (Y = the node's summed y1 plus the parent's push-down slice).  Warp w owns output
+// columns (UP) / rows (DOWN) 8w..8w+7.  The 32-deep k tiles of U and the X^T / Y^T
+// fragments are double-buffered through registers.
+template <int NV, bool UP>
+__global__ void __launch_bounds__(256, 4) k_sweep_tc(const UpTask* __restrict__ ups, const DownTask* __restrict__ dns,
+                                                     const float* __restrict__ Uar, double* __restrict__ XS,
+                                                     const double* __restrict__ Y1, double* __restrict__ PS,
+                                                     double* __restrict__ PUSH)
+{
+    constexpr int KT = 32;
+    constexpr int ROWS = UP ? KT : 64, LD = UP ? 72 : 36;   // padded: conflict-free fragment reads
+    __shared__ float s_u[2][ROWS][LD];
+    __shared__ uint4 s_x[2][4][32][2];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, tq = lane & 3;
+    int K, M, lda, xrow = 0, y1_row = -1, push_row = -1;
+    const float* A;
+    double* out;
+    if constexpr (UP)
+    {
+        const UpTask T = ups[blockIdx.x];
+        K = T.nrow; M = T.nc; lda = T.ld;
+        A = Uar + T.u_off + T.c0;
+        xrow = T.in_row;
+        out = XS + (long long) (T.out_row + T.c0) * NV;
+    } else {
+        const DownTask T = dns[blockIdx.x];
+        K = T.ncol; M = T.nrow; lda = T.ncol;
+        A = Uar + T.u_off;
+        y1_row = T.y1_row; push_row = T.push_row;
+        out = (T.dst_ps ? PS : PUSH) + (long long) T.dst_row * NV;
+    }
+    auto xin = [&](int k, int v) -> double {
+        if constexpr (UP) return XS[(long long) (xrow + k) * NV + v];
+        double b = (y1_row >= 0) ? Y1[(long long) (y1_row + k) * NV + v] : 0.0;
+        if (push_row >= 0) b += PUSH[(long long) (push_row + k) * NV + v];
+        return b;
+    };
+    float ra[8];
+    uint4 rxh = make_uint4(0, 0, 0, 0), rxl = rxh;
+    auto load_tile = [&](int k0) {
+#pragma unroll
+        for (int u = 0; u < 8; u++)
+        {
+            const int e = threadIdx.x + 256 * u;
+            if constexpr (UP)
+            {
+                const int k = e >> 6, m = e & 63;
+                ra[u] = (k0 + k < K && m < M) ? A[(long long) (k0 + k) * lda + m] : 0.f;
+            } else {
+                const int m = e >> 5, k = e & 31;
+                ra[u] = (m < M && k0 + k < K) ? A[(long long) m * lda + k0 + k] : 0.f;
+            }
+        }
+        if (warp < 4)
+        {
+            const int ka = k0 + 8 * warp + tq, kb = ka + 4;
+            float v[4];
+            v[0] = (ka < K && g < NV) ? (float) xin(ka, g) : 0.f;
+            v[1] = (ka < K && g + 8 < NV) ? (float) xin(ka, g + 8) : 0.f;
+            v[2] = (kb < K && g < NV) ? (float) xin(kb, g) : 0.f;
+            v[3] = (kb < K && g + 8 < NV) ? (float) xin(kb, g + 8) : 0.f;
+            uint32_t h[4], l[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+            {
+                h[q] = tf32_rna(v[q]);
+                l[q] = __float_as_uint(v[q] - __uint_as_float(h[q]));
+            }
+            rxh = make_uint4(h[0], h[1], h[2], h[3]);
+            rxl = make_uint4(l[0], l[1], l[2], l[3]);
+        }
+    };
+    auto store_tile = [&](int buf) {
+#pragma unroll
+        for (int u = 0; u < 8; u++)
+        {
+            const int e = threadIdx.x + 256 * u;
+            if constexpr (UP) s_u[buf][e >> 6][e & 63] = ra[u];
+            else s_u[buf][e >> 5][e & 31] = ra[u];
+        }
+        if (warp < 4) { s_x[buf][warp][lane][0] = rxh; s_x[buf][warp][lane][1] = rxl; }
+    };
+
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    if (K > 0)
+    {
+        load_tile(0);
+        store_tile(0);
+    }
+    __syncthreads();
+    int buf = 0;
+    for (int k0 = 0; k0 < K; k0 += KT)
+    {
+        const bool more = k0 + KT < K;
+        if (more) load_tile(k0 + KT);
+        if (8 * warp < M)
+        {
+            float d[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+#pragma unroll
+            for (int ks = 0; ks < 4; ks++)
+            {
+                const uint4 xh = s_x[buf][ks][lane][0], xl = s_x[buf][ks][lane][1];
+                float b0, b1;
+                if constexpr (UP)
+                {
+                    b0 = s_u[buf][8 * ks + tq][8 * warp + g];
+                    b1 = s_u[buf][8 * ks + tq + 4][8 * warp + g];
+                } else {
+                    b0 = s_u[buf][8 * warp + g][8 * ks + tq];
+                    b1 = s_u[buf][8 * warp + g][8 * ks + tq + 4];
+                }
+                const uint32_t h0 = tf32_rna(b0), h1 = tf32_rna(b1);
+                const uint32_t l0 = __float_as_uint(b0 - __uint_as_float(h0)), l1 = __float_as_uint(b1 - __uint_as_float(h1));
+                float (&dd)[4] = d[ks & 1];
+                mma_tf32(dd, xl.x, xl.y, xl.z, xl.w, h0, h1);
+                mma_tf32(dd, xh.x, xh.y, xh.z, xh.w, l0, l1);
+                mma_tf32(dd, xh.x, xh.y, xh.z, xh.w, h0, h1);
+            }
+#pragma unroll
+            for (int q = 0; q < 4; q++) acc[q] += (double) (d[0][q] + d[1][q]);
+        }
+        if (more) store_tile(buf ^ 1);
+        __syncthreads();
+        buf ^= 1;
+    }
+    // rows of the fragment = right-hand sides (g, g+8), columns = outputs (2tq, 2tq+1)
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+    {
+        const int rhs = (q < 2) ? g : g + 8, m = 8 * warp + 2 * tq + (q & 1);
+        if (rhs < NV && m < M) out[(long long) m * NV + rhs] = acc[q];
+    }
+}
+
 // --------------------------------------------------------------- direct sum
 
 template <int KID, int KD>
@@ -1576,9 +1717,18 @@ cudaError_t launch_permute(const double* X, long long x_rs, long long x_cs, cons
 }
 
 template <typename TA>
-cudaError_t launch_up(int NV, const UpTask* t, int n, const TA* U, double* XS, cudaStream_t st)
+cudaError_t launch_up(int NV, const UpTask* t, int n, const TA* U, double* XS, cudaStream_t st, int use_tc)
 {
     if (n <= 0) return cudaSuccess;
+    if constexpr (sizeof(TA) == 4)
+    {
+        if (use_tc && (NV == 8 || NV == 16))
+        {
+            if (NV == 16) k_sweep_tc<16, true><<<n, 256, 0, st>>>(t, nullptr, U, XS, nullptr, nullptr, nullptr);
+            else k_sweep_tc<8, true><<<n, 256, 0, st>>>(t, nullptr, U, XS, nullptr, nullptr, nullptr);
+            return cudaGetLastError();
+        }
+    }
     NV_DISPATCH(NV, {
         if constexpr (NVc >= 4)
             k_sweep_gemm<TA, NVc, true><<<n, 256, 0, st>>>(t, nullptr, U, XS, nullptr, nullptr, nullptr);
@@ -1627,9 +1777,18 @@ cudaError_t launch_blk(int NV, const BlkTask* t, int n, const TA* arena, const d
 
 template <typename TA>
 cudaError_t launch_down(int NV, const DownTask* t, int n, const TA* U, const double* Y1, double* PS, double* PUSH,
-                        cudaStream_t st)
+                        cudaStream_t st, int use_tc)
 {
     if (n <= 0) return cudaSuccess;
+    if constexpr (sizeof(TA) == 4)
+    {
+        if (use_tc && (NV == 8 || NV == 16))
+        {
+            if (NV == 16) k_sweep_tc<16, false><<<n, 256, 0, st>>>(nullptr, t, U, nullptr, Y1, PS, PUSH);
+            else k_sweep_tc<8, false><<<n, 256, 0, st>>>(nullptr, t, U, nullptr, Y1, PS, PUSH);
+            return cudaGetLastError();
+        }
+    }
     NV_DISPATCH(NV, {
         if constexpr (NVc >= 4)
         {
@@ -1761,11 +1920,11 @@ cudaError_t launch_direct(int kid, const double4* trg, int n_trg, const double4*
     return cudaGetLastError();
 }
 
-template cudaError_t launch_up<double>(int, const UpTask*, int, const double*, double*, cudaStream_t);
-template cudaError_t launch_up<float>(int, const UpTask*, int, const float*, double*, cudaStream_t);
+template cudaError_t launch_up<double>(int, const UpTask*, int, const double*, double*, cudaStream_t, int);
+template cudaError_t launch_up<float>(int, const UpTask*, int, const float*, double*, cudaStream_t, int);
 template cudaError_t launch_blk<double>(int, const BlkTask*, int, const double*, const double*, double*, cudaStream_t, int);
 template cudaError_t launch_blk<float>(int, const BlkTask*, int, const float*, const double*, double*, cudaStream_t, int);
-template cudaError_t launch_down<double>(int, const DownTask*, int, const double*, const double*, double*, double*, cudaStream_t);
-template cudaError_t launch_down<float>(int, const DownTask*, int, const float*, const double*, double*, double*, cudaStream_t);
+template cudaError_t launch_down<double>(int, const DownTask*, int, const double*, const double*, double*, double*, cudaStream_t, int);
+template cudaError_t launch_down<float>(int, const DownTask*, int, const float*, const double*, double*, double*, cudaStream_t, int);
 
 }  // namespace h2gpu

@@ -14,13 +14,13 @@ constexpr int KRNL_RPY_ID = 4;
 cudaError_t launch_gather(int NV, const double* X, long long x_rs, long long x_cs, int nv, const int* fwd, int N,
                           double* XS, cudaStream_t st);
 template <typename TA>
-cudaError_t launch_up(int NV, const UpTask* t, int n, const TA* U, double* XS, cudaStream_t st);
+cudaError_t launch_up(int NV, const UpTask* t, int n, const TA* U, double* XS, cudaStream_t st, int use_tc = 0);
 template <typename TA>
 cudaError_t launch_blk(int NV, const BlkTask* t, int n, const TA* arena, const double* XS, double* PS, cudaStream_t st,
                        int use_tc = 0);
 template <typename TA>
 cudaError_t launch_down(int NV, const DownTask* t, int n, const TA* U, const double* Y1, double* PS, double* PUSH,
-                        cudaStream_t st);
+                        cudaStream_t st, int use_tc = 0);
 cudaError_t launch_y1sum(int NV, const Y1Task* t, int n, const int* slots, const double* PS, double* Y1, cudaStream_t st);
 cudaError_t launch_asm(int NV, const AsmTask* t, int n, const int* slots, const double* PS, const int* fwd,
                        double* Y, long long y_rs, long long y_cs, int nv, cudaStream_t st);
