@@ -1006,7 +1006,7 @@ int run_panel(h2gpu_image* im, int NV, int nv, const double* X, long long x_rs, 
             CK(launch_up<float>(NV, im->d_up + b, n, im->d_U32, im->d_XS, s, sweep_tc(im)));
         }
         if (timed) CK(cudaEventRecord(e[3], s));
-        CK(launch_pair(im->kernel_id, NV, im->d_owF, im->n_owF, im->d_pp, im->d_pts32, kp, im->d_XS, im->d_PS, s));
+        CK(launch_pair(im->kernel_id, NV, im->d_owF, im->n_owF, im->d_pp, im->d_pts32, kp, im->d_XS, im->d_PS, s, 1));
         CK(launch_jit(im->kernel_id, 1, NV, im->d_jtF2, im->n_jtF2, im->d_js, im->d_pts32, kp, 1, 1, im->d_XS,
                       im->d_PS, im->d_Y1, s, 1));
         CK(launch_y1sum(NV, im->d_y1t2, im->n_y12, im->d_y1_slots2, im->d_PS, im->d_Y1, s));

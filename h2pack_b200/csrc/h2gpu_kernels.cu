@@ -1097,7 +1097,7 @@ struct PairSmem {
     float k[NW][16][9];
 };
 
-template <int KID, int NV>
+template <int KID, int NV, bool FAR>
 __global__ void __launch_bounds__(32 * kPairWarps, 3) k_jit_pair(const PairOwner* __restrict__ owners,
                                                                  const PairPartner* __restrict__ partners,
                                                                  const float4* __restrict__ pts, KParam kp,
@@ -1112,6 +1112,8 @@ __global__ void __launch_bounds__(32 * kPairWarps, 3) k_jit_pair(const PairOwner
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, tq = lane & 3;
     const PairOwner ow = owners[blockIdx.x];
     const float p0 = (float) kp.p0, c0 = (float) kp.c0;
+    float q0 = 0.f, q1 = 0.f;
+    if constexpr (FAR) ScalarFar<KID>::prep(p0, c0, q0, q1);
     float* sk = &sm.k[warp][0][0];
     float* d2w = &sm.d2[warp][0][0];
 
@@ -1134,7 +1136,12 @@ __global__ void __launch_bounds__(32 * kPairWarps, 3) k_jit_pair(const PairOwner
         }
     };
     auto store_tile = [&](int buf) {
-        if (threadIdx.x < TS) sm.pt[buf][threadIdx.x] = rp;
+        if (threadIdx.x < TS)
+        {
+            float4 q = rp;
+            if (FAR) q.w = q.x * q.x + q.y * q.y + q.z * q.z;   // |b|^2 for the far form of r^2
+            sm.pt[buf][threadIdx.x] = q;
+        }
 #pragma unroll
         for (int u = 0; u < NB; u++)
         {
@@ -1204,20 +1211,38 @@ __global__ void __launch_bounds__(32 * kPairWarps, 3) k_jit_pair(const PairOwner
             {
                 const float ax = x0.x + pb.sx, ay = x0.y + pb.sy, az = x0.z + pb.sz;
                 const float bx = x1.x + pb.sx, by = x1.y + pb.sy, bz = x1.z + pb.sz;
+                // rows (g, g+8) of a as packed pairs; far form: -2a and |a|^2 in b's frame
+                const float2 m_x = make_float2(-2.f * ax, -2.f * bx), m_y = make_float2(-2.f * ay, -2.f * by),
+                             m_z = make_float2(-2.f * az, -2.f * bz);
+                const float2 s2 = make_float2(ax * ax + ay * ay + az * az, bx * bx + by * by + bz * bz);
                 const int ngrp = (nj + 7) >> 3;
                 for (int grp = 0; grp < ngrp; grp++)
                 {
                     const float4 pa = sm.pt[buf][grp * 8 + tq], pc = sm.pt[buf][grp * 8 + tq + 4];
                     float k[4];
+                    if constexpr (FAR)
                     {
-                        float dx = ax - pa.x, dy = ay - pa.y, dz = az - pa.z;
-                        k[0] = Scalar<KID, float>::f(dx * dx + dy * dy + dz * dz, p0, c0);   // (a g,   b t)
-                        dx = bx - pa.x; dy = by - pa.y; dz = bz - pa.z;
-                        k[1] = Scalar<KID, float>::f(dx * dx + dy * dy + dz * dz, p0, c0);   // (a g+8, b t)
-                        dx = ax - pc.x; dy = ay - pc.y; dz = az - pc.z;
-                        k[2] = Scalar<KID, float>::f(dx * dx + dy * dy + dz * dz, p0, c0);   // (a g,   b t+4)
-                        dx = bx - pc.x; dy = by - pc.y; dz = bz - pc.z;
-                        k[3] = Scalar<KID, float>::f(dx * dx + dy * dy + dz * dz, p0, c0);   // (a g+8, b t+4)
+                        auto r2p = [&](const float4& p) {
+                            float2 t = __fadd2_rn(s2, make_float2(p.w, p.w));
+                            t = __ffma2_rn(m_z, make_float2(p.z, p.z), t);
+                            t = __ffma2_rn(m_y, make_float2(p.y, p.y), t);
+                            return __ffma2_rn(m_x, make_float2(p.x, p.x), t);
+                        };
+                        const float2 ka = ScalarFar<KID>::f2(r2p(pa), q0, q1);   // (a g, b t), (a g+8, b t)
+                        const float2 kb = ScalarFar<KID>::f2(r2p(pc), q0, q1);   // (a g, b t+4), (a g+8, b t+4)
+                        k[0] = ka.x; k[1] = ka.y; k[2] = kb.x; k[3] = kb.y;
+                    } else {
+                        auto r2d = [&](const float4& p) {
+                            const float2 dx = __fadd2_rn(make_float2(ax, bx), make_float2(-p.x, -p.x));
+                            const float2 dy = __fadd2_rn(make_float2(ay, by), make_float2(-p.y, -p.y));
+                            const float2 dz = __fadd2_rn(make_float2(az, bz), make_float2(-p.z, -p.z));
+                            return __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+                        };
+                        const float2 ra2 = r2d(pa), rc2 = r2d(pc);
+                        k[0] = Scalar<KID, float>::f(ra2.x, p0, c0);   // (a g,   b t)
+                        k[1] = Scalar<KID, float>::f(ra2.y, p0, c0);   // (a g+8, b t)
+                        k[2] = Scalar<KID, float>::f(rc2.x, p0, c0);   // (a g,   b t+4)
+                        k[3] = Scalar<KID, float>::f(rc2.y, p0, c0);   // (a g+8, b t+4)
                     }
                     // rows of a beyond the chunk contribute nothing to b
                     if (!v0) { k[0] = 0.f; k[2] = 0.f; }
@@ -1870,37 +1895,45 @@ cudaError_t launch_jit(int kid, int fp32, int NV, const JitTarget* tg, int n, co
     }
 }
 
-template <int KID>
-static cudaError_t launch_pair_k(int NV, const PairOwner* ow, int n, const PairPartner* pp, const float4* pts, KParam kp,
-                                 const double* XS, double* PS, cudaStream_t st)
+template <int KID, bool FAR>
+static cudaError_t launch_pair_kf(int NV, const PairOwner* ow, int n, const PairPartner* pp, const float4* pts, KParam kp,
+                                  const double* XS, double* PS, cudaStream_t st)
 {
     if (NV == 16)
     {
         constexpr int b = pair_smem_bytes<16>();
-        cudaError_t e = allow_smem(k_jit_pair<KID, 16>, b);
+        cudaError_t e = allow_smem(k_jit_pair<KID, 16, FAR>, b);
         if (e != cudaSuccess) return e;
-        k_jit_pair<KID, 16><<<n, 32 * kPairWarps, b, st>>>(ow, pp, pts, kp, XS, PS);
+        k_jit_pair<KID, 16, FAR><<<n, 32 * kPairWarps, b, st>>>(ow, pp, pts, kp, XS, PS);
     } else if (NV == 8) {
         constexpr int b = pair_smem_bytes<8>();
-        cudaError_t e = allow_smem(k_jit_pair<KID, 8>, b);
+        cudaError_t e = allow_smem(k_jit_pair<KID, 8, FAR>, b);
         if (e != cudaSuccess) return e;
-        k_jit_pair<KID, 8><<<n, 32 * kPairWarps, b, st>>>(ow, pp, pts, kp, XS, PS);
+        k_jit_pair<KID, 8, FAR><<<n, 32 * kPairWarps, b, st>>>(ow, pp, pts, kp, XS, PS);
     } else {
         return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
 }
 
+template <int KID>
+static cudaError_t launch_pair_k(int NV, const PairOwner* ow, int n, const PairPartner* pp, const float4* pts, KParam kp,
+                                 const double* XS, double* PS, cudaStream_t st, int far)
+{
+    return far ? launch_pair_kf<KID, true>(NV, ow, n, pp, pts, kp, XS, PS, st)
+               : launch_pair_kf<KID, false>(NV, ow, n, pp, pts, kp, XS, PS, st);
+}
+
 cudaError_t launch_pair(int kid, int NV, const PairOwner* ow, int n, const PairPartner* pp, const void* pts, KParam kp,
-                        const double* XS, double* PS, cudaStream_t st)
+                        const double* XS, double* PS, cudaStream_t st, int far)
 {
     if (n <= 0) return cudaSuccess;
     const float4* p = (const float4*) pts;
     switch (kid)
     {
-        case KRNL_COULOMB_ID:  return launch_pair_k<KRNL_COULOMB_ID>(NV, ow, n, pp, p, kp, XS, PS, st);
-        case KRNL_GAUSSIAN_ID: return launch_pair_k<KRNL_GAUSSIAN_ID>(NV, ow, n, pp, p, kp, XS, PS, st);
-        case KRNL_MATERN32_ID: return launch_pair_k<KRNL_MATERN32_ID>(NV, ow, n, pp, p, kp, XS, PS, st);
+        case KRNL_COULOMB_ID:  return launch_pair_k<KRNL_COULOMB_ID>(NV, ow, n, pp, p, kp, XS, PS, st, far);
+        case KRNL_GAUSSIAN_ID: return launch_pair_k<KRNL_GAUSSIAN_ID>(NV, ow, n, pp, p, kp, XS, PS, st, far);
+        case KRNL_MATERN32_ID: return launch_pair_k<KRNL_MATERN32_ID>(NV, ow, n, pp, p, kp, XS, PS, st, far);
         default: return cudaErrorInvalidValue;
     }
 }

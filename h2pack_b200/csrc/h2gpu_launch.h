@@ -28,7 +28,8 @@ cudaError_t launch_jit(int kid, int fp32, int NV, const JitTarget* tg, int n, co
                        KParam kp, int use_shift, int use_tc, const double* XS, double* PS, double* Y1, cudaStream_t st,
                        int far = 0);   // far: every source set is admissible for its target (r > 0)
 cudaError_t launch_pair(int kid, int NV, const PairOwner* ow, int n, const PairPartner* pp, const void* pts, KParam kp,
-                        const double* XS, double* PS, cudaStream_t st);
+                        const double* XS, double* PS, cudaStream_t st,
+                        int far = 0);
 cudaError_t launch_direct(int kid, const double4* trg, int n_trg, const double4* src, int n_src, const double* val,
                           KParam kp, double* out, cudaStream_t st);
 
