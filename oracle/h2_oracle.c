@@ -141,13 +141,13 @@ static void gemv_n(int nrow, int ncol, const double *A, int lda, const double *x
         const double *a = A + (size_t) i * lda;
         double s = 0.0;
         for (int j = 0; j < ncol; j++) s += a[j] * x[j];
-        y[i] = beta * y[i] + s;
+        y[i] = (beta == 0.0) ? s : beta * y[i] + s;   /* BLAS: y is not read when beta == 0 */
     }
 }
 
 static void gemv_t(int nrow, int ncol, const double *A, int lda, const double *x, double beta, double *y)
 {
-    for (int j = 0; j < ncol; j++) y[j] *= beta;
+    for (int j = 0; j < ncol; j++) y[j] = (beta == 0.0) ? 0.0 : y[j] * beta;   /* y not read when beta == 0 */
     for (int i = 0; i < nrow; i++)
     {
         const double *a = A + (size_t) i * lda;
