@@ -389,7 +389,6 @@ __global__ void __launch_bounds__(256, 3) k_blk1(const BlkTask* __restrict__ tas
         for (int cw = 0; cw < ncol; cw += CW)
         {
             const int cend = min(ncol, cw + CW);
-#pragma unroll 2
             for (int cs = cw; cs < cend; cs += 32 * CPL)
             {
                 int c[CPL];
