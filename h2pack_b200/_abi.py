@@ -21,7 +21,7 @@ STATUS_NAMES = {0: "OK", -1: "INVALID", -2: "UNSUPPORTED", -3: "CUDA", -4: "NOME
 KRNL_COULOMB, KRNL_GAUSSIAN, KRNL_MATERN32, KRNL_RPY = 1, 2, 3, 4
 KERNEL_IDS = {"coulomb": KRNL_COULOMB, "gaussian": KRNL_GAUSSIAN, "matern32": KRNL_MATERN32, "rpy": KRNL_RPY}
 PREC_FP64, PREC_MIXED = 0, 1
-JIT_SIMT, JIT_TC, JIT_PAIR = 0, 1, 2
+JIT_SIMT, JIT_TC, JIT_PAIR, BLK_TCGEN05 = 0, 1, 2, 3
 CG_FREE, CG_RUN, CG_CHECK, CG_DONE = 0, 1, 2, 3
 CG_MATVEC, CG_PCG = 0, 1
 ROW_MAJOR, COL_MAJOR = 101, 102

@@ -163,7 +163,8 @@ struct h2gpu_image {
     // tuning (h2gpu_autotune) and captured graph (h2gpu_graph_capture)
     int jit_tc = 1;          // tensor-core JIT kernel for FP32 panels of 8 / 16
     int jit_pair = 0;        // with jit_tc: the pair kernel (each unordered pair once)
-    int blk_tc = 1;          // tensor-core stored-block kernel for FP32 panels of 8 / 16
+    int blk_tc = 1;          // stored-block kernel for FP32 panels of 8 / 16: 1 mma.sync, 2 tcgen05, 0 CUDA cores
+    int* d_status = nullptr; // device status word (bounded waits of the tcgen05 kernel)
     int tuned_nv = 0;        // panel width chosen by the autotuner (0: default rule)
     int n_images = 1;        // matrices in this image (batched images hold several)
     cudaGraph_t graph = nullptr;
@@ -178,7 +179,7 @@ void free_all(h2gpu_image* im)
                     im->d_js, im->d_asm, im->d_asm_slots, im->d_fwd, im->d_bwd, im->d_U64, im->d_U32, im->d_B64,
                     im->d_B32, im->d_D64, im->d_D32, im->d_pts64, im->d_pts32, im->d_XS, im->d_PS, im->d_Y1,
                     im->d_PUSH, im->d_io, im->d_owN, im->d_owF, im->d_pp, im->d_jtN2, im->d_jtF2, im->d_y1t2,
-                    im->d_y1_slots2, im->d_asm2, im->d_asm_slots2};
+                    im->d_y1_slots2, im->d_asm2, im->d_asm_slots2, im->d_status};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (auto& e : im->ev.e)
@@ -1028,7 +1029,7 @@ int run_panel(h2gpu_image* im, int NV, int nv, const double* X, long long x_rs, 
     if (timed) CK(cudaEventRecord(e[1], s));
     if (!im->BD_JIT)
     {
-        if (f32) CK(launch_blk<float>(NV, im->d_blkD, im->n_blkD, im->d_D32, im->d_XS, im->d_PS, s, im->blk_tc));
+        if (f32) CK(launch_blk<float>(NV, im->d_blkD, im->n_blkD, im->d_D32, im->d_XS, im->d_PS, s, im->blk_tc, im->d_status));
         else CK(launch_blk<double>(NV, im->d_blkD, im->n_blkD, im->d_D64, im->d_XS, im->d_PS, s));
     } else {
         CK(launch_jit(im->kernel_id, f32, NV, im->d_jtN, im->n_jtN, im->d_js, f32 ? (const void*) im->d_pts32 : (const void*) im->d_pts64,
@@ -1044,7 +1045,7 @@ int run_panel(h2gpu_image* im, int NV, int nv, const double* X, long long x_rs, 
     if (timed) CK(cudaEventRecord(e[3], s));
     if (!im->BD_JIT)
     {
-        if (f32) CK(launch_blk<float>(NV, im->d_blkB, im->n_blkB, im->d_B32, im->d_XS, im->d_PS, s, im->blk_tc));
+        if (f32) CK(launch_blk<float>(NV, im->d_blkB, im->n_blkB, im->d_B32, im->d_XS, im->d_PS, s, im->blk_tc, im->d_status));
         else CK(launch_blk<double>(NV, im->d_blkB, im->n_blkB, im->d_B64, im->d_XS, im->d_PS, s));
         CK(launch_y1sum(NV, im->d_y1t, im->n_y1, im->d_y1_slots, im->d_PS, im->d_Y1, s));
     } else {
@@ -1063,6 +1064,21 @@ int run_panel(h2gpu_image* im, int NV, int nv, const double* X, long long x_rs, 
     if (timed) CK(cudaEventRecord(e[6], s));
     im->st.n_launches += 4 + (long long) (im->up_beg.size() - 1) + (long long) (im->dn_beg.size() - 1)
                          + (im->BD_JIT ? 0 : 1);
+    return H2GPU_OK;
+}
+
+// Bounded waits inside the tcgen05 block kernel set the image's status word when they
+// expire; a synchronised apply reports it (and clears it) as H2GPU_ERR_DEVICE.
+int check_status(h2gpu_image* im)
+{
+    if (!im->d_status || im->blk_tc != 2 || im->BD_JIT || im->precision != H2GPU_PREC_MIXED) return H2GPU_OK;
+    int st = 0;
+    CK(cudaMemcpy(&st, im->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (st != 0)
+    {
+        CK(cudaMemset(im->d_status, 0, sizeof(int)));
+        return fail(H2GPU_ERR_DEVICE, "tcgen05 block kernel: a bounded wait on the MMA completion expired");
+    }
     return H2GPU_OK;
 }
 
@@ -1092,6 +1108,7 @@ int apply_device(h2gpu_image* im, int n_vec, const double* X, long long x_rs, lo
         int nv = std::min(NV, n_vec - c0);
         TRY(run_panel(im, NV, nv, X + c0 * x_cs, x_rs, x_cs, Y + c0 * y_cs, y_rs, y_cs, s, true));
         CK(cudaEventSynchronize(im->ev.e[6]));
+        TRY(check_status(im));
         float t[6];
         for (int k = 0; k < 6; k++) CK(cudaEventElapsedTime(&t[k], im->ev.e[k], im->ev.e[k + 1]));
         ph[0] += t[0] + t[2];   // gather + upward
@@ -1189,6 +1206,9 @@ H2G_API int h2gpu_image_create(const h2gpu_desc* desc, const h2gpu_options* opt,
             if (cudaEventCreate(&ev) != cudaSuccess) { st = fail(H2GPU_ERR_CUDA, "event creation failed"); break; }
         if (st != H2GPU_OK) break;
         st = upload_plan(im, desc, hp);
+        if (st == H2GPU_OK && (cudaMalloc(&im->d_status, sizeof(int)) != cudaSuccess ||
+                               cudaMemset(im->d_status, 0, sizeof(int)) != cudaSuccess))
+            st = fail(H2GPU_ERR_NOMEM, "status word allocation failed");
     } while (0);
     if (st != H2GPU_OK)
     {
@@ -1657,17 +1677,24 @@ H2G_API int h2gpu_graph_launch(h2gpu_image* im, void* stream)
     return H2GPU_OK;
 }
 
+static void set_variant(h2gpu_image* im, int variant)
+{
+    im->jit_tc = variant != H2GPU_JIT_SIMT;
+    im->jit_pair = variant == H2GPU_JIT_PAIR;
+    im->blk_tc = variant == H2GPU_JIT_SIMT ? 0 : (variant == H2GPU_BLK_TCGEN05 ? 2 : 1);
+}
+
 H2G_API int h2gpu_set_jit_variant(h2gpu_image* im, int variant)
 {
     if (!im) return fail(H2GPU_ERR_INVALID, "image is NULL");
-    REQ(variant == H2GPU_JIT_SIMT || variant == H2GPU_JIT_TC || variant == H2GPU_JIT_PAIR, "unknown JIT variant %d",
-        variant);
+    REQ(variant == H2GPU_JIT_SIMT || variant == H2GPU_JIT_TC || variant == H2GPU_JIT_PAIR ||
+            variant == H2GPU_BLK_TCGEN05, "unknown kernel variant %d", variant);
     if (variant == H2GPU_JIT_PAIR && !im->has_pair)
         return fail(H2GPU_ERR_UNSUPPORTED, "the pair variant needs a JIT image of a scalar kernel");
+    if (variant == H2GPU_BLK_TCGEN05 && im->BD_JIT)
+        return fail(H2GPU_ERR_UNSUPPORTED, "the tcgen05 variant applies to stored-block images");
     std::lock_guard<std::mutex> lk(im->mu);
-    im->jit_tc = variant != H2GPU_JIT_SIMT;
-    im->jit_pair = variant == H2GPU_JIT_PAIR;
-    im->blk_tc = variant != H2GPU_JIT_SIMT;
+    set_variant(im, variant);
     return H2GPU_OK;
 }
 
@@ -1688,7 +1715,7 @@ H2G_API int h2gpu_autotune(h2gpu_image* im, int n_vec, const double* dX, int ldx
     for (int w = 1; w <= full; w <<= 1)
         if (w == full || w >= 4) nvs.push_back(w);
     auto variant = [&]() {
-        if (!im->BD_JIT) return im->blk_tc ? H2GPU_JIT_TC : H2GPU_JIT_SIMT;
+        if (!im->BD_JIT) return im->blk_tc == 2 ? H2GPU_BLK_TCGEN05 : (im->blk_tc ? H2GPU_JIT_TC : H2GPU_JIT_SIMT);
         return im->jit_tc ? (im->jit_pair ? H2GPU_JIT_PAIR : H2GPU_JIT_TC) : H2GPU_JIT_SIMT;
     };
     std::vector<int> vars = {variant()};
@@ -1696,6 +1723,7 @@ H2G_API int h2gpu_autotune(h2gpu_image* im, int n_vec, const double* dX, int ldx
     {
         vars = {H2GPU_JIT_TC, H2GPU_JIT_SIMT};
         if (im->BD_JIT && im->has_pair) vars.push_back(H2GPU_JIT_PAIR);
+        if (!im->BD_JIT) vars.push_back(H2GPU_BLK_TCGEN05);
     }
     float best = 1e30f;
     int bnv = full, bvar = variant();
@@ -1703,10 +1731,8 @@ H2G_API int h2gpu_autotune(h2gpu_image* im, int n_vec, const double* dX, int ldx
     for (int nv : nvs)
         for (int var : vars)
         {
-            if (var == H2GPU_JIT_PAIR && nv != 8 && nv != 16) continue;
-            im->jit_tc = var != H2GPU_JIT_SIMT;
-            im->jit_pair = var == H2GPU_JIT_PAIR;
-            im->blk_tc = var != H2GPU_JIT_SIMT;
+            if ((var == H2GPU_JIT_PAIR || var == H2GPU_BLK_TCGEN05) && nv != 8 && nv != 16) continue;
+            set_variant(im, var);
             TRY(prepare(im, nv));
             float ms = 0;
             for (int rep = 0; rep < 2; rep++)
@@ -1721,9 +1747,8 @@ H2G_API int h2gpu_autotune(h2gpu_image* im, int n_vec, const double* dX, int ldx
             if (ms < best) { best = ms; bnv = nv; bvar = var; }
         }
     im->tuned_nv = bnv;
-    im->jit_tc = bvar != H2GPU_JIT_SIMT;
-    im->jit_pair = bvar == H2GPU_JIT_PAIR;
-    im->blk_tc = bvar != H2GPU_JIT_SIMT;
+    set_variant(im, bvar);
+    TRY(check_status(im));
     if (best_nv) *best_nv = bnv;
     if (best_variant) *best_variant = bvar;
     return H2GPU_OK;

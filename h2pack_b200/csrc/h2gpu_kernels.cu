@@ -1522,6 +1522,260 @@ __global__ void __launch_bounds__(256, 4) k_blk_tc(const BlkTask* __restrict__ t
     }
 }
 
+// ------------------------------------ stored blocks on tcgen05 (TMEM accumulators)
+
+// PTX wrappers (sm_100a).  Shared addresses are 32-bit shared-window addresses.
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t) __cvta_generic_to_shared(p); }
+
+// Shared-memory matrix descriptor: start address, leading / stride byte offsets (16-byte
+// units), version 1, layout type (0 = no swizzle, 2 = 128-byte swizzle).
+__device__ __forceinline__ uint64_t umma_desc(uint32_t start, uint32_t lbo_bytes, uint32_t sbo_bytes, uint32_t layout)
+{
+    return (uint64_t) ((start >> 4) & 0x3FFFu) | ((uint64_t) ((lbo_bytes >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t) ((sbo_bytes >> 4) & 0x3FFFu) << 32) | (1ull << 46) | ((uint64_t) layout << 61);
+}
+
+// Instruction descriptor, kind::tf32: FP32 accumulator, TF32 A and B, A K-major (0) or
+// MN-major (1), B K-major, N = n, M = 64.
+__host__ __device__ constexpr uint32_t umma_idesc_tf32(int n, int a_mn_major)
+{
+    return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t) a_mn_major << 15) | ((uint32_t) (n >> 3) << 17) |
+           ((uint32_t) (64 >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_tf32(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc)
+{
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}"
+                 ::"r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(acc) : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t mbar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t mbar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.b32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok) : "r"(mbar), "r"(parity) : "memory");
+    return ok != 0;
+}
+
+// One stored block task (up to 1024 rows x ncol, FP32 copy) for panels of 8 / 16
+// right-hand sides on the 5th-generation tensor cores, both products per 64 x 64 tile
+// of A with the tile read from HBM once:
+//   C0 (64 rows x NV) += A_tile (64 x 64) V_tile (64 x NV)      A K-major   -> TMEM lanes 0-15 of each sub-partition
+//   C1 (64 cols x NV)  = A_tile^T (64 x 64) W_chunk (64 x NV)   A MN-major  -> TMEM lanes 16-31
+// Both read the same shared copy of the tile (128-byte swizzled rows of 32 columns: a
+// K-major view for C0 and an MN-major view for C1), split into TF32 hi / lo for 3xTF32
+// (hi.hi + lo.hi + hi.lo, FP32 accumulation in TMEM).  One thread issues the 48 MMAs
+// of a tile and commits them to an mbarrier; meanwhile all threads load the next tile
+// from global memory into registers.  C1 of each tile is read from TMEM and added into
+// the task's single C1 slot (stored by the first 64-row chunk); C0 accumulates over a
+// chunk's column tiles in TMEM and is written when the chunk ends.  Every wait on the
+// mbarrier is bounded: on expiry the kernel records a status and stops issuing work.
+struct Tc5Smem {
+    float a_hi[2 * 64 * 32];   // two column blocks (32 columns) x 64 rows, 128 B rows, swizzled
+    float a_lo[2 * 64 * 32];
+    float v_hi[16 * 64];       // V^T (NV x 64 columns), core matrices 8 x 4, K-major
+    float v_lo[16 * 64];
+    float w_hi[16 * 64];       // W^T (NV x 64 rows)
+    float w_lo[16 * 64];
+    unsigned long long mbar;
+    uint32_t tmem;
+};
+
+constexpr int kTc5Threads = 128;
+
+template <int NV>
+__global__ void __launch_bounds__(kTc5Threads, 4) k_blk_tc5(const BlkTask* __restrict__ tasks,
+                                                            const float* __restrict__ arena,
+                                                            const double* __restrict__ XS, double* __restrict__ PS,
+                                                            int* __restrict__ status)
+{
+    constexpr int NB = NV / 8;                         // 8-row groups of the NV x K operands
+    constexpr uint32_t IDESC0 = umma_idesc_tf32(NV, 0), IDESC1 = umma_idesc_tf32(NV, 1);
+    extern __shared__ __align__(1024) unsigned char tc5_raw[];
+    // 1024-byte alignment of the swizzled tiles
+    Tc5Smem& sm = *reinterpret_cast<Tc5Smem*>(tc5_raw + ((1024 - (smem_u32(tc5_raw) & 1023)) & 1023));
+    const BlkTask T = tasks[blockIdx.x];
+    const int ncol = T.ncol, nrow = T.nrow;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const bool do0 = T.out0_row >= 0, do1 = T.out1_row >= 0;
+    const int ntc = (ncol + 63) / 64, nt = ntc * ((nrow + 63) / 64);
+    const float* A0 = arena + T.a_off;
+
+    // TMEM: 32 columns (C0 in lanes 0-15, C1 in lanes 16-31 of each sub-partition)
+    if (warp == 0)
+    {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 32;" ::"r"(smem_u32(&sm.tmem)) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0)
+    {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&sm.mbar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = sm.tmem, mbar = smem_u32(&sm.mbar);
+    const uint32_t a_hi = smem_u32(sm.a_hi), a_lo = smem_u32(sm.a_lo);
+    const uint32_t v_hi = smem_u32(sm.v_hi), v_lo = smem_u32(sm.v_lo), w_hi = smem_u32(sm.w_hi), w_lo = smem_u32(sm.w_lo);
+
+    // registers of the tile being loaded: 32 A values, 8 V values, 8 W values per thread
+    float ra[32];
+    double rv[8 * NB / 2], rw[8 * NB / 2];
+    auto load_tile = [&](int t) {
+        const int rc = (t / ntc) * 64, c0 = (t % ntc) * 64, R = min(64, nrow - rc);
+        const float* A = A0 + (long long) rc * ncol + c0;
+#pragma unroll
+        for (int u = 0; u < 32; u++)
+        {
+            const int e = tid + kTc5Threads * u, r = e >> 6, c = e & 63;
+            ra[u] = (r < R && c0 + c < ncol) ? A[(long long) r * ncol + c] : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < 4 * NB; u++)
+        {
+            const int e = tid + kTc5Threads * u, k = e / NV, n = e % NV;   // 64 x NV
+            rv[u] = (do0 && c0 + k < ncol) ? XS[(long long) (T.in0_row + c0 + k) * NV + n] : 0.0;
+            rw[u] = (do1 && c0 == 0 && k < R) ? XS[(long long) (T.in1_row + rc + k) * NV + n] : 0.0;
+        }
+    };
+    auto split = [](float x, float& h, float& l) {
+        const uint32_t hb = tf32_rna(x);
+        h = __uint_as_float(hb);
+        l = x - h;
+    };
+    auto store_tile = [&](int t) {
+        const int c0 = (t % ntc) * 64;
+#pragma unroll
+        for (int u = 0; u < 32; u++)
+        {
+            const int e = tid + kTc5Threads * u, r = e >> 6, c = e & 63, cc = c & 31;
+            const int off = (c >> 5) * 8192 + (r >> 3) * 1024 + (r & 7) * 128 + ((((cc >> 2) ^ (r & 7)) << 4) | ((cc & 3) << 2));
+            float h, l;
+            split(ra[u], h, l);
+            *reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(sm.a_hi) + off) = h;
+            *reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(sm.a_lo) + off) = l;
+        }
+#pragma unroll
+        for (int u = 0; u < 4 * NB; u++)
+        {
+            const int e = tid + kTc5Threads * u, k = e / NV, n = e % NV;
+            const int off = (((k >> 2) * NB + (n >> 3)) * 128 + (n & 7) * 16 + (k & 3) * 4) >> 2;
+            float h, l;
+            split((float) rv[u], h, l);
+            sm.v_hi[off] = h; sm.v_lo[off] = l;
+            if (c0 == 0)
+            {
+                split((float) rw[u], h, l);
+                sm.w_hi[off] = h; sm.w_lo[off] = l;
+            }
+        }
+    };
+
+    bool ok = true;
+    uint32_t phase = 0;
+    // read back the tile just multiplied: C1 into its slot, C0 at the end of a chunk.
+    // Thread 0 waits (bounded) for the MMAs' commit; the outcome is made uniform.
+    auto drain = [&](int t) {
+        int good = 1;
+        if (tid == 0)
+        {
+            int it = 0;
+            while (!mbar_try_wait(mbar, phase))
+                if (++it > (1 << 22)) { good = 0; break; }
+            if (!good) atomicExch(status, 1);
+        }
+        phase ^= 1;
+        ok = __syncthreads_and(good) != 0;
+        if (!ok) return;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        uint32_t d[16];
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                     : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7]),
+                       "=r"(d[8]), "=r"(d[9]), "=r"(d[10]), "=r"(d[11]), "=r"(d[12]), "=r"(d[13]), "=r"(d[14]), "=r"(d[15])
+                     : "r"(tmem + ((uint32_t) (32 * warp) << 16)));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        const int rc = (t / ntc) * 64, c0 = (t % ntc) * 64, R = min(64, nrow - rc);
+        const int m = 16 * warp + (lane & 15);
+        if (lane >= 16)
+        {
+            if (do1 && c0 + m < ncol)
+            {
+                double* o = PS + (long long) (T.out1_row + c0 + m) * NV;
+#pragma unroll
+                for (int n = 0; n < NV; n++)
+                {
+                    const double v = (double) __uint_as_float(d[n]);
+                    o[n] = (rc == 0) ? v : o[n] + v;
+                }
+            }
+        } else if (do0 && c0 + 64 >= ncol && m < R) {
+            double* o = PS + (long long) (T.out0_row + rc + m) * NV;
+#pragma unroll
+            for (int n = 0; n < NV; n++) o[n] = (double) __uint_as_float(d[n]);
+        }
+    };
+
+    if (nt > 0) load_tile(0);
+    for (int t = 0; t < nt; t++)
+    {
+        if (t > 0) drain(t - 1);
+        if (!ok) break;
+        store_tile(t);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        if (tid == 0)
+        {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const bool chunk_start = (t % ntc) == 0;
+            if (do0)
+                for (int j = 0; j < 8; j++)
+                {
+                    // K-step of 8 columns: column block j / 4, 32-byte step within the row
+                    const uint32_t ao = (j >> 2) * 8192 + (j & 3) * 32, bo = j * 2 * NB * 128;
+                    const uint64_t ah = umma_desc(a_hi + ao, 16, 1024, 2), al = umma_desc(a_lo + ao, 16, 1024, 2);
+                    const uint64_t bh = umma_desc(v_hi + bo, NB * 128, 128, 0), bl = umma_desc(v_lo + bo, NB * 128, 128, 0);
+                    umma_tf32(tmem, al, bh, IDESC0, (chunk_start && j == 0) ? 0u : 1u);
+                    umma_tf32(tmem, ah, bl, IDESC0, 1u);
+                    umma_tf32(tmem, ah, bh, IDESC0, 1u);
+                }
+            if (do1)
+                for (int j = 0; j < 8; j++)
+                {
+                    // K-step of 8 rows: one 8-row group of the swizzled tile (MN-major view:
+                    // 32-column blocks 8192 B apart, 8-row groups 1024 B apart)
+                    const uint32_t ao = j * 1024, bo = j * 2 * NB * 128;
+                    const uint64_t ah = umma_desc(a_hi + ao, 8192, 1024, 2), al = umma_desc(a_lo + ao, 8192, 1024, 2);
+                    const uint64_t bh = umma_desc(w_hi + bo, NB * 128, 128, 0), bl = umma_desc(w_lo + bo, NB * 128, 128, 0);
+                    umma_tf32(tmem + (16u << 16), al, bh, IDESC1, j == 0 ? 0u : 1u);
+                    umma_tf32(tmem + (16u << 16), ah, bl, IDESC1, 1u);
+                    umma_tf32(tmem + (16u << 16), ah, bh, IDESC1, 1u);
+                }
+            umma_commit(mbar);
+        }
+        if (t + 1 < nt) load_tile(t + 1);
+    }
+    if (ok && nt > 0) drain(nt - 1);
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+    {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 32;" ::"r"(tmem) : "memory");
+    }
+}
+
+template <int NV>
+constexpr int tc5_smem_bytes() { return (int) sizeof(Tc5Smem) + 1024; }
+
 // ---------------------------------------------- sweeps on the tensor cores (FP32 U)
 
 // Upward / downward sweep products for FP32 U and panels of 8 / 16 right-hand sides on
@@ -1772,12 +2026,29 @@ static cudaError_t allow_smem(K kern, int bytes)
 
 template <typename TA>
 cudaError_t launch_blk(int NV, const BlkTask* t, int n, const TA* arena, const double* XS, double* PS, cudaStream_t st,
-                       int use_tc)
+                       int use_tc, int* status)
 {
     if constexpr (sizeof(TA) == 4)
     {
         if (use_tc && n > 0 && (NV == 8 || NV == 16))
         {
+            if (use_tc == 2 && status)
+            {
+                // tcgen05 kernel (TMEM accumulators)
+                if (NV == 16)
+                {
+                    constexpr int b = tc5_smem_bytes<16>();
+                    cudaError_t e = allow_smem(k_blk_tc5<16>, b);
+                    if (e != cudaSuccess) return e;
+                    k_blk_tc5<16><<<n, kTc5Threads, b, st>>>(t, arena, XS, PS, status);
+                } else {
+                    constexpr int b = tc5_smem_bytes<8>();
+                    cudaError_t e = allow_smem(k_blk_tc5<8>, b);
+                    if (e != cudaSuccess) return e;
+                    k_blk_tc5<8><<<n, kTc5Threads, b, st>>>(t, arena, XS, PS, status);
+                }
+                return cudaGetLastError();
+            }
             if (NV == 16) k_blk_tc<16><<<n, 256, 0, st>>>(t, arena, XS, PS);
             else k_blk_tc<8><<<n, 256, 0, st>>>(t, arena, XS, PS);
             return cudaGetLastError();
@@ -1955,8 +2226,8 @@ cudaError_t launch_direct(int kid, const double4* trg, int n_trg, const double4*
 
 template cudaError_t launch_up<double>(int, const UpTask*, int, const double*, double*, cudaStream_t, int);
 template cudaError_t launch_up<float>(int, const UpTask*, int, const float*, double*, cudaStream_t, int);
-template cudaError_t launch_blk<double>(int, const BlkTask*, int, const double*, const double*, double*, cudaStream_t, int);
-template cudaError_t launch_blk<float>(int, const BlkTask*, int, const float*, const double*, double*, cudaStream_t, int);
+template cudaError_t launch_blk<double>(int, const BlkTask*, int, const double*, const double*, double*, cudaStream_t, int, int*);
+template cudaError_t launch_blk<float>(int, const BlkTask*, int, const float*, const double*, double*, cudaStream_t, int, int*);
 template cudaError_t launch_down<double>(int, const DownTask*, int, const double*, const double*, double*, double*, cudaStream_t, int);
 template cudaError_t launch_down<float>(int, const DownTask*, int, const float*, const double*, double*, double*, cudaStream_t, int);
 

@@ -17,7 +17,7 @@ template <typename TA>
 cudaError_t launch_up(int NV, const UpTask* t, int n, const TA* U, double* XS, cudaStream_t st, int use_tc = 0);
 template <typename TA>
 cudaError_t launch_blk(int NV, const BlkTask* t, int n, const TA* arena, const double* XS, double* PS, cudaStream_t st,
-                       int use_tc = 0);
+                       int use_tc = 0, int* status = nullptr);   // use_tc: 1 mma.sync, 2 tcgen05
 template <typename TA>
 cudaError_t launch_down(int NV, const DownTask* t, int n, const TA* U, const double* Y1, double* PS, double* PUSH,
                         cudaStream_t st, int use_tc = 0);

@@ -87,8 +87,9 @@ class Image:
         _abi.check(self.lib.h2gpu_graph_launch(self.handle, s), self.lib, "h2gpu_graph_launch")
 
     def set_jit_variant(self, variant: str):
-        """FP32 JIT kernel variant: "simt", "tc" (default) or "pair"."""
-        code = {"simt": _abi.JIT_SIMT, "tc": _abi.JIT_TC, "pair": _abi.JIT_PAIR}[variant]
+        """FP32 kernel variant: "simt", "tc" (default) or "pair" (JIT images), "tcgen05"
+        (stored-block images)."""
+        code = {"simt": _abi.JIT_SIMT, "tc": _abi.JIT_TC, "pair": _abi.JIT_PAIR, "tcgen05": _abi.BLK_TCGEN05}[variant]
         _abi.check(self.lib.h2gpu_set_jit_variant(self.handle, code), self.lib, "h2gpu_set_jit_variant")
 
     def autotune(self, X, Y):
@@ -98,7 +99,7 @@ class Image:
         st = self.lib.h2gpu_autotune(self.handle, X.shape[1], C.c_void_p(X.data_ptr()), X.stride(0),
                                      C.c_void_p(Y.data_ptr()), Y.stride(0), C.byref(nv), C.byref(var))
         _abi.check(st, self.lib, "h2gpu_autotune")
-        return nv.value, ("simt", "tc", "pair")[var.value]
+        return nv.value, ("simt", "tc", "pair", "tcgen05")[var.value]
 
     def matvec(self, x: np.ndarray) -> np.ndarray:
         x = np.ascontiguousarray(x, dtype=np.float64)

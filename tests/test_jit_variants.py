@@ -1,6 +1,6 @@
 """The FP32 kernel variants against the FP64 apply of the same image: for JIT images
 CUDA cores, tensor cores per target and tensor cores per unordered pair; for stored
-blocks CUDA cores and tensor cores.
+blocks CUDA cores, warp-level tensor-core MMAs and tcgen05 (TMEM accumulators).
 
 The reference evaluates every JIT block from both sides with one bi-matvec
 (src/H2Pack_matvec.c:170-236, H2P_matvec_fwd_transform/intmd_mult_JIT); the pair
@@ -28,7 +28,7 @@ def test_variants_match_fp64(name, nv):
         Y64 = img.matmul_device(X).cpu().numpy()
         img.set_precision("mixed")
         outs = {}
-        for var in (("simt", "tc", "pair") if name.endswith("jit") else ("simt", "tc")):
+        for var in (("simt", "tc", "pair") if name.endswith("jit") else ("simt", "tc", "tcgen05")):
             img.set_jit_variant(var)
             Ya = img.matmul_device(X).cpu().numpy()
             Yb = img.matmul_device(X).cpu().numpy()
@@ -50,5 +50,16 @@ def test_pair_variant_refused(name):
         with pytest.raises(RuntimeError):
             img.set_jit_variant("pair")
         img.set_jit_variant("tc")
+    finally:
+        img.close()
+
+
+def test_tcgen05_variant_refused_for_jit_images():
+    from h2pack_b200 import Image
+    h, _ = holder("matern32_jit")
+    img = Image(h.desc, precision="mixed")
+    try:
+        with pytest.raises(RuntimeError):
+            img.set_jit_variant("tcgen05")
     finally:
         img.close()
