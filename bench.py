@@ -52,6 +52,8 @@ def parse():
                    help="jit_matern: the headline configuration; the others print extra lines for the "
                         "other configurations (AOT Coulomb matvec, AOT RPY matmul, batched matrices, "
                         "served requests)")
+    p.add_argument("--variant", default="auto", choices=["auto", "simt", "tc", "tcgen05"],
+                   help="stored-block workloads: FP32 block-product kernel (auto = autotuned)")
     p.add_argument("--precisions", default="fp64,mixed",
                    help="stored-block workloads: which paths to time (comma list)")
     p.add_argument("--n-matrices", type=int, default=512)
@@ -441,8 +443,15 @@ def run_aot_rpy(args):
     Y = torch.empty_like(X)
     out, Ys = {}, {}
     precs = args.precisions.split(",")
+    tuned = None
     for prec in precs:
         H.set_precision(prec)
+        if prec == "mixed":
+            if args.variant == "auto":
+                tuned = img.autotune(X, Y)
+            else:
+                img.set_jit_variant(args.variant)
+                tuned = (16, args.variant)
         s0 = img.stats()
         ms = timed_loop(lambda: img.matmul_device(X, Y), args.steps, args.warmup)
         s1 = img.stats()
@@ -486,6 +495,7 @@ def run_aot_rpy(args):
     main_p = "mixed" if "mixed" in out else precs[0]
     line = {"metric": f"H2 matvecs/s (RPY N={n} AOT, reltol 1e-8, {nv} RHS)", "value": out[main_p]["matvecs_per_s"],
             "unit": "matvecs/s", "workload": "aot_rpy", "n": n, "nvec": nv, "build_seconds": build_s,
+            "tuned_panel_variant": tuned,
             "fp64": out.get("fp64"), "mixed": out.get("mixed"), "rel_err_vs_direct": err,
             "speedup_mixed_vs_fp64": out["fp64"]["ms"] / out["mixed"]["ms"] if len(out) == 2 else None,
             "roofline": {"bound": "hbm", "achieved": out[main_p]["streamed_GBps"], "peak": peak, "unit": "GB/s",

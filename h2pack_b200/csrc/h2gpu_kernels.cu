@@ -1567,19 +1567,24 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t mbar, uint32_t parity)
 // One stored block task (up to 1024 rows x ncol, FP32 copy) for panels of 8 / 16
 // right-hand sides on the 5th-generation tensor cores, both products per 64 x 64 tile
 // of A with the tile read from HBM once:
-//   C0 (64 rows x NV) += A_tile (64 x 64) V_tile (64 x NV)      A K-major   -> TMEM lanes 0-15 of each sub-partition
-//   C1 (64 cols x NV)  = A_tile^T (64 x 64) W_chunk (64 x NV)   A MN-major  -> TMEM lanes 16-31
-// Both read the same shared copy of the tile (128-byte swizzled rows of 32 columns: a
-// K-major view for C0 and an MN-major view for C1), split into TF32 hi / lo for 3xTF32
-// (hi.hi + lo.hi + hi.lo, FP32 accumulation in TMEM).  One thread issues the 48 MMAs
+//   C0 (64 rows x NV) += A_tile (64 x 64) V_tile (64 x NV)      A K-major   -> TMEM columns 0-15
+//   C1 (64 cols x NV)  = A_tile^T (64 x 64) W_chunk (64 x NV)   A MN-major  -> TMEM columns 16-31
+// (an M = 64 accumulator occupies lanes 0-15 of each of the four sub-partitions)
+// The tile is stored twice in shared memory, split into TF32 hi / lo for 3xTF32 (hi.hi
+// + lo.hi + hi.lo, FP32 accumulation in TMEM): 128-byte rows of 32 columns with the
+// 128-byte swizzle (16-byte granules XOR row mod 8) for the K-major view of C0, and the
+// same rows with the 32-byte-granule swizzle (granule XOR row mod 4) that MN-major TF32
+// operands need, for C1.  One thread issues the 48 MMAs
 // of a tile and commits them to an mbarrier; meanwhile all threads load the next tile
 // from global memory into registers.  C1 of each tile is read from TMEM and added into
 // the task's single C1 slot (stored by the first 64-row chunk); C0 accumulates over a
 // chunk's column tiles in TMEM and is written when the chunk ends.  Every wait on the
 // mbarrier is bounded: on expiry the kernel records a status and stops issuing work.
 struct Tc5Smem {
-    float a_hi[2 * 64 * 32];   // two column blocks (32 columns) x 64 rows, 128 B rows, swizzled
+    float a_hi[2 * 64 * 32];   // K-major view: two column blocks (32 columns) x 64 rows, 128 B rows, 128-byte swizzle
     float a_lo[2 * 64 * 32];
+    float t_hi[2 * 64 * 32];   // MN-major view: the same tile in the 32-byte-granule swizzle MN-major TF32 requires
+    float t_lo[2 * 64 * 32];
     float v_hi[16 * 64];       // V^T (NV x 64 columns), core matrices 8 x 4, K-major
     float v_lo[16 * 64];
     float w_hi[16 * 64];       // W^T (NV x 64 rows)
@@ -1608,7 +1613,7 @@ __global__ void __launch_bounds__(kTc5Threads, 4) k_blk_tc5(const BlkTask* __res
     const int ntc = (ncol + 63) / 64, nt = ntc * ((nrow + 63) / 64);
     const float* A0 = arena + T.a_off;
 
-    // TMEM: 32 columns (C0 in lanes 0-15, C1 in lanes 16-31 of each sub-partition)
+    // TMEM: 32 columns (C0 in columns 0-15, C1 in columns 16-31)
     if (warp == 0)
     {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 32;" ::"r"(smem_u32(&sm.tmem)) : "memory");
@@ -1623,7 +1628,7 @@ __global__ void __launch_bounds__(kTc5Threads, 4) k_blk_tc5(const BlkTask* __res
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = sm.tmem, mbar = smem_u32(&sm.mbar);
-    const uint32_t a_hi = smem_u32(sm.a_hi), a_lo = smem_u32(sm.a_lo);
+    const uint32_t a_hi = smem_u32(sm.a_hi), a_lo = smem_u32(sm.a_lo), t_hi = smem_u32(sm.t_hi), t_lo = smem_u32(sm.t_lo);
     const uint32_t v_hi = smem_u32(sm.v_hi), v_lo = smem_u32(sm.v_lo), w_hi = smem_u32(sm.w_hi), w_lo = smem_u32(sm.w_lo);
 
     // registers of the tile being loaded: 32 A values, 8 V values, 8 W values per thread
@@ -1658,10 +1663,13 @@ __global__ void __launch_bounds__(kTc5Threads, 4) k_blk_tc5(const BlkTask* __res
         {
             const int e = tid + kTc5Threads * u, r = e >> 6, c = e & 63, cc = c & 31;
             const int off = (c >> 5) * 8192 + (r >> 3) * 1024 + (r & 7) * 128 + ((((cc >> 2) ^ (r & 7)) << 4) | ((cc & 3) << 2));
+            const int offt = (c >> 5) * 8192 + (r >> 2) * 512 + (r & 3) * 128 + ((((cc >> 3) ^ (r & 3)) << 5) | ((cc & 7) << 2));
             float h, l;
             split(ra[u], h, l);
             *reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(sm.a_hi) + off) = h;
             *reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(sm.a_lo) + off) = l;
+            *reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(sm.t_hi) + offt) = h;
+            *reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(sm.t_lo) + offt) = l;
         }
 #pragma unroll
         for (int u = 0; u < 4 * NB; u++)
@@ -1696,15 +1704,20 @@ __global__ void __launch_bounds__(kTc5Threads, 4) k_blk_tc5(const BlkTask* __res
         ok = __syncthreads_and(good) != 0;
         if (!ok) return;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        uint32_t d[16];
-        asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        // lanes 0-15 of sub-partition w hold rows 16w..16w+15 of both accumulators:
+        // columns 0-15 C0 (rows of the chunk), columns 16-31 C1 (columns of the tile)
+        uint32_t d[32];
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                     "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
                      : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7]),
-                       "=r"(d[8]), "=r"(d[9]), "=r"(d[10]), "=r"(d[11]), "=r"(d[12]), "=r"(d[13]), "=r"(d[14]), "=r"(d[15])
+                       "=r"(d[8]), "=r"(d[9]), "=r"(d[10]), "=r"(d[11]), "=r"(d[12]), "=r"(d[13]), "=r"(d[14]), "=r"(d[15]),
+                       "=r"(d[16]), "=r"(d[17]), "=r"(d[18]), "=r"(d[19]), "=r"(d[20]), "=r"(d[21]), "=r"(d[22]), "=r"(d[23]),
+                       "=r"(d[24]), "=r"(d[25]), "=r"(d[26]), "=r"(d[27]), "=r"(d[28]), "=r"(d[29]), "=r"(d[30]), "=r"(d[31])
                      : "r"(tmem + ((uint32_t) (32 * warp) << 16)));
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
         const int rc = (t / ntc) * 64, c0 = (t % ntc) * 64, R = min(64, nrow - rc);
-        const int m = 16 * warp + (lane & 15);
-        if (lane >= 16)
+        const int m = 16 * warp + lane;
+        if (lane < 16)
         {
             if (do1 && c0 + m < ncol)
             {
@@ -1712,14 +1725,16 @@ __global__ void __launch_bounds__(kTc5Threads, 4) k_blk_tc5(const BlkTask* __res
 #pragma unroll
                 for (int n = 0; n < NV; n++)
                 {
-                    const double v = (double) __uint_as_float(d[n]);
+                    const double v = (double) __uint_as_float(d[16 + n]);
                     o[n] = (rc == 0) ? v : o[n] + v;
                 }
             }
-        } else if (do0 && c0 + 64 >= ncol && m < R) {
-            double* o = PS + (long long) (T.out0_row + rc + m) * NV;
+            if (do0 && c0 + 64 >= ncol && m < R)
+            {
+                double* o = PS + (long long) (T.out0_row + rc + m) * NV;
 #pragma unroll
-            for (int n = 0; n < NV; n++) o[n] = (double) __uint_as_float(d[n]);
+                for (int n = 0; n < NV; n++) o[n] = (double) __uint_as_float(d[n]);
+            }
         }
     };
 
@@ -1750,14 +1765,14 @@ __global__ void __launch_bounds__(kTc5Threads, 4) k_blk_tc5(const BlkTask* __res
             if (do1)
                 for (int j = 0; j < 8; j++)
                 {
-                    // K-step of 8 rows: one 8-row group of the swizzled tile (MN-major view:
-                    // 32-column blocks 8192 B apart, 8-row groups 1024 B apart)
+                    // K-step of 8 rows = two 4-row swizzle atoms of the MN-major copy (32-column
+                    // blocks 8192 B apart, 4-row atoms 512 B apart)
                     const uint32_t ao = j * 1024, bo = j * 2 * NB * 128;
-                    const uint64_t ah = umma_desc(a_hi + ao, 8192, 1024, 2), al = umma_desc(a_lo + ao, 8192, 1024, 2);
+                    const uint64_t ah = umma_desc(t_hi + ao, 8192, 512, 1), al = umma_desc(t_lo + ao, 8192, 512, 1);
                     const uint64_t bh = umma_desc(w_hi + bo, NB * 128, 128, 0), bl = umma_desc(w_lo + bo, NB * 128, 128, 0);
-                    umma_tf32(tmem + (16u << 16), al, bh, IDESC1, j == 0 ? 0u : 1u);
-                    umma_tf32(tmem + (16u << 16), ah, bl, IDESC1, 1u);
-                    umma_tf32(tmem + (16u << 16), ah, bh, IDESC1, 1u);
+                    umma_tf32(tmem + 16u, al, bh, IDESC1, j == 0 ? 0u : 1u);
+                    umma_tf32(tmem + 16u, ah, bl, IDESC1, 1u);
+                    umma_tf32(tmem + 16u, ah, bh, IDESC1, 1u);
                 }
             umma_commit(mbar);
         }
