@@ -22,6 +22,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <map>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -131,6 +132,12 @@ struct h2gpu_image {
     double4* d_pts64 = nullptr;   // global coordinates (x, y, z, radius)
     float4* d_pts32 = nullptr;    // coordinates relative to their node's box center
     size_t n_pts = 0;
+    // source panels of the FP32 tensor-core JIT kernel
+    PanelGroup* d_pg = nullptr;
+    int n_pg = 0, n_pg_pts = 0;   // groups; groups of point sets (the rest are skeleton sets)
+    float4* d_ppts = nullptr;     // 8 float4 per group: the points, paired as the B fragment holds them
+    TileRec* d_tiles = nullptr;   // source tiles of every JIT target chunk
+    uint4* d_pin = nullptr;       // 64 uint4 per group (NV <= 16): inputs split into TF32 hi / lo
 
     // work buffers sized for panels of width NVb
     int NVb = 0;
@@ -179,7 +186,8 @@ void free_all(h2gpu_image* im)
                     im->d_js, im->d_asm, im->d_asm_slots, im->d_fwd, im->d_bwd, im->d_U64, im->d_U32, im->d_B64,
                     im->d_B32, im->d_D64, im->d_D32, im->d_pts64, im->d_pts32, im->d_XS, im->d_PS, im->d_Y1,
                     im->d_PUSH, im->d_io, im->d_owN, im->d_owF, im->d_pp, im->d_jtN2, im->d_jtF2, im->d_y1t2,
-                    im->d_y1_slots2, im->d_asm2, im->d_asm_slots2, im->d_status};
+                    im->d_y1_slots2, im->d_asm2, im->d_asm_slots2, im->d_status, im->d_pg, im->d_ppts,
+                    im->d_pin, im->d_tiles};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (auto& e : im->ev.e)
@@ -320,6 +328,11 @@ struct HostPlan {
     std::vector<int> y1_slots2;
     std::vector<AsmTask> at2;
     std::vector<int> at_slots2;
+    // source panels: groups of the point sets first (filled after the gather), then
+    // those of the skeleton sets (filled after the upward sweep)
+    std::vector<PanelGroup> pg;
+    int pg_pts = 0;
+    std::vector<TileRec> tiles;
 };
 
 int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
@@ -523,6 +536,9 @@ int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
         }
 
         struct Src { int pt0, npt, in_row, node; };
+        // distinct source sets (point-space range), numbered in order of first use
+        std::map<std::pair<int, int>, int> set_id;
+        std::vector<Src> sets;
         auto shift = [&](int tn, int sn, JitSource& s) {
             s.sx = (float) (ctr[3 * tn] - ctr[3 * sn]);
             s.sy = (float) (ctr[3 * tn + 1] - ctr[3 * sn + 1]);
@@ -537,6 +553,9 @@ int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
                 JitSource j;
                 j.pt0 = s.pt0; j.npt = s.npt; j.in_row = s.in_row;
                 shift(tnode, s.node, j);
+                auto ins = set_id.emplace(std::make_pair(s.pt0, s.npt), (int) sets.size());
+                if (ins.second) sets.push_back(s);
+                j.grp = ins.first->second;   // set number until the panel layout is known
                 js.push_back(j);
             }
             int se = (int) js.size();
@@ -721,6 +740,46 @@ int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
             owner_work(hp.owF);
             owner_work(hp.owN);
         }
+
+        // ---- source panels: point sets first, then skeleton sets; each set padded to
+        // whole groups of 8 points
+        std::vector<int> first_grp(sets.size(), 0);
+        for (int pass = 0; pass < 2; pass++)
+        {
+            for (size_t k = 0; k < sets.size(); k++)
+            {
+                const Src& sr = sets[k];
+                if ((sr.pt0 >= d->n_point) != (pass == 1)) continue;
+                first_grp[k] = (int) hp.pg.size();
+                for (int j = 0; j < sr.npt; j += 8)
+                    hp.pg.push_back(PanelGroup{sr.pt0 + j, sr.in_row + j, std::min(8, sr.npt - j), 0});
+            }
+            if (pass == 0) hp.pg_pts = (int) hp.pg.size();
+        }
+        REQ(hp.pg.size() < (1u << 28), "too many source panel groups");
+        for (JitSource& j : js) j.grp = first_grp[j.grp];
+
+        // ---- source tiles (128 points) of every target chunk (chunks of one target set share them)
+        std::map<std::pair<int, int>, std::pair<int, int>> tile_range;
+        for (std::vector<JitTarget>* v : {&jtN, &jtF, &hp.jtN2, &hp.jtF2})
+            for (JitTarget& t : *v)
+            {
+                auto ins = tile_range.emplace(std::make_pair(t.src_beg, t.src_end), std::make_pair(0, 0));
+                if (ins.second)
+                {
+                    ins.first->second.first = (int) hp.tiles.size();
+                    for (int k = t.src_beg; k < t.src_end; k++)
+                        for (int j0 = 0; j0 < js[k].npt; j0 += 128)
+                        {
+                            const int nj = std::min(128, js[k].npt - j0);
+                            hp.tiles.push_back(TileRec{js[k].grp + j0 / 8, (nj + 7) / 8, nj, 0, js[k].sx, js[k].sy, js[k].sz, 0.f});
+                        }
+                    ins.first->second.second = (int) hp.tiles.size();
+                    REQ(hp.tiles.size() < (1u << 30), "too many source tiles");
+                }
+                t.tile_beg = ins.first->second.first;
+                t.tile_end = ins.first->second.second;
+            }
     }
 
     // ---- JIT targets, largest work first (shorter tail of the launch)
@@ -914,6 +973,18 @@ int upload_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
     TRY(upload(hp.y1_slots2, &im->d_y1_slots2, im->bytes));
     TRY(upload(hp.at2, &im->d_asm2, im->bytes));
     TRY(upload(hp.at_slots2, &im->d_asm_slots2, im->bytes));
+    TRY(upload(hp.pg, &im->d_pg, im->bytes));
+    TRY(upload(hp.tiles, &im->d_tiles, im->bytes));
+    im->n_pg = (int) hp.pg.size();
+    im->n_pg_pts = hp.pg_pts;
+    if (im->n_pg > 0 && d->krnl_dim == 1)
+    {
+        // the point half of the panels is static
+        CK(cudaMalloc(&im->d_ppts, sizeof(float4) * 8 * (size_t) im->n_pg));
+        im->bytes += sizeof(float4) * 8 * (size_t) im->n_pg;
+        CK(launch_panel_pts(im->d_pg, im->n_pg, im->d_pts32, im->d_ppts, im->stream));
+        CK(cudaStreamSynchronize(im->stream));
+    }
     if (!d->BD_JIT)
     {
         if (im->B_elems)
@@ -984,6 +1055,13 @@ KParam kparam_of(const h2gpu_image* im)
 // FP32 sweeps on the tensor cores when the image's kernel variant is a tensor-core one.
 int sweep_tc(const h2gpu_image* im) { return im->BD_JIT ? im->jit_tc : im->blk_tc; }
 
+// The tensor-core JIT kernel (FP32 scalar kernels, panels of 8 / 16) reads its sources
+// from the panels; they are refilled from XS for every panel of right-hand sides.
+bool panels_used(const h2gpu_image* im, int NV)
+{
+    return im->BD_JIT && im->kd == 1 && im->jit_tc && im->d_pin && (NV == 8 || NV == 16);
+}
+
 // One panel of NV right-hand sides: X (original order, strides x_rs, x_cs) -> Y.
 int run_panel(h2gpu_image* im, int NV, int nv, const double* X, long long x_rs, long long x_cs, double* Y,
               long long y_rs, long long y_cs, cudaStream_t s, bool timed)
@@ -997,8 +1075,9 @@ int run_panel(h2gpu_image* im, int NV, int nv, const double* X, long long x_rs, 
         if (timed) CK(cudaEventRecord(e[0], s));
         CK(launch_gather(NV, X, x_rs, x_cs, nv, im->d_fwd, im->N, im->d_XS, s));
         if (timed) CK(cudaEventRecord(e[1], s));
+        CK(launch_panel_in(NV, im->d_pg, 0, im->n_pg_pts, im->d_XS, im->d_pin, s));
         CK(launch_jit(im->kernel_id, 1, NV, im->d_jtN2, im->n_jtN2, im->d_js, im->d_pts32, kp, 1, 1, im->d_XS,
-                      im->d_PS, im->d_Y1, s));
+                      im->d_PS, im->d_Y1, s, 0, im->d_ppts, im->d_pin, im->d_tiles));
         CK(launch_pair(im->kernel_id, NV, im->d_owN, im->n_owN, im->d_pp, im->d_pts32, kp, im->d_XS, im->d_PS, s));
         if (timed) CK(cudaEventRecord(e[2], s));
         for (size_t L = 0; L + 1 < im->up_beg.size(); L++)
@@ -1008,8 +1087,9 @@ int run_panel(h2gpu_image* im, int NV, int nv, const double* X, long long x_rs, 
         }
         if (timed) CK(cudaEventRecord(e[3], s));
         CK(launch_pair(im->kernel_id, NV, im->d_owF, im->n_owF, im->d_pp, im->d_pts32, kp, im->d_XS, im->d_PS, s, 1));
+        CK(launch_panel_in(NV, im->d_pg, im->n_pg_pts, im->n_pg - im->n_pg_pts, im->d_XS, im->d_pin, s));
         CK(launch_jit(im->kernel_id, 1, NV, im->d_jtF2, im->n_jtF2, im->d_js, im->d_pts32, kp, 1, 1, im->d_XS,
-                      im->d_PS, im->d_Y1, s, 1));
+                      im->d_PS, im->d_Y1, s, 1, im->d_ppts, im->d_pin, im->d_tiles));
         CK(launch_y1sum(NV, im->d_y1t2, im->n_y12, im->d_y1_slots2, im->d_PS, im->d_Y1, s));
         if (timed) CK(cudaEventRecord(e[4], s));
         for (size_t L = 0; L + 1 < im->dn_beg.size(); L++)
@@ -1020,7 +1100,7 @@ int run_panel(h2gpu_image* im, int NV, int nv, const double* X, long long x_rs, 
         if (timed) CK(cudaEventRecord(e[5], s));
         CK(launch_asm(NV, im->d_asm2, im->n_leaf, im->d_asm_slots2, im->d_PS, im->d_fwd, Y, y_rs, y_cs, nv, s));
         if (timed) CK(cudaEventRecord(e[6], s));
-        im->st.n_launches += 7 + (long long) (im->up_beg.size() - 1) + (long long) (im->dn_beg.size() - 1);
+        im->st.n_launches += 9 + (long long) (im->up_beg.size() - 1) + (long long) (im->dn_beg.size() - 1);
         return H2GPU_OK;
     }
     if (timed) CK(cudaEventRecord(e[0], s));
@@ -1032,8 +1112,11 @@ int run_panel(h2gpu_image* im, int NV, int nv, const double* X, long long x_rs, 
         if (f32) CK(launch_blk<float>(NV, im->d_blkD, im->n_blkD, im->d_D32, im->d_XS, im->d_PS, s, im->blk_tc, im->d_status));
         else CK(launch_blk<double>(NV, im->d_blkD, im->n_blkD, im->d_D64, im->d_XS, im->d_PS, s));
     } else {
+        const bool panels = f32 && panels_used(im, NV);
+        if (panels) CK(launch_panel_in(NV, im->d_pg, 0, im->n_pg_pts, im->d_XS, im->d_pin, s));
         CK(launch_jit(im->kernel_id, f32, NV, im->d_jtN, im->n_jtN, im->d_js, f32 ? (const void*) im->d_pts32 : (const void*) im->d_pts64,
-                      kparam_of(im), f32 ? 1 : 0, im->jit_tc, im->d_XS, im->d_PS, im->d_Y1, s));
+                      kparam_of(im), f32 ? 1 : 0, im->jit_tc, im->d_XS, im->d_PS, im->d_Y1, s, 0, im->d_ppts, im->d_pin, im->d_tiles));
+        im->st.n_launches += panels ? 1 : 0;
     }
     if (timed) CK(cudaEventRecord(e[2], s));
     for (size_t L = 0; L + 1 < im->up_beg.size(); L++)
@@ -1049,8 +1132,11 @@ int run_panel(h2gpu_image* im, int NV, int nv, const double* X, long long x_rs, 
         else CK(launch_blk<double>(NV, im->d_blkB, im->n_blkB, im->d_B64, im->d_XS, im->d_PS, s));
         CK(launch_y1sum(NV, im->d_y1t, im->n_y1, im->d_y1_slots, im->d_PS, im->d_Y1, s));
     } else {
+        const bool panels = f32 && panels_used(im, NV);
+        if (panels) CK(launch_panel_in(NV, im->d_pg, im->n_pg_pts, im->n_pg - im->n_pg_pts, im->d_XS, im->d_pin, s));
         CK(launch_jit(im->kernel_id, f32, NV, im->d_jtF, im->n_jtF, im->d_js, f32 ? (const void*) im->d_pts32 : (const void*) im->d_pts64,
-                      kparam_of(im), f32 ? 1 : 0, im->jit_tc, im->d_XS, im->d_PS, im->d_Y1, s, 1));
+                      kparam_of(im), f32 ? 1 : 0, im->jit_tc, im->d_XS, im->d_PS, im->d_Y1, s, 1, im->d_ppts, im->d_pin, im->d_tiles));
+        im->st.n_launches += panels ? 1 : 0;
     }
     if (timed) CK(cudaEventRecord(e[4], s));
     for (size_t L = 0; L + 1 < im->dn_beg.size(); L++)
@@ -1090,6 +1176,12 @@ int prepare(h2gpu_image* im, int NV)
         TRY(make_f32(im, im->d_U64, &im->d_U32, im->U_elems));
         TRY(make_f32(im, im->d_B64, &im->d_B32, im->B_elems));
         TRY(make_f32(im, im->d_D64, &im->d_D32, im->D_elems));
+        if (im->d_ppts && !im->d_pin)
+        {
+            const size_t b = sizeof(uint4) * 64 * (size_t) im->n_pg;   // panels of up to 16 right-hand sides
+            CK(cudaMalloc(&im->d_pin, b));
+            im->bytes += b;
+        }
     }
     return ensure_work(im, NV);
 }

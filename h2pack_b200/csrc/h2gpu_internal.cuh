@@ -65,12 +65,36 @@ struct JitTarget {
     int out_row;       // row of the chunk's first output row (PS, or Y1 when out_y1)
     int out_y1;        // 1: outputs are the node's y1 rows
     int src_beg, src_end;
+    int tile_beg, tile_end;   // its source tiles (FP32 tensor-core path)
 };
 
 struct JitSource {
     int pt0, npt;      // point-space range of the source set
     int in_row;        // XS row of the input of the first source point
     float sx, sy, sz;  // center(target set) - center(source set), for re-centred FP32 evaluation
+    int grp;           // first 8-point group of the set in the source panels (FP32 tensor-core path)
+};
+
+// Source panels (FP32 tensor-core JIT path): every source set is cut into groups of 8
+// points, padded at its end.  Per group, the points in the pairs the m16n8k8 B fragment
+// holds them (static) and the inputs split into TF32 hi / lo in A-fragment order
+// (refilled from XS for every panel of right-hand sides).
+// One tile (up to 128 points) of a source set for a target (FP32 tensor-core JIT path):
+// the tiles of all the target's source sets in order, so the kernel walks one array.
+struct TileRec {
+    int gb;            // first panel group of the tile
+    int ng;            // groups in the tile (1..16)
+    int nj;            // points in the tile (1..128)
+    int pad0;
+    float sx, sy, sz;  // center(target set) - center(source set)
+    float pad1;
+};
+
+struct PanelGroup {
+    int pt0;           // point-space index of the group's first point
+    int row0;          // XS row of its input
+    int nvalid;        // points of the set in this group (1..8)
+    int pad;
 };
 
 // JIT pair tasks (FP32 tensor-core path): every unordered pair of point sets (a, b)

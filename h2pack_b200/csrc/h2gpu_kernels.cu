@@ -668,6 +668,34 @@ template <> struct Scalar<KRNL_MATERN32_ID, float> {
     }
 };
 
+// The FP32 kernels of two values at once with packed FP32x2 arithmetic, the same
+// operations and roundings as Scalar<K, float>::f (coincident points included).
+template <int KID> struct ScalarF2;
+template <> struct ScalarF2<KRNL_COULOMB_ID> {
+    static __device__ __forceinline__ float2 f2(float2 r2, float p0, float)
+    {
+        return make_float2(r2.x == 0.f ? p0 : rsqrt_approx(r2.x), r2.y == 0.f ? p0 : rsqrt_approx(r2.y));
+    }
+};
+template <> struct ScalarF2<KRNL_GAUSSIAN_ID> {
+    static __device__ __forceinline__ float2 f2(float2 r2, float p0, float)
+    {
+        // exp(-p0 r^2) = 2^((-p0 r^2) log2 e)
+        const float2 t = __fmul2_rn(__fmul2_rn(make_float2(-p0, -p0), r2), make_float2(kLog2e, kLog2e));
+        return make_float2(ex2_approx(t.x), ex2_approx(t.y));
+    }
+};
+template <> struct ScalarF2<KRNL_MATERN32_ID> {
+    static __device__ __forceinline__ float2 f2(float2 r2, float, float c0)
+    {
+        const float2 rs = make_float2(rsqrt_approx(fmaxf(r2.x, 1e-30f)), rsqrt_approx(fmaxf(r2.y, 1e-30f)));
+        const float2 t = __fmul2_rn(make_float2(c0, c0), __fmul2_rn(r2, rs));
+        const float2 u = __fmul2_rn(t, make_float2(kLog2e, kLog2e));
+        const float2 e = make_float2(ex2_approx(u.x), ex2_approx(u.y));
+        return __ffma2_rn(make_float2(-t.x, -t.y), e, e);
+    }
+};
+
 // FP32 kernel values for admissible (well-separated) pairs only: r2 > 0 always, so the
 // coincident-point cases drop out; constants are folded once per launch (prep).
 template <int KID> struct ScalarFar;
@@ -883,188 +911,243 @@ __device__ __forceinline__ void mma_tf32(float (&d)[4], uint32_t a0, uint32_t a1
                  : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
+// Shared-window address of a shared-memory pointer (32-bit, for PTX operands)
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t) __cvta_generic_to_shared(p); }
+
+// cp.async: 16 bytes global -> shared without registers (L2 only), in commit groups
+__device__ __forceinline__ void cp_async16(void* dst, const void* src)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// Source panels of k_jit_tc (one PanelGroup per 8 points of a source set).
+// Points: per group 8 float4, entry [t][0] = {x, x', y, y'}, [t][1] = {z, z', |p|^2, |p'|^2}
+// of the set's points 8g + t and 8g + t + 4 (t < 4): the two sources of one B-fragment
+// register pair, as FP32x2 operands.  Points past the set's end are far away (their
+// inputs are zero).
+__global__ void k_panel_pts(const PanelGroup* __restrict__ pg, int n, const float4* __restrict__ pts,
+                            float4* __restrict__ out)
+{
+    const long long e = blockIdx.x * (long long) blockDim.x + threadIdx.x;
+    if (e >= 8LL * n) return;
+    const int g = (int) (e >> 3), j = (int) (e & 7), t = j & 3, h = j >> 2;
+    const PanelGroup G = pg[g];
+    float4 q = (j < G.nvalid) ? pts[G.pt0 + j] : make_float4(1e6f, 1e6f, 1e6f, 0.f);
+    q.w = q.x * q.x + q.y * q.y + q.z * q.z;
+    float* d = reinterpret_cast<float*>(out + 8LL * g + 2 * t);
+    d[h] = q.x; d[2 + h] = q.y; d[4 + h] = q.z; d[6 + h] = q.w;
+}
+
+// Inputs: per group 2 x 32 uint4, the m16n8k8 A fragment of in^T (16 right-hand sides
+// x the group's 8 points; right-hand sides >= NV are zero) split into TF32 hi (first 32)
+// and lo (last 32): lane l (r = l/4, t = l%4) holds in[t][r], in[t][r+8], in[t+4][r],
+// in[t+4][r+8], each rounded to FP32, hi = rna(x), lo = rna(x - hi).
+template <int NV>
+__global__ void k_panel_in(const PanelGroup* __restrict__ pg, int g0, int n, const double* __restrict__ XS,
+                           uint4* __restrict__ out)
+{
+    const long long e = blockIdx.x * (long long) blockDim.x + threadIdx.x;
+    if (e >= 32LL * n) return;
+    const int g = g0 + (int) (e >> 5), ln = (int) (e & 31), r = ln >> 2, t = ln & 3;
+    const PanelGroup G = pg[g];
+    auto in = [&](int s, int c) -> float {
+        return (s < G.nvalid && c < NV) ? (float) XS[(long long) (G.row0 + s) * NV + c] : 0.f;
+    };
+    const float x[4] = {in(t, r), in(t, r + 8), in(t + 4, r), in(t + 4, r + 8)};
+    uint32_t h[4], l[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+    {
+        h[q] = tf32_rna(x[q]);
+        l[q] = tf32_rna(x[q] - __uint_as_float(h[q]));
+    }
+    out[64LL * g + ln] = make_uint4(h[0], h[1], h[2], h[3]);
+    out[64LL * g + 32 + ln] = make_uint4(l[0], l[1], l[2], l[3]);
+}
+
+// Shared memory of k_jit_tc (dynamic, 52 KB)
+struct JitTcSmem {
+    float4 pt[2][16][4][2];     // points of the tile being computed and of the next one
+    uint4 in[2][16][2][32];     // their inputs (A fragments, hi / lo)
+    double acc[8][8][32];       // FP64 sums of the FP32 segment sums, [warp][n-tile x 4 + q][lane]
+    TileRec rec[4];             // records of the next tiles
+};
+
 // Same work split as k_jit (one CTA per 128-target chunk, owner computes), with the
 // right-hand-side products on the tensor cores.  Warp w owns targets 16w..16w+15.
-// Per group of 8 staged sources each lane evaluates the 4 kernel values of its
-// m16n8k8 A fragment (targets g, g+8 x sources t, t+4; g = lane/4, t = lane%4),
-// splits them into TF32 hi/lo and issues 3 MMAs per 8-RHS n-tile against the
-// sources' inputs, which are staged in shared memory already split and in B-fragment
-// order.  FP32 accumulation per 64-source tile, FP64 sums across tiles.
+// The kernel block is the B operand of m16n8k8 (k = 8 sources x n = 8 targets) and the
+// inputs the A operand (16 right-hand sides x 8 sources), so a lane (g = lane/4,
+// t = lane%4) evaluates, per group of 8 sources and for each of its targets 16w + g and
+// 16w + 8 + g, the values against sources t and t + 4: one FP32x2 pair that is also
+// its B-fragment register pair.  Values are split into TF32 hi / lo and multiplied
+// with the inputs' hi / lo (3xTF32: lo.hi + hi.lo + hi.hi, 3 MMAs per 8 targets).
+// FP32 accumulation over 64 sources (a segment), FP64 sums across segments.
+// Sources come from the panels, already paired and split; a tile of up to 128 sources
+// (16 groups) is two contiguous copies, moved by cp.async into a shared-memory double
+// buffer while the previous tile is computed, so the CTA meets one barrier per 128
+// sources and no registers carry the next tile.
 // FAR (admissible pairs only): r^2 = |a|^2 + |b|^2 - 2 a.b with a the target in the
-// source set's frame (|a|^2 and -2a once per tile, |b|^2 staged in the point's w):
-// 4 instructions instead of 6.  Admissible boxes keep r above the box size, so the
+// source set's frame (|a|^2 and -2a once per tile, |b|^2 from the panel): 4
+// instructions per 2 values.  Admissible boxes keep r above the box size, so the
 // cancellation stays at a few FP32 ulps of r^2 (the near field keeps differences).
+// Warps whose 16 target rows are all past the end of the chunk only take part in the
+// barriers.
 template <int KID, int NV, bool FAR>
-__global__ void __launch_bounds__(256, 4) k_jit_tc(const JitTarget* __restrict__ tgts, const JitSource* __restrict__ srcs,
-                                                   const float4* __restrict__ pts, KParam kp,
-                                                   const double* __restrict__ XS, double* __restrict__ PS,
+__global__ void __launch_bounds__(256, 4) k_jit_tc(const JitTarget* __restrict__ tgts, const TileRec* __restrict__ tiles,
+                                                   const float4* __restrict__ pts, const float4* __restrict__ ppts,
+                                                   const uint4* __restrict__ pin, KParam kp, double* __restrict__ PS,
                                                    double* __restrict__ Y1)
 {
-    constexpr int NT = NV / 8;    // n-tiles of 8 right-hand sides
-    constexpr int TS = 64;        // sources per shared-memory tile
-    constexpr int NG = TS / 8;    // groups of 8 sources per tile
-    constexpr int NB = NG * NT * 32 / 256;   // B-fragment entries staged per thread and tile
-    static_assert(NB >= 1 && NB * 256 == NG * NT * 32, "staging split");
-    __shared__ float4 s_pt[2][TS];
-    __shared__ uint4 s_b[2][NG][NT][32];
-    __shared__ double s_acc[8][NT * 4][32];
+    extern __shared__ __align__(16) unsigned char jtc_raw[];
+    JitTcSmem& sm = *reinterpret_cast<JitTcSmem*>(jtc_raw);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, tq = lane & 3;
     const JitTarget tg = tgts[blockIdx.x];
+    const bool busy = warp * 16 < tg.npt;
     const float p0 = (float) kp.p0, c0 = (float) kp.c0;
     float q0 = 0.f, q1 = 0.f;
     if constexpr (FAR) ScalarFar<KID>::prep(p0, c0, q0, q1);
+    // the lane's two targets (as B-fragment columns of n-tiles 0 and 1)
     const int i0 = warp * 16 + g, i1 = i0 + 8;
-    const bool v0 = i0 < tg.npt, v1 = i1 < tg.npt;
-    const float4 x0 = pts[tg.pt0 + (v0 ? i0 : 0)], x1 = pts[tg.pt0 + (v1 ? i1 : 0)];
-    float acc[NT][4];
+    const float4 x0 = pts[tg.pt0 + (i0 < tg.npt ? i0 : 0)], x1 = pts[tg.pt0 + (i1 < tg.npt ? i1 : 0)];
+    float acc[2][4];
 #pragma unroll
-    for (int n = 0; n < NT; n++)
+    for (int n = 0; n < 2; n++)
 #pragma unroll
-        for (int q = 0; q < 4; q++) { acc[n][q] = 0.f; s_acc[warp][n * 4 + q][lane] = 0.0; }
-
-    // The tiles of all source sets form one sequence; tile k+1 is read from global
-    // memory into registers while tile k is computed from shared memory.
-    int ls = tg.src_beg, lj = 0;            // tile being loaded: source index and offset
-    float4 rp = make_float4(0.f, 0.f, 0.f, 0.f);
-    double rxa[NB], rxb[NB];
-    auto load_tile = [&](int sidx, int j0) {
-        const JitSource sc = srcs[sidx];
-        const int nj = min(TS, sc.npt - j0);
-        if (threadIdx.x < TS)
-            rp = (threadIdx.x < nj) ? pts[sc.pt0 + j0 + threadIdx.x] : make_float4(1e6f, 1e6f, 1e6f, 0.f);
+        for (int q = 0; q < 4; q++) { acc[n][q] = 0.f; sm.acc[warp][n * 4 + q][lane] = 0.0; }
+    auto flush = [&]() {
 #pragma unroll
-        for (int u = 0; u < NB; u++)
-        {
-            const int e = threadIdx.x + u * 256;
-            const int ln = e & 31, n = (e >> 5) % NT, grp = e / (32 * NT);
-            const int sa = grp * 8 + (ln & 3), sb = sa + 4, r = n * 8 + (ln >> 2);
-            rxa[u] = (sa < nj) ? XS[(long long) (sc.in_row + j0 + sa) * NV + r] : 0.0;
-            rxb[u] = (sb < nj) ? XS[(long long) (sc.in_row + j0 + sb) * NV + r] : 0.0;
-        }
+        for (int n = 0; n < 2; n++)
+#pragma unroll
+            for (int q = 0; q < 4; q++) { sm.acc[warp][n * 4 + q][lane] += (double) acc[n][q]; acc[n][q] = 0.f; }
     };
-    auto store_tile = [&](int buf) {
-        if (threadIdx.x < TS)
-        {
-            float4 q = rp;
-            if (FAR) q.w = q.x * q.x + q.y * q.y + q.z * q.z;
-            s_pt[buf][threadIdx.x] = q;
-        }
-#pragma unroll
-        for (int u = 0; u < NB; u++)
-        {
-            const int e = threadIdx.x + u * 256;
-            const int ln = e & 31, n = (e >> 5) % NT, grp = e / (32 * NT);
-            const float xa = (float) rxa[u], xb = (float) rxb[u];
-            const uint32_t ha = tf32_rna(xa), hb = tf32_rna(xb);
-            s_b[buf][grp][n][ln] = make_uint4(ha, hb, tf32_rna(xa - __uint_as_float(ha)), tf32_rna(xb - __uint_as_float(hb)));
-        }
-    };
-    auto advance = [&](int& sidx, int& j0) {
-        j0 += TS;
-        if (j0 >= srcs[sidx].npt) { sidx++; j0 = 0; }
+    // one group: the lane's 2 x 2 values (targets i0, i1 x sources t, t+4) as B-fragment
+    // pairs k0, k1, against the group's inputs
+    auto mma_group = [&](float2 k0, float2 k1, int buf, int grp) {
+        const uint4 ah = sm.in[buf][grp][0][lane], al = sm.in[buf][grp][1][lane];
+        const float2 m1 = make_float2(-1.f, -1.f);
+        const uint32_t h00 = tf32_rna(k0.x), h01 = tf32_rna(k0.y), h10 = tf32_rna(k1.x), h11 = tf32_rna(k1.y);
+        const float2 l0 = __ffma2_rn(make_float2(__uint_as_float(h00), __uint_as_float(h01)), m1, k0);
+        const float2 l1 = __ffma2_rn(make_float2(__uint_as_float(h10), __uint_as_float(h11)), m1, k1);
+        mma_tf32(acc[0], ah.x, ah.y, ah.z, ah.w, __float_as_uint(l0.x), __float_as_uint(l0.y));
+        mma_tf32(acc[1], ah.x, ah.y, ah.z, ah.w, __float_as_uint(l1.x), __float_as_uint(l1.y));
+        mma_tf32(acc[0], al.x, al.y, al.z, al.w, h00, h01);
+        mma_tf32(acc[1], al.x, al.y, al.z, al.w, h10, h11);
+        mma_tf32(acc[0], ah.x, ah.y, ah.z, ah.w, h00, h01);
+        mma_tf32(acc[1], ah.x, ah.y, ah.z, ah.w, h10, h11);
     };
 
-    if (ls < tg.src_end)
-    {
-        load_tile(ls, lj);
-        store_tile(0);
-    }
+    // Pipeline over the chunk's tiles k = 0 .. nt-1: tile k is computed from buffer
+    // k & 1 while tile k+1 sits in the other buffer; after the tile's barrier tile k+2
+    // is copied into buffer k & 1, and the record of tile k+4 into ring slot k & 3.
+    const TileRec* rec = tiles + tg.tile_beg;
+    const int nt = tg.tile_end - tg.tile_beg;
+    auto issue_rec = [&](int k) {   // threads 0, 1: the two 16-byte halves
+        if (threadIdx.x < 2 && k < nt)
+            cp_async16(reinterpret_cast<uint4*>(&sm.rec[k & 3]) + threadIdx.x, reinterpret_cast<const uint4*>(rec + k) + threadIdx.x);
+    };
+    auto issue = [&](int k, int buf) {
+        if (k >= nt) return;
+        const int gb = sm.rec[k & 3].gb, ng = sm.rec[k & 3].ng;
+        const float4* gp = ppts + 8LL * gb;
+        const uint4* gi = pin + 64LL * gb;
+        const int np = ng * 8, nall = np + ng * 64;
+        for (int c = threadIdx.x; c < nall; c += 256)
+        {
+            if (c < np) cp_async16(&sm.pt[buf][0][0][0] + c, gp + c);
+            else cp_async16(&sm.in[buf][0][0][0] + (c - np), gi + (c - np));
+        }
+    };
+    issue_rec(0); issue_rec(1); issue_rec(2); issue_rec(3);
+    cp_async_commit();
+    cp_async_wait_all();
     __syncthreads();
-    int cs = ls, cj = lj, buf = 0;           // tile being computed
-    if (ls < tg.src_end) advance(ls, lj);
-    while (cs < tg.src_end)
+    issue(0, 0); issue(1, 1);
+    cp_async_commit();
+    cp_async_wait_all();
+    __syncthreads();
+    for (int k = 0; k < nt; k++)
     {
-        const bool more = ls < tg.src_end;
-        if (more) load_tile(ls, lj);
+        const int buf = k & 1;
+        if (busy)
         {
-            const JitSource sc = srcs[cs];
-            const int nj = min(TS, sc.npt - cj);
-            const float ax = x0.x + sc.sx, ay = x0.y + sc.sy, az = x0.z + sc.sz;
-            const float bx = x1.x + sc.sx, by = x1.y + sc.sy, bz = x1.z + sc.sz;
-            // far form: -2a and |a|^2 of both target rows in the source set's frame, as
-            // (row g, row g+8) pairs for packed FP32x2 arithmetic
-            const float2 m_x = make_float2(-2.f * ax, -2.f * bx), m_y = make_float2(-2.f * ay, -2.f * by),
-                         m_z = make_float2(-2.f * az, -2.f * bz);
-            const float2 s2 = make_float2(ax * ax + ay * ay + az * az, bx * bx + by * by + bz * bz);
-            const int ngrp = (nj + 7) >> 3;
-#pragma unroll 2
-            for (int grp = 0; grp < ngrp; grp++)
+            const TileRec r = sm.rec[k & 3];
+            const float ax = x0.x + r.sx, ay = x0.y + r.sy, az = x0.z + r.sz;
+            const float bx = x1.x + r.sx, by = x1.y + r.sy, bz = x1.z + r.sz;
+            // segments of 8 groups (64 sources) summed in FP32
+            for (int h = 0; h < r.ng; h += 8)
             {
-                const float4 pa = s_pt[buf][grp * 8 + tq], pb = s_pt[buf][grp * 8 + tq + 4];
-                float k[4];
+                const int ge = min(r.ng, h + 8);
                 if constexpr (FAR)
                 {
-                    // r^2 of rows (g, g+8) against one source point: 4 packed instructions
-                    // for two values.  No clamp: admissible pairs keep r^2 far from 0.
-                    auto r2p = [&](const float4& p) {
-                        float2 t = __fadd2_rn(s2, make_float2(p.w, p.w));
-                        t = __ffma2_rn(m_z, make_float2(p.z, p.z), t);
-                        t = __ffma2_rn(m_y, make_float2(p.y, p.y), t);
-                        return __ffma2_rn(m_x, make_float2(p.x, p.x), t);
-                    };
-                    const float2 ka = ScalarFar<KID>::f2(r2p(pa), q0, q1);   // (g, t), (g+8, t)
-                    const float2 kb = ScalarFar<KID>::f2(r2p(pb), q0, q1);   // (g, t+4), (g+8, t+4)
-                    k[0] = ka.x; k[1] = ka.y; k[2] = kb.x; k[3] = kb.y;
+                    // -2a and |a|^2 of each target in the source set's frame, broadcast
+                    const float2 max2 = make_float2(-2.f * ax, -2.f * ax), may2 = make_float2(-2.f * ay, -2.f * ay),
+                                 maz2 = make_float2(-2.f * az, -2.f * az);
+                    const float2 mbx2 = make_float2(-2.f * bx, -2.f * bx), mby2 = make_float2(-2.f * by, -2.f * by),
+                                 mbz2 = make_float2(-2.f * bz, -2.f * bz);
+                    const float sa2 = ax * ax + ay * ay + az * az, sb2 = bx * bx + by * by + bz * bz;
+                    const float2 sa22 = make_float2(sa2, sa2), sb22 = make_float2(sb2, sb2);
+#pragma unroll 2
+                    for (int grp = h; grp < ge; grp++)
+                    {
+                        const float4 P0 = sm.pt[buf][grp][tq][0], P1 = sm.pt[buf][grp][tq][1];
+                        const float2 px = make_float2(P0.x, P0.y), py = make_float2(P0.z, P0.w);
+                        const float2 pz = make_float2(P1.x, P1.y), pw = make_float2(P1.z, P1.w);
+                        // r^2 of one target against the source pair: 4 packed instructions
+                        // for two values.  No clamp: admissible pairs keep r^2 far from 0.
+                        auto r2p = [&](float2 s, float2 mx, float2 my, float2 mz) {
+                            float2 t = __fadd2_rn(s, pw);
+                            t = __ffma2_rn(mz, pz, t);
+                            t = __ffma2_rn(my, py, t);
+                            return __ffma2_rn(mx, px, t);
+                        };
+                        const float2 k0 = ScalarFar<KID>::f2(r2p(sa22, max2, may2, maz2), q0, q1);
+                        const float2 k1 = ScalarFar<KID>::f2(r2p(sb22, mbx2, mby2, mbz2), q0, q1);
+                        mma_group(k0, k1, buf, grp);
+                    }
                 } else {
-                    // differences of rows (g, g+8) to one source point, packed in pairs
-                    auto r2d = [&](const float4& p) {
-                        const float2 dx = __fadd2_rn(make_float2(ax, bx), make_float2(-p.x, -p.x));
-                        const float2 dy = __fadd2_rn(make_float2(ay, by), make_float2(-p.y, -p.y));
-                        const float2 dz = __fadd2_rn(make_float2(az, bz), make_float2(-p.z, -p.z));
-                        return __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
-                    };
-                    const float2 ra2 = r2d(pa), rb2 = r2d(pb);
-                    k[0] = Scalar<KID, float>::f(ra2.x, p0, c0);   // (g,   t)
-                    k[1] = Scalar<KID, float>::f(ra2.y, p0, c0);   // (g+8, t)
-                    k[2] = Scalar<KID, float>::f(rb2.x, p0, c0);   // (g,   t+4)
-                    k[3] = Scalar<KID, float>::f(rb2.y, p0, c0);   // (g+8, t+4)
+                    const float2 ax2 = make_float2(ax, ax), ay2 = make_float2(ay, ay), az2 = make_float2(az, az);
+                    const float2 bx2 = make_float2(bx, bx), by2 = make_float2(by, by), bz2 = make_float2(bz, bz);
+#pragma unroll 1
+                    for (int grp = h; grp < ge; grp++)
+                    {
+                        const float4 P0 = sm.pt[buf][grp][tq][0], P1 = sm.pt[buf][grp][tq][1];
+                        const float2 px = make_float2(-P0.x, -P0.y), py = make_float2(-P0.z, -P0.w);
+                        const float2 pz = make_float2(-P1.x, -P1.y);
+                        // differences of one target to the source pair, packed
+                        auto r2d = [&](float2 x, float2 y, float2 z) {
+                            const float2 dx = __fadd2_rn(x, px), dy = __fadd2_rn(y, py), dz = __fadd2_rn(z, pz);
+                            return __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+                        };
+                        const float2 k0 = ScalarF2<KID>::f2(r2d(ax2, ay2, az2), p0, c0);
+                        const float2 k1 = ScalarF2<KID>::f2(r2d(bx2, by2, bz2), p0, c0);
+                        mma_group(k0, k1, buf, grp);
+                    }
                 }
-                // hi rounded to TF32; the remainder k - hi (exact in FP32, one packed FMA per
-                // pair) is handed over as is: the MMA reads its TF32 bits (error < 2^-22 of
-                // the kernel value)
-                uint32_t hi[4], lo[4];
-#pragma unroll
-                for (int q = 0; q < 4; q++) hi[q] = tf32_rna(k[q]);
-#pragma unroll
-                for (int q = 0; q < 4; q += 2)
-                {
-                    const float2 l = __ffma2_rn(make_float2(__uint_as_float(hi[q]), __uint_as_float(hi[q + 1])),
-                                                make_float2(-1.f, -1.f), make_float2(k[q], k[q + 1]));
-                    lo[q] = __float_as_uint(l.x);
-                    lo[q + 1] = __float_as_uint(l.y);
-                }
-                uint4 b[NT];
-#pragma unroll
-                for (int n = 0; n < NT; n++) b[n] = s_b[buf][grp][n][lane];
-                // the NT accumulator chains interleaved: consecutive MMAs are independent
-#pragma unroll
-                for (int n = 0; n < NT; n++) mma_tf32(acc[n], lo[0], lo[1], lo[2], lo[3], b[n].x, b[n].y);
-#pragma unroll
-                for (int n = 0; n < NT; n++) mma_tf32(acc[n], hi[0], hi[1], hi[2], hi[3], b[n].z, b[n].w);
-#pragma unroll
-                for (int n = 0; n < NT; n++) mma_tf32(acc[n], hi[0], hi[1], hi[2], hi[3], b[n].x, b[n].y);
+                flush();
             }
-#pragma unroll
-            for (int n = 0; n < NT; n++)
-#pragma unroll
-                for (int q = 0; q < 4; q++) { s_acc[warp][n * 4 + q][lane] += (double) acc[n][q]; acc[n][q] = 0.f; }
         }
-        if (more) store_tile(buf ^ 1);
-        __syncthreads();
-        cs = ls; cj = lj; buf ^= 1;
-        if (more) advance(ls, lj);
+        cp_async_wait_all();                     // tile k+1 and record k+3 have landed (this thread's copies)
+        __syncthreads();                         // ... everyone's, and tile k / record k are no longer read
+        issue(k + 2, buf);
+        issue_rec(k + 4);
+        cp_async_commit();
     }
+    // accumulator (n, q) of lane (g, t): right-hand side g + 8 (q >> 1), target
+    // 16w + 8n + 2t + (q & 1)
     double* base = (tg.out_y1 ? Y1 : PS) + (long long) tg.out_row * NV;
 #pragma unroll
-    for (int n = 0; n < NT; n++)
+    for (int n = 0; n < 2; n++)
 #pragma unroll
         for (int q = 0; q < 4; q++)
         {
-            const int row = (q < 2) ? i0 : i1;
-            const bool ok = (q < 2) ? v0 : v1;
-            if (ok) base[(long long) row * NV + n * 8 + 2 * tq + (q & 1)] = s_acc[warp][n * 4 + q][lane];
+            const int row = warp * 16 + 8 * n + 2 * tq + (q & 1), rhs = g + 8 * (q >> 1);
+            if (row < tg.npt && rhs < NV) base[(long long) row * NV + rhs] = sm.acc[warp][n * 4 + q][lane];
         }
 }
+
+constexpr int jit_tc_smem_bytes() { return (int) sizeof(JitTcSmem); }
 
 // ---------------------------------------- JIT pair kernel (both directions at once)
 
@@ -1525,7 +1608,6 @@ __global__ void __launch_bounds__(256, 4) k_blk_tc(const BlkTask* __restrict__ t
 // ------------------------------------ stored blocks on tcgen05 (TMEM accumulators)
 
 // PTX wrappers (sm_100a).  Shared addresses are 32-bit shared-window addresses.
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t) __cvta_generic_to_shared(p); }
 
 // Shared-memory matrix descriptor: start address, leading / stride byte offsets (16-byte
 // units), version 1, layout type (0 = no swizzle, 2 = 128-byte swizzle).
@@ -1577,8 +1659,10 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t mbar, uint32_t parity)
 // operands need, for C1.  One thread issues the 48 MMAs
 // of a tile and commits them to an mbarrier; meanwhile all threads load the next tile
 // from global memory into registers.  C1 of each tile is read from TMEM and added into
-// the task's single C1 slot (stored by the first 64-row chunk); C0 accumulates over a
-// chunk's column tiles in TMEM and is written when the chunk ends.  Every wait on the
+// the task's single C1 slot (stored by the first 64-row chunk); C0 of each tile is read
+// from TMEM too and summed over the chunk's column tiles in FP64 registers (FP32 sums
+// per 64-column tile, FP64 across tiles, like the mma.sync kernels), then written when
+// the chunk ends.  Every wait on the
 // mbarrier is bounded: on expiry the kernel records a status and stops issuing work.
 struct Tc5Smem {
     float a_hi[2 * 64 * 32];   // K-major view: two column blocks (32 columns) x 64 rows, 128 B rows, 128-byte swizzle
@@ -1596,7 +1680,7 @@ struct Tc5Smem {
 constexpr int kTc5Threads = 128;
 
 template <int NV>
-__global__ void __launch_bounds__(kTc5Threads, 4) k_blk_tc5(const BlkTask* __restrict__ tasks,
+__global__ void __launch_bounds__(kTc5Threads, 2) k_blk_tc5(const BlkTask* __restrict__ tasks,
                                                             const float* __restrict__ arena,
                                                             const double* __restrict__ XS, double* __restrict__ PS,
                                                             int* __restrict__ status)
@@ -1689,7 +1773,11 @@ __global__ void __launch_bounds__(kTc5Threads, 4) k_blk_tc5(const BlkTask* __res
 
     bool ok = true;
     uint32_t phase = 0;
-    // read back the tile just multiplied: C1 into its slot, C0 at the end of a chunk.
+    double c0acc[NV];   // lanes 0-15: the chunk's C0 row 16 warp + lane
+#pragma unroll
+    for (int n = 0; n < NV; n++) c0acc[n] = 0.0;
+    // read back the tile just multiplied: C1 into its slot, C0 into the chunk's FP64 sums
+    // (written at the end of a chunk).
     // Thread 0 waits (bounded) for the MMAs' commit; the outcome is made uniform.
     auto drain = [&](int t) {
         int good = 1;
@@ -1729,11 +1817,21 @@ __global__ void __launch_bounds__(kTc5Threads, 4) k_blk_tc5(const BlkTask* __res
                     o[n] = (rc == 0) ? v : o[n] + v;
                 }
             }
-            if (do0 && c0 + 64 >= ncol && m < R)
+            if (do0)
             {
-                double* o = PS + (long long) (T.out0_row + rc + m) * NV;
 #pragma unroll
-                for (int n = 0; n < NV; n++) o[n] = (double) __uint_as_float(d[n]);
+                for (int n = 0; n < NV; n++) c0acc[n] += (double) __uint_as_float(d[n]);
+                if (c0 + 64 >= ncol)
+                {
+                    if (m < R)
+                    {
+                        double* o = PS + (long long) (T.out0_row + rc + m) * NV;
+#pragma unroll
+                        for (int n = 0; n < NV; n++) o[n] = c0acc[n];
+                    }
+#pragma unroll
+                    for (int n = 0; n < NV; n++) c0acc[n] = 0.0;
+                }
             }
         }
     };
@@ -1750,7 +1848,6 @@ __global__ void __launch_bounds__(kTc5Threads, 4) k_blk_tc5(const BlkTask* __res
         if (tid == 0)
         {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const bool chunk_start = (t % ntc) == 0;
             if (do0)
                 for (int j = 0; j < 8; j++)
                 {
@@ -1758,7 +1855,7 @@ __global__ void __launch_bounds__(kTc5Threads, 4) k_blk_tc5(const BlkTask* __res
                     const uint32_t ao = (j >> 2) * 8192 + (j & 3) * 32, bo = j * 2 * NB * 128;
                     const uint64_t ah = umma_desc(a_hi + ao, 16, 1024, 2), al = umma_desc(a_lo + ao, 16, 1024, 2);
                     const uint64_t bh = umma_desc(v_hi + bo, NB * 128, 128, 0), bl = umma_desc(v_lo + bo, NB * 128, 128, 0);
-                    umma_tf32(tmem, al, bh, IDESC0, (chunk_start && j == 0) ? 0u : 1u);
+                    umma_tf32(tmem, al, bh, IDESC0, j == 0 ? 0u : 1u);
                     umma_tf32(tmem, ah, bl, IDESC0, 1u);
                     umma_tf32(tmem, ah, bh, IDESC0, 1u);
                 }
@@ -2132,7 +2229,7 @@ cudaError_t launch_asm(int NV, const AsmTask* t, int n, const int* slots, const 
 template <int KID, typename T, int KD>
 static cudaError_t launch_jit_k(int NV, const JitTarget* tg, int n, const JitSource* sr, const void* pts, KParam kp,
                                 int use_shift, int use_tc, const double* XS, double* PS, double* Y1, cudaStream_t st,
-                                int far)
+                                int far, const float4* ppts, const uint4* pin, const TileRec* tiles)
 {
     using T4 = typename Vec4<T>::t;
     const T4* p = (const T4*) pts;
@@ -2142,11 +2239,22 @@ static cudaError_t launch_jit_k(int NV, const JitTarget* tg, int n, const JitSou
     {
         if (use_tc && (NV == 16 || NV == 8) && use_shift)
         {
+            // the tensor-core kernel reads the source panels and tile lists
+            if (!ppts || !pin || !tiles) return cudaErrorInvalidValue;
             const float4* p4 = (const float4*) pts;
-            if (NV == 16 && far) k_jit_tc<KID, 16, true><<<n, 256, 0, st>>>(tg, sr, p4, kp, XS, PS, Y1);
-            else if (NV == 16) k_jit_tc<KID, 16, false><<<n, 256, 0, st>>>(tg, sr, p4, kp, XS, PS, Y1);
-            else if (far) k_jit_tc<KID, 8, true><<<n, 256, 0, st>>>(tg, sr, p4, kp, XS, PS, Y1);
-            else k_jit_tc<KID, 8, false><<<n, 256, 0, st>>>(tg, sr, p4, kp, XS, PS, Y1);
+            constexpr int b = jit_tc_smem_bytes();
+            // the dynamic shared-memory opt-in, once per kernel (a function attribute, not a
+            // stream operation: legal inside a stream capture too)
+            static const cudaError_t opt_in = [] {
+                cudaError_t e = allow_smem(k_jit_tc<KID, 16, true>, b);
+                if (e == cudaSuccess) e = allow_smem(k_jit_tc<KID, 16, false>, b);
+                if (e == cudaSuccess) e = allow_smem(k_jit_tc<KID, 8, true>, b);
+                if (e == cudaSuccess) e = allow_smem(k_jit_tc<KID, 8, false>, b);
+                return e;
+            }();
+            if (opt_in != cudaSuccess) return opt_in;
+            if (NV == 16) (far ? k_jit_tc<KID, 16, true> : k_jit_tc<KID, 16, false>)<<<n, 256, b, st>>>(tg, tiles, p4, ppts, pin, kp, PS, Y1);
+            else (far ? k_jit_tc<KID, 8, true> : k_jit_tc<KID, 8, false>)<<<n, 256, b, st>>>(tg, tiles, p4, ppts, pin, kp, PS, Y1);
             return cudaGetLastError();
         }
     }
@@ -2164,21 +2272,40 @@ static cudaError_t launch_jit_k(int NV, const JitTarget* tg, int n, const JitSou
 
 cudaError_t launch_jit(int kid, int fp32, int NV, const JitTarget* tg, int n, const JitSource* sr, const void* pts,
                        KParam kp, int use_shift, int use_tc, const double* XS, double* PS, double* Y1, cudaStream_t st,
-                       int far)
+                       int far, const float4* ppts, const uint4* pin, const TileRec* tiles)
 {
     if (n <= 0) return cudaSuccess;
+#define H2G_JIT_ARGS NV, tg, n, sr, pts, kp, use_shift, use_tc, XS, PS, Y1, st, far, ppts, pin, tiles
     switch (kid)
     {
-        case KRNL_COULOMB_ID:  return fp32 ? launch_jit_k<KRNL_COULOMB_ID, float, 1>(NV, tg, n, sr, pts, kp, use_shift, use_tc, XS, PS, Y1, st, far)
-                                           : launch_jit_k<KRNL_COULOMB_ID, double, 1>(NV, tg, n, sr, pts, kp, use_shift, use_tc, XS, PS, Y1, st, far);
-        case KRNL_GAUSSIAN_ID: return fp32 ? launch_jit_k<KRNL_GAUSSIAN_ID, float, 1>(NV, tg, n, sr, pts, kp, use_shift, use_tc, XS, PS, Y1, st, far)
-                                           : launch_jit_k<KRNL_GAUSSIAN_ID, double, 1>(NV, tg, n, sr, pts, kp, use_shift, use_tc, XS, PS, Y1, st, far);
-        case KRNL_MATERN32_ID: return fp32 ? launch_jit_k<KRNL_MATERN32_ID, float, 1>(NV, tg, n, sr, pts, kp, use_shift, use_tc, XS, PS, Y1, st, far)
-                                           : launch_jit_k<KRNL_MATERN32_ID, double, 1>(NV, tg, n, sr, pts, kp, use_shift, use_tc, XS, PS, Y1, st, far);
-        case KRNL_RPY_ID:      return fp32 ? launch_jit_k<KRNL_RPY_ID, float, 3>(NV, tg, n, sr, pts, kp, use_shift, use_tc, XS, PS, Y1, st, far)
-                                           : launch_jit_k<KRNL_RPY_ID, double, 3>(NV, tg, n, sr, pts, kp, use_shift, use_tc, XS, PS, Y1, st, far);
+        case KRNL_COULOMB_ID:  return fp32 ? launch_jit_k<KRNL_COULOMB_ID, float, 1>(H2G_JIT_ARGS)
+                                           : launch_jit_k<KRNL_COULOMB_ID, double, 1>(H2G_JIT_ARGS);
+        case KRNL_GAUSSIAN_ID: return fp32 ? launch_jit_k<KRNL_GAUSSIAN_ID, float, 1>(H2G_JIT_ARGS)
+                                           : launch_jit_k<KRNL_GAUSSIAN_ID, double, 1>(H2G_JIT_ARGS);
+        case KRNL_MATERN32_ID: return fp32 ? launch_jit_k<KRNL_MATERN32_ID, float, 1>(H2G_JIT_ARGS)
+                                           : launch_jit_k<KRNL_MATERN32_ID, double, 1>(H2G_JIT_ARGS);
+        case KRNL_RPY_ID:      return fp32 ? launch_jit_k<KRNL_RPY_ID, float, 3>(H2G_JIT_ARGS)
+                                           : launch_jit_k<KRNL_RPY_ID, double, 3>(H2G_JIT_ARGS);
         default: return cudaErrorInvalidValue;
     }
+#undef H2G_JIT_ARGS
+}
+
+cudaError_t launch_panel_pts(const PanelGroup* pg, int n, const float4* pts, float4* ppts, cudaStream_t st)
+{
+    if (n <= 0) return cudaSuccess;
+    const long long t = 8LL * n;
+    k_panel_pts<<<(unsigned) ((t + 255) / 256), 256, 0, st>>>(pg, n, pts, ppts);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_panel_in(int NV, const PanelGroup* pg, int g0, int n, const double* XS, uint4* pin, cudaStream_t st)
+{
+    if (n <= 0 || !pin || (NV != 8 && NV != 16)) return cudaSuccess;
+    const long long t = 32LL * n;
+    if (NV == 16) k_panel_in<16><<<(unsigned) ((t + 255) / 256), 256, 0, st>>>(pg, g0, n, XS, pin);
+    else k_panel_in<8><<<(unsigned) ((t + 255) / 256), 256, 0, st>>>(pg, g0, n, XS, pin);
+    return cudaGetLastError();
 }
 
 template <int KID, bool FAR>

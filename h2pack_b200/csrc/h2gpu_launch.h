@@ -24,9 +24,17 @@ cudaError_t launch_down(int NV, const DownTask* t, int n, const TA* U, const dou
 cudaError_t launch_y1sum(int NV, const Y1Task* t, int n, const int* slots, const double* PS, double* Y1, cudaStream_t st);
 cudaError_t launch_asm(int NV, const AsmTask* t, int n, const int* slots, const double* PS, const int* fwd,
                        double* Y, long long y_rs, long long y_cs, int nv, cudaStream_t st);
+// far: every source set is admissible for its target (r > 0); ppts / pin / tiles: the
+// source panels and tile lists, which the tensor-core kernel (FP32 scalar kernels,
+// NV 8 / 16, use_tc) reads
 cudaError_t launch_jit(int kid, int fp32, int NV, const JitTarget* tg, int n, const JitSource* sr, const void* pts,
                        KParam kp, int use_shift, int use_tc, const double* XS, double* PS, double* Y1, cudaStream_t st,
-                       int far = 0);   // far: every source set is admissible for its target (r > 0)
+                       int far = 0, const float4* ppts = nullptr, const uint4* pin = nullptr,
+                       const TileRec* tiles = nullptr);
+// source panels: the points (once per image) and the inputs of groups [g0, g0 + n) for a
+// panel of NV right-hand sides (NV 8 / 16; other widths do nothing)
+cudaError_t launch_panel_pts(const PanelGroup* pg, int n, const float4* pts, float4* ppts, cudaStream_t st);
+cudaError_t launch_panel_in(int NV, const PanelGroup* pg, int g0, int n, const double* XS, uint4* pin, cudaStream_t st);
 cudaError_t launch_pair(int kid, int NV, const PairOwner* ow, int n, const PairPartner* pp, const void* pts, KParam kp,
                         const double* XS, double* PS, cudaStream_t st,
                         int far = 0);
