@@ -172,6 +172,7 @@ struct h2gpu_image {
     int jit_pair = 0;        // with jit_tc: the pair kernel (each unordered pair once)
     int blk_tc = 1;          // stored-block kernel for FP32 panels of 8 / 16: 1 mma.sync, 2 tcgen05, 0 CUDA cores
     int* d_status = nullptr; // device status word (bounded waits of the tcgen05 kernel)
+    int* h_status = nullptr; // pinned host copy, read back at the end of every timed panel
     int tuned_nv = 0;        // panel width chosen by the autotuner (0: default rule)
     int n_images = 1;        // matrices in this image (batched images hold several)
     cudaGraph_t graph = nullptr;
@@ -190,6 +191,7 @@ void free_all(h2gpu_image* im)
                     im->d_pin, im->d_tiles};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    if (im->h_status) cudaFreeHost(im->h_status);
     for (auto& e : im->ev.e)
         if (e) cudaEventDestroy(e);
     if (im->graph_exec) cudaGraphExecDestroy(im->graph_exec);
@@ -1052,6 +1054,13 @@ KParam kparam_of(const h2gpu_image* im)
     return k;
 }
 
+// The tcgen05 stored-block kernel (mixed precision, normal mode) reports through the
+// status word.
+bool uses_status(const h2gpu_image* im)
+{
+    return im->d_status && im->h_status && im->blk_tc == 2 && !im->BD_JIT && im->precision == H2GPU_PREC_MIXED;
+}
+
 // FP32 sweeps on the tensor cores when the image's kernel variant is a tensor-core one.
 int sweep_tc(const h2gpu_image* im) { return im->BD_JIT ? im->jit_tc : im->blk_tc; }
 
@@ -1147,6 +1156,8 @@ int run_panel(h2gpu_image* im, int NV, int nv, const double* X, long long x_rs, 
     }
     if (timed) CK(cudaEventRecord(e[5], s));
     CK(launch_asm(NV, im->d_asm, im->n_asm, im->d_asm_slots, im->d_PS, im->d_fwd, Y, y_rs, y_cs, nv, s));
+    if (timed && uses_status(im))
+        CK(cudaMemcpyAsync(im->h_status, im->d_status, sizeof(int), cudaMemcpyDeviceToHost, s));
     if (timed) CK(cudaEventRecord(e[6], s));
     im->st.n_launches += 4 + (long long) (im->up_beg.size() - 1) + (long long) (im->dn_beg.size() - 1)
                          + (im->BD_JIT ? 0 : 1);
@@ -1154,14 +1165,14 @@ int run_panel(h2gpu_image* im, int NV, int nv, const double* X, long long x_rs, 
 }
 
 // Bounded waits inside the tcgen05 block kernel set the image's status word when they
-// expire; a synchronised apply reports it (and clears it) as H2GPU_ERR_DEVICE.
+// expire; a timed panel copies it back (pinned) before its last event, and a
+// synchronised apply reports it (and clears it) as H2GPU_ERR_DEVICE.
 int check_status(h2gpu_image* im)
 {
-    if (!im->d_status || im->blk_tc != 2 || im->BD_JIT || im->precision != H2GPU_PREC_MIXED) return H2GPU_OK;
-    int st = 0;
-    CK(cudaMemcpy(&st, im->d_status, sizeof(int), cudaMemcpyDeviceToHost));
-    if (st != 0)
+    if (!uses_status(im)) return H2GPU_OK;
+    if (*(volatile int*) im->h_status != 0)
     {
+        *im->h_status = 0;
         CK(cudaMemset(im->d_status, 0, sizeof(int)));
         return fail(H2GPU_ERR_DEVICE, "tcgen05 block kernel: a bounded wait on the MMA completion expired");
     }
@@ -1299,8 +1310,10 @@ H2G_API int h2gpu_image_create(const h2gpu_desc* desc, const h2gpu_options* opt,
         if (st != H2GPU_OK) break;
         st = upload_plan(im, desc, hp);
         if (st == H2GPU_OK && (cudaMalloc(&im->d_status, sizeof(int)) != cudaSuccess ||
-                               cudaMemset(im->d_status, 0, sizeof(int)) != cudaSuccess))
+                               cudaMemset(im->d_status, 0, sizeof(int)) != cudaSuccess ||
+                               cudaHostAlloc(&im->h_status, sizeof(int), cudaHostAllocDefault) != cudaSuccess))
             st = fail(H2GPU_ERR_NOMEM, "status word allocation failed");
+        if (st == H2GPU_OK) *im->h_status = 0;
     } while (0);
     if (st != H2GPU_OK)
     {

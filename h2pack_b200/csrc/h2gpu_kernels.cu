@@ -389,6 +389,10 @@ __global__ void __launch_bounds__(256, 3) k_blk1(const BlkTask* __restrict__ tas
         for (int cw = 0; cw < ncol; cw += CW)
         {
             const int cend = min(ncol, cw + CW);
+            // the out1 value this thread adds to after the window, read now so its latency
+            // hides behind the window's loads (one column per thread: CW = blockDim)
+            double o1 = 0.0;
+            if (do1 && rc > 0 && threadIdx.x < cend - cw) o1 = PS[T.out1_row + cw + threadIdx.x];
             for (int cs = cw; cs < cend; cs += 32 * CPL)
             {
                 int c[CPL];
@@ -443,13 +447,13 @@ __global__ void __launch_bounds__(256, 3) k_blk1(const BlkTask* __restrict__ tas
             if (do1)
             {
                 __syncthreads();
-                for (int t = threadIdx.x; t < cend - cw; t += 256)
+                const int t = threadIdx.x;
+                if (t < cend - cw)
                 {
                     double sum = 0.0;
 #pragma unroll
                     for (int k = 0; k < kWarps; k++) sum += s_q[k][t];
-                    double* o = PS + T.out1_row + cw + t;
-                    *o = (rc == 0) ? sum : *o + sum;
+                    PS[T.out1_row + cw + t] = (rc == 0) ? sum : o1 + sum;
                 }
                 __syncthreads();
             }
@@ -1887,6 +1891,7 @@ __global__ void __launch_bounds__(kTc5Threads, 2) k_blk_tc5(const BlkTask* __res
 
 template <int NV>
 constexpr int tc5_smem_bytes() { return (int) sizeof(Tc5Smem) + 1024; }
+
 
 // ---------------------------------------------- sweeps on the tensor cores (FP32 U)
 
