@@ -1449,7 +1449,8 @@ __global__ void __launch_bounds__(256, 4) k_blk_tc(const BlkTask* __restrict__ t
                                                    const double* __restrict__ XS, double* __restrict__ PS)
 {
     constexpr int CT = 32, S = CT + 4;            // tile width; padded shared row (conflict-free C0 reads)
-    __shared__ float s_a[2][64][S];
+    constexpr int NS = 3;                         // A-tile stages: two tiles in flight during the math
+    __shared__ __align__(16) float s_a[NS][64][S];
     __shared__ uint4 s_w[8][32][2];               // W^T fragments per k-step of 8 rows: hi, lo
     __shared__ uint4 s_v[2][4][32][2];            // V^T fragments per k-step of 8 columns: hi, lo
     const BlkTask T = tasks[blockIdx.x];
@@ -1486,25 +1487,33 @@ __global__ void __launch_bounds__(256, 4) k_blk_tc(const BlkTask* __restrict__ t
         if (do1)
             frag(T.in1_row + rc, R, 8 * warp, s_w[warp][lane][0], s_w[warp][lane][1]);
 
-        // tile staging: 64 x 32 floats, 8 per thread; V^T fragments of the tile's columns
-        float ra[8];
-        uint4 rvh = make_uint4(0, 0, 0, 0), rvl = rvh;
-        auto load_tile = [&](int c0) {
-#pragma unroll
-            for (int u = 0; u < 8; u++)
+        // A tiles (64 x 32 floats, 8 per thread) go straight to shared memory by 4-byte
+        // cp.async (rows start at any float), zero-filled past the block's edges, issued
+        // two tiles ahead; the V^T fragments of the next tile's columns go through
+        // registers (warps 0-3) one tile ahead
+        const int nct = (ncol + CT - 1) / CT;
+        auto issue_tile = [&](int t) {
+            if (t < nct)
             {
-                const int e = threadIdx.x + 256 * u, r = e >> 5, c = e & 31;
-                ra[u] = (r < R && c0 + c < ncol) ? A[(long long) r * ncol + c0 + c] : 0.f;
+                const int c0 = t * CT;
+                float* dst = &s_a[t % NS][0][0];
+#pragma unroll
+                for (int u = 0; u < 8; u++)
+                {
+                    const int e = threadIdx.x + 256 * u, r = e >> 5, c = e & 31;
+                    const bool in = r < R && c0 + c < ncol;
+                    const float* src = in ? A + (long long) r * ncol + c0 + c : A;
+                    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;"
+                                 ::"r"(smem_u32(dst + r * S + c)), "l"(src), "r"(in ? 4 : 0) : "memory");
+                }
             }
+            cp_async_commit();
+        };
+        uint4 rvh = make_uint4(0, 0, 0, 0), rvl = rvh;
+        auto load_v = [&](int c0) {
             if (do0 && warp < 4) frag(T.in0_row + c0, ncol - c0, 8 * warp, rvh, rvl);
         };
-        auto store_tile = [&](int buf) {
-#pragma unroll
-            for (int u = 0; u < 8; u++)
-            {
-                const int e = threadIdx.x + 256 * u;
-                s_a[buf][e >> 5][e & 31] = ra[u];
-            }
+        auto store_v = [&](int buf) {
             if (do0 && warp < 4) { s_v[buf][warp][lane][0] = rvh; s_v[buf][warp][lane][1] = rvl; }
         };
 
@@ -1514,21 +1523,35 @@ __global__ void __launch_bounds__(256, 4) k_blk_tc(const BlkTask* __restrict__ t
 #pragma unroll
             for (int q = 0; q < 4; q++) c0acc[n][q] = 0.0;
 
+        issue_tile(0); issue_tile(1); issue_tile(2);
         if (ncol > 0)
         {
-            load_tile(0);
-            store_tile(0);
+            load_v(0);
+            store_v(0);
         }
+        asm volatile("cp.async.wait_group 2;" ::: "memory");
         __syncthreads();
         int buf = 0;
         for (int c0 = 0; c0 < ncol; c0 += CT)
         {
+            const int t = c0 / CT, sa = t % NS;
             const bool more = c0 + CT < ncol;
-            if (more) load_tile(c0 + CT);
+            if (more) load_v(c0 + CT);
             if (warp < 4)
             {
                 if (do1)
                 {
+                    // the C1 values the later chunks add to, read before the MMAs so their
+                    // latency hides behind them
+                    const int cb = c0 + 8 * warp + 2 * tq;
+                    double old[4] = {0.0, 0.0, 0.0, 0.0};
+                    if (rc > 0)
+#pragma unroll
+                        for (int q = 0; q < 4; q++)
+                        {
+                            const int rhs = (q < 2) ? g : g + 8, col = cb + (q & 1);
+                            if (rhs < NV && col < ncol) old[q] = PS[(long long) (T.out1_row + col) * NV + rhs];
+                        }
                     // C1^T for columns c0 + 8w .. +7: k over the R rows (8 k-steps)
                     float d[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};   // two chains, summed
                     const int ksteps = (R + 7) >> 3;
@@ -1536,8 +1559,8 @@ __global__ void __launch_bounds__(256, 4) k_blk_tc(const BlkTask* __restrict__ t
                     for (int ks = 0; ks < 8; ks++)
                     {
                         if (ks >= ksteps) break;
-                        const float b0 = s_a[buf][8 * ks + tq][8 * warp + g];
-                        const float b1 = s_a[buf][8 * ks + tq + 4][8 * warp + g];
+                        const float b0 = s_a[sa][8 * ks + tq][8 * warp + g];
+                        const float b1 = s_a[sa][8 * ks + tq + 4][8 * warp + g];
                         const uint32_t h0 = tf32_rna(b0), h1 = tf32_rna(b1);
                         const uint32_t l0 = __float_as_uint(b0 - __uint_as_float(h0)),
                                        l1 = __float_as_uint(b1 - __uint_as_float(h1));
@@ -1548,16 +1571,14 @@ __global__ void __launch_bounds__(256, 4) k_blk_tc(const BlkTask* __restrict__ t
                         mma_tf32(dd, wh.x, wh.y, wh.z, wh.w, h0, h1);
                     }
                     // rows of the fragment = right-hand sides (g, g+8), columns = (2tq, 2tq+1)
-                    const int cb = c0 + 8 * warp + 2 * tq;
 #pragma unroll
                     for (int q = 0; q < 4; q++)
                     {
                         const int rhs = (q < 2) ? g : g + 8, col = cb + (q & 1);
                         if (rhs < NV && col < ncol)
                         {
-                            double* o = PS + (long long) (T.out1_row + col) * NV + rhs;
                             const double v = (double) (d[0][q] + d[1][q]);
-                            *o = (rc == 0) ? v : *o + v;
+                            PS[(long long) (T.out1_row + col) * NV + rhs] = (rc == 0) ? v : old[q] + v;
                         }
                     }
                 }
@@ -1575,7 +1596,7 @@ __global__ void __launch_bounds__(256, 4) k_blk_tc(const BlkTask* __restrict__ t
                         for (int n = 0; n < 2; n++)
                         {
                             const int row = 16 * u + 8 * n + g;
-                            const float b0 = s_a[buf][row][8 * ks + tq], b1 = s_a[buf][row][8 * ks + tq + 4];
+                            const float b0 = s_a[sa][row][8 * ks + tq], b1 = s_a[sa][row][8 * ks + tq + 4];
                             const uint32_t h0 = tf32_rna(b0), h1 = tf32_rna(b1);
                             const uint32_t l0 = __float_as_uint(b0 - __uint_as_float(h0)),
                                            l1 = __float_as_uint(b1 - __uint_as_float(h1));
@@ -1590,10 +1611,13 @@ __global__ void __launch_bounds__(256, 4) k_blk_tc(const BlkTask* __restrict__ t
                         for (int q = 0; q < 4; q++) c0acc[n][q] += (double) d[n][q];
                 }
             }
-            if (more) store_tile(buf ^ 1);
-            __syncthreads();
+            if (more) store_v(buf ^ 1);
+            asm volatile("cp.async.wait_group 1;" ::: "memory");   // tile t+1 has landed
+            __syncthreads();                      // ... for every thread; tile t no longer read
+            issue_tile(t + 3);
             buf ^= 1;
         }
+        cp_async_wait_all();
         if (do0 && warp >= 4)
         {
             const int u = warp - 4;
