@@ -14,6 +14,7 @@
 // across blocks go through PS slots in a fixed order, so results are bitwise
 // reproducible run to run.
 #include <cuda_runtime.h>
+#include <cuda_bf16.h>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -1645,21 +1646,6 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t start, uint32_t lbo_bytes
            ((uint64_t) ((sbo_bytes >> 4) & 0x3FFFu) << 32) | (1ull << 46) | ((uint64_t) layout << 61);
 }
 
-// Instruction descriptor, kind::tf32: FP32 accumulator, TF32 A and B, A K-major (0) or
-// MN-major (1), B K-major, N = n, M = 64.
-__host__ __device__ constexpr uint32_t umma_idesc_tf32(int n, int a_mn_major)
-{
-    return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t) a_mn_major << 15) | ((uint32_t) (n >> 3) << 17) |
-           ((uint32_t) (64 >> 4) << 24);
-}
-
-__device__ __forceinline__ void umma_tf32(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc)
-{
-    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-                 "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}"
-                 ::"r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(acc) : "memory");
-}
-
 __device__ __forceinline__ void umma_commit(uint32_t mbar)
 {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar) : "memory");
@@ -1674,50 +1660,74 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t mbar, uint32_t parity)
     return ok != 0;
 }
 
+// ----------------------------- stored blocks on tcgen05, BF16x3 split (one tile layout)
+
+// Instruction descriptor, kind::f16 with BF16 A and B, FP32 accumulator: A K-major (0)
+// or MN-major (1), B K-major, N = n, M = 64.
+__host__ __device__ constexpr uint32_t umma_idesc_bf16(int n, int a_mn_major)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t) a_mn_major << 15) | ((uint32_t) (n >> 3) << 17) |
+           ((uint32_t) (64 >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_f16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc)
+{
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                 ::"r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(acc) : "memory");
+}
+
+// x = h + m + l exactly up to the last bits of l: three BF16 pieces (8 significant bits
+// each) of an FP32 value, each the round-to-nearest of the remainder.
+__device__ __forceinline__ void bf16x3(float x, uint16_t& h, uint16_t& m, uint16_t& l)
+{
+    const __nv_bfloat16 bh = __float2bfloat16_rn(x);
+    const float r1 = x - __bfloat162float(bh);
+    const __nv_bfloat16 bm = __float2bfloat16_rn(r1);
+    const float r2 = r1 - __bfloat162float(bm);
+    const __nv_bfloat16 bl = __float2bfloat16_rn(r2);
+    h = __bfloat16_as_ushort(bh); m = __bfloat16_as_ushort(bm); l = __bfloat16_as_ushort(bl);
+}
+
 // One stored block task (up to 1024 rows x ncol, FP32 copy) for panels of 8 / 16
 // right-hand sides on the 5th-generation tensor cores, both products per 64 x 64 tile
 // of A with the tile read from HBM once:
-//   C0 (64 rows x NV) += A_tile (64 x 64) V_tile (64 x NV)      A K-major   -> TMEM columns 0-15
-//   C1 (64 cols x NV)  = A_tile^T (64 x 64) W_chunk (64 x NV)   A MN-major  -> TMEM columns 16-31
-// (an M = 64 accumulator occupies lanes 0-15 of each of the four sub-partitions)
-// The tile is stored twice in shared memory, split into TF32 hi / lo for 3xTF32 (hi.hi
-// + lo.hi + hi.lo, FP32 accumulation in TMEM): 128-byte rows of 32 columns with the
-// 128-byte swizzle (16-byte granules XOR row mod 8) for the K-major view of C0, and the
-// same rows with the 32-byte-granule swizzle (granule XOR row mod 4) that MN-major TF32
-// operands need, for C1.  One thread issues the 48 MMAs
-// of a tile and commits them to an mbarrier; meanwhile all threads load the next tile
-// from global memory into registers.  C1 of each tile is read from TMEM and added into
-// the task's single C1 slot (stored by the first 64-row chunk); C0 of each tile is read
-// from TMEM too and summed over the chunk's column tiles in FP64 registers (FP32 sums
-// per 64-column tile, FP64 across tiles, like the mma.sync kernels), then written when
-// the chunk ends.  Every wait on the
-// mbarrier is bounded: on expiry the kernel records a status and stops issuing work.
-struct Tc5Smem {
-    float a_hi[2 * 64 * 32];   // K-major view: two column blocks (32 columns) x 64 rows, 128 B rows, 128-byte swizzle
-    float a_lo[2 * 64 * 32];
-    float t_hi[2 * 64 * 32];   // MN-major view: the same tile in the 32-byte-granule swizzle MN-major TF32 requires
-    float t_lo[2 * 64 * 32];
-    float v_hi[16 * 64];       // V^T (NV x 64 columns), core matrices 8 x 4, K-major
-    float v_lo[16 * 64];
-    float w_hi[16 * 64];       // W^T (NV x 64 rows)
-    float w_lo[16 * 64];
+//   C0 (64 rows x NV) += A_tile V_tile       A K-major  (k = the tile's columns) -> TMEM columns 0-15
+//   C1 (64 cols x NV)  = A_tile^T W_chunk    A MN-major (k = the tile's rows)    -> TMEM columns 16-31
+// Each value is split into three BF16 pieces h + m + l (24 significant bits, the whole
+// FP32 value) and the products keep the six terms down to 2^-16 relative
+// (l.h + h.l + m.m + m.h + h.m + h.h, smallest first), summed in FP32 in TMEM over one
+// tile (64 terms deep) and in FP64 across tiles.  With 16-bit pieces one 128-byte-
+// swizzled copy of each piece (rows of 64 columns) serves both the K-major and the
+// MN-major view, so a tile takes 24 KB of shared memory and several CTAs fit an SM.
+// Per tile: the threads store the tile's pieces (loaded into registers while the
+// previous tile's MMAs ran), one thread issues the 48 MMAs and commits them to an
+// mbarrier, the threads load the next tile, then read the accumulators: C1 is added
+// into the task's C1 slot, C0 into FP64 registers written when the 64-row chunk ends.
+// Every wait on the mbarrier is bounded: on expiry the kernel records a status and
+// stops issuing work.
+struct Bf3Smem {
+    uint16_t a[3][64 * 64];    // A tile pieces h, m, l: 64 rows of 128 B, 128-byte swizzle
+    uint16_t v[3][16 * 64];    // V^T pieces (NV rows of the tile's 64 columns)
+    uint16_t w[3][16 * 64];    // W^T pieces (NV rows of the chunk's 64 rows)
+    double c0acc[64][17];      // the chunk's C0 rows in FP64 (row 16 warp + lane; padded)
     unsigned long long mbar;
     uint32_t tmem;
 };
+constexpr int kBf3Threads = 128;
 
-constexpr int kTc5Threads = 128;
+// byte offset of 16-byte granule q (8 BF16) of row r in a 128-byte-swizzled tile
+__device__ __forceinline__ int sw128(int r, int q) { return r * 128 + ((q ^ (r & 7)) << 4); }
 
 template <int NV>
-__global__ void __launch_bounds__(kTc5Threads, 2) k_blk_tc5(const BlkTask* __restrict__ tasks,
+__global__ void __launch_bounds__(kBf3Threads, 5) k_blk_bf3(const BlkTask* __restrict__ tasks,
                                                             const float* __restrict__ arena,
                                                             const double* __restrict__ XS, double* __restrict__ PS,
                                                             int* __restrict__ status)
 {
-    constexpr int NB = NV / 8;                         // 8-row groups of the NV x K operands
-    constexpr uint32_t IDESC0 = umma_idesc_tf32(NV, 0), IDESC1 = umma_idesc_tf32(NV, 1);
-    extern __shared__ __align__(1024) unsigned char tc5_raw[];
-    // 1024-byte alignment of the swizzled tiles
-    Tc5Smem& sm = *reinterpret_cast<Tc5Smem*>(tc5_raw + ((1024 - (smem_u32(tc5_raw) & 1023)) & 1023));
+    constexpr uint32_t IDESC0 = umma_idesc_bf16(NV, 0), IDESC1 = umma_idesc_bf16(NV, 1);
+    extern __shared__ __align__(1024) unsigned char bf3_raw[];
+    Bf3Smem& sm = *reinterpret_cast<Bf3Smem*>(bf3_raw + ((1024 - (smem_u32(bf3_raw) & 1023)) & 1023));
     const BlkTask T = tasks[blockIdx.x];
     const int ncol = T.ncol, nrow = T.nrow;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -1725,7 +1735,6 @@ __global__ void __launch_bounds__(kTc5Threads, 2) k_blk_tc5(const BlkTask* __res
     const int ntc = (ncol + 63) / 64, nt = ntc * ((nrow + 63) / 64);
     const float* A0 = arena + T.a_off;
 
-    // TMEM: 32 columns (C0 in columns 0-15, C1 in columns 16-31)
     if (warp == 0)
     {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 32;" ::"r"(smem_u32(&sm.tmem)) : "memory");
@@ -1740,73 +1749,74 @@ __global__ void __launch_bounds__(kTc5Threads, 2) k_blk_tc5(const BlkTask* __res
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = sm.tmem, mbar = smem_u32(&sm.mbar);
-    const uint32_t a_hi = smem_u32(sm.a_hi), a_lo = smem_u32(sm.a_lo), t_hi = smem_u32(sm.t_hi), t_lo = smem_u32(sm.t_lo);
-    const uint32_t v_hi = smem_u32(sm.v_hi), v_lo = smem_u32(sm.v_lo), w_hi = smem_u32(sm.w_hi), w_lo = smem_u32(sm.w_lo);
+    unsigned char* const a_b = reinterpret_cast<unsigned char*>(sm.a);
+    unsigned char* const v_b = reinterpret_cast<unsigned char*>(sm.v);
+    unsigned char* const w_b = reinterpret_cast<unsigned char*>(sm.w);
+    const uint32_t a_s = smem_u32(sm.a), v_s = smem_u32(sm.v), w_s = smem_u32(sm.w);
 
-    // registers of the tile being loaded: 32 A values, 8 V values, 8 W values per thread
-    float ra[32];
-    double rv[8 * NB / 2], rw[8 * NB / 2];
+    // registers of the tile being loaded: thread t holds 4 granules (8 columns each) of A
+    // and one granule of V^T and of W^T (rows n < NV of 8 consecutive k)
+    float ra[4][8];
+    float rv[8], rw[8];
     auto load_tile = [&](int t) {
         const int rc = (t / ntc) * 64, c0 = (t % ntc) * 64, R = min(64, nrow - rc);
         const float* A = A0 + (long long) rc * ncol + c0;
 #pragma unroll
-        for (int u = 0; u < 32; u++)
+        for (int u = 0; u < 4; u++)
         {
-            const int e = tid + kTc5Threads * u, r = e >> 6, c = e & 63;
-            ra[u] = (r < R && c0 + c < ncol) ? A[(long long) r * ncol + c] : 0.f;
-        }
+            const int gi = tid + kBf3Threads * u, r = gi >> 3, q = gi & 7;
 #pragma unroll
-        for (int u = 0; u < 4 * NB; u++)
+            for (int j = 0; j < 8; j++)
+            {
+                const int c = 8 * q + j;
+                ra[u][j] = (r < R && c0 + c < ncol) ? A[(long long) r * ncol + c] : 0.f;
+            }
+        }
+        const int n = tid >> 3, q = tid & 7;          // V^T / W^T granule: row n, k = 8q .. 8q+7
+#pragma unroll
+        for (int j = 0; j < 8; j++)
         {
-            const int e = tid + kTc5Threads * u, k = e / NV, n = e % NV;   // 64 x NV
-            rv[u] = (do0 && c0 + k < ncol) ? XS[(long long) (T.in0_row + c0 + k) * NV + n] : 0.0;
-            rw[u] = (do1 && c0 == 0 && k < R) ? XS[(long long) (T.in1_row + rc + k) * NV + n] : 0.0;
+            const int k = 8 * q + j;
+            rv[j] = (n < NV && do0 && c0 + k < ncol) ? (float) XS[(long long) (T.in0_row + c0 + k) * NV + n] : 0.f;
+            rw[j] = (n < NV && do1 && c0 == 0 && k < R) ? (float) XS[(long long) (T.in1_row + rc + k) * NV + n] : 0.f;
         }
     };
-    auto split = [](float x, float& h, float& l) {
-        const uint32_t hb = tf32_rna(x);
-        h = __uint_as_float(hb);
-        l = x - h;
+    auto put = [&](unsigned char* base, int stride, int off, const float (&x)[8]) {
+        uint16_t h[8], m[8], l[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) bf16x3(x[j], h[j], m[j], l[j]);
+        auto pack = [](const uint16_t (&e)[8]) {
+            return make_uint4(e[0] | ((uint32_t) e[1] << 16), e[2] | ((uint32_t) e[3] << 16),
+                              e[4] | ((uint32_t) e[5] << 16), e[6] | ((uint32_t) e[7] << 16));
+        };
+        *reinterpret_cast<uint4*>(base + off) = pack(h);
+        *reinterpret_cast<uint4*>(base + stride + off) = pack(m);
+        *reinterpret_cast<uint4*>(base + 2 * stride + off) = pack(l);
     };
     auto store_tile = [&](int t) {
         const int c0 = (t % ntc) * 64;
 #pragma unroll
-        for (int u = 0; u < 32; u++)
+        for (int u = 0; u < 4; u++)
         {
-            const int e = tid + kTc5Threads * u, r = e >> 6, c = e & 63, cc = c & 31;
-            const int off = (c >> 5) * 8192 + (r >> 3) * 1024 + (r & 7) * 128 + ((((cc >> 2) ^ (r & 7)) << 4) | ((cc & 3) << 2));
-            const int offt = (c >> 5) * 8192 + (r >> 2) * 512 + (r & 3) * 128 + ((((cc >> 3) ^ (r & 3)) << 5) | ((cc & 7) << 2));
-            float h, l;
-            split(ra[u], h, l);
-            *reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(sm.a_hi) + off) = h;
-            *reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(sm.a_lo) + off) = l;
-            *reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(sm.t_hi) + offt) = h;
-            *reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(sm.t_lo) + offt) = l;
+            const int gi = tid + kBf3Threads * u, r = gi >> 3, q = gi & 7;
+            put(a_b, 64 * 64 * 2, sw128(r, q), ra[u]);
         }
-#pragma unroll
-        for (int u = 0; u < 4 * NB; u++)
+        const int n = tid >> 3, q = tid & 7;
+        if (n < NV)
         {
-            const int e = tid + kTc5Threads * u, k = e / NV, n = e % NV;
-            const int off = (((k >> 2) * NB + (n >> 3)) * 128 + (n & 7) * 16 + (k & 3) * 4) >> 2;
-            float h, l;
-            split((float) rv[u], h, l);
-            sm.v_hi[off] = h; sm.v_lo[off] = l;
-            if (c0 == 0)
-            {
-                split((float) rw[u], h, l);
-                sm.w_hi[off] = h; sm.w_lo[off] = l;
-            }
+            put(v_b, 16 * 64 * 2, sw128(n, q), rv);
+            if (c0 == 0) put(w_b, 16 * 64 * 2, sw128(n, q), rw);
         }
     };
 
     bool ok = true;
     uint32_t phase = 0;
-    double c0acc[NV];   // lanes 0-15: the chunk's C0 row 16 warp + lane
+    // lanes 0-15: the chunk's C0 row 16 warp + lane, summed in shared memory
+    double* const c0acc = sm.c0acc[(16 * warp + lane) & 63];
+    if (lane < 16)
 #pragma unroll
-    for (int n = 0; n < NV; n++) c0acc[n] = 0.0;
+        for (int n = 0; n < NV; n++) c0acc[n] = 0.0;
     // read back the tile just multiplied: C1 into its slot, C0 into the chunk's FP64 sums
-    // (written at the end of a chunk).
-    // Thread 0 waits (bounded) for the MMAs' commit; the outcome is made uniform.
     auto drain = [&](int t) {
         int good = 1;
         if (tid == 0)
@@ -1820,8 +1830,6 @@ __global__ void __launch_bounds__(kTc5Threads, 2) k_blk_tc5(const BlkTask* __res
         ok = __syncthreads_and(good) != 0;
         if (!ok) return;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        // lanes 0-15 of sub-partition w hold rows 16w..16w+15 of both accumulators:
-        // columns 0-15 C0 (rows of the chunk), columns 16-31 C1 (columns of the tile)
         uint32_t d[32];
         asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
                      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
@@ -1864,6 +1872,8 @@ __global__ void __launch_bounds__(kTc5Threads, 2) k_blk_tc5(const BlkTask* __res
         }
     };
 
+    // the six products of one K-step: (A piece, B piece), smallest first
+    constexpr int PA[6] = {2, 0, 1, 1, 0, 0}, PB[6] = {0, 2, 1, 0, 1, 0};
     if (nt > 0) load_tile(0);
     for (int t = 0; t < nt; t++)
     {
@@ -1876,28 +1886,21 @@ __global__ void __launch_bounds__(kTc5Threads, 2) k_blk_tc5(const BlkTask* __res
         if (tid == 0)
         {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            if (do0)
-                for (int j = 0; j < 8; j++)
+#pragma unroll
+            for (int ks = 0; ks < 4; ks++)          // K-steps of 16
+#pragma unroll
+                for (int p = 0; p < 6; p++)
                 {
-                    // K-step of 8 columns: column block j / 4, 32-byte step within the row
-                    const uint32_t ao = (j >> 2) * 8192 + (j & 3) * 32, bo = j * 2 * NB * 128;
-                    const uint64_t ah = umma_desc(a_hi + ao, 16, 1024, 2), al = umma_desc(a_lo + ao, 16, 1024, 2);
-                    const uint64_t bh = umma_desc(v_hi + bo, NB * 128, 128, 0), bl = umma_desc(v_lo + bo, NB * 128, 128, 0);
-                    umma_tf32(tmem, al, bh, IDESC0, j == 0 ? 0u : 1u);
-                    umma_tf32(tmem, ah, bl, IDESC0, 1u);
-                    umma_tf32(tmem, ah, bh, IDESC0, 1u);
-                }
-            if (do1)
-                for (int j = 0; j < 8; j++)
-                {
-                    // K-step of 8 rows = two 4-row swizzle atoms of the MN-major copy (32-column
-                    // blocks 8192 B apart, 4-row atoms 512 B apart)
-                    const uint32_t ao = j * 1024, bo = j * 2 * NB * 128;
-                    const uint64_t ah = umma_desc(t_hi + ao, 8192, 512, 1), al = umma_desc(t_lo + ao, 8192, 512, 1);
-                    const uint64_t bh = umma_desc(w_hi + bo, NB * 128, 128, 0), bl = umma_desc(w_lo + bo, NB * 128, 128, 0);
-                    umma_tf32(tmem + 16u, al, bh, IDESC1, j == 0 ? 0u : 1u);
-                    umma_tf32(tmem + 16u, ah, bl, IDESC1, 1u);
-                    umma_tf32(tmem + 16u, ah, bh, IDESC1, 1u);
+                    // C0: A K-major (32-byte step along the row), B = V^T K-major
+                    if (do0)
+                        umma_f16(tmem, umma_desc(a_s + PA[p] * 8192 + ks * 32, 16, 1024, 2),
+                                 umma_desc(v_s + PB[p] * 2048 + ks * 32, 16, 1024, 2), IDESC0,
+                                 (ks == 0 && p == 0) ? 0u : 1u);
+                    // C1: A MN-major (16 rows = two 8-row swizzle atoms per step), B = W^T K-major
+                    if (do1)
+                        umma_f16(tmem + 16u, umma_desc(a_s + PA[p] * 8192 + ks * 2048, 8192, 1024, 2),
+                                 umma_desc(w_s + PB[p] * 2048 + ks * 32, 16, 1024, 2), IDESC1,
+                                 (ks == 0 && p == 0) ? 0u : 1u);
                 }
             umma_commit(mbar);
         }
@@ -1914,7 +1917,7 @@ __global__ void __launch_bounds__(kTc5Threads, 2) k_blk_tc5(const BlkTask* __res
 }
 
 template <int NV>
-constexpr int tc5_smem_bytes() { return (int) sizeof(Tc5Smem) + 1024; }
+constexpr int bf3_smem_bytes() { return (int) sizeof(Bf3Smem) + 1024; }
 
 
 // ---------------------------------------------- sweeps on the tensor cores (FP32 U)
@@ -2175,18 +2178,18 @@ cudaError_t launch_blk(int NV, const BlkTask* t, int n, const TA* arena, const d
         {
             if (use_tc == 2 && status)
             {
-                // tcgen05 kernel (TMEM accumulators)
+                // tcgen05 kernel (BF16x3 pieces, TMEM accumulators)
                 if (NV == 16)
                 {
-                    constexpr int b = tc5_smem_bytes<16>();
-                    cudaError_t e = allow_smem(k_blk_tc5<16>, b);
+                    constexpr int b = bf3_smem_bytes<16>();
+                    cudaError_t e = allow_smem(k_blk_bf3<16>, b);
                     if (e != cudaSuccess) return e;
-                    k_blk_tc5<16><<<n, kTc5Threads, b, st>>>(t, arena, XS, PS, status);
+                    k_blk_bf3<16><<<n, kBf3Threads, b, st>>>(t, arena, XS, PS, status);
                 } else {
-                    constexpr int b = tc5_smem_bytes<8>();
-                    cudaError_t e = allow_smem(k_blk_tc5<8>, b);
+                    constexpr int b = bf3_smem_bytes<8>();
+                    cudaError_t e = allow_smem(k_blk_bf3<8>, b);
                     if (e != cudaSuccess) return e;
-                    k_blk_tc5<8><<<n, kTc5Threads, b, st>>>(t, arena, XS, PS, status);
+                    k_blk_bf3<8><<<n, kBf3Threads, b, st>>>(t, arena, XS, PS, status);
                 }
                 return cudaGetLastError();
             }

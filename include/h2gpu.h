@@ -227,7 +227,7 @@ int h2gpu_graph_launch(h2gpu_image *img, void *stream);
 #define H2GPU_JIT_SIMT 0
 #define H2GPU_JIT_TC   1
 #define H2GPU_JIT_PAIR 2
-#define H2GPU_BLK_TCGEN05 3   /* stored-block images: block products on tcgen05 with TMEM accumulators */
+#define H2GPU_BLK_TCGEN05 3   /* stored-block images: block products on tcgen05 (BF16x3 pieces, TMEM accumulators) */
 int h2gpu_autotune(h2gpu_image *img, int n_vec, const double *dX, int ldx, double *dY, int ldy,
                    int *best_nv, int *best_variant);
 
@@ -236,8 +236,9 @@ int h2gpu_autotune(h2gpu_image *img, int n_vec, const double *dX, int ldx, doubl
  * H2GPU_JIT_TC (default) or H2GPU_JIT_PAIR (needs a scalar kernel; panels of 8 or
  * 16 right-hand sides, others use H2GPU_JIT_TC); for stored-block images
  * H2GPU_JIT_TC (default: block products of panels of 8 or 16 on the tensor cores with
- * warp-level MMAs), H2GPU_BLK_TCGEN05 (the same on tcgen05, accumulators in tensor
- * memory) or H2GPU_JIT_SIMT (CUDA cores).  FP64 panels always use the CUDA cores; a captured
+ * warp-level MMAs, 3xTF32), H2GPU_BLK_TCGEN05 (the same on tcgen05: values split into
+ * three BF16 pieces, six products kept, accumulators in tensor memory) or
+ * H2GPU_JIT_SIMT (CUDA cores).  FP64 panels always use the CUDA cores; a captured
  * graph keeps the variant it was captured with.  No counterpart in the reference.
  */
 int h2gpu_set_jit_variant(h2gpu_image *img, int variant);
