@@ -782,7 +782,7 @@ template <> struct Vec4<float> { using t = float4; };
 // in FP32 and every tile sum is added to FP64 accumulators, so an FP32 sum never
 // spans more than one tile of sources.  Outputs are written once, no atomics.
 template <int KID, typename T, int NV, int KD, int TPT>
-__global__ void __launch_bounds__(128 / TPT, sizeof(T) == 4 ? 5 * TPT : 1) k_jit(const JitTarget* __restrict__ tgts, const JitSource* __restrict__ srcs,
+__global__ void __launch_bounds__(128 / TPT, sizeof(T) == 4 ? 5 * TPT : 4 * TPT) k_jit(const JitTarget* __restrict__ tgts, const JitSource* __restrict__ srcs,
                                                    const typename Vec4<T>::t* __restrict__ pts, KParam kp, int use_shift,
                                                    const double* __restrict__ XS, double* __restrict__ PS,
                                                    double* __restrict__ Y1)
@@ -2290,11 +2290,13 @@ static cudaError_t launch_jit_k(int NV, const JitTarget* tg, int n, const JitSou
             return cudaGetLastError();
         }
     }
-    // two targets per thread (64 threads per 128-point chunk) where the accumulators allow it
+    // FP32: two targets per thread (64 threads per 128-point chunk) where the accumulators
+    // allow it; FP64: one target per thread, 4 CTAs per SM (two targets per thread took
+    // 188 registers and left 7 warps per SM to hide the FP64 latencies: 1.4x slower)
     NV_DISPATCH(NV, {
         if constexpr (KD == 3 && NVc > 8)
             return cudaErrorInvalidValue;   // tensor kernels run in panels of <= 8 right-hand sides
-        else if constexpr (KD * NVc <= 16)
+        else if constexpr (KD * NVc <= 16 && sizeof(T) == 4)
             k_jit<KID, T, NVc, KD, 2><<<n, 64, 0, st>>>(tg, sr, p, kp, use_shift, XS, PS, Y1);
         else
             k_jit<KID, T, NVc, KD, 1><<<n, 128, 0, st>>>(tg, sr, p, kp, use_shift, XS, PS, Y1);
