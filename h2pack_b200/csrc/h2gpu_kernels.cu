@@ -107,70 +107,75 @@ __global__ void k_permute(const double* __restrict__ X, long long x_rs, long lon
 
 // ---------------------------------------------------------------- upward
 
-// y0 = U^T w for one column tile of a node per CTA (narrow panels).  Lanes own
-// columns, warps split the rows, the warps' column partials are summed in shared memory.
+// y0 = U^T w for one column tile (<= 64 columns) of a node per CTA (narrow panels).
+// Lane l owns columns c0 + l and c0 + 32 + l; warp w takes rows w, w + 8, ... of each
+// 256-row chunk of the node's rows, eight rows per step (16 loads in flight per lane);
+// the chunk's inputs are staged in shared memory first, and the 8 warps' column sums
+// are added in warp order at the end.
 template <typename TA, int NV>
 __global__ void __launch_bounds__(kThreads) k_up(const UpTask* __restrict__ tasks, const TA* __restrict__ Uar,
                                                  double* __restrict__ XS)
 {
-    constexpr int S = SV<NV>::v;
-    constexpr int RT = 64;
-    __shared__ double s_w[RT * S];
-    __shared__ double s_red[kWarps][32][NV];
+    constexpr int RC = 256;
+    __shared__ double s_w[RC * NV];
+    __shared__ double s_red[kWarps][64][NV];
     const UpTask t = tasks[blockIdx.x];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const TA* U = Uar + t.u_off;
-    const int cend = t.c0 + t.nc;
-    for (int ct = t.c0; ct < cend; ct += 32)
+    const int cend = t.c0 + t.nc, ca = t.c0 + lane, cb = ca + 32;
+    const bool va = ca < cend, vb = cb < cend;
+    double acc[2][NV];
+#pragma unroll
+    for (int v = 0; v < NV; v++) { acc[0][v] = 0.0; acc[1][v] = 0.0; }
+    for (int rc = 0; rc < t.nrow; rc += RC)
     {
-        const int c = ct + lane;
-        double acc[NV];
-#pragma unroll
-        for (int v = 0; v < NV; v++) acc[v] = 0.0;
-        for (int rc = 0; rc < t.nrow; rc += RT)
+        const int nr = min(RC, t.nrow - rc);
+        __syncthreads();
+        for (int i = threadIdx.x; i < nr * NV; i += kThreads) s_w[i] = XS[(long long) (t.in_row + rc) * NV + i];
+        __syncthreads();
+        int r = w;
+        for (; r + 56 < nr; r += 64)
         {
-            const int nr = min(RT, t.nrow - rc);
-            __syncthreads();
-            for (int i = threadIdx.x; i < nr * NV; i += kThreads)
+            TA a[8], b[8];
+#pragma unroll
+            for (int k = 0; k < 8; k++)
             {
-                int r = i / NV, v = i % NV;
-                s_w[r * S + v] = XS[(long long) (t.in_row + rc + r) * NV + v];
+                const TA* row = U + (long long) (rc + r + 8 * k) * t.ld;
+                a[k] = va ? row[ca] : TA(0);
+                b[k] = vb ? row[cb] : TA(0);
             }
-            __syncthreads();
-            if (c < cend)
+#pragma unroll
+            for (int k = 0; k < 8; k++)
+#pragma unroll
+                for (int v = 0; v < NV; v++)
+                {
+                    const double x = s_w[(r + 8 * k) * NV + v];
+                    acc[0][v] = fma(to_d(a[k]), x, acc[0][v]);
+                    acc[1][v] = fma(to_d(b[k]), x, acc[1][v]);
+                }
+        }
+        for (; r < nr; r += 8)
+        {
+            const TA* row = U + (long long) (rc + r) * t.ld;
+            const double a = va ? to_d(row[ca]) : 0.0, b = vb ? to_d(row[cb]) : 0.0;
+#pragma unroll
+            for (int v = 0; v < NV; v++)
             {
-                int r = w;
-                for (; r + kWarps < nr; r += 2 * kWarps)
-                {
-                    double a0 = to_d(U[(long long) (rc + r) * t.ld + c]);
-                    double a1 = to_d(U[(long long) (rc + r + kWarps) * t.ld + c]);
-#pragma unroll
-                    for (int v = 0; v < NV; v++)
-                        acc[v] = fma(a1, s_w[(r + kWarps) * S + v], fma(a0, s_w[r * S + v], acc[v]));
-                }
-                if (r < nr)
-                {
-                    double a0 = to_d(U[(long long) (rc + r) * t.ld + c]);
-#pragma unroll
-                    for (int v = 0; v < NV; v++) acc[v] = fma(a0, s_w[r * S + v], acc[v]);
-                }
+                acc[0][v] = fma(a, s_w[r * NV + v], acc[0][v]);
+                acc[1][v] = fma(b, s_w[r * NV + v], acc[1][v]);
             }
         }
+    }
 #pragma unroll
-        for (int v = 0; v < NV; v++) s_red[w][lane][v] = acc[v];
-        __syncthreads();
-        for (int i = threadIdx.x; i < 32 * NV; i += kThreads)
-        {
-            int cc = i / NV, v = i % NV;
-            if (ct + cc < cend)
-            {
-                double s = 0.0;
+    for (int v = 0; v < NV; v++) { s_red[w][lane][v] = acc[0][v]; s_red[w][lane + 32][v] = acc[1][v]; }
+    __syncthreads();
+    for (int i = threadIdx.x; i < t.nc * NV; i += kThreads)
+    {
+        const int cc = i / NV, v = i % NV;
+        double s = 0.0;
 #pragma unroll
-                for (int k = 0; k < kWarps; k++) s += s_red[k][cc][v];
-                XS[(long long) (t.out_row + ct + cc) * NV + v] = s;
-            }
-        }
-        __syncthreads();
+        for (int k = 0; k < kWarps; k++) s += s_red[k][cc][v];
+        XS[(long long) (t.out_row + t.c0 + cc) * NV + v] = s;
     }
 }
 
