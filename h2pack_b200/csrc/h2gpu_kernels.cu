@@ -575,16 +575,53 @@ __global__ void __launch_bounds__(kThreads) k_blk(const BlkTask* __restrict__ ta
     }
 }
 
+// Downward product of one chunk of <= 64 rows of U per CTA (narrow panels):
+// dst[r] = U[r] (y1 + push).  Warp w owns rows 8w..8w+7; lanes stride the columns, eight
+// loads (one per row) in flight per step; the column inputs y1 + push are staged in
+// shared memory per 256 columns; the eight row sums of a warp meet in one transposed
+// butterfly per right-hand side.
 template <typename TA, int NV>
 __global__ void __launch_bounds__(kThreads) k_down(const DownTask* __restrict__ tasks, const TA* __restrict__ Uar,
                                                    const double* __restrict__ Y1, double* __restrict__ PS,
                                                    double* __restrict__ PUSH)
 {
-    extern __shared__ double dsm[];
+    constexpr int CW = 256;
+    __shared__ double s_x[CW * NV];
     const DownTask t = tasks[blockIdx.x];
-    VFromY1 vin{Y1, PUSH, t.y1_row, t.push_row};
-    double* dst = t.dst_ps ? PS + (long long) t.dst_row * NV : PUSH + (long long) t.dst_row * NV;
-    chunk_apply<TA, NV>(Uar + t.u_off, t.nrow, t.ncol, vin, nullptr, 0, dst, nullptr, dsm);
+    const VFromY1 vin{Y1, PUSH, t.y1_row, t.push_row};
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, ncol = t.ncol;
+    const int r0 = 8 * w, nr = max(0, min(8, t.nrow - r0));
+    const TA* A = Uar + t.u_off + (long long) r0 * ncol;
+    double p[NV][8];
+#pragma unroll
+    for (int v = 0; v < NV; v++)
+#pragma unroll
+        for (int k = 0; k < 8; k++) p[v][k] = 0.0;
+    for (int cw = 0; cw < ncol; cw += CW)
+    {
+        const int cend = min(ncol, cw + CW);
+        __syncthreads();
+        for (int i = threadIdx.x; i < (cend - cw) * NV; i += kThreads) s_x[i] = vin(cw + i / NV, i % NV, NV);
+        __syncthreads();
+        for (int c = cw + lane; c < cend; c += 32)
+        {
+            TA a[8];
+#pragma unroll
+            for (int k = 0; k < 8; k++) a[k] = (k < nr) ? A[(long long) k * ncol + c] : TA(0);
+#pragma unroll
+            for (int k = 0; k < 8; k++)
+#pragma unroll
+                for (int v = 0; v < NV; v++) p[v][k] = fma(to_d(a[k]), s_x[(c - cw) * NV + v], p[v][k]);
+        }
+    }
+    double* dst = (t.dst_ps ? PS : PUSH) + (long long) (t.dst_row + r0) * NV;
+    const int row = nv_of_lane<8>(lane);
+#pragma unroll
+    for (int v = 0; v < NV; v++)
+    {
+        warp_transpose_reduce<8>(p[v], lane);
+        if (lane_writes<8>(lane) && row < nr) dst[(long long) row * NV + v] = p[v][0];
+    }
 }
 
 // y1 of a node = sum of its PS slots (fixed order); rows indexed like the y0 region.
@@ -2239,10 +2276,7 @@ cudaError_t launch_down(int NV, const DownTask* t, int n, const TA* U, const dou
         {
             k_sweep_gemm<TA, NVc, false><<<n, 256, 0, st>>>(nullptr, t, U, nullptr, Y1, PS, PUSH);
         } else {
-            constexpr int b = chunk_smem_bytes<NVc>();
-            cudaError_t e = allow_smem(k_down<TA, NVc>, b);
-            if (e != cudaSuccess) return e;
-            k_down<TA, NVc><<<n, kThreads, b, st>>>(t, U, Y1, PS, PUSH);
+            k_down<TA, NVc><<<n, kThreads, 0, st>>>(t, U, Y1, PS, PUSH);
         }
     });
     return cudaGetLastError();
