@@ -1481,21 +1481,28 @@ constexpr int pair_smem_bytes()
 // the right-hand sides as the M = 16 side of m16n8k8 (3xTF32, FP32 accumulation):
 //   C1^T (NV x ncol) = W^T (NV x R) A        [B operand = A, k = rows]      warps 0-3
 //   C0^T (NV x R)    = V^T (NV x ncol) A^T   [B operand = A^T, k = columns] warps 4-7
-// Column tiles of 32 are staged in shared memory (double-buffered through registers);
-// each tile feeds both products.  Warp w < 4 owns columns 8w..8w+7 of every tile and
-// completes the chunk's part of C1 for them over its R rows, stored by the first chunk
-// into the task's single C1 slot and added by the later ones (FP64; the same thread
-// owns the same element in every chunk); warp 4 + u owns rows 16u..16u+15 of the chunk
-// and sums C0 over the tiles (FP32 per tile, FP64 across tiles).
+// Column tiles of 64 are copied to shared memory by 4-byte cp.async one tile ahead of
+// the math (double buffer, 58 KB of dynamic shared memory, 3 CTAs per SM, one barrier
+// per 64 columns); each tile feeds both products.  Warp w < 4 owns columns
+// 16w..16w+15 of every tile and completes the chunk's part of C1 for them over its R
+// rows (two FP32 chains over alternate 8-row steps), stored by the first chunk into the
+// task's single C1 slot and added by the later ones (FP64; the same thread owns the same
+// element in every chunk; the value it adds to is read before the MMAs); warp 4 + u
+// owns rows 16u..16u+15 of the chunk and sums C0 over the tiles (FP32 per 32 columns,
+// FP64 across).
+struct BlkTcSmem {
+    float a[2][64][68];          // A tiles (64 rows x 64 columns, padded rows), double-buffered
+    uint4 w[8][32][2];           // W^T fragments per k-step of 8 rows: hi, lo
+    uint4 v[2][8][32][2];        // V^T fragments per k-step of 8 columns: hi, lo
+};
+
 template <int NV>
-__global__ void __launch_bounds__(256, 4) k_blk_tc(const BlkTask* __restrict__ tasks, const float* __restrict__ arena,
+__global__ void __launch_bounds__(256, 3) k_blk_tc(const BlkTask* __restrict__ tasks, const float* __restrict__ arena,
                                                    const double* __restrict__ XS, double* __restrict__ PS)
 {
-    constexpr int CT = 32, S = CT + 4;            // tile width; padded shared row (conflict-free C0 reads)
-    constexpr int NS = 3;                         // A-tile stages: two tiles in flight during the math
-    __shared__ __align__(16) float s_a[NS][64][S];
-    __shared__ uint4 s_w[8][32][2];               // W^T fragments per k-step of 8 rows: hi, lo
-    __shared__ uint4 s_v[2][4][32][2];            // V^T fragments per k-step of 8 columns: hi, lo
+    constexpr int CT = 64, S = CT + 4;            // tile width; padded shared row
+    extern __shared__ __align__(16) unsigned char blktc_raw[];
+    BlkTcSmem& sm = *reinterpret_cast<BlkTcSmem*>(blktc_raw);
     const BlkTask T = tasks[blockIdx.x];
     const int ncol = T.ncol;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, tq = lane & 3;
@@ -1520,30 +1527,23 @@ __global__ void __launch_bounds__(256, 4) k_blk_tc(const BlkTask* __restrict__ t
         lo = make_uint4(l[0], l[1], l[2], l[3]);
     };
 
-    // the task's rows in chunks of 64; the chunks' C1 parts add into one slot
     for (int rc = 0; rc < T.nrow; rc += 64)
     {
         const float* A = arena + T.a_off + (long long) rc * ncol;
         const int R = min(64, T.nrow - rc);
-        __syncthreads();                          // previous chunk done with s_w / s_a / s_v
-        // W^T fragments for the chunk (8 k-steps of 8 rows), one warp per k-step
+        __syncthreads();
         if (do1)
-            frag(T.in1_row + rc, R, 8 * warp, s_w[warp][lane][0], s_w[warp][lane][1]);
-
-        // A tiles (64 x 32 floats, 8 per thread) go straight to shared memory by 4-byte
-        // cp.async (rows start at any float), zero-filled past the block's edges, issued
-        // two tiles ahead; the V^T fragments of the next tile's columns go through
-        // registers (warps 0-3) one tile ahead
+            frag(T.in1_row + rc, R, 8 * warp, sm.w[warp][lane][0], sm.w[warp][lane][1]);
         const int nct = (ncol + CT - 1) / CT;
         auto issue_tile = [&](int t) {
             if (t < nct)
             {
                 const int c0 = t * CT;
-                float* dst = &s_a[t % NS][0][0];
+                float* dst = &sm.a[t & 1][0][0];
 #pragma unroll
-                for (int u = 0; u < 8; u++)
+                for (int u = 0; u < 16; u++)
                 {
-                    const int e = threadIdx.x + 256 * u, r = e >> 5, c = e & 31;
+                    const int e = threadIdx.x + 256 * u, r = e >> 6, c = e & 63;
                     const bool in = r < R && c0 + c < ncol;
                     const float* src = in ? A + (long long) r * ncol + c0 + c : A;
                     asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;"
@@ -1554,10 +1554,10 @@ __global__ void __launch_bounds__(256, 4) k_blk_tc(const BlkTask* __restrict__ t
         };
         uint4 rvh = make_uint4(0, 0, 0, 0), rvl = rvh;
         auto load_v = [&](int c0) {
-            if (do0 && warp < 4) frag(T.in0_row + c0, ncol - c0, 8 * warp, rvh, rvl);
+            if (do0) frag(T.in0_row + c0, ncol - c0, 8 * warp, rvh, rvl);
         };
         auto store_v = [&](int buf) {
-            if (do0 && warp < 4) { s_v[buf][warp][lane][0] = rvh; s_v[buf][warp][lane][1] = rvl; }
+            if (do0) { sm.v[buf][warp][lane][0] = rvh; sm.v[buf][warp][lane][1] = rvl; }
         };
 
         double c0acc[2][4];
@@ -1566,80 +1566,82 @@ __global__ void __launch_bounds__(256, 4) k_blk_tc(const BlkTask* __restrict__ t
 #pragma unroll
             for (int q = 0; q < 4; q++) c0acc[n][q] = 0.0;
 
-        issue_tile(0); issue_tile(1); issue_tile(2);
-        if (ncol > 0)
-        {
-            load_v(0);
-            store_v(0);
-        }
-        asm volatile("cp.async.wait_group 2;" ::: "memory");
+        issue_tile(0);
+        if (ncol > 0) { load_v(0); store_v(0); }
+        cp_async_wait_all();
         __syncthreads();
         int buf = 0;
         for (int c0 = 0; c0 < ncol; c0 += CT)
         {
-            const int t = c0 / CT, sa = t % NS;
+            const int t = c0 / CT;
             const bool more = c0 + CT < ncol;
+            issue_tile(t + 1);                    // into the other buffer, read two tiles ago
             if (more) load_v(c0 + CT);
             if (warp < 4)
             {
                 if (do1)
                 {
-                    // the C1 values the later chunks add to, read before the MMAs so their
-                    // latency hides behind them
-                    const int cb = c0 + 8 * warp + 2 * tq;
-                    double old[4] = {0.0, 0.0, 0.0, 0.0};
-                    if (rc > 0)
+                    // C1^T for columns c0 + 16w .. +15 (two n-tiles): k over the R rows
+                    double old[2][4];
+#pragma unroll
+                    for (int j = 0; j < 2; j++)
 #pragma unroll
                         for (int q = 0; q < 4; q++)
                         {
-                            const int rhs = (q < 2) ? g : g + 8, col = cb + (q & 1);
-                            if (rhs < NV && col < ncol) old[q] = PS[(long long) (T.out1_row + col) * NV + rhs];
+                            const int rhs = (q < 2) ? g : g + 8, col = c0 + 16 * warp + 8 * j + 2 * tq + (q & 1);
+                            old[j][q] = (rc > 0 && rhs < NV && col < ncol) ? PS[(long long) (T.out1_row + col) * NV + rhs] : 0.0;
                         }
-                    // C1^T for columns c0 + 8w .. +7: k over the R rows (8 k-steps)
-                    float d[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};   // two chains, summed
+                    float d[2][2][4] = {};                // [n-tile][two chains over alternate k-steps]
                     const int ksteps = (R + 7) >> 3;
 #pragma unroll
                     for (int ks = 0; ks < 8; ks++)
                     {
                         if (ks >= ksteps) break;
-                        const float b0 = s_a[sa][8 * ks + tq][8 * warp + g];
-                        const float b1 = s_a[sa][8 * ks + tq + 4][8 * warp + g];
-                        const uint32_t h0 = tf32_rna(b0), h1 = tf32_rna(b1);
-                        const uint32_t l0 = __float_as_uint(b0 - __uint_as_float(h0)),
-                                       l1 = __float_as_uint(b1 - __uint_as_float(h1));
-                        const uint4 wh = s_w[ks][lane][0], wl = s_w[ks][lane][1];
-                        float (&dd)[4] = d[ks & 1];
-                        mma_tf32(dd, wl.x, wl.y, wl.z, wl.w, h0, h1);
-                        mma_tf32(dd, wh.x, wh.y, wh.z, wh.w, l0, l1);
-                        mma_tf32(dd, wh.x, wh.y, wh.z, wh.w, h0, h1);
-                    }
-                    // rows of the fragment = right-hand sides (g, g+8), columns = (2tq, 2tq+1)
+                        const uint4 wh = sm.w[ks][lane][0], wl = sm.w[ks][lane][1];
 #pragma unroll
-                    for (int q = 0; q < 4; q++)
-                    {
-                        const int rhs = (q < 2) ? g : g + 8, col = cb + (q & 1);
-                        if (rhs < NV && col < ncol)
+                        for (int j = 0; j < 2; j++)
                         {
-                            const double v = (double) (d[0][q] + d[1][q]);
-                            PS[(long long) (T.out1_row + col) * NV + rhs] = (rc == 0) ? v : old[q] + v;
+                            const float b0 = sm.a[buf][8 * ks + tq][16 * warp + 8 * j + g];
+                            const float b1 = sm.a[buf][8 * ks + tq + 4][16 * warp + 8 * j + g];
+                            const uint32_t h0 = tf32_rna(b0), h1 = tf32_rna(b1);
+                            const uint32_t l0 = __float_as_uint(b0 - __uint_as_float(h0)),
+                                           l1 = __float_as_uint(b1 - __uint_as_float(h1));
+                            float (&dd)[4] = d[j][ks & 1];
+                            mma_tf32(dd, wl.x, wl.y, wl.z, wl.w, h0, h1);
+                            mma_tf32(dd, wh.x, wh.y, wh.z, wh.w, l0, l1);
+                            mma_tf32(dd, wh.x, wh.y, wh.z, wh.w, h0, h1);
                         }
                     }
+#pragma unroll
+                    for (int j = 0; j < 2; j++)
+#pragma unroll
+                        for (int q = 0; q < 4; q++)
+                        {
+                            const int rhs = (q < 2) ? g : g + 8, col = c0 + 16 * warp + 8 * j + 2 * tq + (q & 1);
+                            if (rhs < NV && col < ncol)
+                            {
+                                const double v = (double) (d[j][0][q] + d[j][1][q]);
+                                PS[(long long) (T.out1_row + col) * NV + rhs] = (rc == 0) ? v : old[j][q] + v;
+                            }
+                        }
                 }
             } else if (do0) {
-                // C0^T for rows 16u .. 16u+15 (two n-tiles of 8): k over the tile's 32 columns
+                // C0^T for rows 16u .. 16u+15 (two n-tiles of 8): k over the tile's 64 columns
                 const int u = warp - 4;
                 if (16 * u < R)
+#pragma unroll
+                for (int half = 0; half < 2; half++)   // FP32 sums over 32 columns, FP64 across
                 {
                     float d[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
 #pragma unroll
-                    for (int ks = 0; ks < 4; ks++)
+                    for (int ks = 4 * half; ks < 4 * half + 4; ks++)
                     {
-                        const uint4 vh = s_v[buf][ks][lane][0], vl = s_v[buf][ks][lane][1];
+                        const uint4 vh = sm.v[buf][ks][lane][0], vl = sm.v[buf][ks][lane][1];
 #pragma unroll
                         for (int n = 0; n < 2; n++)
                         {
                             const int row = 16 * u + 8 * n + g;
-                            const float b0 = s_a[sa][row][8 * ks + tq], b1 = s_a[sa][row][8 * ks + tq + 4];
+                            const float b0 = sm.a[buf][row][8 * ks + tq], b1 = sm.a[buf][row][8 * ks + tq + 4];
                             const uint32_t h0 = tf32_rna(b0), h1 = tf32_rna(b1);
                             const uint32_t l0 = __float_as_uint(b0 - __uint_as_float(h0)),
                                            l1 = __float_as_uint(b1 - __uint_as_float(h1));
@@ -1655,12 +1657,10 @@ __global__ void __launch_bounds__(256, 4) k_blk_tc(const BlkTask* __restrict__ t
                 }
             }
             if (more) store_v(buf ^ 1);
-            asm volatile("cp.async.wait_group 1;" ::: "memory");   // tile t+1 has landed
+            cp_async_wait_all();                  // tile t+1 has landed
             __syncthreads();                      // ... for every thread; tile t no longer read
-            issue_tile(t + 3);
             buf ^= 1;
         }
-        cp_async_wait_all();
         if (do0 && warp >= 4)
         {
             const int u = warp - 4;
@@ -1675,6 +1675,9 @@ __global__ void __launch_bounds__(256, 4) k_blk_tc(const BlkTask* __restrict__ t
         }
     }
 }
+
+template <int NV>
+constexpr int blk_tc_smem_bytes() { return (int) sizeof(BlkTcSmem); }
 
 // ------------------------------------ stored blocks on tcgen05 (TMEM accumulators)
 
@@ -2235,8 +2238,14 @@ cudaError_t launch_blk(int NV, const BlkTask* t, int n, const TA* arena, const d
                 }
                 return cudaGetLastError();
             }
-            if (NV == 16) k_blk_tc<16><<<n, 256, 0, st>>>(t, arena, XS, PS);
-            else k_blk_tc<8><<<n, 256, 0, st>>>(t, arena, XS, PS);
+            constexpr int b = blk_tc_smem_bytes<16>();
+            static const cudaError_t opt_in = [] {
+                cudaError_t e = allow_smem(k_blk_tc<16>, b);
+                return e == cudaSuccess ? allow_smem(k_blk_tc<8>, b) : e;
+            }();
+            if (opt_in != cudaSuccess) return opt_in;
+            if (NV == 16) k_blk_tc<16><<<n, 256, b, st>>>(t, arena, XS, PS);
+            else k_blk_tc<8><<<n, 256, b, st>>>(t, arena, XS, PS);
             return cudaGetLastError();
         }
     }
