@@ -939,6 +939,104 @@ __global__ void __launch_bounds__(128 / TPT, sizeof(T) == 4 ? 5 * TPT : 4 * TPT)
     }
 }
 
+// FP32 scalar kernels on the CUDA cores (the panels the tensor-core kernel does not
+// take, e.g. the narrow panels of the served form): k_jit's work split (one CTA of 64
+// threads per 128-target chunk, two targets per thread) with the thread's two targets
+// as one FP32x2 pair.  Sources are staged in shared memory with every coordinate and
+// input stored twice (the FP32x2 operand that meets both targets), so a source costs
+// packed instructions only.  FAR (admissible pairs): r^2 = |a|^2 + |b|^2 - 2 a.b as in
+// k_jit_tc; otherwise differences.  FP32 sums per 64-source tile, FP64 across tiles.
+template <int KID, int NV, bool FAR>
+__global__ void __launch_bounds__(64, NV >= 16 ? 8 : 10) k_jit2(const JitTarget* __restrict__ tgts, const JitSource* __restrict__ srcs,
+                                                 const float4* __restrict__ pts, KParam kp,
+                                                 const double* __restrict__ XS, double* __restrict__ PS,
+                                                 double* __restrict__ Y1)
+{
+    constexpr int TILE = 64, NT = 64;
+    __shared__ float4 s_p[TILE][2];          // {x, x, y, y}, {z, z, w, w}; w = |p|^2 (FAR)
+    __shared__ float2 s_in[TILE * NV];       // (in, in)
+    __shared__ double s_acc[2 * NV][NT];     // FP64 sums of the tile sums, [target q x NV + v][thread]
+    const JitTarget tg = tgts[blockIdx.x];
+    const float p0 = (float) kp.p0, c0 = (float) kp.c0;
+    float q0 = 0.f, q1 = 0.f;
+    if constexpr (FAR) ScalarFar<KID>::prep(p0, c0, q0, q1);
+    const int i0 = threadIdx.x, i1 = threadIdx.x + NT;
+    const bool v0 = i0 < tg.npt, v1 = i1 < tg.npt;
+    const float4 x0 = pts[tg.pt0 + (v0 ? i0 : 0)], x1 = pts[tg.pt0 + (v1 ? i1 : 0)];
+    float2 acc[NV];
+#pragma unroll
+    for (int v = 0; v < NV; v++)
+    {
+        acc[v] = make_float2(0.f, 0.f);
+        s_acc[v][threadIdx.x] = 0.0;
+        s_acc[NV + v][threadIdx.x] = 0.0;
+    }
+    const float2 m1 = make_float2(-1.f, -1.f);
+    for (int s = tg.src_beg; s < tg.src_end; s++)
+    {
+        const JitSource sc = srcs[s];
+        const float ax = x0.x + sc.sx, ay = x0.y + sc.sy, az = x0.z + sc.sz;
+        const float bx = x1.x + sc.sx, by = x1.y + sc.sy, bz = x1.z + sc.sz;
+        const float2 X = make_float2(ax, bx), Y = make_float2(ay, by), Z = make_float2(az, bz);
+        const float2 MX = make_float2(-2.f * ax, -2.f * bx), MY = make_float2(-2.f * ay, -2.f * by),
+                     MZ = make_float2(-2.f * az, -2.f * bz);
+        const float2 S2 = make_float2(ax * ax + ay * ay + az * az, bx * bx + by * by + bz * bz);
+        for (int j0 = 0; j0 < sc.npt; j0 += TILE)
+        {
+            const int nj = min(TILE, sc.npt - j0);
+            __syncthreads();
+            if (threadIdx.x < nj)
+            {
+                float4 q = pts[sc.pt0 + j0 + threadIdx.x];
+                if (FAR) q.w = q.x * q.x + q.y * q.y + q.z * q.z;
+                s_p[threadIdx.x][0] = make_float4(q.x, q.x, q.y, q.y);
+                s_p[threadIdx.x][1] = make_float4(q.z, q.z, q.w, q.w);
+            }
+            for (int i = threadIdx.x; i < nj * NV; i += NT)
+            {
+                const float x = (float) XS[(long long) (sc.in_row + j0) * NV + i];
+                s_in[i] = make_float2(x, x);
+            }
+            __syncthreads();
+#pragma unroll 2
+            for (int j = 0; j < nj; j++)
+            {
+                const float4 P0 = s_p[j][0], P1 = s_p[j][1];
+                float2 k;
+                if constexpr (FAR)
+                {
+                    float2 r2 = __fadd2_rn(S2, make_float2(P1.z, P1.w));
+                    r2 = __ffma2_rn(MZ, make_float2(P1.x, P1.y), r2);
+                    r2 = __ffma2_rn(MY, make_float2(P0.z, P0.w), r2);
+                    r2 = __ffma2_rn(MX, make_float2(P0.x, P0.y), r2);
+                    k = ScalarFar<KID>::f2(r2, q0, q1);
+                } else {
+                    const float2 dx = __ffma2_rn(make_float2(P0.x, P0.y), m1, X);
+                    const float2 dy = __ffma2_rn(make_float2(P0.z, P0.w), m1, Y);
+                    const float2 dz = __ffma2_rn(make_float2(P1.x, P1.y), m1, Z);
+                    k = ScalarF2<KID>::f2(__ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz))), p0, c0);
+                }
+#pragma unroll
+                for (int v = 0; v < NV; v++) acc[v] = __ffma2_rn(k, s_in[j * NV + v], acc[v]);
+            }
+#pragma unroll
+            for (int v = 0; v < NV; v++)
+            {
+                s_acc[v][threadIdx.x] += (double) acc[v].x;
+                s_acc[NV + v][threadIdx.x] += (double) acc[v].y;
+                acc[v] = make_float2(0.f, 0.f);
+            }
+        }
+    }
+    double* o = tg.out_y1 ? Y1 : PS;
+#pragma unroll
+    for (int v = 0; v < NV; v++)
+    {
+        if (v0) o[(long long) (tg.out_row + i0) * NV + v] = s_acc[v][threadIdx.x];
+        if (v1) o[(long long) (tg.out_row + i1) * NV + v] = s_acc[NV + v][threadIdx.x];
+    }
+}
+
 // ------------------------------------------------ JIT owner kernel, tensor cores
 
 // TF32 pieces of an FP32 value: hi = rna(x), lo = rna(x - hi); hi*b + lo*b recovers
@@ -2344,6 +2442,13 @@ static cudaError_t launch_jit_k(int NV, const JitTarget* tg, int n, const JitSou
     NV_DISPATCH(NV, {
         if constexpr (KD == 3 && NVc > 8)
             return cudaErrorInvalidValue;   // tensor kernels run in panels of <= 8 right-hand sides
+        else if constexpr (KD == 1 && sizeof(T) == 4)
+        {
+            // scalar FP32 kernels: the two targets of a thread as one FP32x2 pair
+            if (!use_shift) return cudaErrorInvalidValue;   // FP32 evaluation is re-centred
+            if (far) k_jit2<KID, NVc, true><<<n, 64, 0, st>>>(tg, sr, (const float4*) pts, kp, XS, PS, Y1);
+            else k_jit2<KID, NVc, false><<<n, 64, 0, st>>>(tg, sr, (const float4*) pts, kp, XS, PS, Y1);
+        }
         else if constexpr (KD * NVc <= 16 && sizeof(T) == 4)
             k_jit<KID, T, NVc, KD, 2><<<n, 64, 0, st>>>(tg, sr, p, kp, use_shift, XS, PS, Y1);
         else
