@@ -2336,14 +2336,13 @@ cudaError_t launch_blk(int NV, const BlkTask* t, int n, const TA* arena, const d
                 }
                 return cudaGetLastError();
             }
+            // the dynamic shared-memory opt-in is a per-device function attribute (cheap,
+            // and legal inside a stream capture), so it is set at every launch
             constexpr int b = blk_tc_smem_bytes<16>();
-            static const cudaError_t opt_in = [] {
-                cudaError_t e = allow_smem(k_blk_tc<16>, b);
-                return e == cudaSuccess ? allow_smem(k_blk_tc<8>, b) : e;
-            }();
-            if (opt_in != cudaSuccess) return opt_in;
-            if (NV == 16) k_blk_tc<16><<<n, 256, b, st>>>(t, arena, XS, PS);
-            else k_blk_tc<8><<<n, 256, b, st>>>(t, arena, XS, PS);
+            auto kern = NV == 16 ? k_blk_tc<16> : k_blk_tc<8>;
+            cudaError_t e = allow_smem(kern, b);
+            if (e != cudaSuccess) return e;
+            kern<<<n, 256, b, st>>>(t, arena, XS, PS);
             return cudaGetLastError();
         }
     }
@@ -2421,18 +2420,13 @@ static cudaError_t launch_jit_k(int NV, const JitTarget* tg, int n, const JitSou
             if (!ppts || !pin || !tiles) return cudaErrorInvalidValue;
             const float4* p4 = (const float4*) pts;
             constexpr int b = jit_tc_smem_bytes();
-            // the dynamic shared-memory opt-in, once per kernel (a function attribute, not a
-            // stream operation: legal inside a stream capture too)
-            static const cudaError_t opt_in = [] {
-                cudaError_t e = allow_smem(k_jit_tc<KID, 16, true>, b);
-                if (e == cudaSuccess) e = allow_smem(k_jit_tc<KID, 16, false>, b);
-                if (e == cudaSuccess) e = allow_smem(k_jit_tc<KID, 8, true>, b);
-                if (e == cudaSuccess) e = allow_smem(k_jit_tc<KID, 8, false>, b);
-                return e;
-            }();
-            if (opt_in != cudaSuccess) return opt_in;
-            if (NV == 16) (far ? k_jit_tc<KID, 16, true> : k_jit_tc<KID, 16, false>)<<<n, 256, b, st>>>(tg, tiles, p4, ppts, pin, kp, PS, Y1);
-            else (far ? k_jit_tc<KID, 8, true> : k_jit_tc<KID, 8, false>)<<<n, 256, b, st>>>(tg, tiles, p4, ppts, pin, kp, PS, Y1);
+            // the dynamic shared-memory opt-in is a per-device function attribute (cheap,
+            // and legal inside a stream capture), so it is set at every launch
+            auto kern = NV == 16 ? (far ? k_jit_tc<KID, 16, true> : k_jit_tc<KID, 16, false>)
+                                 : (far ? k_jit_tc<KID, 8, true> : k_jit_tc<KID, 8, false>);
+            cudaError_t e = allow_smem(kern, b);
+            if (e != cudaSuccess) return e;
+            kern<<<n, 256, b, st>>>(tg, tiles, p4, ppts, pin, kp, PS, Y1);
             return cudaGetLastError();
         }
     }
