@@ -30,7 +30,13 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "H2 matvecs/s (N=1M Matern-3/2 JIT, 16 RHS)"
+
+def headline_metric(n, nv):
+    """Metric name of the Matern-3/2 JIT workload at N points and nv right-hand sides
+    (the default run: "H2 matvecs/s (N=1M Matern-3/2 JIT, 16 RHS)")."""
+    return f"H2 matvecs/s (N={'1M' if n == 1_000_000 else n} Matern-3/2 JIT, {nv} RHS)"
+
+
 UNIT = "matvecs/s"
 PP_FILE = os.path.join("/tmp", "h2b200_pp_matern32_1e-6.dat")
 
@@ -179,7 +185,7 @@ def run_reference(args):
     sec = sum(ts) / len(ts)
     v = nv / sec
     line = {
-        "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": len(ts), "warmup": warm,
+        "metric": headline_metric(args.n, args.nvec), "value": v, "unit": UNIT, "n_gpus": world, "steps": len(ts), "warmup": warm,
         "ms_per_step": 1e3 * sec, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic", "impl": "reference",
         "config": {"workload": f"H2 JIT matmul, Matern-3/2 l=1, N={args.n}, reltol 1e-6, {nv} RHS N(0,1) "
@@ -304,7 +310,7 @@ def run_ours(args):
 
     if rank == 0:
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "metric": headline_metric(args.n, args.nvec), "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "fp32-mixed (FP32 kernel eval, FP64 accumulation)", "data": "synthetic",
             "config": {"workload": f"H2 JIT matmul, Matern-3/2 l=1, N={args.n} uniform in [0,N^(1/3)]^3, "
