@@ -165,7 +165,7 @@ struct h2gpu_image {
     int* d_y1_slots2 = nullptr;
     AsmTask* d_asm2 = nullptr;
     int* d_asm_slots2 = nullptr;
-    int n_owN = 0, n_owF = 0, n_jtN2 = 0, n_jtF2 = 0, n_y12 = 0;
+    int n_owN = 0, n_owF = 0, n_jtN2 = 0, n_jtF2 = 0, n_y12 = 0, n_asm2 = 0;
 
     // tuning (h2gpu_autotune) and captured graph (h2gpu_graph_capture)
     int jit_tc = 1;          // tensor-core JIT kernel for FP32 panels of 8 / 16
@@ -308,6 +308,9 @@ void node_centers(const h2gpu_desc* d, std::vector<double>& c)
 }
 
 // Everything build_plan produces on the host; uploaded by upload_plan once a device is known.
+// points of an owner set per pair-plan work unit (one CTA's rows)
+constexpr int kPairOwnerChunk = 128;
+
 struct HostPlan {
     std::vector<double> U;
     std::vector<UpTask> up;
@@ -423,7 +426,10 @@ int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
     // ---- partial slots
     long long ps = 0;
     auto alloc = [&](int rows) { long long r = ps; ps += rows; return (int) r; };
-    std::vector<std::vector<int>> y1s(n_node), asms(n_node), pair_y1, pair_asm;
+    std::vector<std::vector<int>> y1s(n_node), asms(n_node);
+    // pair plan slots of a node: (slot, first row) -- a slot of the node's full size
+    // (first row -1), or one of an owner unit covering rows [first row, + 128) of it
+    std::vector<std::vector<std::pair<int, int>>> pair_y1, pair_asm;
     std::vector<char> has_y1(n_node, 0);
     // Stored blocks: one task per block of up to RB rows (larger blocks split evenly
     // into tasks of a multiple of 64 rows).  A task's kernel walks its rows in chunks
@@ -653,7 +659,7 @@ int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
             // about 12 units per SM (148 SMs x 3 CTAs x 4 waves), so the largest owners
             // do not leave a tail.  Every unit has its own slot for a's side and one per
             // partner for b's side.
-            const int PCH = 128;
+            const int PCH = kPairOwnerChunk;
             double w_total = 0.0;
             for (int n = 0; n < n_node; n++)
             {
@@ -662,7 +668,7 @@ int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
             }
             const double w_cap = std::max(w_total / (148.0 * 3 * 4), 128.0 * 512.0);
             auto emit_owner = [&](std::vector<PairOwner>& out, int a, bool isJ, const std::vector<int>& parts,
-                                  std::vector<std::vector<int>>& lists) {
+                                  std::vector<std::vector<std::pair<int, int>>>& lists) {
                 const int na_all = isJ ? d->J_n[a] : npt_of(d, a);
                 const int pa = isJ ? jp0[a] : d->pt_cluster[2 * a];
                 const int in_a = isJ ? N + y0r[a] : mc[2 * a];
@@ -675,7 +681,7 @@ int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
                         PairOwner ow;
                         ow.na = na; ow.pa = pa + c0; ow.in_a = in_a + c0;
                         ow.out_a = alloc(na);
-                        lists[a].push_back(ow.out_a);
+                        lists[a].push_back({ow.out_a, c0});
                         ow.p_beg = (int) hp.partners.size();
                         double w = 0.0;
                         do {
@@ -685,7 +691,7 @@ int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
                             pp.nb = isJ ? d->J_n[b] : npt_of(d, b);
                             pp.in_b = isJ ? N + y0r[b] : mc[2 * b];
                             pp.out_b = alloc(pp.nb);
-                            lists[b].push_back(pp.out_b);
+                            lists[b].push_back({pp.out_b, -1});
                             pp.sx = (float) (ctr[3 * a] - ctr[3 * b]);
                             pp.sy = (float) (ctr[3 * a + 1] - ctr[3 * b + 1]);
                             pp.sz = (float) (ctr[3 * a + 2] - ctr[3 * b + 2]);
@@ -705,7 +711,7 @@ int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
             {
                 int n = d->leaf_nodes[i];
                 int s = alloc(npt_of(d, n));
-                pair_asm[n].push_back(s);
+                pair_asm[n].push_back({s, -1});
                 emit(hp.jtN2, n, d->pt_cluster[2 * n], npt_of(d, n), s, 0, std::vector<Src>{pts_src(n)});
             }
             for (int n = 0; n < n_node; n++)
@@ -716,13 +722,13 @@ int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
                 if (!left.empty() && d->J_n[n] > 0)
                 {
                     int s = alloc(d->U_ncol[n]);
-                    pair_y1[n].push_back(s);
+                    pair_y1[n].push_back({s, -1});
                     emit(hp.jtF2, n, jp0[n], d->J_n[n], s, 0, left);
                 }
                 if (!farL[n].empty())
                 {
                     int s = alloc(npt_of(d, n));
-                    pair_asm[n].push_back(s);
+                    pair_asm[n].push_back({s, -1});
                     emit(hp.jtF2, n, d->pt_cluster[2 * n], npt_of(d, n), s, 0, farL[n]);
                 }
             }
@@ -835,7 +841,7 @@ int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
             bool leaf = d->n_child[n] == 0;
             int dst = leaf ? alloc(nr) : y0r[d->children[n * d->max_child]];
             if (leaf) asms[n].push_back(dst);
-            if (leaf && !pair_asm.empty()) pair_asm[n].push_back(dst);
+            if (leaf && !pair_asm.empty()) pair_asm[n].push_back({dst, -1});
             const int RD = 64;       // downward tasks: one 64-row chunk of U each
             for (int r0 = 0; r0 < nr; r0 += RD)
             {
@@ -867,26 +873,33 @@ int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
     }
     if (im->has_pair)
     {
+        // one sum per 128-row piece of a node: the owner units' slots of that piece and
+        // the same piece of every full-size slot, in the order the slots were made
+        auto pieces = [&](const std::vector<std::pair<int, int>>& ent, int rows, std::vector<int>& slots, auto&& add) {
+            for (int c0 = 0; c0 < rows; c0 += kPairOwnerChunk)
+            {
+                const int beg = (int) slots.size();
+                for (const auto& e : ent)
+                    if (e.second < 0) slots.push_back(e.first + c0);
+                    else if (e.second == c0) slots.push_back(e.first);
+                add(c0, std::min(kPairOwnerChunk, rows - c0), beg, (int) slots.size());
+            }
+        };
         for (int n = 0; n < n_node; n++)
         {
             if (!has_y1[n]) continue;
-            Y1Task t;
-            t.row = y0r[n]; t.nrow = d->U_ncol[n];
-            t.slot_beg = (int) hp.y1_slots2.size();
-            for (int sl : pair_y1[n]) hp.y1_slots2.push_back(sl);
-            t.slot_end = (int) hp.y1_slots2.size();
-            hp.y1t2.push_back(t);
+            pieces(pair_y1[n], d->U_ncol[n], hp.y1_slots2, [&](int c0, int len, int b, int e) {
+                hp.y1t2.push_back(Y1Task{y0r[n] + c0, len, b, e});
+            });
         }
         for (int i = 0; i < d->n_leaf_node; i++)
         {
             int n = d->leaf_nodes[i];
-            AsmTask t;
-            t.row0 = mc[2 * n]; t.nrow = kd * npt_of(d, n);
-            t.slot_beg = (int) hp.at_slots2.size();
-            for (int sl : pair_asm[n]) hp.at_slots2.push_back(sl);
-            t.slot_end = (int) hp.at_slots2.size();
-            hp.at2.push_back(t);
+            pieces(pair_asm[n], kd * npt_of(d, n), hp.at_slots2, [&](int c0, int len, int b, int e) {
+                hp.at2.push_back(AsmTask{mc[2 * n] + c0, len, b, e});
+            });
         }
+        im->n_asm2 = (int) hp.at2.size();
         im->n_owN = (int) hp.owN.size(); im->n_owF = (int) hp.owF.size();
         im->n_jtN2 = (int) hp.jtN2.size(); im->n_jtF2 = (int) hp.jtF2.size(); im->n_y12 = (int) hp.y1t2.size();
     }
@@ -943,6 +956,262 @@ int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
     {
         im->B_elems = d->n_B > 0 ? d->B_ptr[d->n_B] : 0;
         im->D_elems = d->D_ptr[d->n_D];
+    }
+    return H2GPU_OK;
+}
+
+// ------------------------------------------------------------------ plan self-check
+
+// rows [beg, beg + n) of a space counted in cnt; false when they do not fit
+bool mark_rows(std::vector<int>& cnt, long long beg, long long n)
+{
+    if (n < 0 || beg < 0 || beg + n > (long long) cnt.size()) return false;
+    for (long long r = beg; r < beg + n; r++) cnt[r]++;
+    return true;
+}
+
+// Invariants of a built plan (h2gpu_plan_check); everything is recomputed from the
+// descriptor where it can be, so that the check does not restate the builder.
+int check_plan(const h2gpu_image* im, const h2gpu_desc* d, const HostPlan& hp, long long* counts)
+{
+    const int kd = d->krnl_dim, N = kd * d->n_point, n_node = d->n_node;
+    const long long Y0 = im->y0_rows, PSR = im->ps_rows;
+    const int* lvl = d->node_level;
+
+    // ---- upward: per node (keyed by its U offset) every column swept once
+    std::map<long long, std::vector<int>> ucols;
+    std::map<long long, std::pair<int, int>> ushape;   // U offset -> (rows, columns)
+    for (const UpTask& t : hp.up)
+    {
+        REQ(t.nrow >= 1 && t.ld >= 1 && t.nc >= 1 && t.nc <= 64 && t.c0 >= 0 && t.c0 % 64 == 0 && t.c0 + t.nc <= t.ld,
+            "plan: upward task with a bad column tile");
+        auto ins = ushape.emplace(t.u_off, std::make_pair(t.nrow, t.ld));
+        REQ(ins.first->second == std::make_pair(t.nrow, t.ld), "plan: upward tasks of one node disagree on its U");
+        std::vector<int>& c = ucols[t.u_off];
+        if (c.empty()) c.assign(t.ld, 0);
+        for (int j = t.c0; j < t.c0 + t.nc; j++) c[j]++;
+        REQ(t.out_row >= N && (long long) t.out_row + t.c0 + t.nc <= N + Y0, "plan: upward output outside y0");
+        REQ(t.in_row >= 0 && (long long) t.in_row + t.nrow <= N + Y0, "plan: upward input outside the input space");
+        REQ(t.in_row >= N || (long long) t.in_row + t.nrow <= N, "plan: upward input straddles x and y0");
+    }
+    long long u_total = 0;
+    for (const auto& kv : ucols)
+    {
+        for (int v : kv.second) REQ(v == 1, "plan: a column of U is swept %d times upward", v);
+        u_total += (long long) ushape[kv.first].first * ushape[kv.first].second;
+    }
+    REQ(u_total == (long long) im->U_elems, "plan: upward tasks cover %lld of %lld U elements", u_total,
+        (long long) im->U_elems);
+
+    // ---- downward: inside a node's U, disjoint; push-down rows written once and read only when written
+    std::vector<int> push(Y0, 0);
+    std::vector<std::pair<long long, long long>> spans;
+    for (const DownTask& t : hp.dn)
+    {
+        REQ(t.nrow >= 1 && t.nrow <= 64 && t.ncol >= 1, "plan: downward task with a bad shape");
+        auto it = ushape.upper_bound(t.u_off);
+        REQ(it != ushape.begin(), "plan: downward task before the U arena");
+        --it;
+        const long long base = it->first;
+        const int nr = it->second.first, nc = it->second.second;
+        REQ(nc == t.ncol && (t.u_off - base) % nc == 0 && (t.u_off - base) / nc + t.nrow <= nr,
+            "plan: downward task outside its node's U");
+        spans.push_back({t.u_off, t.u_off + (long long) t.nrow * t.ncol});
+        REQ(t.y1_row < 0 || (long long) t.y1_row + t.ncol <= Y0, "plan: downward y1 rows outside y0");
+        REQ(t.push_row < 0 || (long long) t.push_row + t.ncol <= Y0, "plan: downward push rows outside y0");
+        if (!t.dst_ps) REQ(mark_rows(push, t.dst_row, t.nrow), "plan: push-down rows outside y0");
+    }
+    std::sort(spans.begin(), spans.end());
+    for (size_t i = 1; i < spans.size(); i++) REQ(spans[i].first >= spans[i - 1].second, "plan: two downward tasks share rows of U");
+    for (int v : push) REQ(v <= 1, "plan: a push-down row is written %d times", v);
+    for (const DownTask& t : hp.dn)
+        if (t.push_row >= 0)
+            for (int r = 0; r < t.ncol; r++) REQ(push[t.push_row + r] == 1, "plan: a push-down row is read but never written");
+
+    // ---- partial space, y1 rows and assembly of one plan
+    auto check_space = [&](const char* plan, const std::vector<std::pair<long long, long long>>& prod,
+                           const std::vector<std::pair<long long, long long>>& y1w, const std::vector<AsmTask>& at,
+                           const std::vector<int>& at_slots, const std::vector<Y1Task>& y1t,
+                           const std::vector<int>& y1_slots) -> int {
+        std::vector<int> w(PSR, 0), r(PSR, 0), y1(Y0, 0), out(N, 0);
+        for (const auto& p : prod) REQ(mark_rows(w, p.first, p.second), "plan (%s): a slot lies outside the partial space", plan);
+        for (const AsmTask& t : at)
+        {
+            REQ(mark_rows(out, t.row0, t.nrow), "plan (%s): assembly rows outside the output", plan);
+            for (int k = t.slot_beg; k < t.slot_end; k++)
+                REQ(mark_rows(r, at_slots[k], t.nrow), "plan (%s): an assembly slot lies outside the partial space", plan);
+        }
+        for (const Y1Task& t : y1t)
+        {
+            REQ(mark_rows(y1, t.row, t.nrow), "plan (%s): y1 sum rows outside y0", plan);
+            for (int k = t.slot_beg; k < t.slot_end; k++)
+                REQ(mark_rows(r, y1_slots[k], t.nrow), "plan (%s): a y1 slot lies outside the partial space", plan);
+        }
+        for (const auto& p : y1w) REQ(mark_rows(y1, p.first, p.second), "plan (%s): y1 rows outside y0", plan);
+        for (long long i = 0; i < PSR; i++)
+            REQ(w[i] == r[i] && w[i] <= 1, "plan (%s): partial row %lld written %d times, summed %d times", plan, i, w[i], r[i]);
+        for (int v : out) REQ(v == 1, "plan (%s): an output row is assembled %d times", plan, v);
+        for (int v : y1) REQ(v <= 1, "plan (%s): a y1 row is written %d times", plan, v);
+        for (const DownTask& t : hp.dn)
+            if (t.y1_row >= 0)
+                for (int k = 0; k < t.ncol; k++) REQ(y1[t.y1_row + k] == 1, "plan (%s): a y1 row is read but never written", plan);
+        return H2GPU_OK;
+    };
+    std::vector<std::pair<long long, long long>> down_ps;
+    for (const DownTask& t : hp.dn)
+        if (t.dst_ps) down_ps.push_back({t.dst_row, t.nrow});
+    std::vector<std::pair<long long, long long>> prod = down_ps, y1w;
+    for (const std::vector<BlkTask>* v : {&hp.blkB, &hp.blkD})
+        for (const BlkTask& t : *v)
+        {
+            REQ(t.nrow >= 1 && t.ncol >= 1, "plan: stored-block task with a bad shape");
+            if (t.out0_row >= 0) prod.push_back({t.out0_row, t.nrow});
+            if (t.out1_row >= 0) prod.push_back({t.out1_row, t.ncol});
+        }
+    for (const std::vector<JitTarget>* v : {&hp.jtN, &hp.jtF})
+        for (const JitTarget& t : *v) (t.out_y1 ? y1w : prod).push_back({t.out_row, (long long) kd * t.npt});
+    TRY(check_space("one-sided", prod, y1w, hp.at, hp.at_slots, hp.y1t, hp.y1_slots));
+
+    long long pairs_plan = 0;
+    if (d->BD_JIT)
+    {
+        // ---- (target, source) point pairs against H2Pack's pair lists
+        std::vector<long long> jp0(n_node, 0);
+        long long np = d->n_point;
+        for (int n = 0; n < n_node; n++) { jp0[n] = np; np += d->J_n[n]; }
+        auto npt = [&](int n) { return (long long) npt_of(d, n); };
+        long long near_o = 0, far_o = 0, near_u = 0, far_u = 0;   // ordered / unordered (pair plan) counts
+        for (int i = 0; i < d->n_leaf_node; i++) { const long long p = npt(d->leaf_nodes[i]); near_o += p * p; near_u += p * p; }
+        for (int i = 0; i < d->n_r_inadm_pair; i++)
+        {
+            const long long q = npt(d->r_inadm_pairs[2 * i]) * npt(d->r_inadm_pairs[2 * i + 1]);
+            near_o += 2 * q; near_u += q;
+        }
+        for (int i = 0; i < d->n_r_adm_pair; i++)
+        {
+            const int a = d->r_adm_pairs[2 * i], b = d->r_adm_pairs[2 * i + 1];
+            const long long q = lvl[a] == lvl[b] ? (long long) d->J_n[a] * d->J_n[b]
+                              : lvl[a] > lvl[b] ? (long long) d->J_n[a] * npt(b) : (long long) d->J_n[b] * npt(a);
+            far_o += 2 * q;
+            far_u += lvl[a] == lvl[b] ? q : 2 * q;
+        }
+        auto pairs_of = [&](const std::vector<JitTarget>& v) {
+            long long s = 0;
+            for (const JitTarget& t : v)
+            {
+                long long ns = 0;
+                for (int k = t.src_beg; k < t.src_end; k++) ns += hp.js[k].npt;
+                s += (long long) t.npt * ns;
+            }
+            return s;
+        };
+        REQ(pairs_of(hp.jtN) == near_o, "plan: near field evaluates %lld point pairs, the pair lists imply %lld",
+            pairs_of(hp.jtN), near_o);
+        REQ(pairs_of(hp.jtF) == far_o, "plan: far field evaluates %lld point pairs, the pair lists imply %lld",
+            pairs_of(hp.jtF), far_o);
+        pairs_plan = near_o + far_o;
+
+        // ---- sources, tiles and panel groups
+        for (const JitSource& s : hp.js)
+        {
+            REQ(s.npt >= 1 && s.pt0 >= 0 && (long long) s.pt0 + s.npt <= np, "plan: JIT source outside the point space");
+            if (s.pt0 < d->n_point) REQ(s.in_row == kd * s.pt0, "plan: JIT source input row does not match its points");
+            else REQ(s.in_row >= N && (long long) s.in_row + (long long) kd * s.npt <= N + Y0, "plan: JIT source input outside y0");
+            if (kd == 1)
+                for (int j = 0; j < s.npt; j += 8)
+                {
+                    const int g = s.grp + j / 8;
+                    REQ(g >= 0 && g < (int) hp.pg.size(), "plan: panel group outside the panels");
+                    const PanelGroup& G = hp.pg[g];
+                    REQ(G.pt0 == s.pt0 + j && G.row0 == s.in_row + j && G.nvalid == std::min(8, s.npt - j),
+                        "plan: panel groups do not cover a source set in order");
+                }
+        }
+        for (const std::vector<JitTarget>* v : {&hp.jtN, &hp.jtF, &hp.jtN2, &hp.jtF2})
+            for (const JitTarget& t : *v)
+            {
+                REQ(t.npt >= 1 && t.npt <= 128, "plan: JIT target chunk of %d points", t.npt);
+                int k = t.tile_beg;
+                for (int si = t.src_beg; si < t.src_end; si++)
+                    for (int j0 = 0; j0 < hp.js[si].npt; j0 += 128, k++)
+                    {
+                        REQ(k < t.tile_end && k < (int) hp.tiles.size(), "plan: a target has too few source tiles");
+                        const TileRec& T = hp.tiles[k];
+                        const int nj = std::min(128, hp.js[si].npt - j0);
+                        REQ(T.nj == nj && T.ng == (nj + 7) / 8 && T.gb == hp.js[si].grp + j0 / 8,
+                            "plan: source tiles do not cover a source set in order");
+                    }
+                REQ(k == t.tile_end, "plan: a target has too many source tiles");
+            }
+
+        // ---- pair plan: every unordered pair owned once, both sides summed once
+        if (im->has_pair)
+        {
+            std::map<long long, int> set_of;   // first point of a set -> node (leaf point sets, skeleton sets)
+            for (int i = 0; i < d->n_leaf_node; i++) set_of[d->pt_cluster[2 * d->leaf_nodes[i]]] = d->leaf_nodes[i];
+            for (int n = 0; n < n_node; n++)
+                if (d->J_n[n] > 0) set_of[jp0[n]] = n;
+            auto node_at = [&](long long p) {
+                auto it = set_of.upper_bound(p);
+                return it == set_of.begin() ? -1 : std::prev(it)->second;
+            };
+            std::map<std::pair<int, int>, long long> cover;   // (owner, partner) -> owner points covered
+            long long pairs_u = 0;
+            std::vector<std::pair<long long, long long>> prod2 = down_ps;
+            for (const std::vector<PairOwner>* v : {&hp.owN, &hp.owF})
+                for (const PairOwner& o : *v)
+                {
+                    const int a = node_at(o.pa);
+                    REQ(a >= 0 && o.na >= 1 && o.p_beg <= o.p_end && o.p_end <= (int) hp.partners.size(), "plan: bad pair owner");
+                    prod2.push_back({o.out_a, o.na});
+                    for (int k = o.p_beg; k < o.p_end; k++)
+                    {
+                        const PairPartner& pp = hp.partners[k];
+                        const int b = node_at(pp.pb);
+                        REQ(b >= 0, "plan: pair partner is not a point set");
+                        cover[{a, b}] += o.na;
+                        pairs_u += (long long) o.na * pp.nb;
+                        prod2.push_back({pp.out_b, pp.nb});
+                    }
+                }
+            std::map<std::pair<int, int>, long long> want;   // unordered pairs the pair plan must own
+            for (int i = 0; i < d->n_r_inadm_pair; i++)
+            {
+                const int a = d->r_inadm_pairs[2 * i], b = d->r_inadm_pairs[2 * i + 1];
+                want[{std::min(a, b), std::max(a, b)}] = 0;
+            }
+            for (int i = 0; i < d->n_r_adm_pair; i++)
+            {
+                const int a = d->r_adm_pairs[2 * i], b = d->r_adm_pairs[2 * i + 1];
+                if (lvl[a] == lvl[b] && d->J_n[a] > 0 && d->J_n[b] > 0) want[{std::min(a, b), std::max(a, b)}] = 0;
+            }
+            for (const auto& kv : cover)
+            {
+                const int a = kv.first.first, b = kv.first.second;
+                auto it = want.find({std::min(a, b), std::max(a, b)});
+                REQ(it != want.end(), "plan: the pair plan owns nodes %d and %d, which are not a pair", a, b);
+                REQ(cover.count({b, a}) == 0, "plan: the pair of nodes %d and %d is owned both ways", a, b);
+                it->second++;
+            }
+            for (const auto& kv : want) REQ(kv.second == 1, "plan: the pair of nodes %d and %d is not owned", kv.first.first, kv.first.second);
+            for (const std::vector<JitTarget>* v : {&hp.jtN2, &hp.jtF2})
+                for (const JitTarget& t : *v) prod2.push_back({t.out_row, (long long) t.npt});
+            pairs_u += pairs_of(hp.jtN2) + pairs_of(hp.jtF2);
+            REQ(pairs_u == near_u + far_u, "plan: the pair plan evaluates %lld point pairs, the pair lists imply %lld",
+                pairs_u, near_u + far_u);
+            TRY(check_space("pair", prod2, {}, hp.at2, hp.at_slots2, hp.y1t2, hp.y1_slots2));
+        }
+    }
+    if (counts)
+    {
+        counts[0] = (long long) hp.up.size();
+        counts[1] = (long long) hp.dn.size();
+        counts[2] = (long long) (hp.blkB.size() + hp.blkD.size());
+        counts[3] = (long long) (hp.jtN.size() + hp.jtF.size());
+        counts[4] = (long long) hp.tiles.size();
+        counts[5] = (long long) hp.pg.size();
+        counts[6] = PSR;
+        counts[7] = pairs_plan;
     }
     return H2GPU_OK;
 }
@@ -1107,7 +1376,7 @@ int run_panel(h2gpu_image* im, int NV, int nv, const double* X, long long x_rs, 
             CK(launch_down<float>(NV, im->d_dn + b, n, im->d_U32, im->d_Y1, im->d_PS, im->d_PUSH, s, sweep_tc(im)));
         }
         if (timed) CK(cudaEventRecord(e[5], s));
-        CK(launch_asm(NV, im->d_asm2, im->n_leaf, im->d_asm_slots2, im->d_PS, im->d_fwd, Y, y_rs, y_cs, nv, s));
+        CK(launch_asm(NV, im->d_asm2, im->n_asm2, im->d_asm_slots2, im->d_PS, im->d_fwd, Y, y_rs, y_cs, nv, s));
         if (timed) CK(cudaEventRecord(e[6], s));
         im->st.n_launches += 9 + (long long) (im->up_beg.size() - 1) + (long long) (im->dn_beg.size() - 1);
         return H2GPU_OK;
@@ -1456,6 +1725,17 @@ H2G_API int h2gpu_reset_stats(h2gpu_image* im)
     im->st.ms_total = 0;
     for (double& m : im->st.ms_phase) m = 0;
     return H2GPU_OK;
+}
+
+H2G_API int h2gpu_plan_check(const h2gpu_desc* desc, long long* counts)
+{
+    TRY(validate(desc));
+    h2gpu_image* im = new h2gpu_image();   // plan fields only: no stream, event or allocation is made
+    HostPlan hp;
+    int st = build_plan(im, desc, hp);
+    if (st == H2GPU_OK) st = check_plan(im, desc, hp, counts);
+    delete im;
+    return st;
 }
 
 H2G_API size_t h2gpu_image_bytes(const h2gpu_image* im)

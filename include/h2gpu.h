@@ -284,6 +284,27 @@ int h2gpu_reset_stats(h2gpu_image *img);
 size_t h2gpu_image_bytes(const h2gpu_image *img);
 
 /*
+ * Host-only self-check of the apply plan: builds the plan h2gpu_image_create would
+ * upload for desc (no device is touched, no GPU is needed) and verifies that
+ *   - the upward tasks sweep every column of every node's U once and the downward
+ *     tasks every row at most once, inside the node's U;
+ *   - every partial-space row is written by one producer and summed by one
+ *     consumer, every push-down / y1 row a downward task reads is written, and the
+ *     assembly writes every output row once (for each plan an image holds);
+ *   - JIT: the (target, source) point pairs the plan evaluates are the pairs
+ *     H2Pack's pair lists imply (near: each leaf with itself and its inadmissible
+ *     partners; far: the admissible pairs, skeleton or leaf points as the levels
+ *     say), the source tiles and 8-point panel groups cover every source set once
+ *     in order, and the pair plan (scalar kernels) owns every unordered pair once.
+ * counts (H2GPU_PLAN_COUNTS entries, may be NULL): upward tasks, downward tasks,
+ * stored-block tasks, JIT target chunks, source tiles, panel groups, partial-space
+ * rows, JIT point pairs evaluated per right-hand side.  Returns H2GPU_OK or
+ * H2GPU_ERR_INVALID naming the first violated invariant in h2gpu_last_error().
+ */
+#define H2GPU_PLAN_COUNTS 8
+int h2gpu_plan_check(const h2gpu_desc *desc, long long *counts);
+
+/*
  * FP64 direct sum on the device: y_t = sum_s K(x_t, x_s) v_s for n_trg targets
  * and n_src sources (coordinates xpt_dim x n, ld = n, host arrays; values are
  * krnl_dim-interleaved per point as in the H2 vectors).

@@ -6,7 +6,9 @@ source tiles of up to 128 points.  These cases put the padding and the tile edge
 everywhere: leaves of a few points (every group partial), leaves just past a multiple
 of 8, and leaves wider than one 128-point target chunk (chunks whose last warps hold
 no targets).  The mixed result must stay as close to the FP64 GPU result as on the
-regular shapes, for panels of 8 and 16 right-hand sides and for the pair variant.
+regular shapes, for panels of 8 and 16 right-hand sides and for the pair variant
+(including owner sets of more than 128 points, which the pair plan walks in pieces
+of 128 and sums piece by piece).
 """
 import numpy as np
 import pytest
@@ -55,5 +57,28 @@ def test_pair_variant_on_edge_shapes(leaf):
         Y64 = H.matmul(X)
         assert rel(Ytc, Y64) < 2e-6
         assert rel(Ypair, Y64) < 2e-6
+    finally:
+        H.close()
+
+
+@pytest.mark.parametrize("kernel,n,leaf", [("coulomb", 20000, 400), ("gaussian", 8000, 200)])
+def test_pair_variant_on_sets_wider_than_a_unit(kernel, n, leaf):
+    H = H2Matrix(kernel, make_points(kernel, n, 5), KERNEL_PARAMS[kernel], 1e-6, BD_JIT=1, max_leaf_points=leaf,
+                 precision="mixed")
+    try:
+        d = H.describe()
+        widest = max(max(d.J_n[i] for i in range(d.n_node)),
+                     max(d.pt_cluster[2 * i + 1] - d.pt_cluster[2 * i] + 1 for i in range(d.n_node)))
+        assert widest > 128
+        X = np.random.default_rng(7).standard_normal((H.N, 16))
+        img = H.image()
+        img.set_jit_variant("pair")
+        Ypair = H.matmul(X)
+        img.set_jit_variant("tc")
+        Ytc = H.matmul(X)
+        H.set_precision("fp64")
+        Y64 = H.matmul(X)
+        assert rel(Ytc, Y64) < 2e-6
+        assert rel(Ypair, Y64) < 2e-6, rel(Ypair, Y64)
     finally:
         H.close()

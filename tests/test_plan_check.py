@@ -1,0 +1,94 @@
+"""Host-only self-check of the apply plan (h2gpu_plan_check): no GPU needed.
+
+The plan is what h2gpu_image_create uploads: the upward / downward tasks, the
+partial-space slots and the sums that read them, and for JIT images the (target,
+source) point pairs with their source tiles and panel groups, plus the pair plan that
+evaluates every unordered pair once.  The library checks these invariants itself.
+The tests below check two further things:
+
+- The number of point pairs the plan evaluates matches H2Pack's pair lists. The count
+  is recomputed here in Python from the descriptor: near field each leaf with itself
+  and its inadmissible partners; far field the admissible pairs, skeleton or leaf
+  points as the node levels say (src/H2Pack_matvec.c:586-764, :1002-1145).
+- The plan's sizes (tasks, slots) fit the representation.
+
+The shapes cover the golden fixtures and freshly built trees whose point and skeleton
+sets are wider than one 128-point pair-plan unit.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from conftest import KERNEL_PARAMS, make_points
+from oracle import oracle as O
+from h2pack_b200 import _abi
+from h2pack_b200.h2pack import H2Matrix
+from test_host_validation import arrays
+import os
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def plan_check(desc):
+    lib = _abi.libh2gpu()
+    cnt = (C.c_longlong * 8)()
+    st = lib.h2gpu_plan_check(C.byref(desc), cnt)
+    assert st == _abi.H2GPU_OK, lib.h2gpu_last_error().decode()
+    return list(cnt)
+
+
+def pairs_from_lists(d):
+    """Ordered (target point, source point) pairs of one JIT apply, from the pair lists."""
+    npt = lambda n: d.pt_cluster[2 * n + 1] - d.pt_cluster[2 * n] + 1
+    lvl = lambda n: d.node_level[n]
+    s = sum(npt(d.leaf_nodes[i]) ** 2 for i in range(d.n_leaf_node))
+    s += sum(2 * npt(d.r_inadm_pairs[2 * i]) * npt(d.r_inadm_pairs[2 * i + 1]) for i in range(d.n_r_inadm_pair))
+    for i in range(d.n_r_adm_pair):
+        a, b = d.r_adm_pairs[2 * i], d.r_adm_pairs[2 * i + 1]
+        if lvl(a) == lvl(b):
+            s += 2 * d.J_n[a] * d.J_n[b]
+        elif lvl(a) > lvl(b):
+            s += 2 * d.J_n[a] * npt(b)
+        else:
+            s += 2 * d.J_n[b] * npt(a)
+    return s
+
+
+def check(d):
+    c = plan_check(d)
+    n_up, n_dn, n_blk, n_jt, n_tiles, n_pg, ps_rows, pairs = c
+    assert ps_rows > 0
+    if d.n_r_adm_pair > 0:
+        assert n_up > 0 and n_dn > 0
+    if d.BD_JIT:
+        assert n_blk == 0 and n_jt > 0 and n_tiles > 0
+        assert pairs == pairs_from_lists(d)
+        if d.krnl_dim == 1:
+            assert n_pg > 0
+    else:
+        assert n_blk >= d.n_B + d.n_D - d.n_leaf_node and n_jt == 0 and pairs == 0
+    return c
+
+
+@pytest.mark.parametrize("name", ["coulomb_aot", "rpy_aot", "coulomb_jit", "gaussian_jit", "matern32_jit", "rpy_jit"])
+def test_plan_of_golden_fixtures(name):
+    h = O.DescHolder(arrays(os.path.join(GOLDEN, name + ".npz")))
+    check(h.desc)
+
+
+@pytest.mark.parametrize("kernel,n,leaf,jit", [
+    ("coulomb", 20000, 400, 1),     # leaves and skeletons wider than 128 points
+    ("gaussian", 8000, 200, 1),
+    ("matern32", 6000, 300, 1),
+    ("matern32", 1500, 3, 1),       # leaves of a few points: every panel group partial
+    ("rpy", 3000, 100, 1),
+    ("coulomb", 8000, 200, 0),
+    ("rpy", 3000, 100, 0),
+])
+def test_plan_of_built_trees(kernel, n, leaf, jit):
+    H = H2Matrix(kernel, make_points(kernel, n, 5), KERNEL_PARAMS[kernel], 1e-6, BD_JIT=jit, max_leaf_points=leaf)
+    try:
+        check(H.describe())
+    finally:
+        H.close()
