@@ -2010,6 +2010,13 @@ int merge_descs(const h2gpu_desc* ds, int n, MergedDesc& m)
 
 }  // namespace
 
+H2G_API int h2gpu_batch_plan_check(const h2gpu_desc* descs, int n_desc, long long* counts)
+{
+    MergedDesc m;
+    TRY(merge_descs(descs, n_desc, m));
+    return h2gpu_plan_check(&m.d, counts);
+}
+
 H2G_API int h2gpu_batch_create(const h2gpu_desc* descs, int n_desc, const h2gpu_options* opt, h2gpu_image** out)
 {
     if (!out) return fail(H2GPU_ERR_INVALID, "out is NULL");

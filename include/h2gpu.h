@@ -303,6 +303,8 @@ size_t h2gpu_image_bytes(const h2gpu_image *img);
  */
 #define H2GPU_PLAN_COUNTS 8
 int h2gpu_plan_check(const h2gpu_desc *desc, long long *counts);
+/* The same for the merged representation h2gpu_batch_create would build from descs. */
+int h2gpu_batch_plan_check(const h2gpu_desc *descs, int n_desc, long long *counts);
 
 /*
  * FP64 direct sum on the device: y_t = sum_s K(x_t, x_s) v_s for n_trg targets

@@ -92,3 +92,33 @@ def test_plan_of_built_trees(kernel, n, leaf, jit):
         check(H.describe())
     finally:
         H.close()
+
+
+def batch_plan_check(descs):
+    lib = _abi.libh2gpu()
+    arr = (_abi.Desc * len(descs))(*descs)
+    cnt = (C.c_longlong * 8)()
+    st = lib.h2gpu_batch_plan_check(arr, len(descs), cnt)
+    assert st == _abi.H2GPU_OK, lib.h2gpu_last_error().decode()
+    return list(cnt)
+
+
+@pytest.mark.parametrize("kernel,jit", [("coulomb", 1), ("matern32", 1), ("rpy", 1), ("coulomb", 0), ("rpy", 0)])
+def test_batched_plan_is_the_union_of_its_members(kernel, jit):
+    """Members of different depths (and so different min_adm / max_level) merged into
+    one image: the merged plan passes the self-check, and its tasks, tiles, panel
+    groups and evaluated point pairs are the sums of the members' own (nothing is
+    lost or paired across members)."""
+    shapes = [(1500, 100), (6000, 60), (3000, 300)]
+    Hs = [H2Matrix(kernel, make_points(kernel, n, 40 + i), KERNEL_PARAMS[kernel], 1e-6, BD_JIT=jit,
+                   max_leaf_points=leaf) for i, (n, leaf) in enumerate(shapes)]
+    try:
+        ds = [H.describe() for H in Hs]
+        assert len({(d.max_level, d.min_adm_level) for d in ds}) > 1
+        own = [check(d) for d in ds]
+        merged = batch_plan_check(ds)
+        for k in (0, 1, 2, 3, 4, 5, 7):   # all but the partial-space size (pair units depend on the total work)
+            assert merged[k] == sum(c[k] for c in own), k
+    finally:
+        for H in Hs:
+            H.close()
