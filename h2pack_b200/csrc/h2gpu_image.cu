@@ -1065,6 +1065,10 @@ int check_plan(const h2gpu_image* im, const h2gpu_desc* d, const HostPlan& hp, l
         for (const BlkTask& t : *v)
         {
             REQ(t.nrow >= 1 && t.ncol >= 1, "plan: stored-block task with a bad shape");
+            const long long elems = (long long) (v == &hp.blkB ? im->B_elems : im->D_elems);
+            REQ(t.a_off >= 0 && t.a_off + (long long) t.nrow * t.ncol <= elems, "plan: stored-block task outside its arena");
+            REQ(t.in0_row >= 0 && (long long) t.in0_row + t.ncol <= N + Y0, "plan: stored-block input outside the input space");
+            REQ(t.in1_row >= 0 && (long long) t.in1_row + t.nrow <= N + Y0, "plan: stored-block input outside the input space");
             if (t.out0_row >= 0) prod.push_back({t.out0_row, t.nrow});
             if (t.out1_row >= 0) prod.push_back({t.out1_row, t.ncol});
         }
@@ -1131,6 +1135,8 @@ int check_plan(const h2gpu_image* im, const h2gpu_desc* d, const HostPlan& hp, l
             for (const JitTarget& t : *v)
             {
                 REQ(t.npt >= 1 && t.npt <= 128, "plan: JIT target chunk of %d points", t.npt);
+                REQ(t.pt0 >= 0 && (long long) t.pt0 + t.npt <= np, "plan: JIT target outside the point space");
+                REQ(t.src_beg >= 0 && t.src_beg <= t.src_end && t.src_end <= (int) hp.js.size(), "plan: JIT target sources out of range");
                 int k = t.tile_beg;
                 for (int si = t.src_beg; si < t.src_end; si++)
                     for (int j0 = 0; j0 < hp.js[si].npt; j0 += 128, k++)
@@ -1162,13 +1168,17 @@ int check_plan(const h2gpu_image* im, const h2gpu_desc* d, const HostPlan& hp, l
                 for (const PairOwner& o : *v)
                 {
                     const int a = node_at(o.pa);
-                    REQ(a >= 0 && o.na >= 1 && o.p_beg <= o.p_end && o.p_end <= (int) hp.partners.size(), "plan: bad pair owner");
+                    REQ(a >= 0 && o.na >= 1 && o.na <= kPairOwnerChunk && o.p_beg <= o.p_end &&
+                            o.p_end <= (int) hp.partners.size(), "plan: bad pair owner");
+                    REQ(o.pa + o.na <= np && o.in_a >= 0 && (long long) o.in_a + o.na <= N + Y0, "plan: pair owner out of range");
                     prod2.push_back({o.out_a, o.na});
                     for (int k = o.p_beg; k < o.p_end; k++)
                     {
                         const PairPartner& pp = hp.partners[k];
                         const int b = node_at(pp.pb);
                         REQ(b >= 0, "plan: pair partner is not a point set");
+                        REQ(pp.nb >= 1 && pp.pb + pp.nb <= np && pp.in_b >= 0 && (long long) pp.in_b + pp.nb <= N + Y0,
+                            "plan: pair partner out of range");
                         cover[{a, b}] += o.na;
                         pairs_u += (long long) o.na * pp.nb;
                         prod2.push_back({pp.out_b, pp.nb});

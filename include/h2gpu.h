@@ -295,7 +295,9 @@ size_t h2gpu_image_bytes(const h2gpu_image *img);
  *     H2Pack's pair lists imply (near: each leaf with itself and its inadmissible
  *     partners; far: the admissible pairs, skeleton or leaf points as the levels
  *     say), the source tiles and 8-point panel groups cover every source set once
- *     in order, and the pair plan (scalar kernels) owns every unordered pair once.
+ *     in order, and the pair plan (scalar kernels) owns every unordered pair once;
+ *   - every index a kernel takes from a task record (block offsets, input rows, point
+ *     ranges) lies inside the array it indexes (kernels do not bounds-check them).
  * counts (H2GPU_PLAN_COUNTS entries, may be NULL): upward tasks, downward tasks,
  * stored-block tasks, JIT target chunks, source tiles, panel groups, partial-space
  * rows, JIT point pairs evaluated per right-hand side.  Returns H2GPU_OK or
