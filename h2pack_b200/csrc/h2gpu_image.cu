@@ -1567,6 +1567,12 @@ H2G_API int h2gpu_image_create(const h2gpu_desc* desc, const h2gpu_options* opt,
     }
     HostPlan hp;
     int pst = build_plan(im, desc, hp);   // all structural checks happen here, before any CUDA call
+    if (pst == H2GPU_OK)
+    {
+        // the plan self-check of h2gpu_plan_check, on request (the test suite sets it)
+        const char* e = getenv("H2G_PLAN_CHECK");
+        if (e && e[0] == '1') pst = check_plan(im, desc, hp, nullptr);
+    }
     if (pst != H2GPU_OK) { delete im; return pst; }
     int ndev = 0;
     cudaError_t e = cudaGetDeviceCount(&ndev);

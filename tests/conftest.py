@@ -8,6 +8,10 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
+# every image the tests create first passes the host-side plan self-check
+# (h2gpu_plan_check: slots written and summed once, tasks inside their arrays, ...)
+os.environ.setdefault("H2G_PLAN_CHECK", "1")
+
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200, sm_100a)")
