@@ -1115,10 +1115,96 @@ int check_plan(const h2gpu_image* im, const h2gpu_desc* d, const HostPlan& hp, l
             pairs_of(hp.jtF), far_o);
         pairs_plan = near_o + far_o;
 
+        // ---- each target's source sets are exactly the ones its node's pair lists name
+        {
+            std::map<long long, int> leaf_at, jset_at;   // first point of a leaf's points / a skeleton -> node
+            for (int i = 0; i < d->n_leaf_node; i++) leaf_at[d->pt_cluster[2 * d->leaf_nodes[i]]] = d->leaf_nodes[i];
+            for (int n = 0; n < n_node; n++)
+                if (d->J_n[n] > 0) jset_at[jp0[n]] = n;
+            // a set as (node, skeleton?) from its first point; -1 when it is neither
+            auto set_key = [&](long long pt0, int npt_) -> std::pair<int, int> {
+                if (pt0 < d->n_point)
+                {
+                    auto it = leaf_at.find(pt0);
+                    return (it != leaf_at.end() && npt(it->second) == npt_) ? std::make_pair(it->second, 0) : std::make_pair(-1, 0);
+                }
+                auto it = jset_at.find(pt0);
+                return (it != jset_at.end() && d->J_n[it->second] == npt_) ? std::make_pair(it->second, 1) : std::make_pair(-1, 1);
+            };
+            // expected sources of every (node, skeleton?) target set
+            std::map<std::pair<int, int>, std::vector<std::pair<int, int>>> near_src, far_src;
+            for (int i = 0; i < d->n_leaf_node; i++)
+            {
+                const int n = d->leaf_nodes[i];
+                near_src[{n, 0}].push_back({n, 0});
+            }
+            for (int i = 0; i < d->n_r_inadm_pair; i++)
+            {
+                const int a = d->r_inadm_pairs[2 * i], b = d->r_inadm_pairs[2 * i + 1];
+                near_src[{a, 0}].push_back({b, 0});
+                near_src[{b, 0}].push_back({a, 0});
+            }
+            for (int i = 0; i < d->n_r_adm_pair; i++)
+            {
+                const int a = d->r_adm_pairs[2 * i], b = d->r_adm_pairs[2 * i + 1];
+                // empty skeletons contribute nothing and are left out of the expected lists
+                auto add = [&](int t, int ts, int u, int us) {
+                    if (!us || d->J_n[u] > 0) far_src[{t, ts}].push_back({u, us});
+                };
+                if (lvl[a] == lvl[b]) { add(a, 1, b, 1); add(b, 1, a, 1); }
+                else if (lvl[a] > lvl[b]) { add(a, 1, b, 0); add(b, 0, a, 1); }
+                else { add(a, 0, b, 1); add(b, 1, a, 0); }
+            }
+            auto match = [&](const char* field, const std::vector<JitTarget>& v,
+                             std::map<std::pair<int, int>, std::vector<std::pair<int, int>>>& want) -> int {
+                std::map<std::pair<int, int>, long long> rows;   // target set -> points covered by its chunks
+                for (const JitTarget& t : v)
+                {
+                    // the chunk's set: the leaf or skeleton set holding its first point
+                    std::pair<int, int> key{-1, 0};
+                    if (t.pt0 < d->n_point)
+                    {
+                        auto it = leaf_at.upper_bound(t.pt0);
+                        if (it != leaf_at.begin()) key = {std::prev(it)->second, 0};
+                    } else {
+                        auto it = jset_at.upper_bound(t.pt0);
+                        if (it != jset_at.begin()) key = {std::prev(it)->second, 1};
+                    }
+                    REQ(key.first >= 0, "plan (%s): a target chunk belongs to no point set", field);
+                    rows[key] += t.npt;
+                    std::vector<std::pair<int, int>> got;
+                    for (int k = t.src_beg; k < t.src_end; k++)
+                    {
+                        if (hp.js[k].npt == 0) continue;
+                        const auto sk = set_key(hp.js[k].pt0, hp.js[k].npt);
+                        REQ(sk.first >= 0, "plan (%s): a source is not a whole point set", field);
+                        got.push_back(sk);
+                    }
+                    std::vector<std::pair<int, int>> exp = want[key];
+                    std::sort(got.begin(), got.end());
+                    std::sort(exp.begin(), exp.end());
+                    REQ(got == exp, "plan (%s): node %d's sources differ from its pair lists", field, key.first);
+                }
+                for (const auto& kv : want)
+                {
+                    if (kv.second.empty()) continue;
+                    const long long full = kv.first.second ? d->J_n[kv.first.first] : npt(kv.first.first);
+                    if (full == 0) continue;
+                    REQ(rows[kv.first] == full, "plan (%s): node %d's targets cover %lld of %lld points", field,
+                        kv.first.first, rows[kv.first], full);
+                }
+                return H2GPU_OK;
+            };
+            TRY(match("near", hp.jtN, near_src));
+            TRY(match("far", hp.jtF, far_src));
+        }
+
         // ---- sources, tiles and panel groups
         for (const JitSource& s : hp.js)
         {
-            REQ(s.npt >= 1 && s.pt0 >= 0 && (long long) s.pt0 + s.npt <= np, "plan: JIT source outside the point space");
+            // an empty skeleton (rank 0) is a source of no points: nothing to check
+            REQ(s.npt >= 0 && s.pt0 >= 0 && (long long) s.pt0 + s.npt <= np, "plan: JIT source outside the point space");
+            if (s.npt == 0) continue;
             if (s.pt0 < d->n_point) REQ(s.in_row == kd * s.pt0, "plan: JIT source input row does not match its points");
             else REQ(s.in_row >= N && (long long) s.in_row + (long long) kd * s.npt <= N + Y0, "plan: JIT source input outside y0");
             if (kd == 1)

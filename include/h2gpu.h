@@ -291,10 +291,11 @@ size_t h2gpu_image_bytes(const h2gpu_image *img);
  *   - every partial-space row is written by one producer and summed by one
  *     consumer, every push-down / y1 row a downward task reads is written, and the
  *     assembly writes every output row once (for each plan an image holds);
- *   - JIT: the (target, source) point pairs the plan evaluates are the pairs
- *     H2Pack's pair lists imply (near: each leaf with itself and its inadmissible
- *     partners; far: the admissible pairs, skeleton or leaf points as the levels
- *     say), the source tiles and 8-point panel groups cover every source set once
+ *   - JIT: every target's source sets are exactly those H2Pack's pair lists name
+ *     for its node (near: the leaf itself and its inadmissible partners; far: the
+ *     admissible partners, skeleton or leaf points as the levels say), the point
+ *     pairs total what the lists imply, the source tiles and 8-point panel groups
+ *     cover every source set once
  *     in order, and the pair plan (scalar kernels) owns every unordered pair once;
  *   - every index a kernel takes from a task record (block offsets, input rows, point
  *     ranges) lies inside the array it indexes (kernels do not bounds-check them).
