@@ -1076,6 +1076,33 @@ int check_plan(const h2gpu_image* im, const h2gpu_desc* d, const HostPlan& hp, l
         for (const JitTarget& t : *v) (t.out_y1 ? y1w : prod).push_back({t.out_row, (long long) kd * t.npt});
     TRY(check_space("one-sided", prod, y1w, hp.at, hp.at_slots, hp.y1t, hp.y1_slots));
 
+    // ---- stored blocks: the tasks of every B / D block cover its rows once, at its width
+    if (!d->BD_JIT)
+    {
+        auto cover_blocks = [&](const char* which, const std::vector<BlkTask>& tasks, int nb, const int* nrow,
+                                const int* ncol, const size_t* ptr) -> int {
+            std::vector<std::vector<char>> rows(nb);
+            for (const BlkTask& t : tasks)
+            {
+                const size_t* it = std::upper_bound(ptr, ptr + nb + 1, (size_t) t.a_off);
+                const int i = (int) (it - ptr) - 1;
+                REQ(i >= 0 && i < nb && ncol[i] == t.ncol && ((long long) t.a_off - (long long) ptr[i]) % t.ncol == 0,
+                    "plan: a %s task does not start on a row of its block", which);
+                const long long r0 = ((long long) t.a_off - (long long) ptr[i]) / t.ncol;
+                REQ(r0 + t.nrow <= nrow[i], "plan: a %s task runs past its block", which);
+                if (rows[i].empty()) rows[i].assign(nrow[i], 0);
+                for (long long r = r0; r < r0 + t.nrow; r++) REQ(++rows[i][r] == 1, "plan: a row of %s block %d is covered twice", which, i);
+            }
+            for (int i = 0; i < nb; i++)
+                if (nrow[i] > 0 && ncol[i] > 0)
+                    REQ(!rows[i].empty() && std::count(rows[i].begin(), rows[i].end(), 1) == nrow[i],
+                        "plan: %s block %d is not covered by its tasks", which, i);
+            return H2GPU_OK;
+        };
+        TRY(cover_blocks("B", hp.blkB, d->n_B, d->B_nrow, d->B_ncol, d->B_ptr));
+        TRY(cover_blocks("D", hp.blkD, d->n_D, d->D_nrow, d->D_ncol, d->D_ptr));
+    }
+
     long long pairs_plan = 0;
     if (d->BD_JIT)
     {

@@ -287,7 +287,8 @@ size_t h2gpu_image_bytes(const h2gpu_image *img);
  * Host-only self-check of the apply plan: builds the plan h2gpu_image_create would
  * upload for desc (no device is touched, no GPU is needed) and verifies that
  *   - the upward tasks sweep every column of every node's U once and the downward
- *     tasks every row at most once, inside the node's U;
+ *     tasks every row at most once, inside the node's U; the stored-block tasks
+ *     cover every row of every B / D block once;
  *   - every partial-space row is written by one producer and summed by one
  *     consumer, every push-down / y1 row a downward task reads is written, and the
  *     assembly writes every output row once (for each plan an image holds);
