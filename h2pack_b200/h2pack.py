@@ -175,6 +175,25 @@ class Image:
             pass
 
 
+PLAN_COUNT_NAMES = ("up_tasks", "down_tasks", "block_tasks", "jit_targets", "source_tiles", "panel_groups",
+                    "partial_rows", "jit_point_pairs")
+
+
+def plan_check(descs) -> dict:
+    """Host-only self-check of the apply plan (h2gpu_plan_check; no GPU needed) of one
+    descriptor, or of the merged representation of a list of them
+    (h2gpu_batch_plan_check).  Returns the plan's sizes; raises RuntimeError naming the
+    first violated invariant."""
+    lib = _abi.libh2gpu()
+    cnt = (C.c_longlong * len(PLAN_COUNT_NAMES))()
+    if isinstance(descs, (list, tuple)):
+        arr = (_abi.Desc * len(descs))(*descs)
+        _abi.check(lib.h2gpu_batch_plan_check(arr, len(descs), cnt), lib, "h2gpu_batch_plan_check")
+    else:
+        _abi.check(lib.h2gpu_plan_check(C.byref(descs), cnt), lib, "h2gpu_plan_check")
+    return dict(zip(PLAN_COUNT_NAMES, list(cnt)))
+
+
 def direct_sum(kernel, param, src_coord, src_val, trg_coord) -> np.ndarray:
     """FP64 direct sum on the GPU: y_t = sum_s K(x_t, x_s) v_s (examples/direct_nbody.h)."""
     lib = _abi.libh2gpu()
@@ -278,6 +297,10 @@ class H2Matrix:
         d = _abi.Desc()
         self._check(self.lib.h2pb_describe(self.handle, C.byref(d)), "h2pb_describe")
         return d
+
+    def plan_check(self) -> dict:
+        """The host-only plan self-check of this matrix's representation (no GPU needed)."""
+        return plan_check(self.describe())
 
     def sorted_coord(self) -> np.ndarray:
         xd = self.info["xpt_dim"]

@@ -122,3 +122,16 @@ def test_batched_plan_is_the_union_of_its_members(kernel, jit):
     finally:
         for H in Hs:
             H.close()
+
+
+def test_python_wrapper():
+    from h2pack_b200 import plan_check as pc
+    H = H2Matrix("gaussian", make_points("gaussian", 4000, 3), KERNEL_PARAMS["gaussian"], 1e-6, BD_JIT=1,
+                 max_leaf_points=100)
+    try:
+        c = H.plan_check()
+        assert list(c.values()) == plan_check(H.describe())
+        assert c["jit_point_pairs"] == pairs_from_lists(H.describe())
+        assert pc([H.describe(), H.describe()])["jit_point_pairs"] == 2 * c["jit_point_pairs"]
+    finally:
+        H.close()
