@@ -35,10 +35,17 @@ typedef struct h2pb_handle
     int      n_pp;
     int      kernel_id;
     double   build_sec;
-    /* arrays behind the last h2pb_describe() */
-    int     *d_ints;
-    const double **d_ptrs;
+    /* arrays behind every h2pb_describe() of this handle, newest first; each
+       descriptor stays valid until h2pb_destroy */
+    struct desc_store *descs;
 } h2pb_handle;
+
+typedef struct desc_store
+{
+    int *ints;
+    const double **ptrs;
+    struct desc_store *next;
+} desc_store;
 
 static int krnl_dim_of(int kernel_id) { return kernel_id == H2GPU_KRNL_RPY ? 3 : 1; }
 
@@ -148,8 +155,14 @@ H2PB_EXPORT void h2pb_destroy(h2pb_handle *hd)
         free(hd->pp);
     }
     free(hd->krnl_param);
-    free(hd->d_ints);
-    free(hd->d_ptrs);
+    while (hd->descs != NULL)
+    {
+        desc_store *ds = hd->descs;
+        hd->descs = ds->next;
+        free(ds->ints);
+        free((void *) ds->ptrs);
+        free(ds);
+    }
     free(hd);
 }
 
@@ -234,12 +247,19 @@ H2PB_EXPORT int h2pb_describe_h2pack(H2Pack_p h, int kernel_id, const double *pa
     return H2GPU_OK;
 }
 
-/* Descriptor of a handle built by h2pb_build; arrays are owned by the handle. */
+/* Descriptor of a handle built by h2pb_build.  Its arrays are owned by the handle
+   and stay valid until h2pb_destroy: every call gets storage of its own, so a caller
+   may keep several descriptors of one handle (a batch listing a matrix twice, a
+   descriptor kept across a plan check). */
 H2PB_EXPORT int h2pb_describe(h2pb_handle *hd, h2gpu_desc *d)
 {
     if (hd == NULL) return H2GPU_ERR_INVALID;
-    free(hd->d_ints);  hd->d_ints = NULL;
-    free(hd->d_ptrs);  hd->d_ptrs = NULL;
-    return h2pb_describe_h2pack(hd->h2pack, hd->kernel_id, hd->krnl_param, hd->n_krnl_param,
-                                d, &hd->d_ints, &hd->d_ptrs);
+    desc_store *ds = (desc_store *) calloc(1, sizeof(desc_store));
+    if (ds == NULL) return H2GPU_ERR_NOMEM;
+    int st = h2pb_describe_h2pack(hd->h2pack, hd->kernel_id, hd->krnl_param, hd->n_krnl_param,
+                                  d, &ds->ints, &ds->ptrs);
+    if (st != H2GPU_OK) { free(ds); return st; }
+    ds->next = hd->descs;
+    hd->descs = ds;
+    return H2GPU_OK;
 }

@@ -135,3 +135,23 @@ def test_python_wrapper():
         assert pc([H.describe(), H.describe()])["jit_point_pairs"] == 2 * c["jit_point_pairs"]
     finally:
         H.close()
+
+
+def test_descriptors_of_one_handle_stay_valid():
+    """Several descriptors of one handle are all usable at once: each describe() call
+    owns its arrays until the handle is destroyed (a batch listing a matrix twice, or
+    a descriptor kept across a later describe, read no freed memory)."""
+    H = H2Matrix("coulomb", make_points("coulomb", 3000, 5), [], 1e-6, BD_JIT=0, max_leaf_points=100)
+    try:
+        d1 = H.describe()
+        d2 = H.describe()
+        d3 = H.describe()
+        addr = [C.cast(d.U_nrow, C.c_void_p).value for d in (d1, d2, d3)]
+        assert len(set(addr)) == 3           # storage of their own
+        c1 = plan_check(d1)
+        assert plan_check(d2) == c1 and plan_check(d3) == c1
+        merged = batch_plan_check([d1, d2, d3])
+        assert merged[2] == 3 * c1[2]       # stored-block tasks of three copies
+        assert plan_check(d1) == c1          # the oldest is still intact
+    finally:
+        H.close()
