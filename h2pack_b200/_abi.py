@@ -112,6 +112,8 @@ H2PACK_GPU_SYMBOLS = {
     "H2P_permute_matrix_row_forward": (None, [C.c_void_p, C.c_int, C.c_int, _dp, C.c_int, _dp, C.c_int]),
     "H2P_permute_matrix_row_backward": (None, [C.c_void_p, C.c_int, C.c_int, _dp, C.c_int, _dp, C.c_int]),
     "H2P_gpu_set_kernel": (C.c_int, [C.c_void_p, C.c_int, _dp, C.c_int]),
+    "H2P_gpu_kernel_of": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), _dp, C.POINTER(C.c_int)]),
+    "H2P_destroy": (None, [C.POINTER(C.c_void_p)]),
     "H2P_gpu_set_precision": (C.c_int, [C.c_void_p, C.c_int]),
     "H2P_gpu_matvec": (C.c_int, [C.c_void_p, _dp, _dp]),
     "H2P_gpu_matmul": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _dp, C.c_int, _dp, C.c_int]),

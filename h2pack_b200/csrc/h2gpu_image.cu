@@ -1935,7 +1935,10 @@ H2G_API int h2gpu_direct_sum(int kernel_id, const double* krnl_param, int n_krnl
 // (different streams, or different host threads on the same device) race on it.
 // The first call on a device looks up the array's device address with that device
 // current (cudaGetSymbolAddress), so that first call should come before any stream
-// capture.
+// capture.  A mixed-precision image applies FP32 copies of U/B/D that its first
+// allocating apply (h2gpu_matvec, h2gpu_matmul, h2gpu_matmul_device) creates; until
+// then this entry point refuses it with H2GPU_ERR_STATE.  The caller's current device
+// is left as it was.
 
 #define H2GPU_NOALLOC_SCRATCH_DOUBLES (2u * 1024u * 1024u)
 
@@ -1970,6 +1973,13 @@ H2G_API int h2gpu_matvec_device_noalloc(h2gpu_image* im, const double* d_x, doub
     if (!im) return fail(H2GPU_ERR_INVALID, "image is NULL");
     REQ(d_x && d_y, "device vectors are NULL");
     std::lock_guard<std::mutex> lk(im->mu);
+    // the caller's current device is restored on every return
+    int caller_dev = -1;
+    CK(cudaGetDevice(&caller_dev));
+    struct DeviceRestore {
+        int dev;
+        ~DeviceRestore() { cudaSetDevice(dev); }
+    } restore{caller_dev};
     CK(cudaSetDevice(im->device));
     if (im->precision == H2GPU_PREC_MIXED &&
         ((im->U_elems && !im->d_U32) || (im->B_elems && !im->d_B32) || (im->D_elems && !im->d_D32)))

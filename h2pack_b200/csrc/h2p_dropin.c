@@ -7,7 +7,31 @@
  * the handle: n_matvec (src/H2Pack_matvec.c:1283, src/H2Pack_matmul.c:582) and the
  * phase timers timers[MV_*_TIMER_IDX] (src/H2Pack_typedef.h:226-239) that
  * H2P_print_statistic reads.
+ *
+ * Handles and their device images.  A registry maps each H2Pack handle to its device
+ * image.  The registry lock is held only to find, add or unlink an entry; each entry
+ * has its own lock, held for the whole upload -> apply -> download of a call, so calls
+ * on one handle are serialised (the reference is not reentrant per handle either: its
+ * y0 / y1 / thread buffers live in the handle, src/H2Pack_matvec.c:68-92) while calls
+ * on different handles run concurrently.  Entries are reference counted, so a release
+ * that races with an apply on another thread frees the image after that apply ends.
+ *
+ * Kernel identity.  JIT-mode handles evaluate their kernel on the fly, and struct
+ * H2Pack keeps it only as a function pointer plus a parameter pointer
+ * (src/H2Pack_typedef.h:160, :193).  The kernel is identified by calling that
+ * function on a fixed probe point set and matching the values against Coulomb,
+ * Gaussian, Matern-3/2 and RPY with the handle's own parameter; H2P_gpu_set_kernel
+ * overrides the identification.
+ *
+ * Staleness.  An image is reused while the handle's fingerprint is unchanged: sizes,
+ * array addresses and a strided sample of the array contents (U, B, D, coordinates,
+ * pair lists, permutation, skeleton points).  A handle destroyed and rebuilt at the
+ * same addresses with other values is re-uploaded unless every sampled value agrees.
+ * H2P_destroy is interposed: it releases the handle's image before H2Pack frees the
+ * handle (the reference's own H2P_destroy is compiled under the name
+ * H2P_destroy_host, src/H2Pack_typedef.c:210).
  */
+#include <math.h>
 #include <pthread.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -24,20 +48,26 @@ _Static_assert(sizeof(DTYPE) == sizeof(double), "the GPU drop-in is built for DT
 /* h2p_builder.c */
 int h2pb_describe_h2pack(H2Pack_p h, int kernel_id, const double *param, int n_param,
                          h2gpu_desc *d, int **ints_out, const double ***ptrs_out);
+/* H2Pack's own H2P_destroy (src/H2Pack_typedef.c:210), compiled under this name */
+void H2P_destroy_host(H2Pack_p *h2pack_);
 
 typedef struct reg_entry
 {
     H2Pack_p key;
+    pthread_mutex_t mu;       /* held across one apply on this handle              */
+    int refs;                 /* threads holding the entry (registry lock)          */
+    int dead;                 /* unlinked by a release; freed by the last holder    */
     uint64_t fingerprint;
     h2gpu_image *img;
     int kernel_id, n_param, precision;
+    int kernel_set;           /* 1: given by H2P_gpu_set_kernel (not identified)    */
     double param[4];
     double ms_seen[5];
     struct reg_entry *next;
 } reg_entry;
 
 static reg_entry *g_reg = NULL;
-static pthread_mutex_t g_mu = PTHREAD_MUTEX_INITIALIZER;
+static pthread_mutex_t g_mu = PTHREAD_MUTEX_INITIALIZER;   /* registry links and refs only */
 static __thread char g_msg[512];
 
 static uint64_t mix(uint64_t h, uint64_t v)
@@ -46,38 +76,128 @@ static uint64_t mix(uint64_t h, uint64_t v)
     return h;
 }
 
-/* Identity of the arrays the image was built from. */
+static uint64_t bits_of(double v)
+{
+    uint64_t b;
+    memcpy(&b, &v, sizeof(b));
+    return b;
+}
+
+/* up to 32 evenly spaced samples of an array of n doubles */
+static uint64_t sample_doubles(uint64_t f, const double *a, size_t n)
+{
+    if (a == NULL || n == 0) return mix(f, 0);
+    size_t step = n > 32 ? n / 32 : 1;
+    for (size_t i = 0; i < n; i += step) f = mix(f, bits_of(a[i]));
+    return mix(f, bits_of(a[n - 1]));
+}
+
+static uint64_t sample_ints(uint64_t f, const int *a, size_t n)
+{
+    if (a == NULL || n == 0) return mix(f, 0);
+    size_t step = n > 32 ? n / 32 : 1;
+    for (size_t i = 0; i < n; i += step) f = mix(f, (uint64_t) (uint32_t) a[i]);
+    return mix(f, (uint64_t) (uint32_t) a[n - 1]);
+}
+
+/* Identity of the representation the image was built from: sizes, array addresses
+   and a strided sample of the contents. */
 static uint64_t fingerprint(H2Pack_p h)
 {
     uint64_t f = 1469598103934665603ULL;
     f = mix(f, (uint64_t) h->n_point);   f = mix(f, (uint64_t) h->n_node);
     f = mix(f, (uint64_t) h->n_B);       f = mix(f, (uint64_t) h->n_D);
     f = mix(f, (uint64_t) h->BD_JIT);    f = mix(f, (uint64_t) h->krnl_dim);
+    f = mix(f, (uint64_t) h->n_r_adm_pair);  f = mix(f, (uint64_t) h->n_r_inadm_pair);
     f = mix(f, (uint64_t) (uintptr_t) h->U);        f = mix(f, (uint64_t) (uintptr_t) h->B_data);
     f = mix(f, (uint64_t) (uintptr_t) h->D_data);   f = mix(f, (uint64_t) (uintptr_t) h->coord);
     f = mix(f, (uint64_t) (uintptr_t) h->r_adm_pairs);  f = mix(f, (uint64_t) (uintptr_t) h->fwd_pmt_idx);
     f = mix(f, (uint64_t) (uintptr_t) h->J_coord);
+    /* contents */
+    f = sample_doubles(f, h->coord, (size_t) h->xpt_dim * h->n_point);
+    f = sample_ints(f, h->fwd_pmt_idx, (size_t) h->krnl_mat_size);
+    f = sample_ints(f, h->r_adm_pairs, 2 * (size_t) h->n_r_adm_pair);
+    f = sample_ints(f, h->r_inadm_pairs, 2 * (size_t) h->n_r_inadm_pair);
+    if (h->B_ptr != NULL && h->n_B > 0)
+    {
+        f = mix(f, (uint64_t) h->B_ptr[h->n_B]);
+        if (!h->BD_JIT) f = sample_doubles(f, h->B_data, (size_t) h->B_ptr[h->n_B]);
+    }
+    if (h->D_ptr != NULL && h->n_D > 0)
+    {
+        f = mix(f, (uint64_t) h->D_ptr[h->n_D]);
+        if (!h->BD_JIT) f = sample_doubles(f, h->D_data, (size_t) h->D_ptr[h->n_D]);
+    }
+    if (h->U != NULL)
+    {
+        int step = h->n_node > 16 ? h->n_node / 16 : 1;
+        for (int i = 0; i < h->n_node; i += step)
+        {
+            H2P_dense_mat_p u = h->U[i];
+            if (u == NULL) continue;
+            f = mix(f, (uint64_t) u->nrow);  f = mix(f, (uint64_t) u->ncol);
+            if (u->nrow > 0 && u->ncol > 0) f = sample_doubles(f, u->data, (size_t) u->nrow * u->ld);
+        }
+    }
+    if (h->J_coord != NULL)
+    {
+        int step = h->n_node > 16 ? h->n_node / 16 : 1;
+        for (int i = 0; i < h->n_node; i += step)
+        {
+            H2P_dense_mat_p j = h->J_coord[i];
+            if (j != NULL && j->ncol > 0) f = sample_doubles(f, j->data, (size_t) j->nrow * j->ncol);
+        }
+    }
     return f;
 }
 
-static reg_entry *find(H2Pack_p h)
+/* ------------------------------------------------------------------ registry */
+
+static reg_entry *find_locked(H2Pack_p h)
 {
     for (reg_entry *e = g_reg; e != NULL; e = e->next)
         if (e->key == h) return e;
     return NULL;
 }
 
-static reg_entry *find_or_add(H2Pack_p h)
+static void entry_free(reg_entry *e)
 {
-    reg_entry *e = find(h);
-    if (e != NULL) return e;
-    e = (reg_entry *) calloc(1, sizeof(reg_entry));
-    if (e == NULL) return NULL;
-    e->key = h;
-    e->precision = H2GPU_PREC_FP64;
-    e->next = g_reg;
-    g_reg = e;
+    if (e->img) h2gpu_image_destroy(e->img);
+    pthread_mutex_destroy(&e->mu);
+    free(e);
+}
+
+/* Take a reference on the handle's entry (created if absent) and lock it. */
+static reg_entry *acquire(H2Pack_p h)
+{
+    pthread_mutex_lock(&g_mu);
+    reg_entry *e = find_locked(h);
+    if (e == NULL)
+    {
+        e = (reg_entry *) calloc(1, sizeof(reg_entry));
+        if (e != NULL)
+        {
+            e->key = h;
+            e->precision = H2GPU_PREC_FP64;
+            pthread_mutex_init(&e->mu, NULL);
+            e->next = g_reg;
+            g_reg = e;
+        }
+    }
+    if (e != NULL) e->refs++;
+    pthread_mutex_unlock(&g_mu);
+    if (e != NULL) pthread_mutex_lock(&e->mu);
     return e;
+}
+
+/* Unlock the entry and drop the reference; the last holder of a released entry frees it. */
+static void release_ref(reg_entry *e)
+{
+    pthread_mutex_unlock(&e->mu);
+    pthread_mutex_lock(&g_mu);
+    int last = (--e->refs == 0) && e->dead;
+    pthread_mutex_unlock(&g_mu);
+    if (last) entry_free(e);
 }
 
 static int set_msg(int st, const char *what)
@@ -86,25 +206,144 @@ static int set_msg(int st, const char *what)
     return st;
 }
 
-/* Device image of a handle, created or refreshed as needed (caller holds g_mu). */
-static int image_of(H2Pack_p h, reg_entry **out)
+/* ---------------------------------------------------------- kernel identity */
+
+/* The four kernels' values in FP64 from their defining formulas (src/H2Pack_3D_kernels.h:
+   Coulomb :52-83, Gaussian :169-200, Matern-3/2 :388-420, RPY :893-959). */
+static double scalar_value(int kid, double p0, int has_p, double r2)
 {
-    if (h == NULL) return set_msg(H2GPU_ERR_INVALID, "H2Pack handle is NULL");
-    reg_entry *e = find_or_add(h);
-    if (e == NULL) return set_msg(H2GPU_ERR_NOMEM, "registry allocation");
-    uint64_t fp = fingerprint(h);
-    if (e->img != NULL && e->fingerprint == fp) { *out = e; return H2GPU_OK; }
-    if (e->img != NULL) { h2gpu_image_destroy(e->img); e->img = NULL; }
-    if (h->BD_JIT && e->kernel_id == 0)
+    switch (kid)
     {
-        snprintf(g_msg, sizeof(g_msg),
-                 "JIT-mode handle has no kernel id: call H2P_gpu_set_kernel() before the first apply");
-        return H2GPU_ERR_STATE;
+        case H2GPU_KRNL_COULOMB:  return r2 == 0.0 ? (has_p ? p0 : 0.0) : 1.0 / sqrt(r2);
+        case H2GPU_KRNL_GAUSSIAN: return exp(-p0 * r2);
+        case H2GPU_KRNL_MATERN32: { double t = sqrt(3.0) * p0 * sqrt(r2); return (1.0 + t) * exp(-t); }
+        default: return NAN;
+    }
+}
+
+static void rpy_block(double eta, const double *a, const double *b, double *m3 /* 3x3 */)
+{
+    const double C = 1.0 / (6.0 * M_PI * eta);
+    double d[3] = {a[0] - b[0], a[1] - b[1], a[2] - b[2]};
+    double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2], r = sqrt(r2);
+    double ai = a[3], aj = b[3], t1, t2;
+    double ir = r == 0.0 ? 0.0 : 1.0 / r;
+    for (int k = 0; k < 3; k++) d[k] *= ir;
+    if (r > ai + aj)
+    {
+        double c = 0.75 * C * ir, q = (ai * ai + aj * aj) * ir * ir;
+        t1 = c * (1.0 + q / 3.0);
+        t2 = c * (1.0 - q);
+    } else if (r > fabs(ai - aj)) {
+        double s = (ai - aj) * (ai - aj), c = C * ir * ir * ir / (32.0 * ai * aj);
+        t1 = c * (16.0 * r2 * r * (ai + aj) - (s + 3.0 * r2) * (s + 3.0 * r2));
+        t2 = c * 3.0 * (s - r2) * (s - r2);
+    } else {
+        t1 = C / (ai > aj ? ai : aj);
+        t2 = 0.0;
+    }
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) m3[3 * i + j] = t2 * d[i] * d[j] + (i == j ? t1 : 0.0);
+}
+
+#define PROBE_N 6
+
+/* Probe points (x, y, z, radius): distances from 0 to ~3.5, one coincident pair, and
+   RPY radii that reach all three of its distance branches. */
+static const double probe_pts[PROBE_N][4] = {
+    {0.00, 0.00, 0.00, 1.0}, {0.30, 0.10, -0.20, 0.5}, {1.10, -0.40, 0.60, 1.0},
+    {-0.70, 1.90, 0.20, 0.8}, {2.40, 1.30, -1.50, 1.2}, {0.00, 0.00, 0.00, 0.6},
+};
+
+/* Identify the kernel of a JIT handle from its evaluation function and parameter.
+   Returns H2GPU_OK with *kid / param filled, or H2GPU_ERR_UNSUPPORTED. */
+static int identify_kernel(H2Pack_p h, int *kid, double *param, int *n_param)
+{
+    if (h->krnl_eval == NULL) return H2GPU_ERR_UNSUPPORTED;
+    const int xd = h->xpt_dim, kd = h->krnl_dim;
+    double coord[4 * PROBE_N];
+    for (int i = 0; i < PROBE_N; i++)
+        for (int k = 0; k < xd && k < 4; k++) coord[k * PROBE_N + i] = probe_pts[i][k];
+    const int n = kd * PROBE_N;
+    double mat[(3 * PROBE_N) * (3 * PROBE_N)];
+    for (int i = 0; i < n * n; i++) mat[i] = NAN;
+    h->krnl_eval(coord, PROBE_N, PROBE_N, coord, PROBE_N, PROBE_N, h->krnl_param, mat, n);
+    const double *p = (const double *) h->krnl_param;
+    const int has_p = p != NULL;
+    const double p0 = has_p ? p[0] : 0.0;
+
+    if (kd == 3)
+    {
+        if (xd != 4 || !has_p || !(p0 > 0.0)) return H2GPU_ERR_UNSUPPORTED;
+        double worst = 0.0, scale = 0.0;
+        for (int i = 0; i < PROBE_N; i++)
+            for (int j = 0; j < PROBE_N; j++)
+            {
+                double m3[9];
+                rpy_block(p0, probe_pts[i], probe_pts[j], m3);
+                for (int a = 0; a < 3; a++)
+                    for (int b = 0; b < 3; b++)
+                    {
+                        double got = mat[(3 * i + a) * n + 3 * j + b], want = m3[3 * a + b];
+                        if (!(fabs(got - want) <= worst)) worst = fabs(got - want);
+                        if (fabs(want) > scale) scale = fabs(want);
+                    }
+            }
+        if (!(worst <= 1e-6 * scale)) return H2GPU_ERR_UNSUPPORTED;
+        *kid = H2GPU_KRNL_RPY;
+        param[0] = p0;
+        *n_param = 1;
+        return H2GPU_OK;
+    }
+    if (kd != 1) return H2GPU_ERR_UNSUPPORTED;
+    static const int cand[3] = {H2GPU_KRNL_COULOMB, H2GPU_KRNL_GAUSSIAN, H2GPU_KRNL_MATERN32};
+    for (int c = 0; c < 3; c++)
+    {
+        if (cand[c] != H2GPU_KRNL_COULOMB && !(has_p && p0 > 0.0)) continue;
+        double worst = 0.0, scale = 0.0;
+        for (int i = 0; i < PROBE_N; i++)
+            for (int j = 0; j < PROBE_N; j++)
+            {
+                double dx = probe_pts[i][0] - probe_pts[j][0], dy = probe_pts[i][1] - probe_pts[j][1];
+                double dz = probe_pts[i][2] - probe_pts[j][2];
+                double want = scalar_value(cand[c], p0, has_p, dx * dx + dy * dy + dz * dz);
+                double got = mat[i * n + j];
+                if (!(fabs(got - want) <= worst)) worst = fabs(got - want);
+                if (fabs(want) > scale) scale = fabs(want);
+            }
+        if (worst <= 1e-6 * scale)
+        {
+            *kid = cand[c];
+            *n_param = has_p ? 1 : 0;
+            param[0] = p0;
+            return H2GPU_OK;
+        }
+    }
+    return H2GPU_ERR_UNSUPPORTED;
+}
+
+/* --------------------------------------------------------------- device image */
+
+/* Device image of a handle, created or refreshed as needed (caller holds e->mu). */
+static int image_of(H2Pack_p h, reg_entry *e)
+{
+    uint64_t fp = fingerprint(h);
+    if (e->img != NULL && e->fingerprint == fp) return H2GPU_OK;
+    if (e->img != NULL) { h2gpu_image_destroy(e->img); e->img = NULL; }
+    if (h->BD_JIT && !e->kernel_set)
+    {
+        if (identify_kernel(h, &e->kernel_id, e->param, &e->n_param) != H2GPU_OK)
+        {
+            snprintf(g_msg, sizeof(g_msg),
+                     "JIT-mode handle: its kernel function matches none of Coulomb, Gaussian, Matern-3/2 "
+                     "and RPY with its parameter; the GPU path evaluates only these kernels");
+            return H2GPU_ERR_UNSUPPORTED;
+        }
     }
     h2gpu_desc d;
     int *ints = NULL;
     const double **ptrs = NULL;
-    int st = h2pb_describe_h2pack(h, e->kernel_id, e->param, e->n_param, &d, &ints, &ptrs);
+    int st = h2pb_describe_h2pack(h, h->BD_JIT ? e->kernel_id : 0, e->param, e->n_param, &d, &ints, &ptrs);
     if (st != H2GPU_OK)
     {
         snprintf(g_msg, sizeof(g_msg), "handle not supported by the GPU apply path (status %d): "
@@ -120,7 +359,6 @@ static int image_of(H2Pack_p h, reg_entry **out)
     if (st != H2GPU_OK) return set_msg(st, "h2gpu_image_create");
     e->fingerprint = fp;
     memset(e->ms_seen, 0, sizeof(e->ms_seen));
-    *out = e;
     return H2GPU_OK;
 }
 
@@ -143,19 +381,33 @@ DROPIN_API int H2P_gpu_set_kernel(H2Pack_p h, int kernel_id, const double *param
         return set_msg(H2GPU_ERR_INVALID, "H2P_gpu_set_kernel arguments");
     if (kernel_id < H2GPU_KRNL_COULOMB || kernel_id > H2GPU_KRNL_RPY)
         return set_msg(H2GPU_ERR_INVALID, "unknown kernel id");
-    pthread_mutex_lock(&g_mu);
-    reg_entry *e = find_or_add(h);
-    int st = H2GPU_OK;
-    if (e == NULL) st = H2GPU_ERR_NOMEM;
-    else
+    reg_entry *e = acquire(h);
+    if (e == NULL) return set_msg(H2GPU_ERR_NOMEM, "registry allocation");
+    e->kernel_id = kernel_id;
+    e->kernel_set = 1;
+    e->n_param = n_param;
+    memset(e->param, 0, sizeof(e->param));
+    for (int i = 0; i < n_param; i++) e->param[i] = param[i];
+    if (e->img) { h2gpu_image_destroy(e->img); e->img = NULL; }
+    release_ref(e);
+    return H2GPU_OK;
+}
+
+DROPIN_API int H2P_gpu_kernel_of(H2Pack_p h, int *kernel_id, double *param4, int *n_param)
+{
+    if (h == NULL || kernel_id == NULL) return set_msg(H2GPU_ERR_INVALID, "H2P_gpu_kernel_of arguments");
+    reg_entry *e = acquire(h);
+    if (e == NULL) return set_msg(H2GPU_ERR_NOMEM, "registry allocation");
+    int st = e->kernel_set ? H2GPU_OK : identify_kernel(h, &e->kernel_id, e->param, &e->n_param);
+    if (st == H2GPU_OK)
     {
-        e->kernel_id = kernel_id;
-        e->n_param = n_param;
-        memset(e->param, 0, sizeof(e->param));
-        for (int i = 0; i < n_param; i++) e->param[i] = param[i];
-        if (e->img) { h2gpu_image_destroy(e->img); e->img = NULL; }
+        *kernel_id = e->kernel_id;
+        if (param4) memcpy(param4, e->param, sizeof(e->param));
+        if (n_param) *n_param = e->n_param;
+    } else {
+        snprintf(g_msg, sizeof(g_msg), "kernel function matches none of the GPU kernels");
     }
-    pthread_mutex_unlock(&g_mu);
+    release_ref(e);
     return st;
 }
 
@@ -163,55 +415,56 @@ DROPIN_API int H2P_gpu_set_precision(H2Pack_p h, int precision)
 {
     if (h == NULL || (precision != H2GPU_PREC_FP64 && precision != H2GPU_PREC_MIXED))
         return set_msg(H2GPU_ERR_INVALID, "H2P_gpu_set_precision arguments");
-    pthread_mutex_lock(&g_mu);
-    reg_entry *e = find_or_add(h);
+    reg_entry *e = acquire(h);
+    if (e == NULL) return set_msg(H2GPU_ERR_NOMEM, "registry allocation");
     int st = H2GPU_OK;
-    if (e == NULL) st = H2GPU_ERR_NOMEM;
-    else
-    {
-        e->precision = precision;
-        if (e->img) st = h2gpu_set_precision(e->img, precision);
-    }
-    pthread_mutex_unlock(&g_mu);
+    e->precision = precision;
+    if (e->img) st = h2gpu_set_precision(e->img, precision);
+    release_ref(e);
     return st;
 }
 
 DROPIN_API int H2P_gpu_matvec(H2Pack_p h, const double *x, double *y)
 {
-    pthread_mutex_lock(&g_mu);
-    reg_entry *e = NULL;
-    int st = image_of(h, &e);
+    if (h == NULL) return set_msg(H2GPU_ERR_INVALID, "H2Pack handle is NULL");
+    reg_entry *e = acquire(h);
+    if (e == NULL) return set_msg(H2GPU_ERR_NOMEM, "registry allocation");
+    int st = image_of(h, e);
     if (st == H2GPU_OK)
     {
         st = h2gpu_matvec(e->img, x, y);
         if (st == H2GPU_OK) { h->n_matvec++; account(h, e); }
         else set_msg(st, "h2gpu_matvec");
     }
-    pthread_mutex_unlock(&g_mu);
+    release_ref(e);
     return st;
 }
 
 DROPIN_API int H2P_gpu_matmul(H2Pack_p h, int layout, int n_vec, const double *mat_x, int ldx, double *mat_y, int ldy)
 {
-    pthread_mutex_lock(&g_mu);
-    reg_entry *e = NULL;
-    int st = image_of(h, &e);
+    if (h == NULL) return set_msg(H2GPU_ERR_INVALID, "H2Pack handle is NULL");
+    reg_entry *e = acquire(h);
+    if (e == NULL) return set_msg(H2GPU_ERR_NOMEM, "registry allocation");
+    int st = image_of(h, e);
     if (st == H2GPU_OK)
     {
         st = h2gpu_matmul(e->img, layout, n_vec, mat_x, ldx, mat_y, ldy);
         if (st == H2GPU_OK) { h->n_matvec += n_vec; account(h, e); }
         else set_msg(st, "h2gpu_matmul");
     }
-    pthread_mutex_unlock(&g_mu);
+    release_ref(e);
     return st;
 }
 
+/* The handle's device image (created if needed).  It stays owned by the registry and
+   valid until H2P_gpu_release / H2P_destroy of the handle. */
 DROPIN_API h2gpu_image *H2P_gpu_image(H2Pack_p h)
 {
-    pthread_mutex_lock(&g_mu);
-    reg_entry *e = NULL;
-    h2gpu_image *img = (image_of(h, &e) == H2GPU_OK) ? e->img : NULL;
-    pthread_mutex_unlock(&g_mu);
+    if (h == NULL) return NULL;
+    reg_entry *e = acquire(h);
+    if (e == NULL) return NULL;
+    h2gpu_image *img = (image_of(h, e) == H2GPU_OK) ? e->img : NULL;
+    release_ref(e);
     return img;
 }
 
@@ -220,14 +473,16 @@ DROPIN_API int H2P_gpu_release(H2Pack_p h)
     pthread_mutex_lock(&g_mu);
     reg_entry **pp = &g_reg;
     while (*pp != NULL && (*pp)->key != h) pp = &(*pp)->next;
-    if (*pp != NULL)
+    reg_entry *e = *pp;
+    int now = 0;
+    if (e != NULL)
     {
-        reg_entry *e = *pp;
         *pp = e->next;
-        if (e->img) h2gpu_image_destroy(e->img);
-        free(e);
+        e->dead = 1;
+        now = e->refs == 0;
     }
     pthread_mutex_unlock(&g_mu);
+    if (now) entry_free(e);
     return H2GPU_OK;
 }
 
@@ -253,18 +508,30 @@ DROPIN_API void H2P_matmul(H2Pack_p h2pack, const CBLAS_LAYOUT layout, const int
     if (H2P_gpu_matmul(h2pack, (int) layout, n_vec, mat_x, ldx, mat_y, ldy) != H2GPU_OK) die("H2P_matmul");
 }
 
+/* H2P_destroy (src/H2Pack_typedef.h, src/H2Pack_typedef.c:210): the device image of the
+   handle is released first, then H2Pack frees the handle. */
+DROPIN_API void H2P_destroy(H2Pack_p *h2pack_)
+{
+    if (h2pack_ != NULL && *h2pack_ != NULL) H2P_gpu_release(*h2pack_);
+    H2P_destroy_host(h2pack_);
+}
+
 static void permute(H2Pack_p h, int forward, int layout, int n_vec, const double *x, int ldx, double *px, int ldp,
                     const char *what)
 {
-    pthread_mutex_lock(&g_mu);
-    reg_entry *e = NULL;
-    int st = image_of(h, &e);
-    if (st == H2GPU_OK)
+    int st;
+    reg_entry *e = h ? acquire(h) : NULL;
+    if (e == NULL) st = set_msg(h ? H2GPU_ERR_NOMEM : H2GPU_ERR_INVALID, what);
+    else
     {
-        st = h2gpu_permute_matrix_rows(e->img, forward, layout, n_vec, x, ldx, px, ldp);
-        if (st != H2GPU_OK) set_msg(st, what);
+        st = image_of(h, e);
+        if (st == H2GPU_OK)
+        {
+            st = h2gpu_permute_matrix_rows(e->img, forward, layout, n_vec, x, ldx, px, ldp);
+            if (st != H2GPU_OK) set_msg(st, what);
+        }
+        release_ref(e);
     }
-    pthread_mutex_unlock(&g_mu);
     if (st != H2GPU_OK) die(what);
 }
 

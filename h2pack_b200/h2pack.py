@@ -211,6 +211,20 @@ def direct_sum(kernel, param, src_coord, src_val, trg_coord) -> np.ndarray:
     return out
 
 
+def kernel_of(lib, h2pack):
+    """Kernel of an H2Pack handle as the drop-in identifies it from the handle's kernel
+    function and parameter (H2P_gpu_kernel_of): (name, parameters)."""
+    kid, n = C.c_int(), C.c_int()
+    p = np.zeros(4)
+    st = lib.H2P_gpu_kernel_of(C.c_void_p(h2pack) if isinstance(h2pack, int) else h2pack, C.byref(kid), _dptr(p),
+                               C.byref(n))
+    if st != 0:
+        m = lib.H2P_gpu_last_error()
+        raise RuntimeError(f"H2P_gpu_kernel_of failed with status {st}: {m.decode() if m else ''}")
+    names = {v: k for k, v in _abi.KERNEL_IDS.items()}
+    return names[kid.value], list(p[:n.value])
+
+
 class H2Matrix:
     """An H2 matrix built by H2Pack's construction and applied by the GPU drop-in.
 
@@ -242,8 +256,8 @@ class H2Matrix:
                               "krnl_mat_size", "max_leaf_points", "n_thread", "mm_max_n_vec"], list(info)))
         self.N = self.info["krnl_mat_size"]
         self.build_seconds = self.lib.h2pb_build_seconds(h)
-        self._check(self.lib.H2P_gpu_set_kernel(self.h2pack, self.kernel_id, _dptr(self.param), self.n_param),
-                    "H2P_gpu_set_kernel")
+        # JIT handles: the drop-in identifies the kernel from the handle's own kernel
+        # function and parameter, as it does for any H2Pack program
         self.set_precision(precision)
 
     def _check(self, st, what):
@@ -292,6 +306,10 @@ class H2Matrix:
         img._view = C.c_void_p(ptr)
         img.N = self.N
         return _ImageView(img._view, self.N)
+
+    def kernel_of(self):
+        """The kernel the drop-in sees in this handle (H2P_gpu_kernel_of): (name, param list)."""
+        return kernel_of(self.lib, self.h2pack)
 
     def describe(self) -> _abi.Desc:
         d = _abi.Desc()

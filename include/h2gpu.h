@@ -194,7 +194,11 @@ int h2gpu_permute_matrix_rows(h2gpu_image *img, int forward, int layout, int n_v
  * images needing more work space for one right-hand side are rejected with
  * H2GPU_ERR_INVALID.  Calls share that array, so calls that overlap on the GPU race;
  * the first call on a device looks up the array's address and should come before
- * any stream capture.  stream: a cudaStream_t or NULL for the image's own stream.
+ * any stream capture.  A mixed-precision image is refused with H2GPU_ERR_STATE until
+ * one allocating apply (h2gpu_matvec / h2gpu_matmul / h2gpu_matmul_device) has made
+ * its FP32 copies of U, B and D; FP64 images need no such call.  The caller's current
+ * device is restored before returning.  stream: a cudaStream_t or NULL for the
+ * image's own stream.
  */
 int h2gpu_matvec_device_noalloc(h2gpu_image *img, const double *d_x, double *d_y, void *stream);
 

@@ -15,20 +15,31 @@
  * The first call on an H2Pack handle uploads its representation (tree, pair
  * lists, U, B, D, coordinates, permutations) into a device image kept in a
  * registry keyed by the handle; later calls reuse it.  A fingerprint of the
- * handle's arrays is checked on every call, so a handle rebuilt at the same
- * address is re-uploaded.  Like the reference (ASSERT_PRINTF, src/utils.h:56-66)
+ * handle (sizes, array addresses and a strided sample of the array contents) is
+ * checked on every call, so a handle rebuilt or changed in place is re-uploaded.
+ * Calls on one handle are serialised by a lock of that handle; calls on different
+ * handles run concurrently.  Like the reference (ASSERT_PRINTF, src/utils.h:56-66)
  * the void entry points print the reason and abort on failure; the H2P_gpu_*
  * variants return an h2gpu status instead.
  *
+ *   H2P_destroy                      src/H2Pack_typedef.h (src/H2Pack_typedef.c:210):
+ *                                    releases the handle's device image, then frees
+ *                                    the handle as H2Pack does
+ *
+ * JIT-mode handles carry their kernel only as a function pointer and a parameter
+ * pointer (src/H2Pack_typedef.h:160, :193).  The drop-in calls that function on a
+ * fixed probe point set and matches the values against Coulomb, Gaussian,
+ * Matern-3/2 and RPY with the handle's parameter; a JIT handle whose kernel matches
+ * none of them is refused with H2GPU_ERR_UNSUPPORTED (there is no CPU fallback).
+ *
  * Extra entry points (no counterpart in the reference):
- *   H2P_gpu_set_kernel     name the kernel function of a JIT-mode handle.  The
- *                          reference keeps only function pointers to static
- *                          functions (src/H2Pack_typedef.h:193-196), which cannot be
- *                          identified across translation units, so JIT mode needs it.
+ *   H2P_gpu_set_kernel     name the kernel of a JIT-mode handle explicitly instead of
+ *                          identifying it
+ *   H2P_gpu_kernel_of      the kernel id and parameters the drop-in uses for a handle
  *   H2P_gpu_set_precision  H2GPU_PREC_FP64 (default) or H2GPU_PREC_MIXED
  *   H2P_gpu_matvec / H2P_gpu_matmul   status-returning forms
  *   H2P_gpu_image          the handle's device image (for h2gpu_get_stats)
- *   H2P_gpu_release        free the handle's device image (call before H2P_destroy)
+ *   H2P_gpu_release        free the handle's device image early (H2P_destroy does it too)
  *   H2P_gpu_last_error     message of the last failure
  *
  * Handles in HSS mode, RPY-Ewald / periodic handles and H2ERI handles are
@@ -56,7 +67,10 @@ void H2P_permute_matrix_row_forward(struct H2Pack *h2pack, const int layout, con
 void H2P_permute_matrix_row_backward(struct H2Pack *h2pack, const int layout, const int n_vec,
                                      const double *mat_x, const int ldx, double *pmt_mat_x, const int ldp);
 
+void H2P_destroy(struct H2Pack **h2pack_);
+
 int  H2P_gpu_set_kernel(struct H2Pack *h2pack, int kernel_id, const double *param, int n_param);
+int  H2P_gpu_kernel_of(struct H2Pack *h2pack, int *kernel_id, double *param4, int *n_param);
 int  H2P_gpu_set_precision(struct H2Pack *h2pack, int precision);
 int  H2P_gpu_matvec(struct H2Pack *h2pack, const double *x, double *y);
 int  H2P_gpu_matmul(struct H2Pack *h2pack, int layout, int n_vec,

@@ -127,13 +127,12 @@ def test_direct_sum_matches_oracle(kernel):
 
 
 def test_reference_built_handle_through_dropin():
-    """A handle built by the reference library itself, applied by the drop-in."""
+    """A JIT handle built by the reference library itself, applied by the drop-in with
+    no extra call: the kernel is identified from the handle's own kernel function."""
     coord = make_points("matern32", 5000, 13)
     R = O.RefH2("matern32", [1.0], coord, 1e-6, BD_JIT=1, max_leaf_points=100)
     lib = _abi.libh2pack_gpu()
     try:
-        p = np.array([1.0, 0, 0, 0])
-        assert lib.H2P_gpu_set_kernel(R.h2pack, _abi.KRNL_MATERN32, O.dptr(p), 1) == 0
         x = np.random.default_rng(9).standard_normal(R.N)
         y = np.zeros(R.N)
         assert lib.H2P_gpu_matvec(R.h2pack, O.dptr(x), O.dptr(y)) == 0
@@ -142,20 +141,32 @@ def test_reference_built_handle_through_dropin():
         y2 = np.zeros(R.N)
         lib.H2P_matvec(R.h2pack, O.dptr(x), O.dptr(y2))
         assert np.array_equal(y, y2)
+        # an explicit kernel id gives the same image
+        p = np.array([1.0, 0, 0, 0])
+        assert lib.H2P_gpu_set_kernel(R.h2pack, _abi.KRNL_MATERN32, O.dptr(p), 1) == 0
+        y3 = np.zeros(R.N)
+        assert lib.H2P_gpu_matvec(R.h2pack, O.dptr(x), O.dptr(y3)) == 0
+        assert np.array_equal(y, y3)
     finally:
         lib.H2P_gpu_release(R.h2pack)
         R.close()
 
 
-def test_jit_handle_without_kernel_is_refused():
+def test_jit_handle_with_a_wrong_explicit_kernel_differs():
+    """H2P_gpu_set_kernel overrides the identification (a Gaussian handle declared
+    Matern-3/2 is evaluated as Matern-3/2, so its result no longer matches)."""
     coord = make_points("gaussian", 1500, 14)
     R = O.RefH2("gaussian", [1.0], coord, 1e-6, BD_JIT=1, max_leaf_points=100)
     lib = _abi.libh2pack_gpu()
     try:
         x = np.ones(R.N)
         y = np.zeros(R.N)
-        assert lib.H2P_gpu_matvec(R.h2pack, O.dptr(x), O.dptr(y)) == _abi.H2GPU_OK - 5
-        assert b"H2P_gpu_set_kernel" in lib.H2P_gpu_last_error()
+        assert lib.H2P_gpu_matvec(R.h2pack, O.dptr(x), O.dptr(y)) == 0
+        assert rel(y, R.matvec(x)) < TOL64
+        p = np.array([1.0, 0, 0, 0])
+        assert lib.H2P_gpu_set_kernel(R.h2pack, _abi.KRNL_MATERN32, O.dptr(p), 1) == 0
+        assert lib.H2P_gpu_matvec(R.h2pack, O.dptr(x), O.dptr(y)) == 0
+        assert rel(y, R.matvec(x)) > 1e-3
     finally:
         lib.H2P_gpu_release(R.h2pack)
         R.close()

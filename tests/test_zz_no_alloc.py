@@ -39,10 +39,19 @@ def test_noalloc_matches_regular_apply_twice(name, precision):
         y_ref = img.matmul_device(x)            # regular path (allocates its work buffers)
         torch.cuda.synchronize()
         y_ref = y_ref[:, 0].cpu().numpy()
-        for _ in range(2):                      # the scratch keeps the previous call's contents
-            y = torch.full((img.N,), float("nan"), dtype=torch.float64, device="cuda")
-            img.matvec_device_noalloc(x[:, 0].contiguous(), y)
+        x0 = x[:, 0].contiguous()
+        ys = [torch.full((img.N,), float("nan"), dtype=torch.float64, device="cuda") for _ in range(3)]
+        torch.cuda.synchronize()
+        free_before = None
+        for y in ys:                            # the scratch keeps the previous call's contents
+            img.matvec_device_noalloc(x0, y)
             torch.cuda.synchronize()
+            if free_before is None:
+                # the first call on the device may load the library's device module (and
+                # with it the scratch array); later calls allocate nothing on the device
+                free_before = torch.cuda.mem_get_info()[0]
+            else:
+                assert torch.cuda.mem_get_info()[0] == free_before
             assert rel(y.cpu().numpy(), y_ref) < 1e-12
     finally:
         img.close()
@@ -61,3 +70,24 @@ def test_noalloc_rejects_images_beyond_the_limit():
             img.matvec_device_noalloc(x, y)
     finally:
         H.close()
+
+
+def test_noalloc_refuses_mixed_image_before_its_first_apply():
+    """A mixed-precision image holds FP32 copies of U/B/D only after one allocating
+    apply; before that the no-allocation entry point refuses it (status STATE) and
+    leaves the caller's current device unchanged."""
+    import torch
+    img, _h = image_from("coulomb_aot", "mixed")
+    try:
+        x = torch.randn(img.N, dtype=torch.float64, device="cuda")
+        y = torch.zeros_like(x)
+        dev = torch.cuda.current_device()
+        with pytest.raises(RuntimeError, match="STATE"):
+            img.matvec_device_noalloc(x, y)
+        assert torch.cuda.current_device() == dev
+        img.matmul_device(x[:, None].contiguous())     # makes the FP32 copies
+        img.matvec_device_noalloc(x, y)
+        torch.cuda.synchronize()
+        assert torch.isfinite(y).all()
+    finally:
+        img.close()
