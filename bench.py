@@ -304,9 +304,15 @@ def run_ours(args):
                 "peak_source": "nominal FP32 FMA peak 148 SM x 128 lanes x 2 x 1.965 GHz (no measured FP32 figure)",
                 "flop_model": f"unordered point pairs x ({flop_per_pair}) = H2Pack JIT_flops model with 16 RHS"}
 
-    cpu = None
+    cpu, parity = None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(H, args)
+        Xh64 = np.ascontiguousarray(X.cpu().numpy())
+        cpu, Yref = cpu_baseline(H, args, Xh64)
+        if Yref is not None:
+            # same representation, same inputs: the FP64 GPU result against H2Pack's own
+            # CPU H2P_matmul (relative 2-norm over all rows and columns)
+            parity = {"fp64_vs_reference": rel2(Y64.cpu().numpy(), Yref) if fp64 else None,
+                      "mixed_vs_reference": rel2(Ym.cpu().numpy(), Yref)}
 
     if rank == 0:
         line = {
@@ -322,7 +328,7 @@ def run_ours(args):
                        "jit_pairs_B": st["jit_pairs_B"], "jit_pairs_D": st["jit_pairs_D"]},
             "phase_ms": {"gather+up": phase[0], "B_far": phase[1], "down": phase[2], "D_near": phase[3],
                          "assemble": phase[4]},
-            "fp64": fp64, "rel_err_vs_direct": err, "e2e": e2e, "gpu_launches": int(launches),
+            "fp64": fp64, "rel_err_vs_direct": err, "parity": parity, "e2e": e2e, "gpu_launches": int(launches),
             "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)
@@ -331,22 +337,29 @@ def run_ours(args):
         pg.destroy_process_group()
 
 
-def cpu_baseline(H, args):
-    """H2Pack's CPU H2P_matmul (reference library) on the same handle and 16 RHS: one call."""
+def rel2(a, b):
+    """Relative 2-norm difference ||a - b|| / ||b||."""
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def cpu_baseline(H, args, X):
+    """H2Pack's CPU H2P_matmul (reference library) on the same handle and the same 16 RHS
+    the GPU applied: one call.  Returns the baseline record and H2Pack's result."""
     try:
         from oracle import oracle as O
         lib = O.libref()
     except Exception as e:  # pragma: no cover - reported, not fatal
-        return {"value": None, "unavailable": str(e)}
-    nv = args.nvec
-    X = np.random.default_rng(3).standard_normal((H.N, nv))
+        return {"value": None, "unavailable": str(e)}, None
+    nv = X.shape[1]
     Y = np.zeros((H.N, nv))
     t = time.perf_counter()
     lib.H2P_matmul(H.h2pack, 101, nv, O.dptr(X), nv, O.dptr(Y), nv)
     sec = time.perf_counter() - t
     return {"value": nv / sec, "unit": UNIT, "cores": H.info["n_thread"], "kind": "reference",
             "sample": f"1 H2P_matmul ({nv} RHS) of H2Pack compiled from its sources on the same N={args.n} "
-                      f"handle, {sec:.1f} s"}
+                      f"handle and inputs, {sec:.1f} s"}, Y
 
 
 def timed_loop(fn, steps, warm):
@@ -393,19 +406,28 @@ def run_aot_coulomb(args):
                      "stored_GBps": stored / (ms * 1e-3) / 1e9, "ref_model_GBps": st["ref_mv_bytes"] / (ms * 1e-3) / 1e9,
                      "stored_bytes": stored}
     err = None
+    H.set_precision("fp64")
+    y64 = img.matmul_device(x).cpu().numpy()[:, 0]
+    ymx = None
+    if "mixed" in precs:
+        H.set_precision("mixed")
+        ymx = img.matmul_device(x).cpu().numpy()[:, 0]
     if args.check_rows > 0:
-        H.set_precision("fp64")
-        y64 = img.matmul_device(x).cpu().numpy()[:, 0]
         rng = np.random.default_rng(2)
         rows = rng.choice(H.N, min(args.check_rows, H.N), replace=False)
         yd = direct_sum("coulomb", [], coord, x.cpu().numpy()[:, 0], coord[:, rows])
-        err = float(np.linalg.norm(y64[rows] - yd) / np.linalg.norm(yd))
-    cpu = None
+        err = {"fp64": rel2(y64[rows], yd)}
+        if ymx is not None:
+            err["mixed"] = rel2(ymx[rows], yd)
+    cpu, parity = None, None
     if not args.no_cpu_baseline:
         from oracle import oracle as O
         xh = x.cpu().numpy()[:, 0].copy()
         yh = np.zeros(H.N)
         O.libref().H2P_matvec(H.h2pack, O.dptr(xh), O.dptr(yh))
+        # same representation, same input: GPU against H2Pack's own CPU H2P_matvec
+        parity = {"fp64_vs_reference": rel2(y64, yh),
+                  "mixed_vs_reference": rel2(ymx, yh) if ymx is not None else None}
         t = time.perf_counter()
         reps = 3
         for _ in range(reps):
@@ -418,7 +440,7 @@ def run_aot_coulomb(args):
     main_p = "fp64" if "fp64" in out else precs[0]
     line = {"metric": f"H2 matvecs/s (Coulomb N=80k AOT {main_p.upper()}, 1 RHS)", "value": out[main_p]["matvecs_per_s"],
             "unit": "matvecs/s", "workload": "aot_coulomb", "n": n, "build_seconds": build_s,
-            "fp64": out.get("fp64"), "mixed": out.get("mixed"), "rel_err_vs_direct_fp64": err,
+            "fp64": out.get("fp64"), "mixed": out.get("mixed"), "rel_err_vs_direct": err, "parity": parity,
             "roofline": {"bound": "hbm", "achieved": out[main_p]["stored_GBps"], "peak": peak, "unit": "GB/s",
                          "frac": out[main_p]["stored_GBps"] / peak,
                          "note": "stored U (read twice), B and D bytes per matvec / matvec time, of measured copy BW"},
@@ -490,7 +512,7 @@ def run_aot_rpy(args):
                 yc = Ys[prec][:, c].cpu().numpy()[rows]
                 e.append(float(np.linalg.norm(yc - yd) / np.linalg.norm(yd)))
             err[prec] = max(e)
-    cpu = None
+    cpu, parity = None, None
     if not args.no_cpu_baseline:
         from oracle import oracle as O
         from h2pack_b200 import _abi
@@ -500,14 +522,17 @@ def run_aot_rpy(args):
         O.libref().H2P_matmul(H.h2pack, _abi.ROW_MAJOR, nv, O.dptr(Xh), nv, O.dptr(Yh), nv)
         sec = time.perf_counter() - t
         cpu = {"value": nv / sec, "unit": "matvecs/s", "cores": H.info["n_thread"], "kind": "reference",
-               "sample": f"1 H2P_matmul ({nv} RHS) of H2Pack compiled from its sources, same handle, {sec:.1f} s"}
+               "sample": f"1 H2P_matmul ({nv} RHS) of H2Pack compiled from its sources, same handle and "
+                         f"inputs, {sec:.1f} s"}
+        # same representation, same inputs: GPU against H2Pack's own CPU H2P_matmul
+        parity = {f"{p}_vs_reference": rel2(Ys[p].cpu().numpy(), Yh) for p in precs}
     peak = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]) \
         if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else 6650.0
     main_p = "mixed" if "mixed" in out else precs[0]
     line = {"metric": f"H2 matvecs/s (RPY N={n} AOT, reltol 1e-8, {nv} RHS)", "value": out[main_p]["matvecs_per_s"],
             "unit": "matvecs/s", "workload": "aot_rpy", "n": n, "nvec": nv, "build_seconds": build_s,
             "tuned_panel_variant": tuned,
-            "fp64": out.get("fp64"), "mixed": out.get("mixed"), "rel_err_vs_direct": err,
+            "fp64": out.get("fp64"), "mixed": out.get("mixed"), "rel_err_vs_direct": err, "parity": parity,
             "speedup_mixed_vs_fp64": out["fp64"]["ms"] / out["mixed"]["ms"] if len(out) == 2 else None,
             "roofline": {"bound": "hbm", "achieved": out[main_p]["streamed_GBps"], "peak": peak, "unit": "GB/s",
                          "frac": out[main_p]["streamed_GBps"] / peak,
