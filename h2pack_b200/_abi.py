@@ -88,6 +88,8 @@ H2GPU_SYMBOLS = {
     "h2gpu_cg_step": (C.c_int, [C.c_void_p, C.c_int]),
     "h2gpu_cg_check": (C.c_int, [C.c_void_p]),
     "h2gpu_cg_sync": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), _dp]),
+    "h2gpu_cg_query": (C.c_int, [C.c_void_p]),
+    "h2gpu_cg_cancel": (C.c_int, [C.c_void_p, C.c_int]),
     "h2gpu_cg_take": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "h2gpu_cg_history": (C.c_int, [C.c_void_p, C.c_int, _dp, C.c_int]),
     "h2gpu_batch_create": (C.c_int, [C.POINTER(Desc), C.c_int, C.POINTER(Options), C.POINTER(C.c_void_p)]),

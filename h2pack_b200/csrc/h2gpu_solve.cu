@@ -295,6 +295,7 @@ struct h2gpu_cg {
     CgSlot* h_sl = nullptr;     // pinned mirror, refreshed by h2gpu_cg_sync
     double* d_hist = nullptr;
     int refresh = 0;
+    cudaEvent_t done = nullptr; // recorded after the work each h2gpu_cg_step / h2gpu_cg_check enqueues
 };
 
 #define CGCK(call)                                                                     \
@@ -311,7 +312,8 @@ static void cg_free_all(h2gpu_cg* g)
     if (g->d_sl) cudaFree(g->d_sl);
     if (g->d_hist) cudaFree(g->d_hist);
     if (g->h_sl) cudaFreeHost(g->h_sl);
-    g->mem = nullptr; g->d_sl = nullptr; g->d_hist = nullptr; g->h_sl = nullptr;
+    if (g->done) cudaEventDestroy(g->done);
+    g->mem = nullptr; g->d_sl = nullptr; g->d_hist = nullptr; g->h_sl = nullptr; g->done = nullptr;
 }
 
 H2G_API int h2gpu_cg_create(h2gpu_image* img, double mu, int refresh, h2gpu_cg** out)
@@ -334,7 +336,8 @@ H2G_API int h2gpu_cg_create(h2gpu_image* img, double mu, int refresh, h2gpu_cg**
         if (cudaMalloc(&g->mem, sizeof(double) * (5 * panel + (size_t) G * kS)) != cudaSuccess ||
             cudaMalloc(&g->d_sl, sizeof(CgSlot) * kS) != cudaSuccess ||
             cudaMalloc(&g->d_hist, sizeof(double) * kS * kHist) != cudaSuccess ||
-            cudaMallocHost(&g->h_sl, sizeof(CgSlot) * kS) != cudaSuccess)
+            cudaMallocHost(&g->h_sl, sizeof(CgSlot) * kS) != cudaSuccess ||
+            cudaEventCreateWithFlags(&g->done, cudaEventDisableTiming) != cudaSuccess)
         {
             stc = h2gpu::set_error(H2GPU_ERR_NOMEM, "CG engine allocation failed");
             break;
@@ -430,6 +433,7 @@ H2G_API int h2gpu_cg_step(h2gpu_cg* g, int n_iter)
         k_cg_finish<<<1, 256, 0, g->stream>>>(g->c);
     }
     CGCK(cudaGetLastError());
+    CGCK(cudaEventRecord(g->done, g->stream));
     return H2GPU_OK;
 }
 
@@ -445,10 +449,39 @@ H2G_API int h2gpu_cg_check(h2gpu_cg* g)
     k_cg_resid<<<g->c.G, 256, 0, g->stream>>>(g->c);
     k_cg_check_finish<<<1, 256, 0, g->stream>>>(g->c);
     CGCK(cudaGetLastError());
+    CGCK(cudaEventRecord(g->done, g->stream));
     // a checked slot either finished or restarts: until the next sync the host view
     // counts it as running, so the next step's panel covers it
     for (int k = 0; k < kS; k++)
         if (g->h_sl[k].state == H2GPU_CG_CHECK) g->h_sl[k].state = H2GPU_CG_RUN;
+    return H2GPU_OK;
+}
+
+// 1 when the work enqueued by the last h2gpu_cg_step / h2gpu_cg_check has finished (a
+// following h2gpu_cg_sync then returns without waiting on the device), 0 while it runs.
+H2G_API int h2gpu_cg_query(h2gpu_cg* g)
+{
+    if (!g) return h2gpu::set_error(H2GPU_ERR_INVALID, "engine is NULL");
+    std::lock_guard<std::mutex> lk(g->lock);
+    CGCK(cudaSetDevice(g->device));
+    cudaError_t e = cudaEventQuery(g->done);
+    if (e == cudaSuccess) return 1;
+    if (e == cudaErrorNotReady) return 0;
+    return h2gpu::set_error(H2GPU_ERR_CUDA, cudaGetErrorString(e));
+}
+
+// Free a slot whatever its state (a request given up by its caller): iterations already
+// enqueued finish first (stream order), then the slot takes no further part and may be
+// admitted again.
+H2G_API int h2gpu_cg_cancel(h2gpu_cg* g, int slot)
+{
+    if (!g) return h2gpu::set_error(H2GPU_ERR_INVALID, "engine is NULL");
+    if (slot < 0 || slot >= kS) return h2gpu::set_error(H2GPU_ERR_INVALID, "slot out of range [0, 16)");
+    std::lock_guard<std::mutex> lk(g->lock);
+    CGCK(cudaSetDevice(g->device));
+    k_cg_free<<<1, 1, 0, g->stream>>>(g->d_sl, slot);
+    CGCK(cudaGetLastError());
+    g->h_sl[slot].state = H2GPU_CG_FREE;
     return H2GPU_OK;
 }
 

@@ -9,6 +9,14 @@ applies the matrix once to the panel of all its slots (one H2 matmul), a finishe
 request frees its slot at once, and the engines of different matrices run on their
 images' own streams, so their work overlaps on the device.
 
+Engines are decoupled: the scheduler never waits on one engine while others could
+run.  It polls every in-flight engine's completion (``h2gpu_cg_query``, an event
+recorded after its enqueued iterations), collects an engine as soon as it is done and
+relaunches it at once, so requests on a small matrix cycle at that matrix's pace and
+never wait for the iterations of a large one.  A request may carry a deadline
+(``timeout`` seconds after its arrival); past it, it is dropped from the queue or its
+slot is cancelled (``h2gpu_cg_cancel``) and it is returned with status "timeout".
+
 The solver is H2Pack's left-preconditioned CG (examples/PCG/pcg.c:11-152, identity
 preconditioner, shift wrapper of examples/SPDHSS-H2/pcg_tests.c:13-20) in lock step
 for the slots of an engine: FP64 vectors and inner products on the device, the
@@ -42,7 +50,9 @@ class Request:
     arrival: float = 0.0       # seconds from the start of the run
     tol: float = 1e-6
     max_iter: int = 5000
+    timeout: float | None = None   # seconds after arrival; None: no deadline
     # filled by the server
+    status: str = ""           # "done" or "timeout"
     x: torch.Tensor | None = None
     start: float | None = None
     finish: float | None = None
@@ -69,6 +79,7 @@ class SlotBlock:
         self.free = list(range(self.S - 1, -1, -1))
         self.history = False
         self.need_check = False
+        self.inflight = False
         self._st = (C.c_int * 16)()
         self._it = (C.c_int * 16)()
         self._rr = (C.c_double * 16)()
@@ -103,10 +114,33 @@ class SlotBlock:
         if self.need_check:
             _abi.check(self.lib.h2gpu_cg_check(self.h), self.lib, "h2gpu_cg_check")
         _abi.check(self.lib.h2gpu_cg_step(self.h, self.k), self.lib, "h2gpu_cg_step")
+        self.inflight = True
+
+    def ready(self) -> bool:
+        """True when the enqueued work has finished on the device (does not wait)."""
+        st = self.lib.h2gpu_cg_query(self.h)
+        if st < 0:
+            _abi.check(st, self.lib, "h2gpu_cg_query")
+        return st == 1
+
+    def cancel(self, r: Request) -> bool:
+        """Give up a request holding a slot; its slot is free for the next admission."""
+        for k in range(16):
+            if self.req[k] is r:
+                _abi.check(self.lib.h2gpu_cg_cancel(self.h, k), self.lib, "h2gpu_cg_cancel")
+                self.req[k] = None
+                self.free.append(k)
+                return True
+        return False
+
+    def requests(self) -> list:
+        return [r for r in self.req if r is not None]
 
     def collect(self, now_fn, out: list):
-        """Wait for the engine, hand out finished requests, note slots awaiting a check."""
+        """Read the slot records of a finished engine, hand out finished requests, note
+        slots awaiting a check."""
         _abi.check(self.lib.h2gpu_cg_sync(self.h, self._st, self._it, self._rr), self.lib, "h2gpu_cg_sync")
+        self.inflight = False
         t = now_fn()
         self.need_check = False
         for k in range(16):
@@ -129,6 +163,7 @@ class SlotBlock:
                         n = self.lib.h2gpu_cg_history(self.h, k, buf.ctypes.data_as(C.POINTER(C.c_double)), len(buf))
                         r.history = [float(v) for v in buf[:max(0, n)]]
                 r.finish = t
+                r.status = "done"
                 out.append(r)
                 self.req[k] = None
                 self.free.append(k)
@@ -165,10 +200,17 @@ class Server:
             blk.close()
         self.footprint.pop(name, None)
 
-    def run(self, requests: list[Request], realtime: bool = True, history: bool = False) -> list[Request]:
+    def run(self, requests: list[Request], realtime: bool = True, history: bool = False,
+            poll_sleep: float = 50e-6) -> list[Request]:
         """Serve requests whose ``arrival`` offsets follow the wall clock (realtime) or
         are all present at time 0 (realtime=False).  Returns them in completion order.
-        ``history`` records every PCG request's residual norm after each iteration."""
+        ``history`` records every PCG request's residual norm after each iteration.
+
+        Each pass: arrivals join their matrix's FIFO queue; requests past their deadline
+        leave (queue or slot); every in-flight engine whose work has finished is
+        collected; queued requests take the free slots; every idle engine with busy
+        slots is launched.  Nothing waits on one engine while another could make
+        progress."""
         for blk in self.blocks.values():
             blk.history = history
         pending = [(r.arrival if realtime else 0.0, r.rid, r) for r in requests]
@@ -179,6 +221,13 @@ class Server:
 
         def now():
             return time.perf_counter() - t0
+
+        def expired(r, t):
+            return r.timeout is not None and t - (r.arrival if realtime else 0.0) > r.timeout
+
+        def give_up(r, t):
+            r.finish, r.status = t, "timeout"
+            done.append(r)
 
         # the right-hand sides were written on torch's stream; the engines read them on
         # their images' streams
@@ -192,22 +241,43 @@ class Server:
                 waiting[r.matrix].append(r)
             for name, blk in self.blocks.items():
                 q = waiting[name]
+                for r in [r for r in q if expired(r, t)]:
+                    q.remove(r)
+                    give_up(r, t)
+                for r in [r for r in blk.requests() if expired(r, t)]:
+                    blk.cancel(r)
+                    give_up(r, t)
+            progressed = False
+            for blk in self.blocks.values():      # collect every engine that has finished
+                if blk.inflight and blk.ready():
+                    blk.collect(now, done)
+                    progressed = True
+            t = now()
+            for name, blk in self.blocks.items():  # freed slots take queued requests
+                q = waiting[name]
                 while q and blk.admit(q[0], t):
                     q.pop(0)
-            busy = [b for b in self.blocks.values() if b.busy()]
-            if not busy:
-                if pending:
-                    time.sleep(max(0.0, min(pending[0][0] - now(), 0.001)))
-                continue
-            for blk in busy:          # all engines enqueue first: their work overlaps
-                blk.launch()
-            for blk in busy:
+            for blk in self.blocks.values():      # relaunch idle engines at once
+                if not blk.inflight and blk.busy():
+                    blk.launch()
+                    progressed = True
+            if not progressed:
+                nxt = pending[0][0] - now() if pending and not any(b.inflight for b in self.blocks.values()) else 0.0
+                time.sleep(min(max(nxt, poll_sleep), 0.001))
+        for blk in self.blocks.values():          # no engine keeps work in flight
+            if blk.inflight:
+                while not blk.ready():
+                    time.sleep(poll_sleep)
                 blk.collect(now, done)
         return done
 
 
 def latency_stats(reqs: list[Request]) -> dict:
-    lat = np.array([r.finish - r.arrival for r in reqs])
-    span = max(r.finish for r in reqs) - min(r.arrival for r in reqs)
-    return {"n": len(reqs), "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
-            "mean_ms": float(lat.mean() * 1e3), "throughput_req_s": len(reqs) / span if span > 0 else None}
+    """Latency percentiles and throughput of the requests served to completion (requests
+    that timed out are counted separately)."""
+    ok = [r for r in reqs if r.status != "timeout"]
+    lat = np.array([r.finish - r.arrival for r in ok])
+    span = max(r.finish for r in ok) - min(r.arrival for r in ok)
+    return {"n": len(ok), "n_timeout": len(reqs) - len(ok), "p50_ms": float(np.percentile(lat, 50) * 1e3),
+            "p99_ms": float(np.percentile(lat, 99) * 1e3), "mean_ms": float(lat.mean() * 1e3),
+            "throughput_req_s": len(ok) / span if span > 0 else None}

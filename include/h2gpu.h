@@ -280,6 +280,13 @@ int h2gpu_cg_admit(h2gpu_cg *cg, int slot, int kind, const double *d_b, double t
 int h2gpu_cg_step(h2gpu_cg *cg, int n_iter);
 int h2gpu_cg_check(h2gpu_cg *cg);
 int h2gpu_cg_sync(h2gpu_cg *cg, int *state, int *iters, double *relres);   /* 16 entries each */
+/* 1 when the work of the last h2gpu_cg_step / h2gpu_cg_check has finished on the device,
+ * 0 while it runs (no waiting): a scheduler polls its engines and collects each one as
+ * soon as it is done, so engines of small and large matrices do not wait for each other. */
+int h2gpu_cg_query(h2gpu_cg *cg);
+/* Free a slot whatever its state (a request given up, e.g. past its deadline); work
+ * already enqueued finishes first, then the slot may be admitted again. */
+int h2gpu_cg_cancel(h2gpu_cg *cg, int slot);
 int h2gpu_cg_take(h2gpu_cg *cg, int slot, double *d_x);
 int h2gpu_cg_history(h2gpu_cg *cg, int slot, double *out, int max_n);      /* ||r|| per iteration; returns count */
 

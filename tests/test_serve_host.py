@@ -9,6 +9,10 @@ tests check:
 - a finished request frees its slot for the next one at once;
 - every busy engine is launched before any is collected, so their device work
   overlaps;
+- engines are decoupled: a fast engine's requests finish while a slow engine's
+  iterations are still in flight (no head-of-line blocking across matrices);
+- a request past its deadline leaves its queue or its slot (cancelled) with status
+  "timeout", and its slot serves the next request;
 - an unknown matrix is an error.
 """
 import pytest
@@ -17,10 +21,11 @@ from h2pack_b200 import serve
 
 
 class FakeImage:
-    def __init__(self, N, device_bytes):
+    def __init__(self, N, device_bytes, latency=0):
         self.N = N
         self._bytes = device_bytes
         self.lib = None
+        self.latency = latency
 
     def stats(self):
         return {"device_bytes": self._bytes}
@@ -36,6 +41,10 @@ class FakeBlock:
         self.done_iters = {}
         self.history = False
         self.max_in_flight = 0
+        self.inflight = False
+        self.polls_left = 0
+        self.cancelled = []
+        self.latency = getattr(image, "latency", 0)   # polls until a launch is done
 
     def busy(self):
         return len(self.free) < self.S
@@ -54,14 +63,35 @@ class FakeBlock:
         FakeBlock.log.append(("launch", id(self)))
         for k in self.req:
             self.done_iters[k] += self.k
+        self.inflight = True
+        self.polls_left = self.latency
+
+    def ready(self):
+        if self.polls_left > 0:
+            self.polls_left -= 1
+            return False
+        return True
+
+    def requests(self):
+        return list(self.req.values())
+
+    def cancel(self, r):
+        for k, q in list(self.req.items()):
+            if q is r:
+                del self.req[k]
+                self.free.append(k)
+                self.cancelled.append(r.rid)
+                return True
+        return False
 
     def collect(self, now_fn, out):
         FakeBlock.log.append(("collect", id(self)))
+        self.inflight = False
         t = now_fn()
         for k in sorted(self.req):
             r = self.req[k]
             if self.done_iters[k] >= r.max_iter:
-                r.iters, r.finish, r.converged, r.relres = self.done_iters[k], t, True, 0.0
+                r.iters, r.finish, r.converged, r.relres, r.status = self.done_iters[k], t, True, 0.0, "done"
                 out.append(r)
                 del self.req[k]
                 self.free.append(k)
@@ -81,8 +111,8 @@ def fake_engine(monkeypatch):
     return FakeBlock
 
 
-def req(rid, matrix, iters, kind="pcg"):
-    return serve.Request(rid=rid, matrix=matrix, kind=kind, b=None, max_iter=iters)
+def req(rid, matrix, iters, kind="pcg", timeout=None):
+    return serve.Request(rid=rid, matrix=matrix, kind=kind, b=None, max_iter=iters, timeout=timeout)
 
 
 def test_budget_admits_and_refuses(fake_engine):
@@ -130,3 +160,48 @@ def test_unknown_matrix_is_an_error(fake_engine):
     assert srv.admit_matrix("a", FakeImage(4, 0), mu=1e-2)
     with pytest.raises(KeyError):
         srv.run([req(0, "nope", 8)], realtime=False)
+
+
+def test_fast_engine_does_not_wait_for_a_slow_one(fake_engine):
+    """A slow engine (its launches take 200 polls) and a fast one: every request of the
+    fast matrix finishes while the slow engine's first launch is still in flight."""
+    srv = serve.Server(budget_bytes=1e12, max_slots=2, iters_per_sync=8)
+    assert srv.admit_matrix("slow", FakeImage(4, 0, latency=200), mu=1e-2)
+    assert srv.admit_matrix("fast", FakeImage(4, 0), mu=1e-2)
+    reqs = [req(0, "slow", 8)] + [req(1 + i, "fast", 16) for i in range(6)]
+    done = srv.run(reqs, realtime=False, poll_sleep=0.0)
+    order = [r.rid for r in done]
+    assert order[-1] == 0                     # the slow request finishes last ...
+    assert sorted(order[:-1]) == list(range(1, 7))
+    slow = srv.blocks["slow"]
+    collects = [i for i, e in enumerate(FakeBlock.log) if e == ("collect", id(slow))]
+    fast_collects = [i for i, e in enumerate(FakeBlock.log) if e[0] == "collect" and e[1] != id(slow)]
+    assert len(collects) == 1                 # ... after one launch of its own,
+    assert len(fast_collects) >= 6 and max(fast_collects) < collects[0]   # which the fast engine never waited for
+
+
+def test_requests_past_their_deadline_time_out(fake_engine):
+    """One slot: the first request holds it past its deadline and is cancelled; the
+    queued request behind it with a short deadline expires in the queue; the third
+    (no deadline) then runs to completion in the freed slot."""
+    srv = serve.Server(budget_bytes=1e12, max_slots=1, iters_per_sync=8)
+    assert srv.admit_matrix("m", FakeImage(4, 0, latency=10 ** 9), mu=1e-2)
+    blk = srv.blocks["m"]
+    reqs = [req(0, "m", 8, timeout=0.02), req(1, "m", 8, timeout=0.01), req(2, "m", 8)]
+
+    # the slot's first launch never finishes on its own; once request 0 is cancelled the
+    # engine is made fast so that request 2 can complete
+    orig_cancel = blk.cancel
+
+    def cancel(r):
+        ok = orig_cancel(r)
+        blk.latency = 0
+        blk.polls_left = 0
+        return ok
+    blk.cancel = cancel
+    done = srv.run(reqs, realtime=False, poll_sleep=0.0)
+    st = {r.rid: r.status for r in done}
+    assert st == {0: "timeout", 1: "timeout", 2: "done"}
+    assert blk.cancelled == [0]
+    stats = serve.latency_stats(done)
+    assert stats["n"] == 1 and stats["n_timeout"] == 2

@@ -137,3 +137,19 @@ def test_pcg_fp64_follows_reference_pcg(mats):
     k = min(20, len(hist), len(h_gpu))
     assert np.max(np.abs(h_gpu[:k] - hist[:k]) / hist[:k]) < 1e-8
     assert rel(r.x.cpu().numpy(), x) < 1e-3
+
+
+def test_deadline_cancels_a_slot_and_frees_it(mats):
+    """One slot: a PCG request with a tiny deadline is cancelled on the device after its
+    first launch; the matvec queued behind it then takes the freed slot and gives the
+    exact shifted product."""
+    from h2pack_b200.serve import Server
+    H = mats["g"]
+    srv = Server(max_slots=1)
+    assert srv.admit_matrix("g", H.image(), MU, "fp64")
+    slow, mv = requests(H, ["pcg", "matvec"], 11, "g")
+    slow.timeout, slow.tol = 1e-4, 1e-14        # cannot finish in time
+    done = {r.rid: r for r in srv.run([slow, mv], realtime=False)}
+    assert done[slow.rid].status == "timeout" and done[slow.rid].x is None
+    assert done[mv.rid].status == "done"
+    assert rel(done[mv.rid].x.cpu().numpy(), fp64_apply(H, mv.b).cpu().numpy()) < 1e-13
