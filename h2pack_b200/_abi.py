@@ -16,6 +16,7 @@ LIBH2GPU = os.path.join(LIB_DIR, "libh2gpu.so")
 LIBH2PACK_GPU = os.path.join(LIB_DIR, "libH2Pack_gpu.so")
 
 H2GPU_OK = 0
+BLOCKS_GIVEN, BLOCKS_GENERATE = 0, 1
 STATUS_NAMES = {0: "OK", -1: "INVALID", -2: "UNSUPPORTED", -3: "CUDA", -4: "NOMEM", -5: "STATE", -6: "DEVICE"}
 
 KRNL_COULOMB, KRNL_GAUSSIAN, KRNL_MATERN32, KRNL_RPY = 1, 2, 3, 4
@@ -53,7 +54,7 @@ class Desc(C.Structure):
 
 class Options(C.Structure):
     """struct h2gpu_options"""
-    _fields_ = [("precision", C.c_int), ("max_n_vec", C.c_int), ("device", C.c_int)]
+    _fields_ = [("precision", C.c_int), ("max_n_vec", C.c_int), ("device", C.c_int), ("blocks", C.c_int)]
 
 
 class Stats(C.Structure):
@@ -97,6 +98,7 @@ H2GPU_SYMBOLS = {
     "h2gpu_graph_launch": (C.c_int, [C.c_void_p, C.c_void_p]),
     "h2gpu_autotune": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int,
                                  C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "h2gpu_get_blocks": (C.c_int, [C.c_void_p, C.c_int, _dp, C.c_size_t]),
     "h2gpu_get_stats": (C.c_int, [C.c_void_p, C.POINTER(Stats)]),
     "h2gpu_reset_stats": (C.c_int, [C.c_void_p]),
     "h2gpu_image_bytes": (C.c_size_t, [C.c_void_p]),

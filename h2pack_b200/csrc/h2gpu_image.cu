@@ -174,6 +174,8 @@ struct h2gpu_image {
     int* d_status = nullptr; // device status word (bounded waits of the tcgen05 kernel)
     int* h_status = nullptr; // pinned host copy, read back at the end of every timed panel
     int tuned_nv = 0;        // panel width chosen by the autotuner (0: default rule)
+    int gen = 0;             // stored blocks generated on the device (H2GPU_BLOCKS_GENERATE)
+    int f32_only = 0;        // the stored blocks exist in FP32 only (generated for a mixed image)
     int n_images = 1;        // matrices in this image (batched images hold several)
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
@@ -203,7 +205,7 @@ int npt_of(const h2gpu_desc* d, int n) { return d->pt_cluster[2 * n + 1] - d->pt
 
 // Structural checks of the descriptor; every index used by a kernel is checked here,
 // so the device code indexes without bounds checks.
-int validate(const h2gpu_desc* d)
+int validate(const h2gpu_desc* d, bool gen = false)
 {
     REQ(d != nullptr, "descriptor is NULL");
     REQ(d->n_point > 0 && d->n_node > 0 && d->n_leaf_node > 0, "empty representation");
@@ -283,8 +285,18 @@ int validate(const h2gpu_desc* d)
         REQ(d->coord && d->J_n && d->J_coord, "JIT mode needs coordinates and skeleton points");
     } else {
         REQ(d->n_B == d->n_r_adm_pair, "n_B != n_r_adm_pair");
-        REQ(d->n_B == 0 || (d->B_nrow && d->B_ncol && d->B_ptr && d->B_data), "AOT mode needs B blocks");
-        REQ(d->D_nrow && d->D_ncol && d->D_ptr && d->D_data, "AOT mode needs D blocks");
+        REQ(d->n_B == 0 || (d->B_nrow && d->B_ncol && d->B_ptr && (gen || d->B_data)), "AOT mode needs B blocks");
+        REQ(d->D_nrow && d->D_ncol && d->D_ptr && (gen || d->D_data), "AOT mode needs D blocks");
+    }
+    if (gen)
+    {
+        // the blocks are generated from the kernel, the points and the skeleton points
+        REQ(d->kernel_id >= H2GPU_KRNL_COULOMB && d->kernel_id <= H2GPU_KRNL_RPY,
+            "generated blocks need a kernel id (H2GPU_KRNL_*), got %d", d->kernel_id);
+        REQ((d->kernel_id == H2GPU_KRNL_RPY) == (kd == 3), "kernel id does not match krnl_dim");
+        REQ(d->kernel_id != H2GPU_KRNL_RPY || d->xpt_dim == 4, "RPY needs 4 coordinate rows");
+        REQ(d->kernel_id == H2GPU_KRNL_COULOMB || d->n_krnl_param >= 1, "kernel needs a parameter");
+        REQ(d->coord && d->J_n && d->J_coord, "generated blocks need coordinates and skeleton points");
     }
     return H2GPU_OK;
 }
@@ -960,6 +972,78 @@ int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
     return H2GPU_OK;
 }
 
+// ------------------------------------------------- stored blocks generated on the device
+
+// Point arena and generation tasks of the stored blocks (H2GPU_BLOCKS_GENERATE).  Point
+// space as in JIT mode: the sorted points, then the skeleton points of every node.
+// Block i of B pairs (n0, n1) = r_adm_pairs[i]: rows are the skeleton points of n0 when
+// its level is not coarser than n1's, else the points of n0; columns likewise
+// (src/H2Pack_build.c:818-860).  D: the diagonal blocks of the leaves in leaf_nodes
+// order, then the inadmissible pairs, points against points (:1063-1110).
+struct GenPlan {
+    std::vector<double4> pts;
+    std::vector<GenTask> tB, tD;
+};
+
+int build_gen(const h2gpu_desc* d, GenPlan& g)
+{
+    const int kd = d->krnl_dim, n_node = d->n_node;
+    const int* lvl = d->node_level;
+    std::vector<int> jp0(n_node, 0);
+    long long np = d->n_point;
+    for (int n = 0; n < n_node; n++) { jp0[n] = (int) np; np += d->J_n[n]; }
+    REQ(np < (1LL << 31), "too many points");
+    g.pts.resize(np);
+    const bool rad = d->xpt_dim >= 4;
+    for (int p = 0; p < d->n_point; p++)
+        g.pts[p] = make_double4(d->coord[p], d->coord[(size_t) d->n_point + p], d->coord[2 * (size_t) d->n_point + p],
+                                rad ? d->coord[3 * (size_t) d->n_point + p] : 0.0);
+    for (int n = 0; n < n_node; n++)
+    {
+        const int nj = d->J_n[n];
+        if (nj > 0) REQ(d->J_coord[n] != nullptr, "node %d: skeleton coordinates missing", n);
+        const double* J = d->J_coord[n];
+        for (int j = 0; j < nj; j++)
+            g.pts[jp0[n] + j] = make_double4(J[j], J[nj + j], J[2 * nj + j], rad ? J[3 * nj + j] : 0.0);
+    }
+    const int GR = 16;   // row points per task
+    auto emit = [&](std::vector<GenTask>& out, size_t off, int rp0, int nrp, int cp0, int ncp, int nrow, int ncol,
+                    const char* what, int i) {
+        REQ(nrow == kd * nrp && ncol == kd * ncp, "%s block %d is %dx%d, its points give %dx%d", what, i, nrow, ncol,
+            kd * nrp, kd * ncp);
+        const size_t total = what[0] == 'B' ? d->B_ptr[d->n_B] : d->D_ptr[d->n_D];
+        REQ(off + (size_t) nrow * ncol <= total, "%s block %d lies outside the packed arena", what, i);
+        for (int r0 = 0; r0 < nrp; r0 += GR)
+        {
+            GenTask t;
+            t.a_off = (long long) off + (long long) kd * r0 * (long long) ncol;
+            t.row_pt0 = rp0 + r0;
+            t.nrp = std::min(GR, nrp - r0);
+            t.col_pt0 = cp0;
+            t.ncp = ncp;
+            out.push_back(t);
+        }
+        return H2GPU_OK;
+    };
+    for (int i = 0; i < d->n_B; i++)
+    {
+        const int n0 = d->r_adm_pairs[2 * i], n1 = d->r_adm_pairs[2 * i + 1];
+        const bool s0 = lvl[n0] >= lvl[n1], s1 = lvl[n1] >= lvl[n0];
+        const int rp0 = s0 ? jp0[n0] : d->pt_cluster[2 * n0], nrp = s0 ? d->J_n[n0] : npt_of(d, n0);
+        const int cp0 = s1 ? jp0[n1] : d->pt_cluster[2 * n1], ncp = s1 ? d->J_n[n1] : npt_of(d, n1);
+        TRY(emit(g.tB, d->B_ptr[i], rp0, nrp, cp0, ncp, d->B_nrow[i], d->B_ncol[i], "B", i));
+    }
+    for (int i = 0; i < d->n_D; i++)
+    {
+        int n0, n1;
+        if (i < d->n_leaf_node) n0 = n1 = d->leaf_nodes[i];
+        else { n0 = d->r_inadm_pairs[2 * (i - d->n_leaf_node)]; n1 = d->r_inadm_pairs[2 * (i - d->n_leaf_node) + 1]; }
+        TRY(emit(g.tD, d->D_ptr[i], d->pt_cluster[2 * n0], npt_of(d, n0), d->pt_cluster[2 * n1], npt_of(d, n1),
+                 d->D_nrow[i], d->D_ncol[i], "D", i));
+    }
+    return H2GPU_OK;
+}
+
 // ------------------------------------------------------------------ plan self-check
 
 // rows [beg, beg + n) of a space counted in cnt; false when they do not fit
@@ -1379,7 +1463,7 @@ int upload_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
         CK(launch_panel_pts(im->d_pg, im->n_pg, im->d_pts32, im->d_ppts, im->stream));
         CK(cudaStreamSynchronize(im->stream));
     }
-    if (!d->BD_JIT)
+    if (!d->BD_JIT && !im->gen)
     {
         if (im->B_elems)
         {
@@ -1571,9 +1655,58 @@ int check_status(h2gpu_image* im)
     return H2GPU_OK;
 }
 
+// Fill the stored-block arenas on the device (H2GPU_BLOCKS_GENERATE): FP64 for an FP64
+// image, FP32 only for a mixed one.  The point arena and the task lists are freed again.
+int generate_blocks(h2gpu_image* im, const GenPlan& g)
+{
+    const int fp32 = im->precision == H2GPU_PREC_MIXED;
+    const size_t es = fp32 ? 4 : 8;
+    double4* pts = nullptr;
+    GenTask* tasks = nullptr;
+    size_t dummy = 0;
+    int st = H2GPU_OK;
+    do {
+        if ((st = upload(g.pts, &pts, dummy)) != H2GPU_OK) break;
+        std::vector<GenTask> all(g.tB);
+        all.insert(all.end(), g.tD.begin(), g.tD.end());
+        if ((st = upload(all, &tasks, dummy)) != H2GPU_OK) break;
+        void* B = nullptr;
+        void* D = nullptr;
+        cudaError_t e = cudaSuccess;
+        if (im->B_elems) e = cudaMalloc(&B, es * im->B_elems);
+        if (e == cudaSuccess) e = cudaMalloc(&D, es * im->D_elems);
+        if (e != cudaSuccess)
+        {
+            if (B) cudaFree(B);
+            st = fail(H2GPU_ERR_NOMEM, "stored-block arenas of %.1f GB do not fit on the device",
+                      1e-9 * es * (im->B_elems + im->D_elems));
+            break;
+        }
+        if (fp32) { im->d_B32 = (float*) B; im->d_D32 = (float*) D; im->f32_only = 1; }
+        else { im->d_B64 = (double*) B; im->d_D64 = (double*) D; }
+        im->bytes += es * (im->B_elems + im->D_elems);
+        const KParam kp = kparam_of(im);
+        // one launch per block kind, in slices that keep the grid inside its limits
+        const int nB = (int) g.tB.size(), nD = (int) g.tD.size();
+        const int slice = 1 << 24;
+        for (int b = 0; b < nB && e == cudaSuccess; b += slice)
+            e = launch_gen(im->kernel_id, im->kd, fp32, tasks + b, std::min(slice, nB - b), pts, kp, B, im->stream);
+        for (int b = 0; b < nD && e == cudaSuccess; b += slice)
+            e = launch_gen(im->kernel_id, im->kd, fp32, tasks + nB + b, std::min(slice, nD - b), pts, kp, D, im->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(im->stream);
+        if (e != cudaSuccess) st = fail(H2GPU_ERR_CUDA, "stored-block generation failed: %s", cudaGetErrorString(e));
+    } while (0);
+    if (pts) cudaFree(pts);
+    if (tasks) cudaFree(tasks);
+    return st;
+}
+
 int prepare(h2gpu_image* im, int NV)
 {
     CK(cudaSetDevice(im->device));
+    if (im->f32_only && im->precision != H2GPU_PREC_MIXED)
+        return fail(H2GPU_ERR_STATE, "this image holds its stored blocks in FP32 only (generated for mixed "
+                                     "precision); create it in FP64 for FP64 applies");
     if (im->precision == H2GPU_PREC_MIXED)
     {
         TRY(make_f32(im, im->d_U64, &im->d_U32, im->U_elems));
@@ -1664,12 +1797,26 @@ H2G_API int h2gpu_image_create(const h2gpu_desc* desc, const h2gpu_options* opt,
 {
     if (!out) return fail(H2GPU_ERR_INVALID, "out is NULL");
     *out = nullptr;
-    TRY(validate(desc));
     h2gpu_options o;
     h2gpu_default_options(&o);
     if (opt) o = *opt;
     REQ(o.precision == H2GPU_PREC_FP64 || o.precision == H2GPU_PREC_MIXED, "unknown precision %d", o.precision);
+    REQ(o.blocks == H2GPU_BLOCKS_GIVEN || o.blocks == H2GPU_BLOCKS_GENERATE, "unknown blocks option %d", o.blocks);
+    const bool gen = o.blocks == H2GPU_BLOCKS_GENERATE;
+    // generated blocks: the representation is applied as a stored-block (AOT) one whose
+    // B / D arenas the device fills; the descriptor's own B_data / D_data are not read
+    h2gpu_desc dg;
+    if (gen && desc)
+    {
+        dg = *desc;
+        dg.BD_JIT = 0;
+        dg.B_data = nullptr;
+        dg.D_data = nullptr;
+        desc = &dg;
+    }
+    TRY(validate(desc, gen));
     h2gpu_image* im = new h2gpu_image();
+    im->gen = gen;
     {
         const char* e = getenv("H2G_JIT_TC");
         im->jit_tc = !(e && e[0] == '0');
@@ -1679,7 +1826,9 @@ H2G_API int h2gpu_image_create(const h2gpu_desc* desc, const h2gpu_options* opt,
         im->blk_tc = !(e && e[0] == '0');
     }
     HostPlan hp;
+    GenPlan gp;
     int pst = build_plan(im, desc, hp);   // all structural checks happen here, before any CUDA call
+    if (pst == H2GPU_OK && gen) pst = build_gen(desc, gp);
     if (pst == H2GPU_OK)
     {
         // the plan self-check of h2gpu_plan_check, on request (the test suite sets it)
@@ -1707,6 +1856,7 @@ H2G_API int h2gpu_image_create(const h2gpu_desc* desc, const h2gpu_options* opt,
             if (cudaEventCreate(&ev) != cudaSuccess) { st = fail(H2GPU_ERR_CUDA, "event creation failed"); break; }
         if (st != H2GPU_OK) break;
         st = upload_plan(im, desc, hp);
+        if (st == H2GPU_OK && gen) st = generate_blocks(im, gp);
         if (st == H2GPU_OK && (cudaMalloc(&im->d_status, sizeof(int)) != cudaSuccess ||
                                cudaMemset(im->d_status, 0, sizeof(int)) != cudaSuccess ||
                                cudaHostAlloc(&im->h_status, sizeof(int), cudaHostAllocDefault) != cudaSuccess))
@@ -1741,6 +1891,9 @@ H2G_API int h2gpu_set_precision(h2gpu_image* im, int precision)
     if (!im) return fail(H2GPU_ERR_INVALID, "image is NULL");
     REQ(precision == H2GPU_PREC_FP64 || precision == H2GPU_PREC_MIXED, "unknown precision %d", precision);
     std::lock_guard<std::mutex> lk(im->mu);
+    if (im->f32_only && precision != H2GPU_PREC_MIXED)
+        return fail(H2GPU_ERR_STATE, "this image holds its stored blocks in FP32 only (generated for mixed "
+                                     "precision); create it in FP64 for FP64 applies");
     im->precision = precision;
     return H2GPU_OK;
 }
@@ -1831,6 +1984,47 @@ H2G_API int h2gpu_permute_vector(h2gpu_image* im, int forward, const double* x, 
 {
     if (!im) return fail(H2GPU_ERR_INVALID, "image is NULL");
     return h2gpu_permute_matrix_rows(im, forward, H2GPU_COL_MAJOR, 1, x, im->N, px, im->N);
+}
+
+__global__ void k_f32_to_f64(const float* __restrict__ a, double* __restrict__ b, size_t n)
+{
+    for (size_t i = blockIdx.x * (size_t) blockDim.x + threadIdx.x; i < n; i += (size_t) gridDim.x * blockDim.x)
+        b[i] = (double) a[i];
+}
+
+H2G_API int h2gpu_get_blocks(h2gpu_image* im, int which, double* host, size_t n_elems)
+{
+    if (!im || !host) return fail(H2GPU_ERR_INVALID, "NULL argument");
+    REQ(which == 0 || which == 1, "which must be 0 (B) or 1 (D)");
+    std::lock_guard<std::mutex> lk(im->mu);
+    const size_t n = which == 0 ? im->B_elems : im->D_elems;
+    REQ(n_elems == n, "the image holds %zu elements of %s, not %zu", n, which == 0 ? "B" : "D", n_elems);
+    if (n == 0) return H2GPU_OK;
+    const double* d64 = which == 0 ? im->d_B64 : im->d_D64;
+    const float* d32 = which == 0 ? im->d_B32 : im->d_D32;
+    if (!d64 && !d32) return fail(H2GPU_ERR_STATE, "the image stores no blocks (JIT image)");
+    CK(cudaSetDevice(im->device));
+    if (d64)
+    {
+        CK(cudaMemcpy(host, d64, 8 * n, cudaMemcpyDeviceToHost));
+        return H2GPU_OK;
+    }
+    // widen on the device in slices of 64 M elements
+    const size_t slice = (size_t) 1 << 26;
+    double* tmp = nullptr;
+    CK(cudaMalloc(&tmp, 8 * std::min(n, slice)));
+    int st = H2GPU_OK;
+    for (size_t b = 0; b < n && st == H2GPU_OK; b += slice)
+    {
+        const size_t m = std::min(slice, n - b);
+        k_f32_to_f64<<<148 * 8, 256, 0, im->stream>>>(d32 + b, tmp, m);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpyAsync(host + b, tmp, 8 * m, cudaMemcpyDeviceToHost, im->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(im->stream);
+        if (e != cudaSuccess) st = fail(H2GPU_ERR_CUDA, "block copy failed: %s", cudaGetErrorString(e));
+    }
+    cudaFree(tmp);
+    return st;
 }
 
 H2G_API int h2gpu_get_stats(h2gpu_image* im, h2gpu_stats* st)
@@ -2160,6 +2354,8 @@ H2G_API int h2gpu_batch_create(const h2gpu_desc* descs, int n_desc, const h2gpu_
 {
     if (!out) return fail(H2GPU_ERR_INVALID, "out is NULL");
     *out = nullptr;
+    if (opt && opt->blocks != H2GPU_BLOCKS_GIVEN)
+        return fail(H2GPU_ERR_UNSUPPORTED, "batched images take their blocks as given");
     MergedDesc m;
     TRY(merge_descs(descs, n_desc, m));
     TRY(h2gpu_image_create(&m.d, opt, out));

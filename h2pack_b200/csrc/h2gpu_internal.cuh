@@ -113,6 +113,18 @@ struct PairPartner {
     float sx, sy, sz;    // center(a) - center(b)
 };
 
+// Generation of stored blocks on the device (H2P_build_B_AOT, src/H2Pack_build.c:789-889;
+// H2P_build_D_AOT, :1034-1140): rows [kd*r0, kd*(r0 + nr)) of one block,
+// A[kd i + a][kd j + b] = K_ab(row point i, column point j), packed row-major with
+// ld = kd * ncp at the block's offset in H2Pack's B / D packing.
+struct GenTask {
+    long long a_off;   // element offset of the task's first row in the block arena
+    int row_pt0;       // point-space index of the task's first row point
+    int nrp;           // row points in this task (<= 16)
+    int col_pt0;       // point-space index of the block's first column point
+    int ncp;           // column points of the block
+};
+
 // Final assembly of a leaf: Y[fwd[row0 + r]][v] = sum_s PS[slot_s + r][v]
 struct AsmTask {
     int row0, nrow;

@@ -2249,6 +2249,58 @@ __global__ void __launch_bounds__(128) k_direct(const double4* __restrict__ trg,
         for (int a = 0; a < KD; a++) out[(long long) i * KD + a] = acc[a];
 }
 
+// ------------------------------------------------- stored-block generation
+
+// One CTA per GenTask: up to 16 row points of one B / D block against all its column
+// points, in FP64 from the same formulas as the JIT and direct-sum kernels (the values
+// of H2Pack's krnl_eval on the same points, src/H2Pack_build.c:818-860, :1063-1110), then
+// stored in the arena's type.  Column points are staged in shared memory 256 at a time;
+// thread j owns column point j of the stage and writes its kd x kd entries of every row
+// point (consecutive threads write consecutive kd-wide runs of a row).
+constexpr int kGenThreads = 256;
+
+template <int KID, int KD, typename TO>
+__global__ void __launch_bounds__(kGenThreads) k_gen(const GenTask* __restrict__ tasks,
+                                                     const double4* __restrict__ pts, KParam kp,
+                                                     TO* __restrict__ arena)
+{
+    __shared__ double4 s_row[16];
+    const GenTask t = tasks[blockIdx.x];
+    const int tid = threadIdx.x;
+    const long long ld = (long long) KD * t.ncp;
+    if (tid < t.nrp) s_row[tid] = pts[t.row_pt0 + tid];
+    __syncthreads();
+    for (int j0 = 0; j0 < t.ncp; j0 += kGenThreads)
+    {
+        const int j = j0 + tid;
+        if (j >= t.ncp) break;
+        const double4 q = pts[t.col_pt0 + j];
+        TO* col = arena + t.a_off + (long long) KD * j;
+        for (int i = 0; i < t.nrp; i++)
+        {
+            const double4 p = s_row[i];
+            const double dx = p.x - q.x, dy = p.y - q.y, dz = p.z - q.z;
+            if constexpr (KD == 1)
+            {
+                const double r2 = dx * dx + dy * dy + dz * dz;
+                col[(long long) i * ld] = (TO) Scalar<KID, double>::f(r2, kp.p0, kp.c0);
+            } else {
+                double t1, t2, ux, uy, uz;
+                rpy_coef<double>(dx, dy, dz, p.w, q.w, kp.c0, t1, t2, ux, uy, uz);
+                const double u[3] = {ux, uy, uz};
+                TO* row = col + (long long) (3 * i) * ld;
+#pragma unroll
+                for (int a = 0; a < 3; a++)
+                {
+                    const double ta = t2 * u[a];
+#pragma unroll
+                    for (int b = 0; b < 3; b++) row[(long long) a * ld + b] = (TO) (ta * u[b] + (a == b ? t1 : 0.0));
+                }
+            }
+        }
+    }
+}
+
 // ------------------------------------------------------------- launchers
 
 static inline unsigned grid_for(long long n, int threads)
@@ -2545,6 +2597,30 @@ cudaError_t launch_direct(int kid, const double4* trg, int n_trg, const double4*
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
+}
+
+template <typename TO>
+static cudaError_t gen_typed(int kid, const GenTask* t, int n, const double4* pts, KParam kp, TO* arena,
+                             cudaStream_t st)
+{
+    if (n <= 0) return cudaSuccess;
+    switch (kid)
+    {
+        case KRNL_COULOMB_ID:  k_gen<KRNL_COULOMB_ID, 1, TO><<<n, kGenThreads, 0, st>>>(t, pts, kp, arena); break;
+        case KRNL_GAUSSIAN_ID: k_gen<KRNL_GAUSSIAN_ID, 1, TO><<<n, kGenThreads, 0, st>>>(t, pts, kp, arena); break;
+        case KRNL_MATERN32_ID: k_gen<KRNL_MATERN32_ID, 1, TO><<<n, kGenThreads, 0, st>>>(t, pts, kp, arena); break;
+        case KRNL_RPY_ID:      k_gen<KRNL_RPY_ID, 3, TO><<<n, kGenThreads, 0, st>>>(t, pts, kp, arena); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gen(int kid, int kd, int fp32, const GenTask* t, int n, const double4* pts, KParam kp, void* arena,
+                       cudaStream_t st)
+{
+    if ((kid == KRNL_RPY_ID) != (kd == 3)) return cudaErrorInvalidValue;
+    return fp32 ? gen_typed<float>(kid, t, n, pts, kp, (float*) arena, st)
+                : gen_typed<double>(kid, t, n, pts, kp, (double*) arena, st);
 }
 
 template cudaError_t launch_up<double>(int, const UpTask*, int, const double*, double*, cudaStream_t, int);

@@ -38,6 +38,9 @@ cudaError_t launch_panel_in(int NV, const PanelGroup* pg, int g0, int n, const d
 cudaError_t launch_pair(int kid, int NV, const PairOwner* ow, int n, const PairPartner* pp, const void* pts, KParam kp,
                         const double* XS, double* PS, cudaStream_t st,
                         int far = 0);
+// stored-block generation: tasks [0, n) into arena (double or float, per fp32)
+cudaError_t launch_gen(int kid, int kd, int fp32, const GenTask* t, int n, const double4* pts, KParam kp, void* arena,
+                       cudaStream_t st);
 cudaError_t launch_direct(int kid, const double4* trg, int n_trg, const double4* src, int n_src, const double* val,
                           KParam kp, double* out, cudaStream_t st);
 

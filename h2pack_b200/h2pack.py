@@ -50,9 +50,14 @@ def _prec(p) -> int:
 class Image:
     """Device image of one H2 representation (h2gpu_image_create)."""
 
-    def __init__(self, desc: _abi.Desc, precision="fp64", max_n_vec: int = 16, device: int = -1):
+    def __init__(self, desc: _abi.Desc, precision="fp64", max_n_vec: int = 16, device: int = -1,
+                 blocks: str = "given"):
+        """blocks: "given" (stored blocks uploaded from the descriptor, or evaluated on the
+        fly for a JIT descriptor) or "generate" (stored B / D blocks generated on the
+        device from the kernel and the points, as H2P_build_B_AOT / H2P_build_D_AOT do)."""
         self.lib = _abi.libh2gpu()
-        opt = _abi.Options(_prec(precision), int(max_n_vec), int(device))
+        opt = _abi.Options(_prec(precision), int(max_n_vec), int(device),
+                           {"given": _abi.BLOCKS_GIVEN, "generate": _abi.BLOCKS_GENERATE}[blocks])
         h = C.c_void_p()
         _abi.check(self.lib.h2gpu_image_create(C.byref(desc), C.byref(opt), C.byref(h)), self.lib, "h2gpu_image_create")
         self.handle = h
@@ -63,7 +68,7 @@ class Image:
         """One image for many representations (h2gpu_batch_create); vectors are stacked in order."""
         lib = _abi.libh2gpu()
         arr = (_abi.Desc * len(descs))(*descs)
-        opt = _abi.Options(_prec(precision), int(max_n_vec), int(device))
+        opt = _abi.Options(_prec(precision), int(max_n_vec), int(device), _abi.BLOCKS_GIVEN)
         h = C.c_void_p()
         _abi.check(lib.h2gpu_batch_create(arr, len(descs), C.byref(opt), C.byref(h)), lib, "h2gpu_batch_create")
         img = cls.__new__(cls)
@@ -152,6 +157,13 @@ class Image:
         _abi.check(self.lib.h2gpu_permute_vector(self.handle, 1 if forward else 0, _dptr(x), _dptr(y)),
                    self.lib, "h2gpu_permute_vector")
         return y
+
+    def blocks(self, which: str, n_elems: int) -> np.ndarray:
+        """The image's stored B or D blocks (which = "B" / "D") in H2Pack's packing, as FP64."""
+        out = np.empty(int(n_elems))
+        _abi.check(self.lib.h2gpu_get_blocks(self.handle, 0 if which == "B" else 1, _dptr(out), out.size),
+                   self.lib, "h2gpu_get_blocks")
+        return out
 
     def stats(self) -> dict:
         s = _abi.Stats()

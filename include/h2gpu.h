@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define H2GPU_ABI_VERSION 1
+#define H2GPU_ABI_VERSION 2
 
 /* Status codes */
 #define H2GPU_OK               0
@@ -128,12 +128,25 @@ typedef struct h2gpu_desc
     double krnl_param[4];
 } h2gpu_desc;
 
+/* Where the stored B / D blocks of an image come from (h2gpu_options.blocks) */
+#define H2GPU_BLOCKS_GIVEN    0   /* AOT descriptors: uploaded from B_data / D_data;
+                                     JIT descriptors: evaluated on the fly (default)  */
+#define H2GPU_BLOCKS_GENERATE 1   /* stored blocks generated on the device from the kernel,
+                                     the coordinates and the skeleton points, in H2Pack's
+                                     packing (B_ptr / D_ptr): what H2P_build_B_AOT and
+                                     H2P_build_D_AOT compute (src/H2Pack_build.c:789-889,
+                                     :1034-1140); B_data / D_data are not read, so a
+                                     descriptor of a handle built with BD_JIT = 1 works.
+                                     The arena is FP64 for an FP64 image and FP32 only
+                                     for a mixed one (such an image refuses FP64 applies). */
+
 /* Options of an image */
 typedef struct h2gpu_options
 {
     int precision;      /* H2GPU_PREC_FP64 or H2GPU_PREC_MIXED                        */
     int max_n_vec;      /* widest right-hand-side panel per pass (default 16)         */
     int device;         /* CUDA device ordinal (default: current device)              */
+    int blocks;         /* H2GPU_BLOCKS_GIVEN (default) or H2GPU_BLOCKS_GENERATE      */
 } h2gpu_options;
 
 typedef struct h2gpu_image h2gpu_image;
@@ -289,6 +302,15 @@ int h2gpu_cg_query(h2gpu_cg *cg);
 int h2gpu_cg_cancel(h2gpu_cg *cg, int slot);
 int h2gpu_cg_take(h2gpu_cg *cg, int slot, double *d_x);
 int h2gpu_cg_history(h2gpu_cg *cg, int slot, double *out, int max_n);      /* ||r|| per iteration; returns count */
+
+/*
+ * Copy the image's stored blocks (which = 0: B, 1: D) to host memory as doubles, in
+ * H2Pack's packing (element B_ptr[i] / D_ptr[i] starts block i); n_elems must be the
+ * total (B_ptr[n_B] / D_ptr[n_D]).  An image holding FP32 blocks only returns them
+ * widened.  For checking generated blocks against H2P_build_B_AOT / H2P_build_D_AOT;
+ * no counterpart in the reference.
+ */
+int h2gpu_get_blocks(h2gpu_image *img, int which, double *host, size_t n_elems);
 
 int h2gpu_get_stats(h2gpu_image *img, h2gpu_stats *st);
 int h2gpu_reset_stats(h2gpu_image *img);

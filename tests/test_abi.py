@@ -35,7 +35,7 @@ def test_dropin_exports_every_declared_symbol():
 
 
 def test_abi_version():
-    assert _abi.libh2gpu().h2gpu_abi_version() == 1
+    assert _abi.libh2gpu().h2gpu_abi_version() == 2
 
 
 def test_missing_library_fails_loudly(tmp_path, monkeypatch):
