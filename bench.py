@@ -63,7 +63,7 @@ def parse():
     p.add_argument("--precisions", default="fp64,mixed",
                    help="stored-block workloads: which paths to time (comma list)")
     p.add_argument("--n-matrices", type=int, default=512)
-    p.add_argument("--n-requests", type=int, default=96)
+    p.add_argument("--n-requests", type=int, default=1000)
     p.add_argument("--served-matrices", type=int, default=32)
     p.add_argument("--served-nmax", type=int, default=500_000)
     return p.parse_args()
@@ -565,6 +565,8 @@ def run_batched(args):
     build_s = time.time() - t0
     groups = {"coulomb": [H for i, H in enumerate(Hs) if i % 2 == 0],
               "gaussian": [H for i, H in enumerate(Hs) if i % 2 == 1]}
+    from h2pack_b200 import direct_sum
+    coords = [points(int(n), seed=100 + i) for i, n in enumerate(ns)]
     res = {}
     for prec in ("mixed", "fp64"):
         imgs, bufs = [], []
@@ -577,19 +579,52 @@ def run_batched(args):
             imgs.append((img, tuned))
             bufs.append((X, Y))
         ms = timed_loop(lambda: [img.graph_launch() for img, _ in imgs], args.steps, args.warmup)
+        # error against the FP64 direct sum: every 16th member of each kernel group,
+        # 1000 sampled rows, right-hand sides 0 and 7
+        errs = []
+        for gi, (kern, hs) in enumerate(groups.items()):
+            X, Y = bufs[gi]
+            Xc, Yc = X.cpu().numpy(), Y.cpu().numpy()
+            off = 0
+            for j, H in enumerate(hs):
+                idx = 2 * j + gi
+                if j % 16 == 0:
+                    rr = np.random.default_rng(idx).choice(H.N, min(1000, H.N), replace=False)
+                    for c in (0, 7):
+                        yd = direct_sum(kern, [] if kern == "coulomb" else [1.0], coords[idx], Xc[off:off + H.N, c],
+                                        coords[idx][:, rr])
+                        errs.append(rel2(Yc[off + rr, c], yd))
+                off += H.N
         # the same matrices one image each, eager (no batching, no graph)
         singles = [Image(H.describe(), precision=prec) for H in Hs]
         sx = [torch.rand(s.N, 8, dtype=torch.float64, device="cuda") - 0.5 for s in singles]
         ms1 = timed_loop(lambda: [s.matmul_device(x) for s, x in zip(singles, sx)], max(2, args.steps // 2), 1)
         res[prec] = {"ms": ms, "products_per_s": len(Hs) * 8 * 1e3 / ms, "unbatched_ms": ms1,
-                     "tuned": [t for _, t in imgs]}
+                     "tuned": [t for _, t in imgs], "max_rel_err_vs_direct": max(errs), "n_err_checks": len(errs)}
         for s in singles:
             s.close()
         for img, _ in imgs:
             img.close()
+    # CPU baseline: H2Pack's H2P_matmul (reference library, all host cores) looped over a
+    # uniform sample of the matrices (every 8th), 8 right-hand sides each
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+        lib, t_cpu, k = O.libref(), 0.0, 0
+        for i in range(0, len(Hs), 8):
+            H = Hs[i]
+            Xh = np.random.default_rng(i).random((H.N, 8)) - 0.5
+            Yh = np.zeros_like(Xh)
+            t = time.perf_counter()
+            lib.H2P_matmul(H.h2pack, 101, 8, O.dptr(Xh), 8, O.dptr(Yh), 8)
+            t_cpu += time.perf_counter() - t
+            k += 1
+        cpu = {"value": k * 8 / t_cpu, "unit": "products/s", "cores": Hs[0].info["n_thread"], "kind": "reference",
+               "sample": f"sequential H2P_matmul (8 RHS) of H2Pack compiled from its sources over {k} of the "
+                         f"{len(Hs)} matrices (every 8th), {t_cpu:.1f} s"}
     line = {"metric": "batched H2 matrix-RHS products/s", "value": res["mixed"]["products_per_s"], "unit": "products/s",
             "workload": "batched", "n_matrices": len(Hs), "n_total_points": int(ns.sum()), "nvec": 8,
-            "build_seconds": build_s, "mixed": res["mixed"], "fp64": res["fp64"],
+            "build_seconds": build_s, "mixed": res["mixed"], "fp64": res["fp64"], "cpu_baseline": cpu,
             "speedup_mixed_vs_fp64": res["fp64"]["ms"] / res["mixed"]["ms"],
             "speedup_batched_vs_unbatched_mixed": res["mixed"]["unbatched_ms"] / res["mixed"]["ms"]}
     print(json.dumps(line), flush=True)
@@ -609,13 +644,14 @@ def run_served(args):
     rng = np.random.default_rng(5)
     n_mat = args.served_matrices
     ns = log_uniform(rng, 10_000, args.served_nmax, n_mat)
-    Hs = {}
+    Hs, spec = {}, {}
     t0 = time.time()
     for i, n in enumerate(ns):
         kern = "gaussian" if i % 2 == 0 else "matern32"
         ell = float(rng.uniform(0.5, 2.0))
         param = [1.0 / ell ** 2] if kern == "gaussian" else [1.0 / ell]
-        Hs[f"m{i}"] = H2Matrix(kern, points(int(n), seed=200 + i), param, 1e-6, BD_JIT=1, proxy="surface",
+        spec[f"m{i}"] = (kern, param, points(int(n), seed=200 + i))
+        Hs[f"m{i}"] = H2Matrix(kern, spec[f"m{i}"][2], param, 1e-6, BD_JIT=1, proxy="surface",
                                n_thread=os.cpu_count())
     build_s = time.time() - t0
     g = torch.Generator(device="cuda").manual_seed(9)
@@ -626,7 +662,7 @@ def run_served(args):
         kind = "pcg" if rng.random() < 0.5 else "matvec"
         base.append(Request(rid=i, matrix=name, kind=kind, arrival=float(arr[i]),
                             b=torch.randn(Hs[name].N, dtype=torch.float64, device="cuda", generator=g)))
-    out = {}
+    out, done_by_prec = {}, {}
     for prec in [p for p in ("mixed", "fp64") if p in args.precisions.split(",")]:
         srv = Server(budget_bytes=150e9, max_slots=16)
         for name, H in Hs.items():
@@ -636,20 +672,89 @@ def run_served(args):
         for name in list(srv.blocks):
             srv.evict(name)
         st = latency_stats(done)
+        st.update(served_errors(done, spec, Hs))
         pcg = [r for r in done if r.kind == "pcg"]
         st.update({"pcg_iters_mean": float(np.mean([r.iters for r in pcg])) if pcg else 0,
                    "pcg_converged": int(sum(r.converged for r in pcg)), "n_pcg": len(pcg),
                    "max_relres": max((r.relres for r in pcg), default=None)})
         out[prec] = st
+        done_by_prec[prec] = done
     main = out["mixed"] if "mixed" in out else out["fp64"]
+    cpu = None
+    if not args.no_cpu_baseline:
+        cpu = served_cpu_baseline(Hs, done_by_prec.get("fp64") or done_by_prec.get("mixed"))
     line = {"metric": "served requests/s (matvec + PCG on K+mu I, Poisson 2000 req/s)",
             "value": main["throughput_req_s"], "unit": "req/s", "workload": "served",
             "n_matrices": n_mat, "sizes": [int(n) for n in ns], "n_requests": args.n_requests,
-            "build_seconds": build_s, "mixed": out.get("mixed"), "fp64": out.get("fp64"),
+            "build_seconds": build_s, "mixed": out.get("mixed"), "fp64": out.get("fp64"), "cpu_baseline": cpu,
             "speedup_mixed_vs_fp64": (out["fp64"]["mean_ms"] / out["mixed"]["mean_ms"]) if len(out) == 2 else None}
     print(json.dumps(line), flush=True)
     for H in Hs.values():
         H.close()
+
+
+def served_errors(done, spec, Hs, n_check=16, rows=500):
+    """Errors of served results against the FP64 direct sum on sampled rows: a matvec
+    result x against (K + mu I) b, and a PCG solution's residual b - (K + mu I) x, on 500
+    rows of each of n_check requests of each kind (relative to b on those rows)."""
+    from h2pack_b200 import direct_sum
+    mv = [r for r in done if r.kind == "matvec" and r.x is not None][:n_check]
+    pc = [r for r in done if r.kind == "pcg" and r.x is not None][:n_check]
+    e_mv, e_pcg = [], []
+    for group, out in ((mv, e_mv), (pc, e_pcg)):
+        for r in group:
+            kern, param, coord = spec[r.matrix]
+            rr = np.random.default_rng(r.rid).choice(coord.shape[1], min(rows, coord.shape[1]), replace=False)
+            b, x = r.b.cpu().numpy(), r.x.cpu().numpy()
+            if r.kind == "matvec":
+                yd = direct_sum(kern, param, coord, b, coord[:, rr]) + 1e-2 * b[rr]
+                out.append(rel2(x[rr], yd))
+            else:
+                ax = direct_sum(kern, param, coord, x, coord[:, rr]) + 1e-2 * x[rr]
+                out.append(float(np.linalg.norm(b[rr] - ax) / np.linalg.norm(b[rr])))
+    return {"matvec_max_rel_err_vs_direct": max(e_mv) if e_mv else None,
+            "pcg_max_rel_residual_vs_direct": max(e_pcg) if e_pcg else None,
+            "n_err_checks": len(e_mv) + len(e_pcg)}
+
+
+def served_cpu_baseline(Hs, done):
+    """The served stream on the host, as H2Pack's own drivers would run it: a sequential
+    loop of H2P_matvec + mu x (matvec requests) and pcg.c (examples/PCG/pcg.c:11-152) over
+    H2P_matvec (PCG requests), reference library, all host cores.  One H2P_matvec is timed
+    per matrix; the stream's cost is the sum over its requests of (iterations + 1) matvecs
+    of the request's matrix, with the iteration counts the GPU run took (the vector
+    operations of pcg.c are O(N) and not counted).  One real pcg run on the smallest
+    matrix checks that model."""
+    from oracle import oracle as O
+    lib = O.libref()
+    t_mv = {}
+    for name, H in Hs.items():
+        x = np.random.default_rng(1).standard_normal(H.N)
+        y = np.zeros(H.N)
+        lib.H2P_matvec(H.h2pack, O.dptr(x), O.dptr(y))          # warm-up
+        t = time.perf_counter()
+        lib.H2P_matvec(H.h2pack, O.dptr(x), O.dptr(y))
+        t_mv[name] = time.perf_counter() - t
+    ok = [r for r in done if r.status == "done"]
+    cost = sum(t_mv[r.matrix] * (1 + (r.iters if r.kind == "pcg" else 0)) for r in ok)
+    # model check: a real pcg.c run on the smallest matrix
+    small = min(Hs, key=lambda k: Hs[k].N)
+    Hm = Hs[small]
+
+    def cpu_apply(v):
+        y = np.zeros_like(v)
+        lib.H2P_matvec(Hm.h2pack, O.dptr(np.ascontiguousarray(v)), O.dptr(y))
+        return y + 1e-2 * v
+    b = np.random.default_rng(2).standard_normal(Hm.N)
+    t = time.perf_counter()
+    _, _, _, iters, _ = O.pcg(cpu_apply, b, 1e-6, 5000)
+    t_pcg = time.perf_counter() - t
+    return {"value": len(ok) / cost, "unit": "req/s", "cores": next(iter(Hs.values())).info["n_thread"],
+            "kind": "reference",
+            "sample": f"one H2P_matvec of H2Pack compiled from its sources timed per matrix ({len(t_mv)} matrices, "
+                      f"{sum(t_mv.values()):.1f} s), times (iterations + 1) of each of the {len(ok)} served requests; "
+                      f"model check: pcg.c on the N={Hm.N} matrix took {t_pcg:.2f} s for {iters} iterations, "
+                      f"model {t_mv[small] * (iters + 1):.2f} s"}
 
 
 def main():

@@ -1791,6 +1791,7 @@ H2G_API void h2gpu_default_options(h2gpu_options* opt)
     opt->precision = H2GPU_PREC_FP64;
     opt->max_n_vec = 16;
     opt->device = -1;
+    opt->blocks = H2GPU_BLOCKS_GIVEN;
 }
 
 H2G_API int h2gpu_image_create(const h2gpu_desc* desc, const h2gpu_options* opt, h2gpu_image** out)
