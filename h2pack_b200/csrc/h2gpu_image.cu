@@ -1500,6 +1500,8 @@ int ensure_work(h2gpu_image* im, int NV)
     if (im->NVb >= NV) return H2GPU_OK;
     for (double** p : {&im->d_XS, &im->d_PS, &im->d_Y1, &im->d_PUSH})
         if (*p) { cudaFree(*p); *p = nullptr; }
+    im->NVb = 0;          // no buffers until all four are allocated
+    im->work_bytes = 0;
     size_t xs = ((size_t) im->N + im->y0_rows) * NV, ps = (size_t) im->ps_rows * NV, y1 = (size_t) im->y0_rows * NV;
     CK(cudaMalloc(&im->d_XS, 8 * std::max<size_t>(xs, 1)));
     CK(cudaMalloc(&im->d_PS, 8 * std::max<size_t>(ps, 1)));
@@ -1513,8 +1515,18 @@ int ensure_work(h2gpu_image* im, int NV)
 int panel_width(int n_vec, int max_nv)
 {
     int w = 1;
-    while (w < n_vec && w < max_nv && w < 16) w <<= 1;
+    while (w < n_vec && w < max_nv) w <<= 1;
     return w;
+}
+
+// Widest panel of right-hand sides the image's kernels take: 64 for mixed stored-block
+// images (the wide tcgen05 block kernel: one read of every block per 64 right-hand
+// sides), 8 for RPY JIT images, 16 otherwise; never above the image's max_n_vec.
+int panel_cap(const h2gpu_image* im)
+{
+    if (im->BD_JIT && im->kd == 3) return std::min(im->max_nv, 8);
+    if (!im->BD_JIT && im->precision == H2GPU_PREC_MIXED) return std::min(im->max_nv, 64);
+    return std::min(im->max_nv, 16);
 }
 
 KParam kparam_of(const h2gpu_image* im)
@@ -1532,9 +1544,10 @@ KParam kparam_of(const h2gpu_image* im)
 
 // The tcgen05 stored-block kernel (mixed precision, normal mode) reports through the
 // status word.
-bool uses_status(const h2gpu_image* im)
+bool uses_status(const h2gpu_image* im, int NV)
 {
-    return im->d_status && im->h_status && im->blk_tc == 2 && !im->BD_JIT && im->precision == H2GPU_PREC_MIXED;
+    return im->d_status && im->h_status && (im->blk_tc == 2 || NV > 16) && !im->BD_JIT &&
+           im->precision == H2GPU_PREC_MIXED;
 }
 
 // FP32 sweeps on the tensor cores when the image's kernel variant is a tensor-core one.
@@ -1632,7 +1645,7 @@ int run_panel(h2gpu_image* im, int NV, int nv, const double* X, long long x_rs, 
     }
     if (timed) CK(cudaEventRecord(e[5], s));
     CK(launch_asm(NV, im->d_asm, im->n_asm, im->d_asm_slots, im->d_PS, im->d_fwd, Y, y_rs, y_cs, nv, s));
-    if (timed && uses_status(im))
+    if (timed && uses_status(im, NV))
         CK(cudaMemcpyAsync(im->h_status, im->d_status, sizeof(int), cudaMemcpyDeviceToHost, s));
     if (timed) CK(cudaEventRecord(e[6], s));
     im->st.n_launches += 4 + (long long) (im->up_beg.size() - 1) + (long long) (im->dn_beg.size() - 1)
@@ -1645,7 +1658,7 @@ int run_panel(h2gpu_image* im, int NV, int nv, const double* X, long long x_rs, 
 // synchronised apply reports it (and clears it) as H2GPU_ERR_DEVICE.
 int check_status(h2gpu_image* im)
 {
-    if (!uses_status(im)) return H2GPU_OK;
+    if (!im->d_status || !im->h_status) return H2GPU_OK;
     if (*(volatile int*) im->h_status != 0)
     {
         *im->h_status = 0;
@@ -1727,9 +1740,17 @@ int apply_device(h2gpu_image* im, int n_vec, const double* X, long long x_rs, lo
                  long long y_rs, long long y_cs, cudaStream_t s)
 {
     // JIT tensor kernels keep 3 x NV accumulators per target: panels of at most 8 there
-    int NV = panel_width(n_vec, (im->BD_JIT && im->kd == 3) ? std::min(im->max_nv, 8) : im->max_nv);
+    int NV = panel_width(n_vec, panel_cap(im));
     if (im->tuned_nv > 0) NV = std::min(NV, im->tuned_nv);
-    TRY(prepare(im, NV));
+    int pst = prepare(im, NV);
+    if (pst == H2GPU_ERR_NOMEM && NV > 16)
+    {
+        // the work space of a wide panel does not fit: panels of 16
+        cudaGetLastError();
+        NV = 16;
+        pst = prepare(im, NV);
+    }
+    TRY(pst);
     float ph[5] = {0, 0, 0, 0, 0};
     for (int c0 = 0; c0 < n_vec; c0 += NV)
     {
@@ -1756,7 +1777,7 @@ int apply_quiet(h2gpu_image* im, int precision, int n_vec, const double* X, int 
 {
     const int saved = im->precision;
     im->precision = precision;
-    int NV = panel_width(n_vec, (im->BD_JIT && im->kd == 3) ? std::min(im->max_nv, 8) : im->max_nv);
+    int NV = panel_width(n_vec, panel_cap(im));
     if (im->tuned_nv > 0) NV = std::min(NV, im->tuned_nv);
     int st = prepare(im, NV);
     for (int c0 = 0; st == H2GPU_OK && c0 < n_vec; c0 += NV)
@@ -1789,7 +1810,7 @@ H2G_API void h2gpu_default_options(h2gpu_options* opt)
 {
     if (!opt) return;
     opt->precision = H2GPU_PREC_FP64;
-    opt->max_n_vec = 16;
+    opt->max_n_vec = 64;
     opt->device = -1;
     opt->blocks = H2GPU_BLOCKS_GIVEN;
 }
@@ -1846,7 +1867,7 @@ H2G_API int h2gpu_image_create(const h2gpu_desc* desc, const h2gpu_options* opt,
                     cudaGetErrorString(e));
     }
     im->precision = o.precision;
-    im->max_nv = (o.max_n_vec >= 1 && o.max_n_vec <= 16) ? o.max_n_vec : 16;
+    im->max_nv = (o.max_n_vec >= 1 && o.max_n_vec <= 64) ? o.max_n_vec : 64;
     if (o.device >= 0) im->device = o.device;
     else cudaGetDevice(&im->device);
     int st = H2GPU_OK;
@@ -2371,7 +2392,7 @@ H2G_API int h2gpu_graph_capture(h2gpu_image* im, int n_vec, const double* dX, in
     if (!im) return fail(H2GPU_ERR_INVALID, "image is NULL");
     REQ(n_vec >= 1 && ldx >= n_vec && ldy >= n_vec && dX && dY, "bad graph_capture arguments");
     std::lock_guard<std::mutex> lk(im->mu);
-    int NV = panel_width(n_vec, (im->BD_JIT && im->kd == 3) ? std::min(im->max_nv, 8) : im->max_nv);
+    int NV = panel_width(n_vec, panel_cap(im));
     if (im->tuned_nv > 0) NV = std::min(NV, im->tuned_nv);
     TRY(prepare(im, NV));
     if (im->graph_exec) { cudaGraphExecDestroy(im->graph_exec); im->graph_exec = nullptr; }
@@ -2438,7 +2459,7 @@ H2G_API int h2gpu_autotune(h2gpu_image* im, int n_vec, const double* dX, int ldx
     if (!im) return fail(H2GPU_ERR_INVALID, "image is NULL");
     REQ(n_vec >= 1 && ldx >= n_vec && ldy >= n_vec && dX && dY, "bad autotune arguments");
     std::lock_guard<std::mutex> lk(im->mu);
-    const int full = panel_width(n_vec, (im->BD_JIT && im->kd == 3) ? std::min(im->max_nv, 8) : im->max_nv);
+    const int full = panel_width(n_vec, panel_cap(im));
     std::vector<int> nvs;
     for (int w = 1; w <= full; w <<= 1)
         if (w == full || w >= 4) nvs.push_back(w);
@@ -2459,7 +2480,9 @@ H2G_API int h2gpu_autotune(h2gpu_image* im, int n_vec, const double* dX, int ldx
     for (int nv : nvs)
         for (int var : vars)
         {
-            if ((var == H2GPU_JIT_PAIR || var == H2GPU_BLK_TCGEN05) && nv != 8 && nv != 16) continue;
+            // wide panels (32 / 64) have one kernel whatever the variant: time them once
+            if (nv >= 32 && var != vars[0]) continue;
+            if (nv < 32 && (var == H2GPU_JIT_PAIR || var == H2GPU_BLK_TCGEN05) && nv != 8 && nv != 16) continue;
             // the tensor-core kernels exist for panels of 8 and 16; narrower panels run
             // the CUDA-core kernel whatever the variant, so time that once
             if (var == H2GPU_JIT_TC && nv != 8 && nv != 16 && vars.size() > 1) continue;

@@ -2062,6 +2062,244 @@ __global__ void __launch_bounds__(kBf3Threads, 5) k_blk_bf3(const BlkTask* __res
 template <int NV>
 constexpr int bf3_smem_bytes() { return (int) sizeof(Bf3Smem) + 1024; }
 
+// --------------------------- stored blocks on tcgen05, wide panels (32 / 64 right-hand sides)
+
+// The k_blk_bf3 scheme for panels of NV = 32 or 64 right-hand sides, so that a matmul of
+// up to 64 right-hand sides streams every stored block once (H2P_matmul applies each
+// block to up to mm_max_n_vec right-hand sides per read, src/H2Pack_matmul.c:497).
+// Per 64 x 64 tile of A (FP32, read from HBM once, split into BF16 pieces h + m + l):
+//   C0 (64 rows x NV) += A_tile V_tile   (MMA M = 64, N = NV, A K-major)  TMEM columns [0, NV)
+//   C1 (64 cols x NV)  = A_tile^T W      (MMA M = 64, N = NV, A MN-major) TMEM columns [NV, 2 NV)
+// six products per 16-deep K step (l.h + h.l + m.m + m.h + h.m + h.h), FP32 in TMEM over
+// one tile (64 terms), FP64 across tiles (C0 in shared memory per 64-row chunk, C1 added
+// into the task's slot).  V^T / W^T are NV rows of 64 BF16 (128 B, 128-byte swizzle),
+// B operands K-major, as k_blk_bf3.  The accumulators are read back 32 columns at a time.
+// 105 KB of shared memory: two CTAs per SM, whose tile loads and MMAs interleave.
+template <int NV>
+struct Bf3wSmem {
+    uint16_t a[3][64 * 64];    // A tile pieces h, m, l: 64 rows of 128 B, 128-byte swizzle
+    uint16_t v[3][NV * 64];    // V^T pieces (NV rows of the tile's 64 columns)
+    uint16_t w[3][NV * 64];    // W^T pieces (NV rows of the chunk's 64 rows)
+    double c0acc[64][NV + 1];  // the chunk's C0 rows in FP64 (row 16 warp + lane; padded)
+    unsigned long long mbar;
+    uint32_t tmem;
+};
+
+template <int NV>
+constexpr int bf3w_smem_bytes() { return (int) sizeof(Bf3wSmem<NV>) + 1024; }
+
+template <int NV>
+__global__ void __launch_bounds__(kBf3Threads, 2) k_blk_bf3w(const BlkTask* __restrict__ tasks,
+                                                             const float* __restrict__ arena,
+                                                             const double* __restrict__ XS, double* __restrict__ PS,
+                                                             int* __restrict__ status)
+{
+    static_assert(NV == 32 || NV == 64, "wide panels of 32 or 64 right-hand sides");
+    constexpr uint32_t IDESC0 = umma_idesc_bf16(NV, 0), IDESC1 = umma_idesc_bf16(NV, 1);
+    constexpr uint32_t TCOLS = 2 * NV;            // C0 and C1 (a power of two >= 32)
+    constexpr int VG = NV / 16;                   // granules of V^T / W^T per thread
+    constexpr int PIECE_VW = NV * 64 * 2;         // bytes of one piece of V^T / W^T
+    extern __shared__ __align__(1024) unsigned char bf3w_raw[];
+    Bf3wSmem<NV>& sm = *reinterpret_cast<Bf3wSmem<NV>*>(bf3w_raw + ((1024 - (smem_u32(bf3w_raw) & 1023)) & 1023));
+    const BlkTask T = tasks[blockIdx.x];
+    const int ncol = T.ncol, nrow = T.nrow;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const bool do0 = T.out0_row >= 0, do1 = T.out1_row >= 0;
+    const int ntc = (ncol + 63) / 64, nt = ntc * ((nrow + 63) / 64);
+    const float* A0 = arena + T.a_off;
+
+    if (warp == 0)
+    {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(smem_u32(&sm.tmem)), "n"(TCOLS) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0)
+    {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&sm.mbar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = sm.tmem, mbar = smem_u32(&sm.mbar);
+    unsigned char* const a_b = reinterpret_cast<unsigned char*>(sm.a);
+    unsigned char* const v_b = reinterpret_cast<unsigned char*>(sm.v);
+    unsigned char* const w_b = reinterpret_cast<unsigned char*>(sm.w);
+    const uint32_t a_s = smem_u32(sm.a), v_s = smem_u32(sm.v), w_s = smem_u32(sm.w);
+
+    // registers of the tile being loaded: thread t holds 4 granules (8 columns each) of A
+    // and VG granules of V^T and of W^T (row n, 8 consecutive k each)
+    float ra[4][8];
+    float rv[VG][8], rw[VG][8];
+    auto load_tile = [&](int t) {
+        const int rc = (t / ntc) * 64, c0 = (t % ntc) * 64, R = min(64, nrow - rc);
+        const float* A = A0 + (long long) rc * ncol + c0;
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+        {
+            const int gi = tid + kBf3Threads * u, r = gi >> 3, q = gi & 7;
+#pragma unroll
+            for (int j = 0; j < 8; j++)
+            {
+                const int c = 8 * q + j;
+                ra[u][j] = (r < R && c0 + c < ncol) ? A[(long long) r * ncol + c] : 0.f;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < VG; u++)
+        {
+            const int gi = tid + kBf3Threads * u, n = gi >> 3, q = gi & 7;
+#pragma unroll
+            for (int j = 0; j < 8; j++)
+            {
+                const int k = 8 * q + j;
+                rv[u][j] = (do0 && c0 + k < ncol) ? (float) XS[(long long) (T.in0_row + c0 + k) * NV + n] : 0.f;
+                rw[u][j] = (do1 && c0 == 0 && k < R) ? (float) XS[(long long) (T.in1_row + rc + k) * NV + n] : 0.f;
+            }
+        }
+    };
+    auto put = [&](unsigned char* base, int stride, int off, const float (&x)[8]) {
+        uint16_t h[8], m[8], l[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) bf16x3(x[j], h[j], m[j], l[j]);
+        auto pack = [](const uint16_t (&e)[8]) {
+            return make_uint4(e[0] | ((uint32_t) e[1] << 16), e[2] | ((uint32_t) e[3] << 16),
+                              e[4] | ((uint32_t) e[5] << 16), e[6] | ((uint32_t) e[7] << 16));
+        };
+        *reinterpret_cast<uint4*>(base + off) = pack(h);
+        *reinterpret_cast<uint4*>(base + stride + off) = pack(m);
+        *reinterpret_cast<uint4*>(base + 2 * stride + off) = pack(l);
+    };
+    auto store_tile = [&](int t) {
+        const int c0 = (t % ntc) * 64;
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+        {
+            const int gi = tid + kBf3Threads * u, r = gi >> 3, q = gi & 7;
+            put(a_b, 64 * 64 * 2, sw128(r, q), ra[u]);
+        }
+#pragma unroll
+        for (int u = 0; u < VG; u++)
+        {
+            const int gi = tid + kBf3Threads * u, n = gi >> 3, q = gi & 7;
+            put(v_b, PIECE_VW, sw128(n, q), rv[u]);
+            if (c0 == 0) put(w_b, PIECE_VW, sw128(n, q), rw[u]);
+        }
+    };
+
+    bool ok = true;
+    uint32_t phase = 0;
+    // lanes 0-15: the chunk's C0 row 16 warp + lane, summed in shared memory
+    double* const c0acc = sm.c0acc[(16 * warp + lane) & 63];
+    if (lane < 16)
+        for (int n = 0; n < NV; n++) c0acc[n] = 0.0;
+    // read back the tile just multiplied: C1 into its slot, C0 into the chunk's FP64 sums
+    auto drain = [&](int t) {
+        int good = 1;
+        if (tid == 0)
+        {
+            int it = 0;
+            while (!mbar_try_wait(mbar, phase))
+                if (++it > (1 << 22)) { good = 0; break; }
+            if (!good) atomicExch(status, 1);
+        }
+        phase ^= 1;
+        ok = __syncthreads_and(good) != 0;
+        if (!ok) return;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const int rc = (t / ntc) * 64, c0 = (t % ntc) * 64, R = min(64, nrow - rc);
+        const int m = 16 * warp + lane;
+        const bool last_tc = c0 + 64 >= ncol;
+#pragma unroll
+        for (int h = 0; h < 2 * NV / 32; h++)        // 32 accumulator columns at a time
+        {
+            uint32_t d[32];
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                         "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                         : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7]),
+                           "=r"(d[8]), "=r"(d[9]), "=r"(d[10]), "=r"(d[11]), "=r"(d[12]), "=r"(d[13]), "=r"(d[14]), "=r"(d[15]),
+                           "=r"(d[16]), "=r"(d[17]), "=r"(d[18]), "=r"(d[19]), "=r"(d[20]), "=r"(d[21]), "=r"(d[22]), "=r"(d[23]),
+                           "=r"(d[24]), "=r"(d[25]), "=r"(d[26]), "=r"(d[27]), "=r"(d[28]), "=r"(d[29]), "=r"(d[30]), "=r"(d[31])
+                         : "r"(tmem + ((uint32_t) (32 * warp) << 16) + (uint32_t) (32 * h)));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (lane >= 16) continue;
+            const bool is_c1 = 32 * h >= NV;
+            const int n0 = is_c1 ? 32 * h - NV : 32 * h;
+            if (is_c1)
+            {
+                if (do1 && c0 + m < ncol)
+                {
+                    double* o = PS + (long long) (T.out1_row + c0 + m) * NV + n0;
+#pragma unroll
+                    for (int n = 0; n < 32; n++)
+                    {
+                        const double v = (double) __uint_as_float(d[n]);
+                        o[n] = (rc == 0) ? v : o[n] + v;
+                    }
+                }
+            } else if (do0) {
+#pragma unroll
+                for (int n = 0; n < 32; n++) c0acc[n0 + n] += (double) __uint_as_float(d[n]);
+                if (last_tc)
+                {
+                    if (m < R)
+                    {
+                        double* o = PS + (long long) (T.out0_row + rc + m) * NV + n0;
+#pragma unroll
+                        for (int n = 0; n < 32; n++) o[n] = c0acc[n0 + n];
+                    }
+#pragma unroll
+                    for (int n = 0; n < 32; n++) c0acc[n0 + n] = 0.0;
+                }
+            }
+        }
+    };
+
+    // the six products of one K-step: (A piece, B piece), smallest first
+    constexpr int PA[6] = {2, 0, 1, 1, 0, 0}, PB[6] = {0, 2, 1, 0, 1, 0};
+    if (nt > 0) load_tile(0);
+    for (int t = 0; t < nt; t++)
+    {
+        if (t > 0) drain(t - 1);
+        if (!ok) break;
+        store_tile(t);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        if (tid == 0)
+        {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+            for (int ks = 0; ks < 4; ks++)          // K-steps of 16
+#pragma unroll
+                for (int p = 0; p < 6; p++)
+                {
+                    // C0: A K-major (32-byte step along the row), B = V^T K-major
+                    if (do0)
+                        umma_f16(tmem, umma_desc(a_s + PA[p] * 8192 + ks * 32, 16, 1024, 2),
+                                 umma_desc(v_s + PB[p] * PIECE_VW + ks * 32, 16, 1024, 2), IDESC0,
+                                 (ks == 0 && p == 0) ? 0u : 1u);
+                    // C1: A MN-major (16 rows = two 8-row swizzle atoms per step), B = W^T K-major
+                    if (do1)
+                        umma_f16(tmem + (uint32_t) NV, umma_desc(a_s + PA[p] * 8192 + ks * 2048, 8192, 1024, 2),
+                                 umma_desc(w_s + PB[p] * PIECE_VW + ks * 32, 16, 1024, 2), IDESC1,
+                                 (ks == 0 && p == 0) ? 0u : 1u);
+                }
+            umma_commit(mbar);
+        }
+        if (t + 1 < nt) load_tile(t + 1);
+    }
+    if (ok && nt > 0) drain(nt - 1);
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+    {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "n"(TCOLS) : "memory");
+    }
+}
+
 
 // ---------------------------------------------- sweeps on the tensor cores (FP32 U)
 
@@ -2320,10 +2558,23 @@ static inline unsigned grid_for(long long n, int threads)
         default: return cudaErrorInvalidValue;                \
     }
 
+// The same with the wide panels of the mixed stored-block path (gather, sweeps, sums).
+#define NV_DISPATCH_WIDE(nv, ...)                             \
+    switch (nv) {                                             \
+        case 1:  { constexpr int NVc = 1;  __VA_ARGS__; } break; \
+        case 2:  { constexpr int NVc = 2;  __VA_ARGS__; } break; \
+        case 4:  { constexpr int NVc = 4;  __VA_ARGS__; } break; \
+        case 8:  { constexpr int NVc = 8;  __VA_ARGS__; } break; \
+        case 16: { constexpr int NVc = 16; __VA_ARGS__; } break; \
+        case 32: { constexpr int NVc = 32; __VA_ARGS__; } break; \
+        case 64: { constexpr int NVc = 64; __VA_ARGS__; } break; \
+        default: return cudaErrorInvalidValue;                \
+    }
+
 cudaError_t launch_gather(int NV, const double* X, long long x_rs, long long x_cs, int nv, const int* fwd, int N,
                           double* XS, cudaStream_t st)
 {
-    NV_DISPATCH(NV, k_gather<NVc><<<grid_for((long long) N * NVc, 256), 256, 0, st>>>(X, x_rs, x_cs, nv, fwd, N, XS));
+    NV_DISPATCH_WIDE(NV, k_gather<NVc><<<grid_for((long long) N * NVc, 256), 256, 0, st>>>(X, x_rs, x_cs, nv, fwd, N, XS));
     return cudaGetLastError();
 }
 
@@ -2347,7 +2598,7 @@ cudaError_t launch_up(int NV, const UpTask* t, int n, const TA* U, double* XS, c
             return cudaGetLastError();
         }
     }
-    NV_DISPATCH(NV, {
+    NV_DISPATCH_WIDE(NV, {
         if constexpr (NVc >= 4)
             k_sweep_gemm<TA, NVc, true><<<n, 256, 0, st>>>(t, nullptr, U, XS, nullptr, nullptr, nullptr);
         else
@@ -2369,6 +2620,24 @@ cudaError_t launch_blk(int NV, const BlkTask* t, int n, const TA* arena, const d
 {
     if constexpr (sizeof(TA) == 4)
     {
+        if (n > 0 && (NV == 32 || NV == 64))
+        {
+            // wide panels: tcgen05 kernel only (BF16x3 pieces, TMEM accumulators)
+            if (!status) return cudaErrorInvalidValue;
+            if (NV == 64)
+            {
+                constexpr int b = bf3w_smem_bytes<64>();
+                cudaError_t e = allow_smem(k_blk_bf3w<64>, b);
+                if (e != cudaSuccess) return e;
+                k_blk_bf3w<64><<<n, kBf3Threads, b, st>>>(t, arena, XS, PS, status);
+            } else {
+                constexpr int b = bf3w_smem_bytes<32>();
+                cudaError_t e = allow_smem(k_blk_bf3w<32>, b);
+                if (e != cudaSuccess) return e;
+                k_blk_bf3w<32><<<n, kBf3Threads, b, st>>>(t, arena, XS, PS, status);
+            }
+            return cudaGetLastError();
+        }
         if (use_tc && n > 0 && (NV == 8 || NV == 16))
         {
             if (use_tc == 2 && status)
@@ -2429,7 +2698,7 @@ cudaError_t launch_down(int NV, const DownTask* t, int n, const TA* U, const dou
             return cudaGetLastError();
         }
     }
-    NV_DISPATCH(NV, {
+    NV_DISPATCH_WIDE(NV, {
         if constexpr (NVc >= 4)
         {
             k_sweep_gemm<TA, NVc, false><<<n, 256, 0, st>>>(nullptr, t, U, nullptr, Y1, PS, PUSH);
@@ -2443,7 +2712,7 @@ cudaError_t launch_down(int NV, const DownTask* t, int n, const TA* U, const dou
 cudaError_t launch_y1sum(int NV, const Y1Task* t, int n, const int* slots, const double* PS, double* Y1, cudaStream_t st)
 {
     if (n <= 0) return cudaSuccess;
-    NV_DISPATCH(NV, k_y1sum<NVc><<<n, 256, 0, st>>>(t, slots, PS, Y1));
+    NV_DISPATCH_WIDE(NV, k_y1sum<NVc><<<n, 256, 0, st>>>(t, slots, PS, Y1));
     return cudaGetLastError();
 }
 
@@ -2451,7 +2720,7 @@ cudaError_t launch_asm(int NV, const AsmTask* t, int n, const int* slots, const 
                        double* Y, long long y_rs, long long y_cs, int nv, cudaStream_t st)
 {
     if (n <= 0) return cudaSuccess;
-    NV_DISPATCH(NV, k_asm<NVc><<<n, 256, 0, st>>>(t, slots, PS, fwd, Y, y_rs, y_cs, nv));
+    NV_DISPATCH_WIDE(NV, k_asm<NVc><<<n, 256, 0, st>>>(t, slots, PS, fwd, Y, y_rs, y_cs, nv));
     return cudaGetLastError();
 }
 

@@ -50,7 +50,7 @@ def _prec(p) -> int:
 class Image:
     """Device image of one H2 representation (h2gpu_image_create)."""
 
-    def __init__(self, desc: _abi.Desc, precision="fp64", max_n_vec: int = 16, device: int = -1,
+    def __init__(self, desc: _abi.Desc, precision="fp64", max_n_vec: int = 64, device: int = -1,
                  blocks: str = "given"):
         """blocks: "given" (stored blocks uploaded from the descriptor, or evaluated on the
         fly for a JIT descriptor) or "generate" (stored B / D blocks generated on the
@@ -64,7 +64,7 @@ class Image:
         self.N = int(desc.krnl_dim) * int(desc.n_point)
 
     @classmethod
-    def batch(cls, descs, precision="fp64", max_n_vec: int = 16, device: int = -1) -> "Image":
+    def batch(cls, descs, precision="fp64", max_n_vec: int = 64, device: int = -1) -> "Image":
         """One image for many representations (h2gpu_batch_create); vectors are stacked in order."""
         lib = _abi.libh2gpu()
         arr = (_abi.Desc * len(descs))(*descs)

@@ -144,7 +144,8 @@ typedef struct h2gpu_desc
 typedef struct h2gpu_options
 {
     int precision;      /* H2GPU_PREC_FP64 or H2GPU_PREC_MIXED                        */
-    int max_n_vec;      /* widest right-hand-side panel per pass (default 16)         */
+    int max_n_vec;      /* widest right-hand-side panel per pass, <= 64 (default 64;
+                           mixed stored-block images take 32 / 64, others up to 16)   */
     int device;         /* CUDA device ordinal (default: current device)              */
     int blocks;         /* H2GPU_BLOCKS_GIVEN (default) or H2GPU_BLOCKS_GENERATE      */
 } h2gpu_options;
