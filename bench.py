@@ -58,6 +58,9 @@ def parse():
                    help="jit_matern: the headline configuration; the others print extra lines for the "
                         "other configurations (AOT Coulomb matvec, AOT RPY matmul, batched matrices, "
                         "served requests)")
+    p.add_argument("--blocks", default="generate", choices=["generate", "given"],
+                   help="aot_rpy: stored blocks generated on the GPU from a JIT-mode construction, or built "
+                        "on the host and uploaded")
     p.add_argument("--variant", default="auto", choices=["auto", "simt", "tc", "tcgen05"],
                    help="stored-block workloads: FP32 block-product kernel (auto = autotuned)")
     p.add_argument("--precisions", default="fp64,mixed",
@@ -451,53 +454,81 @@ def run_aot_coulomb(args):
 
 def run_aot_rpy(args):
     """RPY 3x3 tensor kernel (a = 1, eta = 1/(6 pi), so C = 1), particles uniform in a cube
-    sized for volume fraction 0.1, reltol 1e-8, stored U/B/D, 64 RHS forces N(0,1); matmul in
-    panels of 16.  The N = 500,000 case needs about 200 GB of FP64 B blocks at this tolerance
-    (25.4 GB measured at N = 50,000 with 512 leaves; 4096 leaves at 500,000), more than one
-    GPU holds, so the default N is the largest tested size whose FP64 image and FP32 copy fit.
-    value = right-hand-side matvecs/s of the mixed (FP32 stored blocks) matmul."""
+    sized for volume fraction 0.1, reltol 1e-8, stored U/B/D (normal mode), 64 RHS forces
+    N(0,1).  With --blocks generate (default) H2Pack's construction runs in JIT mode on the
+    host (U, skeletons, pair lists and block metadata) and the stored B / D blocks are
+    generated on the GPU (H2P_build_B_AOT / H2P_build_D_AOT on the device); with --blocks
+    given the host builds them and they are uploaded.  The stored representation at
+    N = 500,000 holds 55.7 G B entries, 6.8 G D entries and 2.0 G U entries (measured from
+    the construction), about 258 GB in FP32, more than one GPU's memory, so the default N
+    is 200,000 (B 19.0 G, D 1.1 G, U 0.77 G entries: 84 GB in FP32).  The mixed path
+    applies the 64 right-hand sides in one panel (every block read once, tcgen05).
+    value = right-hand-side matvecs/s of the mixed matmul."""
     import torch
-    from h2pack_b200 import H2Matrix, direct_sum
-    n = 100_000 if args.n == 1_000_000 else args.n
+    from h2pack_b200 import H2Matrix, Image, direct_sum
+    gen = args.blocks == "generate"
+    n = (200_000 if gen else 100_000) if args.n == 1_000_000 else args.n
     nv = 64
     rng = np.random.default_rng(31)
     L = (n * 4.0 * np.pi / 3.0 / 0.1) ** (1.0 / 3.0)
     coord = np.vstack([rng.random((3, n)) * L, np.ones((1, n))])
     eta = 1.0 / (6.0 * np.pi)
     t0 = time.time()
-    H = H2Matrix("rpy", coord, [eta], 1e-8, BD_JIT=0, max_leaf_points=300, max_leaf_size=4.0, proxy="surface",
-                 n_thread=os.cpu_count())
+    H = H2Matrix("rpy", coord, [eta], 1e-8, BD_JIT=1 if gen else 0, max_leaf_points=300, max_leaf_size=4.0,
+                 proxy="surface", n_thread=os.cpu_count())
     build_s = time.time() - t0
-    img = H.image()
+    ms_ = H.counters()["mat_size"]
+    entries = {"U": ms_[0], "B": ms_[1], "D": ms_[2]}
     g = torch.Generator(device="cuda").manual_seed(5)
     X = torch.randn(H.N, nv, dtype=torch.float64, device="cuda", generator=g)
     Y = torch.empty_like(X)
     out, Ys = {}, {}
     precs = args.precisions.split(",")
-    tuned = None
+    tuned, gen_s = None, {}
+    free_bytes = torch.cuda.mem_get_info()[0]
     for prec in precs:
-        H.set_precision(prec)
+        es = 8 if prec == "fp64" else 4
+        need = es * (entries["U"] + entries["B"] + entries["D"])
+        if gen and need > 0.92 * free_bytes:
+            out[prec] = {"skipped": f"{prec} stored blocks need {need / 1e9:.0f} GB, {free_bytes / 1e9:.0f} GB free"}
+            continue
+        if gen:
+            torch.cuda.synchronize()
+            t = time.time()
+            img = Image(H.describe(), prec, blocks="generate")
+            gen_s[prec] = time.time() - t
+        else:
+            img = H.image()
+            H.set_precision(prec)
         if prec == "mixed":
             if args.variant == "auto":
                 tuned = img.autotune(X, Y)
             else:
                 img.set_jit_variant(args.variant)
-                tuned = (16, args.variant)
+                tuned = (None, args.variant)
         for _ in range(args.warmup):
             img.matmul_device(X, Y)
         s0 = img.stats()   # phase times of the timed steps only
-        ms = timed_loop(lambda: img.matmul_device(X, Y), args.steps, 0)
+        with ClockSampler(0) as clk:
+            ms = timed_loop(lambda: img.matmul_device(X, Y), args.steps, 0)
         s1 = img.stats()
         ph = [(b - a) / args.steps for a, b in zip(s0["ms_phase"], s1["ms_phase"])]
+        launches = (s1["n_launches"] - s0["n_launches"]) / args.steps
         st = img.stats()
         # bytes of the current precision's copies; U counted twice (upward and downward sweep)
         stored = st["bytes_U"] + st["bytes_B"] + st["bytes_D"]
-        panels = (nv + 15) // 16
-        entries = (st["bytes_U"] / 2 + st["bytes_B"] + st["bytes_D"]) / (8.0 if prec == "fp64" else 4.0)
+        panel = tuned[0] if (prec == "mixed" and tuned and tuned[0]) else 16
+        panels = (nv + panel - 1) // panel
+        ent = (st["bytes_U"] / 2 + st["bytes_B"] + st["bytes_D"]) / (8.0 if prec == "fp64" else 4.0)
         out[prec] = {"ms": ms, "matvecs_per_s": nv * 1e3 / ms, "phase_ms": ph, "stored_bytes": stored,
+                     "panel": panel, "algorithmic_GBps": stored / (ms * 1e-3) / 1e9,
                      "streamed_GBps": panels * stored / (ms * 1e-3) / 1e9,
-                     "model_TFs": 2.0 * nv * 2 * entries / (ms * 1e-3) / 1e12}
+                     "BD_phase_GBps": (st["bytes_B"] + st["bytes_D"]) / ((ph[1] + ph[3]) * 1e-3) / 1e9,
+                     "model_TFs": 2.0 * nv * 2 * ent / (ms * 1e-3) / 1e12, "launches_per_step": launches,
+                     "clocks": clk.summary(), "generate_seconds": gen_s.get(prec)}
         Ys[prec] = Y.clone()
+        if gen:
+            img.close()
     # error of both paths against the FP64 direct sum on sampled points (3 rows each)
     m = min(args.check_rows // 3 if args.check_rows else 0, n)
     err = {}
@@ -505,12 +536,12 @@ def run_aot_rpy(args):
         pts = np.sort(rng.choice(n, m, replace=False))
         rows = (3 * pts[:, None] + np.arange(3)[None, :]).ravel()
         Xc = X.cpu().numpy()
-        for prec in precs:
+        for prec in Ys:
             e = []
             for c in (0, nv // 2):
                 yd = direct_sum("rpy", [eta], coord, Xc[:, c], coord[:, pts])
                 yc = Ys[prec][:, c].cpu().numpy()[rows]
-                e.append(float(np.linalg.norm(yc - yd) / np.linalg.norm(yd)))
+                e.append(rel2(yc, yd))
             err[prec] = max(e)
     cpu, parity = None, None
     if not args.no_cpu_baseline:
@@ -521,23 +552,26 @@ def run_aot_rpy(args):
         t = time.perf_counter()
         O.libref().H2P_matmul(H.h2pack, _abi.ROW_MAJOR, nv, O.dptr(Xh), nv, O.dptr(Yh), nv)
         sec = time.perf_counter() - t
+        mode = "JIT mode (blocks evaluated on the fly)" if gen else "stored blocks"
         cpu = {"value": nv / sec, "unit": "matvecs/s", "cores": H.info["n_thread"], "kind": "reference",
-               "sample": f"1 H2P_matmul ({nv} RHS) of H2Pack compiled from its sources, same handle and "
-                         f"inputs, {sec:.1f} s"}
+               "sample": f"1 H2P_matmul ({nv} RHS) of H2Pack compiled from its sources, same handle ({mode}) "
+                         f"and inputs, {sec:.1f} s"}
         # same representation, same inputs: GPU against H2Pack's own CPU H2P_matmul
-        parity = {f"{p}_vs_reference": rel2(Ys[p].cpu().numpy(), Yh) for p in precs}
+        parity = {f"{p}_vs_reference": rel2(Ys[p].cpu().numpy(), Yh) for p in Ys}
     peak = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]) \
         if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else 6650.0
-    main_p = "mixed" if "mixed" in out else precs[0]
+    main_p = "mixed" if "mixed" in Ys else next(iter(Ys))
     line = {"metric": f"H2 matvecs/s (RPY N={n} AOT, reltol 1e-8, {nv} RHS)", "value": out[main_p]["matvecs_per_s"],
             "unit": "matvecs/s", "workload": "aot_rpy", "n": n, "nvec": nv, "build_seconds": build_s,
-            "tuned_panel_variant": tuned,
+            "blocks": "generated on the GPU" if gen else "built on the host, uploaded",
+            "stored_entries": entries, "tuned_panel_variant": tuned,
             "fp64": out.get("fp64"), "mixed": out.get("mixed"), "rel_err_vs_direct": err, "parity": parity,
-            "speedup_mixed_vs_fp64": out["fp64"]["ms"] / out["mixed"]["ms"] if len(out) == 2 else None,
-            "roofline": {"bound": "hbm", "achieved": out[main_p]["streamed_GBps"], "peak": peak, "unit": "GB/s",
-                         "frac": out[main_p]["streamed_GBps"] / peak,
-                         "note": "stored FP32 U (read twice), B, D bytes x 16-RHS panels per matmul / matmul "
-                                 "time, of measured copy BW"},
+            "speedup_mixed_vs_fp64": out["fp64"]["ms"] / out["mixed"]["ms"]
+            if "ms" in out.get("fp64", {}) and "ms" in out.get("mixed", {}) else None,
+            "roofline": {"bound": "hbm", "achieved": out[main_p]["algorithmic_GBps"], "peak": peak, "unit": "GB/s",
+                         "frac": out[main_p]["algorithmic_GBps"] / peak,
+                         "note": "stored FP32 U (read twice), B and D bytes of one 64-RHS matmul (each block once) / "
+                                 "matmul time, of measured copy BW"},
             "cpu_baseline": cpu, "info": H.info}
     print(json.dumps(line), flush=True)
     H.close()
