@@ -128,7 +128,7 @@ H2PACK_GPU_SYMBOLS = {
 
 BUILDER_SYMBOLS = {
     "h2pb_build": (C.c_void_p, [C.c_int, _dp, C.c_int, C.c_int, _dp, C.c_double, C.c_int, C.c_double,
-                                C.c_int, C.c_int, C.c_char_p, C.c_int, C.c_int]),
+                                C.c_int, C.c_int, C.c_char_p, C.c_int, C.c_int, C.c_int]),
     "h2pb_h2pack": (C.c_void_p, [C.c_void_p]),
     "h2pb_build_seconds": (C.c_double, [C.c_void_p]),
     "h2pb_destroy": (None, [C.c_void_p]),

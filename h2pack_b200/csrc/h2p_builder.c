@@ -73,12 +73,13 @@ static void select_kernel(int kernel_id, kernel_eval_fptr *ev, kernel_bimv_fptr 
  *   pp_fname       : proxy point cache file for proxy_kind 0 (may be NULL)
  *   use_bimv       : 1 pass the kernel's bi-matvec to H2P_build, 0 pass NULL
  *   n_thread       : OpenMP threads for the build (<= 0: OpenMP default)
+ *   hss            : 1 build in HSS mode (H2P_run_HSS, examples/example_HSS.c:55)
  */
 H2PB_EXPORT h2pb_handle *h2pb_build(
     int kernel_id, const double *param, int n_param,
     int n_point, const double *coord, double reltol,
     int max_leaf_points, double max_leaf_size, int BD_JIT,
-    int proxy_kind, const char *pp_fname, int use_bimv, int n_thread)
+    int proxy_kind, const char *pp_fname, int use_bimv, int n_thread, int hss)
 {
     kernel_eval_fptr krnl_eval;
     kernel_bimv_fptr krnl_bimv;
@@ -105,6 +106,7 @@ H2PB_EXPORT h2pb_handle *h2pb_build(
     H2Pack_p h2pack;
     H2P_init(&h2pack, pt_dim, krnl_dim, QR_REL_NRM, &rel_tol);
     if (kernel_id == H2GPU_KRNL_RPY) H2P_run_RPY(h2pack);
+    if (hss) H2P_run_HSS(h2pack);
     const int xpt_dim = h2pack->xpt_dim;
 
     H2P_calc_enclosing_box(pt_dim, n_point, coord, proxy_kind == 0 ? pp_fname : NULL, &h2pack->root_enbox);
@@ -123,7 +125,7 @@ H2PB_EXPORT h2pb_handle *h2pb_build(
         int num_pp = 2 * pt_dim * num_pp_dim * num_pp_dim;
         /* xpt_dim rows so that RPY's radius row exists (zero-filled, src/H2Pack_gen_proxy_point.c:718-722) */
         H2P_generate_proxy_point_surface(pt_dim, xpt_dim, num_pp, h2pack->max_level,
-                                         h2pack->min_adm_level, max_L, &pp);
+                                         hss ? h2pack->HSS_min_adm_level : h2pack->min_adm_level, max_L, &pp);
     }
     hd->pp = pp;
     hd->n_pp = h2pack->max_level + 1;
@@ -205,7 +207,10 @@ H2PB_EXPORT int h2pb_describe_h2pack(H2Pack_p h, int kernel_id, const double *pa
                                      h2gpu_desc *d, int **ints_out, const double ***ptrs_out)
 {
     if (h == NULL || d == NULL) return H2GPU_ERR_INVALID;
-    if (h->is_HSS || h->is_RPY_Ewald || h->is_H2ERI) return H2GPU_ERR_UNSUPPORTED;
+    if (h->is_RPY_Ewald || h->is_H2ERI) return H2GPU_ERR_UNSUPPORTED;
+    /* HSS mode applies the same phases over its own pair lists and minimum admissible
+       level (src/H2Pack_matvec.c:101, :308, :773, :904) */
+    const int hss = h->is_HSS;
     if (h->U == NULL || h->pt_cluster == NULL) return H2GPU_ERR_STATE;
     int n_node = h->n_node;
     int *ints = (int *) malloc(sizeof(int) * 4 * (size_t) n_node);
@@ -227,14 +232,17 @@ H2PB_EXPORT int h2pb_describe_h2pack(H2Pack_p h, int kernel_id, const double *pa
     memset(d, 0, sizeof(*d));
     d->n_point = h->n_point;  d->pt_dim = h->pt_dim;  d->xpt_dim = h->xpt_dim;  d->krnl_dim = h->krnl_dim;
     d->n_node = n_node;  d->n_leaf_node = h->n_leaf_node;  d->max_child = h->max_child;
-    d->max_level = h->max_level;  d->min_adm_level = h->min_adm_level;  d->BD_JIT = h->BD_JIT;
+    d->max_level = h->max_level;  d->BD_JIT = h->BD_JIT;
+    d->min_adm_level = hss ? h->HSS_min_adm_level : h->min_adm_level;
     d->n_child = h->n_child;  d->children = h->children;  d->node_level = h->node_level;
     d->pt_cluster = h->pt_cluster;  d->mat_cluster = h->mat_cluster;
     d->level_n_node = h->level_n_node;  d->level_nodes = h->level_nodes;
     d->leaf_nodes = h->height_nodes;
     d->U_nrow = U_nrow;  d->U_ncol = U_ncol;  d->U_ld = U_ld;  d->U = U;
-    d->n_r_adm_pair = h->n_r_adm_pair;  d->r_adm_pairs = h->r_adm_pairs;
-    d->n_r_inadm_pair = h->n_r_inadm_pair;  d->r_inadm_pairs = h->r_inadm_pairs;
+    d->n_r_adm_pair = hss ? h->HSS_n_r_adm_pair : h->n_r_adm_pair;
+    d->r_adm_pairs = hss ? h->HSS_r_adm_pairs : h->r_adm_pairs;
+    d->n_r_inadm_pair = hss ? h->HSS_n_r_inadm_pair : h->n_r_inadm_pair;
+    d->r_inadm_pairs = hss ? h->HSS_r_inadm_pairs : h->r_inadm_pairs;
     d->n_B = h->n_B;  d->B_nrow = h->B_nrow;  d->B_ncol = h->B_ncol;  d->B_ptr = h->B_ptr;  d->B_data = h->B_data;
     d->n_D = h->n_D;  d->D_nrow = h->D_nrow;  d->D_ncol = h->D_ncol;  d->D_ptr = h->D_ptr;  d->D_data = h->D_data;
     d->coord = h->coord;  d->J_n = J_n;  d->J_coord = J_coord;

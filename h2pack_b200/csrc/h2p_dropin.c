@@ -347,7 +347,7 @@ static int image_of(H2Pack_p h, reg_entry *e)
     if (st != H2GPU_OK)
     {
         snprintf(g_msg, sizeof(g_msg), "handle not supported by the GPU apply path (status %d): "
-                 "HSS, periodic and H2ERI handles are not accelerated", st);
+                 "periodic / RPY-Ewald and H2ERI handles are not accelerated", st);
         return st;
     }
     h2gpu_options opt;

@@ -42,8 +42,9 @@
  *   H2P_gpu_release        free the handle's device image early (H2P_destroy does it too)
  *   H2P_gpu_last_error     message of the last failure
  *
- * Handles in HSS mode, RPY-Ewald / periodic handles and H2ERI handles are
- * rejected with H2GPU_ERR_UNSUPPORTED.
+ * Handles in HSS mode are applied over their HSS pair lists and minimum admissible
+ * level, as H2Pack does (src/H2Pack_matvec.c:101, :308, :773, :904).  RPY-Ewald /
+ * periodic handles and H2ERI handles are rejected with H2GPU_ERR_UNSUPPORTED.
  */
 #ifndef H2P_DROPIN_H
 #define H2P_DROPIN_H

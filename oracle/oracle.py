@@ -278,7 +278,7 @@ class RefH2:
 
     def __init__(self, kernel: str, param, coord: np.ndarray, reltol: float, max_leaf_points: int = 0,
                  max_leaf_size: float = 0.0, BD_JIT: int = 0, proxy: str = "surface",
-                 pp_fname: str | None = None, n_thread: int = 0, use_bimv: bool = True):
+                 pp_fname: str | None = None, n_thread: int = 0, use_bimv: bool = True, hss: bool = False):
         lib = libref()
         self.lib = lib
         self.kernel_id = _abi.KERNEL_IDS[kernel]
@@ -289,7 +289,7 @@ class RefH2:
         h = lib.h2pb_build(self.kernel_id, dptr(self.param), self.n_param, n_point, dptr(self.coord),
                            float(reltol), int(max_leaf_points), float(max_leaf_size), int(BD_JIT),
                            0 if proxy == "id" else 1, pp_fname.encode() if pp_fname else None,
-                           1 if use_bimv else 0, int(n_thread))
+                           1 if use_bimv else 0, int(n_thread), 1 if hss else 0)
         if not h:
             raise RuntimeError("h2pb_build failed")
         self.handle = h

@@ -219,3 +219,31 @@ def test_device_resident_matmul():
         img.close()
     finally:
         H.close()
+
+
+@pytest.mark.parametrize("kernel", ["coulomb", "gaussian", "matern32", "rpy"])
+@pytest.mark.parametrize("jit", [0, 1])
+def test_hss_mode_matches_reference(kernel, jit):
+    """HSS-mode handles (H2P_run_HSS) through the drop-in: the same phases over the HSS
+    pair lists and minimum admissible level (src/H2Pack_matvec.c:101, :308, :773, :904),
+    FP64 within 1e-12 of the reference's HSS H2P_matvec / H2P_matmul, mixed within 2e-6."""
+    coord = make_points(kernel, 2500 if kernel == "rpy" else 5000, 61)
+    R = O.RefH2(kernel, KERNEL_PARAMS[kernel], coord, 1e-6, BD_JIT=jit, hss=True, **build_kwargs(kernel))
+    lib = _abi.libh2pack_gpu()
+    try:
+        rng = np.random.default_rng(62)
+        x = rng.standard_normal(R.N)
+        y = np.zeros(R.N)
+        assert lib.H2P_gpu_matvec(R.h2pack, O.dptr(x), O.dptr(y)) == 0
+        assert rel(y, R.matvec(x)) < TOL64
+        X = rng.standard_normal((R.N, 16))
+        Y = np.zeros_like(X)
+        assert lib.H2P_gpu_matmul(R.h2pack, _abi.ROW_MAJOR, 16, O.dptr(X), 16, O.dptr(Y), 16) == 0
+        Yr = R.matmul(X)
+        assert rel(Y, Yr) < TOL64
+        assert lib.H2P_gpu_set_precision(R.h2pack, _abi.PREC_MIXED) == 0
+        assert lib.H2P_gpu_matmul(R.h2pack, _abi.ROW_MAJOR, 16, O.dptr(X), 16, O.dptr(Y), 16) == 0
+        assert rel(Y, Yr) < 2e-6
+    finally:
+        lib.H2P_gpu_release(R.h2pack)
+        R.close()

@@ -10,14 +10,16 @@ from h2pack_b200 import _abi
 
 pytestmark = pytest.mark.skipif(not O.have_ref(), reason="oracle/_ref not built (needs the H2Pack sources)")
 
-CASES = [(k, jit) for k in ("coulomb", "gaussian", "matern32", "rpy") for jit in (0, 1)]
+CASES = [(k, jit, hss) for k in ("coulomb", "gaussian", "matern32", "rpy") for jit in (0, 1) for hss in (0, 1)]
 
 
-@pytest.mark.parametrize("kernel,jit", CASES)
-def test_restatement_matches_reference(kernel, jit):
+@pytest.mark.parametrize("kernel,jit,hss", CASES)
+def test_restatement_matches_reference(kernel, jit, hss):
+    """H2 and HSS mode (HSS: its own pair lists and minimum admissible level,
+    src/H2Pack_matvec.c:101, :308, :773, :904)."""
     n = 1500 if kernel == "rpy" else 3000
     coord = make_points(kernel, n, seed=11)
-    R = O.RefH2(kernel, KERNEL_PARAMS[kernel], coord, 1e-6, BD_JIT=jit, **build_kwargs(kernel))
+    R = O.RefH2(kernel, KERNEL_PARAMS[kernel], coord, 1e-6, BD_JIT=jit, hss=bool(hss), **build_kwargs(kernel))
     try:
         rng = np.random.default_rng(3)
         x = rng.random(R.N) - 0.5
