@@ -111,6 +111,8 @@ struct h2gpu_image {
     int* d_y1_slots = nullptr;
     BlkTask* d_blkB = nullptr;
     BlkTask* d_blkD = nullptr;
+    WideUnit* d_wide = nullptr;   // units of the 64-wide passes: B pass 0, B pass 1, D pass 0, D pass 1
+    int n_wide[4] = {0, 0, 0, 0};
     JitTarget* d_jtN = nullptr;
     JitTarget* d_jtF = nullptr;
     JitSource* d_js = nullptr;
@@ -190,7 +192,7 @@ void free_all(h2gpu_image* im)
                     im->d_B32, im->d_D64, im->d_D32, im->d_pts64, im->d_pts32, im->d_XS, im->d_PS, im->d_Y1,
                     im->d_PUSH, im->d_io, im->d_owN, im->d_owF, im->d_pp, im->d_jtN2, im->d_jtF2, im->d_y1t2,
                     im->d_y1_slots2, im->d_asm2, im->d_asm_slots2, im->d_status, im->d_pg, im->d_ppts,
-                    im->d_pin, im->d_tiles};
+                    im->d_pin, im->d_tiles, im->d_wide};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (im->h_status) cudaFreeHost(im->h_status);
@@ -330,6 +332,7 @@ struct HostPlan {
     std::vector<Y1Task> y1t;
     std::vector<int> y1_slots;
     std::vector<BlkTask> blkB, blkD;
+    std::vector<WideUnit> wide;   // B pass 0, B pass 1, D pass 0, D pass 1 (counts in n_wide)
     std::vector<JitTarget> jtN, jtF;
     std::vector<JitSource> js;
     std::vector<AsmTask> at;
@@ -513,6 +516,22 @@ int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
             }
         }
         for (int n = 0; n < n_node; n++) has_y1[n] = !y1s[n].empty();
+        // units of the 64-wide passes: pass 0 per 64-row chunk of a task (A V), pass 1 per
+        // 64-column tile of a task (A^T W)
+        auto units = [&](const std::vector<BlkTask>& ts, int pass) {
+            int cnt = 0;
+            for (int i = 0; i < (int) ts.size(); i++)
+            {
+                const BlkTask& t = ts[i];
+                if ((pass == 0 ? t.out0_row : t.out1_row) < 0) continue;
+                for (int o = 0; o < (pass == 0 ? t.nrow : t.ncol); o += 64) { hp.wide.push_back(WideUnit{i, o}); cnt++; }
+            }
+            return cnt;
+        };
+        im->n_wide[0] = units(blkB, 0);
+        im->n_wide[1] = units(blkB, 1);
+        im->n_wide[2] = units(blkD, 0);
+        im->n_wide[3] = units(blkD, 1);
     } else {
         // ---- JIT: point space = sorted points, then the skeleton points of every node
         node_centers(d, ctr);
@@ -1185,6 +1204,33 @@ int check_plan(const h2gpu_image* im, const h2gpu_desc* d, const HostPlan& hp, l
         };
         TRY(cover_blocks("B", hp.blkB, d->n_B, d->B_nrow, d->B_ncol, d->B_ptr));
         TRY(cover_blocks("D", hp.blkD, d->n_D, d->D_nrow, d->D_ncol, d->D_ptr));
+        // ---- units of the 64-wide passes: every 64-row chunk (pass 0) and every 64-column
+        //      tile (pass 1) of every task that has the product, once each
+        long long w0 = 0;
+        const int* nw = im->n_wide;
+        REQ((long long) hp.wide.size() == (long long) nw[0] + nw[1] + nw[2] + nw[3], "plan: wide unit counts");
+        for (int part = 0; part < 4; part++)
+        {
+            const std::vector<BlkTask>& ts = part < 2 ? hp.blkB : hp.blkD;
+            const int pass = part & 1;
+            std::vector<std::vector<char>> seen(ts.size());
+            for (long long k = w0; k < w0 + nw[part]; k++)
+            {
+                const WideUnit u = hp.wide[k];
+                REQ(u.task >= 0 && u.task < (int) ts.size(), "plan: a wide unit names no task");
+                const BlkTask& t = ts[u.task];
+                const int ext = pass == 0 ? t.nrow : t.ncol;
+                REQ((pass == 0 ? t.out0_row : t.out1_row) >= 0, "plan: a wide unit of a product its task lacks");
+                REQ(u.off >= 0 && u.off < ext && u.off % 64 == 0, "plan: a wide unit starts off its 64-grid");
+                if (seen[u.task].empty()) seen[u.task].assign((ext + 63) / 64, 0);
+                REQ(++seen[u.task][u.off / 64] == 1, "plan: a wide unit repeats");
+            }
+            for (size_t i = 0; i < ts.size(); i++)
+                if ((pass == 0 ? ts[i].out0_row : ts[i].out1_row) >= 0)
+                    REQ(!seen[i].empty() && std::count(seen[i].begin(), seen[i].end(), 1) == (long long) seen[i].size(),
+                        "plan: a task's %s is not covered by wide units", pass == 0 ? "rows" : "columns");
+            w0 += nw[part];
+        }
     }
 
     long long pairs_plan = 0;
@@ -1433,6 +1479,7 @@ int upload_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
     TRY(upload(hp.y1_slots, &im->d_y1_slots, im->bytes));
     TRY(upload(hp.blkB, &im->d_blkB, im->bytes));
     TRY(upload(hp.blkD, &im->d_blkD, im->bytes));
+    TRY(upload(hp.wide, &im->d_wide, im->bytes));
     TRY(upload(hp.jtN, &im->d_jtN, im->bytes));
     TRY(upload(hp.jtF, &im->d_jtF, im->bytes));
     TRY(upload(hp.js, &im->d_js, im->bytes));
@@ -1605,9 +1652,19 @@ int run_panel(h2gpu_image* im, int NV, int nv, const double* X, long long x_rs, 
     CK(launch_gather(NV, X, x_rs, x_cs, nv, im->d_fwd, im->N, im->d_XS, s));
     // D phase first: it needs only x (in the graph-free stream order it simply runs before the upward sweep)
     if (timed) CK(cudaEventRecord(e[1], s));
+    const bool wide = f32 && !im->BD_JIT && NV == 64;   // two GEMM passes per block list
     if (!im->BD_JIT)
     {
-        if (f32) CK(launch_blk<float>(NV, im->d_blkD, im->n_blkD, im->d_D32, im->d_XS, im->d_PS, s, im->blk_tc, im->d_status));
+        if (wide)
+        {
+            const int* nw = im->n_wide;
+            CK(launch_blk_wide(0, im->d_blkD, im->d_wide + nw[0] + nw[1], nw[2], im->d_D32, im->d_XS, im->d_PS, s,
+                               im->d_status));
+            CK(launch_blk_wide(1, im->d_blkD, im->d_wide + nw[0] + nw[1] + nw[2], nw[3], im->d_D32, im->d_XS,
+                               im->d_PS, s, im->d_status));
+            im->st.n_launches += 1;
+        }
+        else if (f32) CK(launch_blk<float>(NV, im->d_blkD, im->n_blkD, im->d_D32, im->d_XS, im->d_PS, s, im->blk_tc, im->d_status));
         else CK(launch_blk<double>(NV, im->d_blkD, im->n_blkD, im->d_D64, im->d_XS, im->d_PS, s));
     } else {
         const bool panels = f32 && panels_used(im, NV);
@@ -1626,7 +1683,14 @@ int run_panel(h2gpu_image* im, int NV, int nv, const double* X, long long x_rs, 
     if (timed) CK(cudaEventRecord(e[3], s));
     if (!im->BD_JIT)
     {
-        if (f32) CK(launch_blk<float>(NV, im->d_blkB, im->n_blkB, im->d_B32, im->d_XS, im->d_PS, s, im->blk_tc, im->d_status));
+        if (wide)
+        {
+            const int* nw = im->n_wide;
+            CK(launch_blk_wide(0, im->d_blkB, im->d_wide, nw[0], im->d_B32, im->d_XS, im->d_PS, s, im->d_status));
+            CK(launch_blk_wide(1, im->d_blkB, im->d_wide + nw[0], nw[1], im->d_B32, im->d_XS, im->d_PS, s, im->d_status));
+            im->st.n_launches += 1;
+        }
+        else if (f32) CK(launch_blk<float>(NV, im->d_blkB, im->n_blkB, im->d_B32, im->d_XS, im->d_PS, s, im->blk_tc, im->d_status));
         else CK(launch_blk<double>(NV, im->d_blkB, im->n_blkB, im->d_B64, im->d_XS, im->d_PS, s));
         CK(launch_y1sum(NV, im->d_y1t, im->n_y1, im->d_y1_slots, im->d_PS, im->d_Y1, s));
     } else {

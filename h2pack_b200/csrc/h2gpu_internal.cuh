@@ -58,6 +58,14 @@ struct BlkTask {
     int out0_row, out1_row;   // -1: product not needed
 };
 
+// Unit of the wide-panel stored-block passes: one 64-row chunk of a task (pass 0,
+// A V over all column tiles) or one 64-column tile of a task (pass 1, A^T W over all of
+// the task's rows).
+struct WideUnit {
+    int task;          // index into the block-task list
+    int off;           // first row (pass 0) or first column (pass 1) of the unit
+};
+
 // JIT target: a set of points whose outputs accumulate over a list of source sets
 // (owner computes; each (target, source) kernel block is evaluated by its owner).
 struct JitTarget {

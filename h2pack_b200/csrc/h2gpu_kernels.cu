@@ -2301,6 +2301,228 @@ __global__ void __launch_bounds__(kBf3Threads, 2) k_blk_bf3w(const BlkTask* __re
 }
 
 
+// ------------------------ stored blocks on tcgen05, 64-wide panels as two GEMM passes
+
+// Instruction descriptor, kind::f16 with BF16 A and B, FP32 accumulator, M = 64, N = n,
+// A and B each K-major (0) or MN-major (1).
+__host__ __device__ constexpr uint32_t umma_idesc_bf16_ab(int n, int a_mn_major, int b_mn_major)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t) a_mn_major << 15) | ((uint32_t) b_mn_major << 16) |
+           ((uint32_t) (n >> 3) << 17) | ((uint32_t) (64 >> 4) << 24);
+}
+
+// A panel of 64 right-hand sides applied to the stored blocks as two passes over the block
+// tasks, each a plain GEMM whose outputs are written once (the one-pass kernel's per-tile
+// read-modify-write of the transposed-product slot dominated its memory traffic):
+//   pass 0, one unit per 64-row chunk of a task:     C0 = A_chunk V    (over the column tiles)
+//   pass 1, one unit per 64-column tile of a task:   C1 = A_tile^T W   (over the task's rows)
+// Each 64 x 64 tile of A (FP32) is split into BF16 pieces h + m + l in shared memory
+// (rows of 128 B, 128-byte swizzle).  The right-hand sides of a tile (64 rows of the
+// input space, row-major with the 64 right-hand sides contiguous) are split the same way
+// and used as an MN-major B operand, so they are read with coalesced loads and need no
+// transpose.  Six products per 16-deep K step (l.h + h.l + m.m + m.h + h.m + h.h), FP32 in
+// TMEM over one tile (64 terms), FP64 across tiles in shared memory; the unit's 64 output
+// rows are written once.  The next tile is loaded into registers while the MMAs of the
+// current one run.  Bounded waits record a status and stop.
+struct WideSmem {
+    uint16_t a[3][64 * 64];    // A tile pieces: 64 rows (of A) of 64 BF16, 128-byte swizzle
+    uint16_t b[3][64 * 64];    // right-hand-side pieces: 64 rows (k) of 64 BF16, 128-byte swizzle
+    double acc[64][65];        // FP64 sums of the unit's 64 output rows (padded)
+    unsigned long long mbar;
+    uint32_t tmem;
+};
+
+constexpr int wide_smem_bytes() { return (int) sizeof(WideSmem) + 1024; }
+
+template <int MODE>
+__global__ void __launch_bounds__(kBf3Threads, 2) k_blk_wide(const BlkTask* __restrict__ tasks,
+                                                             const WideUnit* __restrict__ units,
+                                                             const float* __restrict__ arena,
+                                                             const double* __restrict__ XS, double* __restrict__ PS,
+                                                             int* __restrict__ status)
+{
+    constexpr int NV = 64;
+    // pass 0: A K-major, B (V rows) MN-major; pass 1: A MN-major (A^T), B (W rows) MN-major
+    constexpr uint32_t IDESC = umma_idesc_bf16_ab(NV, MODE == 1 ? 1 : 0, 1);
+    extern __shared__ __align__(1024) unsigned char wide_raw[];
+    WideSmem& sm = *reinterpret_cast<WideSmem*>(wide_raw + ((1024 - (smem_u32(wide_raw) & 1023)) & 1023));
+    const WideUnit U = units[blockIdx.x];
+    const BlkTask T = tasks[U.task];
+    const int ncol = T.ncol, nrow = T.nrow;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    // the unit's fixed 64-row chunk (pass 0) or 64-column tile (pass 1), and the tiles it walks
+    const int nt = MODE == 0 ? (ncol + 63) / 64 : (nrow + 63) / 64;
+    const float* A0 = arena + T.a_off;
+
+    if (warp == 0)
+    {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 64;" ::"r"(smem_u32(&sm.tmem)) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0)
+    {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&sm.mbar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    for (int i = tid; i < 64 * 65; i += kBf3Threads) (&sm.acc[0][0])[i] = 0.0;
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = sm.tmem, mbar = smem_u32(&sm.mbar);
+    unsigned char* const a_b = reinterpret_cast<unsigned char*>(sm.a);
+    unsigned char* const b_b = reinterpret_cast<unsigned char*>(sm.b);
+    const uint32_t a_s = smem_u32(sm.a), b_s = smem_u32(sm.b);
+
+    // tile t: rows [rc, rc + R) and columns [c0, c0 + C) of the block task, and the 64 rows
+    // of right-hand sides that meet it (V rows in0 + c0 + k, or W rows in1 + rc + k)
+    auto tile_of = [&](int t, int& rc, int& c0) {
+        if (MODE == 0) { rc = U.off; c0 = 64 * t; }
+        else { rc = 64 * t; c0 = U.off; }
+    };
+    // registers of the tile being loaded: thread t holds 4 granules (row r, 8 consecutive
+    // columns q) of A and 4 granules (row k, 8 consecutive right-hand sides) of the inputs
+    float ra[4][8], rb[4][8];
+    auto load_tile = [&](int t) {
+        int rc, c0;
+        tile_of(t, rc, c0);
+        const int R = min(64, nrow - rc), C = min(64, ncol - c0);
+        const float* A = A0 + (long long) rc * ncol + c0;
+        const int nk = MODE == 0 ? C : R;
+        const double* B = XS + (long long) (MODE == 0 ? T.in0_row + c0 : T.in1_row + rc) * NV;
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+        {
+            const int gi = tid + kBf3Threads * u, r = gi >> 3, q = gi & 7;
+#pragma unroll
+            for (int j = 0; j < 8; j++)
+            {
+                const int c = 8 * q + j;
+                ra[u][j] = (r < R && c < C) ? A[(long long) r * ncol + c] : 0.f;
+            }
+            if (r < nk)
+            {
+                const double2* src = reinterpret_cast<const double2*>(B + (long long) r * NV + 8 * q);
+#pragma unroll
+                for (int j = 0; j < 4; j++)
+                {
+                    const double2 v = src[j];
+                    rb[u][2 * j] = (float) v.x;
+                    rb[u][2 * j + 1] = (float) v.y;
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < 8; j++) rb[u][j] = 0.f;
+            }
+        }
+    };
+    auto put = [&](unsigned char* base, int off, const float (&x)[8]) {
+        uint16_t h[8], m[8], l[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) bf16x3(x[j], h[j], m[j], l[j]);
+        auto pack = [](const uint16_t (&e)[8]) {
+            return make_uint4(e[0] | ((uint32_t) e[1] << 16), e[2] | ((uint32_t) e[3] << 16),
+                              e[4] | ((uint32_t) e[5] << 16), e[6] | ((uint32_t) e[7] << 16));
+        };
+        *reinterpret_cast<uint4*>(base + off) = pack(h);
+        *reinterpret_cast<uint4*>(base + 8192 + off) = pack(m);
+        *reinterpret_cast<uint4*>(base + 16384 + off) = pack(l);
+    };
+    auto store_tile = [&]() {
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+        {
+            const int gi = tid + kBf3Threads * u, r = gi >> 3, q = gi & 7;
+            put(a_b, sw128(r, q), ra[u]);
+            put(b_b, sw128(r, q), rb[u]);
+        }
+    };
+
+    bool ok = true;
+    uint32_t phase = 0;
+    double* const acc = sm.acc[(16 * warp + lane) & 63];
+    // add the tile's FP32 products (TMEM) into the unit's FP64 sums
+    auto drain = [&]() {
+        int good = 1;
+        if (tid == 0)
+        {
+            int it = 0;
+            while (!mbar_try_wait(mbar, phase))
+                if (++it > (1 << 22)) { good = 0; break; }
+            if (!good) atomicExch(status, 1);
+        }
+        phase ^= 1;
+        ok = __syncthreads_and(good) != 0;
+        if (!ok) return;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+        for (int h = 0; h < 2; h++)
+        {
+            uint32_t d[32];
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                         "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                         : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7]),
+                           "=r"(d[8]), "=r"(d[9]), "=r"(d[10]), "=r"(d[11]), "=r"(d[12]), "=r"(d[13]), "=r"(d[14]), "=r"(d[15]),
+                           "=r"(d[16]), "=r"(d[17]), "=r"(d[18]), "=r"(d[19]), "=r"(d[20]), "=r"(d[21]), "=r"(d[22]), "=r"(d[23]),
+                           "=r"(d[24]), "=r"(d[25]), "=r"(d[26]), "=r"(d[27]), "=r"(d[28]), "=r"(d[29]), "=r"(d[30]), "=r"(d[31])
+                         : "r"(tmem + ((uint32_t) (32 * warp) << 16) + (uint32_t) (32 * h)));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (lane < 16)
+#pragma unroll
+                for (int n = 0; n < 32; n++) acc[32 * h + n] += (double) __uint_as_float(d[n]);
+        }
+    };
+
+    constexpr int PA[6] = {2, 0, 1, 1, 0, 0}, PB[6] = {0, 2, 1, 0, 1, 0};
+    if (nt > 0) load_tile(0);
+    for (int t = 0; t < nt; t++)
+    {
+        if (t > 0) drain();
+        if (!ok) break;
+        store_tile();
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        if (tid == 0)
+        {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+            for (int ks = 0; ks < 4; ks++)          // K-steps of 16
+#pragma unroll
+                for (int p = 0; p < 6; p++)
+                {
+                    // pass 0: A K-major (32-byte step along a row); pass 1: A MN-major
+                    // (16 rows = two 8-row swizzle atoms per step); B MN-major in both
+                    const uint64_t ad = MODE == 0 ? umma_desc(a_s + PA[p] * 8192 + ks * 32, 16, 1024, 2)
+                                                  : umma_desc(a_s + PA[p] * 8192 + ks * 2048, 8192, 1024, 2);
+                    umma_f16(tmem, ad, umma_desc(b_s + PB[p] * 8192 + ks * 2048, 8192, 1024, 2), IDESC,
+                             (ks == 0 && p == 0) ? 0u : 1u);
+                }
+            umma_commit(mbar);
+        }
+        if (t + 1 < nt) load_tile(t + 1);
+    }
+    if (ok && nt > 0) drain();
+    // the unit's outputs, written once
+    if (ok && lane < 16)
+    {
+        const int m = 16 * warp + lane;
+        const int lim = MODE == 0 ? min(64, nrow - U.off) : min(64, ncol - U.off);
+        if (m < lim)
+        {
+            double* o = PS + (long long) ((MODE == 0 ? T.out0_row : T.out1_row) + U.off + m) * NV;
+#pragma unroll 8
+            for (int n = 0; n < NV; n++) o[n] = acc[n];
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+    {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 64;" ::"r"(tmem) : "memory");
+    }
+}
+
 // ---------------------------------------------- sweeps on the tensor cores (FP32 U)
 
 // Upward / downward sweep products for FP32 U and panels of 8 / 16 right-hand sides on
@@ -2681,6 +2903,25 @@ cudaError_t launch_blk(int NV, const BlkTask* t, int n, const TA* arena, const d
             k_blk<TA, NVc><<<n, kThreads, b, st>>>(t, arena, XS, PS);
         }
     });
+    return cudaGetLastError();
+}
+
+cudaError_t launch_blk_wide(int mode, const BlkTask* t, const WideUnit* u, int n, const float* arena,
+                            const double* XS, double* PS, cudaStream_t st, int* status)
+{
+    if (n <= 0) return cudaSuccess;
+    if (!status) return cudaErrorInvalidValue;
+    constexpr int b = wide_smem_bytes();
+    if (mode == 0)
+    {
+        cudaError_t e = allow_smem(k_blk_wide<0>, b);
+        if (e != cudaSuccess) return e;
+        k_blk_wide<0><<<n, kBf3Threads, b, st>>>(t, u, arena, XS, PS, status);
+    } else {
+        cudaError_t e = allow_smem(k_blk_wide<1>, b);
+        if (e != cudaSuccess) return e;
+        k_blk_wide<1><<<n, kBf3Threads, b, st>>>(t, u, arena, XS, PS, status);
+    }
     return cudaGetLastError();
 }
 

@@ -18,6 +18,10 @@ cudaError_t launch_up(int NV, const UpTask* t, int n, const TA* U, double* XS, c
 template <typename TA>
 cudaError_t launch_blk(int NV, const BlkTask* t, int n, const TA* arena, const double* XS, double* PS, cudaStream_t st,
                        int use_tc = 0, int* status = nullptr);   // use_tc: 1 mma.sync, 2 tcgen05
+// 64-wide panels of FP32 stored blocks on tcgen05: pass 0 (mode 0, units = 64-row chunks:
+// A V) or pass 1 (mode 1, units = 64-column tiles: A^T W), outputs written once
+cudaError_t launch_blk_wide(int mode, const BlkTask* t, const WideUnit* u, int n, const float* arena,
+                            const double* XS, double* PS, cudaStream_t st, int* status);
 template <typename TA>
 cudaError_t launch_down(int NV, const DownTask* t, int n, const TA* U, const double* Y1, double* PS, double* PUSH,
                         cudaStream_t st, int use_tc = 0);
