@@ -31,6 +31,45 @@ FIXTURES = [
 ]
 
 
+H2FILE_DIR = os.path.join(HERE, "h2file_coulomb")
+REF_EXAMPLES = os.environ.get("H2PACK_EXAMPLES", "/root/reference/examples")
+
+
+def make_h2file():
+    """An H2 matrix stored by H2Pack itself (H2P_store_to_file, src/H2Pack_file_IO.c:17-218,
+    whose JSON encoding is done by H2Pack's examples/meta_txt_to_json.py, run here from the
+    H2Pack tree in a scratch directory), plus inputs and H2Pack's own H2P_matvec /
+    H2P_matmul outputs on the stored representation."""
+    import ctypes as C
+    import shutil
+    import tempfile
+    coord = make_points("coulomb", 400, seed=4321)
+    R = O.RefH2("coulomb", [], coord, 1e-6, max_leaf_points=40, BD_JIT=0, proxy="surface")
+    os.makedirs(H2FILE_DIR, exist_ok=True)
+    lib = O.libref()
+    lib.H2P_store_to_file.argtypes = [C.c_void_p, C.c_char_p, C.c_char_p, C.c_char_p]
+    lib.H2P_store_to_file.restype = None
+    cwd = os.getcwd()
+    with tempfile.TemporaryDirectory() as tmp:
+        shutil.copy(os.path.join(REF_EXAMPLES, "meta_txt_to_json.py"), tmp)
+        os.chmod(os.path.join(tmp, "meta_txt_to_json.py"), 0o755)
+        os.chdir(tmp)
+        try:
+            lib.H2P_store_to_file(R.h2pack, b"meta.json", b"aux.json", b"h2.bin")
+        finally:
+            os.chdir(cwd)
+        for f in ("meta.json", "aux.json", "h2.bin"):
+            shutil.copy(os.path.join(tmp, f), os.path.join(H2FILE_DIR, f))
+    rng = np.random.default_rng(98)
+    x = rng.random(R.N) - 0.5
+    X = rng.standard_normal((R.N, 4))
+    np.savez_compressed(os.path.join(H2FILE_DIR, "io.npz"), x=x, y_ref=R.matvec(x), X=X, Y_ref=R.matmul(X),
+                        coord_in=coord)
+    print("h2file_coulomb", R.info["n_node"], sum(os.path.getsize(os.path.join(H2FILE_DIR, f)) for f in
+                                                 os.listdir(H2FILE_DIR)) // 1024, "KiB")
+    R.close()
+
+
 def main():
     for name, kernel, n, jit, mlp, mls, tol in FIXTURES:
         coord = make_points(kernel, n, seed=1234)
@@ -51,4 +90,8 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    if len(sys.argv) > 1 and sys.argv[1] == "h2file":
+        make_h2file()
+    else:
+        main()
+        make_h2file()
