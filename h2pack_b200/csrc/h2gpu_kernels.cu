@@ -2334,12 +2334,29 @@ struct WideSmem {
 
 constexpr int wide_smem_bytes() { return (int) sizeof(WideSmem) + 1024; }
 
+// Three BF16 pieces h + m + l of a pair of FP32 values, packed two per 32-bit word (element
+// order: the first value in the low half): each piece the round-to-nearest of the
+// remainder, the remainders formed in packed FP32x2 arithmetic (exact: h and m are the
+// leading bits of the value they are subtracted from).
+__device__ __forceinline__ void bf16x3_pair(float x0, float x1, uint32_t& h, uint32_t& m, uint32_t& l)
+{
+    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(h) : "f"(x1), "f"(x0));
+    const float2 m1 = make_float2(-1.f, -1.f);
+    const float2 r1 = __ffma2_rn(make_float2(__uint_as_float(h << 16), __uint_as_float(h & 0xffff0000u)), m1,
+                                 make_float2(x0, x1));
+    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(m) : "f"(r1.y), "f"(r1.x));
+    const float2 r2 = __ffma2_rn(make_float2(__uint_as_float(m << 16), __uint_as_float(m & 0xffff0000u)), m1, r1);
+    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(l) : "f"(r2.y), "f"(r2.x));
+}
+
+constexpr int kWideThreads = 256;
+
 template <int MODE>
-__global__ void __launch_bounds__(kBf3Threads, 2) k_blk_wide(const BlkTask* __restrict__ tasks,
-                                                             const WideUnit* __restrict__ units,
-                                                             const float* __restrict__ arena,
-                                                             const double* __restrict__ XS, double* __restrict__ PS,
-                                                             int* __restrict__ status)
+__global__ void __launch_bounds__(kWideThreads, 2) k_blk_wide(const BlkTask* __restrict__ tasks,
+                                                              const WideUnit* __restrict__ units,
+                                                              const float* __restrict__ arena,
+                                                              const double* __restrict__ XS, double* __restrict__ PS,
+                                                              int* __restrict__ status)
 {
     constexpr int NV = 64;
     // pass 0: A K-major, B (V rows) MN-major; pass 1: A MN-major (A^T), B (W rows) MN-major
@@ -2364,7 +2381,7 @@ __global__ void __launch_bounds__(kBf3Threads, 2) k_blk_wide(const BlkTask* __re
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&sm.mbar)) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    for (int i = tid; i < 64 * 65; i += kBf3Threads) (&sm.acc[0][0])[i] = 0.0;
+    for (int i = tid; i < 64 * 65; i += kWideThreads) (&sm.acc[0][0])[i] = 0.0;
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -2379,9 +2396,9 @@ __global__ void __launch_bounds__(kBf3Threads, 2) k_blk_wide(const BlkTask* __re
         if (MODE == 0) { rc = U.off; c0 = 64 * t; }
         else { rc = 64 * t; c0 = U.off; }
     };
-    // registers of the tile being loaded: thread t holds 4 granules (row r, 8 consecutive
-    // columns q) of A and 4 granules (row k, 8 consecutive right-hand sides) of the inputs
-    float ra[4][8], rb[4][8];
+    // registers of the tile being loaded: thread t holds 2 granules (row r, 8 consecutive
+    // columns q) of A and 2 granules (row k, 8 consecutive right-hand sides) of the inputs
+    float ra[2][8], rb[2][8];
     auto load_tile = [&](int t) {
         int rc, c0;
         tile_of(t, rc, c0);
@@ -2390,9 +2407,9 @@ __global__ void __launch_bounds__(kBf3Threads, 2) k_blk_wide(const BlkTask* __re
         const int nk = MODE == 0 ? C : R;
         const double* B = XS + (long long) (MODE == 0 ? T.in0_row + c0 : T.in1_row + rc) * NV;
 #pragma unroll
-        for (int u = 0; u < 4; u++)
+        for (int u = 0; u < 2; u++)
         {
-            const int gi = tid + kBf3Threads * u, r = gi >> 3, q = gi & 7;
+            const int gi = tid + kWideThreads * u, r = gi >> 3, q = gi & 7;
 #pragma unroll
             for (int j = 0; j < 8; j++)
             {
@@ -2416,22 +2433,18 @@ __global__ void __launch_bounds__(kBf3Threads, 2) k_blk_wide(const BlkTask* __re
         }
     };
     auto put = [&](unsigned char* base, int off, const float (&x)[8]) {
-        uint16_t h[8], m[8], l[8];
+        uint32_t h[4], m[4], l[4];
 #pragma unroll
-        for (int j = 0; j < 8; j++) bf16x3(x[j], h[j], m[j], l[j]);
-        auto pack = [](const uint16_t (&e)[8]) {
-            return make_uint4(e[0] | ((uint32_t) e[1] << 16), e[2] | ((uint32_t) e[3] << 16),
-                              e[4] | ((uint32_t) e[5] << 16), e[6] | ((uint32_t) e[7] << 16));
-        };
-        *reinterpret_cast<uint4*>(base + off) = pack(h);
-        *reinterpret_cast<uint4*>(base + 8192 + off) = pack(m);
-        *reinterpret_cast<uint4*>(base + 16384 + off) = pack(l);
+        for (int j = 0; j < 4; j++) bf16x3_pair(x[2 * j], x[2 * j + 1], h[j], m[j], l[j]);
+        *reinterpret_cast<uint4*>(base + off) = make_uint4(h[0], h[1], h[2], h[3]);
+        *reinterpret_cast<uint4*>(base + 8192 + off) = make_uint4(m[0], m[1], m[2], m[3]);
+        *reinterpret_cast<uint4*>(base + 16384 + off) = make_uint4(l[0], l[1], l[2], l[3]);
     };
     auto store_tile = [&]() {
 #pragma unroll
-        for (int u = 0; u < 4; u++)
+        for (int u = 0; u < 2; u++)
         {
-            const int gi = tid + kBf3Threads * u, r = gi >> 3, q = gi & 7;
+            const int gi = tid + kWideThreads * u, r = gi >> 3, q = gi & 7;
             put(a_b, sw128(r, q), ra[u]);
             put(b_b, sw128(r, q), rb[u]);
         }
@@ -2439,7 +2452,10 @@ __global__ void __launch_bounds__(kBf3Threads, 2) k_blk_wide(const BlkTask* __re
 
     bool ok = true;
     uint32_t phase = 0;
-    double* const acc = sm.acc[(16 * warp + lane) & 63];
+    // warp w reads TMEM lane quadrant w % 4 (rows 16 (w % 4) + lane, lane < 16) and the 32
+    // accumulator columns 32 (w / 4) .. + 31
+    const int quad = warp & 3, half = warp >> 2;
+    double* const acc = sm.acc[(16 * quad + lane) & 63] + 32 * half;
     // add the tile's FP32 products (TMEM) into the unit's FP64 sums
     auto drain = [&]() {
         int good = 1;
@@ -2454,22 +2470,18 @@ __global__ void __launch_bounds__(kBf3Threads, 2) k_blk_wide(const BlkTask* __re
         ok = __syncthreads_and(good) != 0;
         if (!ok) return;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        uint32_t d[32];
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                     "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                     : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7]),
+                       "=r"(d[8]), "=r"(d[9]), "=r"(d[10]), "=r"(d[11]), "=r"(d[12]), "=r"(d[13]), "=r"(d[14]), "=r"(d[15]),
+                       "=r"(d[16]), "=r"(d[17]), "=r"(d[18]), "=r"(d[19]), "=r"(d[20]), "=r"(d[21]), "=r"(d[22]), "=r"(d[23]),
+                       "=r"(d[24]), "=r"(d[25]), "=r"(d[26]), "=r"(d[27]), "=r"(d[28]), "=r"(d[29]), "=r"(d[30]), "=r"(d[31])
+                     : "r"(tmem + ((uint32_t) (32 * quad) << 16) + (uint32_t) (32 * half)));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (lane < 16)
 #pragma unroll
-        for (int h = 0; h < 2; h++)
-        {
-            uint32_t d[32];
-            asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-                         "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-                         : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7]),
-                           "=r"(d[8]), "=r"(d[9]), "=r"(d[10]), "=r"(d[11]), "=r"(d[12]), "=r"(d[13]), "=r"(d[14]), "=r"(d[15]),
-                           "=r"(d[16]), "=r"(d[17]), "=r"(d[18]), "=r"(d[19]), "=r"(d[20]), "=r"(d[21]), "=r"(d[22]), "=r"(d[23]),
-                           "=r"(d[24]), "=r"(d[25]), "=r"(d[26]), "=r"(d[27]), "=r"(d[28]), "=r"(d[29]), "=r"(d[30]), "=r"(d[31])
-                         : "r"(tmem + ((uint32_t) (32 * warp) << 16) + (uint32_t) (32 * h)));
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (lane < 16)
-#pragma unroll
-                for (int n = 0; n < 32; n++) acc[32 * h + n] += (double) __uint_as_float(d[n]);
-        }
+            for (int n = 0; n < 32; n++) acc[n] += (double) __uint_as_float(d[n]);
     };
 
     constexpr int PA[6] = {2, 0, 1, 1, 0, 0}, PB[6] = {0, 2, 1, 0, 1, 0};
@@ -2503,15 +2515,16 @@ __global__ void __launch_bounds__(kBf3Threads, 2) k_blk_wide(const BlkTask* __re
     }
     if (ok && nt > 0) drain();
     // the unit's outputs, written once
+    __syncthreads();
     if (ok && lane < 16)
     {
-        const int m = 16 * warp + lane;
+        const int m = 16 * quad + lane;
         const int lim = MODE == 0 ? min(64, nrow - U.off) : min(64, ncol - U.off);
         if (m < lim)
         {
-            double* o = PS + (long long) ((MODE == 0 ? T.out0_row : T.out1_row) + U.off + m) * NV;
+            double* o = PS + (long long) ((MODE == 0 ? T.out0_row : T.out1_row) + U.off + m) * NV + 32 * half;
 #pragma unroll 8
-            for (int n = 0; n < NV; n++) o[n] = acc[n];
+            for (int n = 0; n < 32; n++) o[n] = acc[n];
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -2533,12 +2546,16 @@ __global__ void __launch_bounds__(kBf3Threads, 2) k_blk_wide(const BlkTask* __re
 // (Y = the node's summed y1 plus the parent's push-down slice).  Warp w owns output
 // columns (UP) / rows (DOWN) 8w..8w+7.  The 32-deep k tiles of U and the X^T / Y^T
 // fragments are double-buffered through registers.
-template <int NV, bool UP>
+// STRIDE: row stride of the vector spaces.  A 64-wide panel (STRIDE = 64) runs as four
+// 16-column sub-panels, blockIdx.y = sub-panel (columns 16 blockIdx.y .. + 15).
+template <int NV, bool UP, int STRIDE = NV>
 __global__ void __launch_bounds__(256, 4) k_sweep_tc(const UpTask* __restrict__ ups, const DownTask* __restrict__ dns,
                                                      const float* __restrict__ Uar, double* __restrict__ XS,
                                                      const double* __restrict__ Y1, double* __restrict__ PS,
                                                      double* __restrict__ PUSH)
 {
+    static_assert(STRIDE == NV || NV == 16, "sub-panels are 16 columns wide");
+    const int v0 = STRIDE == NV ? 0 : 16 * (int) blockIdx.y;
     constexpr int KT = 32;
     constexpr int ROWS = UP ? KT : 64, LD = UP ? 72 : 36;   // padded: conflict-free fragment reads
     __shared__ float s_u[2][ROWS][LD];
@@ -2553,18 +2570,18 @@ __global__ void __launch_bounds__(256, 4) k_sweep_tc(const UpTask* __restrict__ 
         K = T.nrow; M = T.nc; lda = T.ld;
         A = Uar + T.u_off + T.c0;
         xrow = T.in_row;
-        out = XS + (long long) (T.out_row + T.c0) * NV;
+        out = XS + (long long) (T.out_row + T.c0) * STRIDE + v0;
     } else {
         const DownTask T = dns[blockIdx.x];
         K = T.ncol; M = T.nrow; lda = T.ncol;
         A = Uar + T.u_off;
         y1_row = T.y1_row; push_row = T.push_row;
-        out = (T.dst_ps ? PS : PUSH) + (long long) T.dst_row * NV;
+        out = (T.dst_ps ? PS : PUSH) + (long long) T.dst_row * STRIDE + v0;
     }
     auto xin = [&](int k, int v) -> double {
-        if constexpr (UP) return XS[(long long) (xrow + k) * NV + v];
-        double b = (y1_row >= 0) ? Y1[(long long) (y1_row + k) * NV + v] : 0.0;
-        if (push_row >= 0) b += PUSH[(long long) (push_row + k) * NV + v];
+        if constexpr (UP) return XS[(long long) (xrow + k) * STRIDE + v0 + v];
+        double b = (y1_row >= 0) ? Y1[(long long) (y1_row + k) * STRIDE + v0 + v] : 0.0;
+        if (push_row >= 0) b += PUSH[(long long) (push_row + k) * STRIDE + v0 + v];
         return b;
     };
     float ra[8];
@@ -2660,7 +2677,7 @@ __global__ void __launch_bounds__(256, 4) k_sweep_tc(const UpTask* __restrict__ 
     for (int q = 0; q < 4; q++)
     {
         const int rhs = (q < 2) ? g : g + 8, m = 8 * warp + 2 * tq + (q & 1);
-        if (rhs < NV && m < M) out[(long long) m * NV + rhs] = acc[q];
+        if (rhs < NV && m < M) out[(long long) m * STRIDE + rhs] = acc[q];
     }
 }
 
@@ -2813,6 +2830,11 @@ cudaError_t launch_up(int NV, const UpTask* t, int n, const TA* U, double* XS, c
     if (n <= 0) return cudaSuccess;
     if constexpr (sizeof(TA) == 4)
     {
+        if (use_tc && NV == 64)
+        {
+            k_sweep_tc<16, true, 64><<<dim3(n, 4), 256, 0, st>>>(t, nullptr, U, XS, nullptr, nullptr, nullptr);
+            return cudaGetLastError();
+        }
         if (use_tc && (NV == 8 || NV == 16))
         {
             if (NV == 16) k_sweep_tc<16, true><<<n, 256, 0, st>>>(t, nullptr, U, XS, nullptr, nullptr, nullptr);
@@ -2916,11 +2938,11 @@ cudaError_t launch_blk_wide(int mode, const BlkTask* t, const WideUnit* u, int n
     {
         cudaError_t e = allow_smem(k_blk_wide<0>, b);
         if (e != cudaSuccess) return e;
-        k_blk_wide<0><<<n, kBf3Threads, b, st>>>(t, u, arena, XS, PS, status);
+        k_blk_wide<0><<<n, kWideThreads, b, st>>>(t, u, arena, XS, PS, status);
     } else {
         cudaError_t e = allow_smem(k_blk_wide<1>, b);
         if (e != cudaSuccess) return e;
-        k_blk_wide<1><<<n, kBf3Threads, b, st>>>(t, u, arena, XS, PS, status);
+        k_blk_wide<1><<<n, kWideThreads, b, st>>>(t, u, arena, XS, PS, status);
     }
     return cudaGetLastError();
 }
@@ -2932,6 +2954,11 @@ cudaError_t launch_down(int NV, const DownTask* t, int n, const TA* U, const dou
     if (n <= 0) return cudaSuccess;
     if constexpr (sizeof(TA) == 4)
     {
+        if (use_tc && NV == 64)
+        {
+            k_sweep_tc<16, false, 64><<<dim3(n, 4), 256, 0, st>>>(nullptr, t, U, nullptr, Y1, PS, PUSH);
+            return cudaGetLastError();
+        }
         if (use_tc && (NV == 8 || NV == 16))
         {
             if (NV == 16) k_sweep_tc<16, false><<<n, 256, 0, st>>>(nullptr, t, U, nullptr, Y1, PS, PUSH);
