@@ -2325,10 +2325,10 @@ __host__ __device__ constexpr uint32_t umma_idesc_bf16_ab(int n, int a_mn_major,
 // rows are written once.  The next tile is loaded into registers while the MMAs of the
 // current one run.  Bounded waits record a status and stop.
 struct WideSmem {
-    uint16_t a[2][3][64 * 64]; // two stages of A tile pieces: 64 rows (of A) of 64 BF16, 128-byte swizzle
-    uint16_t b[2][3][64 * 64]; // two stages of right-hand-side pieces: 64 rows (k) of 64 BF16, swizzled
+    uint16_t a[3][64 * 64];    // A tile pieces: 64 rows (of A) of 64 BF16, 128-byte swizzle
+    uint16_t b[3][64 * 64];    // right-hand-side pieces: 64 rows (k) of 64 BF16, 128-byte swizzle
     double acc[64][65];        // FP64 sums of the unit's 64 output rows (padded)
-    unsigned long long mbar[2];
+    unsigned long long mbar;
     uint32_t tmem;
 };
 
@@ -2352,7 +2352,7 @@ __device__ __forceinline__ void bf16x3_pair(float x0, float x1, uint32_t& h, uin
 constexpr int kWideThreads = 256;
 
 template <int MODE>
-__global__ void __launch_bounds__(kWideThreads, 1) k_blk_wide(const BlkTask* __restrict__ tasks,
+__global__ void __launch_bounds__(kWideThreads, 2) k_blk_wide(const BlkTask* __restrict__ tasks,
                                                               const WideUnit* __restrict__ units,
                                                               const float* __restrict__ arena,
                                                               const double* __restrict__ XS, double* __restrict__ PS,
@@ -2361,7 +2361,6 @@ __global__ void __launch_bounds__(kWideThreads, 1) k_blk_wide(const BlkTask* __r
     constexpr int NV = 64;
     // pass 0: A K-major, B (V rows) MN-major; pass 1: A MN-major (A^T), B (W rows) MN-major
     constexpr uint32_t IDESC = umma_idesc_bf16_ab(NV, MODE == 1 ? 1 : 0, 1);
-    constexpr int STAGE = 3 * 64 * 64 * 2;       // bytes of one stage of A (or B) pieces
     extern __shared__ __align__(1024) unsigned char wide_raw[];
     WideSmem& sm = *reinterpret_cast<WideSmem*>(wide_raw + ((1024 - (smem_u32(wide_raw) & 1023)) & 1023));
     const WideUnit U = units[blockIdx.x];
@@ -2374,25 +2373,25 @@ __global__ void __launch_bounds__(kWideThreads, 1) k_blk_wide(const BlkTask* __r
 
     if (warp == 0)
     {
-        // two accumulators of 64 columns: tile t uses columns 64 (t & 1)
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 128;" ::"r"(smem_u32(&sm.tmem)) : "memory");
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 64;" ::"r"(smem_u32(&sm.tmem)) : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (tid == 0)
     {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&sm.mbar[0])) : "memory");
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&sm.mbar[1])) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&sm.mbar)) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     for (int i = tid; i < 64 * 65; i += kWideThreads) (&sm.acc[0][0])[i] = 0.0;
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const uint32_t tmem = sm.tmem;
+    const uint32_t tmem = sm.tmem, mbar = smem_u32(&sm.mbar);
     unsigned char* const a_b = reinterpret_cast<unsigned char*>(sm.a);
     unsigned char* const b_b = reinterpret_cast<unsigned char*>(sm.b);
     const uint32_t a_s = smem_u32(sm.a), b_s = smem_u32(sm.b);
 
+    // tile t: rows [rc, rc + R) and columns [c0, c0 + C) of the block task, and the 64 rows
+    // of right-hand sides that meet it (V rows in0 + c0 + k, or W rows in1 + rc + k)
     auto tile_of = [&](int t, int& rc, int& c0) {
         if (MODE == 0) { rc = U.off; c0 = 64 * t; }
         else { rc = 64 * t; c0 = U.off; }
@@ -2441,59 +2440,33 @@ __global__ void __launch_bounds__(kWideThreads, 1) k_blk_wide(const BlkTask* __r
         *reinterpret_cast<uint4*>(base + 8192 + off) = make_uint4(m[0], m[1], m[2], m[3]);
         *reinterpret_cast<uint4*>(base + 16384 + off) = make_uint4(l[0], l[1], l[2], l[3]);
     };
-    auto store_tile = [&](int stage) {
+    auto store_tile = [&]() {
 #pragma unroll
         for (int u = 0; u < 2; u++)
         {
             const int gi = tid + kWideThreads * u, r = gi >> 3, q = gi & 7;
-            put(a_b + stage * STAGE, sw128(r, q), ra[u]);
-            put(b_b + stage * STAGE, sw128(r, q), rb[u]);
-        }
-    };
-    constexpr int PA[6] = {2, 0, 1, 1, 0, 0}, PB[6] = {0, 2, 1, 0, 1, 0};
-    // make the stored stage visible to the tensor cores and issue its 24 MMAs into the
-    // stage's accumulator (thread 0), committed to the stage's mbarrier
-    auto issue = [&](int stage) {
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        __syncthreads();
-        if (tid == 0)
-        {
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t as = a_s + stage * STAGE, bs = b_s + stage * STAGE, d = tmem + 64u * stage;
-#pragma unroll
-            for (int ks = 0; ks < 4; ks++)          // K-steps of 16
-#pragma unroll
-                for (int p = 0; p < 6; p++)
-                {
-                    // pass 0: A K-major (32-byte step along a row); pass 1: A MN-major
-                    // (16 rows = two 8-row swizzle atoms per step); B MN-major in both
-                    const uint64_t ad = MODE == 0 ? umma_desc(as + PA[p] * 8192 + ks * 32, 16, 1024, 2)
-                                                  : umma_desc(as + PA[p] * 8192 + ks * 2048, 8192, 1024, 2);
-                    umma_f16(d, ad, umma_desc(bs + PB[p] * 8192 + ks * 2048, 8192, 1024, 2), IDESC,
-                             (ks == 0 && p == 0) ? 0u : 1u);
-                }
-            umma_commit(smem_u32(&sm.mbar[stage]));
+            put(a_b, sw128(r, q), ra[u]);
+            put(b_b, sw128(r, q), rb[u]);
         }
     };
 
     bool ok = true;
-    uint32_t phase[2] = {0, 0};
+    uint32_t phase = 0;
     // warp w reads TMEM lane quadrant w % 4 (rows 16 (w % 4) + lane, lane < 16) and the 32
-    // accumulator columns 32 (w / 4) .. + 31 of the stage
+    // accumulator columns 32 (w / 4) .. + 31
     const int quad = warp & 3, half = warp >> 2;
     double* const acc = sm.acc[(16 * quad + lane) & 63] + 32 * half;
-    // wait for the MMAs of a stage, then add its FP32 products into the unit's FP64 sums
-    auto drain = [&](int stage) {
+    // add the tile's FP32 products (TMEM) into the unit's FP64 sums
+    auto drain = [&]() {
         int good = 1;
         if (tid == 0)
         {
             int it = 0;
-            while (!mbar_try_wait(smem_u32(&sm.mbar[stage]), phase[stage]))
+            while (!mbar_try_wait(mbar, phase))
                 if (++it > (1 << 22)) { good = 0; break; }
             if (!good) atomicExch(status, 1);
         }
-        phase[stage] ^= 1;
+        phase ^= 1;
         ok = __syncthreads_and(good) != 0;
         if (!ok) return;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -2504,31 +2477,43 @@ __global__ void __launch_bounds__(kWideThreads, 1) k_blk_wide(const BlkTask* __r
                        "=r"(d[8]), "=r"(d[9]), "=r"(d[10]), "=r"(d[11]), "=r"(d[12]), "=r"(d[13]), "=r"(d[14]), "=r"(d[15]),
                        "=r"(d[16]), "=r"(d[17]), "=r"(d[18]), "=r"(d[19]), "=r"(d[20]), "=r"(d[21]), "=r"(d[22]), "=r"(d[23]),
                        "=r"(d[24]), "=r"(d[25]), "=r"(d[26]), "=r"(d[27]), "=r"(d[28]), "=r"(d[29]), "=r"(d[30]), "=r"(d[31])
-                     : "r"(tmem + ((uint32_t) (32 * quad) << 16) + 64u * stage + (uint32_t) (32 * half)));
+                     : "r"(tmem + ((uint32_t) (32 * quad) << 16) + (uint32_t) (32 * half)));
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
         if (lane < 16)
 #pragma unroll
             for (int n = 0; n < 32; n++) acc[n] += (double) __uint_as_float(d[n]);
     };
 
-    // two-stage pipeline: the MMAs of tile t run while tile t + 1 is loaded and the
-    // products of tile t - 1 are drained; a stage is refilled only after its MMAs were waited on
-    if (nt > 0)
+    constexpr int PA[6] = {2, 0, 1, 1, 0, 0}, PB[6] = {0, 2, 1, 0, 1, 0};
+    if (nt > 0) load_tile(0);
+    for (int t = 0; t < nt; t++)
     {
-        load_tile(0);
-        store_tile(0);
-        issue(0);
-        if (nt > 1) load_tile(1);
-        for (int t = 1; t < nt && ok; t++)
+        if (t > 0) drain();
+        if (!ok) break;
+        store_tile();
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        if (tid == 0)
         {
-            const int st = t & 1;
-            store_tile(st);                     // stage st was drained at iteration t - 1 (tile t - 2)
-            issue(st);
-            if (t + 1 < nt) load_tile(t + 1);
-            drain(st ^ 1);                      // tile t - 1
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+            for (int ks = 0; ks < 4; ks++)          // K-steps of 16
+#pragma unroll
+                for (int p = 0; p < 6; p++)
+                {
+                    // pass 0: A K-major (32-byte step along a row); pass 1: A MN-major
+                    // (16 rows = two 8-row swizzle atoms per step); B MN-major in both
+                    const uint64_t ad = MODE == 0 ? umma_desc(a_s + PA[p] * 8192 + ks * 32, 16, 1024, 2)
+                                                  : umma_desc(a_s + PA[p] * 8192 + ks * 2048, 8192, 1024, 2);
+                    umma_f16(tmem, ad, umma_desc(b_s + PB[p] * 8192 + ks * 2048, 8192, 1024, 2), IDESC,
+                             (ks == 0 && p == 0) ? 0u : 1u);
+                }
+            umma_commit(mbar);
         }
-        if (ok) drain((nt - 1) & 1);
+        if (t + 1 < nt) load_tile(t + 1);
     }
+    if (ok && nt > 0) drain();
     // the unit's outputs, written once
     __syncthreads();
     if (ok && lane < 16)
@@ -2542,20 +2527,12 @@ __global__ void __launch_bounds__(kWideThreads, 1) k_blk_wide(const BlkTask* __r
             for (int n = 0; n < 32; n++) o[n] = acc[n];
         }
     }
-    // a failed wait may leave MMAs in flight: wait (bounded) for both stages before the
-    // accumulators are released
-    if (!ok && tid == 0)
-        for (int stg = 0; stg < 2; stg++)
-        {
-            int it = 0;
-            while (!mbar_try_wait(smem_u32(&sm.mbar[stg]), phase[stg]) && ++it < (1 << 22)) {}
-        }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0)
     {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 128;" ::"r"(tmem) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 64;" ::"r"(tmem) : "memory");
     }
 }
 
