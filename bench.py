@@ -54,7 +54,7 @@ def parse():
     p.add_argument("--no-tune", action="store_true", help="keep the default panel width and JIT variant")
     p.add_argument("--check-rows", type=int, default=10_000)
     p.add_argument("--workload", default="jit_matern",
-                   choices=["jit_matern", "aot_coulomb", "aot_rpy", "batched", "served"],
+                   choices=["jit_matern", "aot_coulomb", "aot_rpy", "batched", "served", "peaks"],
                    help="jit_matern: the headline configuration; the others print extra lines for the "
                         "other configurations (AOT Coulomb matvec, AOT RPY matmul, batched matrices, "
                         "served requests)")
@@ -294,7 +294,11 @@ def run_ours(args):
     flop_per_pair = 13 + 4 * nv      # Matern32_3D_krnl_bimv_flop = 17 per pair for one RHS, 4 of them the bi-matvec
     far_flops = st["jit_pairs_B"] * flop_per_pair
     far_ms = phase[1]
-    peak_fp32 = 148 * 128 * 2 * 1.965e9 / 1e12
+    peaks = measured_peaks(local)
+    peak_fp32 = peaks["fp32_tflops"]
+    # MUFU: a Matern-3/2 value costs one rsqrt and one ex2; both directions of an unordered
+    # far-field pair are evaluated (owner computes)
+    mufu_rate = st["jit_pairs_B"] * 4 / (far_ms * 1e-3) / 1e12
     # DRAM traffic of one far-field launch from an ncu capture of the N = 125,000 case of
     # this workload (dram__bytes_read.sum + dram__bytes_write.sum = 28.1 MB: source panels,
     # tile records, coordinates, outputs), scaled by N (the traffic is proportional to the
@@ -304,8 +308,14 @@ def run_ours(args):
                 "achieved": far_flops / (far_ms * 1e-3) / 1e12, "peak": peak_fp32, "unit": "TFLOP/s",
                 "frac": far_flops / (far_ms * 1e-3) / 1e12 / peak_fp32, "traffic": traffic,
                 "traffic_source": "ncu capture of the N=125000 far-field launch, scaled by N",
-                "peak_source": "nominal FP32 FMA peak 148 SM x 128 lanes x 2 x 1.965 GHz (no measured FP32 figure)",
-                "flop_model": f"unordered point pairs x ({flop_per_pair}) = H2Pack JIT_flops model with 16 RHS"}
+                "peak_source": "measured on this GPU by h2gpu_measure_peaks (packed FP32x2 FMA chains on every SM); "
+                               f"nominal 148 SM x 128 lanes x 2 x 1.965 GHz = 74.4 TFLOP/s, frac of nominal "
+                               f"{far_flops / (far_ms * 1e-3) / 1e12 / 74.4:.3f}",
+                "flop_model": f"unordered point pairs x ({flop_per_pair}) = H2Pack JIT_flops model with 16 RHS",
+                "mufu": {"achieved": mufu_rate, "peak": peaks["mufu_tops"], "unit": "10^12 ops/s",
+                         "frac": mufu_rate / peaks["mufu_tops"],
+                         "model": "4 MUFU ops (rsqrt, ex2 per value, both directions) per unordered far-field pair; "
+                                  "peak measured by h2gpu_measure_peaks (ex2.approx chains)"}}
 
     cpu, parity = None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -338,6 +348,29 @@ def run_ours(args):
     H.close()
     if pg is not None:
         pg.destroy_process_group()
+
+
+def measured_peaks(device=0):
+    """FP32 FMA and MUFU throughput of this GPU, measured by the library's micro-benchmark."""
+    import ctypes as C
+    from h2pack_b200 import _abi
+    lib = _abi.libh2gpu()
+    f, m = C.c_double(), C.c_double()
+    _abi.check(lib.h2gpu_measure_peaks(int(device), C.byref(f), C.byref(m)), lib, "h2gpu_measure_peaks")
+    return {"fp32_tflops": f.value, "mufu_tops": m.value}
+
+
+def run_peaks(args):
+    """Measured pipe peaks (the denominators of the JIT roofline) with the clocks seen."""
+    import torch
+    torch.cuda.init()
+    with ClockSampler(0) as clk:
+        p = [measured_peaks(0) for _ in range(3)]
+    line = {"metric": "pipe peaks", "fp32_tflops": max(x["fp32_tflops"] for x in p),
+            "mufu_tops": max(x["mufu_tops"] for x in p), "runs": p,
+            "nominal": {"fp32_tflops": 148 * 128 * 2 * 1.965e9 / 1e12, "mufu_tops": 148 * 16 * 1.965e9 / 1e12},
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
 
 
 def rel2(a, b):
@@ -803,6 +836,8 @@ def main():
         run_batched(args)
     elif args.workload == "served":
         run_served(args)
+    elif args.workload == "peaks":
+        run_peaks(args)
     else:
         run_ours(args)
 

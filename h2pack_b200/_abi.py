@@ -104,6 +104,7 @@ H2GPU_SYMBOLS = {
     "h2gpu_image_bytes": (C.c_size_t, [C.c_void_p]),
     "h2gpu_plan_check": (C.c_int, [C.POINTER(Desc), C.POINTER(C.c_longlong)]),
     "h2gpu_batch_plan_check": (C.c_int, [C.POINTER(Desc), C.c_int, C.POINTER(C.c_longlong)]),
+    "h2gpu_measure_peaks": (C.c_int, [C.c_int, _dp, _dp]),
     "h2gpu_direct_sum": (C.c_int, [C.c_int, _dp, C.c_int, C.c_int, C.c_int, _dp, C.c_int, _dp, _dp, C.c_int, _dp]),
 }
 

@@ -2152,6 +2152,49 @@ H2G_API size_t h2gpu_image_bytes(const h2gpu_image* im)
     return im ? im->bytes + im->work_bytes + 8 * im->io_elems : 0;
 }
 
+H2G_API int h2gpu_measure_peaks(int device, double* fp32_tflops, double* mufu_tops)
+{
+    if (!fp32_tflops || !mufu_tops) return fail(H2GPU_ERR_INVALID, "NULL output");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(H2GPU_ERR_CUDA, "no CUDA device available");
+    if (device < 0) CK(cudaGetDevice(&device));
+    CK(cudaSetDevice(device));
+    int sms = 0;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    float* out = nullptr;
+    CK(cudaMalloc(&out, sizeof(float) * 148 * 64));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    int st = H2GPU_OK;
+    const int blocks = sms * 8, iters = 1 << 14;
+    double res[2] = {0, 0};
+    for (int which = 0; which < 2 && st == H2GPU_OK; which++)
+    {
+        float best = 1e30f;
+        for (int rep = 0; rep < 4 && st == H2GPU_OK; rep++)      // first one warms up
+        {
+            cudaEventRecord(e0, 0);
+            cudaError_t e = launch_peak(which, blocks, iters, out, 0);
+            cudaEventRecord(e1, 0);
+            if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+            if (e != cudaSuccess) { st = fail(H2GPU_ERR_CUDA, "peak kernel: %s", cudaGetErrorString(e)); break; }
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (rep > 0) best = std::min(best, ms);
+        }
+        const double ops = (double) blocks * 256 * iters * 8;      // chain steps
+        res[which] = which == 0 ? ops * 4 / (best * 1e-3) / 1e12   // FFMA2: 2 FMA = 4 flop
+                                : ops / (best * 1e-3) / 1e12;      // ex2 operations
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(out);
+    *fp32_tflops = res[0];
+    *mufu_tops = res[1];
+    return st;
+}
+
 H2G_API int h2gpu_direct_sum(int kernel_id, const double* krnl_param, int n_krnl_param, int xpt_dim, int krnl_dim,
                              const double* src_coord, int n_src, const double* src_val, const double* trg_coord,
                              int n_trg, double* trg_val)

@@ -2778,6 +2778,47 @@ __global__ void __launch_bounds__(kGenThreads) k_gen(const GenTask* __restrict__
     }
 }
 
+// ------------------------------------------------ measured pipe peaks (roofline)
+
+// FP32 FMA pipe: 8 independent packed FP32x2 FMA chains per thread (16 FMAs per
+// iteration step, 32 flop), so the pipe, not a dependency, bounds the rate.
+__global__ void __launch_bounds__(256) k_peak_ffma2(int iters, float seed, float* __restrict__ out)
+{
+    float2 a[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) a[k] = make_float2(seed + k + threadIdx.x, seed - k);
+    const float2 m = make_float2(0.999999f, 1.000001f), c = make_float2(1e-7f, -1e-7f);
+    for (int i = 0; i < iters; i++)
+#pragma unroll
+        for (int k = 0; k < 8; k++) a[k] = __ffma2_rn(a[k], m, c);
+    float s = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; k++) s += a[k].x + a[k].y;
+    if (s == 1234.5f) out[blockIdx.x] = s;   // keeps the chains live
+}
+
+// MUFU pipe: 8 independent ex2.approx chains per thread (the FP32 path's exponential).
+__global__ void __launch_bounds__(256) k_peak_mufu(int iters, float seed, float* __restrict__ out)
+{
+    float a[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) a[k] = -1e-3f * (seed + k + (threadIdx.x & 7));
+    for (int i = 0; i < iters; i++)
+#pragma unroll
+        for (int k = 0; k < 8; k++) a[k] = -ex2_approx(a[k]);
+    float s = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; k++) s += a[k];
+    if (s == 1234.5f) out[blockIdx.x] = s;
+}
+
+cudaError_t launch_peak(int which, int blocks, int iters, float* out, cudaStream_t st)
+{
+    if (which == 0) k_peak_ffma2<<<blocks, 256, 0, st>>>(iters, 1.0f, out);
+    else k_peak_mufu<<<blocks, 256, 0, st>>>(iters, 1.0f, out);
+    return cudaGetLastError();
+}
+
 // ------------------------------------------------------------- launchers
 
 static inline unsigned grid_for(long long n, int threads)

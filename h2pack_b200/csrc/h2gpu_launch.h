@@ -45,6 +45,8 @@ cudaError_t launch_pair(int kid, int NV, const PairOwner* ow, int n, const PairP
 // stored-block generation: tasks [0, n) into arena (double or float, per fp32)
 cudaError_t launch_gen(int kid, int kd, int fp32, const GenTask* t, int n, const double4* pts, KParam kp, void* arena,
                        cudaStream_t st);
+// pipe peak micro-benchmarks: which 0 = FP32 FMA (packed FP32x2), 1 = MUFU ex2
+cudaError_t launch_peak(int which, int blocks, int iters, float* out, cudaStream_t st);
 cudaError_t launch_direct(int kid, const double4* trg, int n_trg, const double4* src, int n_src, const double* val,
                           KParam kp, double* out, cudaStream_t st);
 

@@ -345,6 +345,13 @@ int h2gpu_plan_check(const h2gpu_desc *desc, long long *counts);
 int h2gpu_batch_plan_check(const h2gpu_desc *descs, int n_desc, long long *counts);
 
 /*
+ * Measured pipe peaks of a device (-1: the current one), the denominators of the JIT
+ * kernels' roofline: FP32 FMA throughput (TFLOP/s, packed FP32x2 FMA chains on every SM)
+ * and MUFU throughput (10^12 ex2.approx operations/s).  No counterpart in the reference.
+ */
+int h2gpu_measure_peaks(int device, double *fp32_tflops, double *mufu_tops);
+
+/*
  * FP64 direct sum on the device: y_t = sum_s K(x_t, x_s) v_s for n_trg targets
  * and n_src sources (coordinates xpt_dim x n, ld = n, host arrays; values are
  * krnl_dim-interleaved per point as in the H2 vectors).
