@@ -2596,7 +2596,7 @@ H2G_API int h2gpu_autotune(h2gpu_image* im, int n_vec, const double* dX, int ldx
             if (nv < 32 && (var == H2GPU_JIT_PAIR || var == H2GPU_BLK_TCGEN05) && nv != 8 && nv != 16) continue;
             // the tensor-core kernels exist for panels of 8 and 16; narrower panels run
             // the CUDA-core kernel whatever the variant, so time that once
-            if (var == H2GPU_JIT_TC && nv != 8 && nv != 16 && vars.size() > 1) continue;
+            if (nv < 32 && var == H2GPU_JIT_TC && nv != 8 && nv != 16 && vars.size() > 1) continue;
             set_variant(im, var);
             TRY(prepare(im, nv));
             float ms = 0;

@@ -2390,7 +2390,7 @@ constexpr int kWideThreads = 256;
 
 template <int MODE>
 __global__ void __launch_bounds__(kWideThreads, 2) k_blk_wide(const BlkTask* __restrict__ tasks,
-                                                              const WideUnit* __restrict__ units,
+                                                              const WideUnit* __restrict__ units, int n_units,
                                                               const float* __restrict__ arena,
                                                               const double* __restrict__ XS, double* __restrict__ PS,
                                                               int* __restrict__ status)
@@ -2400,13 +2400,7 @@ __global__ void __launch_bounds__(kWideThreads, 2) k_blk_wide(const BlkTask* __r
     constexpr uint32_t IDESC = umma_idesc_bf16_ab(NV, MODE == 1 ? 1 : 0, 1);
     extern __shared__ __align__(1024) unsigned char wide_raw[];
     WideSmem& sm = *reinterpret_cast<WideSmem*>(wide_raw + ((1024 - (smem_u32(wide_raw) & 1023)) & 1023));
-    const WideUnit U = units[blockIdx.x];
-    const BlkTask T = tasks[U.task];
-    const int ncol = T.ncol, nrow = T.nrow;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    // the unit's fixed 64-row chunk (pass 0) or 64-column tile (pass 1), and the tiles it walks
-    const int nt = MODE == 0 ? (ncol + 63) / 64 : (nrow + 63) / 64;
-    const float* A0 = arena + T.a_off;
 
     if (warp == 0)
     {
@@ -2418,7 +2412,6 @@ __global__ void __launch_bounds__(kWideThreads, 2) k_blk_wide(const BlkTask* __r
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&sm.mbar)) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    for (int i = tid; i < 64 * 65; i += kWideThreads) (&sm.acc[0][0])[i] = 0.0;
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -2426,6 +2419,17 @@ __global__ void __launch_bounds__(kWideThreads, 2) k_blk_wide(const BlkTask* __r
     unsigned char* const a_b = reinterpret_cast<unsigned char*>(sm.a);
     unsigned char* const b_b = reinterpret_cast<unsigned char*>(sm.b);
     const uint32_t a_s = smem_u32(sm.a), b_s = smem_u32(sm.b);
+    bool ok = true;
+    uint32_t phase = 0;
+    // persistent: the CTA takes units blockIdx.x, + gridDim.x, ...
+    for (int ui = blockIdx.x; ui < n_units && ok; ui += gridDim.x)
+    {
+    const WideUnit U = units[ui];
+    const BlkTask T = tasks[U.task];
+    const int ncol = T.ncol, nrow = T.nrow;
+    // the unit's fixed 64-row chunk (pass 0) or 64-column tile (pass 1), and the tiles it walks
+    const int nt = MODE == 0 ? (ncol + 63) / 64 : (nrow + 63) / 64;
+    const float* A0 = arena + T.a_off;
 
     // tile t: rows [rc, rc + R) and columns [c0, c0 + C) of the block task, and the 64 rows
     // of right-hand sides that meet it (V rows in0 + c0 + k, or W rows in1 + rc + k)
@@ -2487,14 +2491,12 @@ __global__ void __launch_bounds__(kWideThreads, 2) k_blk_wide(const BlkTask* __r
         }
     };
 
-    bool ok = true;
-    uint32_t phase = 0;
     // warp w reads TMEM lane quadrant w % 4 (rows 16 (w % 4) + lane, lane < 16) and the 32
     // accumulator columns 32 (w / 4) .. + 31
     const int quad = warp & 3, half = warp >> 2;
     double* const acc = sm.acc[(16 * quad + lane) & 63] + 32 * half;
     // add the tile's FP32 products (TMEM) into the unit's FP64 sums
-    auto drain = [&]() {
+    auto drain = [&](bool first) {
         int good = 1;
         if (tid == 0)
         {
@@ -2517,15 +2519,21 @@ __global__ void __launch_bounds__(kWideThreads, 2) k_blk_wide(const BlkTask* __r
                      : "r"(tmem + ((uint32_t) (32 * quad) << 16) + (uint32_t) (32 * half)));
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
         if (lane < 16)
+        {
+            if (first)
 #pragma unroll
-            for (int n = 0; n < 32; n++) acc[n] += (double) __uint_as_float(d[n]);
+                for (int n = 0; n < 32; n++) acc[n] = (double) __uint_as_float(d[n]);
+            else
+#pragma unroll
+                for (int n = 0; n < 32; n++) acc[n] += (double) __uint_as_float(d[n]);
+        }
     };
 
     constexpr int PA[6] = {2, 0, 1, 1, 0, 0}, PB[6] = {0, 2, 1, 0, 1, 0};
     if (nt > 0) load_tile(0);
     for (int t = 0; t < nt; t++)
     {
-        if (t > 0) drain();
+        if (t > 0) drain(t == 1);
         if (!ok) break;
         store_tile();
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -2550,9 +2558,8 @@ __global__ void __launch_bounds__(kWideThreads, 2) k_blk_wide(const BlkTask* __r
         }
         if (t + 1 < nt) load_tile(t + 1);
     }
-    if (ok && nt > 0) drain();
-    // the unit's outputs, written once
-    __syncthreads();
+    if (ok && nt > 0) drain(nt == 1);
+    // the unit's outputs, written once (each thread writes the sums it added)
     if (ok && lane < 16)
     {
         const int m = 16 * quad + lane;
@@ -2564,6 +2571,7 @@ __global__ void __launch_bounds__(kWideThreads, 2) k_blk_wide(const BlkTask* __r
             for (int n = 0; n < 32; n++) o[n] = acc[n];
         }
     }
+    }   // units
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0)
@@ -3012,15 +3020,19 @@ cudaError_t launch_blk_wide(int mode, const BlkTask* t, const WideUnit* u, int n
     if (n <= 0) return cudaSuccess;
     if (!status) return cudaErrorInvalidValue;
     constexpr int b = wide_smem_bytes();
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int g = n < 2 * sms ? n : 2 * sms;   // persistent: two CTAs per SM walk the units
     if (mode == 0)
     {
         cudaError_t e = allow_smem(k_blk_wide<0>, b);
         if (e != cudaSuccess) return e;
-        k_blk_wide<0><<<n, kWideThreads, b, st>>>(t, u, arena, XS, PS, status);
+        k_blk_wide<0><<<g, kWideThreads, b, st>>>(t, u, n, arena, XS, PS, status);
     } else {
         cudaError_t e = allow_smem(k_blk_wide<1>, b);
         if (e != cudaSuccess) return e;
-        k_blk_wide<1><<<n, kWideThreads, b, st>>>(t, u, arena, XS, PS, status);
+        k_blk_wide<1><<<g, kWideThreads, b, st>>>(t, u, n, arena, XS, PS, status);
     }
     return cudaGetLastError();
 }
