@@ -172,7 +172,6 @@ struct h2gpu_image {
     // tuning (h2gpu_autotune) and captured graph (h2gpu_graph_capture)
     int jit_tc = 1;          // tensor-core JIT kernel for FP32 panels of 8 / 16
     int jit_pair = 0;        // with jit_tc: the pair kernel (each unordered pair once)
-    int jit_soft = 0;        // with jit_tc: far-field exponentials partly on the FMA pipe
     int blk_tc = 1;          // stored-block kernel for FP32 panels of 8 / 16: 1 mma.sync, 2 tcgen05, 0 CUDA cores
     int* d_status = nullptr; // device status word (bounded waits of the tcgen05 kernel)
     int* h_status = nullptr; // pinned host copy, read back at the end of every timed panel
@@ -1698,8 +1697,7 @@ int run_panel(h2gpu_image* im, int NV, int nv, const double* X, long long x_rs, 
         const bool panels = f32 && panels_used(im, NV);
         if (panels) CK(launch_panel_in(NV, im->d_pg, im->n_pg_pts, im->n_pg - im->n_pg_pts, im->d_XS, im->d_pin, s));
         CK(launch_jit(im->kernel_id, f32, NV, im->d_jtF, im->n_jtF, im->d_js, f32 ? (const void*) im->d_pts32 : (const void*) im->d_pts64,
-                      kparam_of(im), f32 ? 1 : 0, (im->jit_tc && im->jit_soft) ? 3 : im->jit_tc, im->d_XS, im->d_PS,
-                      im->d_Y1, s, 1, im->d_ppts, im->d_pin, im->d_tiles));
+                      kparam_of(im), f32 ? 1 : 0, im->jit_tc, im->d_XS, im->d_PS, im->d_Y1, s, 1, im->d_ppts, im->d_pin, im->d_tiles));
         im->st.n_launches += panels ? 1 : 0;
     }
     if (timed) CK(cudaEventRecord(e[4], s));
@@ -1912,8 +1910,6 @@ H2G_API int h2gpu_image_create(const h2gpu_desc* desc, const h2gpu_options* opt,
         im->jit_pair = (e && e[0] == '1');
         e = getenv("H2G_BLK_TC");
         im->blk_tc = !(e && e[0] == '0');
-        e = getenv("H2G_JIT_SOFT");
-        im->jit_soft = (e && e[0] == '1');
     }
     HostPlan hp;
     GenPlan gp;

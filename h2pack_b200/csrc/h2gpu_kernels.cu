@@ -743,31 +743,8 @@ template <> struct ScalarF2<KRNL_MATERN32_ID> {
     }
 };
 
-// 2^t for two values on the FMA pipe instead of the MUFU pipe: t = n + f with n the
-// nearest integer (added to the exponent bits) and 2^f, |f| <= 1/2, by a degree-5
-// polynomial fitted here to the relative error of 2^f on [-1/2, 1/2] (least squares with
-// Lawson reweighting; max relative error 2.3e-7 in FP32 Horner form, the accuracy of
-// ex2.approx).  t is clamped at -125 (2^-125 is negligible next to every kept value).
-__device__ __forceinline__ float2 ex2_soft2(float2 t)
-{
-    t = make_float2(fmaxf(t.x, -125.f), fmaxf(t.y, -125.f));
-    const float2 tm = __fadd2_rn(t, make_float2(12582912.f, 12582912.f));    // 1.5 * 2^23: rounds t
-    const float2 n = __fadd2_rn(tm, make_float2(-12582912.f, -12582912.f));
-    const float2 f = __ffma2_rn(n, make_float2(-1.f, -1.f), t);              // t - n, exact
-    float2 p = make_float2(0.001327647129073739f, 0.001327647129073739f);
-    p = __ffma2_rn(p, f, make_float2(0.009675540961325169f, 0.009675540961325169f));
-    p = __ffma2_rn(p, f, make_float2(0.05550713092088699f, 0.05550713092088699f));
-    p = __ffma2_rn(p, f, make_float2(0.24022120237350464f, 0.24022120237350464f));
-    p = __ffma2_rn(p, f, make_float2(0.6931469440460205f, 0.6931469440460205f));
-    p = __ffma2_rn(p, f, make_float2(1.0000001192092896f, 1.0000001192092896f));
-    // the low bits of tm hold n (two's complement); << 23 moves it into the exponent field
-    return make_float2(__int_as_float(__float_as_int(p.x) + (__float_as_int(tm.x) << 23)),
-                       __int_as_float(__float_as_int(p.y) + (__float_as_int(tm.y) << 23)));
-}
-
 // FP32 kernel values for admissible (well-separated) pairs only: r2 > 0 always, so the
 // coincident-point cases drop out; constants are folded once per launch (prep).
-// f2s: f2 with the exponential on the FMA pipe (ex2_soft2), where the kernel has one.
 template <int KID> struct ScalarFar;
 // f2: the same for two values at once with packed FP32x2 arithmetic (sm_100).
 template <> struct ScalarFar<KRNL_COULOMB_ID> {
@@ -777,7 +754,6 @@ template <> struct ScalarFar<KRNL_COULOMB_ID> {
     {
         return make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
     }
-    static __device__ __forceinline__ float2 f2s(float2 r2, float q0, float q1) { return f2(r2, q0, q1); }
 };
 template <> struct ScalarFar<KRNL_GAUSSIAN_ID> {
     static __device__ __forceinline__ void prep(float p0, float, float& q0, float& q1) { q0 = -p0 * kLog2e; q1 = 0.f; }
@@ -786,10 +762,6 @@ template <> struct ScalarFar<KRNL_GAUSSIAN_ID> {
     {
         const float2 t = __fmul2_rn(r2, make_float2(q0, q0));
         return make_float2(ex2_approx(t.x), ex2_approx(t.y));
-    }
-    static __device__ __forceinline__ float2 f2s(float2 r2, float q0, float)
-    {
-        return ex2_soft2(__fmul2_rn(r2, make_float2(q0, q0)));
     }
 };
 template <> struct ScalarFar<KRNL_MATERN32_ID> {
@@ -805,12 +777,6 @@ template <> struct ScalarFar<KRNL_MATERN32_ID> {
         const float2 r = __fmul2_rn(r2, make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y)));
         const float2 t = __fmul2_rn(r, make_float2(q1, q1));
         const float2 e = make_float2(ex2_approx(t.x), ex2_approx(t.y));
-        return __ffma2_rn(__fmul2_rn(r, make_float2(-q0, -q0)), e, e);
-    }
-    static __device__ __forceinline__ float2 f2s(float2 r2, float q0, float q1)
-    {
-        const float2 r = __fmul2_rn(r2, make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y)));
-        const float2 e = ex2_soft2(__fmul2_rn(r, make_float2(q1, q1)));
         return __ffma2_rn(__fmul2_rn(r, make_float2(-q0, -q0)), e, e);
     }
 };
@@ -1173,9 +1139,7 @@ struct JitTcSmem {
 // cancellation stays at a few FP32 ulps of r^2 (the near field keeps differences).
 // Warps whose 16 target rows are all past the end of the chunk only take part in the
 // barriers.
-// SOFT (FAR only): the second target's exponentials on the FMA pipe (ScalarFar::f2s), which
-// moves a quarter of the MUFU work to the FP32 pipe.
-template <int KID, int NV, bool FAR, bool SOFT = false>
+template <int KID, int NV, bool FAR>
 __global__ void __launch_bounds__(256, 4) k_jit_tc(const JitTarget* __restrict__ tgts, const TileRec* __restrict__ tiles,
                                                    const float4* __restrict__ pts, const float4* __restrict__ ppts,
                                                    const uint4* __restrict__ pin, KParam kp, double* __restrict__ PS,
@@ -1284,8 +1248,7 @@ __global__ void __launch_bounds__(256, 4) k_jit_tc(const JitTarget* __restrict__
                             return __ffma2_rn(mx, px, t);
                         };
                         const float2 k0 = ScalarFar<KID>::f2(r2p(sa22, max2, may2, maz2), q0, q1);
-                        const float2 k1 = SOFT ? ScalarFar<KID>::f2s(r2p(sb22, mbx2, mby2, mbz2), q0, q1)
-                                               : ScalarFar<KID>::f2(r2p(sb22, mbx2, mby2, mbz2), q0, q1);
+                        const float2 k1 = ScalarFar<KID>::f2(r2p(sb22, mbx2, mby2, mbz2), q0, q1);
                         mma_group(k0, k1, buf, grp);
                     }
                 } else {
@@ -3101,12 +3064,8 @@ static cudaError_t launch_jit_k(int NV, const JitTarget* tg, int n, const JitSou
             constexpr int b = jit_tc_smem_bytes();
             // the dynamic shared-memory opt-in is a per-device function attribute (cheap,
             // and legal inside a stream capture), so it is set at every launch
-            // use_tc == 3: the far-field kernel with part of the exponentials on the FMA pipe
-            const bool soft = use_tc == 3 && far;
-            auto kern = NV == 16 ? (far ? (soft ? k_jit_tc<KID, 16, true, true> : k_jit_tc<KID, 16, true>)
-                                        : k_jit_tc<KID, 16, false>)
-                                 : (far ? (soft ? k_jit_tc<KID, 8, true, true> : k_jit_tc<KID, 8, true>)
-                                        : k_jit_tc<KID, 8, false>);
+            auto kern = NV == 16 ? (far ? k_jit_tc<KID, 16, true> : k_jit_tc<KID, 16, false>)
+                                 : (far ? k_jit_tc<KID, 8, true> : k_jit_tc<KID, 8, false>);
             cudaError_t e = allow_smem(kern, b);
             if (e != cudaSuccess) return e;
             kern<<<n, 256, b, st>>>(tg, tiles, p4, ppts, pin, kp, PS, Y1);
