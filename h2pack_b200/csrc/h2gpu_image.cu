@@ -518,15 +518,24 @@ int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
         for (int n = 0; n < n_node; n++) has_y1[n] = !y1s[n].empty();
         // units of the 64-wide passes: pass 0 per 64-row chunk of a task (A V), pass 1 per
         // 64-column tile of a task (A^T W)
+        // Pass-0 units are ordered by their input rows (the column node's y0 / x slice),
+        // so that consecutive units, walked by the persistent CTAs in order, read the same
+        // 64-wide input rows from L2; pass-1 units read their task's own rows and keep the
+        // task order (tasks of one row node are adjacent).
         auto units = [&](const std::vector<BlkTask>& ts, int pass) {
-            int cnt = 0;
+            std::vector<WideUnit> us;
             for (int i = 0; i < (int) ts.size(); i++)
             {
                 const BlkTask& t = ts[i];
                 if ((pass == 0 ? t.out0_row : t.out1_row) < 0) continue;
-                for (int o = 0; o < (pass == 0 ? t.nrow : t.ncol); o += 64) { hp.wide.push_back(WideUnit{i, o}); cnt++; }
+                for (int o = 0; o < (pass == 0 ? t.nrow : t.ncol); o += 64) us.push_back(WideUnit{i, o});
             }
-            return cnt;
+            if (pass == 0)
+                std::stable_sort(us.begin(), us.end(), [&](const WideUnit& a, const WideUnit& b) {
+                    return ts[a.task].in0_row < ts[b.task].in0_row;
+                });
+            hp.wide.insert(hp.wide.end(), us.begin(), us.end());
+            return (int) us.size();
         };
         im->n_wide[0] = units(blkB, 0);
         im->n_wide[1] = units(blkB, 1);
