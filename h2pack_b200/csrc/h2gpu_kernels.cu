@@ -2364,7 +2364,6 @@ __global__ void __launch_bounds__(kWideThreads, 2) k_blk_wide(const BlkTask* __r
     extern __shared__ __align__(1024) unsigned char wide_raw[];
     WideSmem& sm = *reinterpret_cast<WideSmem*>(wide_raw + ((1024 - (smem_u32(wide_raw) & 1023)) & 1023));
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    if ((int) blockIdx.x >= n_units) return;
 
     if (warp == 0)
     {
@@ -2383,23 +2382,32 @@ __global__ void __launch_bounds__(kWideThreads, 2) k_blk_wide(const BlkTask* __r
     unsigned char* const a_b = reinterpret_cast<unsigned char*>(sm.a);
     unsigned char* const b_b = reinterpret_cast<unsigned char*>(sm.b);
     const uint32_t a_s = smem_u32(sm.a), b_s = smem_u32(sm.b);
+    bool ok = true;
+    uint32_t phase = 0;
+    // persistent: the CTA takes units blockIdx.x, + gridDim.x, ...
+    for (int ui = blockIdx.x; ui < n_units && ok; ui += gridDim.x)
+    {
+    const WideUnit U = units[ui];
+    const BlkTask T = tasks[U.task];
+    const int ncol = T.ncol, nrow = T.nrow;
+    // the unit's fixed 64-row chunk (pass 0) or 64-column tile (pass 1), and the tiles it walks
+    const int nt = MODE == 0 ? (ncol + 63) / 64 : (nrow + 63) / 64;
+    const float* A0 = arena + T.a_off;
 
-    // The CTA walks the units blockIdx.x, + gridDim.x, ... tile by tile as one stream of
-    // steps, so the next step's tile (possibly the next unit's first) is loaded while the
-    // current one is multiplied.
-    auto tiles_of = [&](int ui) {
-        const BlkTask& T = tasks[units[ui].task];
-        return MODE == 0 ? (T.ncol + 63) / 64 : (T.nrow + 63) / 64;
+    // tile t: rows [rc, rc + R) and columns [c0, c0 + C) of the block task, and the 64 rows
+    // of right-hand sides that meet it (V rows in0 + c0 + k, or W rows in1 + rc + k)
+    auto tile_of = [&](int t, int& rc, int& c0) {
+        if (MODE == 0) { rc = U.off; c0 = 64 * t; }
+        else { rc = 64 * t; c0 = U.off; }
     };
     // registers of the tile being loaded: thread t holds 2 granules (row r, 8 consecutive
     // columns q) of A and 2 granules (row k, 8 consecutive right-hand sides) of the inputs
     float ra[2][8], rb[2][8];
-    auto load_tile = [&](int ui, int t) {
-        const WideUnit U = units[ui];
-        const BlkTask T = tasks[U.task];
-        const int rc = MODE == 0 ? U.off : 64 * t, c0 = MODE == 0 ? 64 * t : U.off;
-        const int R = min(64, T.nrow - rc), C = min(64, T.ncol - c0);
-        const float* A = arena + T.a_off + (long long) rc * T.ncol + c0;
+    auto load_tile = [&](int t) {
+        int rc, c0;
+        tile_of(t, rc, c0);
+        const int R = min(64, nrow - rc), C = min(64, ncol - c0);
+        const float* A = A0 + (long long) rc * ncol + c0;
         const int nk = MODE == 0 ? C : R;
         const double* B = XS + (long long) (MODE == 0 ? T.in0_row + c0 : T.in1_row + rc) * NV;
 #pragma unroll
@@ -2410,7 +2418,7 @@ __global__ void __launch_bounds__(kWideThreads, 2) k_blk_wide(const BlkTask* __r
             for (int j = 0; j < 8; j++)
             {
                 const int c = 8 * q + j;
-                ra[u][j] = (r < R && c < C) ? A[(long long) r * T.ncol + c] : 0.f;
+                ra[u][j] = (r < R && c < C) ? A[(long long) r * ncol + c] : 0.f;
             }
             if (r < nk)
             {
@@ -2446,14 +2454,11 @@ __global__ void __launch_bounds__(kWideThreads, 2) k_blk_wide(const BlkTask* __r
         }
     };
 
-    bool ok = true;
-    uint32_t phase = 0;
     // warp w reads TMEM lane quadrant w % 4 (rows 16 (w % 4) + lane, lane < 16) and the 32
     // accumulator columns 32 (w / 4) .. + 31
     const int quad = warp & 3, half = warp >> 2;
     double* const acc = sm.acc[(16 * quad + lane) & 63] + 32 * half;
-    // wait for the step's MMAs and add its FP32 products into the unit's FP64 sums (the
-    // unit's first tile initialises them)
+    // add the tile's FP32 products (TMEM) into the unit's FP64 sums
     auto drain = [&](bool first) {
         int good = 1;
         if (tid == 0)
@@ -2486,33 +2491,13 @@ __global__ void __launch_bounds__(kWideThreads, 2) k_blk_wide(const BlkTask* __r
                 for (int n = 0; n < 32; n++) acc[n] += (double) __uint_as_float(d[n]);
         }
     };
-    // the unit's 64 output rows, written once (each thread writes the sums it added)
-    auto write_unit = [&](int ui) {
-        if (lane >= 16) return;
-        const WideUnit U = units[ui];
-        const BlkTask T = tasks[U.task];
-        const int m = 16 * quad + lane;
-        const int lim = MODE == 0 ? min(64, T.nrow - U.off) : min(64, T.ncol - U.off);
-        if (m < lim)
-        {
-            double* o = PS + (long long) ((MODE == 0 ? T.out0_row : T.out1_row) + U.off + m) * NV + 32 * half;
-#pragma unroll 8
-            for (int n = 0; n < 32; n++) o[n] = acc[n];
-        }
-    };
 
     constexpr int PA[6] = {2, 0, 1, 1, 0, 0}, PB[6] = {0, 2, 1, 0, 1, 0};
-    int ui = blockIdx.x, t = 0, nt = tiles_of(ui);
-    int pui = -1, pt = 0, pnt = 0;             // the step whose MMAs are in flight
-    load_tile(ui, 0);
-    while (ok)
+    if (nt > 0) load_tile(0);
+    for (int t = 0; t < nt; t++)
     {
-        if (pui >= 0)
-        {
-            drain(pt == 0);
-            if (!ok) break;
-            if (pt + 1 == pnt) write_unit(pui);
-        }
+        if (t > 0) drain(t == 1);
+        if (!ok) break;
         store_tile();
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -2534,22 +2519,22 @@ __global__ void __launch_bounds__(kWideThreads, 2) k_blk_wide(const BlkTask* __r
                 }
             umma_commit(mbar);
         }
-        pui = ui; pt = t; pnt = nt;
-        // the next step: the unit's next tile, or the CTA's next unit
-        if (++t == nt)
-        {
-            ui += gridDim.x;
-            t = 0;
-            if (ui >= n_units) break;
-            nt = tiles_of(ui);
-        }
-        load_tile(ui, t);
+        if (t + 1 < nt) load_tile(t + 1);
     }
-    if (ok && pui >= 0)
+    if (ok && nt > 0) drain(nt == 1);
+    // the unit's outputs, written once (each thread writes the sums it added)
+    if (ok && lane < 16)
     {
-        drain(pt == 0);
-        if (ok) write_unit(pui);
+        const int m = 16 * quad + lane;
+        const int lim = MODE == 0 ? min(64, nrow - U.off) : min(64, ncol - U.off);
+        if (m < lim)
+        {
+            double* o = PS + (long long) ((MODE == 0 ? T.out0_row : T.out1_row) + U.off + m) * NV + 32 * half;
+#pragma unroll 8
+            for (int n = 0; n < 32; n++) o[n] = acc[n];
+        }
     }
+    }   // units
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0)
