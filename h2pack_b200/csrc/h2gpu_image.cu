@@ -147,6 +147,7 @@ struct h2gpu_image {
     double* d_PS = nullptr;
     double* d_Y1 = nullptr;
     double* d_PUSH = nullptr;
+    uint16_t* d_XS3 = nullptr;   // 64-wide panels of mixed stored-block images: XS split into BF16 pieces
     // host-API staging
     double* d_io = nullptr;
     size_t io_elems = 0;
@@ -192,7 +193,7 @@ void free_all(h2gpu_image* im)
                     im->d_B32, im->d_D64, im->d_D32, im->d_pts64, im->d_pts32, im->d_XS, im->d_PS, im->d_Y1,
                     im->d_PUSH, im->d_io, im->d_owN, im->d_owF, im->d_pp, im->d_jtN2, im->d_jtF2, im->d_y1t2,
                     im->d_y1_slots2, im->d_asm2, im->d_asm_slots2, im->d_status, im->d_pg, im->d_ppts,
-                    im->d_pin, im->d_tiles, im->d_wide};
+                    im->d_pin, im->d_tiles, im->d_wide, im->d_XS3};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (im->h_status) cudaFreeHost(im->h_status);
@@ -1556,6 +1557,7 @@ int ensure_work(h2gpu_image* im, int NV)
     if (im->NVb >= NV) return H2GPU_OK;
     for (double** p : {&im->d_XS, &im->d_PS, &im->d_Y1, &im->d_PUSH})
         if (*p) { cudaFree(*p); *p = nullptr; }
+    if (im->d_XS3) { cudaFree(im->d_XS3); im->d_XS3 = nullptr; }
     im->NVb = 0;          // no buffers until all four are allocated
     im->work_bytes = 0;
     size_t xs = ((size_t) im->N + im->y0_rows) * NV, ps = (size_t) im->ps_rows * NV, y1 = (size_t) im->y0_rows * NV;
@@ -1563,7 +1565,14 @@ int ensure_work(h2gpu_image* im, int NV)
     CK(cudaMalloc(&im->d_PS, 8 * std::max<size_t>(ps, 1)));
     CK(cudaMalloc(&im->d_Y1, 8 * std::max<size_t>(y1, 1)));
     CK(cudaMalloc(&im->d_PUSH, 8 * std::max<size_t>(y1, 1)));
-    im->work_bytes = 8 * (xs + ps + 2 * y1);
+    size_t xs3 = 0;
+    if (NV == 64 && !im->BD_JIT)
+    {
+        // the 64-wide block passes read their inputs as BF16 pieces (3 x 2 bytes per value)
+        xs3 = 3 * ((size_t) im->N + im->y0_rows) * 64;
+        CK(cudaMalloc(&im->d_XS3, 2 * xs3));
+    }
+    im->work_bytes = 8 * (xs + ps + 2 * y1) + 2 * xs3;
     im->NVb = NV;
     return H2GPU_OK;
 }
@@ -1657,21 +1666,23 @@ int run_panel(h2gpu_image* im, int NV, int nv, const double* X, long long x_rs, 
         im->st.n_launches += 9 + (long long) (im->up_beg.size() - 1) + (long long) (im->dn_beg.size() - 1);
         return H2GPU_OK;
     }
+    const bool wide = f32 && !im->BD_JIT && NV == 64;   // two GEMM passes per block list
+    const long long xs_rows = (long long) im->N + im->y0_rows;
     if (timed) CK(cudaEventRecord(e[0], s));
     CK(launch_gather(NV, X, x_rs, x_cs, nv, im->d_fwd, im->N, im->d_XS, s));
+    if (wide) CK(launch_split3(im->d_XS, 0, im->N, xs_rows, im->d_XS3, s));
     // D phase first: it needs only x (in the graph-free stream order it simply runs before the upward sweep)
     if (timed) CK(cudaEventRecord(e[1], s));
-    const bool wide = f32 && !im->BD_JIT && NV == 64;   // two GEMM passes per block list
     if (!im->BD_JIT)
     {
         if (wide)
         {
             const int* nw = im->n_wide;
-            CK(launch_blk_wide(0, im->d_blkD, im->d_wide + nw[0] + nw[1], nw[2], im->d_D32, im->d_XS, im->d_PS, s,
-                               im->d_status));
-            CK(launch_blk_wide(1, im->d_blkD, im->d_wide + nw[0] + nw[1] + nw[2], nw[3], im->d_D32, im->d_XS,
+            CK(launch_blk_wide(0, im->d_blkD, im->d_wide + nw[0] + nw[1], nw[2], im->d_D32, im->d_XS3, xs_rows,
                                im->d_PS, s, im->d_status));
-            im->st.n_launches += 1;
+            CK(launch_blk_wide(1, im->d_blkD, im->d_wide + nw[0] + nw[1] + nw[2], nw[3], im->d_D32, im->d_XS3,
+                               xs_rows, im->d_PS, s, im->d_status));
+            im->st.n_launches += 2;   // the second pass and the split of the inputs
         }
         else if (f32) CK(launch_blk<float>(NV, im->d_blkD, im->n_blkD, im->d_D32, im->d_XS, im->d_PS, s, im->blk_tc, im->d_status));
         else CK(launch_blk<double>(NV, im->d_blkD, im->n_blkD, im->d_D64, im->d_XS, im->d_PS, s));
@@ -1695,9 +1706,12 @@ int run_panel(h2gpu_image* im, int NV, int nv, const double* X, long long x_rs, 
         if (wide)
         {
             const int* nw = im->n_wide;
-            CK(launch_blk_wide(0, im->d_blkB, im->d_wide, nw[0], im->d_B32, im->d_XS, im->d_PS, s, im->d_status));
-            CK(launch_blk_wide(1, im->d_blkB, im->d_wide + nw[0], nw[1], im->d_B32, im->d_XS, im->d_PS, s, im->d_status));
-            im->st.n_launches += 1;
+            CK(launch_split3(im->d_XS, im->N, im->y0_rows, xs_rows, im->d_XS3, s));   // the skeleton rows y0
+            CK(launch_blk_wide(0, im->d_blkB, im->d_wide, nw[0], im->d_B32, im->d_XS3, xs_rows, im->d_PS, s,
+                               im->d_status));
+            CK(launch_blk_wide(1, im->d_blkB, im->d_wide + nw[0], nw[1], im->d_B32, im->d_XS3, xs_rows, im->d_PS, s,
+                               im->d_status));
+            im->st.n_launches += 2;   // the second pass and the split of the inputs
         }
         else if (f32) CK(launch_blk<float>(NV, im->d_blkB, im->n_blkB, im->d_B32, im->d_XS, im->d_PS, s, im->blk_tc, im->d_status));
         else CK(launch_blk<double>(NV, im->d_blkB, im->n_blkB, im->d_B64, im->d_XS, im->d_PS, s));

@@ -2326,7 +2326,7 @@ __host__ __device__ constexpr uint32_t umma_idesc_bf16_ab(int n, int a_mn_major,
 // current one run.  Bounded waits record a status and stop.
 struct WideSmem {
     uint16_t a[3][64 * 64];    // A tile pieces: 64 rows (of A) of 64 BF16, 128-byte swizzle
-    uint16_t b[3][64 * 64];    // right-hand-side pieces: 64 rows (k) of 64 BF16, 128-byte swizzle
+    uint16_t b[2][3][64 * 64]; // right-hand-side pieces, two stages: 64 rows (k) of 64 BF16, swizzled
     double acc[64][65];        // FP64 sums of the unit's 64 output rows (padded)
     unsigned long long mbar;
     uint32_t tmem;
@@ -2351,16 +2351,47 @@ __device__ __forceinline__ void bf16x3_pair(float x0, float x1, uint32_t& h, uin
 
 constexpr int kWideThreads = 256;
 
+// 16-byte global -> shared copy whose bytes past src_bytes (0 or 16) are zero-filled
+__device__ __forceinline__ void cp_async16_zfill(void* dst, const void* src, int src_bytes)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(src_bytes)
+                 : "memory");
+}
+
+// The 64-wide input space split once per panel into BF16 pieces h + m + l (bf16x3_pair),
+// piece p of row r at XS3[(p * rows + r) * 64 + v]: the B operands of the 64-wide block
+// passes are then copied tile by tile with no conversion.
+__global__ void k_split3(const double* __restrict__ XS, long long row0, long long n, long long rows,
+                         uint16_t* __restrict__ XS3)
+{
+    const long long ng = n * 8;   // granules of 8 right-hand sides
+    for (long long g = blockIdx.x * (long long) blockDim.x + threadIdx.x; g < ng; g += (long long) gridDim.x * blockDim.x)
+    {
+        const long long r = row0 + g / 8;
+        const int q = (int) (g % 8);
+        const double* x = XS + r * 64 + 8 * q;
+        uint32_t h[4], m[4], l[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) bf16x3_pair((float) x[2 * j], (float) x[2 * j + 1], h[j], m[j], l[j]);
+        uint4* o = reinterpret_cast<uint4*>(XS3 + r * 64 + 8 * q);
+        const long long ps = rows * 64 / 8;   // one piece, in uint4
+        o[0] = make_uint4(h[0], h[1], h[2], h[3]);
+        o[ps] = make_uint4(m[0], m[1], m[2], m[3]);
+        o[2 * ps] = make_uint4(l[0], l[1], l[2], l[3]);
+    }
+}
+
 template <int MODE>
 __global__ void __launch_bounds__(kWideThreads, 2) k_blk_wide(const BlkTask* __restrict__ tasks,
                                                               const WideUnit* __restrict__ units, int n_units,
                                                               const float* __restrict__ arena,
-                                                              const double* __restrict__ XS, double* __restrict__ PS,
-                                                              int* __restrict__ status)
+                                                              const uint16_t* __restrict__ XS3, long long rows3,
+                                                              double* __restrict__ PS, int* __restrict__ status)
 {
     constexpr int NV = 64;
     // pass 0: A K-major, B (V rows) MN-major; pass 1: A MN-major (A^T), B (W rows) MN-major
     constexpr uint32_t IDESC = umma_idesc_bf16_ab(NV, MODE == 1 ? 1 : 0, 1);
+    constexpr int STAGE_B = 3 * 64 * 64 * 2;      // bytes of one stage of right-hand-side pieces
     extern __shared__ __align__(1024) unsigned char wide_raw[];
     WideSmem& sm = *reinterpret_cast<WideSmem*>(wide_raw + ((1024 - (smem_u32(wide_raw) & 1023)) & 1023));
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -2384,157 +2415,159 @@ __global__ void __launch_bounds__(kWideThreads, 2) k_blk_wide(const BlkTask* __r
     const uint32_t a_s = smem_u32(sm.a), b_s = smem_u32(sm.b);
     bool ok = true;
     uint32_t phase = 0;
-    // persistent: the CTA takes units blockIdx.x, + gridDim.x, ...
-    for (int ui = blockIdx.x; ui < n_units && ok; ui += gridDim.x)
-    {
-    const WideUnit U = units[ui];
-    const BlkTask T = tasks[U.task];
-    const int ncol = T.ncol, nrow = T.nrow;
-    // the unit's fixed 64-row chunk (pass 0) or 64-column tile (pass 1), and the tiles it walks
-    const int nt = MODE == 0 ? (ncol + 63) / 64 : (nrow + 63) / 64;
-    const float* A0 = arena + T.a_off;
-
-    // tile t: rows [rc, rc + R) and columns [c0, c0 + C) of the block task, and the 64 rows
-    // of right-hand sides that meet it (V rows in0 + c0 + k, or W rows in1 + rc + k)
-    auto tile_of = [&](int t, int& rc, int& c0) {
-        if (MODE == 0) { rc = U.off; c0 = 64 * t; }
-        else { rc = 64 * t; c0 = U.off; }
-    };
-    // registers of the tile being loaded: thread t holds 2 granules (row r, 8 consecutive
-    // columns q) of A and 2 granules (row k, 8 consecutive right-hand sides) of the inputs
-    float ra[2][8], rb[2][8];
-    auto load_tile = [&](int t) {
-        int rc, c0;
-        tile_of(t, rc, c0);
-        const int R = min(64, nrow - rc), C = min(64, ncol - c0);
-        const float* A = A0 + (long long) rc * ncol + c0;
-        const int nk = MODE == 0 ? C : R;
-        const double* B = XS + (long long) (MODE == 0 ? T.in0_row + c0 : T.in1_row + rc) * NV;
-#pragma unroll
-        for (int u = 0; u < 2; u++)
-        {
-            const int gi = tid + kWideThreads * u, r = gi >> 3, q = gi & 7;
-#pragma unroll
-            for (int j = 0; j < 8; j++)
-            {
-                const int c = 8 * q + j;
-                ra[u][j] = (r < R && c < C) ? A[(long long) r * ncol + c] : 0.f;
-            }
-            if (r < nk)
-            {
-                const double2* src = reinterpret_cast<const double2*>(B + (long long) r * NV + 8 * q);
-#pragma unroll
-                for (int j = 0; j < 4; j++)
-                {
-                    const double2 v = src[j];
-                    rb[u][2 * j] = (float) v.x;
-                    rb[u][2 * j + 1] = (float) v.y;
-                }
-            } else {
-#pragma unroll
-                for (int j = 0; j < 8; j++) rb[u][j] = 0.f;
-            }
-        }
-    };
-    auto put = [&](unsigned char* base, int off, const float (&x)[8]) {
-        uint32_t h[4], m[4], l[4];
-#pragma unroll
-        for (int j = 0; j < 4; j++) bf16x3_pair(x[2 * j], x[2 * j + 1], h[j], m[j], l[j]);
-        *reinterpret_cast<uint4*>(base + off) = make_uint4(h[0], h[1], h[2], h[3]);
-        *reinterpret_cast<uint4*>(base + 8192 + off) = make_uint4(m[0], m[1], m[2], m[3]);
-        *reinterpret_cast<uint4*>(base + 16384 + off) = make_uint4(l[0], l[1], l[2], l[3]);
-    };
-    auto store_tile = [&]() {
-#pragma unroll
-        for (int u = 0; u < 2; u++)
-        {
-            const int gi = tid + kWideThreads * u, r = gi >> 3, q = gi & 7;
-            put(a_b, sw128(r, q), ra[u]);
-            put(b_b, sw128(r, q), rb[u]);
-        }
-    };
-
     // warp w reads TMEM lane quadrant w % 4 (rows 16 (w % 4) + lane, lane < 16) and the 32
     // accumulator columns 32 (w / 4) .. + 31
     const int quad = warp & 3, half = warp >> 2;
     double* const acc = sm.acc[(16 * quad + lane) & 63] + 32 * half;
-    // add the tile's FP32 products (TMEM) into the unit's FP64 sums
-    auto drain = [&](bool first) {
-        int good = 1;
-        if (tid == 0)
-        {
-            int it = 0;
-            while (!mbar_try_wait(mbar, phase))
-                if (++it > (1 << 22)) { good = 0; break; }
-            if (!good) atomicExch(status, 1);
-        }
-        phase ^= 1;
-        ok = __syncthreads_and(good) != 0;
-        if (!ok) return;
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        uint32_t d[32];
-        asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-                     "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-                     : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7]),
-                       "=r"(d[8]), "=r"(d[9]), "=r"(d[10]), "=r"(d[11]), "=r"(d[12]), "=r"(d[13]), "=r"(d[14]), "=r"(d[15]),
-                       "=r"(d[16]), "=r"(d[17]), "=r"(d[18]), "=r"(d[19]), "=r"(d[20]), "=r"(d[21]), "=r"(d[22]), "=r"(d[23]),
-                       "=r"(d[24]), "=r"(d[25]), "=r"(d[26]), "=r"(d[27]), "=r"(d[28]), "=r"(d[29]), "=r"(d[30]), "=r"(d[31])
-                     : "r"(tmem + ((uint32_t) (32 * quad) << 16) + (uint32_t) (32 * half)));
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        if (lane < 16)
-        {
-            if (first)
-#pragma unroll
-                for (int n = 0; n < 32; n++) acc[n] = (double) __uint_as_float(d[n]);
-            else
-#pragma unroll
-                for (int n = 0; n < 32; n++) acc[n] += (double) __uint_as_float(d[n]);
-        }
-    };
-
     constexpr int PA[6] = {2, 0, 1, 1, 0, 0}, PB[6] = {0, 2, 1, 0, 1, 0};
-    if (nt > 0) load_tile(0);
-    for (int t = 0; t < nt; t++)
+
+    // persistent: the CTA takes units blockIdx.x, + gridDim.x, ...
+    for (int ui = blockIdx.x; ui < n_units && ok; ui += gridDim.x)
     {
-        if (t > 0) drain(t == 1);
-        if (!ok) break;
-        store_tile();
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        __syncthreads();
-        if (tid == 0)
-        {
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const WideUnit U = units[ui];
+        const BlkTask T = tasks[U.task];
+        const int ncol = T.ncol, nrow = T.nrow;
+        // the unit's fixed 64-row chunk (pass 0) or 64-column tile (pass 1), and the tiles it walks
+        const int nt = MODE == 0 ? (ncol + 63) / 64 : (nrow + 63) / 64;
+        const float* A0 = arena + T.a_off;
+        auto tile_of = [&](int t, int& rc, int& c0) {
+            if (MODE == 0) { rc = U.off; c0 = 64 * t; }
+            else { rc = 64 * t; c0 = U.off; }
+        };
+        // the A tile is loaded into registers (thread t: 2 granules, row r, 8 consecutive
+        // columns q) and split into shared memory; the right-hand-side pieces of a tile are
+        // copied from XS3 by cp.async into one of two stages (rows past the tile's extent
+        // zero-filled)
+        float ra[2][8];
+        auto load_a = [&](int t) {
+            int rc, c0;
+            tile_of(t, rc, c0);
+            const int R = min(64, nrow - rc), C = min(64, ncol - c0);
+            const float* A = A0 + (long long) rc * ncol + c0;
 #pragma unroll
-            for (int ks = 0; ks < 4; ks++)          // K-steps of 16
+            for (int u = 0; u < 2; u++)
+            {
+                const int gi = tid + kWideThreads * u, r = gi >> 3, q = gi & 7;
 #pragma unroll
-                for (int p = 0; p < 6; p++)
+                for (int j = 0; j < 8; j++)
                 {
-                    // pass 0: A K-major (32-byte step along a row); pass 1: A MN-major
-                    // (16 rows = two 8-row swizzle atoms per step); B MN-major in both
-                    const uint64_t ad = MODE == 0 ? umma_desc(a_s + PA[p] * 8192 + ks * 32, 16, 1024, 2)
-                                                  : umma_desc(a_s + PA[p] * 8192 + ks * 2048, 8192, 1024, 2);
-                    umma_f16(tmem, ad, umma_desc(b_s + PB[p] * 8192 + ks * 2048, 8192, 1024, 2), IDESC,
-                             (ks == 0 && p == 0) ? 0u : 1u);
+                    const int c = 8 * q + j;
+                    ra[u][j] = (r < R && c < C) ? A[(long long) r * ncol + c] : 0.f;
                 }
-            umma_commit(mbar);
-        }
-        if (t + 1 < nt) load_tile(t + 1);
-    }
-    if (ok && nt > 0) drain(nt == 1);
-    // the unit's outputs, written once (each thread writes the sums it added)
-    if (ok && lane < 16)
-    {
-        const int m = 16 * quad + lane;
-        const int lim = MODE == 0 ? min(64, nrow - U.off) : min(64, ncol - U.off);
-        if (m < lim)
+            }
+        };
+        auto issue_b = [&](int t, int stage) {
+            int rc, c0;
+            tile_of(t, rc, c0);
+            const int nk = MODE == 0 ? min(64, ncol - c0) : min(64, nrow - rc);
+            const long long row0 = MODE == 0 ? (long long) T.in0_row + c0 : (long long) T.in1_row + rc;
+#pragma unroll
+            for (int u = 0; u < 6; u++)
+            {
+                const int i = tid + kWideThreads * u, pc = i >> 9, r = (i >> 3) & 63, q = i & 7;
+                const uint16_t* src = XS3 + ((long long) pc * rows3 + row0 + (r < nk ? r : 0)) * 64 + 8 * q;
+                cp_async16_zfill(b_b + stage * STAGE_B + pc * 8192 + sw128(r, q), src, r < nk ? 16 : 0);
+            }
+            cp_async_commit();
+        };
+        auto store_a = [&]() {
+#pragma unroll
+            for (int u = 0; u < 2; u++)
+            {
+                const int gi = tid + kWideThreads * u, r = gi >> 3, q = gi & 7;
+                uint32_t h[4], m[4], l[4];
+#pragma unroll
+                for (int j = 0; j < 4; j++) bf16x3_pair(ra[u][2 * j], ra[u][2 * j + 1], h[j], m[j], l[j]);
+                const int off = sw128(r, q);
+                *reinterpret_cast<uint4*>(a_b + off) = make_uint4(h[0], h[1], h[2], h[3]);
+                *reinterpret_cast<uint4*>(a_b + 8192 + off) = make_uint4(m[0], m[1], m[2], m[3]);
+                *reinterpret_cast<uint4*>(a_b + 16384 + off) = make_uint4(l[0], l[1], l[2], l[3]);
+            }
+        };
+        // wait for the tile's MMAs and add its FP32 products into the unit's FP64 sums (the
+        // unit's first tile initialises them)
+        auto drain = [&](bool first) {
+            int good = 1;
+            if (tid == 0)
+            {
+                int it = 0;
+                while (!mbar_try_wait(mbar, phase))
+                    if (++it > (1 << 22)) { good = 0; break; }
+                if (!good) atomicExch(status, 1);
+            }
+            phase ^= 1;
+            ok = __syncthreads_and(good) != 0;
+            if (!ok) return;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            uint32_t d[32];
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                         "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                         : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7]),
+                           "=r"(d[8]), "=r"(d[9]), "=r"(d[10]), "=r"(d[11]), "=r"(d[12]), "=r"(d[13]), "=r"(d[14]), "=r"(d[15]),
+                           "=r"(d[16]), "=r"(d[17]), "=r"(d[18]), "=r"(d[19]), "=r"(d[20]), "=r"(d[21]), "=r"(d[22]), "=r"(d[23]),
+                           "=r"(d[24]), "=r"(d[25]), "=r"(d[26]), "=r"(d[27]), "=r"(d[28]), "=r"(d[29]), "=r"(d[30]), "=r"(d[31])
+                         : "r"(tmem + ((uint32_t) (32 * quad) << 16) + (uint32_t) (32 * half)));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (lane < 16)
+            {
+                if (first)
+#pragma unroll
+                    for (int n = 0; n < 32; n++) acc[n] = (double) __uint_as_float(d[n]);
+                else
+#pragma unroll
+                    for (int n = 0; n < 32; n++) acc[n] += (double) __uint_as_float(d[n]);
+            }
+        };
+
+        issue_b(0, 0);
+        load_a(0);
+        for (int t = 0; t < nt; t++)
         {
-            double* o = PS + (long long) ((MODE == 0 ? T.out0_row : T.out1_row) + U.off + m) * NV + 32 * half;
+            if (t > 0) drain(t == 1);
+            if (!ok) break;
+            store_a();
+            cp_async_wait_all();                     // this thread's copies of tile t's inputs
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncthreads();
+            if (tid == 0)
+            {
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t bs = b_s + (uint32_t) ((t & 1) * STAGE_B);
+#pragma unroll
+                for (int ks = 0; ks < 4; ks++)          // K-steps of 16
+#pragma unroll
+                    for (int p = 0; p < 6; p++)
+                    {
+                        // pass 0: A K-major (32-byte step along a row); pass 1: A MN-major
+                        // (16 rows = two 8-row swizzle atoms per step); B MN-major in both
+                        const uint64_t ad = MODE == 0 ? umma_desc(a_s + PA[p] * 8192 + ks * 32, 16, 1024, 2)
+                                                      : umma_desc(a_s + PA[p] * 8192 + ks * 2048, 8192, 1024, 2);
+                        umma_f16(tmem, ad, umma_desc(bs + PB[p] * 8192 + ks * 2048, 8192, 1024, 2), IDESC,
+                                 (ks == 0 && p == 0) ? 0u : 1u);
+                    }
+                umma_commit(mbar);
+            }
+            if (t + 1 < nt)
+            {
+                issue_b(t + 1, (t + 1) & 1);         // that stage's previous tile (t - 1) was waited on
+                load_a(t + 1);
+            }
+        }
+        if (ok && nt > 0) drain(nt == 1);
+        // the unit's outputs, written once (each thread writes the sums it added)
+        if (ok && lane < 16)
+        {
+            const int m = 16 * quad + lane;
+            const int lim = MODE == 0 ? min(64, nrow - U.off) : min(64, ncol - U.off);
+            if (m < lim)
+            {
+                double* o = PS + (long long) ((MODE == 0 ? T.out0_row : T.out1_row) + U.off + m) * NV + 32 * half;
 #pragma unroll 8
-            for (int n = 0; n < 32; n++) o[n] = acc[n];
+                for (int n = 0; n < 32; n++) o[n] = acc[n];
+            }
         }
     }
-    }   // units
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0)
@@ -2980,8 +3013,16 @@ cudaError_t launch_blk(int NV, const BlkTask* t, int n, const TA* arena, const d
     return cudaGetLastError();
 }
 
+cudaError_t launch_split3(const double* XS, long long row0, long long n, long long rows, uint16_t* XS3,
+                          cudaStream_t st)
+{
+    if (n <= 0) return cudaSuccess;
+    k_split3<<<grid_for(n * 8, 256), 256, 0, st>>>(XS, row0, n, rows, XS3);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_blk_wide(int mode, const BlkTask* t, const WideUnit* u, int n, const float* arena,
-                            const double* XS, double* PS, cudaStream_t st, int* status)
+                            const uint16_t* XS3, long long rows3, double* PS, cudaStream_t st, int* status)
 {
     if (n <= 0) return cudaSuccess;
     if (!status) return cudaErrorInvalidValue;
@@ -2994,11 +3035,11 @@ cudaError_t launch_blk_wide(int mode, const BlkTask* t, const WideUnit* u, int n
     {
         cudaError_t e = allow_smem(k_blk_wide<0>, b);
         if (e != cudaSuccess) return e;
-        k_blk_wide<0><<<g, kWideThreads, b, st>>>(t, u, n, arena, XS, PS, status);
+        k_blk_wide<0><<<g, kWideThreads, b, st>>>(t, u, n, arena, XS3, rows3, PS, status);
     } else {
         cudaError_t e = allow_smem(k_blk_wide<1>, b);
         if (e != cudaSuccess) return e;
-        k_blk_wide<1><<<g, kWideThreads, b, st>>>(t, u, n, arena, XS, PS, status);
+        k_blk_wide<1><<<g, kWideThreads, b, st>>>(t, u, n, arena, XS3, rows3, PS, status);
     }
     return cudaGetLastError();
 }

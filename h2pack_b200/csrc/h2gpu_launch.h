@@ -21,7 +21,10 @@ cudaError_t launch_blk(int NV, const BlkTask* t, int n, const TA* arena, const d
 // 64-wide panels of FP32 stored blocks on tcgen05: pass 0 (mode 0, units = 64-row chunks:
 // A V) or pass 1 (mode 1, units = 64-column tiles: A^T W), outputs written once
 cudaError_t launch_blk_wide(int mode, const BlkTask* t, const WideUnit* u, int n, const float* arena,
-                            const double* XS, double* PS, cudaStream_t st, int* status);
+                            const uint16_t* XS3, long long rows3, double* PS, cudaStream_t st, int* status);
+// rows [row0, row0 + n) of the 64-wide input space (row stride 64) into its BF16 pieces
+cudaError_t launch_split3(const double* XS, long long row0, long long n, long long rows, uint16_t* XS3,
+                          cudaStream_t st);
 template <typename TA>
 cudaError_t launch_down(int NV, const DownTask* t, int n, const TA* U, const double* Y1, double* PS, double* PUSH,
                         cudaStream_t st, int use_tc = 0);
