@@ -133,11 +133,13 @@ struct h2gpu_image {
     size_t D_elems = 0;
     double4* d_pts64 = nullptr;   // global coordinates (x, y, z, radius)
     float4* d_pts32 = nullptr;    // coordinates relative to their node's box center
+    float4* d_pts32lo = nullptr;  // Coulomb: their low parts (coordinate - FP32 coordinate)
     size_t n_pts = 0;
     // source panels of the FP32 tensor-core JIT kernel
     PanelGroup* d_pg = nullptr;
     int n_pg = 0, n_pg_pts = 0;   // groups; groups of point sets (the rest are skeleton sets)
     float4* d_ppts = nullptr;     // 8 float4 per group: the points, paired as the B fragment holds them
+    float4* d_pplo = nullptr;     // Coulomb: 6 float4 per group, the low parts of those points
     TileRec* d_tiles = nullptr;   // source tiles of every JIT target chunk
     uint4* d_pin = nullptr;       // 64 uint4 per group (NV <= 16): inputs split into TF32 hi / lo
 
@@ -193,7 +195,7 @@ void free_all(h2gpu_image* im)
                     im->d_B32, im->d_D64, im->d_D32, im->d_pts64, im->d_pts32, im->d_XS, im->d_PS, im->d_Y1,
                     im->d_PUSH, im->d_io, im->d_owN, im->d_owF, im->d_pp, im->d_jtN2, im->d_jtF2, im->d_y1t2,
                     im->d_y1_slots2, im->d_asm2, im->d_asm_slots2, im->d_status, im->d_pg, im->d_ppts,
-                    im->d_pin, im->d_tiles, im->d_wide, im->d_XS3};
+                    im->d_pin, im->d_tiles, im->d_wide, im->d_XS3, im->d_pts32lo, im->d_pplo};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (im->h_status) cudaFreeHost(im->h_status);
@@ -320,6 +322,19 @@ void node_centers(const h2gpu_desc* d, std::vector<double>& c)
             }
         for (int k = 0; k < 3; k++) c[3 * n + k] = 0.5 * (lo[k] + hi[k]);
     }
+    // Centers on a grid of 2^(e - 21) with 2^e >= max |center|: every center is an
+    // integer multiple of the quantum below 2^21 in magnitude, so the difference of two
+    // centers (a frame shift) is exact in FP32.  Moving a frame's origin by less than
+    // a quantum changes nothing else.
+    double m = 0.0;
+    for (double v : c) m = std::max(m, std::fabs(v));
+    if (m > 0.0)
+    {
+        int e = 0;
+        std::frexp(m, &e);   // m < 2^e
+        const double q = std::ldexp(1.0, e - 21);
+        for (double& v : c) v = std::nearbyint(v / q) * q;
+    }
 }
 
 // Everything build_plan produces on the host; uploaded by upload_plan once a device is known.
@@ -341,6 +356,7 @@ struct HostPlan {
     std::vector<int> fw, bw;
     std::vector<double4> p64;
     std::vector<float4> p32;
+    std::vector<float4> p32lo;    // Coulomb only
     // pair plan (FP32 tensor-core path of scalar JIT kernels)
     std::vector<PairOwner> owN, owF;
     std::vector<PairPartner> partners;
@@ -561,6 +577,17 @@ int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
         p64.resize(np);
         p32.resize(np);
         const bool rad = d->xpt_dim >= 4;
+        // Coulomb (singular at r = 0): the FP32 near field forms differences from hi + lo
+        // coordinates, so nearby points keep their relative distance accuracy
+        const bool lo_parts = d->kernel_id == H2GPU_KRNL_COULOMB;
+        if (lo_parts) hp.p32lo.resize(np);
+        auto rel32 = [&](size_t p, double x, double y, double z, double a, const double* c) {
+            const double rx = x - c[0], ry = y - c[1], rz = z - c[2];
+            p32[p] = make_float4((float) rx, (float) ry, (float) rz, (float) a);
+            if (lo_parts)
+                hp.p32lo[p] = make_float4((float) (rx - (double) p32[p].x), (float) (ry - (double) p32[p].y),
+                                          (float) (rz - (double) p32[p].z), 0.f);
+        };
         for (int p = 0; p < d->n_point; p++)
         {
             double x = d->coord[p], y = d->coord[(size_t) d->n_point + p], z = d->coord[2 * (size_t) d->n_point + p];
@@ -568,7 +595,7 @@ int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
             REQ(leaf_of[p] >= 0, "point %d belongs to no leaf", p);
             const double* c = &ctr[3 * leaf_of[p]];
             p64[p] = make_double4(x, y, z, a);
-            p32[p] = make_float4((float) (x - c[0]), (float) (y - c[1]), (float) (z - c[2]), (float) a);
+            rel32(p, x, y, z, a, c);
         }
         for (int n = 0; n < n_node; n++)
         {
@@ -580,7 +607,7 @@ int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
                 const double* J = d->J_coord[n];
                 double x = J[j], y = J[nj + j], z = J[2 * nj + j], a = rad ? J[3 * nj + j] : 0.0;
                 p64[jp0[n] + j] = make_double4(x, y, z, a);
-                p32[jp0[n] + j] = make_float4((float) (x - c[0]), (float) (y - c[1]), (float) (z - c[2]), (float) a);
+                rel32(jp0[n] + j, x, y, z, a, c);
             }
         }
 
@@ -1499,6 +1526,7 @@ int upload_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
     TRY(upload(hp.bw, &im->d_bwd, im->bytes));
     TRY(upload(hp.p64, &im->d_pts64, im->bytes));
     TRY(upload(hp.p32, &im->d_pts32, im->bytes));
+    TRY(upload(hp.p32lo, &im->d_pts32lo, im->bytes));
     TRY(upload(hp.owN, &im->d_owN, im->bytes));
     TRY(upload(hp.owF, &im->d_owF, im->bytes));
     TRY(upload(hp.partners, &im->d_pp, im->bytes));
@@ -1518,6 +1546,12 @@ int upload_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
         CK(cudaMalloc(&im->d_ppts, sizeof(float4) * 8 * (size_t) im->n_pg));
         im->bytes += sizeof(float4) * 8 * (size_t) im->n_pg;
         CK(launch_panel_pts(im->d_pg, im->n_pg, im->d_pts32, im->d_ppts, im->stream));
+        if (im->d_pts32lo)
+        {
+            CK(cudaMalloc(&im->d_pplo, sizeof(float4) * 6 * (size_t) im->n_pg));
+            im->bytes += sizeof(float4) * 6 * (size_t) im->n_pg;
+            CK(launch_panel_lo(im->d_pg, im->n_pg, im->d_pts32lo, im->d_pplo, im->stream));
+        }
         CK(cudaStreamSynchronize(im->stream));
     }
     if (!d->BD_JIT && !im->gen)
@@ -1640,8 +1674,9 @@ int run_panel(h2gpu_image* im, int NV, int nv, const double* X, long long x_rs, 
         if (timed) CK(cudaEventRecord(e[1], s));
         CK(launch_panel_in(NV, im->d_pg, 0, im->n_pg_pts, im->d_XS, im->d_pin, s));
         CK(launch_jit(im->kernel_id, 1, NV, im->d_jtN2, im->n_jtN2, im->d_js, im->d_pts32, kp, 1, 1, im->d_XS,
-                      im->d_PS, im->d_Y1, s, 0, im->d_ppts, im->d_pin, im->d_tiles));
-        CK(launch_pair(im->kernel_id, NV, im->d_owN, im->n_owN, im->d_pp, im->d_pts32, kp, im->d_XS, im->d_PS, s));
+                      im->d_PS, im->d_Y1, s, 0, im->d_ppts, im->d_pin, im->d_tiles, im->d_pts32lo, im->d_pplo));
+        CK(launch_pair(im->kernel_id, NV, im->d_owN, im->n_owN, im->d_pp, im->d_pts32, kp, im->d_XS, im->d_PS, s, 0,
+                       im->d_pts32lo));
         if (timed) CK(cudaEventRecord(e[2], s));
         for (size_t L = 0; L + 1 < im->up_beg.size(); L++)
         {
@@ -1690,7 +1725,8 @@ int run_panel(h2gpu_image* im, int NV, int nv, const double* X, long long x_rs, 
         const bool panels = f32 && panels_used(im, NV);
         if (panels) CK(launch_panel_in(NV, im->d_pg, 0, im->n_pg_pts, im->d_XS, im->d_pin, s));
         CK(launch_jit(im->kernel_id, f32, NV, im->d_jtN, im->n_jtN, im->d_js, f32 ? (const void*) im->d_pts32 : (const void*) im->d_pts64,
-                      kparam_of(im), f32 ? 1 : 0, im->jit_tc, im->d_XS, im->d_PS, im->d_Y1, s, 0, im->d_ppts, im->d_pin, im->d_tiles));
+                      kparam_of(im), f32 ? 1 : 0, im->jit_tc, im->d_XS, im->d_PS, im->d_Y1, s, 0, im->d_ppts, im->d_pin, im->d_tiles,
+                      im->d_pts32lo, im->d_pplo));
         im->st.n_launches += panels ? 1 : 0;
     }
     if (timed) CK(cudaEventRecord(e[2], s));

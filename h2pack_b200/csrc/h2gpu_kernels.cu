@@ -18,6 +18,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
+#include <type_traits>
 #include "h2gpu_internal.cuh"
 #include "h2gpu_launch.h"
 
@@ -743,6 +744,21 @@ template <> struct ScalarF2<KRNL_MATERN32_ID> {
     }
 };
 
+// Exact-difference form of the near field (Coulomb): a coordinate is carried as
+// hi + lo (both FP32, hi = the re-centred coordinate rounded to FP32).  The target's
+// coordinate in the source set's frame is a + s with s the frame shift, which the
+// host makes exactly representable; two_sum returns the rounded sum and the low part
+// a' + (rounding error of a + s) (Knuth's TwoSum).  A difference is then
+// (ahi - bhi) + (alo - blo): the first term is exact or rounded relative to itself,
+// so r keeps ~FP32 relative accuracy however close two points are (the plain
+// difference of rounded coordinates loses eps * box / r).
+__device__ __forceinline__ void two_sum(float a, float s, float alo, float& hi, float& lo)
+{
+    hi = a + s;
+    const float bp = hi - a;
+    lo = ((a - (hi - bp)) + (s - bp)) + alo;
+}
+
 // FP32 kernel values for admissible (well-separated) pairs only: r2 > 0 always, so the
 // coincident-point cases drop out; constants are folded once per launch (prep).
 template <int KID> struct ScalarFar;
@@ -945,15 +961,18 @@ __global__ void __launch_bounds__(128 / TPT, sizeof(T) == 4 ? 5 * TPT : 4 * TPT)
 // as one FP32x2 pair.  Sources are staged in shared memory with every coordinate and
 // input stored twice (the FP32x2 operand that meets both targets), so a source costs
 // packed instructions only.  FAR (admissible pairs): r^2 = |a|^2 + |b|^2 - 2 a.b as in
-// k_jit_tc; otherwise differences.  FP32 sums per 64-source tile, FP64 across tiles.
+// k_jit_tc; otherwise differences (exact-difference form for Coulomb, see two_sum).
+// FP32 sums per 64-source tile, FP64 across tiles.
 template <int KID, int NV, bool FAR>
 __global__ void __launch_bounds__(64, NV >= 16 ? 8 : 10) k_jit2(const JitTarget* __restrict__ tgts, const JitSource* __restrict__ srcs,
                                                  const float4* __restrict__ pts, KParam kp,
                                                  const double* __restrict__ XS, double* __restrict__ PS,
-                                                 double* __restrict__ Y1)
+                                                 double* __restrict__ Y1, const float4* __restrict__ plo)
 {
+    constexpr bool EX = KID == KRNL_COULOMB_ID && !FAR;
     constexpr int TILE = 64, NT = 64;
-    __shared__ float4 s_p[TILE][2];          // {x, x, y, y}, {z, z, w, w}; w = |p|^2 (FAR)
+    __shared__ float4 s_p[TILE][2];          // {x, x, y, y}, {z, z, w, w}; w = |p|^2 (FAR), z' (EX)
+    __shared__ float4 s_l[EX ? TILE : 1];    // {x', x', y', y'} (EX)
     __shared__ float2 s_in[TILE * NV];       // (in, in)
     __shared__ double s_acc[2 * NV][NT];     // FP64 sums of the tile sums, [target q x NV + v][thread]
     const JitTarget tg = tgts[blockIdx.x];
@@ -963,6 +982,8 @@ __global__ void __launch_bounds__(64, NV >= 16 ? 8 : 10) k_jit2(const JitTarget*
     const int i0 = threadIdx.x, i1 = threadIdx.x + NT;
     const bool v0 = i0 < tg.npt, v1 = i1 < tg.npt;
     const float4 x0 = pts[tg.pt0 + (v0 ? i0 : 0)], x1 = pts[tg.pt0 + (v1 ? i1 : 0)];
+    float4 l0 = make_float4(0.f, 0.f, 0.f, 0.f), l1 = l0;
+    if constexpr (EX) { l0 = plo[tg.pt0 + (v0 ? i0 : 0)]; l1 = plo[tg.pt0 + (v1 ? i1 : 0)]; }
     float2 acc[NV];
 #pragma unroll
     for (int v = 0; v < NV; v++)
@@ -981,6 +1002,13 @@ __global__ void __launch_bounds__(64, NV >= 16 ? 8 : 10) k_jit2(const JitTarget*
         const float2 MX = make_float2(-2.f * ax, -2.f * bx), MY = make_float2(-2.f * ay, -2.f * by),
                      MZ = make_float2(-2.f * az, -2.f * bz);
         const float2 S2 = make_float2(ax * ax + ay * ay + az * az, bx * bx + by * by + bz * bz);
+        float2 XH = X, YH = Y, ZH = Z, XL = make_float2(0.f, 0.f), YL = XL, ZL = XL;
+        if constexpr (EX)
+        {
+            two_sum(x0.x, sc.sx, l0.x, XH.x, XL.x); two_sum(x1.x, sc.sx, l1.x, XH.y, XL.y);
+            two_sum(x0.y, sc.sy, l0.y, YH.x, YL.x); two_sum(x1.y, sc.sy, l1.y, YH.y, YL.y);
+            two_sum(x0.z, sc.sz, l0.z, ZH.x, ZL.x); two_sum(x1.z, sc.sz, l1.z, ZH.y, ZL.y);
+        }
         for (int j0 = 0; j0 < sc.npt; j0 += TILE)
         {
             const int nj = min(TILE, sc.npt - j0);
@@ -989,6 +1017,12 @@ __global__ void __launch_bounds__(64, NV >= 16 ? 8 : 10) k_jit2(const JitTarget*
             {
                 float4 q = pts[sc.pt0 + j0 + threadIdx.x];
                 if (FAR) q.w = q.x * q.x + q.y * q.y + q.z * q.z;
+                if constexpr (EX)
+                {
+                    const float4 ql = plo[sc.pt0 + j0 + threadIdx.x];
+                    q.w = ql.z;
+                    s_l[threadIdx.x] = make_float4(ql.x, ql.x, ql.y, ql.y);
+                }
                 s_p[threadIdx.x][0] = make_float4(q.x, q.x, q.y, q.y);
                 s_p[threadIdx.x][1] = make_float4(q.z, q.z, q.w, q.w);
             }
@@ -1010,6 +1044,15 @@ __global__ void __launch_bounds__(64, NV >= 16 ? 8 : 10) k_jit2(const JitTarget*
                     r2 = __ffma2_rn(MY, make_float2(P0.z, P0.w), r2);
                     r2 = __ffma2_rn(MX, make_float2(P0.x, P0.y), r2);
                     k = ScalarFar<KID>::f2(r2, q0, q1);
+                } else if constexpr (EX) {
+                    const float4 L = s_l[j];
+                    const float2 dx = __fadd2_rn(__ffma2_rn(make_float2(P0.x, P0.y), m1, XH),
+                                                 __ffma2_rn(make_float2(L.x, L.y), m1, XL));
+                    const float2 dy = __fadd2_rn(__ffma2_rn(make_float2(P0.z, P0.w), m1, YH),
+                                                 __ffma2_rn(make_float2(L.z, L.w), m1, YL));
+                    const float2 dz = __fadd2_rn(__ffma2_rn(make_float2(P1.x, P1.y), m1, ZH),
+                                                 __ffma2_rn(make_float2(P1.z, P1.w), m1, ZL));
+                    k = ScalarF2<KID>::f2(__ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz))), p0, c0);
                 } else {
                     const float2 dx = __ffma2_rn(make_float2(P0.x, P0.y), m1, X);
                     const float2 dy = __ffma2_rn(make_float2(P0.z, P0.w), m1, Y);
@@ -1085,6 +1128,22 @@ __global__ void k_panel_pts(const PanelGroup* __restrict__ pg, int n, const floa
     d[h] = q.x; d[2 + h] = q.y; d[4 + h] = q.z; d[6 + h] = q.w;
 }
 
+// Low parts of the panel points (Coulomb near field): per group 6 float4 = 24 floats,
+// [4t + h] = x', [4t + 2 + h] = y', [16 + 2t + h] = z' of point 8g + t + 4h (t < 4), the
+// same pairing as k_panel_pts; points past the set's end have zero low parts.
+__global__ void k_panel_lo(const PanelGroup* __restrict__ pg, int n, const float4* __restrict__ lo,
+                           float4* __restrict__ out)
+{
+    const long long e = blockIdx.x * (long long) blockDim.x + threadIdx.x;
+    if (e >= 8LL * n) return;
+    const int g = (int) (e >> 3), j = (int) (e & 7), t = j & 3, h = j >> 2;
+    const PanelGroup G = pg[g];
+    const float4 q = (j < G.nvalid) ? lo[G.pt0 + j] : make_float4(0.f, 0.f, 0.f, 0.f);
+    float* d = reinterpret_cast<float*>(out + 6LL * g);
+    d[4 * t + h] = q.x; d[4 * t + 2 + h] = q.y; d[16 + 2 * t + h] = q.z;
+}
+
+
 // Inputs: per group 2 x 32 uint4, the m16n8k8 A fragment of in^T (16 right-hand sides
 // x the group's 8 points; right-hand sides >= NV are zero) split into TF32 hi (first 32)
 // and lo (last 32): lane l (r = l/4, t = l%4) holds in[t][r], in[t][r+8], in[t+4][r],
@@ -1119,6 +1178,10 @@ struct JitTcSmem {
     double acc[8][8][32];       // FP64 sums of the FP32 segment sums, [warp][n-tile x 4 + q][lane]
     TileRec rec[4];             // records of the next tiles
 };
+// ... with the low parts of the points (Coulomb near field, 55 KB: still 4 CTAs per SM)
+struct JitTcSmemEx : JitTcSmem {
+    float4 lo[2][16][6];
+};
 
 // Same work split as k_jit (one CTA per 128-target chunk, owner computes), with the
 // right-hand-side products on the tensor cores.  Warp w owns targets 16w..16w+15.
@@ -1143,10 +1206,14 @@ template <int KID, int NV, bool FAR>
 __global__ void __launch_bounds__(256, 4) k_jit_tc(const JitTarget* __restrict__ tgts, const TileRec* __restrict__ tiles,
                                                    const float4* __restrict__ pts, const float4* __restrict__ ppts,
                                                    const uint4* __restrict__ pin, KParam kp, double* __restrict__ PS,
-                                                   double* __restrict__ Y1)
+                                                   double* __restrict__ Y1, const float4* __restrict__ plo,
+                                                   const float4* __restrict__ pplo)
 {
+    // EX: exact differences (Coulomb near field; plo / pplo = low parts of the points / panels)
+    constexpr bool EX = KID == KRNL_COULOMB_ID && !FAR;
+    using SM = typename std::conditional<EX, JitTcSmemEx, JitTcSmem>::type;
     extern __shared__ __align__(16) unsigned char jtc_raw[];
-    JitTcSmem& sm = *reinterpret_cast<JitTcSmem*>(jtc_raw);
+    SM& sm = *reinterpret_cast<SM*>(jtc_raw);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, tq = lane & 3;
     const JitTarget tg = tgts[blockIdx.x];
     const bool busy = warp * 16 < tg.npt;
@@ -1197,11 +1264,12 @@ __global__ void __launch_bounds__(256, 4) k_jit_tc(const JitTarget* __restrict__
         const int gb = sm.rec[k & 3].gb, ng = sm.rec[k & 3].ng;
         const float4* gp = ppts + 8LL * gb;
         const uint4* gi = pin + 64LL * gb;
-        const int np = ng * 8, nall = np + ng * 64;
+        const int np = ng * 8, nin = np + ng * 64, nall = nin + (EX ? ng * 6 : 0);
         for (int c = threadIdx.x; c < nall; c += 256)
         {
             if (c < np) cp_async16(&sm.pt[buf][0][0][0] + c, gp + c);
-            else cp_async16(&sm.in[buf][0][0][0] + (c - np), gi + (c - np));
+            else if (c < nin) cp_async16(&sm.in[buf][0][0][0] + (c - np), gi + (c - np));
+            else if constexpr (EX) cp_async16(&sm.lo[buf][0][0] + (c - nin), pplo + 6LL * gb + (c - nin));
         }
     };
     issue_rec(0); issue_rec(1); issue_rec(2); issue_rec(3);
@@ -1251,6 +1319,34 @@ __global__ void __launch_bounds__(256, 4) k_jit_tc(const JitTarget* __restrict__
                         const float2 k1 = ScalarFar<KID>::f2(r2p(sb22, mbx2, mby2, mbz2), q0, q1);
                         mma_group(k0, k1, buf, grp);
                     }
+                } else if constexpr (EX) {
+                    // targets as hi + lo in the source set's frame (the shift is exact); the
+                    // low parts are read per tile (few registers stay live across tiles)
+                    const float4 l0 = plo[tg.pt0 + (i0 < tg.npt ? i0 : 0)], l1 = plo[tg.pt0 + (i1 < tg.npt ? i1 : 0)];
+                    float ahx, ahy, ahz, alx, aly, alz, bhx, bhy, bhz, blx, bly, blz;
+                    two_sum(x0.x, r.sx, l0.x, ahx, alx); two_sum(x0.y, r.sy, l0.y, ahy, aly);
+                    two_sum(x0.z, r.sz, l0.z, ahz, alz);
+                    two_sum(x1.x, r.sx, l1.x, bhx, blx); two_sum(x1.y, r.sy, l1.y, bhy, bly);
+                    two_sum(x1.z, r.sz, l1.z, bhz, blz);
+#pragma unroll 1
+                    for (int grp = h; grp < ge; grp++)
+                    {
+                        const float4 P0 = sm.pt[buf][grp][tq][0], P1 = sm.pt[buf][grp][tq][1];
+                        const float4 L0 = sm.lo[buf][grp][tq], LZ = sm.lo[buf][grp][4 + (tq >> 1)];
+                        const float2 lz = (tq & 1) ? make_float2(LZ.z, LZ.w) : make_float2(LZ.x, LZ.y);
+                        const float2 m1 = make_float2(-1.f, -1.f);
+                        // (th - p) + (tl - p') per coordinate, both sources of the pair at once
+                        auto d2 = [&](float th, float tl, float2 p, float2 q) {
+                            return __fadd2_rn(__ffma2_rn(p, m1, make_float2(th, th)), __ffma2_rn(q, m1, make_float2(tl, tl)));
+                        };
+                        const float2 PX = make_float2(P0.x, P0.y), PY = make_float2(P0.z, P0.w), PZ = make_float2(P1.x, P1.y);
+                        const float2 QX = make_float2(L0.x, L0.y), QY = make_float2(L0.z, L0.w);
+                        float2 dx = d2(ahx, alx, PX, QX), dy = d2(ahy, aly, PY, QY), dz = d2(ahz, alz, PZ, lz);
+                        const float2 k0 = ScalarF2<KID>::f2(__ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz))), p0, c0);
+                        dx = d2(bhx, blx, PX, QX); dy = d2(bhy, bly, PY, QY); dz = d2(bhz, blz, PZ, lz);
+                        const float2 k1 = ScalarF2<KID>::f2(__ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz))), p0, c0);
+                        mma_group(k0, k1, buf, grp);
+                    }
                 } else {
                     const float2 ax2 = make_float2(ax, ax), ay2 = make_float2(ay, ay), az2 = make_float2(az, az);
                     const float2 bx2 = make_float2(bx, bx), by2 = make_float2(by, by), bz2 = make_float2(bz, bz);
@@ -1292,7 +1388,7 @@ __global__ void __launch_bounds__(256, 4) k_jit_tc(const JitTarget* __restrict__
         }
 }
 
-constexpr int jit_tc_smem_bytes() { return (int) sizeof(JitTcSmem); }
+constexpr int jit_tc_smem_bytes(bool ex) { return (int) (ex ? sizeof(JitTcSmemEx) : sizeof(JitTcSmem)); }
 
 // ---------------------------------------- JIT pair kernel (both directions at once)
 
@@ -1319,6 +1415,7 @@ template <int NV>
 struct PairSmem {
     static constexpr int NT = NV / 8, TS = 64, NG = TS / 8, NW = kPairWarps;
     float4 pt[2][TS];
+    float4 lo[2][TS];          // low parts of the points (Coulomb near field)
     uint4 b[2][NG][NT][32];
     double acc[NW][NT * 4][32];
     float d2[NW][TS][NV];
@@ -1329,8 +1426,10 @@ template <int KID, int NV, bool FAR>
 __global__ void __launch_bounds__(32 * kPairWarps, 3) k_jit_pair(const PairOwner* __restrict__ owners,
                                                                  const PairPartner* __restrict__ partners,
                                                                  const float4* __restrict__ pts, KParam kp,
-                                                                 const double* __restrict__ XS, double* __restrict__ PS)
+                                                                 const double* __restrict__ XS, double* __restrict__ PS,
+                                                                 const float4* __restrict__ plo)
 {
+    constexpr bool EX = KID == KRNL_COULOMB_ID && !FAR;   // exact differences (see two_sum)
     using SM = PairSmem<NV>;
     constexpr int NT = SM::NT, TS = SM::TS, NG = SM::NG, NW = SM::NW, NTH = 32 * NW;
     constexpr int NB = NG * NT * 32 / NTH;        // B-fragment entries staged per thread and tile
@@ -1346,13 +1445,16 @@ __global__ void __launch_bounds__(32 * kPairWarps, 3) k_jit_pair(const PairOwner
     float* d2w = &sm.d2[warp][0][0];
 
     // staging of one tile (points of b and its inputs split into TF32 hi / lo)
-    float4 rp = make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 rp = make_float4(0.f, 0.f, 0.f, 0.f), rl = rp;
     double rxa[NB], rxb[NB];
     auto load_tile = [&](int pi, int j0) {
         const PairPartner pb = partners[pi];
         const int nj = min(TS, pb.nb - j0);
         if (threadIdx.x < TS)
+        {
             rp = (threadIdx.x < nj) ? pts[pb.pb + j0 + threadIdx.x] : make_float4(1e6f, 1e6f, 1e6f, 0.f);
+            if constexpr (EX) rl = (threadIdx.x < nj) ? plo[pb.pb + j0 + threadIdx.x] : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
 #pragma unroll
         for (int u = 0; u < NB; u++)
         {
@@ -1369,6 +1471,7 @@ __global__ void __launch_bounds__(32 * kPairWarps, 3) k_jit_pair(const PairOwner
             float4 q = rp;
             if (FAR) q.w = q.x * q.x + q.y * q.y + q.z * q.z;   // |b|^2 for the far form of r^2
             sm.pt[buf][threadIdx.x] = q;
+            if constexpr (EX) sm.lo[buf][threadIdx.x] = rl;
         }
 #pragma unroll
         for (int u = 0; u < NB; u++)
@@ -1443,6 +1546,17 @@ __global__ void __launch_bounds__(32 * kPairWarps, 3) k_jit_pair(const PairOwner
                 const float2 m_x = make_float2(-2.f * ax, -2.f * bx), m_y = make_float2(-2.f * ay, -2.f * by),
                              m_z = make_float2(-2.f * az, -2.f * bz);
                 const float2 s2 = make_float2(ax * ax + ay * ay + az * az, bx * bx + by * by + bz * bz);
+                // exact-difference form: rows (g, g+8) of a as hi + lo pairs in b's frame
+                float2 hx = make_float2(ax, bx), hy = make_float2(ay, by), hz = make_float2(az, bz);
+                float2 lx = make_float2(0.f, 0.f), ly = lx, lz = lx;
+                if constexpr (EX)
+                {
+                    // the low parts of a's rows, read per tile (fewer live registers)
+                    const float4 l0 = plo[ow.pa + ch + (v0 ? i0 : 0)], l1 = plo[ow.pa + ch + (v1 ? i1 : 0)];
+                    two_sum(x0.x, pb.sx, l0.x, hx.x, lx.x); two_sum(x1.x, pb.sx, l1.x, hx.y, lx.y);
+                    two_sum(x0.y, pb.sy, l0.y, hy.x, ly.x); two_sum(x1.y, pb.sy, l1.y, hy.y, ly.y);
+                    two_sum(x0.z, pb.sz, l0.z, hz.x, lz.x); two_sum(x1.z, pb.sz, l1.z, hz.y, lz.y);
+                }
                 const int ngrp = (nj + 7) >> 3;
                 for (int grp = 0; grp < ngrp; grp++)
                 {
@@ -1459,6 +1573,21 @@ __global__ void __launch_bounds__(32 * kPairWarps, 3) k_jit_pair(const PairOwner
                         const float2 ka = ScalarFar<KID>::f2(r2p(pa), q0, q1);   // (a g, b t), (a g+8, b t)
                         const float2 kb = ScalarFar<KID>::f2(r2p(pc), q0, q1);   // (a g, b t+4), (a g+8, b t+4)
                         k[0] = ka.x; k[1] = ka.y; k[2] = kb.x; k[3] = kb.y;
+                    } else if constexpr (EX) {
+                        auto r2e = [&](const float4& p, const float4& q) {
+                            const float2 dx = __fadd2_rn(__fadd2_rn(hx, make_float2(-p.x, -p.x)),
+                                                         __fadd2_rn(lx, make_float2(-q.x, -q.x)));
+                            const float2 dy = __fadd2_rn(__fadd2_rn(hy, make_float2(-p.y, -p.y)),
+                                                         __fadd2_rn(ly, make_float2(-q.y, -q.y)));
+                            const float2 dz = __fadd2_rn(__fadd2_rn(hz, make_float2(-p.z, -p.z)),
+                                                         __fadd2_rn(lz, make_float2(-q.z, -q.z)));
+                            return __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+                        };
+                        const float2 ra2 = r2e(pa, sm.lo[buf][grp * 8 + tq]), rc2 = r2e(pc, sm.lo[buf][grp * 8 + tq + 4]);
+                        k[0] = Scalar<KID, float>::f(ra2.x, p0, c0);
+                        k[1] = Scalar<KID, float>::f(ra2.y, p0, c0);
+                        k[2] = Scalar<KID, float>::f(rc2.x, p0, c0);
+                        k[3] = Scalar<KID, float>::f(rc2.y, p0, c0);
                     } else {
                         auto r2d = [&](const float4& p) {
                             const float2 dx = __fadd2_rn(make_float2(ax, bx), make_float2(-p.x, -p.x));
@@ -3092,10 +3221,13 @@ cudaError_t launch_asm(int NV, const AsmTask* t, int n, const int* slots, const 
 template <int KID, typename T, int KD>
 static cudaError_t launch_jit_k(int NV, const JitTarget* tg, int n, const JitSource* sr, const void* pts, KParam kp,
                                 int use_shift, int use_tc, const double* XS, double* PS, double* Y1, cudaStream_t st,
-                                int far, const float4* ppts, const uint4* pin, const TileRec* tiles)
+                                int far, const float4* ppts, const uint4* pin, const TileRec* tiles,
+                                const float4* lo, const float4* plo)
 {
     using T4 = typename Vec4<T>::t;
     const T4* p = (const T4*) pts;
+    // the FP32 Coulomb near field reads the low parts of the points
+    if (KID == KRNL_COULOMB_ID && sizeof(T) == 4 && !far && !lo) return cudaErrorInvalidValue;
     // FP32 scalar kernels on panels of 8 or 16: right-hand-side products on the tensor
     // cores unless the image chose the CUDA-core kernel (autotuner, H2G_JIT_TC=0)
     if constexpr (KD == 1 && sizeof(T) == 4)
@@ -3104,15 +3236,16 @@ static cudaError_t launch_jit_k(int NV, const JitTarget* tg, int n, const JitSou
         {
             // the tensor-core kernel reads the source panels and tile lists
             if (!ppts || !pin || !tiles) return cudaErrorInvalidValue;
+            if (KID == KRNL_COULOMB_ID && !far && !plo) return cudaErrorInvalidValue;
             const float4* p4 = (const float4*) pts;
-            constexpr int b = jit_tc_smem_bytes();
+            const int b = jit_tc_smem_bytes(KID == KRNL_COULOMB_ID && !far);
             // the dynamic shared-memory opt-in is a per-device function attribute (cheap,
             // and legal inside a stream capture), so it is set at every launch
             auto kern = NV == 16 ? (far ? k_jit_tc<KID, 16, true> : k_jit_tc<KID, 16, false>)
                                  : (far ? k_jit_tc<KID, 8, true> : k_jit_tc<KID, 8, false>);
             cudaError_t e = allow_smem(kern, b);
             if (e != cudaSuccess) return e;
-            kern<<<n, 256, b, st>>>(tg, tiles, p4, ppts, pin, kp, PS, Y1);
+            kern<<<n, 256, b, st>>>(tg, tiles, p4, ppts, pin, kp, PS, Y1, lo, plo);
             return cudaGetLastError();
         }
     }
@@ -3126,8 +3259,8 @@ static cudaError_t launch_jit_k(int NV, const JitTarget* tg, int n, const JitSou
         {
             // scalar FP32 kernels: the two targets of a thread as one FP32x2 pair
             if (!use_shift) return cudaErrorInvalidValue;   // FP32 evaluation is re-centred
-            if (far) k_jit2<KID, NVc, true><<<n, 64, 0, st>>>(tg, sr, (const float4*) pts, kp, XS, PS, Y1);
-            else k_jit2<KID, NVc, false><<<n, 64, 0, st>>>(tg, sr, (const float4*) pts, kp, XS, PS, Y1);
+            if (far) k_jit2<KID, NVc, true><<<n, 64, 0, st>>>(tg, sr, (const float4*) pts, kp, XS, PS, Y1, lo);
+            else k_jit2<KID, NVc, false><<<n, 64, 0, st>>>(tg, sr, (const float4*) pts, kp, XS, PS, Y1, lo);
         }
         else if constexpr (KD * NVc <= 16 && sizeof(T) == 4)
             k_jit<KID, T, NVc, KD, 2><<<n, 64, 0, st>>>(tg, sr, p, kp, use_shift, XS, PS, Y1);
@@ -3139,10 +3272,11 @@ static cudaError_t launch_jit_k(int NV, const JitTarget* tg, int n, const JitSou
 
 cudaError_t launch_jit(int kid, int fp32, int NV, const JitTarget* tg, int n, const JitSource* sr, const void* pts,
                        KParam kp, int use_shift, int use_tc, const double* XS, double* PS, double* Y1, cudaStream_t st,
-                       int far, const float4* ppts, const uint4* pin, const TileRec* tiles)
+                       int far, const float4* ppts, const uint4* pin, const TileRec* tiles, const float4* lo,
+                       const float4* plo)
 {
     if (n <= 0) return cudaSuccess;
-#define H2G_JIT_ARGS NV, tg, n, sr, pts, kp, use_shift, use_tc, XS, PS, Y1, st, far, ppts, pin, tiles
+#define H2G_JIT_ARGS NV, tg, n, sr, pts, kp, use_shift, use_tc, XS, PS, Y1, st, far, ppts, pin, tiles, lo, plo
     switch (kid)
     {
         case KRNL_COULOMB_ID:  return fp32 ? launch_jit_k<KRNL_COULOMB_ID, float, 1>(H2G_JIT_ARGS)
@@ -3166,6 +3300,14 @@ cudaError_t launch_panel_pts(const PanelGroup* pg, int n, const float4* pts, flo
     return cudaGetLastError();
 }
 
+cudaError_t launch_panel_lo(const PanelGroup* pg, int n, const float4* lo, float4* out, cudaStream_t st)
+{
+    if (n <= 0) return cudaSuccess;
+    const long long t = 8LL * n;
+    k_panel_lo<<<(unsigned) ((t + 255) / 256), 256, 0, st>>>(pg, n, lo, out);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_panel_in(int NV, const PanelGroup* pg, int g0, int n, const double* XS, uint4* pin, cudaStream_t st)
 {
     if (n <= 0 || !pin || (NV != 8 && NV != 16)) return cudaSuccess;
@@ -3177,19 +3319,20 @@ cudaError_t launch_panel_in(int NV, const PanelGroup* pg, int g0, int n, const d
 
 template <int KID, bool FAR>
 static cudaError_t launch_pair_kf(int NV, const PairOwner* ow, int n, const PairPartner* pp, const float4* pts, KParam kp,
-                                  const double* XS, double* PS, cudaStream_t st)
+                                  const double* XS, double* PS, cudaStream_t st, const float4* lo)
 {
+    if (KID == KRNL_COULOMB_ID && !FAR && !lo) return cudaErrorInvalidValue;
     if (NV == 16)
     {
         constexpr int b = pair_smem_bytes<16>();
         cudaError_t e = allow_smem(k_jit_pair<KID, 16, FAR>, b);
         if (e != cudaSuccess) return e;
-        k_jit_pair<KID, 16, FAR><<<n, 32 * kPairWarps, b, st>>>(ow, pp, pts, kp, XS, PS);
+        k_jit_pair<KID, 16, FAR><<<n, 32 * kPairWarps, b, st>>>(ow, pp, pts, kp, XS, PS, lo);
     } else if (NV == 8) {
         constexpr int b = pair_smem_bytes<8>();
         cudaError_t e = allow_smem(k_jit_pair<KID, 8, FAR>, b);
         if (e != cudaSuccess) return e;
-        k_jit_pair<KID, 8, FAR><<<n, 32 * kPairWarps, b, st>>>(ow, pp, pts, kp, XS, PS);
+        k_jit_pair<KID, 8, FAR><<<n, 32 * kPairWarps, b, st>>>(ow, pp, pts, kp, XS, PS, lo);
     } else {
         return cudaErrorInvalidValue;
     }
@@ -3198,22 +3341,22 @@ static cudaError_t launch_pair_kf(int NV, const PairOwner* ow, int n, const Pair
 
 template <int KID>
 static cudaError_t launch_pair_k(int NV, const PairOwner* ow, int n, const PairPartner* pp, const float4* pts, KParam kp,
-                                 const double* XS, double* PS, cudaStream_t st, int far)
+                                 const double* XS, double* PS, cudaStream_t st, int far, const float4* lo)
 {
-    return far ? launch_pair_kf<KID, true>(NV, ow, n, pp, pts, kp, XS, PS, st)
-               : launch_pair_kf<KID, false>(NV, ow, n, pp, pts, kp, XS, PS, st);
+    return far ? launch_pair_kf<KID, true>(NV, ow, n, pp, pts, kp, XS, PS, st, lo)
+               : launch_pair_kf<KID, false>(NV, ow, n, pp, pts, kp, XS, PS, st, lo);
 }
 
 cudaError_t launch_pair(int kid, int NV, const PairOwner* ow, int n, const PairPartner* pp, const void* pts, KParam kp,
-                        const double* XS, double* PS, cudaStream_t st, int far)
+                        const double* XS, double* PS, cudaStream_t st, int far, const float4* lo)
 {
     if (n <= 0) return cudaSuccess;
     const float4* p = (const float4*) pts;
     switch (kid)
     {
-        case KRNL_COULOMB_ID:  return launch_pair_k<KRNL_COULOMB_ID>(NV, ow, n, pp, p, kp, XS, PS, st, far);
-        case KRNL_GAUSSIAN_ID: return launch_pair_k<KRNL_GAUSSIAN_ID>(NV, ow, n, pp, p, kp, XS, PS, st, far);
-        case KRNL_MATERN32_ID: return launch_pair_k<KRNL_MATERN32_ID>(NV, ow, n, pp, p, kp, XS, PS, st, far);
+        case KRNL_COULOMB_ID:  return launch_pair_k<KRNL_COULOMB_ID>(NV, ow, n, pp, p, kp, XS, PS, st, far, lo);
+        case KRNL_GAUSSIAN_ID: return launch_pair_k<KRNL_GAUSSIAN_ID>(NV, ow, n, pp, p, kp, XS, PS, st, far, lo);
+        case KRNL_MATERN32_ID: return launch_pair_k<KRNL_MATERN32_ID>(NV, ow, n, pp, p, kp, XS, PS, st, far, lo);
         default: return cudaErrorInvalidValue;
     }
 }

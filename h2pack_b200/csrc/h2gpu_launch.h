@@ -33,18 +33,21 @@ cudaError_t launch_asm(int NV, const AsmTask* t, int n, const int* slots, const 
                        double* Y, long long y_rs, long long y_cs, int nv, cudaStream_t st);
 // far: every source set is admissible for its target (r > 0); ppts / pin / tiles: the
 // source panels and tile lists, which the tensor-core kernel (FP32 scalar kernels,
-// NV 8 / 16, use_tc) reads
+// NV 8 / 16, use_tc) reads; lo / plo: the low parts of the FP32 points and of the
+// panels, which the FP32 Coulomb near field needs (exact differences)
 cudaError_t launch_jit(int kid, int fp32, int NV, const JitTarget* tg, int n, const JitSource* sr, const void* pts,
                        KParam kp, int use_shift, int use_tc, const double* XS, double* PS, double* Y1, cudaStream_t st,
                        int far = 0, const float4* ppts = nullptr, const uint4* pin = nullptr,
-                       const TileRec* tiles = nullptr);
+                       const TileRec* tiles = nullptr, const float4* lo = nullptr, const float4* plo = nullptr);
 // source panels: the points (once per image) and the inputs of groups [g0, g0 + n) for a
 // panel of NV right-hand sides (NV 8 / 16; other widths do nothing)
 cudaError_t launch_panel_pts(const PanelGroup* pg, int n, const float4* pts, float4* ppts, cudaStream_t st);
+// the low parts of the panel points (6 float4 per group)
+cudaError_t launch_panel_lo(const PanelGroup* pg, int n, const float4* lo, float4* out, cudaStream_t st);
 cudaError_t launch_panel_in(int NV, const PanelGroup* pg, int g0, int n, const double* XS, uint4* pin, cudaStream_t st);
 cudaError_t launch_pair(int kid, int NV, const PairOwner* ow, int n, const PairPartner* pp, const void* pts, KParam kp,
                         const double* XS, double* PS, cudaStream_t st,
-                        int far = 0);
+                        int far = 0, const float4* lo = nullptr);
 // stored-block generation: tasks [0, n) into arena (double or float, per fp32)
 cudaError_t launch_gen(int kid, int kd, int fp32, const GenTask* t, int n, const double4* pts, KParam kp, void* arena,
                        cudaStream_t st);
