@@ -161,6 +161,10 @@ struct h2gpu_image {
 
     // pair plan: each unordered JIT pair evaluated once (FP32 tensor-core path)
     int has_pair = 0;
+    int blk1_small[2][2] = {{0, 0}, {0, 0}};   // [B, D][FP64, FP32]: leading tasks that blk1_fits
+    // FP32 far field in the difference form: some admissible pair's boxes are too close
+    // for r^2 = |a|^2 + |b|^2 - 2 a.b (HSS mode: siblings are admissible and may touch)
+    int far_diff = 0;
     PairOwner* d_owN = nullptr;
     PairOwner* d_owF = nullptr;
     PairPartner* d_pp = nullptr;
@@ -307,9 +311,10 @@ int validate(const h2gpu_desc* d, bool gen = false)
 }
 
 // Center of the bounding box of every node's points.
-void node_centers(const h2gpu_desc* d, std::vector<double>& c)
+void node_centers(const h2gpu_desc* d, std::vector<double>& c, std::vector<double>* half = nullptr)
 {
     c.assign(3 * (size_t) d->n_node, 0.0);
+    if (half) half->assign(3 * (size_t) d->n_node, 0.0);
     for (int n = 0; n < d->n_node; n++)
     {
         double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
@@ -321,6 +326,8 @@ void node_centers(const h2gpu_desc* d, std::vector<double>& c)
                 hi[k] = std::max(hi[k], x);
             }
         for (int k = 0; k < 3; k++) c[3 * n + k] = 0.5 * (lo[k] + hi[k]);
+        if (half)
+            for (int k = 0; k < 3; k++) (*half)[3 * n + k] = 0.5 * std::max(0.0, hi[k] - lo[k]);
     }
     // Centers on a grid of 2^(e - 21) with 2^e >= max |center|: every center is an
     // integer multiple of the quantum below 2^21 in magnitude, so the difference of two
@@ -533,6 +540,25 @@ int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
             }
         }
         for (int n = 0; n < n_node; n++) has_y1[n] = !y1s[n].empty();
+        // one-RHS kernel (k_blk1): tasks one warp takes first, those within the FP64
+        // limit before those within the FP32 limit only; stable, so the tasks of one row
+        // node stay adjacent within a class (the outputs do not depend on task order)
+        for (int li = 0; li < 2; li++)
+        {
+            std::vector<BlkTask>& ts = li == 0 ? blkB : blkD;
+            auto cls = [](const BlkTask& t) {
+                return blk1_fits(t.nrow, t.ncol, 8) ? 0 : (blk1_fits(t.nrow, t.ncol, 4) ? 1 : 2);
+            };
+            std::stable_sort(ts.begin(), ts.end(), [&](const BlkTask& a, const BlkTask& b) { return cls(a) < cls(b); });
+            int n64 = 0, n32 = 0;
+            for (const BlkTask& t : ts)
+            {
+                n64 += cls(t) == 0;
+                n32 += cls(t) <= 1;
+            }
+            im->blk1_small[li][0] = n64;
+            im->blk1_small[li][1] = n32;
+        }
         // units of the 64-wide passes: pass 0 per 64-row chunk of a task (A V), pass 1 per
         // 64-column tile of a task (A^T W)
         // Pass-0 units are ordered by their input rows (the column node's y0 / x slice),
@@ -560,7 +586,34 @@ int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
         im->n_wide[3] = units(blkD, 1);
     } else {
         // ---- JIT: point space = sorted points, then the skeleton points of every node
-        node_centers(d, ctr);
+        std::vector<double> half;
+        node_centers(d, ctr, &half);
+        // The FP32 far field forms r^2 = |a|^2 + |b|^2 - 2 a.b in the source box's frame;
+        // its rounding error relative to r^2 is a few eps times
+        // F = (max |a|^2 + max |b|^2) / min r^2, with |b| <= the source box's half-diagonal,
+        // |a| <= the center distance + the target box's, r >= the gap between the boxes.
+        // H2Pack's admissibility (a gap of one box width) keeps F near 10, or ~30 with
+        // pairs two levels apart; touching boxes (HSS mode: every sibling pair is
+        // admissible) make it unbounded.  Any pair with F > 64, in either direction,
+        // switches the image's FP32 far field to the difference form.
+        im->far_diff = 0;
+        for (int i = 0; i < d->n_r_adm_pair && !im->far_diff; i++)
+        {
+            const int a = d->r_adm_pairs[2 * i], b = d->r_adm_pairs[2 * i + 1];
+            double gap2 = 0.0, dc2 = 0.0, ha2 = 0.0, hb2 = 0.0;
+            for (int k = 0; k < 3; k++)
+            {
+                const double dc = std::fabs(ctr[3 * a + k] - ctr[3 * b + k]);
+                const double g = dc - half[3 * a + k] - half[3 * b + k];
+                if (g > 0.0) gap2 += g * g;
+                dc2 += dc * dc;
+                ha2 += half[3 * a + k] * half[3 * a + k];
+                hb2 += half[3 * b + k] * half[3 * b + k];
+            }
+            const double dcn = std::sqrt(dc2), ha = std::sqrt(ha2), hb = std::sqrt(hb2);
+            const double num = std::max((dcn + ha) * (dcn + ha) + hb2, (dcn + hb) * (dcn + hb) + ha2);
+            if (!(num <= 64.0 * gap2)) im->far_diff = 1;
+        }
         std::vector<int> jp0(n_node, 0);
         long long np = d->n_point;
         for (int n = 0; n < n_node; n++) { jp0[n] = (int) np; np += d->J_n[n]; }
@@ -1212,6 +1265,18 @@ int check_plan(const h2gpu_image* im, const h2gpu_desc* d, const HostPlan& hp, l
             if (t.out0_row >= 0) prod.push_back({t.out0_row, t.nrow});
             if (t.out1_row >= 0) prod.push_back({t.out1_row, t.ncol});
         }
+    // the one-RHS kernel gives the leading blk1_small tasks of a list one warp each
+    for (int li = 0; li < 2; li++)
+    {
+        const std::vector<BlkTask>& ts = li == 0 ? hp.blkB : hp.blkD;
+        for (int pi = 0; pi < 2; pi++)
+        {
+            const int ns = im->blk1_small[li][pi];
+            REQ(ns >= 0 && ns <= (int) ts.size(), "plan: bad count of one-warp stored-block tasks");
+            for (int i = 0; i < ns; i++)
+                REQ(blk1_fits(ts[i].nrow, ts[i].ncol, pi == 0 ? 8 : 4), "plan: one-warp stored-block task too large");
+        }
+    }
     for (const std::vector<JitTarget>* v : {&hp.jtN, &hp.jtF})
         for (const JitTarget& t : *v) (t.out_y1 ? y1w : prod).push_back({t.out_row, (long long) kd * t.npt});
     TRY(check_space("one-sided", prod, y1w, hp.at, hp.at_slots, hp.y1t, hp.y1_slots));
@@ -1684,10 +1749,12 @@ int run_panel(h2gpu_image* im, int NV, int nv, const double* X, long long x_rs, 
             CK(launch_up<float>(NV, im->d_up + b, n, im->d_U32, im->d_XS, s, sweep_tc(im)));
         }
         if (timed) CK(cudaEventRecord(e[3], s));
-        CK(launch_pair(im->kernel_id, NV, im->d_owF, im->n_owF, im->d_pp, im->d_pts32, kp, im->d_XS, im->d_PS, s, 1));
+        CK(launch_pair(im->kernel_id, NV, im->d_owF, im->n_owF, im->d_pp, im->d_pts32, kp, im->d_XS, im->d_PS, s,
+                       im->far_diff ? 0 : 1, im->d_pts32lo));
         CK(launch_panel_in(NV, im->d_pg, im->n_pg_pts, im->n_pg - im->n_pg_pts, im->d_XS, im->d_pin, s));
         CK(launch_jit(im->kernel_id, 1, NV, im->d_jtF2, im->n_jtF2, im->d_js, im->d_pts32, kp, 1, 1, im->d_XS,
-                      im->d_PS, im->d_Y1, s, 1, im->d_ppts, im->d_pin, im->d_tiles));
+                      im->d_PS, im->d_Y1, s, im->far_diff ? 0 : 1, im->d_ppts, im->d_pin, im->d_tiles, im->d_pts32lo,
+                      im->d_pplo));
         CK(launch_y1sum(NV, im->d_y1t2, im->n_y12, im->d_y1_slots2, im->d_PS, im->d_Y1, s));
         if (timed) CK(cudaEventRecord(e[4], s));
         for (size_t L = 0; L + 1 < im->dn_beg.size(); L++)
@@ -1719,8 +1786,10 @@ int run_panel(h2gpu_image* im, int NV, int nv, const double* X, long long x_rs, 
                                xs_rows, im->d_PS, s, im->d_status));
             im->st.n_launches += 2;   // the second pass and the split of the inputs
         }
-        else if (f32) CK(launch_blk<float>(NV, im->d_blkD, im->n_blkD, im->d_D32, im->d_XS, im->d_PS, s, im->blk_tc, im->d_status));
-        else CK(launch_blk<double>(NV, im->d_blkD, im->n_blkD, im->d_D64, im->d_XS, im->d_PS, s));
+        else if (f32) CK(launch_blk<float>(NV, im->d_blkD, im->n_blkD, im->d_D32, im->d_XS, im->d_PS, s, im->blk_tc, im->d_status,
+                                           im->blk1_small[1][1]));
+        else CK(launch_blk<double>(NV, im->d_blkD, im->n_blkD, im->d_D64, im->d_XS, im->d_PS, s, 0, nullptr,
+                                   im->blk1_small[1][0]));
     } else {
         const bool panels = f32 && panels_used(im, NV);
         if (panels) CK(launch_panel_in(NV, im->d_pg, 0, im->n_pg_pts, im->d_XS, im->d_pin, s));
@@ -1749,14 +1818,17 @@ int run_panel(h2gpu_image* im, int NV, int nv, const double* X, long long x_rs, 
                                im->d_status));
             im->st.n_launches += 2;   // the second pass and the split of the inputs
         }
-        else if (f32) CK(launch_blk<float>(NV, im->d_blkB, im->n_blkB, im->d_B32, im->d_XS, im->d_PS, s, im->blk_tc, im->d_status));
-        else CK(launch_blk<double>(NV, im->d_blkB, im->n_blkB, im->d_B64, im->d_XS, im->d_PS, s));
+        else if (f32) CK(launch_blk<float>(NV, im->d_blkB, im->n_blkB, im->d_B32, im->d_XS, im->d_PS, s, im->blk_tc, im->d_status,
+                                           im->blk1_small[0][1]));
+        else CK(launch_blk<double>(NV, im->d_blkB, im->n_blkB, im->d_B64, im->d_XS, im->d_PS, s, 0, nullptr,
+                                   im->blk1_small[0][0]));
         CK(launch_y1sum(NV, im->d_y1t, im->n_y1, im->d_y1_slots, im->d_PS, im->d_Y1, s));
     } else {
         const bool panels = f32 && panels_used(im, NV);
         if (panels) CK(launch_panel_in(NV, im->d_pg, im->n_pg_pts, im->n_pg - im->n_pg_pts, im->d_XS, im->d_pin, s));
         CK(launch_jit(im->kernel_id, f32, NV, im->d_jtF, im->n_jtF, im->d_js, f32 ? (const void*) im->d_pts32 : (const void*) im->d_pts64,
-                      kparam_of(im), f32 ? 1 : 0, im->jit_tc, im->d_XS, im->d_PS, im->d_Y1, s, 1, im->d_ppts, im->d_pin, im->d_tiles));
+                      kparam_of(im), f32 ? 1 : 0, im->jit_tc, im->d_XS, im->d_PS, im->d_Y1, s, im->far_diff ? 0 : 1,
+                      im->d_ppts, im->d_pin, im->d_tiles, im->d_pts32lo, im->d_pplo));
         im->st.n_launches += panels ? 1 : 0;
     }
     if (timed) CK(cudaEventRecord(e[4], s));

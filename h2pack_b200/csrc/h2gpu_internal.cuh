@@ -58,6 +58,16 @@ struct BlkTask {
     int out0_row, out1_row;   // -1: product not needed
 };
 
+// Stored-block tasks of one right-hand side (k_blk1) small enough for one warp: at most
+// 256 columns, 512 rows and 128 KB of block values.  The plan puts them first in each
+// block-task list (those within the FP64 limit, then those within the FP32 limit only).
+constexpr int kBlk1WarpCols = 256, kBlk1WarpRows = 512;
+constexpr long long kBlk1WarpBytes = 128 * 1024;
+__host__ __device__ inline bool blk1_fits(int nrow, int ncol, int elem_bytes)
+{
+    return ncol <= kBlk1WarpCols && nrow <= kBlk1WarpRows && (long long) nrow * ncol * elem_bytes <= kBlk1WarpBytes;
+}
+
 // Unit of the wide-panel stored-block passes: one 64-row chunk of a task (pass 0,
 // A V over all column tiles) or one 64-column tile of a task (pass 1, A^T W over all of
 // the task's rows).

@@ -364,22 +364,126 @@ __device__ __forceinline__ void chunk_apply(const TA* __restrict__ A, int R, int
         for (int i = threadIdx.x; i < R * NV; i += kThreads) out0[i] = s_o0[i];
 }
 
-// Stored block (task of up to 1024 rows), single right-hand side (the matvec path,
-// memory bound).  The task is walked in chunks of 64 rows; warp w owns rows
-// 8w..8w+7 of a chunk and its lanes sweep the columns 32*CPL at a time (CPL = 1: with
-// two columns per lane the FP32 copy measured 1.7x slower, latency-bound).  A v completes per lane across the sweep and is combined with one transposed
-// butterfly per chunk (no cross-warp sum: the warp owns its rows); the 8 warps'
-// partials of A^T w are summed in warp order through shared memory every 256 columns
-// and added into the task's single out1 slot (stored by the first chunk, added by
-// the later ones; the same thread owns the same column in every chunk).
+// Stored blocks, single right-hand side (the matvec path, memory bound).  One launch.
+// A task of at most 256 columns, 512 rows and 128 KB (blk1_fits: the B blocks of the
+// usual leaf sizes, and their D blocks in FP32) is one warp's, 8 per CTA.  The lane owns
+// columns lane + 32j; their A^T w sums (and, for FP32 blocks, their inputs) live in the
+// warp's rows of shared memory for the whole block (only the lane touches its columns:
+// no barrier; registers stay free for the loads in flight).  The rows are walked 8
+// at a time with all of a pass's loads in flight (FP32: two 32-column passes, 16 loads
+// per lane), and the 8 rows' A v partials are combined with one transposed butterfly.
+// Every warp runs its own task, so 24 independent load chains per SM hide each other's
+// latency (one CTA per task left long serial chains of task, input, block loads,
+// barriers and output per ~100 KB block).  Larger tasks get a CTA each (blk1_cta): one
+// warp per 200 KB FP64 block measured slower (fewer warps than slots in the last
+// wave).  The plan orders each task list small-first; n_small is the count for TA.
+// Sums: FP64 blocks in FP64; FP32 blocks in FP32 over one pass (8 rows, or the <= 8
+// column passes of a row) and widened per sum.
 template <typename TA>
-__global__ void __launch_bounds__(256, 3) k_blk1(const BlkTask* __restrict__ tasks, const TA* __restrict__ arena,
-                                              const double* __restrict__ XS, double* __restrict__ PS)
+__device__ __forceinline__ void blk1_warp(const BlkTask& T, const TA* __restrict__ arena,
+                                          const double* __restrict__ XS, double* __restrict__ PS,
+                                          double* __restrict__ sq, float* __restrict__ sv, int lane)
+{
+    constexpr bool F32 = sizeof(TA) == 4;
+    constexpr int PASS = F32 ? 2 : 1;          // 32-column passes whose loads are issued together
+    const int ncol = T.ncol, nrow = T.nrow;
+    const bool do0 = T.out0_row >= 0, do1 = T.out1_row >= 0;
+    const int J = (ncol + 31) >> 5;
+    const TA* A = arena + T.a_off;
+#pragma unroll
+    for (int j = 0; j < 8; j++)
+    {
+        const int c = lane + 32 * j;
+        sq[c] = 0.0;
+        if constexpr (F32) sv[c] = (do0 && c < ncol) ? (float) XS[T.in0_row + c] : 0.f;
+    }
+    for (int r0 = 0; r0 < nrow; r0 += 8)
+    {
+        const int nr = min(8, nrow - r0);
+        double wr[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) wr[k] = (do1 && k < nr) ? XS[T.in1_row + r0 + k] : 0.0;
+        double p[8];
+        float pf[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) { p[k] = 0.0; pf[k] = 0.f; }
+#pragma unroll 1
+        for (int j0 = 0; j0 < J; j0 += PASS)
+        {
+            TA a[PASS][8];
+#pragma unroll
+            for (int u = 0; u < PASS; u++)
+            {
+                const int c = lane + 32 * (j0 + u);
+                const bool cv = c < ncol;
+#pragma unroll
+                for (int k = 0; k < 8; k++) a[u][k] = (cv && k < nr) ? A[(long long) (r0 + k) * ncol + c] : TA(0);
+            }
+#pragma unroll
+            for (int u = 0; u < PASS; u++)
+            {
+                const int j = j0 + u;
+                if constexpr (F32)
+                {
+                    const float v = sv[lane + 32 * j];
+                    float q = 0.f;
+#pragma unroll
+                    for (int k = 0; k < 8; k++)
+                    {
+                        q = fmaf(a[u][k], (float) wr[k], q);
+                        pf[k] = fmaf(a[u][k], v, pf[k]);
+                    }
+                    sq[lane + 32 * j] += (double) q;
+                } else {
+                    const int c = lane + 32 * j;
+                    const double v = (do0 && c < ncol) ? XS[T.in0_row + c] : 0.0;
+                    double q = 0.0;
+#pragma unroll
+                    for (int k = 0; k < 8; k++)
+                    {
+                        q = fma(to_d(a[u][k]), wr[k], q);
+                        p[k] = fma(to_d(a[u][k]), v, p[k]);
+                    }
+                    sq[lane + 32 * j] += q;
+                }
+            }
+        }
+        if (do0)
+        {
+            if constexpr (F32)
+            {
+#pragma unroll
+                for (int k = 0; k < 8; k++) p[k] = (double) pf[k];
+            }
+            warp_transpose_reduce<8>(p, lane);
+            const int row = nv_of_lane<8>(lane);
+            if (lane_writes<8>(lane) && row < nr) PS[T.out0_row + r0 + row] = p[0];
+        }
+    }
+    if (do1)
+    {
+#pragma unroll
+        for (int j = 0; j < 8; j++)
+        {
+            const int c = lane + 32 * j;
+            if (c < ncol) PS[T.out1_row + c] = sq[c];
+        }
+    }
+}
+
+// A task walked by the whole CTA (chunks of 64 rows; warp w owns rows 8w..8w+7 of a
+// chunk and its lanes sweep the columns 32 at a time).  A v completes per lane across
+// the sweep and is combined with one transposed butterfly per chunk; the 8 warps'
+// partials of A^T w are summed in warp order through shared memory every 256 columns
+// and added into the task's single out1 slot (stored by the first chunk, added by the
+// later ones; the same thread owns the same column in every chunk).
+template <typename TA>
+__device__ __forceinline__ void blk1_cta(const BlkTask& T, const TA* __restrict__ arena,
+                                         const double* __restrict__ XS, double* __restrict__ PS,
+                                         double (*s_q)[256])
 {
     constexpr int CPL = 1;
     constexpr int CW = 256;                       // columns per shared reduction of A^T w
-    __shared__ double s_q[kWarps][CW];
-    const BlkTask T = tasks[blockIdx.x];
     const int ncol = T.ncol, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const bool do0 = T.out0_row >= 0, do1 = T.out1_row >= 0;
     for (int rc = 0; rc < T.nrow; rc += 64)
@@ -471,6 +575,36 @@ __global__ void __launch_bounds__(256, 3) k_blk1(const BlkTask* __restrict__ tas
             const int row = nv_of_lane<8>(lane);
             if (lane_writes<8>(lane) && row < nr) PS[T.out0_row + r0 + row] = p[0];
         }
+    }
+}
+
+
+// CTAs [0, ceil(n_small / 8)): 8 small tasks each, one per warp; the rest: one larger
+// task each (tasks [n_small, n)).
+template <typename TA>
+__global__ void __launch_bounds__(256, 3) k_blk1(const BlkTask* __restrict__ tasks, int n, int n_small,
+                                              const TA* __restrict__ arena, const double* __restrict__ XS,
+                                              double* __restrict__ PS)
+{
+    __shared__ double s_q[kWarps][256];
+    __shared__ float s_v[sizeof(TA) == 4 ? kWarps : 1][256];
+    const int nw = (n_small + kWarps - 1) / kWarps;
+    if ((int) blockIdx.x < nw)
+    {
+        const int w = threadIdx.x >> 5;
+        const int t = blockIdx.x * kWarps + w;
+        if (t < n_small)
+        {
+            const BlkTask T = tasks[t];
+            blk1_warp<TA>(T, arena, XS, PS, s_q[w], s_v[sizeof(TA) == 4 ? w : 0], threadIdx.x & 31);
+        }
+        return;
+    }
+    const int t = n_small + (int) blockIdx.x - nw;
+    if (t < n)
+    {
+        const BlkTask T = tasks[t];
+        blk1_cta<TA>(T, arena, XS, PS, s_q);
     }
 }
 
@@ -3074,7 +3208,7 @@ static cudaError_t allow_smem(K kern, int bytes)
 
 template <typename TA>
 cudaError_t launch_blk(int NV, const BlkTask* t, int n, const TA* arena, const double* XS, double* PS, cudaStream_t st,
-                       int use_tc, int* status)
+                       int use_tc, int* status, int n_small)
 {
     if constexpr (sizeof(TA) == 4)
     {
@@ -3131,7 +3265,8 @@ cudaError_t launch_blk(int NV, const BlkTask* t, int n, const TA* arena, const d
         {
             k_blk_gemm<TA, NVc><<<n, 256, 0, st>>>(t, arena, XS, PS);
         } else if constexpr (NVc == 1) {
-            k_blk1<TA><<<n, 256, 0, st>>>(t, arena, XS, PS);
+            const int ns = n_small < 0 ? 0 : (n_small > n ? n : n_small);
+            k_blk1<TA><<<(ns + kWarps - 1) / kWarps + (n - ns), 256, 0, st>>>(t, n, ns, arena, XS, PS);
         } else {
             constexpr int b = chunk_smem_bytes<NVc>();
             cudaError_t e = allow_smem(k_blk<TA, NVc>, b);
@@ -3402,8 +3537,8 @@ cudaError_t launch_gen(int kid, int kd, int fp32, const GenTask* t, int n, const
 
 template cudaError_t launch_up<double>(int, const UpTask*, int, const double*, double*, cudaStream_t, int);
 template cudaError_t launch_up<float>(int, const UpTask*, int, const float*, double*, cudaStream_t, int);
-template cudaError_t launch_blk<double>(int, const BlkTask*, int, const double*, const double*, double*, cudaStream_t, int, int*);
-template cudaError_t launch_blk<float>(int, const BlkTask*, int, const float*, const double*, double*, cudaStream_t, int, int*);
+template cudaError_t launch_blk<double>(int, const BlkTask*, int, const double*, const double*, double*, cudaStream_t, int, int*, int);
+template cudaError_t launch_blk<float>(int, const BlkTask*, int, const float*, const double*, double*, cudaStream_t, int, int*, int);
 template cudaError_t launch_down<double>(int, const DownTask*, int, const double*, const double*, double*, double*, cudaStream_t, int);
 template cudaError_t launch_down<float>(int, const DownTask*, int, const float*, const double*, double*, double*, cudaStream_t, int);
 

@@ -17,7 +17,8 @@ template <typename TA>
 cudaError_t launch_up(int NV, const UpTask* t, int n, const TA* U, double* XS, cudaStream_t st, int use_tc = 0);
 template <typename TA>
 cudaError_t launch_blk(int NV, const BlkTask* t, int n, const TA* arena, const double* XS, double* PS, cudaStream_t st,
-                       int use_tc = 0, int* status = nullptr);   // use_tc: 1 mma.sync, 2 tcgen05
+                       int use_tc = 0, int* status = nullptr,    // use_tc: 1 mma.sync, 2 tcgen05
+                       int n_small = 0);   // NV 1: leading tasks that blk1_fits for TA (one warp each)
 // 64-wide panels of FP32 stored blocks on tcgen05: pass 0 (mode 0, units = 64-row chunks:
 // A V) or pass 1 (mode 1, units = 64-column tiles: A^T W), outputs written once
 cudaError_t launch_blk_wide(int mode, const BlkTask* t, const WideUnit* u, int n, const float* arena,
