@@ -421,16 +421,17 @@ int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
             for (int k = 0; k < d->n_child[n]; k++) s += d->U_ncol[d->children[n * d->max_child + k]];
             REQ(nr == s, "node %d: U has %d rows, children ranks sum to %d", n, nr, s);
         }
-        u_off[n] = ue;
-        ue += (long long) nr * nc;
+        u_off[n] = ue;                                  // a multiple of 4: every stride is
+        ue += (long long) nr * ((nc + 3) & ~3);
     }
     std::vector<double>& U = hp.U;
-    U.resize(ue);
+    U.assign(ue, 0.0);                                  // zero padding
     for (int n = 0; n < n_node; n++)
     {
         int nr = d->U_nrow[n], nc = d->U_ncol[n], ld = d->U_ld[n];
         if (nr == 0 || nc == 0 || lvl[n] < min_adm) continue;
-        for (int r = 0; r < nr; r++) memcpy(&U[u_off[n] + (long long) r * nc], d->U[n] + (size_t) r * ld, 8 * nc);
+        const int ld4 = (nc + 3) & ~3;
+        for (int r = 0; r < nr; r++) memcpy(&U[u_off[n] + (long long) r * ld4], d->U[n] + (size_t) r * ld, 8 * nc);
     }
     im->U_elems = ue;
 
@@ -450,7 +451,7 @@ int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
                 UpTask t;
                 t.u_off = u_off[n];
                 t.nrow = nr;
-                t.ld = nc;
+                t.ld = (nc + 3) & ~3;
                 t.c0 = c0;
                 t.nc = std::min(64, nc - c0);
                 t.in_row = d->n_child[n] == 0 ? mc[2 * n] : N + y0r[d->children[n * d->max_child]];
@@ -967,7 +968,8 @@ int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
             for (int r0 = 0; r0 < nr; r0 += RD)
             {
                 DownTask t;
-                t.u_off = u_off[n] + (long long) r0 * nc;
+                t.ld = (nc + 3) & ~3;
+                t.u_off = u_off[n] + (long long) r0 * t.ld;
                 t.nrow = std::min(RD, nr - r0); t.ncol = nc;
                 t.y1_row = has_y1[n] ? y0r[n] : -1;
                 t.push_row = push ? y0r[n] : -1;
@@ -1173,11 +1175,12 @@ int check_plan(const h2gpu_image* im, const h2gpu_desc* d, const HostPlan& hp, l
 
     // ---- upward: per node (keyed by its U offset) every column swept once
     std::map<long long, std::vector<int>> ucols;
-    std::map<long long, std::pair<int, int>> ushape;   // U offset -> (rows, columns)
+    std::map<long long, std::pair<int, int>> ushape;   // U offset -> (rows, row stride)
     for (const UpTask& t : hp.up)
     {
         REQ(t.nrow >= 1 && t.ld >= 1 && t.nc >= 1 && t.nc <= 64 && t.c0 >= 0 && t.c0 % 64 == 0 && t.c0 + t.nc <= t.ld,
             "plan: upward task with a bad column tile");
+        REQ(t.u_off % 4 == 0 && t.ld % 4 == 0, "plan: U not aligned for 16-byte rows");
         auto ins = ushape.emplace(t.u_off, std::make_pair(t.nrow, t.ld));
         REQ(ins.first->second == std::make_pair(t.nrow, t.ld), "plan: upward tasks of one node disagree on its U");
         std::vector<int>& c = ucols[t.u_off];
@@ -1188,9 +1191,14 @@ int check_plan(const h2gpu_image* im, const h2gpu_desc* d, const HostPlan& hp, l
         REQ(t.in_row >= N || (long long) t.in_row + t.nrow <= N, "plan: upward input straddles x and y0");
     }
     long long u_total = 0;
+    std::map<long long, int> ucount;                   // U offset -> columns (the rest is padding)
     for (const auto& kv : ucols)
     {
-        for (int v : kv.second) REQ(v == 1, "plan: a column of U is swept %d times upward", v);
+        int nc = 0;
+        while (nc < (int) kv.second.size() && kv.second[nc] == 1) nc++;
+        for (int j = nc; j < (int) kv.second.size(); j++)
+            REQ(kv.second[j] == 0 && j - nc < 3, "plan: a column of U is swept %d times upward", kv.second[j]);
+        ucount[kv.first] = nc;
         u_total += (long long) ushape[kv.first].first * ushape[kv.first].second;
     }
     REQ(u_total == (long long) im->U_elems, "plan: upward tasks cover %lld of %lld U elements", u_total,
@@ -1206,10 +1214,10 @@ int check_plan(const h2gpu_image* im, const h2gpu_desc* d, const HostPlan& hp, l
         REQ(it != ushape.begin(), "plan: downward task before the U arena");
         --it;
         const long long base = it->first;
-        const int nr = it->second.first, nc = it->second.second;
-        REQ(nc == t.ncol && (t.u_off - base) % nc == 0 && (t.u_off - base) / nc + t.nrow <= nr,
+        const int nr = it->second.first, ld = it->second.second;
+        REQ(t.ld == ld && ucount[base] == t.ncol && (t.u_off - base) % ld == 0 && (t.u_off - base) / ld + t.nrow <= nr,
             "plan: downward task outside its node's U");
-        spans.push_back({t.u_off, t.u_off + (long long) t.nrow * t.ncol});
+        spans.push_back({t.u_off, t.u_off + (long long) t.nrow * t.ld});
         REQ(t.y1_row < 0 || (long long) t.y1_row + t.ncol <= Y0, "plan: downward y1 rows outside y0");
         REQ(t.push_row < 0 || (long long) t.push_row + t.ncol <= Y0, "plan: downward push rows outside y0");
         if (!t.dst_ps) REQ(mark_rows(push, t.dst_row, t.nrow), "plan: push-down rows outside y0");
@@ -1572,6 +1580,8 @@ int check_plan(const h2gpu_image* im, const h2gpu_desc* d, const HostPlan& hp, l
 }
 
 
+KParam kparam_of(const h2gpu_image* im);
+
 int upload_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
 {
     TRY(upload(hp.U, &im->d_U64, im->bytes));
@@ -1610,7 +1620,7 @@ int upload_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
         // the point half of the panels is static
         CK(cudaMalloc(&im->d_ppts, sizeof(float4) * 8 * (size_t) im->n_pg));
         im->bytes += sizeof(float4) * 8 * (size_t) im->n_pg;
-        CK(launch_panel_pts(im->d_pg, im->n_pg, im->d_pts32, im->d_ppts, im->stream));
+        CK(launch_panel_pts(im->d_pg, im->n_pg, im->d_pts32, kparam_of(im).sigma, im->d_ppts, im->stream));
         if (im->d_pts32lo)
         {
             CK(cudaMalloc(&im->d_pplo, sizeof(float4) * 6 * (size_t) im->n_pg));
@@ -1695,12 +1705,20 @@ int panel_cap(const h2gpu_image* im)
 
 KParam kparam_of(const h2gpu_image* im)
 {
-    KParam k{0.0, 0.0};
+    KParam k{0.0, 0.0, 1.f, 0.f};
+    const float log2e = 1.4426950408889634f;
     switch (im->kernel_id)
     {
         case H2GPU_KRNL_COULOMB: k.p0 = im->n_kp > 0 ? im->kp[0] : 0.0; break;
-        case H2GPU_KRNL_GAUSSIAN: k.p0 = im->kp[0]; break;
-        case H2GPU_KRNL_MATERN32: k.p0 = im->kp[0]; k.c0 = -1.7320508075688772 * im->kp[0]; break;
+        case H2GPU_KRNL_GAUSSIAN: k.p0 = im->kp[0]; k.sigma = (float) k.p0 * log2e; break;
+        case H2GPU_KRNL_MATERN32:
+        {
+            k.p0 = im->kp[0];
+            k.c0 = -1.7320508075688772 * im->kp[0];
+            const float q1 = (float) k.c0 * log2e;
+            k.sigma = q1 * q1;
+            break;
+        }
         case H2GPU_KRNL_RPY: k.p0 = im->kp[0]; k.c0 = 1.0 / (6.0 * M_PI * im->kp[0]); break;
     }
     return k;

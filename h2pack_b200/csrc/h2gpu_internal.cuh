@@ -21,9 +21,12 @@ namespace h2gpu {
 // Upward task, one tile of <= 64 columns of a node's U:
 //   XS[out_row + c][v] = sum_r U[r][c] * XS[in_row + r][v],  c0 <= c < c0 + nc
 // (H2P_matvec_fwd_transform, src/H2Pack_matvec.c:126-156)
+// U arena: every node's U row-major with its row stride rounded up to a multiple of 4
+// elements (zero padding) and its offset a multiple of 4, so that 16-byte loads of FP32
+// rows are aligned.
 struct UpTask {
     long long u_off;   // element offset of the node's U in the U arena (row-major)
-    int nrow, ld;      // rows of U, row stride (= columns of U)
+    int nrow, ld;      // rows of U, row stride (columns of U rounded up to a multiple of 4)
     int c0, nc;        // column tile
     int in_row;        // leaf: first row of its x slice; non-leaf: y0 row of its first child
     int out_row;       // y0 row of the node
@@ -35,6 +38,7 @@ struct UpTask {
 struct DownTask {
     long long u_off;          // element offset of the chunk's first row of U
     int nrow, ncol;
+    int ld;                   // row stride of U (as UpTask::ld)
     int y1_row;               // -1: the node has no admissible-pair contributions
     int push_row;             // -1: no push-down from the parent
     int dst_ps;               // 1: destination is a PS slot (leaf), 0: PUSH rows (children)
@@ -153,6 +157,8 @@ struct AsmTask {
 struct KParam {
     double p0;         // Coulomb: value on r == 0; Gaussian: l; Matern: l; RPY: eta
     double c0;         // derived constant (Matern: -sqrt(3) l; RPY: 1 / (6 pi eta))
+    float sigma;       // FP32 far field: the scale of r^2 its kernel form takes (ScalarFar)
+    float pad;
 };
 
 }  // namespace h2gpu

@@ -212,7 +212,7 @@ __global__ void __launch_bounds__(256) k_sweep_gemm(const UpTask* __restrict__ u
         out = XS + (long long) (T.out_row + T.c0) * NV;
     } else {
         const DownTask T = dns[blockIdx.x];
-        K = T.ncol; M = T.nrow; lda = T.ncol;
+        K = T.ncol; M = T.nrow; lda = T.ld;
         A = Uar + T.u_off;
         y1_row = T.y1_row; push_row = T.push_row;
         out = (T.dst_ps ? PS : PUSH) + (long long) T.dst_row * NV;
@@ -724,9 +724,9 @@ __global__ void __launch_bounds__(kThreads) k_down(const DownTask* __restrict__ 
     __shared__ double s_x[CW * NV];
     const DownTask t = tasks[blockIdx.x];
     const VFromY1 vin{Y1, PUSH, t.y1_row, t.push_row};
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, ncol = t.ncol;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, ncol = t.ncol, ld = t.ld;
     const int r0 = 8 * w, nr = max(0, min(8, t.nrow - r0));
-    const TA* A = Uar + t.u_off + (long long) r0 * ncol;
+    const TA* A = Uar + t.u_off + (long long) r0 * ld;
     double p[NV][8];
 #pragma unroll
     for (int v = 0; v < NV; v++)
@@ -742,7 +742,7 @@ __global__ void __launch_bounds__(kThreads) k_down(const DownTask* __restrict__ 
         {
             TA a[8];
 #pragma unroll
-            for (int k = 0; k < 8; k++) a[k] = (k < nr) ? A[(long long) k * ncol + c] : TA(0);
+            for (int k = 0; k < 8; k++) a[k] = (k < nr) ? A[(long long) k * ld + c] : TA(0);
 #pragma unroll
             for (int k = 0; k < 8; k++)
 #pragma unroll
@@ -894,40 +894,33 @@ __device__ __forceinline__ void two_sum(float a, float s, float alo, float& hi, 
 }
 
 // FP32 kernel values for admissible (well-separated) pairs only: r2 > 0 always, so the
-// coincident-point cases drop out; constants are folded once per launch (prep).
+// coincident-point cases drop out.  They take r^2 scaled by KParam::sigma (the callers
+// scale |a|^2, -2a and the panels' |b|^2), which folds a constant multiply into the
+// r^2 form: Gaussian exp(-l r^2) = 2^-(sigma r^2) with sigma = l log2 e; Matern
+// (1 + s ln 2) 2^-s with s = sqrt(sigma r^2) = sqrt(3) log2 e r / l.  prep folds the
+// remaining constants once per launch.  f2: two values at once (packed FP32x2).
 template <int KID> struct ScalarFar;
-// f2: the same for two values at once with packed FP32x2 arithmetic (sm_100).
-template <> struct ScalarFar<KRNL_COULOMB_ID> {
+template <> struct ScalarFar<KRNL_COULOMB_ID> {    // sigma = 1
     static __device__ __forceinline__ void prep(float, float, float& q0, float& q1) { q0 = 0.f; q1 = 0.f; }
-    static __device__ __forceinline__ float f(float r2, float, float) { return rsqrt_approx(r2); }
     static __device__ __forceinline__ float2 f2(float2 r2, float, float)
     {
         return make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
     }
 };
 template <> struct ScalarFar<KRNL_GAUSSIAN_ID> {
-    static __device__ __forceinline__ void prep(float p0, float, float& q0, float& q1) { q0 = -p0 * kLog2e; q1 = 0.f; }
-    static __device__ __forceinline__ float f(float r2, float q0, float) { return ex2_approx(r2 * q0); }
-    static __device__ __forceinline__ float2 f2(float2 r2, float q0, float)
+    static __device__ __forceinline__ void prep(float, float, float& q0, float& q1) { q0 = 0.f; q1 = 0.f; }
+    static __device__ __forceinline__ float2 f2(float2 r2s, float, float)
     {
-        const float2 t = __fmul2_rn(r2, make_float2(q0, q0));
-        return make_float2(ex2_approx(t.x), ex2_approx(t.y));
+        return make_float2(ex2_approx(-r2s.x), ex2_approx(-r2s.y));
     }
 };
 template <> struct ScalarFar<KRNL_MATERN32_ID> {
-    static __device__ __forceinline__ void prep(float, float c0, float& q0, float& q1) { q0 = c0; q1 = c0 * kLog2e; }
-    static __device__ __forceinline__ float f(float r2, float q0, float q1)
+    static __device__ __forceinline__ void prep(float, float, float& q0, float& q1) { q0 = 0.6931471805599453f; q1 = 0.f; }
+    static __device__ __forceinline__ float2 f2(float2 r2s, float ln2, float)
     {
-        const float r = r2 * rsqrt_approx(r2);
-        const float e = ex2_approx(q1 * r);
-        return fmaf(-q0 * r, e, e);
-    }
-    static __device__ __forceinline__ float2 f2(float2 r2, float q0, float q1)
-    {
-        const float2 r = __fmul2_rn(r2, make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y)));
-        const float2 t = __fmul2_rn(r, make_float2(q1, q1));
-        const float2 e = make_float2(ex2_approx(t.x), ex2_approx(t.y));
-        return __ffma2_rn(__fmul2_rn(r, make_float2(-q0, -q0)), e, e);
+        const float2 s = __fmul2_rn(r2s, make_float2(rsqrt_approx(r2s.x), rsqrt_approx(r2s.y)));
+        const float2 e = make_float2(ex2_approx(-s.x), ex2_approx(-s.y));
+        return __fmul2_rn(__ffma2_rn(s, make_float2(ln2, ln2), make_float2(1.f, 1.f)), e);
     }
 };
 
@@ -1133,9 +1126,11 @@ __global__ void __launch_bounds__(64, NV >= 16 ? 8 : 10) k_jit2(const JitTarget*
         const float ax = x0.x + sc.sx, ay = x0.y + sc.sy, az = x0.z + sc.sz;
         const float bx = x1.x + sc.sx, by = x1.y + sc.sy, bz = x1.z + sc.sz;
         const float2 X = make_float2(ax, bx), Y = make_float2(ay, by), Z = make_float2(az, bz);
-        const float2 MX = make_float2(-2.f * ax, -2.f * bx), MY = make_float2(-2.f * ay, -2.f * by),
-                     MZ = make_float2(-2.f * az, -2.f * bz);
-        const float2 S2 = make_float2(ax * ax + ay * ay + az * az, bx * bx + by * by + bz * bz);
+        // far form, scaled by sigma (ScalarFar)
+        const float m2s = -2.f * kp.sigma;
+        const float2 MX = make_float2(m2s * ax, m2s * bx), MY = make_float2(m2s * ay, m2s * by),
+                     MZ = make_float2(m2s * az, m2s * bz);
+        const float2 S2 = make_float2(kp.sigma * (ax * ax + ay * ay + az * az), kp.sigma * (bx * bx + by * by + bz * bz));
         float2 XH = X, YH = Y, ZH = Z, XL = make_float2(0.f, 0.f), YL = XL, ZL = XL;
         if constexpr (EX)
         {
@@ -1150,7 +1145,7 @@ __global__ void __launch_bounds__(64, NV >= 16 ? 8 : 10) k_jit2(const JitTarget*
             if (threadIdx.x < nj)
             {
                 float4 q = pts[sc.pt0 + j0 + threadIdx.x];
-                if (FAR) q.w = q.x * q.x + q.y * q.y + q.z * q.z;
+                if (FAR) q.w = kp.sigma * (q.x * q.x + q.y * q.y + q.z * q.z);
                 if constexpr (EX)
                 {
                     const float4 ql = plo[sc.pt0 + j0 + threadIdx.x];
@@ -1245,11 +1240,12 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 // Source panels of k_jit_tc (one PanelGroup per 8 points of a source set).
-// Points: per group 8 float4, entry [t][0] = {x, x', y, y'}, [t][1] = {z, z', |p|^2, |p'|^2}
+// Points: per group 8 float4, entry [t][0] = {x, x', y, y'}, [t][1] = {z, z', s|p|^2, s|p'|^2}
+// (s = KParam::sigma, the far field's scale of r^2)
 // of the set's points 8g + t and 8g + t + 4 (t < 4): the two sources of one B-fragment
 // register pair, as FP32x2 operands.  Points past the set's end are far away (their
 // inputs are zero).
-__global__ void k_panel_pts(const PanelGroup* __restrict__ pg, int n, const float4* __restrict__ pts,
+__global__ void k_panel_pts(const PanelGroup* __restrict__ pg, int n, const float4* __restrict__ pts, float sigma,
                             float4* __restrict__ out)
 {
     const long long e = blockIdx.x * (long long) blockDim.x + threadIdx.x;
@@ -1257,7 +1253,7 @@ __global__ void k_panel_pts(const PanelGroup* __restrict__ pg, int n, const floa
     const int g = (int) (e >> 3), j = (int) (e & 7), t = j & 3, h = j >> 2;
     const PanelGroup G = pg[g];
     float4 q = (j < G.nvalid) ? pts[G.pt0 + j] : make_float4(1e6f, 1e6f, 1e6f, 0.f);
-    q.w = q.x * q.x + q.y * q.y + q.z * q.z;
+    q.w = sigma * (q.x * q.x + q.y * q.y + q.z * q.z);
     float* d = reinterpret_cast<float*>(out + 8LL * g + 2 * t);
     d[h] = q.x; d[2 + h] = q.y; d[4 + h] = q.z; d[6 + h] = q.w;
 }
@@ -1428,12 +1424,14 @@ __global__ void __launch_bounds__(256, 4) k_jit_tc(const JitTarget* __restrict__
                 const int ge = min(r.ng, h + 8);
                 if constexpr (FAR)
                 {
-                    // -2a and |a|^2 of each target in the source set's frame, broadcast
-                    const float2 max2 = make_float2(-2.f * ax, -2.f * ax), may2 = make_float2(-2.f * ay, -2.f * ay),
-                                 maz2 = make_float2(-2.f * az, -2.f * az);
-                    const float2 mbx2 = make_float2(-2.f * bx, -2.f * bx), mby2 = make_float2(-2.f * by, -2.f * by),
-                                 mbz2 = make_float2(-2.f * bz, -2.f * bz);
-                    const float sa2 = ax * ax + ay * ay + az * az, sb2 = bx * bx + by * by + bz * bz;
+                    // -2a and |a|^2 of each target in the source set's frame, scaled by
+                    // sigma as the panels' |b|^2 (ScalarFar), broadcast
+                    const float m2s = -2.f * kp.sigma;
+                    const float2 max2 = make_float2(m2s * ax, m2s * ax), may2 = make_float2(m2s * ay, m2s * ay),
+                                 maz2 = make_float2(m2s * az, m2s * az);
+                    const float2 mbx2 = make_float2(m2s * bx, m2s * bx), mby2 = make_float2(m2s * by, m2s * by),
+                                 mbz2 = make_float2(m2s * bz, m2s * bz);
+                    const float sa2 = kp.sigma * (ax * ax + ay * ay + az * az), sb2 = kp.sigma * (bx * bx + by * by + bz * bz);
                     const float2 sa22 = make_float2(sa2, sa2), sb22 = make_float2(sb2, sb2);
 #pragma unroll 2
                     for (int grp = h; grp < ge; grp++)
@@ -1603,7 +1601,7 @@ __global__ void __launch_bounds__(32 * kPairWarps, 3) k_jit_pair(const PairOwner
         if (threadIdx.x < TS)
         {
             float4 q = rp;
-            if (FAR) q.w = q.x * q.x + q.y * q.y + q.z * q.z;   // |b|^2 for the far form of r^2
+            if (FAR) q.w = kp.sigma * (q.x * q.x + q.y * q.y + q.z * q.z);   // s |b|^2 for the far form of r^2
             sm.pt[buf][threadIdx.x] = q;
             if constexpr (EX) sm.lo[buf][threadIdx.x] = rl;
         }
@@ -1676,10 +1674,12 @@ __global__ void __launch_bounds__(32 * kPairWarps, 3) k_jit_pair(const PairOwner
             {
                 const float ax = x0.x + pb.sx, ay = x0.y + pb.sy, az = x0.z + pb.sz;
                 const float bx = x1.x + pb.sx, by = x1.y + pb.sy, bz = x1.z + pb.sz;
-                // rows (g, g+8) of a as packed pairs; far form: -2a and |a|^2 in b's frame
-                const float2 m_x = make_float2(-2.f * ax, -2.f * bx), m_y = make_float2(-2.f * ay, -2.f * by),
-                             m_z = make_float2(-2.f * az, -2.f * bz);
-                const float2 s2 = make_float2(ax * ax + ay * ay + az * az, bx * bx + by * by + bz * bz);
+                // rows (g, g+8) of a as packed pairs; far form: -2a and |a|^2 in b's frame,
+                // scaled by sigma (ScalarFar)
+                const float m2s = -2.f * kp.sigma;
+                const float2 m_x = make_float2(m2s * ax, m2s * bx), m_y = make_float2(m2s * ay, m2s * by),
+                             m_z = make_float2(m2s * az, m2s * bz);
+                const float2 s2 = make_float2(kp.sigma * (ax * ax + ay * ay + az * az), kp.sigma * (bx * bx + by * by + bz * bz));
                 // exact-difference form: rows (g, g+8) of a as hi + lo pairs in b's frame
                 float2 hx = make_float2(ax, bx), hy = make_float2(ay, by), hz = make_float2(az, bz);
                 float2 lx = make_float2(0.f, 0.f), ly = lx, lz = lx;
@@ -2862,7 +2862,7 @@ __global__ void __launch_bounds__(256, 4) k_sweep_tc(const UpTask* __restrict__ 
     const int v0 = STRIDE == NV ? 0 : 16 * (int) blockIdx.y;
     constexpr int KT = 32;
     constexpr int ROWS = UP ? KT : 64, LD = UP ? 72 : 36;   // padded: conflict-free fragment reads
-    __shared__ float s_u[2][ROWS][LD];
+    __shared__ __align__(16) float s_u[2][ROWS][LD];
     __shared__ uint4 s_x[2][4][32][2];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, tq = lane & 3;
     int K, M, lda, xrow = 0, y1_row = -1, push_row = -1;
@@ -2877,7 +2877,7 @@ __global__ void __launch_bounds__(256, 4) k_sweep_tc(const UpTask* __restrict__ 
         out = XS + (long long) (T.out_row + T.c0) * STRIDE + v0;
     } else {
         const DownTask T = dns[blockIdx.x];
-        K = T.ncol; M = T.nrow; lda = T.ncol;
+        K = T.ncol; M = T.nrow; lda = T.ld;
         A = Uar + T.u_off;
         y1_row = T.y1_row; push_row = T.push_row;
         out = (T.dst_ps ? PS : PUSH) + (long long) T.dst_row * STRIDE + v0;
@@ -2888,20 +2888,23 @@ __global__ void __launch_bounds__(256, 4) k_sweep_tc(const UpTask* __restrict__ 
         if (push_row >= 0) b += PUSH[(long long) (push_row + k) * STRIDE + v0 + v];
         return b;
     };
-    float ra[8];
+    // U tile: 512 float4 (16-byte loads: U rows are padded to a multiple of 4 elements with
+    // zeros and start on 16-byte boundaries, so a vector that starts inside a row stays in it)
+    float4 ra[2];
     uint4 rxh = make_uint4(0, 0, 0, 0), rxl = rxh;
     auto load_tile = [&](int k0) {
 #pragma unroll
-        for (int u = 0; u < 8; u++)
+        for (int u = 0; u < 2; u++)
         {
             const int e = threadIdx.x + 256 * u;
+            const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
             if constexpr (UP)
             {
-                const int k = e >> 6, m = e & 63;
-                ra[u] = (k0 + k < K && m < M) ? A[(long long) (k0 + k) * lda + m] : 0.f;
+                const int k = e >> 4, m = (e & 15) * 4;
+                ra[u] = (k0 + k < K && m < M) ? *reinterpret_cast<const float4*>(A + (long long) (k0 + k) * lda + m) : z;
             } else {
-                const int m = e >> 5, k = e & 31;
-                ra[u] = (m < M && k0 + k < K) ? A[(long long) m * lda + k0 + k] : 0.f;
+                const int m = e >> 3, k = (e & 7) * 4;
+                ra[u] = (m < M && k0 + k < K) ? *reinterpret_cast<const float4*>(A + (long long) m * lda + k0 + k) : z;
             }
         }
         if (warp < 4)
@@ -2925,11 +2928,11 @@ __global__ void __launch_bounds__(256, 4) k_sweep_tc(const UpTask* __restrict__ 
     };
     auto store_tile = [&](int buf) {
 #pragma unroll
-        for (int u = 0; u < 8; u++)
+        for (int u = 0; u < 2; u++)
         {
             const int e = threadIdx.x + 256 * u;
-            if constexpr (UP) s_u[buf][e >> 6][e & 63] = ra[u];
-            else s_u[buf][e >> 5][e & 31] = ra[u];
+            if constexpr (UP) *reinterpret_cast<float4*>(&s_u[buf][e >> 4][(e & 15) * 4]) = ra[u];
+            else *reinterpret_cast<float4*>(&s_u[buf][e >> 3][(e & 7) * 4]) = ra[u];
         }
         if (warp < 4) { s_x[buf][warp][lane][0] = rxh; s_x[buf][warp][lane][1] = rxl; }
     };
@@ -3427,11 +3430,11 @@ cudaError_t launch_jit(int kid, int fp32, int NV, const JitTarget* tg, int n, co
 #undef H2G_JIT_ARGS
 }
 
-cudaError_t launch_panel_pts(const PanelGroup* pg, int n, const float4* pts, float4* ppts, cudaStream_t st)
+cudaError_t launch_panel_pts(const PanelGroup* pg, int n, const float4* pts, float sigma, float4* ppts, cudaStream_t st)
 {
     if (n <= 0) return cudaSuccess;
     const long long t = 8LL * n;
-    k_panel_pts<<<(unsigned) ((t + 255) / 256), 256, 0, st>>>(pg, n, pts, ppts);
+    k_panel_pts<<<(unsigned) ((t + 255) / 256), 256, 0, st>>>(pg, n, pts, sigma, ppts);
     return cudaGetLastError();
 }
 

@@ -42,7 +42,7 @@ cudaError_t launch_jit(int kid, int fp32, int NV, const JitTarget* tg, int n, co
                        const TileRec* tiles = nullptr, const float4* lo = nullptr, const float4* plo = nullptr);
 // source panels: the points (once per image) and the inputs of groups [g0, g0 + n) for a
 // panel of NV right-hand sides (NV 8 / 16; other widths do nothing)
-cudaError_t launch_panel_pts(const PanelGroup* pg, int n, const float4* pts, float4* ppts, cudaStream_t st);
+cudaError_t launch_panel_pts(const PanelGroup* pg, int n, const float4* pts, float sigma, float4* ppts, cudaStream_t st);
 // the low parts of the panel points (6 float4 per group)
 cudaError_t launch_panel_lo(const PanelGroup* pg, int n, const float4* lo, float4* out, cudaStream_t st);
 cudaError_t launch_panel_in(int NV, const PanelGroup* pg, int g0, int n, const double* XS, uint4* pin, cudaStream_t st);
