@@ -128,6 +128,10 @@ struct h2gpu_image {
     double* d_B64 = nullptr;
     float* d_B32 = nullptr;
     size_t B_elems = 0;
+    size_t B32_elems = 0, D32_elems = 0;   // FP32 arenas (rows padded, BlkTask)
+    // per block: FP64 offset (H2Pack's packing), FP32 offset, rows, columns ([0] B, [1] D)
+    struct BlkMap { long long off64, off32; int nrow, ncol; };
+    std::vector<BlkMap> bmap[2];
     double* d_D64 = nullptr;
     float* d_D32 = nullptr;
     size_t D_elems = 0;
@@ -379,6 +383,20 @@ struct HostPlan {
     std::vector<TileRec> tiles;
 };
 
+// FP32 arena offsets of n blocks stored one after the other with rows of f32_ld(ncol)
+// elements (every offset a multiple of 4); returns the arena's element count
+long long pack_f32(int n, const int* nrow, const int* ncol, std::vector<long long>& off)
+{
+    off.assign(n, 0);
+    long long e = 0;
+    for (int i = 0; i < n; i++)
+    {
+        off[i] = e;
+        e += (long long) nrow[i] * f32_ld(ncol[i]);
+    }
+    return e;
+}
+
 int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
 {
     const int kd = d->krnl_dim, N = kd * d->n_point, n_node = d->n_node, min_adm = d->min_adm_level;
@@ -489,6 +507,14 @@ int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
 
     if (!d->BD_JIT)
     {
+        std::vector<long long> off32B, off32D;
+        im->B32_elems = (size_t) pack_f32(d->n_B, d->B_nrow, d->B_ncol, off32B);
+        im->D32_elems = (size_t) pack_f32(d->n_D, d->D_nrow, d->D_ncol, off32D);
+        for (int k = 0; k < 2; k++) im->bmap[k].clear();
+        for (int i = 0; i < d->n_B; i++)
+            im->bmap[0].push_back({(long long) d->B_ptr[i], off32B[i], d->B_nrow[i], d->B_ncol[i]});
+        for (int i = 0; i < d->n_D; i++)
+            im->bmap[1].push_back({(long long) d->D_ptr[i], off32D[i], d->D_nrow[i], d->D_ncol[i]});
         for (int i = 0; i < d->n_B; i++)
         {
             int n0 = d->r_adm_pairs[2 * i], n1 = d->r_adm_pairs[2 * i + 1];
@@ -514,6 +540,7 @@ int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
                 t.a_off = (long long) d->B_ptr[i] + (long long) r0 * nc;
                 t.nrow = rr; t.ncol = nc; t.in0_row = in0; t.in1_row = in1 + r0;
                 t.out0_row = s0 + r0; t.out1_row = s1;
+                t.ld32 = f32_ld(nc); t.a32 = off32B[i] + (long long) r0 * t.ld32; t.pad = 0;
                 blkB.push_back(t);
             }
         }
@@ -537,6 +564,7 @@ int build_plan(h2gpu_image* im, const h2gpu_desc* d, HostPlan& hp)
                 t.a_off = (long long) d->D_ptr[i] + (long long) r0 * nc;
                 t.nrow = rr; t.ncol = nc; t.in0_row = mc[2 * n1]; t.in1_row = mc[2 * n0] + r0;
                 t.out0_row = s0 + r0; t.out1_row = s1;
+                t.ld32 = f32_ld(nc); t.a32 = off32D[i] + (long long) r0 * t.ld32; t.pad = 0;
                 blkD.push_back(t);
             }
         }
@@ -1118,6 +1146,9 @@ int build_gen(const h2gpu_desc* d, GenPlan& g)
             g.pts[jp0[n] + j] = make_double4(J[j], J[nj + j], J[2 * nj + j], rad ? J[3 * nj + j] : 0.0);
     }
     const int GR = 16;   // row points per task
+    std::vector<long long> off32B, off32D;
+    pack_f32(d->n_B, d->B_nrow, d->B_ncol, off32B);
+    pack_f32(d->n_D, d->D_nrow, d->D_ncol, off32D);
     auto emit = [&](std::vector<GenTask>& out, size_t off, int rp0, int nrp, int cp0, int ncp, int nrow, int ncol,
                     const char* what, int i) {
         REQ(nrow == kd * nrp && ncol == kd * ncp, "%s block %d is %dx%d, its points give %dx%d", what, i, nrow, ncol,
@@ -1128,6 +1159,7 @@ int build_gen(const h2gpu_desc* d, GenPlan& g)
         {
             GenTask t;
             t.a_off = (long long) off + (long long) kd * r0 * (long long) ncol;
+            t.a32 = (what[0] == 'B' ? off32B[i] : off32D[i]) + (long long) kd * r0 * (long long) f32_ld(ncol);
             t.row_pt0 = rp0 + r0;
             t.nrp = std::min(GR, nrp - r0);
             t.col_pt0 = cp0;
@@ -1268,6 +1300,9 @@ int check_plan(const h2gpu_image* im, const h2gpu_desc* d, const HostPlan& hp, l
             REQ(t.nrow >= 1 && t.ncol >= 1, "plan: stored-block task with a bad shape");
             const long long elems = (long long) (v == &hp.blkB ? im->B_elems : im->D_elems);
             REQ(t.a_off >= 0 && t.a_off + (long long) t.nrow * t.ncol <= elems, "plan: stored-block task outside its arena");
+            const long long elems32 = (long long) (v == &hp.blkB ? im->B32_elems : im->D32_elems);
+            REQ(t.ld32 == f32_ld(t.ncol) && t.a32 >= 0 && t.a32 % 4 == 0 && t.a32 + (long long) t.nrow * t.ld32 <= elems32,
+                "plan: stored-block task outside its FP32 arena");
             REQ(t.in0_row >= 0 && (long long) t.in0_row + t.ncol <= N + Y0, "plan: stored-block input outside the input space");
             REQ(t.in1_row >= 0 && (long long) t.in1_row + t.nrow <= N + Y0, "plan: stored-block input outside the input space");
             if (t.out0_row >= 0) prod.push_back({t.out0_row, t.nrow});
@@ -1650,6 +1685,30 @@ __global__ void k_to_f32(const double* __restrict__ a, float* __restrict__ b, si
         b[i] = (float) a[i];
 }
 
+// FP32 copy of a stored-block arena in the padded layout: one CTA per block task (the
+// tasks of a list cover every block row once), padding written as zeros
+__global__ void k_blk_to_f32(const BlkTask* __restrict__ tasks, const double* __restrict__ a, float* __restrict__ b)
+{
+    const BlkTask t = tasks[blockIdx.x];
+    const long long n = (long long) t.nrow * t.ld32;
+    for (long long i = threadIdx.x; i < n; i += blockDim.x)
+    {
+        const int r = (int) (i / t.ld32), c = (int) (i % t.ld32);
+        b[t.a32 + i] = c < t.ncol ? (float) a[t.a_off + (long long) r * t.ncol + c] : 0.f;
+    }
+}
+
+int make_f32_blocks(h2gpu_image* im, const BlkTask* tasks, int n, const double* src, float** dst, size_t n32)
+{
+    if (n32 == 0 || *dst) return H2GPU_OK;
+    CK(cudaMalloc(dst, 4 * n32));
+    if (n > 0) k_blk_to_f32<<<n, 256, 0, im->stream>>>(tasks, src, *dst);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(im->stream));
+    im->bytes += 4 * n32;
+    return H2GPU_OK;
+}
+
 int make_f32(h2gpu_image* im, const double* src, float** dst, size_t n)
 {
     if (n == 0 || *dst) return H2GPU_OK;
@@ -1898,27 +1957,30 @@ int generate_blocks(h2gpu_image* im, const GenPlan& g)
         if ((st = upload(all, &tasks, dummy)) != H2GPU_OK) break;
         void* B = nullptr;
         void* D = nullptr;
+        const size_t nB = fp32 ? im->B32_elems : im->B_elems, nD = fp32 ? im->D32_elems : im->D_elems;
         cudaError_t e = cudaSuccess;
-        if (im->B_elems) e = cudaMalloc(&B, es * im->B_elems);
-        if (e == cudaSuccess) e = cudaMalloc(&D, es * im->D_elems);
+        if (nB) e = cudaMalloc(&B, es * nB);
+        if (e == cudaSuccess) e = cudaMalloc(&D, es * std::max<size_t>(nD, 1));
         if (e != cudaSuccess)
         {
             if (B) cudaFree(B);
-            st = fail(H2GPU_ERR_NOMEM, "stored-block arenas of %.1f GB do not fit on the device",
-                      1e-9 * es * (im->B_elems + im->D_elems));
+            st = fail(H2GPU_ERR_NOMEM, "stored-block arenas of %.1f GB do not fit on the device", 1e-9 * es * (nB + nD));
             break;
         }
         if (fp32) { im->d_B32 = (float*) B; im->d_D32 = (float*) D; im->f32_only = 1; }
         else { im->d_B64 = (double*) B; im->d_D64 = (double*) D; }
-        im->bytes += es * (im->B_elems + im->D_elems);
+        im->bytes += es * (nB + nD);
+        // the FP32 rows' padding stays zero (the kernels read it through 16-byte loads)
+        if (fp32 && nB) e = cudaMemsetAsync(B, 0, es * nB, im->stream);
+        if (fp32 && nD && e == cudaSuccess) e = cudaMemsetAsync(D, 0, es * nD, im->stream);
         const KParam kp = kparam_of(im);
         // one launch per block kind, in slices that keep the grid inside its limits
-        const int nB = (int) g.tB.size(), nD = (int) g.tD.size();
+        const int tB = (int) g.tB.size(), tD = (int) g.tD.size();
         const int slice = 1 << 24;
-        for (int b = 0; b < nB && e == cudaSuccess; b += slice)
-            e = launch_gen(im->kernel_id, im->kd, fp32, tasks + b, std::min(slice, nB - b), pts, kp, B, im->stream);
-        for (int b = 0; b < nD && e == cudaSuccess; b += slice)
-            e = launch_gen(im->kernel_id, im->kd, fp32, tasks + nB + b, std::min(slice, nD - b), pts, kp, D, im->stream);
+        for (int b = 0; b < tB && e == cudaSuccess; b += slice)
+            e = launch_gen(im->kernel_id, im->kd, fp32, tasks + b, std::min(slice, tB - b), pts, kp, B, im->stream);
+        for (int b = 0; b < tD && e == cudaSuccess; b += slice)
+            e = launch_gen(im->kernel_id, im->kd, fp32, tasks + tB + b, std::min(slice, tD - b), pts, kp, D, im->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(im->stream);
         if (e != cudaSuccess) st = fail(H2GPU_ERR_CUDA, "stored-block generation failed: %s", cudaGetErrorString(e));
     } while (0);
@@ -1936,8 +1998,8 @@ int prepare(h2gpu_image* im, int NV)
     if (im->precision == H2GPU_PREC_MIXED)
     {
         TRY(make_f32(im, im->d_U64, &im->d_U32, im->U_elems));
-        TRY(make_f32(im, im->d_B64, &im->d_B32, im->B_elems));
-        TRY(make_f32(im, im->d_D64, &im->d_D32, im->D_elems));
+        TRY(make_f32_blocks(im, im->d_blkB, im->n_blkB, im->d_B64, &im->d_B32, im->B32_elems));
+        TRY(make_f32_blocks(im, im->d_blkD, im->n_blkD, im->d_D64, &im->d_D32, im->D32_elems));
         if (im->d_ppts && !im->d_pin)
         {
             const size_t b = sizeof(uint4) * 64 * (size_t) im->n_pg;   // panels of up to 16 right-hand sides
@@ -2221,11 +2283,6 @@ H2G_API int h2gpu_permute_vector(h2gpu_image* im, int forward, const double* x, 
     return h2gpu_permute_matrix_rows(im, forward, H2GPU_COL_MAJOR, 1, x, im->N, px, im->N);
 }
 
-__global__ void k_f32_to_f64(const float* __restrict__ a, double* __restrict__ b, size_t n)
-{
-    for (size_t i = blockIdx.x * (size_t) blockDim.x + threadIdx.x; i < n; i += (size_t) gridDim.x * blockDim.x)
-        b[i] = (double) a[i];
-}
 
 H2G_API int h2gpu_get_blocks(h2gpu_image* im, int which, double* host, size_t n_elems)
 {
@@ -2244,21 +2301,33 @@ H2G_API int h2gpu_get_blocks(h2gpu_image* im, int which, double* host, size_t n_
         CK(cudaMemcpy(host, d64, 8 * n, cudaMemcpyDeviceToHost));
         return H2GPU_OK;
     }
-    // widen on the device in slices of 64 M elements
-    const size_t slice = (size_t) 1 << 26;
-    double* tmp = nullptr;
-    CK(cudaMalloc(&tmp, 8 * std::min(n, slice)));
+    // the FP32 arena (padded rows, blocks in order) in runs of whole blocks of up to 64 M
+    // elements: copied to the host, widened and unpadded into H2Pack's packing
+    const std::vector<h2gpu_image::BlkMap>& bm = im->bmap[which];
+    const size_t cap = std::max<size_t>((size_t) 1 << 26, [&] {
+        size_t m = 0;
+        for (const auto& b : bm) m = std::max(m, (size_t) b.nrow * f32_ld(b.ncol));
+        return m;
+    }());
+    std::vector<float> tmp(cap);
     int st = H2GPU_OK;
-    for (size_t b = 0; b < n && st == H2GPU_OK; b += slice)
+    for (size_t i0 = 0; i0 < bm.size() && st == H2GPU_OK;)
     {
-        const size_t m = std::min(slice, n - b);
-        k_f32_to_f64<<<148 * 8, 256, 0, im->stream>>>(d32 + b, tmp, m);
-        cudaError_t e = cudaGetLastError();
-        if (e == cudaSuccess) e = cudaMemcpyAsync(host + b, tmp, 8 * m, cudaMemcpyDeviceToHost, im->stream);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(im->stream);
-        if (e != cudaSuccess) st = fail(H2GPU_ERR_CUDA, "block copy failed: %s", cudaGetErrorString(e));
+        size_t i1 = i0, m = 0;
+        while (i1 < bm.size() && m + (size_t) bm[i1].nrow * f32_ld(bm[i1].ncol) <= cap)
+            m += (size_t) bm[i1].nrow * f32_ld(bm[i1].ncol), i1++;
+        cudaError_t e = cudaMemcpy(tmp.data(), d32 + bm[i0].off32, 4 * m, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) { st = fail(H2GPU_ERR_CUDA, "block copy failed: %s", cudaGetErrorString(e)); break; }
+        for (size_t i = i0; i < i1; i++)
+        {
+            const auto& b = bm[i];
+            const int ld = f32_ld(b.ncol);
+            const float* srow = tmp.data() + (b.off32 - bm[i0].off32);
+            for (int r = 0; r < b.nrow; r++)
+                for (int c = 0; c < b.ncol; c++) host[b.off64 + (long long) r * b.ncol + c] = srow[(long long) r * ld + c];
+        }
+        i0 = i1;
     }
-    cudaFree(tmp);
     return st;
 }
 

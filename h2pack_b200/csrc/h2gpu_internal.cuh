@@ -55,11 +55,19 @@ struct Y1Task {
 //                           PS[out1_row + c] = A[:, c]^T * XS[in1_row : +nrow]
 // One read of the block feeds both products, as CBLAS_BI_GEMV does
 // (src/H2Pack_matvec.c:26-65, used at :333-379 and :929-932).
+// Stored-block arenas: the FP64 arena keeps H2Pack's packing (B_ptr / D_ptr, rows of
+// ncol elements); the FP32 arena pads every row to a multiple of 4 elements with zeros
+// and starts every block on a 16-byte boundary, so FP32 rows take 16-byte loads.
+__host__ __device__ inline int f32_ld(int ncol) { return (ncol + 3) & ~3; }
+
 struct BlkTask {
-    long long a_off;   // element offset of the chunk's first row in the block arena
-    int nrow, ncol;    // rows in this chunk, columns (= leading dimension)
+    long long a_off;   // element offset of the chunk's first row in the FP64 arena
+    int nrow, ncol;    // rows in this chunk, columns (= the FP64 row stride)
     int in0_row, in1_row;
     int out0_row, out1_row;   // -1: product not needed
+    long long a32;     // element offset of the chunk's first row in the FP32 arena
+    int ld32;          // FP32 row stride, f32_ld(ncol)
+    int pad;
 };
 
 // Stored-block tasks of one right-hand side (k_blk1) small enough for one warp: at most
@@ -140,11 +148,12 @@ struct PairPartner {
 // A[kd i + a][kd j + b] = K_ab(row point i, column point j), packed row-major with
 // ld = kd * ncp at the block's offset in H2Pack's B / D packing.
 struct GenTask {
-    long long a_off;   // element offset of the task's first row in the block arena
+    long long a_off;   // element offset of the task's first row in the FP64 arena (ld = kd * ncp)
     int row_pt0;       // point-space index of the task's first row point
     int nrp;           // row points in this task (<= 16)
     int col_pt0;       // point-space index of the block's first column point
     int ncp;           // column points of the block
+    long long a32;     // ... in the FP32 arena (ld = f32_ld(kd * ncp))
 };
 
 // Final assembly of a leaf: Y[fwd[row0 + r]][v] = sum_s PS[slot_s + r][v]

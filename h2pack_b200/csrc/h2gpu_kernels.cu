@@ -30,6 +30,21 @@ constexpr unsigned kFull = 0xffffffffu;
 
 template <int NV> struct SV { static constexpr int v = (NV > 1) ? NV + 1 : 1; };  // padded smem row stride
 
+// A stored-block task's offset and row stride in the arena of element type TA (the FP32
+// arena pads its rows, BlkTask)
+template <typename TA>
+__device__ __forceinline__ long long blk_off(const BlkTask& T)
+{
+    if constexpr (sizeof(TA) == 4) return T.a32;
+    else return T.a_off;
+}
+template <typename TA>
+__device__ __forceinline__ int blk_ld(const BlkTask& T)
+{
+    if constexpr (sizeof(TA) == 4) return T.ld32;
+    else return T.ncol;
+}
+
 __device__ __forceinline__ double to_d(double x) { return x; }
 __device__ __forceinline__ double to_d(float x) { return (double) x; }
 
@@ -292,7 +307,7 @@ template <int NV>
 constexpr int chunk_smem_bytes() { return 8 * (64 * SV<NV>::v + 32 * SV<NV>::v + 64 * NV + kWarps * 32 * NV); }
 
 template <typename TA, int NV, typename VIN>
-__device__ __forceinline__ void chunk_apply(const TA* __restrict__ A, int R, int ncol, VIN vin,
+__device__ __forceinline__ void chunk_apply(const TA* __restrict__ A, int R, int ncol, int lda, VIN vin,
                                             const double* __restrict__ win_XS, int win_row,
                                             double* __restrict__ out0, double* __restrict__ out1,
                                             double* __restrict__ smem, bool add1 = false)
@@ -325,7 +340,7 @@ __device__ __forceinline__ void chunk_apply(const TA* __restrict__ A, int R, int
         for (int v = 0; v < NV; v++) acc1[v] = 0.0;
         for (int r = w; r < R; r += kWarps)
         {
-            double a = cin ? to_d(A[(long long) r * ncol + c]) : 0.0;
+            double a = cin ? to_d(A[(long long) r * lda + c]) : 0.0;
             if (do1)
             {
 #pragma unroll
@@ -389,7 +404,8 @@ __device__ __forceinline__ void blk1_warp(const BlkTask& T, const TA* __restrict
     const int ncol = T.ncol, nrow = T.nrow;
     const bool do0 = T.out0_row >= 0, do1 = T.out1_row >= 0;
     const int J = (ncol + 31) >> 5;
-    const TA* A = arena + T.a_off;
+    const TA* A = arena + blk_off<TA>(T);
+    const int lda = blk_ld<TA>(T);
 #pragma unroll
     for (int j = 0; j < 8; j++)
     {
@@ -417,7 +433,7 @@ __device__ __forceinline__ void blk1_warp(const BlkTask& T, const TA* __restrict
                 const int c = lane + 32 * (j0 + u);
                 const bool cv = c < ncol;
 #pragma unroll
-                for (int k = 0; k < 8; k++) a[u][k] = (cv && k < nr) ? A[(long long) (r0 + k) * ncol + c] : TA(0);
+                for (int k = 0; k < 8; k++) a[u][k] = (cv && k < nr) ? A[(long long) (r0 + k) * lda + c] : TA(0);
             }
 #pragma unroll
             for (int u = 0; u < PASS; u++)
@@ -490,7 +506,7 @@ __device__ __forceinline__ void blk1_cta(const BlkTask& T, const TA* __restrict_
     {
         const int nr = max(0, min(8, min(64, T.nrow - rc) - 8 * w));   // rows of this warp
         const int r0 = rc + 8 * w;
-        const TA* A = arena + T.a_off + (long long) r0 * ncol;
+        const TA* A = arena + blk_off<TA>(T) + (long long) r0 * blk_ld<TA>(T);
         double wr[8];
 #pragma unroll
         for (int k = 0; k < 8; k++) wr[k] = (do1 && k < nr) ? XS[T.in1_row + r0 + k] : 0.0;
@@ -517,7 +533,7 @@ __device__ __forceinline__ void blk1_cta(const BlkTask& T, const TA* __restrict_
                     cv[j] = c[j] < cend;
                     vc[j] = (do0 && cv[j]) ? XS[T.in0_row + c[j]] : 0.0;
 #pragma unroll
-                    for (int k = 0; k < 8; k++) a[j][k] = (cv[j] && k < nr) ? A[(long long) k * ncol + c[j]] : TA(0);
+                    for (int k = 0; k < 8; k++) a[j][k] = (cv[j] && k < nr) ? A[(long long) k * blk_ld<TA>(T) + c[j]] : TA(0);
                 }
                 if constexpr (sizeof(TA) == 4)
                 {
@@ -631,7 +647,8 @@ __global__ void __launch_bounds__(256) k_blk_gemm(const BlkTask* __restrict__ ta
     // the task's rows in chunks of RT; the chunks' C1 parts add into one slot
     for (int rc = 0; rc < T.nrow; rc += RT)
     {
-    const TA* A = arena + T.a_off + (long long) rc * ncol;
+    const int lda = blk_ld<TA>(T);
+    const TA* A = arena + blk_off<TA>(T) + (long long) rc * lda;
     const int R = min(RT, T.nrow - rc);
     double acc0[VPT0];
 #pragma unroll
@@ -649,7 +666,7 @@ __global__ void __launch_bounds__(256) k_blk_gemm(const BlkTask* __restrict__ ta
         for (int i = t; i < RT * CT; i += 256)
         {
             int r = i / CT, c = i % CT;
-            sA[r][c] = (r < R && ct + c < ncol) ? to_d(A[(long long) r * ncol + ct + c]) : 0.0;
+            sA[r][c] = (r < R && ct + c < ncol) ? to_d(A[(long long) r * lda + ct + c]) : 0.0;
         }
         if (do0)
             for (int i = t; i < CT * NV; i += 256)
@@ -703,7 +720,8 @@ __global__ void __launch_bounds__(kThreads) k_blk(const BlkTask* __restrict__ ta
     // the task's rows in chunks of 64; the chunks' A^T w parts add into one slot
     for (int rc = 0; rc < t.nrow; rc += 64)
     {
-        chunk_apply<TA, NV>(arena + t.a_off + (long long) rc * t.ncol, min(64, t.nrow - rc), t.ncol, vin, XS,
+        chunk_apply<TA, NV>(arena + blk_off<TA>(t) + (long long) rc * blk_ld<TA>(t), min(64, t.nrow - rc), t.ncol,
+                            blk_ld<TA>(t), vin, XS,
                             t.in1_row + rc, t.out0_row >= 0 ? PS + (long long) (t.out0_row + rc) * NV : nullptr,
                             t.out1_row >= 0 ? PS + (long long) t.out1_row * NV : nullptr, dsm, rc > 0);
         __syncthreads();
@@ -1890,7 +1908,7 @@ __global__ void __launch_bounds__(256, 3) k_blk_tc(const BlkTask* __restrict__ t
 
     for (int rc = 0; rc < T.nrow; rc += 64)
     {
-        const float* A = arena + T.a_off + (long long) rc * ncol;
+        const float* A = arena + T.a32 + (long long) rc * T.ld32;
         const int R = min(64, T.nrow - rc);
         __syncthreads();
         if (do1)
@@ -1906,7 +1924,7 @@ __global__ void __launch_bounds__(256, 3) k_blk_tc(const BlkTask* __restrict__ t
                 {
                     const int e = threadIdx.x + 256 * u, r = e >> 6, c = e & 63;
                     const bool in = r < R && c0 + c < ncol;
-                    const float* src = in ? A + (long long) r * ncol + c0 + c : A;
+                    const float* src = in ? A + (long long) r * T.ld32 + c0 + c : A;
                     asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;"
                                  ::"r"(smem_u32(dst + r * S + c)), "l"(src), "r"(in ? 4 : 0) : "memory");
                 }
@@ -2139,7 +2157,7 @@ __global__ void __launch_bounds__(kBf3Threads, 5) k_blk_bf3(const BlkTask* __res
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const bool do0 = T.out0_row >= 0, do1 = T.out1_row >= 0;
     const int ntc = (ncol + 63) / 64, nt = ntc * ((nrow + 63) / 64);
-    const float* A0 = arena + T.a_off;
+    const float* A0 = arena + T.a32;
 
     if (warp == 0)
     {
@@ -2166,7 +2184,7 @@ __global__ void __launch_bounds__(kBf3Threads, 5) k_blk_bf3(const BlkTask* __res
     float rv[8], rw[8];
     auto load_tile = [&](int t) {
         const int rc = (t / ntc) * 64, c0 = (t % ntc) * 64, R = min(64, nrow - rc);
-        const float* A = A0 + (long long) rc * ncol + c0;
+        const float* A = A0 + (long long) rc * T.ld32 + c0;
 #pragma unroll
         for (int u = 0; u < 4; u++)
         {
@@ -2175,7 +2193,7 @@ __global__ void __launch_bounds__(kBf3Threads, 5) k_blk_bf3(const BlkTask* __res
             for (int j = 0; j < 8; j++)
             {
                 const int c = 8 * q + j;
-                ra[u][j] = (r < R && c0 + c < ncol) ? A[(long long) r * ncol + c] : 0.f;
+                ra[u][j] = (r < R && c0 + c < ncol) ? A[(long long) r * T.ld32 + c] : 0.f;
             }
         }
         const int n = tid >> 3, q = tid & 7;          // V^T / W^T granule: row n, k = 8q .. 8q+7
@@ -2369,7 +2387,7 @@ __global__ void __launch_bounds__(kBf3Threads, 2) k_blk_bf3w(const BlkTask* __re
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const bool do0 = T.out0_row >= 0, do1 = T.out1_row >= 0;
     const int ntc = (ncol + 63) / 64, nt = ntc * ((nrow + 63) / 64);
-    const float* A0 = arena + T.a_off;
+    const float* A0 = arena + T.a32;
 
     if (warp == 0)
     {
@@ -2397,7 +2415,7 @@ __global__ void __launch_bounds__(kBf3Threads, 2) k_blk_bf3w(const BlkTask* __re
     float rv[VG][8], rw[VG][8];
     auto load_tile = [&](int t) {
         const int rc = (t / ntc) * 64, c0 = (t % ntc) * 64, R = min(64, nrow - rc);
-        const float* A = A0 + (long long) rc * ncol + c0;
+        const float* A = A0 + (long long) rc * T.ld32 + c0;
 #pragma unroll
         for (int u = 0; u < 4; u++)
         {
@@ -2406,7 +2424,7 @@ __global__ void __launch_bounds__(kBf3Threads, 2) k_blk_bf3w(const BlkTask* __re
             for (int j = 0; j < 8; j++)
             {
                 const int c = 8 * q + j;
-                ra[u][j] = (r < R && c0 + c < ncol) ? A[(long long) r * ncol + c] : 0.f;
+                ra[u][j] = (r < R && c0 + c < ncol) ? A[(long long) r * T.ld32 + c] : 0.f;
             }
         }
 #pragma unroll
@@ -2692,30 +2710,33 @@ __global__ void __launch_bounds__(kWideThreads, 2) k_blk_wide(const BlkTask* __r
         const int ncol = T.ncol, nrow = T.nrow;
         // the unit's fixed 64-row chunk (pass 0) or 64-column tile (pass 1), and the tiles it walks
         const int nt = MODE == 0 ? (ncol + 63) / 64 : (nrow + 63) / 64;
-        const float* A0 = arena + T.a_off;
+        const float* A0 = arena + T.a32;
+        const int lda = T.ld32;
         auto tile_of = [&](int t, int& rc, int& c0) {
             if (MODE == 0) { rc = U.off; c0 = 64 * t; }
             else { rc = 64 * t; c0 = U.off; }
         };
         // the A tile is loaded into registers (thread t: 2 granules, row r, 8 consecutive
-        // columns q) and split into shared memory; the right-hand-side pieces of a tile are
-        // copied from XS3 by cp.async into one of two stages (rows past the tile's extent
-        // zero-filled)
-        float ra[2][8];
+        // columns q, as two 16-byte loads: FP32 rows are padded to 16 bytes with zeros, so
+        // a vector that starts before the row's end stays in the row) and split into shared
+        // memory; the right-hand-side pieces of a tile are copied from XS3 by cp.async into
+        // one of two stages (rows past the tile's extent zero-filled)
+        float4 ra[2][2];
         auto load_a = [&](int t) {
             int rc, c0;
             tile_of(t, rc, c0);
             const int R = min(64, nrow - rc), C = min(64, ncol - c0);
-            const float* A = A0 + (long long) rc * ncol + c0;
+            const float* A = A0 + (long long) rc * lda + c0;
 #pragma unroll
             for (int u = 0; u < 2; u++)
             {
                 const int gi = tid + kWideThreads * u, r = gi >> 3, q = gi & 7;
 #pragma unroll
-                for (int j = 0; j < 8; j++)
+                for (int h = 0; h < 2; h++)
                 {
-                    const int c = 8 * q + j;
-                    ra[u][j] = (r < R && c < C) ? A[(long long) r * ncol + c] : 0.f;
+                    const int c = 8 * q + 4 * h;
+                    ra[u][h] = (r < R && c < C) ? *reinterpret_cast<const float4*>(A + (long long) r * lda + c)
+                                                : make_float4(0.f, 0.f, 0.f, 0.f);
                 }
             }
         };
@@ -2739,8 +2760,10 @@ __global__ void __launch_bounds__(kWideThreads, 2) k_blk_wide(const BlkTask* __r
             {
                 const int gi = tid + kWideThreads * u, r = gi >> 3, q = gi & 7;
                 uint32_t h[4], m[4], l[4];
-#pragma unroll
-                for (int j = 0; j < 4; j++) bf16x3_pair(ra[u][2 * j], ra[u][2 * j + 1], h[j], m[j], l[j]);
+                bf16x3_pair(ra[u][0].x, ra[u][0].y, h[0], m[0], l[0]);
+                bf16x3_pair(ra[u][0].z, ra[u][0].w, h[1], m[1], l[1]);
+                bf16x3_pair(ra[u][1].x, ra[u][1].y, h[2], m[2], l[2]);
+                bf16x3_pair(ra[u][1].z, ra[u][1].w, h[3], m[3], l[3]);
                 const int off = sw128(r, q);
                 *reinterpret_cast<uint4*>(a_b + off) = make_uint4(h[0], h[1], h[2], h[3]);
                 *reinterpret_cast<uint4*>(a_b + 8192 + off) = make_uint4(m[0], m[1], m[2], m[3]);
@@ -3051,7 +3074,9 @@ __global__ void __launch_bounds__(kGenThreads) k_gen(const GenTask* __restrict__
     __shared__ double4 s_row[16];
     const GenTask t = tasks[blockIdx.x];
     const int tid = threadIdx.x;
-    const long long ld = (long long) KD * t.ncp;
+    // FP64: H2Pack's packing; FP32: rows padded to 16 bytes (the padding is zeroed by the host)
+    const long long ld = sizeof(TO) == 4 ? (long long) f32_ld(KD * t.ncp) : (long long) KD * t.ncp;
+    const long long a0 = sizeof(TO) == 4 ? t.a32 : t.a_off;
     if (tid < t.nrp) s_row[tid] = pts[t.row_pt0 + tid];
     __syncthreads();
     for (int j0 = 0; j0 < t.ncp; j0 += kGenThreads)
@@ -3059,7 +3084,7 @@ __global__ void __launch_bounds__(kGenThreads) k_gen(const GenTask* __restrict__
         const int j = j0 + tid;
         if (j >= t.ncp) break;
         const double4 q = pts[t.col_pt0 + j];
-        TO* col = arena + t.a_off + (long long) KD * j;
+        TO* col = arena + a0 + (long long) KD * j;
         for (int i = 0; i < t.nrp; i++)
         {
             const double4 p = s_row[i];
