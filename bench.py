@@ -730,9 +730,10 @@ def run_served(args):
     for i in range(args.n_requests):
         name = f"m{int(rng.integers(n_mat))}"
         kind = "pcg" if rng.random() < 0.5 else "matvec"
-        # PCG solves stop at 0.9e-6 on the H2 operator, so that the residual against the
-        # exact operator (the H2 error included) stays within the requested 1e-6
-        base.append(Request(rid=i, matrix=name, kind=kind, arrival=float(arr[i]), tol=0.9e-6,
+        # PCG solves stop at 0.8e-6 on the H2 operator, so that the residual against the
+        # exact operator (the H2 error, amplified by (K + mu I)^-1, included) stays within
+        # the requested 1e-6 (at 0.9e-6 the FP64 solves ended at 1.03e-6)
+        base.append(Request(rid=i, matrix=name, kind=kind, arrival=float(arr[i]), tol=0.8e-6,
                             b=torch.randn(Hs[name].N, dtype=torch.float64, device="cuda", generator=g)))
     out, done_by_prec = {}, {}
     for prec in [p for p in ("mixed", "fp64") if p in args.precisions.split(",")]:
