@@ -1256,6 +1256,8 @@ __device__ __forceinline__ void cp_async16(void* dst, const void* src)
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 // Source panels of k_jit_tc (one PanelGroup per 8 points of a source set).
 // Points: per group 8 float4, entry [t][0] = {x, x', y, y'}, [t][1] = {z, z', s|p|^2, s|p'|^2}
@@ -2871,8 +2873,10 @@ __global__ void __launch_bounds__(kWideThreads, 2) k_blk_wide(const BlkTask* __r
 //   upward   (UP):  C^T (NV x nc) = X^T (NV x nrow) U[:, c0 : c0 + nc]    B = U,   k = rows of U
 //   downward (!UP): C^T (NV x 64) = Y^T (NV x ncol) U[r0 : r0 + 64, :]^T  B = U^T, k = columns of U
 // (Y = the node's summed y1 plus the parent's push-down slice).  Warp w owns output
-// columns (UP) / rows (DOWN) 8w..8w+7.  The 32-deep k tiles of U and the X^T / Y^T
-// fragments are double-buffered through registers.
+// columns (UP) / rows (DOWN) 8w..8w+7.  The 32-deep k tiles of U come through a
+// three-stage shared-memory ring filled by 16-byte cp.async (two tiles in flight
+// without registers); the X^T / Y^T fragments are split by warps 0-3 one tile ahead
+// and double-buffered in shared memory.
 // STRIDE: row stride of the vector spaces.  A 64-wide panel (STRIDE = 64) runs as four
 // 16-column sub-panels, blockIdx.y = sub-panel (columns 16 blockIdx.y .. + 15).
 template <int NV, bool UP, int STRIDE = NV>
@@ -2883,9 +2887,9 @@ __global__ void __launch_bounds__(256, 4) k_sweep_tc(const UpTask* __restrict__ 
 {
     static_assert(STRIDE == NV || NV == 16, "sub-panels are 16 columns wide");
     const int v0 = STRIDE == NV ? 0 : 16 * (int) blockIdx.y;
-    constexpr int KT = 32;
+    constexpr int KT = 32, NS = 3;                          // tile depth, U ring stages
     constexpr int ROWS = UP ? KT : 64, LD = UP ? 72 : 36;   // padded: conflict-free fragment reads
-    __shared__ __align__(16) float s_u[2][ROWS][LD];
+    __shared__ __align__(16) float s_u[NS][ROWS][LD];
     __shared__ uint4 s_x[2][4][32][2];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, tq = lane & 3;
     int K, M, lda, xrow = 0, y1_row = -1, push_row = -1;
@@ -2911,27 +2915,37 @@ __global__ void __launch_bounds__(256, 4) k_sweep_tc(const UpTask* __restrict__ 
         if (push_row >= 0) b += PUSH[(long long) (push_row + k) * STRIDE + v0 + v];
         return b;
     };
-    // U tile: 512 float4 (16-byte loads: U rows are padded to a multiple of 4 elements with
-    // zeros and start on 16-byte boundaries, so a vector that starts inside a row stays in it)
-    float4 ra[2];
-    uint4 rxh = make_uint4(0, 0, 0, 0), rxl = rxh;
-    auto load_tile = [&](int k0) {
-#pragma unroll
-        for (int u = 0; u < 2; u++)
+    const int nt = (K + KT - 1) / KT;
+    // U tiles: a ring of NS stages filled by 16-byte cp.async (U rows are padded to a
+    // multiple of 4 elements with zeros and start on 16-byte boundaries, so a vector that
+    // starts inside a row stays in it; vectors past the tile's extent are zero-filled), so
+    // NS - 1 tiles are in flight without registers.  One commit group per tile (empty
+    // past the end), so that wait_group(NS - 2) means "tile t has landed".
+    auto issue_u = [&](int t) {
+        if (t < nt)
         {
-            const int e = threadIdx.x + 256 * u;
-            const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
-            if constexpr (UP)
+            const int k0 = t * KT;
+            float* st = &s_u[t % NS][0][0];
+#pragma unroll
+            for (int u = 0; u < 2; u++)
             {
-                const int k = e >> 4, m = (e & 15) * 4;
-                ra[u] = (k0 + k < K && m < M) ? *reinterpret_cast<const float4*>(A + (long long) (k0 + k) * lda + m) : z;
-            } else {
-                const int m = e >> 3, k = (e & 7) * 4;
-                ra[u] = (m < M && k0 + k < K) ? *reinterpret_cast<const float4*>(A + (long long) m * lda + k0 + k) : z;
+                const int e = threadIdx.x + 256 * u;
+                int r, c;
+                bool in;
+                if constexpr (UP) { r = e >> 4; c = (e & 15) * 4; in = k0 + r < K && c < M; }
+                else { r = e >> 3; c = (e & 7) * 4; in = r < M && k0 + c < K; }
+                const float* src = !in ? A : (UP ? A + (long long) (k0 + r) * lda + c : A + (long long) r * lda + k0 + c);
+                cp_async16_zfill(st + r * LD + c, src, in ? 16 : 0);
             }
         }
+        cp_async_commit();
+    };
+    // input fragments of a tile (warps 0-3, one k-step each), split into TF32 hi / lo
+    uint4 rxh = make_uint4(0, 0, 0, 0), rxl = rxh;
+    auto load_x = [&](int t) {
         if (warp < 4)
         {
+            const int k0 = t * KT;
             const int ka = k0 + 8 * warp + tq, kb = ka + 4;
             float v[4];
             v[0] = (ka < K && g < NV) ? (float) xin(ka, g) : 0.f;
@@ -2949,29 +2963,26 @@ __global__ void __launch_bounds__(256, 4) k_sweep_tc(const UpTask* __restrict__ 
             rxl = make_uint4(l[0], l[1], l[2], l[3]);
         }
     };
-    auto store_tile = [&](int buf) {
-#pragma unroll
-        for (int u = 0; u < 2; u++)
-        {
-            const int e = threadIdx.x + 256 * u;
-            if constexpr (UP) *reinterpret_cast<float4*>(&s_u[buf][e >> 4][(e & 15) * 4]) = ra[u];
-            else *reinterpret_cast<float4*>(&s_u[buf][e >> 3][(e & 7) * 4]) = ra[u];
-        }
+    auto store_x = [&](int buf) {
         if (warp < 4) { s_x[buf][warp][lane][0] = rxh; s_x[buf][warp][lane][1] = rxl; }
     };
 
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    if (K > 0)
+#pragma unroll
+    for (int t = 0; t < NS - 1; t++) issue_u(t);
+    if (nt > 0)
     {
-        load_tile(0);
-        store_tile(0);
+        load_x(0);
+        store_x(0);
     }
-    __syncthreads();
-    int buf = 0;
-    for (int k0 = 0; k0 < K; k0 += KT)
+    for (int t = 0; t < nt; t++)
     {
-        const bool more = k0 + KT < K;
-        if (more) load_tile(k0 + KT);
+        cp_async_wait_group<NS - 2>();     // this thread's copies of tile t have landed
+        __syncthreads();                   // everyone's; tile t - 1 (its stage, its x buffer) is no longer read
+        issue_u(t + NS - 1);               // into the stage tile t - 1 used
+        const bool more = t + 1 < nt;
+        if (more) load_x(t + 1);
+        const int st = t % NS, buf = t & 1;
         if (8 * warp < M)
         {
             float d[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
@@ -2982,11 +2993,11 @@ __global__ void __launch_bounds__(256, 4) k_sweep_tc(const UpTask* __restrict__ 
                 float b0, b1;
                 if constexpr (UP)
                 {
-                    b0 = s_u[buf][8 * ks + tq][8 * warp + g];
-                    b1 = s_u[buf][8 * ks + tq + 4][8 * warp + g];
+                    b0 = s_u[st][8 * ks + tq][8 * warp + g];
+                    b1 = s_u[st][8 * ks + tq + 4][8 * warp + g];
                 } else {
-                    b0 = s_u[buf][8 * warp + g][8 * ks + tq];
-                    b1 = s_u[buf][8 * warp + g][8 * ks + tq + 4];
+                    b0 = s_u[st][8 * warp + g][8 * ks + tq];
+                    b1 = s_u[st][8 * warp + g][8 * ks + tq + 4];
                 }
                 const uint32_t h0 = tf32_rna(b0), h1 = tf32_rna(b1);
                 const uint32_t l0 = __float_as_uint(b0 - __uint_as_float(h0)), l1 = __float_as_uint(b1 - __uint_as_float(h1));
@@ -2998,10 +3009,9 @@ __global__ void __launch_bounds__(256, 4) k_sweep_tc(const UpTask* __restrict__ 
 #pragma unroll
             for (int q = 0; q < 4; q++) acc[q] += (double) (d[0][q] + d[1][q]);
         }
-        if (more) store_tile(buf ^ 1);
-        __syncthreads();
-        buf ^= 1;
+        if (more) store_x(buf ^ 1);        // read by tile t + 1 after the next barrier
     }
+    cp_async_wait_all();
     // rows of the fragment = right-hand sides (g, g+8), columns = outputs (2tq, 2tq+1)
 #pragma unroll
     for (int q = 0; q < 4; q++)
