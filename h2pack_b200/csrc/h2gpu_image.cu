@@ -1762,26 +1762,28 @@ int panel_cap(const h2gpu_image* im)
     return std::min(im->max_nv, 16);
 }
 
-KParam kparam_of(const h2gpu_image* im)
+KParam kparam_from(int kernel_id, const double* kp, int n_kp)
 {
     KParam k{0.0, 0.0, 1.f, 0.f};
     const float log2e = 1.4426950408889634f;
-    switch (im->kernel_id)
+    switch (kernel_id)
     {
-        case H2GPU_KRNL_COULOMB: k.p0 = im->n_kp > 0 ? im->kp[0] : 0.0; break;
-        case H2GPU_KRNL_GAUSSIAN: k.p0 = im->kp[0]; k.sigma = (float) k.p0 * log2e; break;
+        case H2GPU_KRNL_COULOMB: k.p0 = n_kp > 0 ? kp[0] : 0.0; break;
+        case H2GPU_KRNL_GAUSSIAN: k.p0 = kp[0]; k.sigma = (float) k.p0 * log2e; break;
         case H2GPU_KRNL_MATERN32:
         {
-            k.p0 = im->kp[0];
-            k.c0 = -1.7320508075688772 * im->kp[0];
+            k.p0 = kp[0];
+            k.c0 = -1.7320508075688772 * kp[0];
             const float q1 = (float) k.c0 * log2e;
             k.sigma = q1 * q1;
             break;
         }
-        case H2GPU_KRNL_RPY: k.p0 = im->kp[0]; k.c0 = 1.0 / (6.0 * M_PI * im->kp[0]); break;
+        case H2GPU_KRNL_RPY: k.p0 = kp[0]; k.c0 = 1.0 / (6.0 * M_PI * kp[0]); break;
     }
     return k;
 }
+
+KParam kparam_of(const h2gpu_image* im) { return kparam_from(im->kernel_id, im->kp, im->n_kp); }
 
 // The tcgen05 stored-block kernel (mixed precision, normal mode) reports through the
 // status word.
@@ -2455,6 +2457,128 @@ H2G_API int h2gpu_direct_sum(int kernel_id, const double* krnl_param, int n_krnl
     cudaFree(ds); cudaFree(dt); cudaFree(dv); cudaFree(dout);
     return st;
 }
+
+// ============================================== construction: interpolative decompositions
+
+H2G_API int h2gpu_id_batch(int kernel_id, const double* krnl_param, int n_krnl_param, double reltol, int n_blk,
+                           const int* ncand, int npp, const double* cand, const double* prox, int* rank, int* perm,
+                           double** E, long long* e_off)
+{
+    if (!E || !e_off || !rank || (n_blk > 0 && (!ncand || !cand || !perm)) || (npp > 0 && !prox) || n_blk < 0 || npp < 0)
+        return fail(H2GPU_ERR_INVALID, "bad h2gpu_id_batch arguments");
+    *E = nullptr;
+    REQ(kernel_id == H2GPU_KRNL_COULOMB || kernel_id == H2GPU_KRNL_GAUSSIAN || kernel_id == H2GPU_KRNL_MATERN32,
+        "interpolative decompositions on the GPU take the scalar kernels (id %d)", kernel_id);
+    REQ(kernel_id == H2GPU_KRNL_COULOMB || (n_krnl_param >= 1 && krnl_param), "kernel parameter missing");
+    REQ(reltol > 0.0, "reltol must be positive");
+    int max_nc = 0;
+    for (int b = 0; b < n_blk; b++)
+    {
+        REQ(ncand[b] >= 0, "block %d: negative size", b);
+        max_nc = std::max(max_nc, ncand[b]);
+    }
+    REQ(id_qr_smem_bytes(max_nc, npp) <= 200 * 1024, "blocks of %d candidates x %d proxy points exceed the "
+                                                     "shared memory of one CTA", max_nc, npp);
+    if (npp == 0 || max_nc == 0)
+    {
+        // no proxy points (levels without admissible pairs) or no candidates: rank 0
+        long long o = 0;
+        e_off[0] = 0;
+        for (int b = 0; b < n_blk; b++)
+        {
+            rank[b] = 0;
+            for (int j = 0; j < ncand[b]; j++) perm[o + j] = j;
+            o += ncand[b];
+            e_off[b + 1] = 0;
+        }
+        *E = (double*) malloc(8);
+        return *E ? H2GPU_OK : fail(H2GPU_ERR_NOMEM, "host buffer of the interpolation matrices");
+    }
+    int caller_dev = 0;
+    CK(cudaGetDevice(&caller_dev));
+    const KParam kp = kparam_from(kernel_id, krnl_param, n_krnl_param);
+    // chunks of blocks whose workspaces (ncand x npp doubles each) stay within 4 GB
+    std::vector<long long> coff(n_blk + 1, 0);
+    for (int b = 0; b < n_blk; b++) coff[b + 1] = coff[b] + ncand[b];
+    std::vector<int> rk(n_blk, 0);
+    double* d_prox = nullptr;
+    int st = H2GPU_OK;
+    auto cuda_fail = [&](cudaError_t e, const char* what) {
+        if (e != cudaSuccess && st == H2GPU_OK)
+            st = fail(e == cudaErrorMemoryAllocation ? H2GPU_ERR_NOMEM : H2GPU_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+        return e != cudaSuccess;
+    };
+    if (npp > 0 && !cuda_fail(cudaMalloc(&d_prox, 8 * 3 * (size_t) npp), "proxy upload"))
+        cuda_fail(cudaMemcpy(d_prox, prox, 8 * 3 * (size_t) npp, cudaMemcpyHostToDevice), "proxy upload");
+    std::vector<std::vector<double>> Eb(n_blk);
+    const long long budget = 4LL << 27;   // doubles (4 GB)
+    for (int b0 = 0; b0 < n_blk && st == H2GPU_OK;)
+    {
+        int b1 = b0;
+        long long w = 0;
+        while (b1 < n_blk && (b1 == b0 || w + (long long) ncand[b1] * npp <= budget)) w += (long long) ncand[b1++] * npp;
+        std::vector<IdBlock> blks(b1 - b0);
+        std::vector<double> cc(3 * (size_t) (coff[b1] - coff[b0]));
+        long long wo = 0;
+        int mx = 0;
+        for (int b = b0; b < b1; b++)
+        {
+            IdBlock& B = blks[b - b0];
+            B.ncand = ncand[b]; B.npp = npp;
+            B.cand_off = 3 * (coff[b] - coff[b0]); B.prox_off = 0; B.w_off = wo; B.perm_off = coff[b] - coff[b0];
+            wo += (long long) ncand[b] * npp;
+            mx = std::max(mx, ncand[b]);
+            memcpy(&cc[B.cand_off], cand + 3 * coff[b], 8 * 3 * (size_t) ncand[b]);
+        }
+        IdBlock* d_blk = nullptr;
+        double *d_cand = nullptr, *d_W = nullptr;
+        int *d_rank = nullptr, *d_perm = nullptr;
+        const size_t nperm = (size_t) (coff[b1] - coff[b0]);
+        if (!cuda_fail(cudaMalloc(&d_blk, sizeof(IdBlock) * blks.size()), "work space") &&
+            !cuda_fail(cudaMalloc(&d_cand, 8 * std::max<size_t>(cc.size(), 1)), "work space") &&
+            !cuda_fail(cudaMalloc(&d_W, 8 * (size_t) std::max<long long>(wo, 1)), "work space") &&
+            !cuda_fail(cudaMalloc(&d_rank, 4 * blks.size()), "work space") &&
+            !cuda_fail(cudaMalloc(&d_perm, 4 * std::max<size_t>(nperm, 1)), "work space") &&
+            !cuda_fail(cudaMemcpy(d_blk, blks.data(), sizeof(IdBlock) * blks.size(), cudaMemcpyHostToDevice), "upload") &&
+            !cuda_fail(cc.empty() ? cudaSuccess : cudaMemcpy(d_cand, cc.data(), 8 * cc.size(), cudaMemcpyHostToDevice), "upload") &&
+            !cuda_fail(launch_id(kernel_id, d_blk, (int) blks.size(), mx, npp, d_cand, d_prox, kp, d_W, reltol, d_rank,
+                                 d_perm, 0), "interpolative decomposition") &&
+            !cuda_fail(cudaMemcpy(rk.data() + b0, d_rank, 4 * blks.size(), cudaMemcpyDeviceToHost), "download") &&
+            !cuda_fail(nperm ? cudaMemcpy(perm + coff[b0], d_perm, 4 * nperm, cudaMemcpyDeviceToHost) : cudaSuccess, "download"))
+        {
+            // E of block b: columns r .. n-1 of R (column stride npp), rows 0 .. r-1
+            for (int b = b0; b < b1 && st == H2GPU_OK; b++)
+            {
+                const int r = rk[b], n = ncand[b];
+                if (r == 0 || r == n) continue;
+                Eb[b].resize((size_t) r * (n - r));
+                cuda_fail(cudaMemcpy2D(Eb[b].data(), 8 * (size_t) r, d_W + blks[b - b0].w_off + (long long) r * npp,
+                                       8 * (size_t) npp, 8 * (size_t) r, (size_t) (n - r), cudaMemcpyDeviceToHost),
+                          "download");
+            }
+        }
+        for (void* p : {(void*) d_blk, (void*) d_cand, (void*) d_W, (void*) d_rank, (void*) d_perm})
+            if (p) cudaFree(p);
+        b0 = b1;
+    }
+    if (d_prox) cudaFree(d_prox);
+    cudaSetDevice(caller_dev);
+    if (st != H2GPU_OK) return st;
+    e_off[0] = 0;
+    for (int b = 0; b < n_blk; b++)
+    {
+        rank[b] = rk[b];
+        e_off[b + 1] = e_off[b] + (long long) rk[b] * (ncand[b] - rk[b]);
+    }
+    double* out = (double*) malloc(8 * (size_t) std::max<long long>(e_off[n_blk], 1));
+    if (!out) return fail(H2GPU_ERR_NOMEM, "host buffer of the interpolation matrices");
+    for (int b = 0; b < n_blk; b++)
+        if (!Eb[b].empty()) memcpy(out + e_off[b], Eb[b].data(), 8 * Eb[b].size());
+    *E = out;
+    return H2GPU_OK;
+}
+
+H2G_API void h2gpu_free(void* p) { free(p); }
 
 // ================================================== apply without allocation
 //

@@ -156,6 +156,14 @@ struct GenTask {
     long long a32;     // ... in the FP32 arena (ld = f32_ld(kd * ncp))
 };
 
+// One block of a batch of interpolative decompositions (construction of U): the
+// kernel matrix of ncand candidate points against npp proxy points, its candidate and
+// proxy coordinates (dim-major, 3 x n) and its workspace (ncand x npp, row-major)
+struct IdBlock {
+    int ncand, npp;
+    long long cand_off, prox_off, w_off, perm_off;
+};
+
 // Final assembly of a leaf: Y[fwd[row0 + r]][v] = sum_s PS[slot_s + r][v]
 struct AsmTask {
     int row0, nrow;

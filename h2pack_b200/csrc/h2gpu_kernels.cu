@@ -2865,6 +2865,192 @@ __global__ void __launch_bounds__(kWideThreads, 2) k_blk_wide(const BlkTask* __r
     }
 }
 
+// ------------------------------------ interpolative decompositions (construction of U)
+
+// The construction step of the projection matrices (H2P_build_H2_UJ_proxy,
+// src/H2Pack_build.c:32-270, with H2P_ID_compress / H2P_partial_pivot_QR,
+// src/H2Pack_ID_compress.c:51-189 and :491-576), for scalar kernels.  Block b is the
+// kernel matrix of a node's candidate points (shifted to its box center) against its
+// level's proxy points, A[i][j] = K(c_i, p_j), stored row-major (ncand x npp) -- that
+// is, A^T column-major, whose columns (one per candidate) are what the pivoted QR
+// ranks.
+
+// A of every block: one CTA per (block, 64 candidate rows)
+template <int KID>
+__global__ void __launch_bounds__(256) k_id_eval(const IdBlock* __restrict__ blks, const double* __restrict__ cand,
+                                                 const double* __restrict__ prox, KParam kp, double* __restrict__ W)
+{
+    const IdBlock B = blks[blockIdx.y];
+    const int r0 = 64 * blockIdx.x;
+    if (r0 >= B.ncand) return;
+    const int nr = min(64, B.ncand - r0);
+    const double* c = cand + B.cand_off;
+    const double* q = prox + B.prox_off;
+    double* w = W + B.w_off;
+    for (long long e = threadIdx.x; e < (long long) nr * B.npp; e += blockDim.x)
+    {
+        const int i = r0 + (int) (e / B.npp), j = (int) (e % B.npp);
+        const double dx = c[i] - q[j], dy = c[B.ncand + i] - q[B.npp + j], dz = c[2 * B.ncand + i] - q[2 * B.npp + j];
+        w[(long long) i * B.npp + j] = Scalar<KID, double>::f(dx * dx + dy * dy + dz * dz, kp.p0, kp.c0);
+    }
+}
+
+constexpr int kIdThreads = 512, kIdWarps = kIdThreads / 32;
+static_assert(kIdWarps == kIdQrWarps, "shared-memory layout of k_id_qr");
+
+// block-wide sum (all threads get it); scratch: kIdWarps doubles
+__device__ __forceinline__ double id_block_sum(double v, double* scratch)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) scratch[w] = v;
+    __syncthreads();
+    double s = 0.0;
+    for (int k = 0; k < kIdWarps; k++) s += scratch[k];   // fixed order
+    return s;
+}
+
+// block-wide argmax of val[j] over j in [j0, n): the largest value, the smallest index
+// among equal ones (as a first-strictly-greater scan); scratch: kIdWarps (double, int)
+__device__ __forceinline__ void id_block_argmax(const double* val, int j0, int n, double* sv, int* si, double& best,
+                                                int& arg)
+{
+    double b = -1.0;
+    int a = n;
+    for (int j = j0 + (int) threadIdx.x; j < n; j += blockDim.x)
+        if (val[j] > b) { b = val[j]; a = j; }
+    for (int o = 16; o > 0; o >>= 1)
+    {
+        const double ob = __shfl_xor_sync(0xffffffffu, b, o);
+        const int oa = __shfl_xor_sync(0xffffffffu, a, o);
+        if (ob > b || (ob == b && oa < a)) { b = ob; a = oa; }
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) { sv[w] = b; si[w] = a; }
+    __syncthreads();
+    b = -1.0;
+    a = n;
+    for (int k = 0; k < kIdWarps; k++)
+        if (sv[k] > b || (sv[k] == b && si[k] < a)) { b = sv[k]; a = si[k]; }
+    best = b;
+    arg = a;
+}
+
+// Column-pivoted Householder QR of A^T (m = npp rows, n = ncand columns, column j at
+// W + j m) with H2Pack's stopping rule (stop when the largest remaining column norm
+// falls below max(sqrt(m) 1e-15, reltol) times the largest initial one, H2P_ID_QR with
+// QR_REL_NRM), its column-norm downdates (recomputed when the downdated square falls to
+// 1e-10 or below), then E = R11^-1 R12 in place (columns r .. n-1, rows 0 .. r-1).
+// One CTA per block; outputs rank and the column permutation.
+__global__ void __launch_bounds__(kIdThreads) k_id_qr(const IdBlock* __restrict__ blks, double* __restrict__ W,
+                                                      double reltol, int* __restrict__ rank_out,
+                                                      int* __restrict__ perm_out)
+{
+    extern __shared__ __align__(16) unsigned char id_raw[];
+    const IdBlock B = blks[blockIdx.x];
+    const int m = B.npp, n = B.ncand;
+    double* const cn = reinterpret_cast<double*>(id_raw);          // n column norms
+    double* const v = cn + n;                                       // m: Householder vector
+    double* const sv = v + m;                                       // kIdWarps
+    int* const perm = reinterpret_cast<int*>(sv + kIdWarps);        // n
+    int* const si = perm + n;                                       // kIdWarps
+    double* const A = W + B.w_off;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int max_iter = min(m, n);
+    for (int j = warp; j < n; j += kIdWarps)
+    {
+        double s = 0.0;
+        for (int k = lane; k < m; k += 32) { const double x = A[(long long) j * m + k]; s += x * x; }
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) { cn[j] = sqrt(s); perm[j] = j; }
+    }
+    __syncthreads();
+    double norm_p;
+    int pivot;
+    id_block_argmax(cn, 0, n, sv, si, norm_p, pivot);
+    if (pivot >= n) { norm_p = 0.0; pivot = 0; }
+    const double stop_norm = fmax(sqrt((double) m) * 1e-15, reltol) * norm_p;
+    int r = max_iter;
+    for (int i = 0; i < max_iter; i++)
+    {
+        // (a zero remaining column ends it too: nothing left to orthogonalise)
+        if (norm_p < stop_norm || !(norm_p > 0.0)) { r = i; break; }
+        // swap column i with the pivot column
+        if (pivot != i)
+        {
+            double* ci = A + (long long) i * m;
+            double* cp = A + (long long) pivot * m;
+            for (int k = tid; k < m; k += kIdThreads) { const double t = ci[k]; ci[k] = cp[k]; cp[k] = t; }
+            if (tid == 0)
+            {
+                const int tp = perm[i]; perm[i] = perm[pivot]; perm[pivot] = tp;
+                const double tn = cn[i]; cn[i] = cn[pivot]; cn[pivot] = tn;
+            }
+        }
+        __syncthreads();
+        // Householder vector of column i, rows i .. m-1
+        double* const h = A + (long long) i * m + i;
+        const int hl = m - i;
+        double s = 0.0;
+        for (int k = tid; k < hl; k += kIdThreads) s += h[k] * h[k];
+        const double h_norm = sqrt(id_block_sum(s, sv));
+        const double x0 = h[0];
+        const double sign = x0 > 0.0 ? 1.0 : -1.0;
+        const double v0 = x0 + sign * h_norm;
+        s = 0.0;
+        for (int k = tid; k < hl; k += kIdThreads) { const double x = k == 0 ? v0 : h[k]; s += x * x; }
+        const double inv = 1.0 / sqrt(id_block_sum(s, sv));
+        for (int k = tid; k < hl; k += kIdThreads) v[k] = (k == 0 ? v0 : h[k]) * inv;
+        __syncthreads();
+        // trailing columns: one warp per column
+        for (int j = i + 1 + warp; j < n; j += kIdWarps)
+        {
+            double* const c = A + (long long) j * m + i;
+            double d = 0.0;
+            for (int k = lane; k < hl; k += 32) d += v[k] * c[k];
+            for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+            d *= 2.0;
+            for (int k = lane; k < hl; k += 32) c[k] -= d * v[k];
+            __syncwarp();
+            if (cn[j] < stop_norm)
+            {
+                if (lane == 0) cn[j] = 0.0;
+                continue;
+            }
+            const double c0 = c[0];
+            const double t = cn[j] * cn[j] - c0 * c0;
+            if (t <= 1e-10)
+            {
+                double q = 0.0;
+                for (int k = 1 + lane; k < hl; k += 32) q += c[k] * c[k];
+                for (int o = 16; o > 0; o >>= 1) q += __shfl_xor_sync(0xffffffffu, q, o);
+                if (lane == 0) cn[j] = sqrt(q);
+            } else if (lane == 0) {
+                cn[j] = sqrt(t);
+            }
+        }
+        for (int k = tid; k < hl; k += kIdThreads) h[k] = k == 0 ? -sign * h_norm : 0.0;
+        __syncthreads();
+        id_block_argmax(cn, i + 1, n, sv, si, norm_p, pivot);
+        if (pivot >= n) { norm_p = 0.0; pivot = i + 1; }
+    }
+    // E = R11^-1 R12: one thread per column of R12 (back substitution)
+    for (int c = r + tid; c < n; c += kIdThreads)
+    {
+        double* const b = A + (long long) c * m;
+        for (int k = r - 1; k >= 0; k--)
+        {
+            double x = b[k];
+            for (int l = k + 1; l < r; l++) x -= A[(long long) l * m + k] * b[l];
+            b[k] = x / A[(long long) k * m + k];
+        }
+    }
+    if (tid == 0) rank_out[blockIdx.x] = r;
+    for (int j = tid; j < n; j += kIdThreads) perm_out[B.perm_off + j] = perm[j];
+}
+
 // ---------------------------------------------- sweeps on the tensor cores (FP32 U)
 
 // Upward / downward sweep products for FP32 U and panels of 8 / 16 right-hand sides on
@@ -3532,6 +3718,27 @@ cudaError_t launch_pair(int kid, int NV, const PairOwner* ow, int n, const PairP
         case KRNL_MATERN32_ID: return launch_pair_k<KRNL_MATERN32_ID>(NV, ow, n, pp, p, kp, XS, PS, st, far, lo);
         default: return cudaErrorInvalidValue;
     }
+}
+
+cudaError_t launch_id(int kid, const IdBlock* blks, int n, int max_ncand, int max_npp, const double* cand,
+                      const double* prox, KParam kp, double* W, double reltol, int* rank, int* perm, cudaStream_t st)
+{
+    if (n <= 0) return cudaSuccess;
+    const dim3 ge((unsigned) ((max_ncand + 63) / 64), (unsigned) n);
+    switch (kid)
+    {
+        case KRNL_COULOMB_ID:  k_id_eval<KRNL_COULOMB_ID><<<ge, 256, 0, st>>>(blks, cand, prox, kp, W); break;
+        case KRNL_GAUSSIAN_ID: k_id_eval<KRNL_GAUSSIAN_ID><<<ge, 256, 0, st>>>(blks, cand, prox, kp, W); break;
+        case KRNL_MATERN32_ID: k_id_eval<KRNL_MATERN32_ID><<<ge, 256, 0, st>>>(blks, cand, prox, kp, W); break;
+        default: return cudaErrorInvalidValue;
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const int b = id_qr_smem_bytes(max_ncand, max_npp);
+    e = allow_smem(k_id_qr, b);
+    if (e != cudaSuccess) return e;
+    k_id_qr<<<n, kIdThreads, b, st>>>(blks, W, reltol, rank, perm);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_direct(int kid, const double4* trg, int n_trg, const double4* src, int n_src, const double* val,

@@ -56,5 +56,13 @@ cudaError_t launch_gen(int kid, int kd, int fp32, const GenTask* t, int n, const
 cudaError_t launch_peak(int which, int blocks, int iters, float* out, cudaStream_t st);
 cudaError_t launch_direct(int kid, const double4* trg, int n_trg, const double4* src, int n_src, const double* val,
                           KParam kp, double* out, cudaStream_t st);
+// dynamic shared memory of the pivoted-QR kernel for blocks of up to ncand candidates and
+// npp proxy points (column norms, Householder vector, permutation, reduction scratch)
+constexpr int kIdQrWarps = 16;
+constexpr int id_qr_smem_bytes(int ncand, int npp) { return 8 * (ncand + npp + kIdQrWarps) + 4 * (ncand + kIdQrWarps); }
+// interpolative decompositions of n kernel blocks (scalar kernels): kernel matrices
+// into W, pivoted QR, E = R11^-1 R12 in place; rank[b], perm[perm_off + j]
+cudaError_t launch_id(int kid, const IdBlock* blks, int n, int max_ncand, int max_npp, const double* cand,
+                      const double* prox, KParam kp, double* W, double reltol, int* rank, int* perm, cudaStream_t st);
 
 }  // namespace h2gpu

@@ -257,7 +257,7 @@ static const double probe_pts[PROBE_N][4] = {
 
 /* Identify the kernel of a JIT handle from its evaluation function and parameter.
    Returns H2GPU_OK with *kid / param filled, or H2GPU_ERR_UNSUPPORTED. */
-static int identify_kernel(H2Pack_p h, int *kid, double *param, int *n_param)
+int h2p_identify_kernel(H2Pack_p h, int *kid, double *param, int *n_param)
 {
     if (h->krnl_eval == NULL) return H2GPU_ERR_UNSUPPORTED;
     const int xd = h->xpt_dim, kd = h->krnl_dim;
@@ -332,7 +332,7 @@ static int image_of(H2Pack_p h, reg_entry *e)
     if (e->img != NULL) { h2gpu_image_destroy(e->img); e->img = NULL; }
     if (h->BD_JIT && !e->kernel_set)
     {
-        if (identify_kernel(h, &e->kernel_id, e->param, &e->n_param) != H2GPU_OK)
+        if (h2p_identify_kernel(h, &e->kernel_id, e->param, &e->n_param) != H2GPU_OK)
         {
             snprintf(g_msg, sizeof(g_msg),
                      "JIT-mode handle: its kernel function matches none of Coulomb, Gaussian, Matern-3/2 "
@@ -398,7 +398,7 @@ DROPIN_API int H2P_gpu_kernel_of(H2Pack_p h, int *kernel_id, double *param4, int
     if (h == NULL || kernel_id == NULL) return set_msg(H2GPU_ERR_INVALID, "H2P_gpu_kernel_of arguments");
     reg_entry *e = acquire(h);
     if (e == NULL) return set_msg(H2GPU_ERR_NOMEM, "registry allocation");
-    int st = e->kernel_set ? H2GPU_OK : identify_kernel(h, &e->kernel_id, e->param, &e->n_param);
+    int st = e->kernel_set ? H2GPU_OK : h2p_identify_kernel(h, &e->kernel_id, e->param, &e->n_param);
     if (st == H2GPU_OK)
     {
         *kernel_id = e->kernel_id;

@@ -19,6 +19,8 @@
  *                        and H2P_permute_matrix_row_{forward,backward}
  *                        (src/H2Pack_matmul.h:47-54)
  *   h2gpu_direct_sum     direct_nbody (examples/direct_nbody.h:2-54)
+ *   h2gpu_id_batch       the interpolative decompositions of H2P_build_H2_UJ_proxy
+ *                        (src/H2Pack_build.c:32-270, src/H2Pack_ID_compress.c:491-576)
  *   h2gpu_get_stats      the timers[] / mat_size[] / JIT_flops[] counters
  *                        (src/H2Pack_typedef.h:200-204, :226-239) read by
  *                        H2P_print_statistic (src/H2Pack_typedef.c:345-524)
@@ -360,6 +362,31 @@ int h2gpu_direct_sum(int kernel_id, const double *krnl_param, int n_krnl_param,
                      int xpt_dim, int krnl_dim,
                      const double *src_coord, int n_src, const double *src_val,
                      const double *trg_coord, int n_trg, double *trg_val);
+
+/*
+ * Interpolative decompositions of a batch of kernel blocks on the device: the
+ * construction step of the projection matrices for scalar kernels
+ * (H2P_build_H2_UJ_proxy, src/H2Pack_build.c:32-270, its per-node
+ * H2P_ID_compress, src/H2Pack_ID_compress.c:491-576).  Block b is the kernel
+ * matrix of ncand[b] candidate points (3 x ncand[b], dim-major, blocks one after the
+ * other in cand) against the npp proxy points (3 x npp, dim-major) of one level:
+ * A_b[i][j] = K(c_i, p_j).  A_b^T is factored by column-pivoted Householder QR with
+ * H2Pack's relative-norm stopping rule at reltol (H2P_partial_pivot_QR,
+ * src/H2Pack_ID_compress.c:51-189), and E_b = R11^-1 R12 is formed.  Outputs:
+ * rank[b]; perm (sum of ncand, blocks one after the other): the column order of the
+ * QR, whose first rank[b] entries are the skeleton candidates; *E: a buffer allocated
+ * here (release with h2gpu_free) holding E_b (rank x (ncand - rank), column-major,
+ * ld = rank) from element e_off[b] (e_off has n_blk + 1 entries).  Pivot choices can
+ * differ from the CPU's where two column norms agree to rounding, so skeletons match
+ * the reference's in accuracy, not index by index.  No counterpart beyond
+ * H2Pack's internal function.
+ */
+int h2gpu_id_batch(int kernel_id, const double *krnl_param, int n_krnl_param, double reltol, int n_blk,
+                   const int *ncand, int npp, const double *cand, const double *prox, int *rank, int *perm,
+                   double **E, long long *e_off);
+
+/* Release a buffer allocated by the library (h2gpu_id_batch). */
+void h2gpu_free(void *p);
 
 #ifdef __cplusplus
 }

@@ -36,6 +36,7 @@
  *   H2P_gpu_set_kernel     name the kernel of a JIT-mode handle explicitly instead of
  *                          identifying it
  *   H2P_gpu_kernel_of      the kernel id and parameters the drop-in uses for a handle
+ *   H2P_gpu_build_uj       construction: U / J of scalar kernels on the GPU (off by default)
  *   H2P_gpu_set_precision  H2GPU_PREC_FP64 (default) or H2GPU_PREC_MIXED
  *   H2P_gpu_matvec / H2P_gpu_matmul   status-returning forms
  *   H2P_gpu_image          the handle's device image (for h2gpu_get_stats)
@@ -72,6 +73,17 @@ void H2P_destroy(struct H2Pack **h2pack_);
 
 int  H2P_gpu_set_kernel(struct H2Pack *h2pack, int kernel_id, const double *param, int n_param);
 int  H2P_gpu_kernel_of(struct H2Pack *h2pack, int *kernel_id, double *param4, int *n_param);
+
+/* Construction on the GPU: with on = 1 (or H2GPU_BUILD_UJ=1 in the environment), later
+   H2P_build calls of scalar-kernel H2 handles (Coulomb, Gaussian, Matern 3/2, relative-
+   norm stop, 3-D) compute the projection matrices U and skeleton sets J on the device
+   (h2gpu_id_batch, one batch per tree level) in place of H2P_build_H2_UJ_proxy
+   (src/H2Pack_build.c:32-270); other handles, HSS mode and on = 0 (the default) run
+   H2Pack's CPU code.  A device failure prints a message and falls back to it.  The
+   skeletons match H2Pack's in accuracy (pivots can differ where column norms tie). */
+void H2P_gpu_build_uj(int on);
+/* How many H2P_build calls so far had their U / J computed on the device. */
+int  H2P_gpu_build_uj_count(void);
 int  H2P_gpu_set_precision(struct H2Pack *h2pack, int precision);
 int  H2P_gpu_matvec(struct H2Pack *h2pack, const double *x, double *y);
 int  H2P_gpu_matmul(struct H2Pack *h2pack, int layout, int n_vec,
