@@ -109,6 +109,8 @@ H2GPU_SYMBOLS = {
     "h2gpu_id_batch": (C.c_int, [C.c_int, _dp, C.c_int, C.c_double, C.c_int, _ip, C.c_int, _dp, _dp, _ip, _ip,
                                  C.POINTER(_dp), C.POINTER(C.c_longlong)]),
     "h2gpu_free": (None, [C.c_void_p]),
+    "h2gpu_pp_sketch_id": (C.c_int, [C.c_int, _dp, C.c_int, C.c_double, C.c_int, _dp, C.c_int, _dp, _ip, _ip, _dp,
+                                     _ip, _ip]),
 }
 
 # Entry points of the drop-in library (include/h2p_dropin.h) and of the construction driver.
@@ -123,6 +125,8 @@ H2PACK_GPU_SYMBOLS = {
     "H2P_gpu_kernel_of": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), _dp, C.POINTER(C.c_int)]),
     "H2P_gpu_build_uj": (None, [C.c_int]),
     "H2P_gpu_build_uj_count": (C.c_int, []),
+    "H2P_gpu_build_pp": (None, [C.c_int]),
+    "H2P_gpu_build_pp_count": (C.c_int, []),
     "H2P_destroy": (None, [C.POINTER(C.c_void_p)]),
     "H2P_gpu_set_precision": (C.c_int, [C.c_void_p, C.c_int]),
     "H2P_gpu_matvec": (C.c_int, [C.c_void_p, _dp, _dp]),

@@ -2464,9 +2464,12 @@ H2G_API int h2gpu_id_batch(int kernel_id, const double* krnl_param, int n_krnl_p
                            const int* ncand, int npp, const double* cand, const double* prox, int* rank, int* perm,
                            double** E, long long* e_off)
 {
-    if (!E || !e_off || !rank || (n_blk > 0 && (!ncand || !cand || !perm)) || (npp > 0 && !prox) || n_blk < 0 || npp < 0)
+    // E == NULL: skeletons only (no interpolation matrices, e_off unused)
+    const int want_e = E != nullptr;
+    if ((want_e && !e_off) || !rank || (n_blk > 0 && (!ncand || !cand || !perm)) || (npp > 0 && !prox) || n_blk < 0 ||
+        npp < 0)
         return fail(H2GPU_ERR_INVALID, "bad h2gpu_id_batch arguments");
-    *E = nullptr;
+    if (want_e) *E = nullptr;
     REQ(kernel_id == H2GPU_KRNL_COULOMB || kernel_id == H2GPU_KRNL_GAUSSIAN || kernel_id == H2GPU_KRNL_MATERN32,
         "interpolative decompositions on the GPU take the scalar kernels (id %d)", kernel_id);
     REQ(kernel_id == H2GPU_KRNL_COULOMB || (n_krnl_param >= 1 && krnl_param), "kernel parameter missing");
@@ -2483,14 +2486,15 @@ H2G_API int h2gpu_id_batch(int kernel_id, const double* krnl_param, int n_krnl_p
     {
         // no proxy points (levels without admissible pairs) or no candidates: rank 0
         long long o = 0;
-        e_off[0] = 0;
+        if (want_e) e_off[0] = 0;
         for (int b = 0; b < n_blk; b++)
         {
             rank[b] = 0;
             for (int j = 0; j < ncand[b]; j++) perm[o + j] = j;
             o += ncand[b];
-            e_off[b + 1] = 0;
+            if (want_e) e_off[b + 1] = 0;
         }
+        if (!want_e) return H2GPU_OK;
         *E = (double*) malloc(8);
         return *E ? H2GPU_OK : fail(H2GPU_ERR_NOMEM, "host buffer of the interpolation matrices");
     }
@@ -2530,6 +2534,12 @@ H2G_API int h2gpu_id_batch(int kernel_id, const double* krnl_param, int n_krnl_p
             mx = std::max(mx, ncand[b]);
             memcpy(&cc[B.cand_off], cand + 3 * coff[b], 8 * 3 * (size_t) ncand[b]);
         }
+        if (mx == 0)   // only blocks without candidates: rank 0
+        {
+            for (int b = b0; b < b1; b++) rk[b] = 0;
+            b0 = b1;
+            continue;
+        }
         IdBlock* d_blk = nullptr;
         double *d_cand = nullptr, *d_W = nullptr;
         int *d_rank = nullptr, *d_perm = nullptr;
@@ -2542,12 +2552,12 @@ H2G_API int h2gpu_id_batch(int kernel_id, const double* krnl_param, int n_krnl_p
             !cuda_fail(cudaMemcpy(d_blk, blks.data(), sizeof(IdBlock) * blks.size(), cudaMemcpyHostToDevice), "upload") &&
             !cuda_fail(cc.empty() ? cudaSuccess : cudaMemcpy(d_cand, cc.data(), 8 * cc.size(), cudaMemcpyHostToDevice), "upload") &&
             !cuda_fail(launch_id(kernel_id, d_blk, (int) blks.size(), mx, npp, d_cand, d_prox, kp, d_W, reltol, d_rank,
-                                 d_perm, 0), "interpolative decomposition") &&
+                                 d_perm, 0, want_e), "interpolative decomposition") &&
             !cuda_fail(cudaMemcpy(rk.data() + b0, d_rank, 4 * blks.size(), cudaMemcpyDeviceToHost), "download") &&
             !cuda_fail(nperm ? cudaMemcpy(perm + coff[b0], d_perm, 4 * nperm, cudaMemcpyDeviceToHost) : cudaSuccess, "download"))
         {
             // E of block b: columns r .. n-1 of R (column stride npp), rows 0 .. r-1
-            for (int b = b0; b < b1 && st == H2GPU_OK; b++)
+            for (int b = b0; b < b1 && st == H2GPU_OK && want_e; b++)
             {
                 const int r = rk[b], n = ncand[b];
                 if (r == 0 || r == n) continue;
@@ -2564,12 +2574,10 @@ H2G_API int h2gpu_id_batch(int kernel_id, const double* krnl_param, int n_krnl_p
     if (d_prox) cudaFree(d_prox);
     cudaSetDevice(caller_dev);
     if (st != H2GPU_OK) return st;
+    for (int b = 0; b < n_blk; b++) rank[b] = rk[b];
+    if (!want_e) return H2GPU_OK;
     e_off[0] = 0;
-    for (int b = 0; b < n_blk; b++)
-    {
-        rank[b] = rk[b];
-        e_off[b + 1] = e_off[b] + (long long) rk[b] * (ncand[b] - rk[b]);
-    }
+    for (int b = 0; b < n_blk; b++) e_off[b + 1] = e_off[b] + (long long) rk[b] * (ncand[b] - rk[b]);
     double* out = (double*) malloc(8 * (size_t) std::max<long long>(e_off[n_blk], 1));
     if (!out) return fail(H2GPU_ERR_NOMEM, "host buffer of the interpolation matrices");
     for (int b = 0; b < n_blk; b++)
@@ -2579,6 +2587,65 @@ H2G_API int h2gpu_id_batch(int kernel_id, const double* krnl_param, int n_krnl_p
 }
 
 H2G_API void h2gpu_free(void* p) { free(p); }
+
+H2G_API int h2gpu_pp_sketch_id(int kernel_id, const double* krnl_param, int n_krnl_param, double reltol, int nx,
+                               const double* X0, int ny, const double* Y0, const int* st_rowptr, const int* st_col,
+                               const double* st_val, int* rank, int* perm)
+{
+    if (nx <= 0 || ny <= 0 || !X0 || !Y0 || !st_rowptr || !st_col || !st_val || !rank || !perm)
+        return fail(H2GPU_ERR_INVALID, "bad h2gpu_pp_sketch_id arguments");
+    REQ(kernel_id == H2GPU_KRNL_COULOMB || kernel_id == H2GPU_KRNL_GAUSSIAN || kernel_id == H2GPU_KRNL_MATERN32,
+        "proxy points on the GPU take the scalar kernels (id %d)", kernel_id);
+    REQ(kernel_id == H2GPU_KRNL_COULOMB || (n_krnl_param >= 1 && krnl_param), "kernel parameter missing");
+    REQ(reltol > 0.0, "reltol must be positive");
+    REQ(id_qr_smem_bytes(nx, nx) <= 200 * 1024, "%d candidates exceed the shared memory of one CTA", nx);
+    const long long nnz = st_rowptr[nx];
+    REQ(st_rowptr[0] == 0 && nnz >= 0, "bad CSR row pointer");
+    for (int c = 0; c < nx; c++) REQ(st_rowptr[c + 1] >= st_rowptr[c], "bad CSR row pointer");
+    for (long long p = 0; p < nnz; p++) REQ(st_col[p] >= 0 && st_col[p] < ny, "CSR column %lld out of range", p);
+    int caller_dev = 0;
+    CK(cudaGetDevice(&caller_dev));
+    struct DeviceRestore {
+        int dev;
+        ~DeviceRestore() { cudaSetDevice(dev); }
+    } restore{caller_dev};
+    const KParam kp = kparam_from(kernel_id, krnl_param, n_krnl_param);
+    double *dX = nullptr, *dY = nullptr, *dv = nullptr, *dW = nullptr;
+    int *drp = nullptr, *dc = nullptr, *drank = nullptr, *dperm = nullptr;
+    IdBlock* dblk = nullptr;
+    IdBlock B{nx, nx, 0, 0, 0, 0};
+    cudaError_t e = cudaSuccess;
+    auto step = [&](cudaError_t x) { if (e == cudaSuccess) e = x; };
+    step(cudaMalloc(&dX, 8 * 3 * (size_t) nx));
+    step(cudaMalloc(&dY, 8 * 3 * (size_t) ny));
+    step(cudaMalloc(&drp, 4 * (size_t) (nx + 1)));
+    step(cudaMalloc(&dc, 4 * (size_t) std::max<long long>(nnz, 1)));
+    step(cudaMalloc(&dv, 8 * (size_t) std::max<long long>(nnz, 1)));
+    step(cudaMalloc(&dW, 8 * (size_t) nx * nx));
+    step(cudaMalloc(&drank, 4));
+    step(cudaMalloc(&dperm, 4 * (size_t) nx));
+    step(cudaMalloc(&dblk, sizeof(IdBlock)));
+    if (e == cudaSuccess)
+    {
+        step(cudaMemcpy(dX, X0, 8 * 3 * (size_t) nx, cudaMemcpyHostToDevice));
+        step(cudaMemcpy(dY, Y0, 8 * 3 * (size_t) ny, cudaMemcpyHostToDevice));
+        step(cudaMemcpy(drp, st_rowptr, 4 * (size_t) (nx + 1), cudaMemcpyHostToDevice));
+        if (nnz > 0) step(cudaMemcpy(dc, st_col, 4 * (size_t) nnz, cudaMemcpyHostToDevice));
+        if (nnz > 0) step(cudaMemcpy(dv, st_val, 8 * (size_t) nnz, cudaMemcpyHostToDevice));
+        step(cudaMemcpy(dblk, &B, sizeof(IdBlock), cudaMemcpyHostToDevice));
+        step(launch_pp_sketch(kernel_id, nx, dX, ny, dY, drp, dc, dv, kp, dW, 0));
+        step(launch_id(kernel_id, dblk, 1, nx, nx, nullptr, nullptr, kp, dW, reltol, drank, dperm, 0, 0));
+        step(cudaMemcpy(rank, drank, 4, cudaMemcpyDeviceToHost));
+        step(cudaMemcpy(perm, dperm, 4 * (size_t) nx, cudaMemcpyDeviceToHost));
+    }
+    for (void* p : {(void*) dX, (void*) dY, (void*) drp, (void*) dc, (void*) dv, (void*) dW, (void*) drank,
+                    (void*) dperm, (void*) dblk})
+        if (p) cudaFree(p);
+    if (e != cudaSuccess)
+        return fail(e == cudaErrorMemoryAllocation ? H2GPU_ERR_NOMEM : H2GPU_ERR_CUDA, "proxy-point sketch: %s",
+                    cudaGetErrorString(e));
+    return H2GPU_OK;
+}
 
 // ================================================== apply without allocation
 //

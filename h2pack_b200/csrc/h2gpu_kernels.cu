@@ -2895,6 +2895,30 @@ __global__ void __launch_bounds__(256) k_id_eval(const IdBlock* __restrict__ blk
     }
 }
 
+// The reduced candidate matrix of proxy-point generation (H2P_generate_proxy_point_nlayer,
+// src/H2Pack_gen_proxy_point.c:106-131): W = K(X0, Y0) S with S a sparse random matrix
+// given as S^T in CSR (nx rows), W nx x nx row-major; the kernel values are evaluated
+// where S has nonzeros, never stored.  One thread per element of W.
+template <int KID>
+__global__ void __launch_bounds__(256) k_pp_sketch(int nx, const double* __restrict__ X0, int ny,
+                                                   const double* __restrict__ Y0, const int* __restrict__ rowptr,
+                                                   const int* __restrict__ col, const double* __restrict__ val,
+                                                   KParam kp, double* __restrict__ W)
+{
+    const long long e = blockIdx.x * (long long) blockDim.x + threadIdx.x;
+    if (e >= (long long) nx * nx) return;
+    const int i = (int) (e / nx), c = (int) (e % nx);
+    const double x = X0[i], y = X0[nx + i], z = X0[2 * nx + i];
+    double s = 0.0;
+    for (int p = rowptr[c]; p < rowptr[c + 1]; p++)
+    {
+        const int k = col[p];
+        const double dx = x - Y0[k], dy = y - Y0[ny + k], dz = z - Y0[2 * ny + k];
+        s += val[p] * Scalar<KID, double>::f(dx * dx + dy * dy + dz * dz, kp.p0, kp.c0);
+    }
+    W[e] = s;
+}
+
 constexpr int kIdThreads = 512, kIdWarps = kIdThreads / 32;
 static_assert(kIdWarps == kIdQrWarps, "shared-memory layout of k_id_qr");
 
@@ -2946,7 +2970,7 @@ __device__ __forceinline__ void id_block_argmax(const double* val, int j0, int n
 // One CTA per block; outputs rank and the column permutation.
 __global__ void __launch_bounds__(kIdThreads) k_id_qr(const IdBlock* __restrict__ blks, double* __restrict__ W,
                                                       double reltol, int* __restrict__ rank_out,
-                                                      int* __restrict__ perm_out)
+                                                      int* __restrict__ perm_out, int want_e)
 {
     extern __shared__ __align__(16) unsigned char id_raw[];
     const IdBlock B = blks[blockIdx.x];
@@ -3037,7 +3061,7 @@ __global__ void __launch_bounds__(kIdThreads) k_id_qr(const IdBlock* __restrict_
         if (pivot >= n) { norm_p = 0.0; pivot = i + 1; }
     }
     // E = R11^-1 R12: one thread per column of R12 (back substitution)
-    for (int c = r + tid; c < n; c += kIdThreads)
+    for (int c = r + tid; want_e && c < n; c += kIdThreads)
     {
         double* const b = A + (long long) c * m;
         for (int k = r - 1; k >= 0; k--)
@@ -3721,23 +3745,43 @@ cudaError_t launch_pair(int kid, int NV, const PairOwner* ow, int n, const PairP
 }
 
 cudaError_t launch_id(int kid, const IdBlock* blks, int n, int max_ncand, int max_npp, const double* cand,
-                      const double* prox, KParam kp, double* W, double reltol, int* rank, int* perm, cudaStream_t st)
+                      const double* prox, KParam kp, double* W, double reltol, int* rank, int* perm, cudaStream_t st,
+                      int want_e)
 {
-    if (n <= 0) return cudaSuccess;
-    const dim3 ge((unsigned) ((max_ncand + 63) / 64), (unsigned) n);
+    if (n <= 0 || max_ncand <= 0 || max_npp <= 0) return cudaErrorInvalidValue;
+    if (cand)   // kernel matrices from coordinates (else W already holds the matrices)
+    {
+        const dim3 ge((unsigned) ((max_ncand + 63) / 64), (unsigned) n);
+        switch (kid)
+        {
+            case KRNL_COULOMB_ID:  k_id_eval<KRNL_COULOMB_ID><<<ge, 256, 0, st>>>(blks, cand, prox, kp, W); break;
+            case KRNL_GAUSSIAN_ID: k_id_eval<KRNL_GAUSSIAN_ID><<<ge, 256, 0, st>>>(blks, cand, prox, kp, W); break;
+            case KRNL_MATERN32_ID: k_id_eval<KRNL_MATERN32_ID><<<ge, 256, 0, st>>>(blks, cand, prox, kp, W); break;
+            default: return cudaErrorInvalidValue;
+        }
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    const int b = id_qr_smem_bytes(max_ncand, max_npp);
+    cudaError_t e = allow_smem(k_id_qr, b);
+    if (e != cudaSuccess) return e;
+    k_id_qr<<<n, kIdThreads, b, st>>>(blks, W, reltol, rank, perm, want_e);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pp_sketch(int kid, int nx, const double* X0, int ny, const double* Y0, const int* rowptr,
+                             const int* col, const double* val, KParam kp, double* W, cudaStream_t st)
+{
+    if (nx <= 0 || ny <= 0) return cudaErrorInvalidValue;
+    const long long t = (long long) nx * nx;
+    const unsigned g = (unsigned) ((t + 255) / 256);
     switch (kid)
     {
-        case KRNL_COULOMB_ID:  k_id_eval<KRNL_COULOMB_ID><<<ge, 256, 0, st>>>(blks, cand, prox, kp, W); break;
-        case KRNL_GAUSSIAN_ID: k_id_eval<KRNL_GAUSSIAN_ID><<<ge, 256, 0, st>>>(blks, cand, prox, kp, W); break;
-        case KRNL_MATERN32_ID: k_id_eval<KRNL_MATERN32_ID><<<ge, 256, 0, st>>>(blks, cand, prox, kp, W); break;
+        case KRNL_COULOMB_ID:  k_pp_sketch<KRNL_COULOMB_ID><<<g, 256, 0, st>>>(nx, X0, ny, Y0, rowptr, col, val, kp, W); break;
+        case KRNL_GAUSSIAN_ID: k_pp_sketch<KRNL_GAUSSIAN_ID><<<g, 256, 0, st>>>(nx, X0, ny, Y0, rowptr, col, val, kp, W); break;
+        case KRNL_MATERN32_ID: k_pp_sketch<KRNL_MATERN32_ID><<<g, 256, 0, st>>>(nx, X0, ny, Y0, rowptr, col, val, kp, W); break;
         default: return cudaErrorInvalidValue;
     }
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    const int b = id_qr_smem_bytes(max_ncand, max_npp);
-    e = allow_smem(k_id_qr, b);
-    if (e != cudaSuccess) return e;
-    k_id_qr<<<n, kIdThreads, b, st>>>(blks, W, reltol, rank, perm);
     return cudaGetLastError();
 }
 

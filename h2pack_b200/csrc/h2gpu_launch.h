@@ -62,7 +62,12 @@ constexpr int kIdQrWarps = 16;
 constexpr int id_qr_smem_bytes(int ncand, int npp) { return 8 * (ncand + npp + kIdQrWarps) + 4 * (ncand + kIdQrWarps); }
 // interpolative decompositions of n kernel blocks (scalar kernels): kernel matrices
 // into W, pivoted QR, E = R11^-1 R12 in place; rank[b], perm[perm_off + j]
+// (cand == nullptr: W already holds the blocks' matrices; want_e = 0: no E)
 cudaError_t launch_id(int kid, const IdBlock* blks, int n, int max_ncand, int max_npp, const double* cand,
-                      const double* prox, KParam kp, double* W, double reltol, int* rank, int* perm, cudaStream_t st);
+                      const double* prox, KParam kp, double* W, double reltol, int* rank, int* perm, cudaStream_t st,
+                      int want_e = 1);
+// proxy-point generation: W = K(X0, Y0) S (nx x nx), S^T in CSR with nx rows
+cudaError_t launch_pp_sketch(int kid, int nx, const double* X0, int ny, const double* Y0, const int* rowptr,
+                             const int* col, const double* val, KParam kp, double* W, cudaStream_t st);
 
 }  // namespace h2gpu

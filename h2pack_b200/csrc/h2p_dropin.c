@@ -255,20 +255,22 @@ static const double probe_pts[PROBE_N][4] = {
     {-0.70, 1.90, 0.20, 0.8}, {2.40, 1.30, -1.50, 1.2}, {0.00, 0.00, 0.00, 0.6},
 };
 
-/* Identify the kernel of a JIT handle from its evaluation function and parameter.
-   Returns H2GPU_OK with *kid / param filled, or H2GPU_ERR_UNSUPPORTED. */
-int h2p_identify_kernel(H2Pack_p h, int *kid, double *param, int *n_param)
+/* Identify a kernel from its evaluation function and parameter (points of xd
+   coordinate rows, kd x kd values per pair).  Returns H2GPU_OK with *kid / param
+   filled, or H2GPU_ERR_UNSUPPORTED.  Also used by the GPU construction (h2p_uj.c,
+   h2p_pp.c). */
+int h2p_identify_kernel_fn(kernel_eval_fptr krnl_eval, const void *krnl_param, int xd, int kd, int *kid,
+                           double *param, int *n_param)
 {
-    if (h->krnl_eval == NULL) return H2GPU_ERR_UNSUPPORTED;
-    const int xd = h->xpt_dim, kd = h->krnl_dim;
+    if (krnl_eval == NULL) return H2GPU_ERR_UNSUPPORTED;
     double coord[4 * PROBE_N];
     for (int i = 0; i < PROBE_N; i++)
         for (int k = 0; k < xd && k < 4; k++) coord[k * PROBE_N + i] = probe_pts[i][k];
     const int n = kd * PROBE_N;
     double mat[(3 * PROBE_N) * (3 * PROBE_N)];
     for (int i = 0; i < n * n; i++) mat[i] = NAN;
-    h->krnl_eval(coord, PROBE_N, PROBE_N, coord, PROBE_N, PROBE_N, h->krnl_param, mat, n);
-    const double *p = (const double *) h->krnl_param;
+    krnl_eval(coord, PROBE_N, PROBE_N, coord, PROBE_N, PROBE_N, krnl_param, mat, n);
+    const double *p = (const double *) krnl_param;
     const int has_p = p != NULL;
     const double p0 = has_p ? p[0] : 0.0;
 
@@ -320,6 +322,12 @@ int h2p_identify_kernel(H2Pack_p h, int *kid, double *param, int *n_param)
         }
     }
     return H2GPU_ERR_UNSUPPORTED;
+}
+
+/* The kernel of a handle (its evaluation function and parameter). */
+int h2p_identify_kernel(H2Pack_p h, int *kid, double *param, int *n_param)
+{
+    return h2p_identify_kernel_fn(h->krnl_eval, h->krnl_param, h->xpt_dim, h->krnl_dim, kid, param, n_param);
 }
 
 /* --------------------------------------------------------------- device image */

@@ -43,7 +43,7 @@ DROPIN_API void H2P_gpu_build_uj(int on) { g_uj_gpu = on ? 1 : 0; }
 /* How many H2P_build calls so far had their U / J computed on the device. */
 DROPIN_API int H2P_gpu_build_uj_count(void) { return g_uj_built; }
 
-static int uj_gpu_enabled(void)
+static int h2p_uj_gpu_enabled(void)
 {
     if (g_uj_gpu < 0)
     {
@@ -215,7 +215,7 @@ DROPIN_API void H2P_build_H2_UJ_proxy(H2Pack_p h2pack)
 {
     int kid = 0, n_param = 0;
     double param[4] = {0.0, 0.0, 0.0, 0.0};
-    if (uj_gpu_enabled() && h2pack->krnl_dim == 1 && h2pack->pt_dim == 3 && h2pack->QR_stop_type == QR_REL_NRM &&
+    if (h2p_uj_gpu_enabled() && h2pack->krnl_dim == 1 && h2pack->pt_dim == 3 && h2pack->QR_stop_type == QR_REL_NRM &&
         h2p_identify_kernel(h2pack, &kid, param, &n_param) == H2GPU_OK && kid != H2GPU_KRNL_RPY &&
         build_uj_gpu(h2pack, kid, param, n_param) == 0)
     {

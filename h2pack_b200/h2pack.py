@@ -247,7 +247,7 @@ class H2Matrix:
     def __init__(self, kernel, coord: np.ndarray, param=(), reltol: float = 1e-6, BD_JIT: int = 0,
                  max_leaf_points: int = 0, max_leaf_size: float = 0.0, proxy: str = "surface",
                  pp_fname: str | None = None, precision="fp64", n_thread: int = 0, hss: bool = False,
-                 build_uj_gpu: bool = False):
+                 build_uj_gpu: bool = False, build_pp_gpu: bool = False):
         self.lib = _abi.libh2pack_gpu()
         self.kernel_id = _kernel_id(kernel)
         self.param = np.zeros(4)
@@ -258,6 +258,7 @@ class H2Matrix:
         # projection matrices U / J of the construction on the GPU (scalar kernels) or by
         # H2Pack's own CPU code
         self.lib.H2P_gpu_build_uj(1 if build_uj_gpu else 0)
+        self.lib.H2P_gpu_build_pp(1 if build_pp_gpu else 0)
         h = self.lib.h2pb_build(self.kernel_id, _dptr(self.param), self.n_param, n_point, _dptr(self.coord),
                                 float(reltol), int(max_leaf_points), float(max_leaf_size), int(BD_JIT),
                                 0 if proxy == "id" else 1, pp_fname.encode() if pp_fname else None, 1, int(n_thread),

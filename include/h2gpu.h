@@ -376,7 +376,8 @@ int h2gpu_direct_sum(int kernel_id, const double *krnl_param, int n_krnl_param,
  * rank[b]; perm (sum of ncand, blocks one after the other): the column order of the
  * QR, whose first rank[b] entries are the skeleton candidates; *E: a buffer allocated
  * here (release with h2gpu_free) holding E_b (rank x (ncand - rank), column-major,
- * ld = rank) from element e_off[b] (e_off has n_blk + 1 entries).  Pivot choices can
+ * ld = rank) from element e_off[b] (e_off has n_blk + 1 entries); with E = NULL only
+ * rank and perm are computed (e_off unused).  Pivot choices can
  * differ from the CPU's where two column norms agree to rounding, so skeletons match
  * the reference's in accuracy, not index by index.  No counterpart beyond
  * H2Pack's internal function.
@@ -387,6 +388,19 @@ int h2gpu_id_batch(int kernel_id, const double *krnl_param, int n_krnl_param, do
 
 /* Release a buffer allocated by the library (h2gpu_id_batch). */
 void h2gpu_free(void *p);
+
+/*
+ * The candidate reduction of proxy-point generation on the device
+ * (H2P_generate_proxy_point_nlayer, src/H2Pack_gen_proxy_point.c:106-159): the
+ * sketch W = K(X0, Y0) S of nx candidate points X0 against ny outer points Y0 (both
+ * 3 x n, dim-major), S given as S^T in CSR (nx rows: st_rowptr[nx + 1], st_col,
+ * st_val; H2P_gen_rand_sparse_mat_trans's output), followed by the interpolative
+ * decomposition of W's rows at reltol (as h2gpu_id_batch, skeletons only): rank and
+ * perm (nx; the first rank entries are the selected candidates).
+ */
+int h2gpu_pp_sketch_id(int kernel_id, const double *krnl_param, int n_krnl_param, double reltol, int nx,
+                       const double *X0, int ny, const double *Y0, const int *st_rowptr, const int *st_col,
+                       const double *st_val, int *rank, int *perm);
 
 #ifdef __cplusplus
 }

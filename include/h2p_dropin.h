@@ -84,6 +84,15 @@ int  H2P_gpu_kernel_of(struct H2Pack *h2pack, int *kernel_id, double *param4, in
 void H2P_gpu_build_uj(int on);
 /* How many H2P_build calls so far had their U / J computed on the device. */
 int  H2P_gpu_build_uj_count(void);
+/* Numerical proxy points on the GPU: with on = 1 (or H2GPU_BUILD_PP=1), later
+   H2P_generate_proxy_point_ID_file calls of scalar kernels select each level's proxy
+   points on the device (H2P_generate_proxy_point_nlayer, src/H2Pack_gen_proxy_point.c:
+   56-330, algorithm 2, reltol >= 1e-12, H2Pack's own random candidates); off by
+   default: one CTA per 2000 x 2000 sketch decomposition is slower than H2Pack's
+   multithreaded CPU code.  The proxy points give H2Pack's accuracy. */
+void H2P_gpu_build_pp(int on);
+/* How many proxy-point levels so far were selected on the device. */
+int  H2P_gpu_build_pp_count(void);
 int  H2P_gpu_set_precision(struct H2Pack *h2pack, int precision);
 int  H2P_gpu_matvec(struct H2Pack *h2pack, const double *x, double *y);
 int  H2P_gpu_matmul(struct H2Pack *h2pack, int layout, int n_vec,

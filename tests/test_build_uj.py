@@ -82,3 +82,29 @@ def test_gpu_uj_as_accurate_as_h2pack(kernel, jit):
     finally:
         Hc.close()
         Hg.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kernel", ["gaussian", "matern32"])
+def test_gpu_proxy_points_as_accurate_as_h2pack(kernel):
+    """Numerical proxy points (H2P_generate_proxy_point_ID_file, generated afresh: no
+    cache file) selected on the device give the construction H2Pack's accuracy."""
+    P = make_points(kernel, 6000, 43)
+    par = KERNEL_PARAMS[kernel]
+    Hc = H2Matrix(kernel, P, par, 1e-6, BD_JIT=1, max_leaf_points=200, proxy="id")
+    n0 = Hc.lib.H2P_gpu_build_pp_count()
+    Hg = H2Matrix(kernel, P, par, 1e-6, BD_JIT=1, max_leaf_points=200, proxy="id", build_pp_gpu=True)
+    try:
+        assert Hg.lib.H2P_gpu_build_pp_count() > n0     # levels selected on the device
+        sc, sg = _skeleton_sizes(Hc), _skeleton_sizes(Hg)
+        assert abs(int(sg.sum()) - int(sc.sum())) <= 0.10 * sc.sum(), (sc.sum(), sg.sum())
+        rng = np.random.default_rng(4)
+        x = rng.random(Hc.N) - 0.5
+        rows = rng.choice(Hc.N, 2000, replace=False)
+        yd = direct_sum(kernel, par, P, x, P[:, rows])
+        ec = rel(Hc.matvec(x)[rows], yd)
+        eg = rel(Hg.matvec(x)[rows], yd)
+        assert eg <= max(3.0 * ec, 1e-6), (ec, eg)
+    finally:
+        Hc.close()
+        Hg.close()
