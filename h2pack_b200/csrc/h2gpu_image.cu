@@ -2480,8 +2480,16 @@ H2G_API int h2gpu_id_batch(int kernel_id, const double* krnl_param, int n_krnl_p
         REQ(ncand[b] >= 0, "block %d: negative size", b);
         max_nc = std::max(max_nc, ncand[b]);
     }
-    REQ(id_qr_smem_bytes(max_nc, npp) <= 200 * 1024, "blocks of %d candidates x %d proxy points exceed the "
-                                                     "shared memory of one CTA", max_nc, npp);
+    // Blocks decomposed alone by the grid-wide QR: those whose work space exceeds the
+    // shared memory of one CTA, and large blocks (>= 2^20 entries) of a level with too
+    // few of them to fill the GPU one CTA each (one SM would stream each one's trailing
+    // matrix per pivot step).
+    auto big = [&](int b) { return (long long) ncand[b] * npp >= (1LL << 20); };
+    int n_big = 0;
+    for (int b = 0; b < n_blk; b++) n_big += big(b);
+    auto solo = [&](int b) {
+        return id_qr_smem_bytes(ncand[b], npp) > 200 * 1024 || (big(b) && n_big < 64);
+    };
     if (npp == 0 || max_nc == 0)
     {
         // no proxy points (levels without admissible pairs) or no candidates: rank 0
@@ -2520,7 +2528,12 @@ H2G_API int h2gpu_id_batch(int kernel_id, const double* krnl_param, int n_krnl_p
     {
         int b1 = b0;
         long long w = 0;
-        while (b1 < n_blk && (b1 == b0 || w + (long long) ncand[b1] * npp <= budget)) w += (long long) ncand[b1++] * npp;
+        const bool alone = solo(b0) && ncand[b0] > 0;
+        if (alone)
+            b1 = b0 + 1;
+        else
+            while (b1 < n_blk && (b1 == b0 || (w + (long long) ncand[b1] * npp <= budget && !solo(b1))))
+                w += (long long) ncand[b1++] * npp;
         std::vector<IdBlock> blks(b1 - b0);
         std::vector<double> cc(3 * (size_t) (coff[b1] - coff[b0]));
         long long wo = 0;
@@ -2543,7 +2556,19 @@ H2G_API int h2gpu_id_batch(int kernel_id, const double* krnl_param, int n_krnl_p
         IdBlock* d_blk = nullptr;
         double *d_cand = nullptr, *d_W = nullptr;
         int *d_rank = nullptr, *d_perm = nullptr;
+        void* d_work = nullptr;
         const size_t nperm = (size_t) (coff[b1] - coff[b0]);
+        auto decompose = [&]() {
+            if (!alone)
+                return launch_id(kernel_id, d_blk, (int) blks.size(), mx, npp, d_cand, d_prox, kp, d_W, reltol, d_rank,
+                                 d_perm, 0, want_e);
+            int sms = 0;
+            cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, caller_dev);
+            if (e == cudaSuccess) e = cudaMalloc(&d_work, qr_grid_work_bytes(npp, mx));
+            if (e == cudaSuccess) e = launch_id_eval(kernel_id, d_blk, 1, mx, d_cand, d_prox, kp, d_W, 0);
+            if (e == cudaSuccess) e = launch_qr_grid(d_W, npp, mx, reltol, d_work, d_rank, d_perm, sms, want_e, 0);
+            return e;
+        };
         if (!cuda_fail(cudaMalloc(&d_blk, sizeof(IdBlock) * blks.size()), "work space") &&
             !cuda_fail(cudaMalloc(&d_cand, 8 * std::max<size_t>(cc.size(), 1)), "work space") &&
             !cuda_fail(cudaMalloc(&d_W, 8 * (size_t) std::max<long long>(wo, 1)), "work space") &&
@@ -2551,8 +2576,7 @@ H2G_API int h2gpu_id_batch(int kernel_id, const double* krnl_param, int n_krnl_p
             !cuda_fail(cudaMalloc(&d_perm, 4 * std::max<size_t>(nperm, 1)), "work space") &&
             !cuda_fail(cudaMemcpy(d_blk, blks.data(), sizeof(IdBlock) * blks.size(), cudaMemcpyHostToDevice), "upload") &&
             !cuda_fail(cc.empty() ? cudaSuccess : cudaMemcpy(d_cand, cc.data(), 8 * cc.size(), cudaMemcpyHostToDevice), "upload") &&
-            !cuda_fail(launch_id(kernel_id, d_blk, (int) blks.size(), mx, npp, d_cand, d_prox, kp, d_W, reltol, d_rank,
-                                 d_perm, 0, want_e), "interpolative decomposition") &&
+            !cuda_fail(decompose(), "interpolative decomposition") &&
             !cuda_fail(cudaMemcpy(rk.data() + b0, d_rank, 4 * blks.size(), cudaMemcpyDeviceToHost), "download") &&
             !cuda_fail(nperm ? cudaMemcpy(perm + coff[b0], d_perm, 4 * nperm, cudaMemcpyDeviceToHost) : cudaSuccess, "download"))
         {
@@ -2567,7 +2591,7 @@ H2G_API int h2gpu_id_batch(int kernel_id, const double* krnl_param, int n_krnl_p
                           "download");
             }
         }
-        for (void* p : {(void*) d_blk, (void*) d_cand, (void*) d_W, (void*) d_rank, (void*) d_perm})
+        for (void* p : {(void*) d_blk, (void*) d_cand, (void*) d_W, (void*) d_rank, (void*) d_perm, d_work})
             if (p) cudaFree(p);
         b0 = b1;
     }
@@ -2598,7 +2622,6 @@ H2G_API int h2gpu_pp_sketch_id(int kernel_id, const double* krnl_param, int n_kr
         "proxy points on the GPU take the scalar kernels (id %d)", kernel_id);
     REQ(kernel_id == H2GPU_KRNL_COULOMB || (n_krnl_param >= 1 && krnl_param), "kernel parameter missing");
     REQ(reltol > 0.0, "reltol must be positive");
-    REQ(id_qr_smem_bytes(nx, nx) <= 200 * 1024, "%d candidates exceed the shared memory of one CTA", nx);
     const long long nnz = st_rowptr[nx];
     REQ(st_rowptr[0] == 0 && nnz >= 0, "bad CSR row pointer");
     for (int c = 0; c < nx; c++) REQ(st_rowptr[c + 1] >= st_rowptr[c], "bad CSR row pointer");
@@ -2612,10 +2635,11 @@ H2G_API int h2gpu_pp_sketch_id(int kernel_id, const double* krnl_param, int n_kr
     const KParam kp = kparam_from(kernel_id, krnl_param, n_krnl_param);
     double *dX = nullptr, *dY = nullptr, *dv = nullptr, *dW = nullptr;
     int *drp = nullptr, *dc = nullptr, *drank = nullptr, *dperm = nullptr;
-    IdBlock* dblk = nullptr;
-    IdBlock B{nx, nx, 0, 0, 0, 0};
+    void* dwork = nullptr;
+    int sms = 0;
     cudaError_t e = cudaSuccess;
     auto step = [&](cudaError_t x) { if (e == cudaSuccess) e = x; };
+    step(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, caller_dev));
     step(cudaMalloc(&dX, 8 * 3 * (size_t) nx));
     step(cudaMalloc(&dY, 8 * 3 * (size_t) ny));
     step(cudaMalloc(&drp, 4 * (size_t) (nx + 1)));
@@ -2624,7 +2648,7 @@ H2G_API int h2gpu_pp_sketch_id(int kernel_id, const double* krnl_param, int n_kr
     step(cudaMalloc(&dW, 8 * (size_t) nx * nx));
     step(cudaMalloc(&drank, 4));
     step(cudaMalloc(&dperm, 4 * (size_t) nx));
-    step(cudaMalloc(&dblk, sizeof(IdBlock)));
+    step(cudaMalloc(&dwork, qr_grid_work_bytes(nx, nx)));
     if (e == cudaSuccess)
     {
         step(cudaMemcpy(dX, X0, 8 * 3 * (size_t) nx, cudaMemcpyHostToDevice));
@@ -2632,14 +2656,14 @@ H2G_API int h2gpu_pp_sketch_id(int kernel_id, const double* krnl_param, int n_kr
         step(cudaMemcpy(drp, st_rowptr, 4 * (size_t) (nx + 1), cudaMemcpyHostToDevice));
         if (nnz > 0) step(cudaMemcpy(dc, st_col, 4 * (size_t) nnz, cudaMemcpyHostToDevice));
         if (nnz > 0) step(cudaMemcpy(dv, st_val, 8 * (size_t) nnz, cudaMemcpyHostToDevice));
-        step(cudaMemcpy(dblk, &B, sizeof(IdBlock), cudaMemcpyHostToDevice));
         step(launch_pp_sketch(kernel_id, nx, dX, ny, dY, drp, dc, dv, kp, dW, 0));
-        step(launch_id(kernel_id, dblk, 1, nx, nx, nullptr, nullptr, kp, dW, reltol, drank, dperm, 0, 0));
+        // one nx x nx matrix: the pivoted QR spread over the whole GPU
+        step(launch_qr_grid(dW, nx, nx, reltol, dwork, drank, dperm, sms, 0, 0));
         step(cudaMemcpy(rank, drank, 4, cudaMemcpyDeviceToHost));
         step(cudaMemcpy(perm, dperm, 4 * (size_t) nx, cudaMemcpyDeviceToHost));
     }
     for (void* p : {(void*) dX, (void*) dY, (void*) drp, (void*) dc, (void*) dv, (void*) dW, (void*) drank,
-                    (void*) dperm, (void*) dblk})
+                    (void*) dperm, dwork})
         if (p) cudaFree(p);
     if (e != cudaSuccess)
         return fail(e == cudaErrorMemoryAllocation ? H2GPU_ERR_NOMEM : H2GPU_ERR_CUDA, "proxy-point sketch: %s",

@@ -3075,6 +3075,142 @@ __global__ void __launch_bounds__(kIdThreads) k_id_qr(const IdBlock* __restrict_
     for (int j = tid; j < n; j += kIdThreads) perm_out[B.perm_off + j] = perm[j];
 }
 
+// The same QR for one large matrix (the proxy-point sketch, large nodes of a level with
+// few of them), spread over the whole GPU: per iteration i one single-CTA launch picks
+// the pivot, swaps it in and forms the Householder vector (k_qrg_pivot), then a grid of
+// CTAs updates the trailing columns, one warp per column (k_qrg_update).  Launches past
+// the stopping point return at once (the state's done flag).  Same arithmetic, pivot
+// order and stopping rule as k_id_qr.
+struct QrgState {
+    double stop_norm;   // reltol until the first pivot step scales it
+    int done, rank;
+};
+
+__global__ void __launch_bounds__(kIdThreads) k_qrg_init(const double* __restrict__ A, int m, int n, double reltol,
+                                                         double* __restrict__ cn, int* __restrict__ perm,
+                                                         QrgState* __restrict__ st)
+{
+    // column norms: the grid's warps over the columns
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int j = gw; j < n; j += nw)
+    {
+        double s = 0.0;
+        for (int k = lane; k < m; k += 32) { const double x = A[(long long) j * m + k]; s += x * x; }
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) { cn[j] = sqrt(s); perm[j] = j; }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) { st->done = 0; st->rank = min(m, n); st->stop_norm = reltol; }
+}
+
+// one CTA: stop test, pivot swap, Householder vector v (m - i entries) and the finished
+// column i; step 0 also scales the stopping norm by the largest initial column norm
+__global__ void __launch_bounds__(kIdThreads) k_qrg_pivot(double* __restrict__ A, int m, int n, int i,
+                                                          double* __restrict__ cn, int* __restrict__ perm,
+                                                          double* __restrict__ v, QrgState* __restrict__ st)
+{
+    __shared__ double sv[kIdWarps];
+    __shared__ int si[kIdWarps];
+    if (st->done) return;
+    const int tid = threadIdx.x;
+    double norm_p;
+    int pivot;
+    id_block_argmax(cn, i, n, sv, si, norm_p, pivot);   // (holds barriers: every thread has read st)
+    if (pivot >= n) { norm_p = 0.0; pivot = i; }
+    double stop_norm = st->stop_norm;
+    if (i == 0) stop_norm = fmax(sqrt((double) m) * 1e-15, stop_norm) * norm_p;
+    __syncthreads();
+    if (tid == 0 && i == 0) st->stop_norm = stop_norm;
+    if (norm_p < stop_norm || !(norm_p > 0.0))
+    {
+        if (tid == 0) { st->done = 1; st->rank = i; }
+        return;
+    }
+    if (pivot != i)
+    {
+        double* ci = A + (long long) i * m;
+        double* cp = A + (long long) pivot * m;
+        for (int k = tid; k < m; k += kIdThreads) { const double t = ci[k]; ci[k] = cp[k]; cp[k] = t; }
+        if (tid == 0)
+        {
+            const int tp = perm[i]; perm[i] = perm[pivot]; perm[pivot] = tp;
+            const double tn = cn[i]; cn[i] = cn[pivot]; cn[pivot] = tn;
+        }
+    }
+    __syncthreads();
+    double* const h = A + (long long) i * m + i;
+    const int hl = m - i;
+    double s = 0.0;
+    for (int k = tid; k < hl; k += kIdThreads) s += h[k] * h[k];
+    const double h_norm = sqrt(id_block_sum(s, sv));
+    const double x0 = h[0];
+    const double sign = x0 > 0.0 ? 1.0 : -1.0;
+    const double v0 = x0 + sign * h_norm;
+    s = 0.0;
+    for (int k = tid; k < hl; k += kIdThreads) { const double x = k == 0 ? v0 : h[k]; s += x * x; }
+    const double inv = 1.0 / sqrt(id_block_sum(s, sv));
+    for (int k = tid; k < hl; k += kIdThreads) v[k] = (k == 0 ? v0 : h[k]) * inv;
+    __syncthreads();
+    for (int k = tid; k < hl; k += kIdThreads) h[k] = k == 0 ? -sign * h_norm : 0.0;
+}
+
+// trailing columns j = i + 1 .. n - 1, one warp per column across the grid
+__global__ void __launch_bounds__(256) k_qrg_update(double* __restrict__ A, int m, int n, int i,
+                                                    double* __restrict__ cn, const double* __restrict__ v,
+                                                    const QrgState* __restrict__ st)
+{
+    if (st->done) return;
+    const double stop_norm = st->stop_norm;
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    const int hl = m - i;
+    for (int j = i + 1 + gw; j < n; j += nw)
+    {
+        double* const c = A + (long long) j * m + i;
+        double d = 0.0;
+        for (int k = lane; k < hl; k += 32) d += v[k] * c[k];
+        for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+        d *= 2.0;
+        for (int k = lane; k < hl; k += 32) c[k] -= d * v[k];
+        __syncwarp();
+        if (cn[j] < stop_norm)
+        {
+            if (lane == 0) cn[j] = 0.0;
+            continue;
+        }
+        const double c0 = c[0];
+        const double t = cn[j] * cn[j] - c0 * c0;
+        if (t <= 1e-10)
+        {
+            double q = 0.0;
+            for (int k = 1 + lane; k < hl; k += 32) q += c[k] * c[k];
+            for (int o = 16; o > 0; o >>= 1) q += __shfl_xor_sync(0xffffffffu, q, o);
+            if (lane == 0) cn[j] = sqrt(q);
+        } else if (lane == 0) {
+            cn[j] = sqrt(t);
+        }
+    }
+}
+
+// the rank out, then (want_e) E = R11^-1 R12 in place, one thread per column of R12
+__global__ void __launch_bounds__(256) k_qrg_trsm(double* __restrict__ A, int m, int n,
+                                                  const QrgState* __restrict__ st, int want_e, int* __restrict__ rank_out)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0) rank_out[0] = st->rank;
+    if (!want_e) return;
+    const int r = st->rank;
+    for (int c = r + blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+    {
+        double* const b = A + (long long) c * m;
+        for (int k = r - 1; k >= 0; k--)
+        {
+            double x = b[k];
+            for (int l = k + 1; l < r; l++) x -= A[(long long) l * m + k] * b[l];
+            b[k] = x / A[(long long) k * m + k];
+        }
+    }
+}
+
 // ---------------------------------------------- sweeps on the tensor cores (FP32 U)
 
 // Upward / downward sweep products for FP32 U and panels of 8 / 16 right-hand sides on
@@ -3744,6 +3880,21 @@ cudaError_t launch_pair(int kid, int NV, const PairOwner* ow, int n, const PairP
     }
 }
 
+cudaError_t launch_id_eval(int kid, const IdBlock* blks, int n, int max_ncand, const double* cand, const double* prox,
+                           KParam kp, double* W, cudaStream_t st)
+{
+    if (n <= 0 || max_ncand <= 0 || !cand) return cudaErrorInvalidValue;
+    const dim3 ge((unsigned) ((max_ncand + 63) / 64), (unsigned) n);
+    switch (kid)
+    {
+        case KRNL_COULOMB_ID:  k_id_eval<KRNL_COULOMB_ID><<<ge, 256, 0, st>>>(blks, cand, prox, kp, W); break;
+        case KRNL_GAUSSIAN_ID: k_id_eval<KRNL_GAUSSIAN_ID><<<ge, 256, 0, st>>>(blks, cand, prox, kp, W); break;
+        case KRNL_MATERN32_ID: k_id_eval<KRNL_MATERN32_ID><<<ge, 256, 0, st>>>(blks, cand, prox, kp, W); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
 cudaError_t launch_id(int kid, const IdBlock* blks, int n, int max_ncand, int max_npp, const double* cand,
                       const double* prox, KParam kp, double* W, double reltol, int* rank, int* perm, cudaStream_t st,
                       int want_e)
@@ -3751,21 +3902,50 @@ cudaError_t launch_id(int kid, const IdBlock* blks, int n, int max_ncand, int ma
     if (n <= 0 || max_ncand <= 0 || max_npp <= 0) return cudaErrorInvalidValue;
     if (cand)   // kernel matrices from coordinates (else W already holds the matrices)
     {
-        const dim3 ge((unsigned) ((max_ncand + 63) / 64), (unsigned) n);
-        switch (kid)
-        {
-            case KRNL_COULOMB_ID:  k_id_eval<KRNL_COULOMB_ID><<<ge, 256, 0, st>>>(blks, cand, prox, kp, W); break;
-            case KRNL_GAUSSIAN_ID: k_id_eval<KRNL_GAUSSIAN_ID><<<ge, 256, 0, st>>>(blks, cand, prox, kp, W); break;
-            case KRNL_MATERN32_ID: k_id_eval<KRNL_MATERN32_ID><<<ge, 256, 0, st>>>(blks, cand, prox, kp, W); break;
-            default: return cudaErrorInvalidValue;
-        }
-        cudaError_t e = cudaGetLastError();
+        cudaError_t e = launch_id_eval(kid, blks, n, max_ncand, cand, prox, kp, W, st);
         if (e != cudaSuccess) return e;
     }
     const int b = id_qr_smem_bytes(max_ncand, max_npp);
     cudaError_t e = allow_smem(k_id_qr, b);
     if (e != cudaSuccess) return e;
     k_id_qr<<<n, kIdThreads, b, st>>>(blks, W, reltol, rank, perm, want_e);
+    return cudaGetLastError();
+}
+
+size_t qr_grid_work_bytes(int m, int n)
+{
+    const size_t a = (sizeof(QrgState) + 15) & ~(size_t) 15;
+    return a + 8 * ((size_t) std::max(n, 1) + (size_t) std::max(m, 1));
+}
+
+cudaError_t launch_qr_grid(double* A, int m, int n, double reltol, void* work, int* rank, int* perm, int sms,
+                           int want_e, cudaStream_t st)
+{
+    if (m <= 0 || n <= 0 || sms <= 0) return cudaErrorInvalidValue;
+    QrgState* S = (QrgState*) work;
+    double* const cn = (double*) ((char*) work + ((sizeof(QrgState) + 15) & ~(size_t) 15));
+    double* const v = cn + n;
+    const int gu = std::max(1, std::min(4 * sms, (n + 7) / 8));   // 8 warps per CTA of k_qrg_update
+    k_qrg_init<<<std::max(1, std::min(sms, (n + 15) / 16)), kIdThreads, 0, st>>>(A, m, n, reltol, cn, perm, S);
+    cudaError_t e = cudaGetLastError();
+    const int mi = std::min(m, n);
+    for (int i = 0; i < mi && e == cudaSuccess; i++)
+    {
+        k_qrg_pivot<<<1, kIdThreads, 0, st>>>(A, m, n, i, cn, perm, v, S);
+        if (i + 1 < n) k_qrg_update<<<gu, 256, 0, st>>>(A, m, n, i, cn, v, S);
+        e = cudaGetLastError();
+        if (e == cudaSuccess && (i & 63) == 63 && i + 1 < mi)
+        {
+            // past the stopping point the launches only return: end the loop there
+            int done = 0;
+            e = cudaMemcpyAsync(&done, &S->done, sizeof(int), cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            if (e == cudaSuccess && done) break;
+        }
+    }
+    if (e != cudaSuccess) return e;
+    const int gt = want_e ? std::max(1, std::min(4 * sms, (n + 255) / 256)) : 1;
+    k_qrg_trsm<<<gt, 256, 0, st>>>(A, m, n, S, want_e, rank);
     return cudaGetLastError();
 }
 

@@ -66,6 +66,16 @@ constexpr int id_qr_smem_bytes(int ncand, int npp) { return 8 * (ncand + npp + k
 cudaError_t launch_id(int kid, const IdBlock* blks, int n, int max_ncand, int max_npp, const double* cand,
                       const double* prox, KParam kp, double* W, double reltol, int* rank, int* perm, cudaStream_t st,
                       int want_e = 1);
+// the pivoted QR (and E, if want_e) of one large matrix A^T (m x n, column j at A + j m)
+// over the whole GPU, 2 launches per iteration (k_id_qr's arithmetic and stopping rule);
+// work: qr_grid_work_bytes(m, n) of device memory (16-byte aligned); rank: 1 device int;
+// perm: n device ints; sms: the device's SM count
+size_t qr_grid_work_bytes(int m, int n);
+cudaError_t launch_qr_grid(double* A, int m, int n, double reltol, void* work, int* rank, int* perm, int sms,
+                           int want_e, cudaStream_t st);
+// the kernel matrices of launch_id alone (W[b] = K(cand_b, prox)^T, column j = candidate j)
+cudaError_t launch_id_eval(int kid, const IdBlock* blks, int n, int max_ncand, const double* cand, const double* prox,
+                           KParam kp, double* W, cudaStream_t st);
 // proxy-point generation: W = K(X0, Y0) S (nx x nx), S^T in CSR with nx rows
 cudaError_t launch_pp_sketch(int kid, int nx, const double* X0, int ny, const double* Y0, const int* rowptr,
                              const int* col, const double* val, KParam kp, double* W, cudaStream_t st);

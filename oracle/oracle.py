@@ -37,6 +37,7 @@ REF_SYMBOLS.update({
     "H2P_matvec": (None, [C.c_void_p, _dp, _dp]),
     "H2P_matmul": (None, [C.c_void_p, C.c_int, C.c_int, _dp, C.c_int, _dp, C.c_int]),
     "H2P_print_statistic": (None, [C.c_void_p]),
+    "H2P_partial_pivot_QR": (None, [C.c_void_p, C.c_int, C.c_double, C.c_int, _ip, _ip, C.c_int, _dp]),
 })
 ORACLE_SYMBOLS = {
     "h2o_eval": (None, [C.c_int, _dp, C.c_int, _dp, C.c_int, C.c_int, _dp, C.c_int, C.c_int, _dp, C.c_int]),
@@ -75,6 +76,40 @@ def dptr(a: np.ndarray):
 
 def iptr(a: np.ndarray):
     return a.ctypes.data_as(_ip)
+
+
+# ------------------------------------------------- interpolative decompositions
+class _DenseMat(C.Structure):
+    """H2Pack's H2P_dense_mat (src/H2Pack_aux_structs.h:150-157)."""
+    _fields_ = [("nrow", C.c_int), ("ncol", C.c_int), ("ld", C.c_int), ("size", C.c_int), ("data", _dp)]
+
+
+def ref_pivot_qr(cols: np.ndarray, reltol: float, n_thread: int = 1):
+    """H2Pack's own column-pivoted Householder QR (H2P_partial_pivot_QR,
+    src/H2Pack_ID_compress.c:51-189, relative-norm stop as H2P_ID_compress calls it)
+    run from ``libh2ref.so`` on a matrix given as ``cols`` (n x m: row j is column j of
+    the m x n matrix decomposed).  Returns (R as n x m, column j of R in row j; the
+    permutation; the rank)."""
+    R = np.ascontiguousarray(cols, dtype=np.float64).copy()
+    n, m = R.shape
+    A = _DenseMat(m, n, m, m * n, dptr(R))
+    perm = np.zeros(max(n, 1), dtype=np.int32)
+    r = C.c_int(0)
+    buf = np.zeros(max(n, 1))
+    libref().H2P_partial_pivot_QR(C.byref(A), min(m, n), float(reltol), 1, iptr(perm), C.byref(r), int(n_thread),
+                                  dptr(buf))
+    return R, perm[:n], r.value
+
+
+def ref_interp(R: np.ndarray, r: int) -> np.ndarray:
+    """E = R11^-1 R12 of a pivoted QR (the interpolation part of H2P_ID_compress,
+    src/H2Pack_ID_compress.c:491-576), r x (n - r), from ``ref_pivot_qr``'s R."""
+    Rt = R.T   # m x n
+    n = Rt.shape[1]
+    if r == 0 or r == n:
+        return np.zeros((r, n - r))
+    import scipy.linalg
+    return scipy.linalg.solve_triangular(Rt[:r, :r], Rt[:r, r:], lower=False)
 
 
 # ----------------------------------------------------------------- kernels
