@@ -152,16 +152,19 @@ def test_pp_sketch_id_matches_h2pack_qr(kernel):
     for c in range(nx):
         S[col[rowptr[c]:rowptr[c + 1]], c] = val[rowptr[c]:rowptr[c + 1]]
     W = K @ S
-    _, perm_ref, r_ref = oracle.ref_pivot_qr(W, reltol, n_thread=os.cpu_count() or 1)
+    R, perm_ref, r_ref = oracle.ref_pivot_qr(W, reltol, n_thread=os.cpu_count() or 1)
     r = int(rank[0])
     assert r == r_ref
     assert sorted(perm.tolist()) == list(range(nx))
     if not np.array_equal(perm, perm_ref):
-        # Late pivots may swap where two downdated column norms tie to rounding (the
-        # downdate cn^2 - c0^2 cancels): the pivot order must agree well into the rank,
-        # and the chosen rows must approximate the sketch as well as H2Pack's.
+        # Late pivots can swap where two downdated column norms tie to rounding: the
+        # downdate cn^2 - c0^2 loses digits as (|R_00| / |R_ii|)^2, and H2Pack's own QR
+        # on this Matern sketch with one ulp of noise on the input diverges at step 181
+        # of 345 (|R_ii| / |R_00| = 1.3e-6).  So: the same pivots while
+        # |R_ii| >= 1e-5 |R_00|, and rows that approximate the sketch as well as H2Pack's.
         d = int(np.argmax(perm != perm_ref))
-        assert d >= 0.9 * r, (d, r)
+        dg = np.abs(np.diag(R.T[:r_ref, :r_ref]))
+        assert dg[d] < 1e-5 * dg[0], (d, r, dg[d] / dg[0])
 
         def id_residual(skel):
             At = W.T
