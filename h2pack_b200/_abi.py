@@ -111,6 +111,11 @@ H2GPU_SYMBOLS = {
     "h2gpu_free": (None, [C.c_void_p]),
     "h2gpu_pp_sketch_id": (C.c_int, [C.c_int, _dp, C.c_int, C.c_double, C.c_int, _dp, C.c_int, _dp, _ip, _ip, _dp,
                                      _ip, _ip]),
+    "h2gpu_ulv_create": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "h2gpu_ulv_destroy": (C.c_int, [C.c_void_p]),
+    "h2gpu_ulv_solve": (C.c_int, [C.c_void_p, C.c_int, _dp, _dp]),
+    "h2gpu_ulv_solve_device": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "h2gpu_ulv_bytes": (C.c_size_t, [C.c_void_p]),
 }
 
 # Entry points of the drop-in library (include/h2p_dropin.h) and of the construction driver.
@@ -134,6 +139,16 @@ H2PACK_GPU_SYMBOLS = {
     "H2P_gpu_image": (C.c_void_p, [C.c_void_p]),
     "H2P_gpu_release": (C.c_int, [C.c_void_p]),
     "H2P_gpu_last_error": (C.c_char_p, []),
+    "H2P_HSS_ULV_Cholesky_solve": (None, [C.c_void_p, C.c_int, _dp, _dp]),
+    "H2P_HSS_ULV_LU_solve": (None, [C.c_void_p, C.c_int, _dp, _dp]),
+    "H2P_gpu_ULV_solve": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _dp, _dp]),
+    "H2P_gpu_ULV_release": (C.c_int, [C.c_void_p]),
+    # H2Pack's own ULV code inside the library: the factorizations, and its CPU solves
+    # under their aliased names
+    "H2P_HSS_ULV_Cholesky_factorize": (None, [C.c_void_p, C.c_double]),
+    "H2P_HSS_ULV_LU_factorize": (None, [C.c_void_p, C.c_double]),
+    "H2P_HSS_ULV_Cholesky_solve_host": (None, [C.c_void_p, C.c_int, _dp, _dp]),
+    "H2P_HSS_ULV_LU_solve_host": (None, [C.c_void_p, C.c_int, _dp, _dp]),
 }
 
 BUILDER_SYMBOLS = {

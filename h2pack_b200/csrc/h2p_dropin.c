@@ -50,6 +50,8 @@ int h2pb_describe_h2pack(H2Pack_p h, int kernel_id, const double *param, int n_p
                          h2gpu_desc *d, int **ints_out, const double ***ptrs_out);
 /* H2Pack's own H2P_destroy (src/H2Pack_typedef.c:210), compiled under this name */
 void H2P_destroy_host(H2Pack_p *h2pack_);
+/* h2p_ulv.c: the handle's device ULV factors */
+int H2P_gpu_ULV_release(H2Pack_p h);
 
 typedef struct reg_entry
 {
@@ -517,10 +519,14 @@ DROPIN_API void H2P_matmul(H2Pack_p h2pack, const CBLAS_LAYOUT layout, const int
 }
 
 /* H2P_destroy (src/H2Pack_typedef.h, src/H2Pack_typedef.c:210): the device image of the
-   handle is released first, then H2Pack frees the handle. */
+   handle and its device ULV factors are released first, then H2Pack frees the handle. */
 DROPIN_API void H2P_destroy(H2Pack_p *h2pack_)
 {
-    if (h2pack_ != NULL && *h2pack_ != NULL) H2P_gpu_release(*h2pack_);
+    if (h2pack_ != NULL && *h2pack_ != NULL)
+    {
+        H2P_gpu_release(*h2pack_);
+        H2P_gpu_ULV_release(*h2pack_);
+    }
     H2P_destroy_host(h2pack_);
 }
 

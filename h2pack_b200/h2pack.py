@@ -266,6 +266,7 @@ class H2Matrix:
         if not h:
             raise RuntimeError("H2Pack construction (h2pb_build) failed")
         self.handle = h
+        self._hss = bool(hss)
         self.h2pack = self.lib.h2pb_h2pack(h)
         info = (C.c_longlong * 16)()
         self.lib.h2pb_info(self.h2pack, info)
@@ -312,6 +313,27 @@ class H2Matrix:
         """H2P_matmul on caller-owned host memory (e.g. pinned torch tensors)."""
         st = self.lib.H2P_gpu_matmul(self.h2pack, layout, n_vec, C.cast(X_ptr, _dp), ldx, C.cast(Y_ptr, _dp), ldy)
         self._check(st, "H2P_matmul")
+
+    def ulv_factorize(self, shift: float = 0.0, lu: bool = False):
+        """H2Pack's own ULV factorization of an HSS-mode matrix (plus shift on the
+        diagonal): H2P_HSS_ULV_Cholesky_factorize, or H2P_HSS_ULV_LU_factorize with lu
+        (src/H2Pack_HSS_ULV.c:601, :16).  Runs on the host; the solves run on the GPU."""
+        if not self._hss:
+            raise RuntimeError("the ULV factorization needs a matrix built with hss=True")
+        fn = self.lib.H2P_HSS_ULV_LU_factorize if lu else self.lib.H2P_HSS_ULV_Cholesky_factorize
+        fn(self.h2pack, float(shift))
+        self._ulv_lu = bool(lu)
+
+    def ulv_solve(self, b: np.ndarray, op: int = 3) -> np.ndarray:
+        """x = the ULV solve of b on the GPU (H2P_HSS_ULV_Cholesky_solve / _LU_solve,
+        op 1, 2 or 3 as H2Pack's)."""
+        if not hasattr(self, "_ulv_lu"):
+            raise RuntimeError("call ulv_factorize first")
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.empty(self.N)
+        self._check(self.lib.H2P_gpu_ULV_solve(self.h2pack, int(self._ulv_lu), int(op), _dptr(b), _dptr(x)),
+                    "H2P_HSS_ULV_solve")
+        return x
 
     def image(self) -> Image:
         """A non-owning Image view of the handle's device image."""

@@ -402,6 +402,52 @@ int h2gpu_pp_sketch_id(int kernel_id, const double *krnl_param, int n_krnl_param
                        const double *X0, int ny, const double *Y0, const int *st_rowptr, const int *st_col,
                        const double *st_val, int *rank, int *perm);
 
+/* ------------------------------------------------------------------ HSS ULV solve
+ *
+ * The ULV factors of an HSS-mode matrix (H2P_HSS_ULV_Cholesky_factorize,
+ * src/H2Pack_HSS_ULV.c:601-979, or H2P_HSS_ULV_LU_factorize, :16-427; the handle's
+ * ULV_Ls / ULV_idx / ULV_p / ULV_Q / ULV_L, src/H2Pack_typedef.h:153-191) uploaded to
+ * the device, and the ULV solve there (replaces H2P_HSS_ULV_Cholesky_solve, :981-1159,
+ * and H2P_HSS_ULV_LU_solve, :429-599).  All descriptor arrays are host memory, read
+ * during h2gpu_ulv_create only.  Per node i (every node of levels 0 .. max_level):
+ *   Ls[i]               ULV_Ls[i];
+ *   m[i], idx[i]        ULV_idx[i]: m[i] indices into the permuted vector;
+ *   q_ncol[i], Q[i]     ULV_Q[i]: (m[i] + 1) x q_ncol[i] row-major (ld q_ncol[i]): the
+ *                       Householder vectors of a row-major GEQRF below the diagonal and
+ *                       tau in the last row; ignored at the root (level 0);
+ *   L[i], l_ld[i]       ULV_L[i]: m[i] x m[i] row-major;
+ *   p[i]                LU only: ULV_p[i], m[i] - Ls[i] entries.
+ * The device keeps each node's explicit Q (formed from the reflectors at create) and
+ * L, both m x m, and runs one launch per tree level per sweep (one CTA per node).
+ */
+typedef struct h2gpu_ulv h2gpu_ulv;
+
+typedef struct h2gpu_ulv_desc
+{
+    int lu;                        /* 0: Cholesky factors, 1: LU factors              */
+    int n_node, max_level, n_leaf_node, krnl_mat_size;
+    const int *level_n_node;       /* max_level + 1                                   */
+    const int *level_nodes;        /* (max_level + 1) x n_leaf_node; level 0 = root   */
+    const int *fwd_pmt_idx;        /* krnl_mat_size: permuted[i] = b[fwd_pmt_idx[i]]  */
+    const int *bwd_pmt_idx;        /* krnl_mat_size: x[i] = permuted[bwd_pmt_idx[i]]  */
+    const int *Ls, *m, *q_ncol, *l_ld;          /* n_node each                        */
+    const int *const *idx;                      /* n_node pointers                    */
+    const double *const *Q, *const *L;          /* n_node pointers                    */
+    const int *const *p;                        /* n_node pointers (LU), else NULL    */
+    int device;                    /* CUDA device ordinal, -1: current device         */
+} h2gpu_ulv_desc;
+
+int h2gpu_ulv_create(const h2gpu_ulv_desc *desc, h2gpu_ulv **out);
+int h2gpu_ulv_destroy(h2gpu_ulv *u);
+/* x = the ULV solve of b, as the reference's op: 1 the first sweep (Cholesky: L^-1;
+   LU: U^-1 part, levels max_level .. 0), 2 the second (Cholesky: L^-T; LU: L^-1
+   part), 3 both (the solve with the factored matrix).  Host arrays of krnl_mat_size. */
+int h2gpu_ulv_solve(h2gpu_ulv *u, int op, const double *b, double *x);
+/* The same on device arrays, enqueued on `stream` (a cudaStream_t; NULL: the
+   library's stream of this factorization); returns once enqueued. */
+int h2gpu_ulv_solve_device(h2gpu_ulv *u, int op, const double *d_b, double *d_x, void *stream);
+size_t h2gpu_ulv_bytes(const h2gpu_ulv *u);
+
 #ifdef __cplusplus
 }
 #endif

@@ -41,6 +41,8 @@
  *   H2P_gpu_matvec / H2P_gpu_matmul   status-returning forms
  *   H2P_gpu_image          the handle's device image (for h2gpu_get_stats)
  *   H2P_gpu_release        free the handle's device image early (H2P_destroy does it too)
+ *   H2P_gpu_ULV_solve      status-returning form of the HSS ULV solves
+ *   H2P_gpu_ULV_release    free the handle's device ULV factors early
  *   H2P_gpu_last_error     message of the last failure
  *
  * Handles in HSS mode are applied over their HSS pair lists and minimum admissible
@@ -71,6 +73,13 @@ void H2P_permute_matrix_row_backward(struct H2Pack *h2pack, const int layout, co
 
 void H2P_destroy(struct H2Pack **h2pack_);
 
+/* HSS ULV solves on the GPU (replace src/H2Pack_HSS_ULV.c:981 and :429, same
+   signatures, checks and messages; the factorizations H2P_HSS_ULV_Cholesky_factorize /
+   H2P_HSS_ULV_LU_factorize stay H2Pack's).  The handle's factors are uploaded on the
+   first solve after each factorization; a device failure prints the reason and aborts. */
+void H2P_HSS_ULV_Cholesky_solve(struct H2Pack *h2pack, const int op, const double *b, double *x);
+void H2P_HSS_ULV_LU_solve(struct H2Pack *h2pack, const int op, const double *b, double *x);
+
 int  H2P_gpu_set_kernel(struct H2Pack *h2pack, int kernel_id, const double *param, int n_param);
 int  H2P_gpu_kernel_of(struct H2Pack *h2pack, int *kernel_id, double *param4, int *n_param);
 
@@ -88,8 +97,8 @@ int  H2P_gpu_build_uj_count(void);
    H2P_generate_proxy_point_ID_file calls of scalar kernels select each level's proxy
    points on the device (H2P_generate_proxy_point_nlayer, src/H2Pack_gen_proxy_point.c:
    56-330, algorithm 2, reltol >= 1e-12, H2Pack's own random candidates); off by
-   default: one CTA per 2000 x 2000 sketch decomposition is slower than H2Pack's
-   multithreaded CPU code.  The proxy points give H2Pack's accuracy. */
+   default, since late pivots can differ from H2Pack's where column norms tie to
+   rounding.  The proxy points give H2Pack's accuracy. */
 void H2P_gpu_build_pp(int on);
 /* How many proxy-point levels so far were selected on the device. */
 int  H2P_gpu_build_pp_count(void);
@@ -100,6 +109,10 @@ int  H2P_gpu_matmul(struct H2Pack *h2pack, int layout, int n_vec,
 h2gpu_image *H2P_gpu_image(struct H2Pack *h2pack);
 int  H2P_gpu_release(struct H2Pack *h2pack);
 const char *H2P_gpu_last_error(void);
+/* Status-returning form of the two ULV solves (lu = 1: LU factors, 0: Cholesky). */
+int  H2P_gpu_ULV_solve(struct H2Pack *h2pack, int lu, int op, const double *b, double *x);
+/* Free the handle's device ULV factors early (H2P_destroy does it too). */
+int  H2P_gpu_ULV_release(struct H2Pack *h2pack);
 
 #ifdef __cplusplus
 }

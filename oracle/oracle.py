@@ -38,6 +38,10 @@ REF_SYMBOLS.update({
     "H2P_matmul": (None, [C.c_void_p, C.c_int, C.c_int, _dp, C.c_int, _dp, C.c_int]),
     "H2P_print_statistic": (None, [C.c_void_p]),
     "H2P_partial_pivot_QR": (None, [C.c_void_p, C.c_int, C.c_double, C.c_int, _ip, _ip, C.c_int, _dp]),
+    "H2P_HSS_ULV_Cholesky_factorize": (None, [C.c_void_p, C.c_double]),
+    "H2P_HSS_ULV_LU_factorize": (None, [C.c_void_p, C.c_double]),
+    "H2P_HSS_ULV_Cholesky_solve": (None, [C.c_void_p, C.c_int, _dp, _dp]),
+    "H2P_HSS_ULV_LU_solve": (None, [C.c_void_p, C.c_int, _dp, _dp]),
 })
 ORACLE_SYMBOLS = {
     "h2o_eval": (None, [C.c_int, _dp, C.c_int, _dp, C.c_int, C.c_int, _dp, C.c_int, C.c_int, _dp, C.c_int]),
@@ -343,6 +347,19 @@ class RefH2:
         if st != 0:
             raise RuntimeError(f"h2pb_describe status {st}")
         return d
+
+    def ulv_factorize(self, shift: float = 0.0, lu: bool = False):
+        """The reference's HSS ULV factorization (src/H2Pack_HSS_ULV.c:601 / :16)."""
+        (self.lib.H2P_HSS_ULV_LU_factorize if lu else self.lib.H2P_HSS_ULV_Cholesky_factorize)(self.h2pack, shift)
+        self._ulv_lu = bool(lu)
+
+    def ulv_solve(self, b: np.ndarray, op: int = 3) -> np.ndarray:
+        """The reference's ULV solve on the CPU (src/H2Pack_HSS_ULV.c:981 / :429)."""
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.empty(self.N)
+        (self.lib.H2P_HSS_ULV_LU_solve if self._ulv_lu else self.lib.H2P_HSS_ULV_Cholesky_solve)(
+            self.h2pack, int(op), dptr(b), dptr(x))
+        return x
 
     def matvec(self, x: np.ndarray) -> np.ndarray:
         x = np.ascontiguousarray(x, dtype=np.float64)
