@@ -6,9 +6,15 @@ The factorizations stay H2Pack's own (src/H2Pack_HSS_ULV.c:601, :16); the solves
 - CPU: the reference library's own factorization and solve of (A + shift I) invert the
   HSS operator (pins the checker); without a device the GPU solve refuses (no CPU path).
 - GPU: the device solve of every op (1, 2, 3) agrees with H2Pack's solve on the same
-  handle's factors and with the reference library built from the same points; the
-  drop-in entry point gives the same bits as the status form; a new factorization of
-  the handle (another shift, LU after Cholesky) is picked up by the next solve.
+  handle's factors (its own code, compiled into the library under the name
+  H2P_HSS_ULV_*_solve_host); op 3 inverts the shifted HSS operator; the drop-in entry
+  point gives the same bits as the status form; a new factorization of the handle
+  (another shift, LU after Cholesky) is picked up by the next solve.
+
+Ops 1 and 2 alone depend on the factorization's own choices (Householder signs, ranks),
+so the comparison is on the same factors: two separate builds from the same points can
+differ by a pivot tie in an interpolative decomposition (one skeleton point in 28,274
+for the Gaussian case at N = 12,000).
 """
 import ctypes as C
 
@@ -66,11 +72,9 @@ def test_gpu_solve_has_no_cpu_fallback():
 @pytest.mark.gpu
 @pytest.mark.parametrize("kernel,lu,shift", CASES)
 def test_gpu_ulv_solve_matches_h2pack(kernel, lu, shift):
-    H, P = _build(kernel, 20000, 63)
-    R = _build_ref(kernel, P)
+    H, _ = _build(kernel, 12000, 63)
     try:
         H.ulv_factorize(shift, lu=lu)
-        R.ulv_factorize(shift, lu=lu)
         host = H.lib.H2P_HSS_ULV_LU_solve_host if lu else H.lib.H2P_HSS_ULV_Cholesky_solve_host
         dropin = H.lib.H2P_HSS_ULV_LU_solve if lu else H.lib.H2P_HSS_ULV_Cholesky_solve
         rng = np.random.default_rng(7)
@@ -80,7 +84,6 @@ def test_gpu_ulv_solve_matches_h2pack(kernel, lu, shift):
             xh = np.empty(H.N)
             host(H.h2pack, op, _dp(b), _dp(xh))          # H2Pack's solve, same factors
             assert rel(x, xh) < TOL, (op, rel(x, xh))
-            assert rel(x, R.ulv_solve(b, op)) < TOL, op   # the reference library
             xd = np.empty(H.N)
             dropin(H.h2pack, op, _dp(b), _dp(xd))        # the replaced entry point
             assert np.array_equal(xd, x)
@@ -90,7 +93,6 @@ def test_gpu_ulv_solve_matches_h2pack(kernel, lu, shift):
         assert rel(H.matvec(x) + shift * x, b) < 1e-8
     finally:
         H.close()
-        R.close()
 
 
 @pytest.mark.gpu
