@@ -46,7 +46,8 @@
  *   H2P_gpu_last_error     message of the last failure
  *
  * Handles in HSS mode are applied over their HSS pair lists and minimum admissible
- * level, as H2Pack does (src/H2Pack_matvec.c:101, :308, :773, :904).  RPY-Ewald /
+ * level, as H2Pack does (src/H2Pack_matvec.c:101, :308, :773, :904), and their ULV
+ * solves run on the GPU after H2Pack's own factorization.  RPY-Ewald /
  * periodic handles and H2ERI handles are rejected with H2GPU_ERR_UNSUPPORTED.
  */
 #ifndef H2P_DROPIN_H
