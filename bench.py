@@ -54,10 +54,10 @@ def parse():
     p.add_argument("--no-tune", action="store_true", help="keep the default panel width and JIT variant")
     p.add_argument("--check-rows", type=int, default=10_000)
     p.add_argument("--workload", default="jit_matern",
-                   choices=["jit_matern", "aot_coulomb", "aot_rpy", "batched", "served", "peaks"],
+                   choices=["jit_matern", "aot_coulomb", "aot_rpy", "batched", "served", "peaks", "ulv"],
                    help="jit_matern: the headline configuration; the others print extra lines for the "
                         "other configurations (AOT Coulomb matvec, AOT RPY matmul, batched matrices, "
-                        "served requests)")
+                        "served requests, HSS ULV solves)")
     p.add_argument("--blocks", default="generate", choices=["generate", "given"],
                    help="aot_rpy: stored blocks generated on the GPU from a JIT-mode construction, or built "
                         "on the host and uploaded")
@@ -485,6 +485,57 @@ def run_aot_coulomb(args):
     H.close()
 
 
+def run_ulv(args):
+    """HSS ULV solves: Gaussian kernel (l = 1) HSS matrix, N = 20,000 by default, reltol
+    1e-6, default leaf size, shift 1e-2; H2Pack's Cholesky ULV factorization on the host,
+    then op-3 solves (x = (A + shift I)^-1 b) through the drop-in with host arrays (each
+    solve copies b in and x out).  cpu_baseline: H2Pack's own solve on the same factors
+    (its code compiled into the drop-in library as H2P_HSS_ULV_Cholesky_solve_host; its
+    two vector permutations go through the drop-in's GPU permutation)."""
+    os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")   # H2Pack's OpenMP threads call BLAS
+    import ctypes as C
+    from h2pack_b200 import H2Matrix
+    n = 20_000 if args.n == 1_000_000 else args.n
+    shift = 1e-2
+    threads = min(16, os.cpu_count() or 1)
+    coord = points(n, seed=5)
+    t0 = time.time()
+    H = H2Matrix("gaussian", coord, [1.0], 1e-6, BD_JIT=1, hss=True, n_thread=threads)
+    build_s = time.time() - t0
+    t0 = time.time()
+    H.ulv_factorize(shift)
+    fact_s = time.time() - t0
+    b = np.random.default_rng(1).standard_normal(H.N)
+    t0 = time.perf_counter()
+    x = H.ulv_solve(b, 3)                     # uploads the factors, forms Q on the device
+    first_s = time.perf_counter() - t0
+    for _ in range(args.warmup):
+        x = H.ulv_solve(b, 3)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        x = H.ulv_solve(b, 3)
+    ms = (time.perf_counter() - t0) / args.steps * 1e3
+    residual = rel2(H.matvec(x) + shift * x, b)
+    dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    xh = np.empty(H.N)
+    H.lib.H2P_HSS_ULV_Cholesky_solve_host(H.h2pack, 3, dp(b), dp(xh))
+    reps = 5
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        H.lib.H2P_HSS_ULV_Cholesky_solve_host(H.h2pack, 3, dp(b), dp(xh))
+    cpu_ms = (time.perf_counter() - t0) / reps * 1e3
+    launches = 2 * (H.info["max_level"] + 1) + 2
+    line = {"metric": f"HSS ULV solves/s (Gaussian N={n}, Cholesky, op 3, host arrays)", "value": 1e3 / ms,
+            "unit": "solves/s", "workload": "ulv", "n": n, "ms_per_solve": ms, "steps": args.steps,
+            "warmup": args.warmup, "dtype": "f64", "build_seconds": build_s, "factorize_seconds": fact_s,
+            "first_solve_seconds": first_s, "gpu_launches": launches, "max_level": H.info["max_level"],
+            "parity_vs_h2pack_solve": rel2(x, xh), "residual_vs_hss_operator": residual,
+            "cpu_baseline": {"value": 1e3 / cpu_ms, "unit": "solves/s", "cores": threads, "kind": "reference",
+                             "sample": f"{reps} H2P_HSS_ULV_Cholesky_solve of H2Pack's code on the same factors"}}
+    print(json.dumps(line), flush=True)
+    H.close()
+
+
 def run_aot_rpy(args):
     """RPY 3x3 tensor kernel (a = 1, eta = 1/(6 pi), so C = 1), particles uniform in a cube
     sized for volume fraction 0.1, reltol 1e-8, stored U/B/D (normal mode), 64 RHS forces
@@ -844,6 +895,8 @@ def main():
         run_served(args)
     elif args.workload == "peaks":
         run_peaks(args)
+    elif args.workload == "ulv":
+        run_ulv(args)
     else:
         run_ours(args)
 

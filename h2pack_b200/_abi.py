@@ -68,6 +68,20 @@ class Stats(C.Structure):
     ]
 
 
+_pp_i = C.POINTER(C.POINTER(C.c_int))
+_pp_d = C.POINTER(C.POINTER(C.c_double))
+
+
+class UlvDesc(C.Structure):
+    """struct h2gpu_ulv_desc"""
+    _fields_ = [
+        ("lu", C.c_int), ("n_node", C.c_int), ("max_level", C.c_int), ("n_leaf_node", C.c_int),
+        ("krnl_mat_size", C.c_int), ("level_n_node", _ip), ("level_nodes", _ip), ("fwd_pmt_idx", _ip),
+        ("bwd_pmt_idx", _ip), ("Ls", _ip), ("m", _ip), ("q_ncol", _ip), ("l_ld", _ip), ("idx", _pp_i),
+        ("Q", _pp_d), ("L", _pp_d), ("p", _pp_i), ("device", C.c_int),
+    ]
+
+
 # Every symbol include/h2gpu.h declares, with its ctypes signature.
 H2GPU_SYMBOLS = {
     "h2gpu_abi_version": (C.c_int, []),

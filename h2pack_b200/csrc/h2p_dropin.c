@@ -498,6 +498,18 @@ DROPIN_API int H2P_gpu_release(H2Pack_p h)
 
 DROPIN_API const char *H2P_gpu_last_error(void) { return g_msg; }
 
+/* h2p_ulv.c: a failure of the ULV solve, reported through the same message (msg NULL:
+   the engine's message) */
+int h2p_dropin_fail(int st, const char *what, const char *msg)
+{
+    if (msg != NULL)
+    {
+        snprintf(g_msg, sizeof(g_msg), "%s: %s", what, msg);
+        return st;
+    }
+    return set_msg(st, what);
+}
+
 static void die(const char *what)
 {
     fprintf(stderr, "[FATAL] H2Pack GPU drop-in, %s failed: %s\n", what, g_msg);

@@ -29,6 +29,10 @@
 
 #define DROPIN_API __attribute__((visibility("default")))
 
+/* h2p_dropin.c: record a failure in H2P_gpu_last_error's message */
+int h2p_dropin_fail(int st, const char *what, const char *msg);
+const char *H2P_gpu_last_error(void);
+
 typedef struct ulv_entry
 {
     H2Pack_p key;
@@ -153,7 +157,7 @@ static int upload(H2Pack_p h, int lu, h2gpu_ulv **out)
     {
         free(ints);
         free(ptrs);
-        return H2GPU_ERR_NOMEM;
+        return h2p_dropin_fail(H2GPU_ERR_NOMEM, "H2P_HSS_ULV_solve", "host allocation");
     }
     int *m = ints, *qn = ints + n, *ld = ints + 2 * n, *Ls = ints + 3 * n;
     const int **idx = (const int **) ptrs;
@@ -166,7 +170,9 @@ static int upload(H2Pack_p h, int lu, h2gpu_ulv **out)
         H2P_dense_mat_p q = h->ULV_Q[i], l = h->ULV_L[i];
         if (ix == NULL || q == NULL || l == NULL || (lu && (h->ULV_p == NULL || h->ULV_p[i] == NULL)))
         {
-            st = H2GPU_ERR_STATE;
+            st = h2p_dropin_fail(H2GPU_ERR_STATE, "H2P_HSS_ULV_solve",
+                                 lu ? "the handle holds no LU factors (H2P_HSS_ULV_LU_factorize)"
+                                    : "the handle's ULV factors are incomplete");
             break;
         }
         m[i] = ix->length;
@@ -180,7 +186,10 @@ static int upload(H2Pack_p h, int lu, h2gpu_ulv **out)
         /* the reference's solve assumes these shapes (src/H2Pack_HSS_ULV.c:1036-1046) */
         if (l->nrow != m[i] || l->ncol != m[i] || (i != root && q->ncol > 0 && (q->nrow != m[i] + 1 || q->ld != q->ncol)) ||
             (lu && h->ULV_p[i]->length != m[i] - Ls[i]))
-            st = H2GPU_ERR_INVALID;
+        {
+            st = h2p_dropin_fail(H2GPU_ERR_INVALID, "H2P_HSS_ULV_solve", "factor shapes differ from H2Pack's layout");
+            break;
+        }
     }
     if (st == H2GPU_OK)
     {
@@ -205,6 +214,7 @@ static int upload(H2Pack_p h, int lu, h2gpu_ulv **out)
         d.p = lu ? p : NULL;
         d.device = -1;
         st = h2gpu_ulv_create(&d, out);
+        if (st != H2GPU_OK) h2p_dropin_fail(st, "uploading the ULV factors", NULL);
     }
     free(ints);
     free(ptrs);
@@ -216,12 +226,14 @@ static int upload(H2Pack_p h, int lu, h2gpu_ulv **out)
    the two replaced solves; counts the solve and its time on the handle. */
 DROPIN_API int H2P_gpu_ULV_solve(H2Pack_p h, int lu, int op, const double *b, double *x)
 {
-    if (h == NULL || b == NULL || x == NULL) return H2GPU_ERR_INVALID;
-    if (!h->is_HSS || h->ULV_idx == NULL) return H2GPU_ERR_STATE;
-    if (op < 1 || op > 3) return H2GPU_ERR_INVALID;
+    const char *what = "H2P_HSS_ULV_solve";
+    if (h == NULL || b == NULL || x == NULL) return h2p_dropin_fail(H2GPU_ERR_INVALID, what, "NULL argument");
+    if (!h->is_HSS) return h2p_dropin_fail(H2GPU_ERR_STATE, what, "H2Pack is not running in HSS mode");
+    if (h->ULV_idx == NULL) return h2p_dropin_fail(H2GPU_ERR_STATE, what, "no ULV factorization on the handle");
+    if (op < 1 || op > 3) return h2p_dropin_fail(H2GPU_ERR_INVALID, what, "op must be 1, 2 or 3");
     const double st0 = wtime();
     ulv_entry *e = acquire(h);
-    if (e == NULL) return H2GPU_ERR_NOMEM;
+    if (e == NULL) return h2p_dropin_fail(H2GPU_ERR_NOMEM, what, "host allocation");
     pthread_mutex_lock(&e->mu);
     int st = H2GPU_OK;
     const uint64_t f = fingerprint(h, lu);
@@ -229,11 +241,15 @@ DROPIN_API int H2P_gpu_ULV_solve(H2Pack_p h, int lu, int op, const double *b, do
     {
         if (e->ulv != NULL) h2gpu_ulv_destroy(e->ulv);
         e->ulv = NULL;
-        st = upload(h, lu, &e->ulv);
+        st = upload(h, lu, &e->ulv);   /* records its own failure message */
         e->fingerprint = f;
         e->lu = lu;
     }
-    if (st == H2GPU_OK) st = h2gpu_ulv_solve(e->ulv, op, b, x);
+    if (st == H2GPU_OK)
+    {
+        st = h2gpu_ulv_solve(e->ulv, op, b, x);
+        if (st != H2GPU_OK) h2p_dropin_fail(st, what, NULL);
+    }
     pthread_mutex_unlock(&e->mu);
     release_ref(e);
     if (st == H2GPU_OK)
@@ -265,8 +281,7 @@ static void solve_or_die(H2Pack_p h, int lu, int op, const DTYPE *b, DTYPE *x, c
     const int st = H2P_gpu_ULV_solve(h, lu, op, b, x);
     if (st != H2GPU_OK)
     {
-        const char *m = h2gpu_last_error();
-        fprintf(stderr, "[H2Pack GPU] %s failed (status %d): %s\n", name, st, m ? m : "");
+        fprintf(stderr, "[FATAL] H2Pack GPU drop-in, %s failed (status %d): %s\n", name, st, H2P_gpu_last_error());
         abort();
     }
 }

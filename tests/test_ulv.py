@@ -69,6 +69,97 @@ def test_gpu_solve_has_no_cpu_fallback():
         H.close()
 
 
+def test_solve_refuses_handles_without_factors():
+    """The status form names what is missing, as the reference's messages do
+    (src/H2Pack_HSS_ULV.c:983-992); no device is touched."""
+    from h2pack_b200 import _abi
+    P = make_points("gaussian", 2000, 65)
+    b = np.ones(2000)
+    x = np.empty(2000)
+    for hss, msg in ((False, "HSS mode"), (True, "no ULV factorization")):
+        H = H2Matrix("gaussian", P, [1.0], 1e-6, BD_JIT=1, max_leaf_points=100, hss=hss)
+        try:
+            st = H.lib.H2P_gpu_ULV_solve(H.h2pack, 0, 3, _dp(b), _dp(x))
+            assert _abi.STATUS_NAMES[st] == "STATE"
+            assert msg in H.lib.H2P_gpu_last_error().decode()
+            st = H.lib.H2P_gpu_ULV_solve(H.h2pack, 0, 4, _dp(b), _dp(x))
+            assert st != 0
+        finally:
+            H.close()
+
+
+def _tiny_desc(lu=0, **bad):
+    """Factors of a two-level tree by hand: root 0 over leaves 1 and 2 (two points each,
+    one Householder vector each), for the host-side checks of h2gpu_ulv_create."""
+    from h2pack_b200 import _abi
+    keep = []
+
+    def ia(v):
+        a = np.ascontiguousarray(v, dtype=np.int32)
+        keep.append(a)
+        return a.ctypes.data_as(C.POINTER(C.c_int))
+
+    def da(v):
+        a = np.ascontiguousarray(v, dtype=np.float64)
+        keep.append(a)
+        return a.ctypes.data_as(C.POINTER(C.c_double))
+
+    idx = bad.get("idx", [[0, 2], [0, 1], [2, 3]])
+    m = [len(i) for i in idx]
+    Ls = bad.get("Ls", [0, 1, 1])
+    q_ncol = bad.get("q_ncol", [0, 1, 1])
+    Q = [None] + [da([[1.0], [0.5], [1.2]]) for _ in range(2)]   # (m + 1) x 1: vector, tau
+    L = [da(np.eye(mm) * 2.0) for mm in m]
+    p = bad.get("p", [[0, 1], [0], [0]])
+    d = _abi.UlvDesc()
+    d.lu = lu
+    d.n_node, d.max_level, d.n_leaf_node, d.krnl_mat_size = 3, 1, 2, 4
+    d.level_n_node = ia(bad.get("level_n_node", [1, 2]))
+    d.level_nodes = ia(bad.get("level_nodes", [0, -1, 1, 2]))
+    d.fwd_pmt_idx = ia(bad.get("fwd", [0, 1, 2, 3]))
+    d.bwd_pmt_idx = ia([0, 1, 2, 3])
+    d.Ls, d.m, d.q_ncol, d.l_ld = ia(Ls), ia(m), ia(q_ncol), ia(m)
+    d.idx = (C.POINTER(C.c_int) * 3)(*[ia(i) for i in idx])
+    d.Q = (C.POINTER(C.c_double) * 3)(*[q if q is not None else C.POINTER(C.c_double)() for q in Q])
+    d.L = (C.POINTER(C.c_double) * 3)(*L)
+    d.p = (C.POINTER(C.c_int) * 3)(*[ia(x) for x in p]) if lu else None
+    d.device = -1
+    d._keep = keep
+    return d
+
+
+@pytest.mark.parametrize("bad,lu,status", [
+    ({"idx": [[0, 2], [0, 9], [2, 3]]}, 0, "INVALID"),            # index outside the vector
+    ({"fwd": [0, 1, 2, 7]}, 0, "INVALID"),                        # permutation entry
+    ({"level_n_node": [2, 1], "level_nodes": [0, 1, 2, -1]}, 0, "INVALID"),   # level 0 not the root alone
+    ({"level_nodes": [0, -1, 1, 1]}, 0, "INVALID"),               # a node twice
+    ({"Ls": [0, 3, 1]}, 0, "INVALID"),                            # Ls > m
+    ({"q_ncol": [0, 3, 1]}, 0, "UNSUPPORTED"),                    # more reflectors than rows
+    ({"p": [[0, 1], [4], [0]]}, 1, "INVALID"),                    # LU pivot out of range
+])
+def test_ulv_create_checks_factors_on_the_host(bad, lu, status):
+    """h2gpu_ulv_create range-checks every index the kernels use before any device
+    work, so malformed factors are refused with a status (no GPU needed)."""
+    from h2pack_b200 import _abi
+    lib = _abi.libh2gpu()
+    out = C.c_void_p()
+    st = lib.h2gpu_ulv_create(C.byref(_tiny_desc(lu, **bad)), C.byref(out))
+    assert _abi.STATUS_NAMES[st] == status, lib.h2gpu_last_error()
+    assert not out.value
+
+
+def test_ulv_create_valid_factors_need_a_device():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    from h2pack_b200 import _abi
+    lib = _abi.libh2gpu()
+    out = C.c_void_p()
+    for lu in (0, 1):
+        st = lib.h2gpu_ulv_create(C.byref(_tiny_desc(lu)), C.byref(out))
+        assert _abi.STATUS_NAMES[st] == "CUDA" and not out.value
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("kernel,lu,shift", CASES)
 def test_gpu_ulv_solve_matches_h2pack(kernel, lu, shift):
