@@ -444,7 +444,10 @@ int h2gpu_ulv_destroy(h2gpu_ulv *u);
    part), 3 both (the solve with the factored matrix).  Host arrays of krnl_mat_size. */
 int h2gpu_ulv_solve(h2gpu_ulv *u, int op, const double *b, double *x);
 /* The same on device arrays, enqueued on `stream` (a cudaStream_t; NULL: the
-   library's stream of this factorization); returns once enqueued. */
+   library's stream of this factorization); returns once enqueued.  Every solve of one
+   h2gpu_ulv works in that object's permuted-vector buffer, so solves of one object
+   must not overlap on the device (enqueue them on one stream; the drop-in serialises
+   per handle); different objects are independent. */
 int h2gpu_ulv_solve_device(h2gpu_ulv *u, int op, const double *d_b, double *d_x, void *stream);
 size_t h2gpu_ulv_bytes(const h2gpu_ulv *u);
 
