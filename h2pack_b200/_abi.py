@@ -177,6 +177,8 @@ BUILDER_SYMBOLS = {
     "h2pb_coord": (_dp, [C.c_void_p]),
     "h2pb_coord_idx": (_ip, [C.c_void_p]),
     "h2pb_describe": (C.c_int, [C.c_void_p, C.POINTER(Desc)]),
+    "h2pb_describe_ulv": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_void_p)]),
+    "h2pb_free": (None, [C.c_void_p]),
 }
 
 

@@ -271,3 +271,65 @@ H2PB_EXPORT int h2pb_describe(h2pb_handle *hd, h2gpu_desc *d)
     hd->descs = ds;
     return H2GPU_OK;
 }
+
+/* The ULV factors of an HSS handle (after H2P_HSS_ULV_Cholesky_factorize, lu = 0, or
+   H2P_HSS_ULV_LU_factorize, lu = 1) as an h2gpu_ulv_desc over the handle's own arrays
+   (ULV_Ls / ULV_idx / ULV_p / ULV_Q / ULV_L, src/H2Pack_typedef.h:153-191).  *buf holds
+   the descriptor's per-node tables; release it with h2pb_free after the last use of d.
+   Returns H2GPU_ERR_STATE without factors of that kind. */
+H2PB_EXPORT int h2pb_describe_ulv(H2Pack_p h, int lu, h2gpu_ulv_desc *d, void **buf)
+{
+    if (h == NULL || d == NULL || buf == NULL) return H2GPU_ERR_INVALID;
+    *buf = NULL;
+    if (!h->is_HSS || h->ULV_idx == NULL || h->ULV_L == NULL || h->ULV_Q == NULL || (lu && h->ULV_p == NULL))
+        return H2GPU_ERR_STATE;
+    const int n = h->n_node;
+    char *mem = (char *) malloc(sizeof(int) * 4 * (size_t) n + sizeof(void *) * 4 * (size_t) n);
+    if (mem == NULL) return H2GPU_ERR_NOMEM;
+    const void **ptrs = (const void **) mem;
+    int *ints = (int *) (mem + sizeof(void *) * 4 * (size_t) n);
+    int *m = ints, *qn = ints + n, *ld = ints + 2 * n, *Ls = ints + 3 * n;
+    const int **idx = (const int **) ptrs;
+    const double **Q = (const double **) (ptrs + n), **L = (const double **) (ptrs + 2 * n);
+    const int **p = (const int **) (ptrs + 3 * n);
+    const int root = h->level_nodes[0];
+    for (int i = 0; i < n; i++)
+    {
+        if (h->ULV_idx[i] == NULL || h->ULV_L[i] == NULL || h->ULV_Q[i] == NULL || (lu && h->ULV_p[i] == NULL))
+        {
+            free(mem);
+            return H2GPU_ERR_STATE;
+        }
+        m[i] = h->ULV_idx[i]->length;
+        Ls[i] = h->ULV_Ls[i];
+        ld[i] = h->ULV_L[i]->ld;
+        qn[i] = i == root ? 0 : h->ULV_Q[i]->ncol;
+        idx[i] = h->ULV_idx[i]->data;
+        L[i] = h->ULV_L[i]->data;
+        Q[i] = i == root ? NULL : h->ULV_Q[i]->data;
+        p[i] = lu ? h->ULV_p[i]->data : NULL;
+    }
+    memset(d, 0, sizeof(*d));
+    d->lu = lu;
+    d->n_node = n;
+    d->max_level = h->max_level;
+    d->n_leaf_node = h->n_leaf_node;
+    d->krnl_mat_size = h->krnl_mat_size;
+    d->level_n_node = h->level_n_node;
+    d->level_nodes = h->level_nodes;
+    d->fwd_pmt_idx = h->fwd_pmt_idx;
+    d->bwd_pmt_idx = h->bwd_pmt_idx;
+    d->Ls = Ls;
+    d->m = m;
+    d->q_ncol = qn;
+    d->l_ld = ld;
+    d->idx = idx;
+    d->Q = Q;
+    d->L = L;
+    d->p = lu ? p : NULL;
+    d->device = -1;
+    *buf = mem;
+    return H2GPU_OK;
+}
+
+H2PB_EXPORT void h2pb_free(void *p) { free(p); }

@@ -23,6 +23,10 @@
  *   h2o_eval     kernel matrix evaluation   src/H2Pack_3D_kernels.h (Coulomb :50-161,
  *                Gaussian :167-268, Matern 3/2 :384-497, RPY :893-959)
  *   h2o_direct_sum  direct_nbody            examples/direct_nbody.h:2-54
+ *   h2o_ulv_solve  H2P_HSS_ULV_Cholesky_solve src/H2Pack_HSS_ULV.c:981-1159 and
+ *                H2P_HSS_ULV_LU_solve       src/H2Pack_HSS_ULV.c:429-599 over the
+ *                plain h2gpu_ulv_desc view of the factors; Q applied from its
+ *                Householder vectors as ORMQR does
  *
  * Parity of this restatement is pinned against the reference library itself
  * (built from the reference sources into oracle/_ref) by tests/test_oracle_pin.py.
@@ -543,4 +547,124 @@ H2O_EXPORT void h2o_direct_sum(int kernel_id, const double *param, int n_param, 
         }
     }
     free(mat); free(cs); free(ct);
+}
+
+/* ---------------------------------------------------------------- HSS ULV solve */
+
+/* b = Q^T b (trans) or Q b, Q = H(0) .. H(k-1) from a row-major GEQRF of m rows (A:
+   m x k, ld k, vector j below the diagonal of column j with an implicit 1; tau: the
+   row after A), as LAPACK's ORMQR with side 'L' */
+static void ulv_apply_q(const double *A, int m, int k, int trans, double *b)
+{
+    const double *tau = A + (size_t) m * k;
+    for (int t = 0; t < k; t++)
+    {
+        const int j = trans ? t : k - 1 - t;
+        double s = b[j];
+        for (int i = j + 1; i < m; i++) s += A[(size_t) i * k + j] * b[i];
+        s *= tau[j];
+        b[j] -= s;
+        for (int i = j + 1; i < m; i++) b[i] -= s * A[(size_t) i * k + j];
+    }
+}
+
+/* one node of one sweep (src/H2Pack_HSS_ULV.c:1030-1067 / :1107-1148 Cholesky,
+   :480-520 / :545-590 LU) on b0 = the node's entries of the permuted vector */
+static void ulv_node(const h2gpu_ulv_desc *d, int node, int has_q, int up, double *b0, double *tmp)
+{
+    const int m = d->m[node], I = d->Ls[node], n2 = m - I, ld = d->l_ld[node];
+    const double *L = d->L[node];
+    double *b1 = b0, *b2 = b0 + I;
+    const double *T = L + (size_t) I * ld + I;
+    if (up)
+    {
+        if (has_q) ulv_apply_q(d->Q[node], m, d->q_ncol[node], 1, b0);
+        if (d->lu)
+        {
+            memcpy(tmp, b2, sizeof(double) * (size_t) n2);
+            for (int j = 0; j < n2; j++) b2[j] = tmp[d->p[node][j]];
+        }
+        for (int r = 0; r < n2; r++)                 /* b2 = L22 \ b2 (LU: unit diagonal) */
+        {
+            double s = b2[r];
+            for (int c = 0; c < r; c++) s -= T[(size_t) r * ld + c] * b2[c];
+            b2[r] = d->lu ? s : s / T[(size_t) r * ld + r];
+        }
+        for (int r = 0; r < I; r++)                  /* b1 -= L12 b2 */
+        {
+            double s = 0.0;
+            for (int c = 0; c < n2; c++) s += L[(size_t) r * ld + I + c] * b2[c];
+            b1[r] -= s;
+        }
+    } else {
+        if (!d->lu)
+        {
+            for (int c = 0; c < n2; c++)             /* b2 -= L12^T b1 */
+            {
+                double s = 0.0;
+                for (int r = 0; r < I; r++) s += L[(size_t) r * ld + I + c] * b1[r];
+                b2[c] -= s;
+            }
+            for (int r = n2 - 1; r >= 0; r--)        /* b2 = L22^T \ b2 */
+            {
+                double s = b2[r];
+                for (int c = r + 1; c < n2; c++) s -= T[(size_t) c * ld + r] * b2[c];
+                b2[r] = s / T[(size_t) r * ld + r];
+            }
+        } else {
+            for (int r = 0; r < n2; r++)             /* b2 -= LD21 b1 */
+            {
+                double s = 0.0;
+                for (int c = 0; c < I; c++) s += L[(size_t) (I + r) * ld + c] * b1[c];
+                b2[r] -= s;
+            }
+            for (int r = n2 - 1; r >= 0; r--)        /* b2 = U0 \ b2 */
+            {
+                double s = b2[r];
+                for (int c = r + 1; c < n2; c++) s -= T[(size_t) r * ld + c] * b2[c];
+                b2[r] = s / T[(size_t) r * ld + r];
+            }
+        }
+        if (has_q) ulv_apply_q(d->Q[node], m, d->q_ncol[node], 0, b0);
+    }
+}
+
+/* x = the ULV solve of b (op 1, 2 or 3 as the reference's); the root (level 0) has no
+   Q.  Returns 0, or -1 on a bad argument or allocation failure. */
+H2O_EXPORT int h2o_ulv_solve(const h2gpu_ulv_desc *d, int op, const double *b, double *x)
+{
+    if (d == NULL || b == NULL || x == NULL || op < 1 || op > 3) return -1;
+    const int n = d->krnl_mat_size;
+    int mmax = 1;
+    for (int i = 0; i < d->n_node; i++) mmax = d->m[i] > mmax ? d->m[i] : mmax;
+    double *px = (double *) malloc(sizeof(double) * (size_t) n);
+    double *b0 = (double *) malloc(sizeof(double) * (size_t) mmax);
+    double *tmp = (double *) malloc(sizeof(double) * (size_t) mmax);
+    if (px == NULL || b0 == NULL || tmp == NULL)
+    {
+        free(px); free(b0); free(tmp);
+        return -1;
+    }
+    for (int i = 0; i < n; i++) px[i] = b[d->fwd_pmt_idx[i]];
+    for (int pass = 0; pass < 2; pass++)
+    {
+        const int up = pass == 0;
+        if (!(op & (up ? 1 : 2))) continue;
+        for (int t = 0; t <= d->max_level; t++)
+        {
+            const int lvl = up ? d->max_level - t : t;
+            for (int j = 0; j < d->level_n_node[lvl]; j++)
+            {
+                const int node = d->level_nodes[(size_t) lvl * d->n_leaf_node + j];
+                const int m = d->m[node];
+                const int has_q = lvl > 0 && d->q_ncol[node] > 0;
+                for (int k = 0; k < m; k++) b0[k] = px[d->idx[node][k]];
+                ulv_node(d, node, has_q, up, b0, tmp);
+                for (int k = 0; k < m; k++) px[d->idx[node][k]] = b0[k];
+            }
+        }
+    }
+    for (int i = 0; i < n; i++) x[i] = px[d->bwd_pmt_idx[i]];
+    free(px); free(b0); free(tmp);
+    return 0;
 }

@@ -42,6 +42,8 @@ REF_SYMBOLS.update({
     "H2P_HSS_ULV_LU_factorize": (None, [C.c_void_p, C.c_double]),
     "H2P_HSS_ULV_Cholesky_solve": (None, [C.c_void_p, C.c_int, _dp, _dp]),
     "H2P_HSS_ULV_LU_solve": (None, [C.c_void_p, C.c_int, _dp, _dp]),
+    "h2pb_describe_ulv": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(_abi.UlvDesc), C.POINTER(C.c_void_p)]),
+    "h2pb_free": (None, [C.c_void_p]),
 })
 ORACLE_SYMBOLS = {
     "h2o_eval": (None, [C.c_int, _dp, C.c_int, _dp, C.c_int, C.c_int, _dp, C.c_int, C.c_int, _dp, C.c_int]),
@@ -49,6 +51,7 @@ ORACLE_SYMBOLS = {
     "h2o_matmul": (C.c_int, [C.POINTER(_abi.Desc), C.c_int, C.c_int, _dp, C.c_int, _dp, C.c_int]),
     "h2o_direct_sum": (None, [C.c_int, _dp, C.c_int, C.c_int, C.c_int, _dp, C.c_int, C.c_int, _dp,
                               _dp, C.c_int, C.c_int, _dp]),
+    "h2o_ulv_solve": (C.c_int, [C.POINTER(_abi.UlvDesc), C.c_int, _dp, _dp]),
 }
 
 _libs: dict = {}
@@ -352,6 +355,23 @@ class RefH2:
         """The reference's HSS ULV factorization (src/H2Pack_HSS_ULV.c:601 / :16)."""
         (self.lib.H2P_HSS_ULV_LU_factorize if lu else self.lib.H2P_HSS_ULV_Cholesky_factorize)(self.h2pack, shift)
         self._ulv_lu = bool(lu)
+
+    def ulv_solve_oracle(self, b: np.ndarray, op: int = 3) -> np.ndarray:
+        """The restatement's ULV solve (h2_oracle.c, h2o_ulv_solve) on this handle's
+        factors, through the plain h2gpu_ulv_desc view."""
+        d = _abi.UlvDesc()
+        buf = C.c_void_p()
+        st = self.lib.h2pb_describe_ulv(self.h2pack, int(self._ulv_lu), C.byref(d), C.byref(buf))
+        if st != 0:
+            raise RuntimeError(f"h2pb_describe_ulv status {st}")
+        try:
+            b = np.ascontiguousarray(b, dtype=np.float64)
+            x = np.empty(self.N)
+            if liboracle().h2o_ulv_solve(C.byref(d), int(op), dptr(b), dptr(x)) != 0:
+                raise RuntimeError("h2o_ulv_solve failed")
+            return x
+        finally:
+            self.lib.h2pb_free(buf)
 
     def ulv_solve(self, b: np.ndarray, op: int = 3) -> np.ndarray:
         """The reference's ULV solve on the CPU (src/H2Pack_HSS_ULV.c:981 / :429)."""

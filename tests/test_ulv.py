@@ -4,7 +4,9 @@ The factorizations stay H2Pack's own (src/H2Pack_HSS_ULV.c:601, :16); the solves
 (:981-1159, :429-599) run on the device, one launch per tree level.  Checks:
 
 - CPU: the reference library's own factorization and solve of (A + shift I) invert the
-  HSS operator (pins the checker); without a device the GPU solve refuses (no CPU path).
+  HSS operator, and the restatement in oracle/h2_oracle.c reproduces the reference's
+  solve on the same factors (pins the checker); without a device the GPU solve refuses
+  (no CPU path); malformed factors are refused on the host.
 - GPU: the device solve of every op (1, 2, 3) agrees with H2Pack's solve on the same
   handle's factors (its own code, compiled into the library under the name
   H2P_HSS_ULV_*_solve_host); op 3 inverts the shifted HSS operator; the drop-in entry
@@ -45,6 +47,20 @@ def _dp(a):
     return a.ctypes.data_as(C.POINTER(C.c_double))
 
 
+def _oracle_solve(H, lu, b, op):
+    """h2o_ulv_solve (oracle/h2_oracle.c) on the factors of the drop-in's handle H."""
+    from h2pack_b200 import _abi
+    d = _abi.UlvDesc()
+    buf = C.c_void_p()
+    assert H.lib.h2pb_describe_ulv(H.h2pack, int(lu), C.byref(d), C.byref(buf)) == 0
+    try:
+        x = np.empty(H.N)
+        assert oracle.liboracle().h2o_ulv_solve(C.byref(d), int(op), _dp(b), _dp(x)) == 0
+        return x
+    finally:
+        H.lib.h2pb_free(buf)
+
+
 def test_reference_ulv_inverts_the_hss_operator():
     R = _build_ref("gaussian", make_points("gaussian", 3000, 61))
     try:
@@ -52,6 +68,22 @@ def test_reference_ulv_inverts_the_hss_operator():
         b = np.random.default_rng(1).standard_normal(R.N)
         x = R.ulv_solve(b, 3)
         assert rel(R.matvec(x) + 1e-2 * x, b) < 1e-9
+    finally:
+        R.close()
+
+
+@pytest.mark.parametrize("kernel,lu,shift", [("gaussian", False, 1e-2), ("gaussian", True, 1e-2),
+                                              ("matern32", False, 1e-1), ("coulomb", True, 1.0)])
+def test_oracle_ulv_solve_pinned_to_reference(kernel, lu, shift):
+    """The restatement (oracle/h2_oracle.c, h2o_ulv_solve) over the plain descriptor of
+    the reference library's own factors gives the reference's solve, every op."""
+    R = _build_ref(kernel, make_points(kernel, 6000, 66))
+    try:
+        R.ulv_factorize(shift, lu=lu)
+        rng = np.random.default_rng(9)
+        for op in (1, 2, 3):
+            b = rng.standard_normal(R.N)
+            assert rel(R.ulv_solve_oracle(b, op), R.ulv_solve(b, op)) < 1e-12, op
     finally:
         R.close()
 
@@ -175,6 +207,8 @@ def test_gpu_ulv_solve_matches_h2pack(kernel, lu, shift):
             xh = np.empty(H.N)
             host(H.h2pack, op, _dp(b), _dp(xh))          # H2Pack's solve, same factors
             assert rel(x, xh) < TOL, (op, rel(x, xh))
+            # the restatement (each of the two within TOL of H2Pack's solve)
+            assert rel(x, _oracle_solve(H, lu, b, op)) < 2 * TOL, op
             xd = np.empty(H.N)
             dropin(H.h2pack, op, _dp(b), _dp(xd))        # the replaced entry point
             assert np.array_equal(xd, x)
