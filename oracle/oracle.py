@@ -8,7 +8,11 @@ this module, and only as the checker.  It wraps two libraries built by
   (construction + CPU ``H2P_matvec`` / ``H2P_matmul``), the ground truth;
 * ``libh2oracle.so`` -- ``h2_oracle.c``, a plain-C restatement of the apply
   path over the flat ``h2gpu_desc`` view, pinned to ``libh2ref.so`` by
-  ``tests/test_oracle_pin.py``.
+  ``tests/test_oracle_pin.py``, and of the HSS ULV solves over ``h2gpu_ulv_desc``,
+  pinned by ``tests/test_ulv.py``.
+
+It also runs the reference's own column-pivoted QR (``ref_pivot_qr``) as the checker
+of the construction's interpolative decompositions.
 
 It also converts a descriptor to and from plain numpy arrays, which is the
 format of the golden fixtures in ``tests/golden``.
