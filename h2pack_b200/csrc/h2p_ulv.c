@@ -146,78 +146,36 @@ DROPIN_API int H2P_gpu_ULV_release(H2Pack_p h)
     return H2GPU_OK;
 }
 
-/* the descriptor of the handle's factors (arrays owned by the caller's buffers) */
+/* h2p_builder.c: the handle's factors as an h2gpu_ulv_desc */
+int h2pb_describe_ulv(H2Pack_p h, int lu, h2gpu_ulv_desc *d, void **buf);
+
+/* the handle's factors onto the device; records its own failure message */
 static int upload(H2Pack_p h, int lu, h2gpu_ulv **out)
 {
-    const int n = h->n_node;
-    int *ints = (int *) malloc(sizeof(int) * 4 * (size_t) n);
-    const void **ptrs = (const void **) malloc(sizeof(void *) * 4 * (size_t) n);
-    int st = H2GPU_OK;
-    if (ints == NULL || ptrs == NULL)
-    {
-        free(ints);
-        free(ptrs);
-        return h2p_dropin_fail(H2GPU_ERR_NOMEM, "H2P_HSS_ULV_solve", "host allocation");
-    }
-    int *m = ints, *qn = ints + n, *ld = ints + 2 * n, *Ls = ints + 3 * n;
-    const int **idx = (const int **) ptrs;
-    const double **Q = (const double **) (ptrs + n), **L = (const double **) (ptrs + 2 * n);
-    const int **p = (const int **) (ptrs + 3 * n);
+    const char *what = "H2P_HSS_ULV_solve";
+    h2gpu_ulv_desc d;
+    void *buf = NULL;
+    int st = h2pb_describe_ulv(h, lu, &d, &buf);
+    if (st == H2GPU_ERR_STATE)
+        return h2p_dropin_fail(st, what, lu ? "the handle holds no LU factors (H2P_HSS_ULV_LU_factorize)"
+                                            : "the handle's ULV factors are incomplete");
+    if (st != H2GPU_OK) return h2p_dropin_fail(st, what, "host allocation");
+    /* the reference's solve assumes these shapes (src/H2Pack_HSS_ULV.c:1036-1046) */
     const int root = h->level_nodes[0];
-    for (int i = 0; i < n && st == H2GPU_OK; i++)
+    for (int i = 0; i < h->n_node && st == H2GPU_OK; i++)
     {
-        H2P_int_vec_p ix = h->ULV_idx[i];
         H2P_dense_mat_p q = h->ULV_Q[i], l = h->ULV_L[i];
-        if (ix == NULL || q == NULL || l == NULL || (lu && (h->ULV_p == NULL || h->ULV_p[i] == NULL)))
-        {
-            st = h2p_dropin_fail(H2GPU_ERR_STATE, "H2P_HSS_ULV_solve",
-                                 lu ? "the handle holds no LU factors (H2P_HSS_ULV_LU_factorize)"
-                                    : "the handle's ULV factors are incomplete");
-            break;
-        }
-        m[i] = ix->length;
-        Ls[i] = h->ULV_Ls[i];
-        ld[i] = l->ld;
-        qn[i] = i == root ? 0 : q->ncol;
-        idx[i] = ix->data;
-        L[i] = l->data;
-        Q[i] = i == root ? NULL : q->data;
-        p[i] = lu ? h->ULV_p[i]->data : NULL;
-        /* the reference's solve assumes these shapes (src/H2Pack_HSS_ULV.c:1036-1046) */
-        if (l->nrow != m[i] || l->ncol != m[i] || (i != root && q->ncol > 0 && (q->nrow != m[i] + 1 || q->ld != q->ncol)) ||
-            (lu && h->ULV_p[i]->length != m[i] - Ls[i]))
-        {
-            st = h2p_dropin_fail(H2GPU_ERR_INVALID, "H2P_HSS_ULV_solve", "factor shapes differ from H2Pack's layout");
-            break;
-        }
+        if (l->nrow != d.m[i] || l->ncol != d.m[i] ||
+            (i != root && q->ncol > 0 && (q->nrow != d.m[i] + 1 || q->ld != q->ncol)) ||
+            (lu && h->ULV_p[i]->length != d.m[i] - d.Ls[i]))
+            st = h2p_dropin_fail(H2GPU_ERR_INVALID, what, "factor shapes differ from H2Pack's layout");
     }
     if (st == H2GPU_OK)
     {
-        h2gpu_ulv_desc d;
-        memset(&d, 0, sizeof(d));
-        d.lu = lu;
-        d.n_node = n;
-        d.max_level = h->max_level;
-        d.n_leaf_node = h->n_leaf_node;
-        d.krnl_mat_size = h->krnl_mat_size;
-        d.level_n_node = h->level_n_node;
-        d.level_nodes = h->level_nodes;
-        d.fwd_pmt_idx = h->fwd_pmt_idx;
-        d.bwd_pmt_idx = h->bwd_pmt_idx;
-        d.Ls = Ls;
-        d.m = m;
-        d.q_ncol = qn;
-        d.l_ld = ld;
-        d.idx = idx;
-        d.Q = Q;
-        d.L = L;
-        d.p = lu ? p : NULL;
-        d.device = -1;
         st = h2gpu_ulv_create(&d, out);
         if (st != H2GPU_OK) h2p_dropin_fail(st, "uploading the ULV factors", NULL);
     }
-    free(ints);
-    free(ptrs);
+    free(buf);
     return st;
 }
 

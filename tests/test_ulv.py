@@ -95,8 +95,13 @@ def test_gpu_solve_has_no_cpu_fallback():
     H, _ = _build("gaussian", 2000, 62)
     try:
         H.ulv_factorize(1e-2)
-        with pytest.raises(RuntimeError):
+        # H2Pack's factors pass every host check of h2gpu_ulv_create; only the device is missing
+        with pytest.raises(RuntimeError, match="no CUDA device"):
             H.ulv_solve(np.ones(H.N))
+        # an LU solve on a Cholesky-factored handle: no LU factors to upload
+        b, x = np.ones(H.N), np.empty(H.N)
+        st = H.lib.H2P_gpu_ULV_solve(H.h2pack, 1, 3, _dp(b), _dp(x))
+        assert st != 0 and "LU factors" in H.lib.H2P_gpu_last_error().decode()
     finally:
         H.close()
 
