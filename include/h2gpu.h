@@ -418,7 +418,9 @@ int h2gpu_pp_sketch_id(int kernel_id, const double *krnl_param, int n_krnl_param
  *   L[i], l_ld[i]       ULV_L[i]: m[i] x m[i] row-major;
  *   p[i]                LU only: ULV_p[i], m[i] - Ls[i] entries.
  * The device keeps each node's explicit Q (formed from the reflectors at create) and
- * L, both m x m, and runs one launch per tree level per sweep (one CTA per node).
+ * L, both m x m, and runs one launch per tree level per sweep (one CTA per node, the
+ * node's vector in shared memory: nodes of more than 13,872 rows are refused with
+ * H2GPU_ERR_UNSUPPORTED).
  */
 typedef struct h2gpu_ulv h2gpu_ulv;
 
