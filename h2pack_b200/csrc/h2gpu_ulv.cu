@@ -544,12 +544,17 @@ H2G_API int h2gpu_ulv_create(const h2gpu_ulv_desc* d, h2gpu_ulv** out)
     if (d_jobs) cudaFree(d_jobs);
     if (st == H2GPU_OK)
     {
-        const int sm = smem_bytes(m_cap);
-        for (cudaError_t e : {cudaFuncSetAttribute(k_ulv_level<CH_UP>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm),
-                              cudaFuncSetAttribute(k_ulv_level<CH_DOWN>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm),
-                              cudaFuncSetAttribute(k_ulv_level<LU_UP>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm),
-                              cudaFuncSetAttribute(k_ulv_level<LU_DOWN>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm)})
-            step(e, "shared memory of the solve kernels");
+        // The limit is a per-function setting of the process: it is set to the device's
+        // opt-in maximum, the same value for every object, so that creating a
+        // factorization with smaller nodes never lowers it under another's launches.
+        int optin = 0;
+        if (step(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev), "device query") &&
+            smem_bytes(m_cap) > optin)
+            st = ulv_fail(H2GPU_ERR_UNSUPPORTED, "a node of %d rows exceeds one CTA's shared memory", m_cap);
+        for (auto kern : {k_ulv_level<CH_UP>, k_ulv_level<CH_DOWN>, k_ulv_level<LU_UP>, k_ulv_level<LU_DOWN>})
+            if (st == H2GPU_OK)
+                step(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, optin),
+                     "shared memory of the solve kernels");
     }
     if (st != H2GPU_OK)
     {

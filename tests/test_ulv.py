@@ -236,3 +236,25 @@ def test_gpu_ulv_follows_refactorization():
             assert rel(H.matvec(x) + shift * x, b) < 1e-8, (shift, lu)
     finally:
         H.close()
+
+
+@pytest.mark.gpu
+def test_gpu_two_factorizations_alive():
+    """Two handles' factors on the device at once, the second with smaller nodes: the
+    first still solves, bit for bit as before (the solve kernels' shared-memory limit is
+    a process-wide setting that a later, smaller factorization must not lower)."""
+    A, _ = _build("gaussian", 12000, 67)
+    B, _ = _build("gaussian", 1500, 68)
+    try:
+        A.ulv_factorize(1e-2)
+        B.ulv_factorize(1e-2)
+        rng = np.random.default_rng(10)
+        ba, bb = rng.standard_normal(A.N), rng.standard_normal(B.N)
+        xa = A.ulv_solve(ba)
+        xb = B.ulv_solve(bb)
+        assert np.array_equal(A.ulv_solve(ba), xa)
+        assert rel(A.matvec(xa) + 1e-2 * xa, ba) < 1e-8
+        assert rel(B.matvec(xb) + 1e-2 * xb, bb) < 1e-8
+    finally:
+        A.close()
+        B.close()
