@@ -525,11 +525,27 @@ def run_ulv(args):
         H.lib.H2P_HSS_ULV_Cholesky_solve_host(H.h2pack, 3, dp(b), dp(xh))
     cpu_ms = (time.perf_counter() - t0) / reps * 1e3
     launches = 2 * (H.info["max_level"] + 1) + 2
+    # algorithmic bytes per solve: every node's L, and Q below the root, read once per sweep
+    from h2pack_b200 import _abi
+    d, buf = _abi.UlvDesc(), C.c_void_p()
+    factor_bytes = None
+    if H.lib.h2pb_describe_ulv(H.h2pack, 0, C.byref(d), C.byref(buf)) == 0:
+        root = d.level_nodes[0]
+        factor_bytes = sum(8.0 * d.m[i] ** 2 * (1 + (i != root and d.q_ncol[i] > 0)) for i in range(d.n_node))
+        H.lib.h2pb_free(buf)
+    peak = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]) \
+        if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else 6650.0
+    roof = None
+    if factor_bytes:
+        gbs = 2 * factor_bytes / (ms * 1e-3) / 1e9
+        roof = {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak, "traffic": None,
+                "note": f"{2 * factor_bytes / 1e9:.3f} GB of Q and L per solve (two sweeps) / solve time incl. "
+                        "host copies"}
     line = {"metric": f"HSS ULV solves/s (Gaussian N={n}, Cholesky, op 3, host arrays)", "value": 1e3 / ms,
             "unit": "solves/s", "workload": "ulv", "n": n, "ms_per_solve": ms, "steps": args.steps,
             "warmup": args.warmup, "dtype": "f64", "build_seconds": build_s, "factorize_seconds": fact_s,
             "first_solve_seconds": first_s, "gpu_launches": launches, "max_level": H.info["max_level"],
-            "parity_vs_h2pack_solve": rel2(x, xh), "residual_vs_hss_operator": residual,
+            "parity_vs_h2pack_solve": rel2(x, xh), "residual_vs_hss_operator": residual, "roofline": roof,
             "cpu_baseline": {"value": 1e3 / cpu_ms, "unit": "solves/s", "cores": threads, "kind": "reference",
                              "sample": f"{reps} H2P_HSS_ULV_Cholesky_solve of H2Pack's code on the same factors"}}
     print(json.dumps(line), flush=True)
