@@ -5,6 +5,8 @@
   unchanged against the drop-in library by oracle/Makefile, run with "0" on stdin (do not
   store the matrix) and print their error against their own direct N-body sum; it must
   stay within the construction tolerance 1e-6 that the programs print beside it.
+* H2Pack's own extra/test_HSS_scalar.c (HSS build, matvec, ULV LU factorization and
+  solve) runs unchanged on the drop-in; its errors stay within the spread of its CPU build.
 * Two handles applied from two host threads at once give the results they give alone.
 * A handle whose arrays change in place (same addresses and sizes) is re-uploaded.
 * H2P_destroy releases the handle's device image.
@@ -39,6 +41,29 @@ def test_reference_example_runs_unchanged_on_the_dropin(program, tmp_path):
     err, tol = float(m.group(1)), float(t.group(1))
     print(f"{program}: error {err:.3e} (threshold {tol:.0e})")
     assert err <= tol
+
+
+def test_reference_hss_test_program_runs_unchanged_on_the_dropin(tmp_path):
+    """H2Pack's own extra/test_HSS_scalar.c (Gaussian kernel, N = 8,000, JIT mode): an
+    HSS build, H2P_matvec against its direct N-body sum, then H2P_HSS_ULV_LU_factorize
+    with shift 0 and H2P_HSS_ULV_LU_solve of A x0, compiled unchanged against the
+    drop-in by oracle/Makefile, so that the apply and the ULV solve run on the GPU.  The
+    program draws its points from the clock; the bounds cover the spread of its CPU
+    build (oracle/_ref/test_HSS_scalar_cpu) over three runs at this size: HSS error
+    1.3e-5 .. 5.8e-5, solve error 1.1e-11 .. 4.2e-11."""
+    exe = os.path.join(REF_BIN, "test_HSS_scalar_gpu")
+    assert os.path.exists(exe), f"{exe} is built by oracle/Makefile (make -C oracle examples)"
+    env = dict(os.environ, OMP_NUM_THREADS=str(min(os.cpu_count() or 8, 32)), OPENBLAS_NUM_THREADS="1")
+    args = ["3", "8000", "1e-6", "1", "1", str(tmp_path / "pp_gaussian.dat")]
+    r = subprocess.run([exe, *args], capture_output=True, text=True, cwd=tmp_path, env=env, timeout=900)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    m = re.search(r"validation points: \|\|y_\{HSS\} - y\|\|_2 / \|\|y\|\|_2 = ([0-9.eE+-]+)", r.stdout)
+    u = re.search(r"H2P_HSS_ULV_LU_solve relerr = ([0-9.eE+-]+)", r.stdout)
+    assert m and u, r.stdout[-2000:]
+    err, solve_err = float(m.group(1)), float(u.group(1))
+    print(f"test_HSS_scalar on the drop-in: HSS error {err:.3e}, ULV LU solve error {solve_err:.3e}")
+    assert err < 1e-3
+    assert solve_err < 1e-8
 
 
 def test_two_handles_from_two_threads():
