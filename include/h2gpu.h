@@ -377,10 +377,13 @@ int h2gpu_direct_sum(int kernel_id, const double *krnl_param, int n_krnl_param,
  * QR, whose first rank[b] entries are the skeleton candidates; *E: a buffer allocated
  * here (release with h2gpu_free) holding E_b (rank x (ncand - rank), column-major,
  * ld = rank) from element e_off[b] (e_off has n_blk + 1 entries); with E = NULL only
- * rank and perm are computed (e_off unused).  Pivot choices can
- * differ from the CPU's where two column norms agree to rounding, so skeletons match
- * the reference's in accuracy, not index by index.  No counterpart beyond
- * H2Pack's internal function.
+ * rank and perm are computed (e_off unused).  Each block takes one CTA, except
+ * blocks whose work space exceeds a CTA's shared memory and blocks of at least 2^20
+ * entries in a batch with fewer than 64 of them: those are decomposed one at a time
+ * over the whole GPU (two launches per pivot step), with the same arithmetic.  Pivot
+ * choices can differ from the CPU's where two downdated column norms agree to
+ * rounding, so skeletons match the reference's in accuracy, not always index by
+ * index.  No counterpart beyond H2Pack's internal function.
  */
 int h2gpu_id_batch(int kernel_id, const double *krnl_param, int n_krnl_param, double reltol, int n_blk,
                    const int *ncand, int npp, const double *cand, const double *prox, int *rank, int *perm,
@@ -395,7 +398,8 @@ void h2gpu_free(void *p);
  * sketch W = K(X0, Y0) S of nx candidate points X0 against ny outer points Y0 (both
  * 3 x n, dim-major), S given as S^T in CSR (nx rows: st_rowptr[nx + 1], st_col,
  * st_val; H2P_gen_rand_sparse_mat_trans's output), followed by the interpolative
- * decomposition of W's rows at reltol (as h2gpu_id_batch, skeletons only): rank and
+ * decomposition of W's rows at reltol (as h2gpu_id_batch, skeletons only, over the
+ * whole GPU): rank and
  * perm (nx; the first rank entries are the selected candidates).
  */
 int h2gpu_pp_sketch_id(int kernel_id, const double *krnl_param, int n_krnl_param, double reltol, int nx,
