@@ -7,6 +7,8 @@
   stay within the construction tolerance 1e-6 that the programs print beside it.
 * H2Pack's own extra/test_HSS_scalar.c (HSS build, matvec, ULV LU factorization and
   solve) runs unchanged on the drop-in; its errors stay within the spread of its CPU build.
+* examples/SPDHSS-H2/example_regularHSS.c (PCG on an H2 operator preconditioned by the
+  HSS ULV solve) runs unchanged on the drop-in and converges as its CPU build does.
 * Two handles applied from two host threads at once give the results they give alone.
 * A handle whose arrays change in place (same addresses and sizes) is re-uploaded.
 * H2P_destroy releases the handle's device image.
@@ -64,6 +66,31 @@ def test_reference_hss_test_program_runs_unchanged_on_the_dropin(tmp_path):
     print(f"test_HSS_scalar on the drop-in: HSS error {err:.3e}, ULV LU solve error {solve_err:.3e}")
     assert err < 1e-3
     assert solve_err < 1e-8
+
+
+def test_reference_hss_preconditioned_pcg_runs_unchanged_on_the_dropin(tmp_path):
+    """H2Pack's examples/SPDHSS-H2/example_regularHSS.c (Gaussian l = 0.1, shift 1,
+    N = 8,000, JIT mode): an H2 matrix applied by H2P_matvec, a rank-100 HSS matrix,
+    H2P_HSS_ULV_Cholesky_factorize, and PCG on the shifted H2 operator preconditioned by
+    H2P_HSS_ULV_Cholesky_solve (pcg_tests.c:41-45), compiled unchanged against the
+    drop-in: both the operator and the preconditioner run on the GPU.  Its CPU build
+    (oracle/_ref/example_regularHSS_cpu) converged in 4 iterations to a relative
+    residual of 6.1e-5 .. 6.6e-5 in three runs (points drawn from the clock)."""
+    exe = os.path.join(REF_BIN, "example_regularHSS_gpu")
+    assert os.path.exists(exe), f"{exe} is built by oracle/Makefile (make -C oracle examples)"
+    env = dict(os.environ, OMP_NUM_THREADS=str(min(os.cpu_count() or 8, 32)), OPENBLAS_NUM_THREADS="1")
+    args = ["3", "8000", "1e-6", "1", "1", "random", "0.1", "1.0"]
+    r = subprocess.run([exe, *args], capture_output=True, text=True, cwd=tmp_path, env=env, timeout=900)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    if "The constructed HSS matrix is non-SPD" in r.stdout:
+        pytest.skip("this random point set gave a non-SPD rank-100 HSS matrix (the program skips PCG)")
+    assert "The constructed HSS matrix is SPD" in r.stdout, r.stdout[-2000:]
+    it = re.search(r"PCG: Converged in (\d+) iterations", r.stdout)
+    rr = re.search(r"PCG stopped after \d+ iterations, relres = ([0-9.eE+-]+)", r.stdout)
+    assert it and rr, r.stdout[-2000:]
+    print(f"example_regularHSS on the drop-in: {it.group(1)} iterations, relres {rr.group(1)}")
+    assert int(it.group(1)) <= 10
+    assert float(rr.group(1)) < 1e-4
 
 
 def test_two_handles_from_two_threads():
