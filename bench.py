@@ -494,7 +494,7 @@ def run_ulv(args):
     two vector permutations go through the drop-in's GPU permutation)."""
     os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")   # H2Pack's OpenMP threads call BLAS
     import ctypes as C
-    from h2pack_b200 import H2Matrix
+    from h2pack_b200 import H2Matrix, _abi
     n = 20_000 if args.n == 1_000_000 else args.n
     shift = 1e-2
     threads = min(16, os.cpu_count() or 1)
@@ -518,6 +518,7 @@ def run_ulv(args):
     residual = rel2(H.matvec(x) + shift * x, b)
     dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
     xh = np.empty(H.N)
+    _abi.blas_one_thread(H.lib)    # H2Pack's solve calls BLAS inside its OpenMP loops
     H.lib.H2P_HSS_ULV_Cholesky_solve_host(H.h2pack, 3, dp(b), dp(xh))
     reps = 5
     t0 = time.perf_counter()
@@ -526,7 +527,6 @@ def run_ulv(args):
     cpu_ms = (time.perf_counter() - t0) / reps * 1e3
     launches = 2 * (H.info["max_level"] + 1) + 2
     # algorithmic bytes per solve: every node's L, and Q below the root, read once per sweep
-    from h2pack_b200 import _abi
     d, buf = _abi.UlvDesc(), C.c_void_p()
     factor_bytes = None
     if H.lib.h2pb_describe_ulv(H.h2pack, 0, C.byref(d), C.byref(buf)) == 0:

@@ -218,6 +218,20 @@ def libh2pack_gpu() -> C.CDLL:
     return _load(LIBH2PACK_GPU, [H2PACK_GPU_SYMBOLS, BUILDER_SYMBOLS])
 
 
+def blas_one_thread(lib: C.CDLL) -> None:
+    """Pin the OpenBLAS that H2Pack's code in `lib` calls to one thread.  H2Pack's ULV
+    factorizations and solves call BLAS / LAPACK from inside their OpenMP loops
+    (src/H2Pack_HSS_ULV.c), and its construction leaves the BLAS at n_thread threads
+    (src/H2Pack_build.c:269, :644); with a pthreads OpenBLAS, such nested calls from
+    several OpenMP threads race.  One BLAS thread per OpenMP thread is how H2Pack's own
+    construction loops call it."""
+    f = getattr(lib, "openblas_set_num_threads", None)
+    if f is not None:
+        f.argtypes = [C.c_int]
+        f.restype = None
+        f(1)
+
+
 def check(status: int, lib: C.CDLL | None = None, what: str = "") -> None:
     if status != H2GPU_OK:
         msg = ""

@@ -321,6 +321,7 @@ class H2Matrix:
         if not self._hss:
             raise RuntimeError("the ULV factorization needs a matrix built with hss=True")
         fn = self.lib.H2P_HSS_ULV_LU_factorize if lu else self.lib.H2P_HSS_ULV_Cholesky_factorize
+        _abi.blas_one_thread(self.lib)
         fn(self.h2pack, float(shift))
         self._ulv_lu = bool(lu)
 

@@ -357,6 +357,7 @@ class RefH2:
 
     def ulv_factorize(self, shift: float = 0.0, lu: bool = False):
         """The reference's HSS ULV factorization (src/H2Pack_HSS_ULV.c:601 / :16)."""
+        _abi.blas_one_thread(self.lib)
         (self.lib.H2P_HSS_ULV_LU_factorize if lu else self.lib.H2P_HSS_ULV_Cholesky_factorize)(self.h2pack, shift)
         self._ulv_lu = bool(lu)
 
@@ -381,6 +382,7 @@ class RefH2:
         """The reference's ULV solve on the CPU (src/H2Pack_HSS_ULV.c:981 / :429)."""
         b = np.ascontiguousarray(b, dtype=np.float64)
         x = np.empty(self.N)
+        _abi.blas_one_thread(self.lib)
         (self.lib.H2P_HSS_ULV_LU_solve if self._ulv_lu else self.lib.H2P_HSS_ULV_Cholesky_solve)(
             self.h2pack, int(op), dptr(b), dptr(x))
         return x
