@@ -74,11 +74,12 @@ def test_reference_ulv_inverts_the_hss_operator():
 
 
 @pytest.mark.parametrize("kernel,lu,shift", [("gaussian", False, 1e-2), ("gaussian", True, 1e-2),
-                                              ("matern32", False, 1e-1), ("coulomb", True, 1.0)])
+                                              ("matern32", False, 1e-1), ("coulomb", True, 1.0),
+                                              ("rpy", False, 1e-1), ("rpy", True, 1e-1)])
 def test_oracle_ulv_solve_pinned_to_reference(kernel, lu, shift):
     """The restatement (oracle/h2_oracle.c, h2o_ulv_solve) over the plain descriptor of
     the reference library's own factors gives the reference's solve, every op."""
-    R = _build_ref(kernel, make_points(kernel, 6000, 66))
+    R = _build_ref(kernel, make_points(kernel, 2000 if kernel == "rpy" else 6000, 66))
     try:
         R.ulv_factorize(shift, lu=lu)
         rng = np.random.default_rng(9)
@@ -225,6 +226,29 @@ def test_gpu_ulv_solve_matches_h2pack(kernel, lu, shift):
         assert rel(H.matvec(x) + shift * x, b) < 1e-8
     finally:
         H.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kernel,lu,shift", [("gaussian", False, 1e-2), ("rpy", False, 1e-1), ("rpy", True, 1e-1)])
+def test_gpu_ulv_solve_on_reference_handles(kernel, lu, shift):
+    """A handle built and factorized by the reference library itself, solved by the
+    drop-in on the GPU (the struct layout is H2Pack's): every op against the reference
+    library's own CPU solve of the same factors, the RPY tensor kernel (3 rows per
+    point) included."""
+    from h2pack_b200 import _abi
+    lib = _abi.libh2pack_gpu()
+    R = _build_ref(kernel, make_points(kernel, 2000 if kernel == "rpy" else 6000, 69))
+    try:
+        R.ulv_factorize(shift, lu=lu)
+        rng = np.random.default_rng(11)
+        for op in (1, 2, 3):
+            b = rng.standard_normal(R.N)
+            x = np.empty(R.N)
+            assert lib.H2P_gpu_ULV_solve(R.h2pack, int(lu), op, _dp(b), _dp(x)) == 0, lib.H2P_gpu_last_error()
+            assert rel(x, R.ulv_solve(b, op)) < TOL, op
+    finally:
+        lib.H2P_gpu_ULV_release(R.h2pack)    # the reference's H2P_destroy does not know the drop-in
+        R.close()
 
 
 @pytest.mark.gpu
