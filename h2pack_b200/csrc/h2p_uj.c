@@ -27,6 +27,7 @@
 #include <string.h>
 
 #include "H2Pack.h"
+#include "H2Pack_utils.h"
 #include "h2gpu.h"
 
 #define DROPIN_API __attribute__((visibility("default")))
